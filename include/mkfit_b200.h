@@ -1,0 +1,128 @@
+/*
+ * mkfit_b200 -- C ABI of the B200-native Kalman-filter tracking hot path.
+ *
+ * Plain C types only: pointers, sizes and POD structs. Every entry point
+ * returns an int status (MKFG_OK = 0), never aborts, and records a message
+ * retrievable with mkfg_last_error(). All device work is enqueued on the
+ * stream of the context (or the stream the caller passes), so calls from
+ * different host threads on different contexts are independent.
+ *
+ * Data layout (the reference's Matriplex layout, Matriplex/Matriplex.h:63-68,
+ * widened to a whole batch): structure of arrays, lane fastest. Element e of
+ * item i lives at base[e * stride + i]. Track parameters are the reference's
+ * CCS coordinates (x, y, z, 1/pT, phi, theta); covariances are 21 floats in
+ * packed lower-triangle order (Matriplex/MatriplexSym.h:15-22); hit
+ * covariances are 6 floats in the same order.
+ */
+#ifndef MKFIT_B200_H
+#define MKFIT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+enum {
+  MKFG_OK = 0,
+  MKFG_ERR_BAD_INPUT = 1, /* invalid argument, size or pointer */
+  MKFG_ERR_CUDA = 2,      /* a CUDA runtime call failed */
+  MKFG_ERR_OVERFLOW = 3,  /* a device capacity was exceeded (results truncated) */
+  MKFG_ERR_TIMEOUT = 4,   /* a bounded device wait gave up */
+  MKFG_ERR_NO_DEVICE = 5  /* no usable sm_100 device */
+};
+
+/* Propagation flag bits (reference PropagationFlagsEnum, Config.h:17-23). */
+enum { MKFG_PF_NONE = 0, MKFG_PF_PARAM_BFIELD = 0x1, MKFG_PF_MATERIAL = 0x2 };
+
+/* Copies the calling thread's last error message (NUL-terminated). */
+void mkfg_last_error(char* buf, size_t len);
+
+/* Library version string, e.g. "mkfit_b200 0.1 sm_100a". */
+const char* mkfg_version(void);
+
+/* --------------------------------------------------------------- context */
+/* A context binds one CUDA device and one stream and owns the device copies
+ * of the material map, the detector geometry and scratch buffers for the
+ * host-buffer entry points. Replaces the reference's per-thread worker pools
+ * (mkFit/Pool.h:15-58, mkFit/MkBuilder.h:34-49). */
+typedef struct mkfg_context mkfg_context;
+
+int mkfg_context_create(int device, mkfg_context** out);
+int mkfg_context_destroy(mkfg_context* ctx);
+/* The cudaStream_t used by the context, as an opaque pointer. */
+void* mkfg_context_stream(mkfg_context* ctx);
+int mkfg_context_synchronize(mkfg_context* ctx);
+
+/* Upload the (z, r) material grid, 300 x 120 floats each, row = z bin
+ * (reference Config::RlgridME / XigridME, Config.h:123-165, filled there by
+ * fillZRgridME, MaterialEffects.h:277-290). Host pointers. */
+int mkfg_set_material(mkfg_context* ctx, const float* rl_grid, const float* xi_grid);
+
+/* Measures the device's FP32 FMA throughput (TFLOP/s) with a register-only
+ * kernel: the roofline denominator of this library's kernels, which run on
+ * the FP32 CUDA cores. No reference counterpart (measurement utility). */
+int mkfg_probe_fp32_peak(mkfg_context* ctx, int iters, double* tflops);
+
+/* ------------------------------------------------------------ track SoA */
+typedef struct {
+  float* par;   /* [6][stride]  */
+  float* err;   /* [21][stride] */
+  int32_t* chg; /* [stride]     */
+  int32_t n;    /* number of tracks */
+  int32_t stride;
+} mkfg_tracks;
+
+/* Hits of an event: all layers in one SoA buffer, layer l occupying items
+ * [layer_begin[l], layer_begin[l+1]). Reference: std::vector<HitVec>
+ * (Event.h) / Hit (Hit.h:185-304). */
+typedef struct {
+  const float* pos;          /* [3][stride] x, y, z */
+  const float* err;          /* [6][stride] packed symmetric */
+  const int32_t* layer_begin;/* [n_layers + 1], device pointer */
+  int32_t n_layers;
+  int32_t stride;
+} mkfg_hits;
+
+/* ------------------------------------------------------------------ fit */
+/* Kalman fit over a fixed sequence of hits per track: for each layer step
+ * l, propagate to the hit's radius (barrel) or z (endcap) and update.
+ * Replaces MkFitter::InputTracksForFit + FitTracksWithInterSlurp +
+ * OutputFittedTracks (mkFit/MkFitter.cc:286-363, 505-522) and the steered
+ * form FitTracksSteered (mkFit/MkFitter.cc:473-503).
+ *
+ *   hot_index [n_steps][hot_stride]: index of track i's hit within layer
+ *     hit_layer[l]; a negative index uses the layer's hit 0, as the
+ *     reference's packer does (mkFit/MkFitter.cc:344-348).
+ *   hit_layer [n_steps]: host array, layer of each step.
+ *   endcap_mask: bit l set -> step l is an endcap (z) step.
+ *   out_chi2 (optional, [n]): sum over steps of the predicted-residual chi2
+ *     (kalmanOperation with KFO_Calculate_Chi2|KFO_Update_Params).
+ * All array pointers are device pointers; in and out may alias. */
+typedef struct {
+  mkfg_tracks in;
+  mkfg_tracks out;
+  mkfg_hits hits;
+  const int32_t* hot_index;
+  int32_t hot_stride;
+  int32_t n_steps;
+  const int32_t* hit_layer; /* host */
+  uint64_t endcap_mask;
+  uint32_t pflags;
+  float* out_chi2;
+} mkfg_fit_args;
+
+int mkfg_fit(mkfg_context* ctx, const mkfg_fit_args* args);
+
+/* Same fit from HOST buffers: copies inputs to device scratch owned by the
+ * context, fits, copies outputs back, synchronizes. The pointers inside
+ * args (including hits.layer_begin) are host pointers here. */
+int mkfg_fit_host(mkfg_context* ctx, const mkfg_fit_args* args);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MKFIT_B200_H */

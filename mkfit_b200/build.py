@@ -1,0 +1,56 @@
+"""Builds the CUDA extension library in-tree for sm_100a.
+
+    python -m mkfit_b200.build            # -> mkfit_b200/_lib/libmkfit_b200.so
+
+The library is a plain shared object with a C ABI (include/mkfit_b200.h);
+Python loads it with ctypes. Incremental: objects are rebuilt when their
+source or any header in csrc/ is newer.
+"""
+import glob
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OUT_DIR = os.path.join(HERE, "_lib")
+OBJ_DIR = os.path.join(OUT_DIR, "obj")
+LIB = os.path.join(OUT_DIR, "libmkfit_b200.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+         "-Xptxas", "-warn-spills"]
+
+
+def _newer(dst, srcs):
+    if not os.path.exists(dst):
+        return True
+    t = os.path.getmtime(dst)
+    return any(os.path.getmtime(s) > t for s in srcs)
+
+
+def build(verbose=False, extra_flags=()):
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    gen = os.path.join(CSRC, "generated_ops.cuh")
+    if _newer(gen, [os.path.join(CSRC, "gen_ops.py")]):
+        subprocess.check_call([sys.executable, os.path.join(CSRC, "gen_ops.py")])
+    headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) + \
+        glob.glob(os.path.join(HERE, "..", "include", "*.h"))
+    objs = []
+    for src in sorted(glob.glob(os.path.join(CSRC, "*.cu"))):
+        obj = os.path.join(OBJ_DIR, os.path.basename(src)[:-3] + ".o")
+        objs.append(obj)
+        if _newer(obj, [src] + headers):
+            cmd = [NVCC] + ARCH + FLAGS + list(extra_flags) + ["-c", src, "-o", obj]
+            if verbose:
+                print(" ".join(cmd))
+            subprocess.check_call(cmd)
+    if _newer(LIB, objs):
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        subprocess.check_call(cmd)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose=True))

@@ -1,0 +1,76 @@
+"""Pins the oracle: the FP64 restatement against the reference's own CPU
+Matriplex fit (compiled from the reference sources) and against the golden
+fixtures that reference produced."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from mkfit_b200 import synth
+from tests.tolerances import par_scaled_err, cov_scaled_err
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "fit_*.npz")))
+
+
+def _grids(g):
+    return synth.toy_material_grid(g["radii"])
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=os.path.basename)
+def test_reference_reproduces_golden(reflib, path):
+    """The in-process reference build reproduces the committed fixtures
+    bit for bit (same Matriplex width)."""
+    g = np.load(path)
+    if reflib.width() != int(g["matriplex_width"]):
+        pytest.skip("fixture made with another Matriplex width")
+    rl, xi = _grids(g)
+    par, err, chg, _ = reflib.fit(g["par"], g["err"], g["chg"], g["hit_pos"], g["hit_err"], rl, xi,
+                                  pflags=int(g["pflags"]))
+    np.testing.assert_array_equal(par, g["ref_par"])
+    np.testing.assert_array_equal(err, g["ref_err"])
+    np.testing.assert_array_equal(chg, g["ref_chg"])
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=os.path.basename)
+def test_restatement_matches_golden(restate, path):
+    """FP64 restatement vs the reference's FP32 outputs: agreement at the
+    level of FP32 rounding of the same algorithm."""
+    g = np.load(path)
+    rl, xi = _grids(g)
+    par, err, _ = restate.fit(g["par"], g["err"], g["chg"], g["hit_pos"], g["hit_err"], rl, xi,
+                              pflags=int(g["pflags"]))
+    ep = par_scaled_err(g["ref_par"], par, err)
+    ec = cov_scaled_err(g["ref_err"], err)
+    assert np.median(ep) < 1e-6
+    assert ep.max() < 1e-3
+    assert np.median(ec) < 1e-5
+    assert ec.max() < 5e-3
+
+
+def test_restatement_matches_reference_fresh(reflib, restate):
+    """Same check on a fresh 2000-track toy event run through the reference
+    build (not only the fixtures)."""
+    ev = synth.gen_fit_event(2000, seed=77)
+    par, err, _, _ = reflib.fit(ev.par, ev.err, ev.chg, ev.hit_pos, ev.hit_err, ev.rl_grid,
+                                ev.xi_grid, pflags=2)
+    dpar, derr, chi2 = restate.fit(ev.par, ev.err, ev.chg, ev.hit_pos, ev.hit_err, ev.rl_grid,
+                                   ev.xi_grid, pflags=2)
+    ep = par_scaled_err(par, dpar, derr)
+    ec = cov_scaled_err(err, derr)
+    assert np.percentile(ep, 99.9) < 1e-4
+    assert np.percentile(ec, 99.9) < 1e-3
+    # Physics sanity of the synthetic event + fit: chi2/ndf of order 1.
+    assert 0.3 < np.median(chi2) / 20 < 2.0
+
+
+def test_reference_threads_deterministic(reflib):
+    """The reference's results do not depend on the shim's thread count."""
+    ev = synth.gen_fit_event(1000, seed=5)
+    reflib.set_threads(1)
+    a = reflib.fit(ev.par, ev.err, ev.chg, ev.hit_pos, ev.hit_err, ev.rl_grid, ev.xi_grid)
+    reflib.set_threads(4)
+    b = reflib.fit(ev.par, ev.err, ev.chg, ev.hit_pos, ev.hit_err, ev.rl_grid, ev.xi_grid)
+    reflib.set_threads(1)
+    for x, y in zip(a[:3], b[:3]):
+        np.testing.assert_array_equal(x, y)
