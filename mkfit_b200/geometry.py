@@ -1,0 +1,64 @@
+"""Detector description and finding configuration (CMS-2017).
+
+The numbers come from the reference's own geometry plugin, exported once
+into geom/cms2017.npz by geom/make_cms2017.py (layer table, per-region
+layer plans, search-window parameters, iteration parameters, propagation
+flags and the (z, r) material grid).
+"""
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+# Column meaning of Geometry.layer_desc (one row per layer).
+LAYER_FIELDS = ["is_barrel", "rin", "rout", "zmin", "zmax", "propagate_to", "q_bin",
+                "has_hole", "hole_min", "hole_max", "is_pix", "is_stereo",
+                "min_dphi", "max_dphi", "min_dq", "max_dq",
+                "c_dp_sf", "c_dp_0", "c_dp_1", "c_dp_2",
+                "c_dq_sf", "c_dq_0", "c_dq_1", "c_dq_2",
+                "c_c2_sf", "c_c2_0", "c_c2_1", "c_c2_2",
+                "layer_type", "is_seed", "subdet", "pad"]
+
+# Region indices (TrackerInfo::EtaRegion).
+REG_ENDCAP_NEG, REG_TRANSITION_NEG, REG_BARREL, REG_TRANSITION_POS, REG_ENDCAP_POS = range(5)
+
+
+class Geometry:
+    def __init__(self, path=None):
+        d = np.load(path or os.path.join(HERE, "geom", "cms2017.npz"))
+        self.arrays = {k: d[k] for k in d.files}
+        self.layer_desc = self.arrays["layer_desc"].astype(np.float32)
+        self.n_layers = self.layer_desc.shape[0]
+        self.plans = self.arrays["plans"]
+        self.plan_len = self.arrays["plan_len"]
+        self.pickup = self.arrays["pickup"]
+        self.region_order = self.arrays["region_order"]
+        self.iter_params = self.arrays["iter_params"]
+        self.flags = self.arrays["flags"]
+        self.eta = self.arrays["eta"]
+        self.rl = self.arrays["rl"]
+        self.xi = self.arrays["xi"]
+
+    def field(self, name):
+        return self.layer_desc[:, LAYER_FIELDS.index(name)]
+
+    def layer(self, i):
+        return {k: float(self.layer_desc[i, j]) for j, k in enumerate(LAYER_FIELDS)}
+
+    @property
+    def n_regions(self):
+        return self.plans.shape[0]
+
+    def plan(self, region):
+        return [int(x) for x in self.plans[region, :self.plan_len[region]]]
+
+
+_default = None
+
+
+def cms2017():
+    global _default
+    if _default is None:
+        _default = Geometry()
+    return _default

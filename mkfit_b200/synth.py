@@ -198,3 +198,334 @@ def gen_fit_event(n_tracks=20000, seed=0xC0FFEE, radii=None, pt_range=(0.5, 10.0
         hit_pos=np.ascontiguousarray(hpos, dtype=np.float32),
         hit_err=np.ascontiguousarray(herr, dtype=np.float32),
         radii=radii, rl_grid=rl, xi_grid=xi, seed=seed)
+
+
+# =============================================================================
+# CMS-2017 finding events
+# =============================================================================
+
+class CmsEvent:
+    """Finding workload on the CMS-2017 geometry. Hits of all layers in one
+    SoA buffer (layer l at [layer_begin[l], layer_begin[l+1])); seeds with up
+    to 4 hits given as (layer, index within layer)."""
+
+    def __init__(self, **kw):
+        self.__dict__.update(kw)
+
+    @property
+    def n_seeds(self):
+        return self.seed_chg.shape[0]
+
+    @property
+    def n_hits(self):
+        return int(self.layer_begin[-1])
+
+
+def _next_crossing(st, rs, is_barrel, zmin, zmax, rin, rout, hole, hmin, hmax, ptarget, done_mask):
+    """For every live track, the smallest positive arc length to a layer
+    surface it has not crossed yet and that is inside the layer's active
+    extent. Barrel surfaces are cylinders r = propagate_to (outgoing side
+    only), endcap surfaces planes z = propagate_to. Returns (s, layer) with
+    s = inf where nothing is left before the apex."""
+    n = st["x"].shape[0]
+    L = is_barrel.shape[0]
+    kap = st["kappa"][:, None]
+    xc = st["x"] - np.sin(st["phi"]) / st["kappa"]
+    yc = st["y"] + np.cos(st["phi"]) / st["kappa"]
+    rho = 1.0 / np.abs(st["kappa"])
+    d = np.hypot(xc, yc)
+    alpha = np.arctan2(yc, xc)
+    # psi: angle of the track point seen from the circle centre; dpsi/ds = kappa.
+    psi0 = np.arctan2(st["y"] - yc, st["x"] - xc)
+    period = 2 * np.pi * rho
+    s_apex = np.mod((alpha - psi0) / st["kappa"], period)
+    s = np.full((n, L), np.inf)
+    # Barrel cylinders.
+    rb = ptarget[None, :]
+    c = (rb ** 2 - d[:, None] ** 2 - rho[:, None] ** 2) / (2 * d[:, None] * rho[:, None])
+    ok = np.abs(c) <= 1.0
+    ac = np.arccos(np.clip(c, -1, 1))
+    for sgn in (1.0, -1.0):
+        psi = alpha[:, None] + sgn * ac
+        ss = np.mod((psi - psi0[:, None]) / kap, period[:, None])
+        good = ok & is_barrel[None, :] & (ss > 1e-6) & (ss <= s_apex[:, None])
+        s = np.where(good & (ss < s), ss, s)
+    zc = st["z"][:, None] + s / np.tan(st["theta"])[:, None]
+    s = np.where(is_barrel[None, :] & ((zc < zmin[None, :]) | (zc > zmax[None, :])), np.inf, s)
+    # Endcap planes.
+    se = (ptarget[None, :] - st["z"][:, None]) * np.tan(st["theta"])[:, None]
+    good = (~is_barrel[None, :]) & (se > 1e-6) & (se <= s_apex[:, None])
+    ph = st["phi"][:, None] + kap * se
+    xe = st["x"][:, None] + (np.sin(ph) - np.sin(st["phi"])[:, None]) / kap
+    ye = st["y"][:, None] - (np.cos(ph) - np.cos(st["phi"])[:, None]) / kap
+    re = np.hypot(xe, ye)
+    inside = (re > rin[None, :]) & (re < rout[None, :]) & ~(hole[None, :] & (re > hmin[None, :]) & (re < hmax[None, :]))
+    s = np.where(good & inside, se, s)
+    s = np.where(done_mask, np.inf, s)
+    lay = np.argmin(s, axis=1)
+    return s[np.arange(n), lay], lay
+
+
+def gen_cms_event(n_tracks=800, seed=0xC0FFEE, geom=None, pt_range=(0.5, 50.0), eta_max=2.4,
+                  noise_frac=0.01, noise_scale=None, vtx_sigma_xy=0.01, vtx_sigma_z=5.0,
+                  r_start=1.0, overlap_prob=0.05, strip_len=10.0):
+    """Synthetic CMS-2017 event: helices with pT log-uniform in pt_range,
+    |eta| < eta_max, transported through the layer table with a Highland
+    multiple-scattering kick from the reference material grid at each
+    crossing; one hit per crossed layer (pixel: 0.003 cm in both measured
+    directions; strip: 0.01 cm in r-phi, uniform along a strip of
+    `strip_len` cm on the long axis) plus, with probability `overlap_prob`
+    on strip layers, a second hit in the neighbouring module; noise hits at
+    `noise_frac` of each layer's signal-hit count (times `noise_scale[l]`
+    when given) uniform in the layer's extent. Seeds: the first three pixel
+    hits of every track that has them, with the true state at the third hit
+    and a fixed diagonal covariance."""
+    from .geometry import cms2017
+    g = geom or cms2017()
+    rng = np.random.default_rng(seed)
+    n = n_tracks
+    L = g.n_layers
+    is_barrel = g.field("is_barrel") > 0.5
+    zmin, zmax = g.field("zmin").astype(np.float64), g.field("zmax").astype(np.float64)
+    rin, rout = g.field("rin").astype(np.float64), g.field("rout").astype(np.float64)
+    hole = g.field("has_hole") > 0.5
+    hmin, hmax = g.field("hole_min").astype(np.float64), g.field("hole_max").astype(np.float64)
+    is_pix = g.field("is_pix") > 0.5
+    is_stereo = g.field("is_stereo") > 0.5
+    # Generation surfaces: the layer's nominal surface; stereo layers (which
+    # share it with their mono partner) are placed 0.5 cm further out.
+    ptarget = g.field("propagate_to").astype(np.float64)
+    ptarget = ptarget + np.where(is_stereo, 0.5 * np.sign(np.where(is_barrel, 1.0, ptarget)), 0.0)
+
+    pt = np.exp(rng.uniform(np.log(pt_range[0]), np.log(pt_range[1]), n))
+    eta = rng.uniform(-eta_max, eta_max, n)
+    phi = rng.uniform(-math.pi, math.pi, n)
+    q = np.where(rng.random(n) < 0.5, -1, 1).astype(np.int32)
+    vx = rng.normal(0, vtx_sigma_xy, n)
+    vy = rng.normal(0, vtx_sigma_xy, n)
+    vz = rng.normal(0, vtx_sigma_z, n)
+    theta = 2.0 * np.arctan(np.exp(-eta))
+    hel = Helix(vx, vy, vz, pt, phi, theta, q)
+    s0 = hel.s_at_radius(np.full(n, r_start))
+    x, y, z, ph = hel.at(s0)
+    st = dict(x=x, y=y, z=z, phi=ph, theta=theta.copy(), pt=pt.copy(),
+              kappa=-q / curvature_radius(pt))
+    done = np.zeros((n, L), dtype=bool)
+    alive = np.ones(n, dtype=bool)
+    hits = []  # (track, layer, x, y, z, phi_dir, theta_dir, pt)
+    mpi = 0.140
+    for _ in range(4 * L):
+        idx = np.nonzero(alive)[0]
+        if idx.size == 0:
+            break
+        sub = {k: v[idx] for k, v in st.items()}
+        s, lay = _next_crossing(sub, None, is_barrel, zmin, zmax, rin, rout, hole, hmin, hmax,
+                                ptarget, done[idx])
+        fin = np.isfinite(s)
+        alive[idx[~fin]] = False
+        idx, s, lay = idx[fin], s[fin], lay[fin]
+        if idx.size == 0:
+            break
+        kap = st["kappa"][idx]
+        ph1 = st["phi"][idx] + kap * s
+        x1 = st["x"][idx] + (np.sin(ph1) - np.sin(st["phi"][idx])) / kap
+        y1 = st["y"][idx] - (np.cos(ph1) - np.cos(st["phi"][idx])) / kap
+        z1 = st["z"][idx] + s / np.tan(st["theta"][idx])
+        done[idx, lay] = True
+        hits.append(np.stack([idx, lay, x1, y1, z1, ph1, st["theta"][idx], st["pt"][idx]], axis=1))
+        # Multiple scattering from the material grid at the crossing.
+        r1 = np.hypot(x1, y1)
+        zb = np.minimum((np.abs(z1) * 300 / 300.0).astype(np.int64), 299)
+        rbn = np.minimum((r1 * 120 / 120.0).astype(np.int64), 119)
+        radl = g.rl[zb, rbn].astype(np.float64)
+        th = st["theta"][idx]
+        p = st["pt"][idx] / np.sin(th)
+        beta = p / np.sqrt(p * p + mpi * mpi)
+        geo = np.where(is_barrel[lay], 1.0 / np.sin(th), 1.0 / np.abs(np.cos(th)))
+        xx0 = np.maximum(radl * geo, 1e-9)
+        t0 = np.where(radl > 0, highland(p, beta, xx0), 0.0)
+        st["theta"][idx] = th + rng.normal(0, 1, idx.size) * t0
+        st["phi"][idx] = ph1 + rng.normal(0, 1, idx.size) * t0 / np.sin(th)
+        st["x"][idx], st["y"][idx], st["z"][idx] = x1, y1, z1
+        # Stop tracks leaving the tracker volume.
+        out = (np.abs(z1) > 290) | (r1 > 115)
+        alive[idx[out]] = False
+
+    H = np.concatenate(hits, axis=0) if hits else np.zeros((0, 8))
+    trk = H[:, 0].astype(np.int64)
+    lay = H[:, 1].astype(np.int64)
+    # Order hits of each track along the trajectory (generation order).
+    order = np.arange(H.shape[0])
+
+    def smear(Hs, lay_s):
+        m = Hs.shape[0]
+        x0, y0, z0 = Hs[:, 2], Hs[:, 3], Hs[:, 4]
+        pphi = np.arctan2(y0, x0)
+        pix = is_pix[lay_s]
+        brl = is_barrel[lay_s]
+        stereo = is_stereo[lay_s]
+        sig_t = np.where(pix, 0.003, 0.01)
+        dt = rng.normal(0, 1, m) * sig_t
+        # long axis: pixel Gaussian 0.003; strip uniform along the strip
+        # (stereo strips: 0.1 cm Gaussian, a matched 2-D measurement).
+        long_sig = np.where(pix, 0.003, np.where(stereo, 0.1, strip_len / math.sqrt(12.0)))
+        dl = np.where(pix | stereo, rng.normal(0, 1, m) * long_sig,
+                      rng.uniform(-0.5, 0.5, m) * strip_len)
+        tx, ty = -np.sin(pphi), np.cos(pphi)
+        hx = x0 + tx * dt
+        hy = y0 + ty * dt
+        hz = z0.copy()
+        # barrel: long axis = z; endcap: long axis = radial.
+        hz = np.where(brl, hz + dl, hz)
+        hx = np.where(brl, hx, hx + np.cos(pphi) * dl)
+        hy = np.where(brl, hy, hy + np.sin(pphi) * dl)
+        e = np.zeros((6, m))
+        st2 = sig_t ** 2
+        ll2 = long_sig ** 2
+        sp, cp = np.sin(pphi), np.cos(pphi)
+        # barrel: transverse (r-phi) in xy, long in z.
+        bxx, bxy, byy, bzz = st2 * sp * sp, -st2 * sp * cp, st2 * cp * cp, ll2
+        # endcap: xy = R diag(radial=ll2, tangential=st2) R^T, zz tiny.
+        exx = ll2 * cp * cp + st2 * sp * sp
+        exy = (ll2 - st2) * sp * cp
+        eyy = ll2 * sp * sp + st2 * cp * cp
+        e[0] = np.where(brl, bxx, exx)
+        e[1] = np.where(brl, bxy, exy)
+        e[2] = np.where(brl, byy, eyy)
+        e[5] = np.where(brl, bzz, 1e-6)
+        return np.stack([hx, hy, hz]), e
+
+    pos, err = smear(H, lay)
+    # Module ids (12 bits): barrel 64 phi x 32 z segments, endcap 64 phi x 32 r rings.
+    def module_id(px, py, pz, lay_s):
+        pphi = np.arctan2(py, px)
+        iphi = np.clip(((pphi + math.pi) / (2 * math.pi) * 64).astype(np.int64), 0, 63)
+        brl = is_barrel[lay_s]
+        fz = (pz - zmin[lay_s]) / np.maximum(zmax[lay_s] - zmin[lay_s], 1e-6)
+        fr = (np.hypot(px, py) - rin[lay_s]) / np.maximum(rout[lay_s] - rin[lay_s], 1e-6)
+        iq = np.clip((np.where(brl, fz, fr) * 32).astype(np.int64), 0, 31)
+        return (iphi * 32 + iq).astype(np.int32)
+
+    detid = module_id(H[:, 2], H[:, 3], H[:, 4], lay)
+    mc = trk.astype(np.int32)
+
+    # Overlap hits on strip layers: a second measurement in the neighbouring
+    # module, 0.3 cm further out along the track.
+    ov = (~is_pix[lay]) & (rng.random(H.shape[0]) < overlap_prob)
+    if ov.any():
+        Ho = H[ov].copy()
+        kap = -np.sign(np.zeros(ov.sum()) + 1)  # placeholder, replaced below
+        qtrk = q[trk[ov]].astype(np.float64)
+        kap = -qtrk / curvature_radius(Ho[:, 7])
+        ds = 0.3
+        ph2 = Ho[:, 5] + kap * ds
+        Ho[:, 2] = Ho[:, 2] + (np.sin(ph2) - np.sin(Ho[:, 5])) / kap
+        Ho[:, 3] = Ho[:, 3] - (np.cos(ph2) - np.cos(Ho[:, 5])) / kap
+        Ho[:, 4] = Ho[:, 4] + ds / np.tan(Ho[:, 6])
+        lay_o = lay[ov]
+        pos_o, err_o = smear(Ho, lay_o)
+        det_o = ((detid[ov] + 32) % 2048).astype(np.int32)
+        pos = np.concatenate([pos, pos_o], axis=1)
+        err = np.concatenate([err, err_o], axis=1)
+        lay = np.concatenate([lay, lay_o])
+        detid = np.concatenate([detid, det_o])
+        mc = np.concatenate([mc, trk[ov].astype(np.int32)])
+        trk = np.concatenate([trk, trk[ov]])
+        order = np.concatenate([order, np.full(ov.sum(), 1 << 40)])
+
+    # Noise hits.
+    n_sig = np.bincount(lay, minlength=L)
+    scale = np.ones(L) if noise_scale is None else np.asarray(noise_scale, dtype=np.float64)
+    n_noise = rng.poisson(noise_frac * n_sig * scale)
+    nz_pos, nz_err, nz_lay, nz_det = [], [], [], []
+    for l in range(L):
+        k = int(n_noise[l])
+        if k == 0:
+            continue
+        pphi = rng.uniform(-math.pi, math.pi, k)
+        if is_barrel[l]:
+            r = np.full(k, ptarget[l])
+            zz = rng.uniform(zmin[l], zmax[l], k)
+        else:
+            r = rng.uniform(rin[l], rout[l], k)
+            if hole[l]:
+                r = np.where((r > hmin[l]) & (r < hmax[l]), rin[l] + 0.5 * (hmin[l] - rin[l]), r)
+            zz = np.full(k, ptarget[l])
+        Hn = np.zeros((k, 8))
+        Hn[:, 2], Hn[:, 3], Hn[:, 4] = r * np.cos(pphi), r * np.sin(pphi), zz
+        pn, en = smear(Hn, np.full(k, l))
+        nz_pos.append(pn)
+        nz_err.append(en)
+        nz_lay.append(np.full(k, l))
+        nz_det.append(module_id(Hn[:, 2], Hn[:, 3], Hn[:, 4], np.full(k, l)))
+    if nz_pos:
+        pos = np.concatenate([pos] + nz_pos, axis=1)
+        err = np.concatenate([err] + nz_err, axis=1)
+        lay = np.concatenate([lay] + nz_lay)
+        detid = np.concatenate([detid] + nz_det).astype(np.int32)
+        nn = sum(a.shape[0] for a in nz_lay)
+        mc = np.concatenate([mc, np.full(nn, -1, np.int32)])
+        trk = np.concatenate([trk, np.full(nn, -1)])
+        order = np.concatenate([order, np.full(nn, 1 << 41)])
+
+    m = lay.shape[0]
+    # Strip charge per cm: mostly saturated (always passes the charge cut),
+    # a fifth spread over [1700, 3600] so the cut is exercised.
+    cpcm = np.where(is_pix[lay], -1,
+                    np.where(rng.random(m) < 0.8, 4000, rng.integers(1700, 3600, m))).astype(np.int32)
+
+    # Group by layer, random order within a layer.
+    perm = np.lexsort((rng.random(m), lay))
+    lay_sorted = lay[perm]
+    layer_begin = np.zeros(L + 1, np.int32)
+    layer_begin[1:] = np.cumsum(np.bincount(lay_sorted, minlength=L))
+    inv = np.empty(m, np.int64)
+    inv[perm] = np.arange(m)
+    index_in_layer = inv - layer_begin[lay]
+
+    # Seeds: first three pixel hits (generation order) of each track.
+    sig_idx = np.nonzero((mc >= 0) & is_pix[lay] & (order < (1 << 40)))[0]
+    sig_idx = sig_idx[np.lexsort((order[sig_idx], trk[sig_idx]))]
+    seeds = []
+    t_prev, cnt = -1, 0
+    first3 = {}
+    for h in sig_idx:
+        t = int(trk[h])
+        if t != t_prev:
+            t_prev, cnt = t, 0
+        if cnt < 3:
+            first3.setdefault(t, []).append(h)
+        cnt += 1
+    seed_tracks = sorted(t for t, v in first3.items() if len(v) == 3)
+    ns = len(seed_tracks)
+    spar = np.zeros((6, ns))
+    serr = np.zeros((21, ns))
+    schg = np.zeros(ns, np.int32)
+    snh = np.full(ns, 3, np.int32)
+    shl = np.full((ns, 4), -1, np.int32)
+    shi = np.full((ns, 4), -1, np.int32)
+    for i, t in enumerate(seed_tracks):
+        hs = first3[t]
+        h3 = hs[2]
+        Hh = H[h3]  # true crossing of the third seed hit (signal hits precede overlaps)
+        spar[:, i] = [Hh[2], Hh[3], Hh[4], 1.0 / Hh[7], Hh[5], Hh[6]]
+        d = [0.01 ** 2, 0.01 ** 2, 0.01 ** 2, (0.05 / Hh[7]) ** 2, 0.005 ** 2, 0.005 ** 2]
+        for k, (a, b) in enumerate(SYM6):
+            if a == b:
+                serr[k, i] = d[a]
+        schg[i] = q[t]
+        for k, h in enumerate(hs):
+            shl[i, k] = lay[h]
+            shi[i, k] = index_in_layer[h]
+    return CmsEvent(
+        n_layers=L, layer_begin=layer_begin,
+        hit_pos=np.ascontiguousarray(pos[:, perm], np.float32),
+        hit_err=np.ascontiguousarray(err[:, perm], np.float32),
+        hit_detid=np.ascontiguousarray(detid[perm], np.int32),
+        hit_cpcm=np.ascontiguousarray(cpcm[perm], np.int32),
+        hit_mc=np.ascontiguousarray(mc[perm], np.int32),
+        seed_par=np.ascontiguousarray(spar, np.float32),
+        seed_err=np.ascontiguousarray(serr, np.float32),
+        seed_chg=schg, seed_nhits=snh, seed_hit_layer=shl, seed_hit_index=shi,
+        seed_mc=np.array(seed_tracks, np.int32), n_tracks=n, seed=seed,
+        n_signal_hits=int((mc >= 0).sum()))

@@ -130,3 +130,69 @@ class Restate:
                         ms.ctypes.data if ms is not None else None,
                         out_par, out_err, chi2.ctypes.data if chi2 is not None else None)
         return out_par, out_err, chi2
+
+
+def _load_find_api(lib):
+    c_int_p = ctypes.POINTER(ctypes.c_int)
+    lib.ref_cms2017_sizes.argtypes = [c_int_p, c_int_p, c_int_p]
+    lib.ref_cms2017_export.argtypes = [_f32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _f32p,
+                                       _i32p, _f32p, _f32p, _f32p]
+    lib.ref_find.restype = ctypes.c_int
+    lib.ref_find.argtypes = ([ctypes.c_int, _i32p, _f32p, _f32p, _i32p, _i32p, ctypes.c_int,
+                              _f32p, _f32p, _i32p, _i32p, _i32p, _i32p, ctypes.c_int,
+                              ctypes.c_float, ctypes.c_int, ctypes.c_int] +
+                             [_i32p, _i32p, _i32p, _f32p, _f32p, _i32p, _f32p, _f32p] +
+                             [_i32p] * 5 + [_i32p, _i32p, ctypes.POINTER(ctypes.c_double)])
+
+
+def cms2017_export(reflib):
+    """CMS-2017 geometry + iteration-0 configuration from the reference's
+    own plugin (Geoms/CMS-2017.cc), as numpy arrays."""
+    lib = reflib.lib
+    _load_find_api(lib)
+    nl, nr, mp = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    lib.ref_cms2017_sizes(ctypes.byref(nl), ctypes.byref(nr), ctypes.byref(mp))
+    nl, nr, mp = nl.value, nr.value, mp.value
+    out = dict(layer_desc=np.zeros((nl, 32), np.float32), plans=np.zeros((nr, mp), np.int32),
+               plan_len=np.zeros(nr, np.int32), pickup=np.zeros(nr, np.int32),
+               bkfit_last=np.zeros(nr, np.int32), bksearch_pickup=np.zeros(nr, np.int32),
+               region_order=np.zeros(nr, np.int32), iter_params=np.zeros(8, np.float32),
+               flags=np.zeros(4, np.int32), eta=np.zeros(3, np.float32),
+               rl=np.zeros((300, 120), np.float32), xi=np.zeros((300, 120), np.float32))
+    lib.ref_cms2017_export(out["layer_desc"], out["plans"], out["plan_len"], out["pickup"],
+                           out["bkfit_last"], out["bksearch_pickup"], out["region_order"],
+                           out["iter_params"], out["flags"], out["eta"], out["rl"], out["xi"])
+    return out
+
+
+def ref_find(reflib, ev, max_cands=6, chi2_cut=30.0, zero_c2=True, repeat=1):
+    """Reference clone-engine finding (find_tracks_load_seeds +
+    FindTracksCloneEngine) on a synth.CmsEvent. Returns a dict of per-seed
+    candidate arrays (see oracle/ref_driver.cc ref_find)."""
+    lib = reflib.lib
+    _load_find_api(lib)
+    ns = ev.n_seeds
+    m = max_cands
+    o = dict(n_cands=np.zeros(ns, np.int32), region=np.zeros(ns, np.int32),
+             sorted_pos=np.zeros(ns, np.int32), par=np.zeros((ns * m, 6), np.float32),
+             err=np.zeros((ns * m, 21), np.float32), chg=np.zeros(ns * m, np.int32),
+             chi2=np.zeros(ns * m, np.float32), score=np.zeros(ns * m, np.float32),
+             nfound=np.zeros(ns * m, np.int32), ntot=np.zeros(ns * m, np.int32),
+             noverlap=np.zeros(ns * m, np.int32), ninside=np.zeros(ns * m, np.int32),
+             ntail=np.zeros(ns * m, np.int32), hit_idx=np.zeros((ns * m, 64), np.int32),
+             hit_lyr=np.zeros((ns * m, 64), np.int32))
+    secs = ctypes.c_double(0)
+    c = lambda a, t: np.ascontiguousarray(a, t)
+    rc = lib.ref_find(ev.n_layers, c(ev.layer_begin, np.int32), c(ev.hit_pos, np.float32),
+                      c(ev.hit_err, np.float32), c(ev.hit_detid, np.int32),
+                      c(ev.hit_cpcm, np.int32), ns, c(ev.seed_par, np.float32),
+                      c(ev.seed_err, np.float32), c(ev.seed_chg, np.int32),
+                      c(ev.seed_nhits, np.int32), c(ev.seed_hit_layer, np.int32),
+                      c(ev.seed_hit_index, np.int32), m, float(chi2_cut), int(zero_c2),
+                      int(repeat), o["n_cands"], o["region"], o["sorted_pos"], o["par"], o["err"],
+                      o["chg"], o["chi2"], o["score"], o["nfound"], o["ntot"], o["noverlap"],
+                      o["ninside"], o["ntail"], o["hit_idx"], o["hit_lyr"], ctypes.byref(secs))
+    if rc != 0:
+        raise RuntimeError(f"ref_find failed rc={rc}")
+    o["seconds"] = secs.value
+    return o

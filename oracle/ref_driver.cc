@@ -160,3 +160,228 @@ int ref_fit(int n_tracks, int n_layers, const float* par, const float* err, cons
 }
 
 }  // extern "C"
+
+//==============================================================================
+// CMS-2017 geometry and clone-engine finding
+//==============================================================================
+
+namespace {
+
+// Exposes the builder's comb-candidate storage for export (the reference
+// keeps it protected; MkBuilder.h:92-100).
+struct RefBuilder : public MkBuilder {
+  EventOfCombCandidates& eocc() { return m_event_of_comb_cands; }
+};
+
+constexpr int kLayerDescLen = 32;
+
+void ensure_cms2017() {
+  if (g_cms2017_loaded) return;
+  Config::silent = true;
+  auto creator = (TrackerInfoCreator_foo)TrackerInfoCrator_ptr;
+  creator(Config::TrkInfo, Config::ItrInfo, false);
+  fillZRgridME();
+  g_cms2017_loaded = true;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Geometry export sizes: n_layers, n_regions, max plan length.
+int ref_cms2017_sizes(int* n_layers, int* n_regions, int* max_plan) {
+  ensure_cms2017();
+  const IterationConfig& ic = Config::ItrInfo[0];
+  *n_layers = (int)Config::TrkInfo.m_layers.size();
+  *n_regions = ic.m_n_regions;
+  int mp = 0;
+  for (auto& sp : ic.m_steering_params) mp = std::max(mp, (int)sp.m_layer_plan.size());
+  *max_plan = mp;
+  return 0;
+}
+
+// Exports the CMS-2017 detector description and iteration-0 configuration
+// (Geoms/CMS-2017.cc:717-790 and the generated CMS-2017.acc tables).
+//   layer_desc[n_layers][32]: see mkfit_b200/geometry.py LAYER_FIELDS
+//   plans[n_regions][max_plan] (-1 padded), plan_len/pickup/bkfit_last/
+//   bksearch_pickup[n_regions], region_order[n_regions]
+//   iter_params[8]: maxCands, maxHoles, maxConsecHoles, chi2Cut_min,
+//                   chi2CutOverlap, pTCutOverlap, nlayers_per_seed, -
+//   flags[4]: requires_prop_to_hit, inter pflags, intra pflags, bkfit pflags
+//   eta[3]: transition begin/end, endcap end
+//   rl/xi[300*120]: material grid after fillZRgridME()
+int ref_cms2017_export(float* layer_desc, int* plans, int* plan_len, int* pickup,
+                       int* bkfit_last, int* bksearch_pickup, int* region_order,
+                       float* iter_params, int* flags, float* eta, float* rl, float* xi) {
+  ensure_cms2017();
+  const TrackerInfo& ti = Config::TrkInfo;
+  const IterationConfig& ic = Config::ItrInfo[0];
+  int n_layers, n_regions, max_plan;
+  ref_cms2017_sizes(&n_layers, &n_regions, &max_plan);
+  for (int l = 0; l < n_layers; ++l) {
+    const LayerInfo& L = ti.m_layers[l];
+    const IterationLayerConfig& C = ic.m_layer_configs[l];
+    float* d = layer_desc + l * kLayerDescLen;
+    std::fill(d, d + kLayerDescLen, 0.f);
+    d[0] = L.is_barrel();
+    d[1] = L.m_rin;
+    d[2] = L.m_rout;
+    d[3] = L.m_zmin;
+    d[4] = L.m_zmax;
+    d[5] = L.m_propagate_to;
+    d[6] = L.m_q_bin;
+    d[7] = L.m_has_r_range_hole;
+    d[8] = L.m_has_r_range_hole ? L.m_hole_r_min : 0.f;
+    d[9] = L.m_has_r_range_hole ? L.m_hole_r_max : 0.f;
+    d[10] = L.is_pix_lyr();
+    d[11] = L.is_stereo_lyr();
+    d[12] = C.m_select_min_dphi;
+    d[13] = C.m_select_max_dphi;
+    d[14] = C.m_select_min_dq;
+    d[15] = C.m_select_max_dq;
+    d[16] = C.c_dp_sf; d[17] = C.c_dp_0; d[18] = C.c_dp_1; d[19] = C.c_dp_2;
+    d[20] = C.c_dq_sf; d[21] = C.c_dq_0; d[22] = C.c_dq_1; d[23] = C.c_dq_2;
+    d[24] = C.c_c2_sf; d[25] = C.c_c2_0; d[26] = C.c_c2_1; d[27] = C.c_c2_2;
+    d[28] = (float)L.m_layer_type;
+    d[29] = L.is_seed_lyr();
+    d[30] = L.is_tib_lyr() || L.is_tob_lyr() ? 1.f : (L.is_tid_lyr() || L.is_tec_lyr() ? 2.f : 0.f);
+  }
+  for (int r = 0; r < n_regions; ++r) {
+    const SteeringParams& sp = ic.m_steering_params[r];
+    plan_len[r] = (int)sp.m_layer_plan.size();
+    pickup[r] = sp.m_fwd_search_pickup;
+    bkfit_last[r] = sp.m_bkw_fit_last;
+    bksearch_pickup[r] = sp.m_bkw_search_pickup;
+    for (int i = 0; i < max_plan; ++i)
+      plans[r * max_plan + i] = i < plan_len[r] ? sp.m_layer_plan[i].m_layer : -1;
+    region_order[r] = ic.m_region_order[r];
+  }
+  const IterationParams& ip = ic.m_params;
+  iter_params[0] = ip.maxCandsPerSeed;
+  iter_params[1] = ip.maxHolesPerCand;
+  iter_params[2] = ip.maxConsecHoles;
+  iter_params[3] = ip.chi2Cut_min;
+  iter_params[4] = ip.chi2CutOverlap;
+  iter_params[5] = ip.pTCutOverlap;
+  iter_params[6] = ip.nlayers_per_seed;
+  iter_params[7] = 0;
+  flags[0] = Config::finding_requires_propagation_to_hit_pos;
+  flags[1] = Config::finding_inter_layer_pflags._raw_ & 3;
+  flags[2] = Config::finding_intra_layer_pflags._raw_ & 3;
+  flags[3] = Config::backward_fit_pflags._raw_ & 3;
+  eta[0] = ti.m_eta_trans_beg;
+  eta[1] = ti.m_eta_trans_end;
+  eta[2] = ti.m_eta_ecap_end;
+  std::memcpy(rl, Config::RlgridME, sizeof(Config::RlgridME));
+  std::memcpy(xi, Config::XigridME, sizeof(Config::XigridME));
+  return 0;
+}
+
+// Clone-engine combinatorial finding on one event, CMS-2017 geometry,
+// iteration 0 with overrides (BASELINE config: max cands per seed, flat
+// chi2 cut: the dynamic c2 parameters are zeroed when zero_c2 != 0).
+//
+// Hits: layer l occupies [layer_begin[l], layer_begin[l+1]) of pos[3][nh],
+//   err[6][nh]; detid[nh] (12-bit module id), cpcm[nh] (< 0: pixel hit,
+//   otherwise the strip charge per cm given to Hit::setupAsStrip).
+// Seeds: par[6][ns], err[21][ns], chg[ns]; seed_nhits[ns] (<= 4) hits given
+//   as seed_hit_layer[ns][4], seed_hit_index[ns][4] (index within layer).
+// Outputs, indexed by input seed (label), m = max_cands:
+//   n_cands[ns], region[ns], sorted_pos[ns] (position after the seed sort),
+//   c_par[ns*m][6], c_err[ns*m][21], c_chg, c_chi2, c_score, c_nfound,
+//   c_ntot, c_noverlap, c_ninside, c_ntail [ns*m],
+//   c_hit_idx / c_hit_lyr [ns*m][64].
+int ref_find(int n_layers_in, const int* layer_begin, const float* hpos, const float* herr,
+             const int* detid, const int* cpcm, int ns, const float* spar, const float* serr,
+             const int* schg, const int* seed_nhits, const int* seed_hit_layer,
+             const int* seed_hit_index, int max_cands, float chi2_cut, int zero_c2, int repeat,
+             int* n_cands, int* region, int* sorted_pos, float* c_par, float* c_err, int* c_chg,
+             float* c_chi2, float* c_score, int* c_nfound, int* c_ntot, int* c_noverlap,
+             int* c_ninside, int* c_ntail, int* c_hit_idx, int* c_hit_lyr, double* best_seconds) {
+  ensure_cms2017();
+  fillZRgridME();  // the fit entry may have replaced the material grid
+  const int n_layers = (int)Config::TrkInfo.m_layers.size();
+  if (n_layers_in != n_layers) return -1;
+
+  IterationConfig itconf = Config::ItrInfo[0];
+  itconf.m_params.maxCandsPerSeed = max_cands;
+  itconf.m_backward_params.maxCandsPerSeed = max_cands;
+  itconf.m_params.chi2Cut_min = chi2_cut;
+  itconf.m_backward_params.chi2Cut_min = chi2_cut;
+  if (zero_c2)
+    for (auto& lc : itconf.m_layer_configs) lc.c_c2_0 = lc.c_c2_1 = lc.c_c2_2 = 0.f;
+
+  const int nh_tot = layer_begin[n_layers];
+  std::vector<HitVec> layer_hits(n_layers);
+  for (int l = 0; l < n_layers; ++l) {
+    for (int h = layer_begin[l]; h < layer_begin[l + 1]; ++h) {
+      Hit hit = make_hit(h, nh_tot, hpos, herr);
+      if (cpcm[h] < 0)
+        hit.setupAsPixel(detid[h], 1, 1);
+      else
+        hit.setupAsStrip(detid[h], cpcm[h], 1);
+      layer_hits[l].push_back(hit);
+    }
+  }
+  EventOfHits eoh(Config::TrkInfo);
+  for (int l = 0; l < n_layers; ++l) eoh.SuckInHits(l, layer_hits[l]);
+
+  TrackVec seeds;
+  seeds.reserve(ns);
+  for (int s = 0; s < ns; ++s) {
+    Track t = make_track(s, ns, spar, serr, schg);
+    t.setLabel(s);
+    for (int k = 0; k < seed_nhits[s]; ++k)
+      t.addHitIdx(seed_hit_index[s * 4 + k], seed_hit_layer[s * 4 + k], 0.f);
+    seeds.push_back(t);
+  }
+
+  MkJob job({Config::TrkInfo, itconf, eoh, nullptr});
+  double best = 1e30;
+  RefBuilder builder;
+  for (int r = 0; r < std::max(1, repeat); ++r) {
+    builder.begin_event(&job, nullptr, "ref_find");
+    builder.find_tracks_load_seeds(seeds);
+    const double t0 = now_s();
+    builder.FindTracksCloneEngine();
+    best = std::min(best, now_s() - t0);
+    if (r + 1 < std::max(1, repeat)) builder.end_event();
+  }
+  if (best_seconds) *best_seconds = best;
+
+  EventOfCombCandidates& eocc = builder.eocc();
+  std::fill(n_cands, n_cands + ns, 0);
+  for (int i = 0; i < eocc.m_size; ++i) {
+    CombCandidate& cc = eocc[i];
+    if (cc.empty()) continue;
+    const int s = cc.front().label();
+    if (s < 0 || s >= ns) return -2;
+    sorted_pos[s] = i;
+    region[s] = cc.front().getEtaRegion();
+    n_cands[s] = std::min((int)cc.size(), max_cands);
+    for (int c = 0; c < n_cands[s]; ++c) {
+      const TrackCand& tc = cc[c];
+      const int slot = s * max_cands + c;
+      for (int k = 0; k < 6; ++k) c_par[slot * 6 + k] = tc.parameters()[k];
+      for (int k = 0; k < 21; ++k) c_err[slot * 21 + k] = tc.errors().Array()[k];
+      c_chg[slot] = tc.charge();
+      c_chi2[slot] = tc.chi2();
+      c_score[slot] = tc.score();
+      c_nfound[slot] = tc.nFoundHits();
+      c_ntot[slot] = tc.nTotalHits();
+      c_noverlap[slot] = tc.nOverlapHits();
+      c_ninside[slot] = tc.nInsideMinusOneHits();
+      c_ntail[slot] = tc.nTailMinusOneHits();
+      Track t = tc.exportTrack(false);
+      const int nh = std::min(t.nTotalHits(), Config::nMaxTrkHits);
+      for (int k = 0; k < Config::nMaxTrkHits; ++k) {
+        c_hit_idx[slot * Config::nMaxTrkHits + k] = k < nh ? t.getHitIdx(k) : -100;
+        c_hit_lyr[slot * Config::nMaxTrkHits + k] = k < nh ? t.getHitLyr(k) : -100;
+      }
+    }
+  }
+  builder.end_event();
+  return 0;
+}
+
+}  // extern "C"

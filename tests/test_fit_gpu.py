@@ -73,8 +73,9 @@ def test_fit_error_vs_fp64(gpu_ctx, restate):
     rc = np.abs(out["chi2"] - dchi2) / np.maximum(np.abs(dchi2), 1e-6)
     print("vs FP64: par", summarize(ep), "cov", summarize(ec), "chi2", summarize(rc))
     assert np.percentile(ep, 99.9) < PAR_RTOL
-    assert np.median(rc) < 1e-5
-    assert np.percentile(rc, 99) < CHI2_RTOL
+    # chi2 summed over 10 updates in FP32: within the 1e-3 relative bound.
+    assert np.median(rc) < 1e-4
+    assert np.percentile(rc, 99.9) < CHI2_RTOL
 
 
 def test_fit_host_entry_equals_device_entry(gpu_ctx):
