@@ -121,6 +121,105 @@ int mkfg_fit(mkfg_context* ctx, const mkfg_fit_args* args);
  * args (including hits.layer_begin) are host pointers here. */
 int mkfg_fit_host(mkfg_context* ctx, const mkfg_fit_args* args);
 
+
+/* ------------------------------------------------------------- finding */
+/* Detector geometry + finding iteration configuration. Replaces the
+ * reference's TrackerInfo / IterationConfig as consumed by MkBuilder
+ * (TrackerInfo.h:35-147, mkFit/IterationConfig.h:44-124,
+ * mkFit/SteeringParams.h:36-163). Host pointers; copied by the call.
+ *
+ * layer_desc: n_layers rows of 32 floats:
+ *   0 is_barrel, 1 rin, 2 rout, 3 zmin, 4 zmax, 5 propagate_to, 6 q_bin
+ *   (> 0 bin width, < 0 number of bins), 7 has_r_hole, 8 hole_rmin,
+ *   9 hole_rmax, 10 is_pixel, 11 is_stereo, 12-15 min/max dphi, min/max dq,
+ *   16-19 c_dp_{sf,0,1,2}, 20-23 c_dq_{sf,0,1,2}, 24-27 c_c2_{sf,0,1,2},
+ *   28 layer type, 29 is_seed, 30-31 unused.
+ * plans: n_regions rows of max_plan layer ids (-1 padded); the forward
+ * search starts after plan position pickup[r]. */
+typedef struct {
+  int32_t n_layers;
+  const float* layer_desc;
+  int32_t n_regions;
+  int32_t max_plan;
+  const int32_t* plans;
+  const int32_t* plan_len;
+  const int32_t* pickup;
+  int32_t max_cands_per_seed; /* <= 8 */
+  int32_t max_holes_per_cand;
+  int32_t max_consec_holes;
+  float chi2_cut_min;
+  float chi2_cut_overlap;
+  float pt_cut_overlap;
+  uint32_t inter_layer_pflags; /* Config::finding_inter_layer_pflags */
+  uint32_t intra_layer_pflags; /* Config::finding_intra_layer_pflags */
+  int32_t requires_prop_to_hit; /* Config::finding_requires_propagation_to_hit_pos; must be 1 */
+} mkfg_find_config;
+
+int mkfg_finder_setup(mkfg_context* ctx, const mkfg_find_config* cfg);
+
+/* One event: hits (layer l at [layer_begin[l], layer_begin[l+1])) and seeds.
+ * Host pointers. cpcm: strip charge per cm as given to Hit::setupAsStrip,
+ * negative for pixel hits (Hit.h:285-300); detid: 12-bit module id in the
+ * layer. Seed hits: [n_seeds][4] (layer, index within layer), seed_nhits
+ * of them valid. */
+typedef struct {
+  int32_t n_layers;
+  const int32_t* layer_begin;
+  const float* pos; /* [3][n_hits] */
+  const float* err; /* [6][n_hits] */
+  const int32_t* detid;
+  const int32_t* cpcm;
+  int32_t n_seeds;
+  const float* seed_par; /* [6][n_seeds] */
+  const float* seed_err; /* [21][n_seeds] */
+  const int32_t* seed_chg;
+  const int32_t* seed_nhits;
+  const int32_t* seed_hit_layer;
+  const int32_t* seed_hit_index;
+} mkfg_event;
+
+/* Finding output, indexed by input seed; m = max_cands_per_seed slots per
+ * seed, best first (after MergeCandsAndBestShortOne). Host pointers; any
+ * may be NULL to skip. Hit lists: [n_seeds*m][64] (index, layer), unused
+ * entries -100. */
+typedef struct {
+  int32_t* n_cands;
+  int32_t* region;
+  float* par;  /* [n_seeds*m][6] */
+  float* err;  /* [n_seeds*m][21] */
+  int32_t* chg;
+  float* chi2;
+  float* score;
+  int32_t* nfound;
+  int32_t* ntot;
+  int32_t* noverlap;
+  int32_t* ninside;
+  int32_t* ntail;
+  int32_t* hit_idx;
+  int32_t* hit_lyr;
+} mkfg_find_out;
+
+/* Plain form, the drop-in for MkBuilder::find_tracks_load_seeds +
+ * FindTracksCloneEngine (mkFit/MkBuilder.cc:1491-1501, 1847-2058) on one
+ * event: upload (host hit-index build as LayerOfHits::SuckInHits and seed
+ * partition as import_seeds), run (one launch sequence per layer step),
+ * download (export of all candidates, as TrackCand::exportTrack). */
+int mkfg_find_upload(mkfg_context* ctx, const mkfg_event* ev);
+int mkfg_find_run(mkfg_context* ctx);
+int mkfg_find_download(mkfg_context* ctx, int32_t n_seeds, mkfg_find_out* out);
+int mkfg_find_event(mkfg_context* ctx, const mkfg_event* ev, mkfg_find_out* out);
+
+/* Host-only (no device needed): the hit-index build and seed ordering that
+ * mkfg_find_upload performs, for inspection and tests. bins: all layers'
+ * (q bin x 256 phi bin) entries (first | last << 16), layer after layer;
+ * *n_bins receives the count (pass bins = NULL to query it). srank[n_hits]:
+ * per sorted position (layer by layer) the hit's index within its layer
+ * (LayerOfHits::GetOriginalHitIndex). seed_order[n_seeds]: input seed at
+ * each sorted position; seed_region[n_seeds]: eta region per input seed. */
+int mkfg_prepare_event_host(const mkfg_find_config* cfg, const mkfg_event* ev, uint32_t* bins,
+                            int32_t* n_bins, int32_t* srank, int32_t* seed_order,
+                            int32_t* seed_region);
+
 #ifdef __cplusplus
 }
 #endif

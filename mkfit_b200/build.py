@@ -38,6 +38,14 @@ def build(verbose=False, extra_flags=()):
     headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) + \
         glob.glob(os.path.join(HERE, "..", "include", "*.h"))
     objs = []
+    for src in sorted(glob.glob(os.path.join(CSRC, "*.cc"))):
+        obj = os.path.join(OBJ_DIR, os.path.basename(src)[:-3] + "_host.o")
+        objs.append(obj)
+        if _newer(obj, [src] + headers):
+            cmd = [os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-fPIC", "-c", src, "-o", obj]
+            if verbose:
+                print(" ".join(cmd))
+            subprocess.check_call(cmd)
     for src in sorted(glob.glob(os.path.join(CSRC, "*.cu"))):
         obj = os.path.join(OBJ_DIR, os.path.basename(src)[:-3] + ".o")
         objs.append(obj)

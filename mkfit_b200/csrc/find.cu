@@ -1,6 +1,1195 @@
-// Combinatorial track finding (clone engine) -- device side and C ABI.
+// Clone-engine combinatorial track finding: device kernels and C ABI.
+//
+// Plain form (the drop-in for MkBuilder::FindTracksCloneEngine,
+// mkFit/MkBuilder.cc:1847-2058): for every layer-plan step, four launches
+//   1. prep   : seed activation, candidate unroll + low-pT looper stop,
+//               propagation to the layer, SelectHitIndices, missed-layer
+//               handling, hole records        (one thread per candidate)
+//   2. chi2   : propagate to each selected hit, chi2, strip checks,
+//               hit records                   (one thread per (cand, hit))
+//   3. clone  : per-seed ranking of the records (warp top-M selection),
+//               overlap hits, extras, best short candidate, new candidates
+//               (one warp per seed) -- CandCloner::ProcessSeedRange
+//   4. update : UpdateWithLastHit for candidates that took a hit
+// then one merge launch (MergeCandsAndBestShortOne) and one export launch.
 #include "internal.h"
+#include "find_host.h"
+#include "find_steps.cuh"
+
+#include <algorithm>
+#include <climits>
+#include <cstring>
+#include <vector>
 
 namespace mkfg {
-void finder_release(mkfg_context* ctx) { (void)ctx; }
+
+constexpr int kBlock = 256;
+
+//------------------------------------------------------------------------------
+// Kernel 1: prep
+//------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_prep(EventDev E, const FindConfigDev* __restrict__ Cp,
+                                                 int step) {
+  const FindConfigDev& C = *Cp;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = t / kSlots, c = t % kSlots;
+  const bool in_range = s < E.n_seeds;
+  const int lane = threadIdx.x & 31;
+  const unsigned grp = 0xffu << (lane & ~7);
+
+  int reg = 0, layer = -1, prev_layer = -1, state = kFinished, ncand = 0, buf = 0;
+  if (in_range) {
+    reg = E.region[s];
+    layer = plan_layer(C, reg, step);
+    prev_layer = layer >= 0 ? C.plan[reg][C.pickup[reg] + step - 1] : -1;
+    state = E.state[s];
+    ncand = E.n_cands[s];
+    buf = E.cur[s];
+    // find_tracks_unroll_candidates (mkFit/MkBuilder.cc:1503-1566).
+    if (layer >= 0 && state == kDormant && E.pickup_layer[s] == prev_layer) state = kFinding;
+  }
+  const int slot = s * kSlots + c;
+  const CandSoA& B = E.cand[buf];
+  bool active = false;
+  float par[6], err[21];
+  int chg = 0;
+  if (in_range && layer >= 0 && state == kFinding && c < ncand) {
+    const int last = B.last[slot];
+    if (hot_index(node_hot_of(E, s, last)) != -2) {
+      load_state(B, slot, par, err);
+      chg = B.chg[slot];
+      active = true;
+      const float pt = fabsf(1.f / par[3]);
+      if (pt < 1.2f) {
+        const float dphi = fabsf(f_atan2(par[1], par[0]) - par[4]);
+        if (par[0] * par[0] + par[1] * par[1] > 625.f && dphi > 1.371f && dphi < 4.512f) {
+          B.last[slot] = arena_append(E, s, -2, layer, 0.f, last);
+          B.nmiss[slot] += 1;
+          active = false;
+        }
+      }
+    }
+  }
+  const unsigned act = __ballot_sync(0xffffffffu, active) & grp;
+  if (in_range && c == 0) {
+    if (layer >= 0 && state == kFinding && act == 0) state = kFinished;
+    E.state[s] = state;
+  }
+  if (!in_range) return;
+
+  // Default: no records for this slot.
+  const size_t rbase = (size_t)s * kRecPerSeed + c * kRecPerCand;
+  int xs = 0, wsr = kWsrOutside, extra = 0;
+  if (active) {
+    const LayerDev& L = C.layer[layer];
+    float ppar[6], perr[21];
+    if (L.is_barrel)
+      propagate_to_r(par, err, chg, L.propagate_to, C.inter_pflags, C.mat, false, ppar, perr);
+    else
+      propagate_to_z(par, err, chg, L.propagate_to, C.inter_pflags, C.mat, false, ppar, perr);
+    const int ev_base = 0;
+    const int hit_base = E.layer_begin[ev_base + layer];
+    const int stride = E.cand[0].cap;
+    xs = select_hits(E, L, layer, hit_base, ppar, perr, E.xhit + slot, stride, wsr);
+    // find_tracks_handle_missed_layers (mkFit/MkBuilder.cc:1568-1637).
+    const float cand_r = hypot_f(ppar[0], ppar[1]);
+    if (L.is_barrel && cand_r < L.rin) {
+      xs = 0;
+      wsr = kWsrOutside;
+      extra = (reg == 2) ? 2 : 1;
+      if (extra == 2)
+        E.extra_last[slot] = arena_append(E, s, -2, layer, 0.f, B.last[slot]);
+    } else if (wsr == kWsrOutside) {
+      extra = 1;
+    }
+#pragma unroll
+    for (int e = 0; e < 6; ++e) E.ppar[e * stride + slot] = ppar[e];
+#pragma unroll
+    for (int e = 0; e < 21; ++e) E.perr[e * stride + slot] = perr[e];
+    // Hole record (MkFinder::FindCandidatesCloneEngine, :1245-1283).
+    if (wsr != kWsrOutside) {
+      const int nin = B.ninside[slot], ntl = B.ntail[slot];
+      int fake = ((nin + ntl) < C.max_holes && ntl < C.max_consec_holes) ? -1 : -2;
+      if (wsr == kWsrEdge) fake = -3;
+      const int nfound = B.nfound[slot], nover = B.nover[slot];
+      const int ntail_rec = fake == -1 ? ntl + 1 : ntl;
+      const float pt = fabsf(1.0f / ppar[3]);
+      const float chi2 = B.chi2[slot];
+      const size_t r = rbase + kMaxXHits;
+      E.rhit[r] = fake;
+      E.rmodule[r] = -1;
+      E.rcounts[r] = nfound | (ntail_rec << 8) | (nover << 16) | (nin << 24);
+      E.rpt[r] = pt;
+      E.rchi2[r] = chi2;
+      E.rchi2hit[r] = 0.f;
+      E.rscore[r] = score_struct(nfound, ntail_rec, nover, nin, chi2, pt);
+    } else {
+      E.rhit[rbase + kMaxXHits] = kRecInvalid;
+    }
+    if (xs > 0) {
+      const int base = atomicAdd(&E.pair_count[step], xs);
+      for (int h = 0; h < xs; ++h) E.pairs[base + h] = slot * kMaxXHits + h;
+    }
+  } else {
+    E.rhit[rbase + kMaxXHits] = kRecInvalid;
+  }
+  for (int h = 0; h < kMaxXHits; ++h)
+    if (h >= xs) E.rhit[rbase + h] = kRecInvalid;
+  E.xsize[slot] = active ? xs : 0;
+  E.wsr[slot] = wsr | (extra << 8);
+}
+
+//------------------------------------------------------------------------------
+// Kernel 2: chi2 of every (candidate, selected hit) pair
+// (MkFinder::FindCandidatesCloneEngine, mkFit/MkFinder.cc:1116-1240).
+//------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_chi2(EventDev E, const FindConfigDev* __restrict__ Cp,
+                                                 int step) {
+  const FindConfigDev& C = *Cp;
+  const int n_pairs = E.pair_count[step];
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n_pairs; p += gridDim.x * blockDim.x) {
+    const int code = E.pairs[p];
+    const int slot = code / kMaxXHits, h = code % kMaxXHits;
+    const int s = slot / kSlots, c = slot % kSlots;
+    const int reg = E.region[s];
+    const int layer = plan_layer(C, reg, step);
+    const LayerDev& L = C.layer[layer];
+    const int stride = E.cand[0].cap;
+    float ppar[6], perr[21];
+#pragma unroll
+    for (int e = 0; e < 6; ++e) ppar[e] = E.ppar[e * stride + slot];
+#pragma unroll
+    for (int e = 0; e < 21; ++e) perr[e] = E.perr[e * stride + slot];
+    const CandSoA& B = E.cand[E.cur[s]];
+    const int chg = B.chg[slot];
+    const int hidx = E.xhit[h * stride + slot];
+    const int g = E.layer_begin[layer] + hidx;
+    float mpos[3], merr[6];
+#pragma unroll
+    for (int e = 0; e < 3; ++e) mpos[e] = __ldg(E.hpos + e * E.hstride + g);
+#pragma unroll
+    for (int e = 0; e < 6; ++e) merr[e] = __ldg(E.herr + e * E.hstride + g);
+    const uint32_t info = __ldg(E.hinfo + g);
+
+    // kalmanPropagateAndComputeChi2[Endcap] (mkFit/KalmanUtilsMPlex.cc:518-544, 744-770).
+    float hpar[6], herr_[21];
+    float chi2;
+    if (L.is_barrel) {
+      propagate_to_r(ppar, perr, chg, hypot_f(mpos[0], mpos[1]), C.intra_pflags, C.mat, false,
+                     hpar, herr_);
+      chi2 = kalman_barrel<true, false>(hpar, herr_, mpos, merr, hpar, herr_);
+    } else {
+      propagate_to_z(ppar, perr, chg, mpos[2], C.intra_pflags, C.mat, false, hpar, herr_);
+      chi2 = kalman_endcap<true, false>(hpar, herr_, mpos, merr, hpar, herr_);
+    }
+    chi2 = fabsf(chi2);
+    const size_t r = (size_t)s * kRecPerSeed + c * kRecPerCand + h;
+    bool ok = chi2 < dynamic_chi2_cut(L, C.chi2_cut_min, ppar);
+    if (ok && !L.is_pix) {
+      ok = strip_q_compatible(L.is_barrel, perr, hpar, mpos, merr);
+      ok &= strip_charge_ok(L.is_barrel, info >> 12, hpar, merr);
+    }
+    const int nfound = B.nfound[slot];
+    if (ok && L.is_pix) {
+      // Seed-hit layer check on the first (seed) nodes of the arena.
+      for (int i = 0; i <= nfound && i <= 2; ++i)
+        if (hot_layer(node_hot_of(E, s, i)) == layer) ok = false;
+    }
+    if (!ok) {
+      E.rhit[r] = kRecInvalid;
+      continue;
+    }
+    const int nover = B.nover[slot], nholes = B.ninside[slot] + B.ntail[slot];
+    const float pt = fabsf(1.0f / ppar[3]);
+    const float tchi2 = B.chi2[slot] + chi2;
+    E.rhit[r] = hidx;
+    E.rmodule[r] = info & 0xfff;
+    E.rcounts[r] = (nfound + 1) | (0 << 8) | (nover << 16) | (nholes << 24);
+    E.rpt[r] = pt;
+    E.rchi2[r] = tchi2;
+    E.rchi2hit[r] = chi2;
+    E.rscore[r] = score_struct(nfound + 1, 0, nover, nholes, tchi2, pt);
+  }
+}
+
+//------------------------------------------------------------------------------
+// Kernel 3: per-seed candidate cloning (CandCloner::ProcessSeedRange,
+// mkFit/CandCloner.cc:36-189). One warp per seed.
+//------------------------------------------------------------------------------
+struct NewCand {
+  int parent;    // slot offset (0..7) in the current buffer, or 8 + extra slot
+  int hit;       // added hit index (or hole code)
+  float chi2hit;
+  int ov;        // overlap: match index 0/1 in the parent's pair, or -1
+  float score;
+  int is_extra;  // 1: held-back copy (extra), 2: extra with a stop (-2) node
+};
+
+__device__ __forceinline__ void copy_slot(const CandSoA& from, int fs, const CandSoA& to, int ts) {
+#pragma unroll
+  for (int e = 0; e < 6; ++e) to.par[e * to.cap + ts] = from.par[e * from.cap + fs];
+#pragma unroll
+  for (int e = 0; e < 21; ++e) to.err[e * to.cap + ts] = from.err[e * from.cap + fs];
+  to.chg[ts] = from.chg[fs];
+  to.chi2[ts] = from.chi2[fs];
+  to.score[ts] = from.score[fs];
+  to.last[ts] = from.last[fs];
+  to.nfound[ts] = from.nfound[fs];
+  to.nmiss[ts] = from.nmiss[fs];
+  to.nover[ts] = from.nover[fs];
+  to.ninside[ts] = from.ninside[fs];
+  to.ntail[ts] = from.ntail[fs];
+}
+
+// TrackCand::addHitIdx counters (mkFit/HitStructures.h:714-735).
+__device__ __forceinline__ void add_hit_counts(int hit, float chi2, int& nfound, int& nmiss,
+                                               int& ninside, int& ntail, float& tchi2) {
+  if (hit >= 0 || hit == -9) {
+    ++nfound;
+    tchi2 += chi2;
+    ninside += ntail;
+    ntail = 0;
+  } else {
+    ++nmiss;
+    if (hit == -1) ++ntail;
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_clone(EventDev E, const FindConfigDev* __restrict__ Cp,
+                                                  int step) {
+  const FindConfigDev& C = *Cp;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int s = warp;
+  if (s >= E.n_seeds) return;
+  const int reg = E.region[s];
+  const int layer = plan_layer(C, reg, step);
+  if (layer < 0) return;
+  const int state = E.state[s];
+  if (state == kDormant) return;
+  const int ncand = E.n_cands[s];
+  const int cur = E.cur[s];
+  const CandSoA& B = E.cand[cur];
+  const CandSoA& N = E.cand[cur ^ 1];
+  const size_t rb = (size_t)s * kRecPerSeed;
+  const int M = C.max_cands;
+
+  // Overlap candidates per parent (CandCloner consults them in :120-124);
+  // filled in hit order as MkFinder does (:1212-1216).
+  __shared__ HitMatchPair s_hm[kBlock / 32][kSlots];
+  HitMatchPair* hm = s_hm[threadIdx.x >> 5];
+  if (lane < kSlots) {
+    HitMatchPair p;
+    p.reset();
+    if (lane < ncand) {
+      for (int h = 0; h < kMaxXHits; ++h) {
+        const size_t r = rb + lane * kRecPerCand + h;
+        const int hit = E.rhit[r];
+        if (hit == kRecInvalid) continue;
+        const float c2 = E.rchi2hit[r];
+        if (c2 < C.chi2_cut_overlap) p.consider(hit, E.rmodule[r], c2);
+      }
+    }
+    hm[lane] = p;
+  }
+  __syncwarp();
+
+  // Valid records: up to kRecPerSeed, held 5 per lane.
+  constexpr int kPer = (kRecPerSeed + 31) / 32;
+  float sc[kPer];
+  bool valid[kPer];
+  int n_valid = 0;
+#pragma unroll
+  for (int k = 0; k < kPer; ++k) {
+    const int idx = lane + 32 * k;
+    valid[k] = false;
+    sc[k] = 0.f;
+    if (idx < kRecPerSeed) {
+      const int c = idx / kRecPerCand;
+      if (c < ncand && E.rhit[rb + idx] != kRecInvalid) {
+        valid[k] = true;
+        sc[k] = E.rscore[rb + idx];
+      }
+    }
+    n_valid += __popc(__ballot_sync(0xffffffffu, valid[k]));
+  }
+
+  // Extras (held-back candidates) in candidate order (MkBuilder.cc:1600-1626).
+  int extras[kSlots];
+  int extra_kind[kSlots];
+  int n_extras = 0;
+  if (state == kFinding) {
+    for (int c = 0; c < ncand; ++c) {
+      const int k = E.wsr[s * kSlots + c] >> 8;
+      if (k) {
+        extras[n_extras] = c;
+        extra_kind[n_extras] = k;
+        ++n_extras;
+      }
+    }
+  }
+
+  if (n_valid == 0) {
+    // hitsForSeed empty (CandCloner.cc:163-172).
+    if (state != kFinding) return;
+    for (int i = 0; i < n_extras; ++i) {
+      const int c = extras[i];
+      const int src = s * kSlots + c, dst = s * kSlots + i;
+      for (int f = lane; f < 37; f += 32) {
+        if (f < 6) N.par[f * N.cap + dst] = B.par[f * B.cap + src];
+        else if (f < 27) N.err[(f - 6) * N.cap + dst] = B.err[(f - 6) * B.cap + src];
+      }
+      if (lane == 0) {
+        N.chg[dst] = B.chg[src];
+        N.chi2[dst] = B.chi2[src];
+        N.score[dst] = B.score[src];
+        N.nfound[dst] = B.nfound[src];
+        N.nover[dst] = B.nover[src];
+        N.ninside[dst] = B.ninside[src];
+        N.ntail[dst] = B.ntail[src];
+        if (extra_kind[i] == 2) {
+          N.last[dst] = E.extra_last[src];
+          N.nmiss[dst] = B.nmiss[src] + 1;
+        } else {
+          N.last[dst] = B.last[src];
+          N.nmiss[dst] = B.nmiss[src];
+        }
+        E.upd[dst] = 0;
+      }
+    }
+    if (lane == 0) {
+      E.n_cands[s] = n_extras;
+      E.cur[s] = cur ^ 1;
+    }
+    return;
+  }
+
+  // Top-num_hits records in (score desc, record index asc) order: the
+  // reference's std::sort by score; on exact score ties this order is the
+  // stable one.
+  const int num_hits = min(n_valid, M);
+  int top[kSlots];
+  for (int i = 0; i < num_hits; ++i) {
+    float best = -INFINITY;
+    int bidx = INT_MAX;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      const int idx = lane + 32 * k;
+      if (valid[k] && (sc[k] > best || (sc[k] == best && idx < bidx))) {
+        best = sc[k];
+        bidx = idx;
+      }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const float ob = __shfl_xor_sync(0xffffffffu, best, off);
+      const int oi = __shfl_xor_sync(0xffffffffu, bidx, off);
+      if (ob > best || (ob == best && oi < bidx)) {
+        best = ob;
+        bidx = oi;
+      }
+    }
+    top[i] = bidx;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k)
+      if (lane + 32 * k == bidx) valid[k] = false;
+  }
+
+  // Build the new candidate list (sequential logic of ProcessSeedRange).
+  NewCand nc[kSlots];
+  int n_pushed = 0;
+  int ei = 0;
+  float bs_score = E.bshort_valid[s] ? E.bshort.score[s] : -1e16f;  // getScoreWorstPossible
+  int bs_from = -1;
+  for (int ih = 0; ih < num_hits; ++ih) {
+    const int idx = top[ih];
+    const size_t r = rb + idx;
+    const int parent = idx / kRecPerCand;
+    const int hit = E.rhit[r];
+    const float score = E.rscore[r];
+    if (hit == -2) {
+      if (score > bs_score) {
+        bs_score = score;
+        bs_from = idx;
+      }
+      continue;
+    }
+    while (ei < n_extras && E.cand[cur].score[s * kSlots + extras[ei]] > score && n_pushed < M) {
+      nc[n_pushed++] = NewCand{extras[ei], 0, 0.f, -1, 0.f, extra_kind[ei]};
+      ++ei;
+    }
+    if (n_pushed >= M) break;
+    int ov = -1;
+    const float ppt = fabsf(1.f / B.par[3 * B.cap + s * kSlots + parent]);
+    if (ppt > C.pt_cut_overlap && hit >= 0) ov = hm[parent].find(hit, E.rmodule[r]);
+    nc[n_pushed++] = NewCand{parent, hit, E.rchi2hit[r], ov, score, 0};
+  }
+  while (ei < n_extras && n_pushed < M) {
+    nc[n_pushed++] = NewCand{extras[ei], 0, 0.f, -1, 0.f, extra_kind[ei]};
+    ++ei;
+  }
+
+  // Best short candidate (a -2 record scoring above the current best).
+  if (bs_from >= 0) {
+    const int parent = bs_from / kRecPerCand;
+    const int src = s * kSlots + parent;
+    for (int f = lane; f < 27; f += 32) {
+      if (f < 6) E.bshort.par[f * E.bshort.cap + s] = B.par[f * B.cap + src];
+      else E.bshort.err[(f - 6) * E.bshort.cap + s] = B.err[(f - 6) * B.cap + src];
+    }
+    if (lane == 0) {
+      int nfound = B.nfound[src], nmiss = B.nmiss[src], nin = B.ninside[src], ntl = B.ntail[src];
+      float chi2 = B.chi2[src];
+      add_hit_counts(-2, 0.f, nfound, nmiss, nin, ntl, chi2);
+      E.bshort.last[s] = arena_append(E, s, -2, layer, 0.f, B.last[src]);
+      E.bshort.chg[s] = B.chg[src];
+      E.bshort.chi2[s] = chi2;
+      E.bshort.score[s] = bs_score;
+      E.bshort.nfound[s] = nfound;
+      E.bshort.nmiss[s] = nmiss;
+      E.bshort.nover[s] = B.nover[src];
+      E.bshort.ninside[s] = nin;
+      E.bshort.ntail[s] = ntl;
+      E.bshort_valid[s] = 1;
+    }
+  }
+
+  // Materialize the new candidates into the other buffer.
+  for (int i = 0; i < n_pushed; ++i) {
+    const NewCand& n = nc[i];
+    const int src = s * kSlots + n.parent, dst = s * kSlots + i;
+    for (int f = lane; f < 27; f += 32) {
+      if (f < 6) N.par[f * N.cap + dst] = B.par[f * B.cap + src];
+      else N.err[(f - 6) * N.cap + dst] = B.err[(f - 6) * B.cap + src];
+    }
+    if (lane == 0) {
+      int nfound = B.nfound[src], nmiss = B.nmiss[src], nin = B.ninside[src], ntl = B.ntail[src];
+      int nover = B.nover[src];
+      float chi2 = B.chi2[src];
+      int last = B.last[src];
+      float score = B.score[src];
+      int upd = 0;
+      if (n.is_extra) {
+        if (n.is_extra == 2) {
+          last = E.extra_last[src];
+          ++nmiss;
+        }
+      } else {
+        add_hit_counts(n.hit, n.chi2hit, nfound, nmiss, nin, ntl, chi2);
+        last = arena_append(E, s, n.hit, layer, n.chi2hit, last);
+        score = n.score;
+        if (n.ov >= 0) {
+          const HitMatchPair& p = hm[n.parent];
+          add_hit_counts(p.hit[n.ov], p.chi2[n.ov], nfound, nmiss, nin, ntl, chi2);
+          last = arena_append(E, s, p.hit[n.ov], layer, p.chi2[n.ov], last);
+          ++nover;
+        }
+        upd = n.hit >= 0;
+      }
+      N.chg[dst] = B.chg[src];
+      N.chi2[dst] = chi2;
+      N.score[dst] = score;
+      N.last[dst] = last;
+      N.nfound[dst] = nfound;
+      N.nmiss[dst] = nmiss;
+      N.nover[dst] = nover;
+      N.ninside[dst] = nin;
+      N.ntail[dst] = ntl;
+      E.upd[dst] = upd;
+    }
+  }
+  if (lane == 0) {
+    E.n_cands[s] = n_pushed;
+    E.cur[s] = cur ^ 1;
+  }
+}
+
+//------------------------------------------------------------------------------
+// Kernel 4: UpdateWithLastHit + CopyOutParErr (mkFit/MkFinder.cc:1291-1335,
+// kalmanPropagateAndUpdate[Endcap], mkFit/KalmanUtilsMPlex.cc:471-505, 697-731).
+//------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_update(EventDev E, const FindConfigDev* __restrict__ Cp,
+                                                   int step) {
+  const FindConfigDev& C = *Cp;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = t / kSlots, c = t % kSlots;
+  if (s >= E.n_seeds) return;
+  const int reg = E.region[s];
+  const int layer = plan_layer(C, reg, step);
+  if (layer < 0) return;
+  if (c >= E.n_cands[s]) return;
+  const int slot = s * kSlots + c;
+  if (!E.upd[slot]) return;
+  E.upd[slot] = 0;
+  const CandSoA& B = E.cand[E.cur[s]];
+  float par[6], err[21];
+  load_state(B, slot, par, err);
+  int chg = B.chg[slot];
+  const int hv = node_hot_of(E, s, B.last[slot]);
+  const int hl = hot_layer(hv);
+  // After an arena overflow (reported through err_flags) the last node may
+  // not be a hit: skip rather than read outside the hit arrays.
+  if (hot_index(hv) < 0 || hl < 0 || hl >= C.n_layers) return;
+  const int g = E.layer_begin[hl] + hot_index(hv);
+  float mpos[3], merr[6];
+#pragma unroll
+  for (int e = 0; e < 3; ++e) mpos[e] = __ldg(E.hpos + e * E.hstride + g);
+#pragma unroll
+  for (int e = 0; e < 6; ++e) merr[e] = __ldg(E.herr + e * E.hstride + g);
+  const LayerDev& L = C.layer[hl];
+  float ppar[6], perr[21];
+  if (L.is_barrel) {
+    propagate_to_r(par, err, chg, hypot_f(mpos[0], mpos[1]), C.inter_pflags, C.mat, false, ppar, perr);
+    kalman_barrel<false, true>(ppar, perr, mpos, merr, par, err);
+  } else {
+    propagate_to_z(par, err, chg, mpos[2], C.inter_pflags, C.mat, false, ppar, perr);
+    kalman_endcap<false, true>(ppar, perr, mpos, merr, par, err);
+  }
+  if (par[3] < 0) {
+    chg = -chg;
+    par[3] = -par[3];
+  }
+  store_state(B, slot, par, err);
+  B.chg[slot] = chg;
+}
+
+//------------------------------------------------------------------------------
+// Kernel 5: CombCandidate::MergeCandsAndBestShortOne (update_score, sort)
+// (mkFit/HitStructures.cc:511-552). One thread per seed.
+//------------------------------------------------------------------------------
+__device__ __forceinline__ float cand_score(const CandSoA& B, int slot) {
+  const float pt = fabsf(1.f / B.par[3 * B.cap + slot]);
+  float chi2 = B.chi2[slot];
+  if (chi2 < 0) chi2 = 0.f;
+  return score_calc(B.nfound[slot], 0, B.nover[slot], B.ninside[slot], chi2, pt, false);
+}
+
+__global__ void k_merge(EventDev E, const FindConfigDev* __restrict__ Cp) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= E.n_seeds) return;
+  const FindConfigDev& C = *Cp;
+  const int cur = E.cur[s];
+  const CandSoA& B = E.cand[cur];
+  const CandSoA& N = E.cand[cur ^ 1];
+  int n = E.n_cands[s];
+  float score[kSlots + 1];
+  int order[kSlots + 1];
+  for (int c = 0; c < n; ++c) {
+    score[c] = cand_score(B, s * kSlots + c);
+    order[c] = c;
+  }
+  // Insertion sort by score, descending (std::sort on <= 16 elements).
+  for (int i = 1; i < n; ++i) {
+    const int o = order[i];
+    const float v = score[o];
+    int j = i;
+    while (j > 0 && score[order[j - 1]] < v) {
+      order[j] = order[j - 1];
+      --j;
+    }
+    order[j] = o;
+  }
+  const bool has_bs = E.bshort_valid[s];
+  float bs = has_bs ? cand_score(E.bshort, s) : 0.f;
+  int ins = -1;  // position of the best short candidate in the final list
+  if (n > 0) {
+    if (has_bs && bs > score[order[n - 1]]) {
+      int ci = 0;
+      while (score[order[ci]] > bs) ++ci;
+      if (n >= C.max_cands) --n;
+      ins = ci;
+    }
+  } else if (has_bs) {
+    ins = 0;
+  }
+  // Write the final list into the other buffer: sorted cands with the
+  // best short one inserted.
+  int w = 0;
+  for (int i = 0; i <= n; ++i) {
+    if (i == ins) {
+      const int dst = s * kSlots + w;
+      copy_slot(E.bshort, s, N, dst);
+      N.score[dst] = bs;
+      ++w;
+    }
+    if (i == n) break;
+    const int src = s * kSlots + order[i];
+    const int dst = s * kSlots + w;
+    copy_slot(B, src, N, dst);
+    N.score[dst] = score[order[i]];
+    ++w;
+  }
+  E.n_cands[s] = w;
+  E.cur[s] = cur ^ 1;
+  E.bshort_valid[s] = 0;
+}
+
+//------------------------------------------------------------------------------
+// Kernel 6: export (TrackCand::exportTrack, mkFit/HitStructures.cc:448-478).
+//------------------------------------------------------------------------------
+struct FindOutDev {
+  int* n_cands;
+  int* region;
+  float* par;
+  float* err;
+  int* chg;
+  float* chi2;
+  float* score;
+  int* nfound;
+  int* ntot;
+  int* noverlap;
+  int* ninside;
+  int* ntail;
+  int* hit_idx;
+  int* hit_lyr;
+  int m;  // output slots per seed
+};
+
+__global__ void k_export(EventDev E, FindOutDev O) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = t / kSlots, c = t % kSlots;
+  if (s >= E.n_seeds || c >= O.m) return;
+  const int label = E.seed_label[s];
+  const int n = E.n_cands[s];
+  if (c == 0) {
+    O.n_cands[label] = min(n, O.m);
+    O.region[label] = E.region[s];
+  }
+  if (c >= n) return;
+  const CandSoA& B = E.cand[E.cur[s]];
+  const int slot = s * kSlots + c;
+  const int o = label * O.m + c;
+  for (int e = 0; e < 6; ++e) O.par[o * 6 + e] = B.par[e * B.cap + slot];
+  for (int e = 0; e < 21; ++e) O.err[o * 21 + e] = B.err[e * B.cap + slot];
+  O.chg[o] = B.chg[slot];
+  O.chi2[o] = B.chi2[slot];
+  O.score[o] = B.score[slot];
+  O.nfound[o] = B.nfound[slot];
+  const int ntot = B.nfound[slot] + B.nmiss[slot];
+  O.ntot[o] = ntot;
+  O.noverlap[o] = B.nover[slot];
+  O.ninside[o] = B.ninside[slot];
+  O.ntail[o] = B.ntail[slot];
+  int node = B.last[slot];
+  for (int k = kExportHits - 1; k >= 0; --k) {
+    O.hit_idx[o * kExportHits + k] = -100;
+    O.hit_lyr[o * kExportHits + k] = -100;
+  }
+  for (int k = ntot - 1; k >= 0; --k) {
+    const int hv = node_hot_of(E, s, node);
+    if (k < kExportHits) {
+      O.hit_idx[o * kExportHits + k] = hot_index(hv);
+      O.hit_lyr[o * kExportHits + k] = hot_layer(hv);
+    }
+    node = E.node_prev[(size_t)s * E.hot_cap + node];
+    if (node < 0) break;
+  }
+}
+
+//------------------------------------------------------------------------------
+// Host side
+//------------------------------------------------------------------------------
+struct Finder {
+  bool configured = false;
+  FindConfigDev host_cfg;
+  FindConfigDev* d_cfg = nullptr;
+  std::vector<LayerBinning> binning;
+  std::vector<float> layer_desc;  // n_layers x LC_COUNT
+  int n_bins = 0;
+  // Event device memory (grow-only arenas).
+  DevBuf hits, seeds, cands, scratch, recs, arena, outb;
+  EventDev ev{};
+  int n_seeds = 0;
+  int events_loaded = 0;
+};
+
+namespace {
+
+Finder* finder_of(mkfg_context* ctx) {
+  if (!ctx->finder) ctx->finder = new Finder;
+  return static_cast<Finder*>(ctx->finder);
+}
+
+template <typename T>
+T* carve(char*& p, size_t n) {
+  T* r = reinterpret_cast<T*>(p);
+  p += ((n * sizeof(T) + 255) / 256) * 256;
+  return r;
+}
+size_t rounded(size_t bytes) { return ((bytes + 255) / 256) * 256; }
+
+}  // namespace
+
+void finder_release(mkfg_context* ctx) {
+  if (!ctx || !ctx->finder) return;
+  Finder* f = static_cast<Finder*>(ctx->finder);
+  if (f->d_cfg) cudaFree(f->d_cfg);
+  f->hits.release();
+  f->seeds.release();
+  f->cands.release();
+  f->scratch.release();
+  f->recs.release();
+  f->arena.release();
+  f->outb.release();
+  delete f;
+  ctx->finder = nullptr;
+}
+
 }  // namespace mkfg
+
+using namespace mkfg;
+
+extern "C" int mkfg_finder_setup(mkfg_context* ctx, const mkfg_find_config* cfg) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  MKFG_REQUIRE(cfg && cfg->layer_desc && cfg->plans && cfg->plan_len && cfg->pickup,
+               "null finder configuration");
+  MKFG_REQUIRE(cfg->n_layers > 0 && cfg->n_layers <= kMaxLayers, "n_layers out of range");
+  MKFG_REQUIRE(cfg->n_regions > 0 && cfg->n_regions <= kMaxRegions, "n_regions out of range");
+  MKFG_REQUIRE(cfg->max_plan > 0 && cfg->max_plan <= kMaxPlan, "max_plan out of range");
+  MKFG_REQUIRE(cfg->max_cands_per_seed >= 1 && cfg->max_cands_per_seed <= kSlots,
+               "max_cands_per_seed must be in [1, %d]", kSlots);
+  MKFG_REQUIRE(cfg->requires_prop_to_hit == 1,
+               "only the propagate-to-hit finding mode (CMS geometries) is implemented");
+  Finder* f = finder_of(ctx);
+  FindConfigDev& H = f->host_cfg;
+  std::memset(&H, 0, sizeof(H));
+  f->layer_desc.assign(cfg->layer_desc, cfg->layer_desc + (size_t)cfg->n_layers * LC_COUNT);
+  f->binning.resize(cfg->n_layers);
+  int off = 0;
+  for (int l = 0; l < cfg->n_layers; ++l) {
+    const float* d = cfg->layer_desc + (size_t)l * LC_COUNT;
+    LayerBinning b = setup_layer_binning(d);
+    b.bin_offset = off;
+    off += b.nq * kPhiBins;
+    f->binning[l] = b;
+    LayerDev& L = H.layer[l];
+    L.rin = d[LC_RIN];
+    L.rout = d[LC_ROUT];
+    L.zmin = d[LC_ZMIN];
+    L.zmax = d[LC_ZMAX];
+    L.propagate_to = d[LC_PROPAGATE_TO];
+    L.hole_min = d[LC_HOLE_MIN];
+    L.hole_max = d[LC_HOLE_MAX];
+    L.min_dphi = d[LC_MIN_DPHI];
+    L.max_dphi = d[LC_MAX_DPHI];
+    L.min_dq = d[LC_MIN_DQ];
+    L.max_dq = d[LC_MAX_DQ];
+    L.c_dp_sf = d[LC_C_DP_SF]; L.c_dp_0 = d[LC_C_DP_0]; L.c_dp_1 = d[LC_C_DP_1]; L.c_dp_2 = d[LC_C_DP_2];
+    L.c_dq_sf = d[LC_C_DQ_SF]; L.c_dq_0 = d[LC_C_DQ_0]; L.c_dq_1 = d[LC_C_DQ_1]; L.c_dq_2 = d[LC_C_DQ_2];
+    L.c_c2_sf = d[LC_C_C2_SF]; L.c_c2_0 = d[LC_C_C2_0]; L.c_c2_1 = d[LC_C_C2_1]; L.c_c2_2 = d[LC_C_C2_2];
+    L.qmin = b.qmin;
+    L.fq = b.fq;
+    L.nq = b.nq;
+    L.bin_offset = b.bin_offset;
+    L.is_barrel = b.barrel;
+    L.has_hole = d[LC_HAS_HOLE] > 0.5f;
+    L.is_pix = d[LC_IS_PIX] > 0.5f;
+  }
+  f->n_bins = off;
+  H.n_layers = cfg->n_layers;
+  H.n_regions = cfg->n_regions;
+  int max_steps = 0;
+  for (int r = 0; r < cfg->n_regions; ++r) {
+    H.plan_len[r] = cfg->plan_len[r];
+    H.pickup[r] = cfg->pickup[r];
+    MKFG_REQUIRE(cfg->plan_len[r] <= kMaxPlan && cfg->pickup[r] >= 0 &&
+                     cfg->pickup[r] < std::max(1, cfg->plan_len[r]),
+                 "bad plan for region %d", r);
+    for (int i = 0; i < cfg->plan_len[r]; ++i) {
+      const int l = cfg->plans[r * cfg->max_plan + i];
+      MKFG_REQUIRE(l >= 0 && l < cfg->n_layers, "plan layer out of range");
+      H.plan[r][i] = l;
+    }
+    max_steps = std::max(max_steps, cfg->plan_len[r] - cfg->pickup[r] - 1);
+  }
+  H.max_steps = max_steps;
+  H.max_cands = cfg->max_cands_per_seed;
+  H.max_holes = cfg->max_holes_per_cand;
+  H.max_consec_holes = cfg->max_consec_holes;
+  H.chi2_cut_min = cfg->chi2_cut_min;
+  H.chi2_cut_overlap = cfg->chi2_cut_overlap;
+  H.pt_cut_overlap = cfg->pt_cut_overlap;
+  H.inter_pflags = cfg->inter_layer_pflags;
+  H.intra_pflags = cfg->intra_layer_pflags;
+  H.mat = Material{ctx->d_rl, ctx->d_xi};
+  if (!f->d_cfg) MKFG_CUDA_TRY(cudaMalloc(&f->d_cfg, sizeof(FindConfigDev)));
+  MKFG_CUDA_TRY(cudaMemcpyAsync(f->d_cfg, &H, sizeof(H), cudaMemcpyHostToDevice, ctx->stream));
+  MKFG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  f->configured = true;
+  return MKFG_OK;
+}
+
+namespace mkfg {
+
+// Host preparation + upload of one event into the finder's device buffers.
+static int upload_event(mkfg_context* ctx, Finder* f, const mkfg_event* ev) {
+  const int L = f->host_cfg.n_layers;
+  MKFG_REQUIRE(ev->n_layers == L, "event has %d layers, configuration %d", ev->n_layers, L);
+  const int nh = ev->layer_begin[L];
+  for (int l = 0; l < L; ++l)
+    MKFG_REQUIRE(ev->layer_begin[l + 1] - ev->layer_begin[l] <= 65535,
+                 "layer %d holds more than 65535 hits", l);
+  const int S = ev->n_seeds;
+  for (int s = 0; s < S; ++s)
+    MKFG_REQUIRE(ev->seed_nhits[s] >= 1 && ev->seed_nhits[s] <= 4, "seed %d hit count", s);
+
+  // Hits: bins and sorted arrays.
+  EventHitsPrep prep;
+  prepare_event_hits(f->binning, ev->layer_begin, L, ev->pos, nh, ev->detid, ev->cpcm, prep);
+  // Seed partition and order.
+  SeedInput si{S, ev->seed_par, ev->seed_chg, ev->seed_nhits, ev->seed_hit_layer, ev->seed_hit_index};
+  SeedOrder so;
+  partition_seeds_cms2017(f->layer_desc.data(), L, si, ev->layer_begin, ev->pos, nh, so);
+
+  cudaStream_t st = ctx->stream;
+  int rc;
+  // ---- hits
+  {
+    const size_t need = rounded(sizeof(float) * 9 * std::max(nh, 1)) + rounded(4 * std::max(nh, 1)) +
+                        rounded(4 * (L + 1)) + rounded(4 * std::max(f->n_bins, 1)) +
+                        3 * rounded(4 * std::max(nh, 1));
+    if ((rc = f->hits.ensure(need))) return rc;
+    char* p = f->hits.as<char>();
+    float* d_pos = carve<float>(p, 3 * (size_t)std::max(nh, 1));
+    float* d_err = carve<float>(p, 6 * (size_t)std::max(nh, 1));
+    uint32_t* d_info = carve<uint32_t>(p, std::max(nh, 1));
+    int* d_lb = carve<int>(p, L + 1);
+    uint32_t* d_bins = carve<uint32_t>(p, std::max(f->n_bins, 1));
+    float* d_sphi = carve<float>(p, std::max(nh, 1));
+    float* d_sq = carve<float>(p, std::max(nh, 1));
+    int* d_srank = carve<int>(p, std::max(nh, 1));
+    if (nh > 0) {
+      MKFG_CUDA_TRY(cudaMemcpyAsync(d_pos, ev->pos, 12 * (size_t)nh, cudaMemcpyHostToDevice, st));
+      MKFG_CUDA_TRY(cudaMemcpyAsync(d_err, ev->err, 24 * (size_t)nh, cudaMemcpyHostToDevice, st));
+      MKFG_CUDA_TRY(cudaMemcpyAsync(d_info, prep.hinfo.data(), 4 * (size_t)nh, cudaMemcpyHostToDevice, st));
+      MKFG_CUDA_TRY(cudaMemcpyAsync(d_sphi, prep.sphi.data(), 4 * (size_t)nh, cudaMemcpyHostToDevice, st));
+      MKFG_CUDA_TRY(cudaMemcpyAsync(d_sq, prep.sq.data(), 4 * (size_t)nh, cudaMemcpyHostToDevice, st));
+      MKFG_CUDA_TRY(cudaMemcpyAsync(d_srank, prep.srank.data(), 4 * (size_t)nh, cudaMemcpyHostToDevice, st));
+    }
+    MKFG_CUDA_TRY(cudaMemcpyAsync(d_lb, ev->layer_begin, 4 * (size_t)(L + 1), cudaMemcpyHostToDevice, st));
+    MKFG_CUDA_TRY(cudaMemcpyAsync(d_bins, prep.bins.data(), 4 * (size_t)f->n_bins, cudaMemcpyHostToDevice, st));
+    f->ev.hpos = d_pos;
+    f->ev.herr = d_err;
+    f->ev.hstride = std::max(nh, 1);
+    f->ev.hinfo = d_info;
+    f->ev.layer_begin = d_lb;
+    f->ev.bins = d_bins;
+    f->ev.sphi = d_sphi;
+    f->ev.sq = d_sq;
+    f->ev.srank = d_srank;
+  }
+  // ---- seeds and candidates
+  const int SC = std::max(S, 1) * kSlots;
+  const int max_steps = f->host_cfg.max_steps;
+  const int M = f->host_cfg.max_cands;
+  const int hot_cap = ((8 + max_steps * (2 * M + 3)) + 31) / 32 * 32;
+  {
+    const size_t per_buf = rounded(4 * (size_t)SC) * 37;
+    const size_t need = 2 * per_buf + rounded(4 * (size_t)std::max(S, 1)) * 37 + rounded(4 * (size_t)std::max(S, 1)) * 9;
+    if ((rc = f->cands.ensure(need))) return rc;
+    char* p = f->cands.as<char>();
+    auto mk = [&](int cap) {
+      CandSoA b;
+      b.cap = cap;
+      b.par = carve<float>(p, 6 * (size_t)cap);
+      b.err = carve<float>(p, 21 * (size_t)cap);
+      b.chg = carve<int>(p, cap);
+      b.chi2 = carve<float>(p, cap);
+      b.score = carve<float>(p, cap);
+      b.last = carve<int>(p, cap);
+      b.nfound = carve<int>(p, cap);
+      b.nmiss = carve<int>(p, cap);
+      b.nover = carve<int>(p, cap);
+      b.ninside = carve<int>(p, cap);
+      b.ntail = carve<int>(p, cap);
+      return b;
+    };
+    f->ev.cand[0] = mk(SC);
+    f->ev.cand[1] = mk(SC);
+    f->ev.bshort = mk(std::max(S, 1));
+    const int SS = std::max(S, 1);
+    f->ev.seed_label = carve<int>(p, SS);
+    f->ev.seed_event = carve<int>(p, SS);
+    f->ev.region = carve<int>(p, SS);
+    f->ev.pickup_layer = carve<int>(p, SS);
+    f->ev.state = carve<int>(p, SS);
+    f->ev.n_cands = carve<int>(p, SS);
+    f->ev.cur = carve<int>(p, SS);
+    f->ev.hot_size = carve<int>(p, SS);
+    f->ev.bshort_valid = carve<int>(p, SS);
+  }
+  {
+    const size_t need = rounded(4 * (size_t)SC) * (27 + kMaxXHits + 4) + rounded(4 * (size_t)SC * kMaxXHits) +
+                        rounded(4 * (size_t)(max_steps + 2)) + rounded(64);
+    if ((rc = f->scratch.ensure(need))) return rc;
+    char* p = f->scratch.as<char>();
+    f->ev.ppar = carve<float>(p, 6 * (size_t)SC);
+    f->ev.perr = carve<float>(p, 21 * (size_t)SC);
+    f->ev.xsize = carve<int>(p, SC);
+    f->ev.xhit = carve<int>(p, (size_t)kMaxXHits * SC);
+    f->ev.wsr = carve<int>(p, SC);
+    f->ev.extra_last = carve<int>(p, SC);
+    f->ev.upd = carve<int>(p, SC);
+    f->ev.pairs = carve<int>(p, (size_t)SC * kMaxXHits);
+    f->ev.pair_count = carve<int>(p, max_steps + 2);
+    f->ev.err_flags = carve<int>(p, 16);
+  }
+  {
+    const size_t nrec = (size_t)std::max(S, 1) * kRecPerSeed;
+    if ((rc = f->recs.ensure(rounded(4 * nrec) * 7))) return rc;
+    char* p = f->recs.as<char>();
+    f->ev.rscore = carve<float>(p, nrec);
+    f->ev.rchi2 = carve<float>(p, nrec);
+    f->ev.rchi2hit = carve<float>(p, nrec);
+    f->ev.rpt = carve<float>(p, nrec);
+    f->ev.rhit = carve<int>(p, nrec);
+    f->ev.rmodule = carve<int>(p, nrec);
+    f->ev.rcounts = carve<int>(p, nrec);
+  }
+  {
+    const size_t nn = (size_t)std::max(S, 1) * hot_cap;
+    if ((rc = f->arena.ensure(rounded(4 * nn) * 3))) return rc;
+    char* p = f->arena.as<char>();
+    f->ev.node_hot = carve<int>(p, nn);
+    f->ev.node_chi2 = carve<float>(p, nn);
+    f->ev.node_prev = carve<int>(p, nn);
+    f->ev.hot_cap = hot_cap;
+  }
+  f->ev.n_seeds = S;
+
+  // Initial candidates: the seeds in sorted order (CombCandidate::ImportSeed,
+  // mkFit/HitStructures.cc:483-509). Built on the host, uploaded once.
+  std::vector<float> par(6 * (size_t)SC, 0.f), err(21 * (size_t)SC, 0.f), fz(SC, 0.f);
+  std::vector<int> chg(SC, 0), last(SC, 0), nfound(SC, 0), nmiss(SC, 0), zi(SC, 0);
+  std::vector<float> chi2(SC, 0.f), score(SC, 0.f);
+  std::vector<int> label(std::max(S, 1)), region(std::max(S, 1)), pickup(std::max(S, 1)),
+      state(std::max(S, 1), kDormant), ncand(std::max(S, 1), 1), cur(std::max(S, 1), 0),
+      hot_size(std::max(S, 1)), zero(std::max(S, 1), 0);
+  std::vector<int> node_hot((size_t)std::max(S, 1) * hot_cap, 0), node_prev((size_t)std::max(S, 1) * hot_cap, -1);
+  std::vector<float> node_chi2((size_t)std::max(S, 1) * hot_cap, 0.f);
+  for (int s = 0; s < S; ++s) {
+    const int i = so.order[s];
+    label[s] = i;
+    region[s] = so.region[i];
+    const int nhs = ev->seed_nhits[i];
+    pickup[s] = ev->seed_hit_layer[i * 4 + nhs - 1];
+    const int slot = s * kSlots;
+    for (int e = 0; e < 6; ++e) par[e * SC + slot] = ev->seed_par[e * S + i];
+    for (int e = 0; e < 21; ++e) err[e * SC + slot] = ev->seed_err[e * S + i];
+    chg[slot] = ev->seed_chg[i];
+    int nf = 0, nm = 0, nin = 0, ntl = 0;
+    int prev = -1;
+    for (int k = 0; k < nhs; ++k) {
+      const int hi = ev->seed_hit_index[i * 4 + k], hl = ev->seed_hit_layer[i * 4 + k];
+      node_hot[(size_t)s * hot_cap + k] = (hi & 0xffffff) | (hl << 24);
+      node_prev[(size_t)s * hot_cap + k] = prev;
+      prev = k;
+      if (hi >= 0 || hi == -9) {
+        ++nf;
+        nin += ntl;
+        ntl = 0;
+      } else {
+        ++nm;
+        if (hi == -1) ++ntl;
+      }
+    }
+    hot_size[s] = nhs;
+    last[slot] = nhs - 1;
+    nfound[slot] = nf;
+    nmiss[slot] = nm;
+    const float pt = std::abs(1.f / par[3 * SC + slot]);
+    // getScoreCand(cand) with default arguments (Track.h / HitStructures.h:519-531).
+    {
+      const float maxBonus = 8.0f;
+      float bonus = 0.2f * nf + 4.0f;
+      float penalty = 8.0f;
+      if (pt < 0.9f) {
+        penalty *= 1.5f;
+        bonus = std::min(bonus * 1.0f, maxBonus);
+      }
+      score[slot] = bonus * nf + 0.0f * 0 - penalty * nin - 3.0f * 0 - 0.0f;
+    }
+  }
+  auto up = [&](void* d, const void* h, size_t bytes) -> int {
+    MKFG_CUDA_TRY(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st));
+    return MKFG_OK;
+  };
+  CandSoA& B0 = f->ev.cand[0];
+  const int SS = std::max(S, 1);
+  if ((rc = up(B0.par, par.data(), 4 * par.size()))) return rc;
+  if ((rc = up(B0.err, err.data(), 4 * err.size()))) return rc;
+  if ((rc = up(B0.chg, chg.data(), 4 * (size_t)SC))) return rc;
+  if ((rc = up(B0.chi2, chi2.data(), 4 * (size_t)SC))) return rc;
+  if ((rc = up(B0.score, score.data(), 4 * (size_t)SC))) return rc;
+  if ((rc = up(B0.last, last.data(), 4 * (size_t)SC))) return rc;
+  if ((rc = up(B0.nfound, nfound.data(), 4 * (size_t)SC))) return rc;
+  if ((rc = up(B0.nmiss, nmiss.data(), 4 * (size_t)SC))) return rc;
+  MKFG_CUDA_TRY(cudaMemsetAsync(B0.nover, 0, 4 * (size_t)SC, st));
+  MKFG_CUDA_TRY(cudaMemsetAsync(B0.ninside, 0, 4 * (size_t)SC, st));
+  MKFG_CUDA_TRY(cudaMemsetAsync(B0.ntail, 0, 4 * (size_t)SC, st));
+  if ((rc = up(f->ev.seed_label, label.data(), 4 * (size_t)SS))) return rc;
+  MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.seed_event, 0, 4 * (size_t)SS, st));
+  if ((rc = up(f->ev.region, region.data(), 4 * (size_t)SS))) return rc;
+  if ((rc = up(f->ev.pickup_layer, pickup.data(), 4 * (size_t)SS))) return rc;
+  if ((rc = up(f->ev.state, state.data(), 4 * (size_t)SS))) return rc;
+  if ((rc = up(f->ev.n_cands, ncand.data(), 4 * (size_t)SS))) return rc;
+  if ((rc = up(f->ev.cur, cur.data(), 4 * (size_t)SS))) return rc;
+  if ((rc = up(f->ev.hot_size, hot_size.data(), 4 * (size_t)SS))) return rc;
+  MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.bshort_valid, 0, 4 * (size_t)SS, st));
+  if ((rc = up(f->ev.node_hot, node_hot.data(), 4 * node_hot.size()))) return rc;
+  if ((rc = up(f->ev.node_prev, node_prev.data(), 4 * node_prev.size()))) return rc;
+  if ((rc = up(f->ev.node_chi2, node_chi2.data(), 4 * node_chi2.size()))) return rc;
+  MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.upd, 0, 4 * (size_t)SC, st));
+  MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.pair_count, 0, 4 * (size_t)(max_steps + 2), st));
+  MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.err_flags, 0, 64, st));
+  // Keep host staging alive until the copies have been consumed.
+  MKFG_CUDA_TRY(cudaStreamSynchronize(st));
+  f->n_seeds = S;
+  f->events_loaded = 1;
+  return MKFG_OK;
+}
+
+static int run_plain(mkfg_context* ctx, Finder* f) {
+  const int S = f->n_seeds;
+  if (S == 0) return MKFG_OK;
+  cudaStream_t st = ctx->stream;
+  const int threads_c = S * kSlots;
+  const int grid_c = (threads_c + kBlock - 1) / kBlock;
+  const int grid_w = (S * 32 + kBlock - 1) / kBlock;
+  const int grid_p = std::min((S * kSlots * 4 + kBlock - 1) / kBlock, 148 * 16);
+  MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.pair_count, 0, 4 * (size_t)(f->host_cfg.max_steps + 2), st));
+  for (int step = 1; step <= f->host_cfg.max_steps; ++step) {
+    k_prep<<<grid_c, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+    k_chi2<<<std::max(grid_p, 1), kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+    k_clone<<<grid_w, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+    k_update<<<grid_c, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+  }
+  k_merge<<<(S + 127) / 128, 128, 0, st>>>(f->ev, f->d_cfg);
+  MKFG_CUDA_TRY(cudaGetLastError());
+  return MKFG_OK;
+}
+
+static int download(mkfg_context* ctx, Finder* f, mkfg_find_out* out, int n_seeds_in) {
+  const int S = f->n_seeds;
+  const int m = f->host_cfg.max_cands;
+  const size_t no = (size_t)std::max(n_seeds_in, 1) * m;
+  const size_t need = rounded(4 * (size_t)std::max(n_seeds_in, 1)) * 2 +
+                      rounded(4 * no) * (6 + 21 + 9) + rounded(4 * no * kExportHits) * 2;
+  int rc;
+  if ((rc = f->outb.ensure(need))) return rc;
+  char* p = f->outb.as<char>();
+  FindOutDev O;
+  O.m = m;
+  O.n_cands = carve<int>(p, std::max(n_seeds_in, 1));
+  O.region = carve<int>(p, std::max(n_seeds_in, 1));
+  O.par = carve<float>(p, 6 * no);
+  O.err = carve<float>(p, 21 * no);
+  O.chg = carve<int>(p, no);
+  O.chi2 = carve<float>(p, no);
+  O.score = carve<float>(p, no);
+  O.nfound = carve<int>(p, no);
+  O.ntot = carve<int>(p, no);
+  O.noverlap = carve<int>(p, no);
+  O.ninside = carve<int>(p, no);
+  O.ntail = carve<int>(p, no);
+  O.hit_idx = carve<int>(p, no * kExportHits);
+  O.hit_lyr = carve<int>(p, no * kExportHits);
+  cudaStream_t st = ctx->stream;
+  MKFG_CUDA_TRY(cudaMemsetAsync(O.n_cands, 0, 4 * (size_t)n_seeds_in, st));
+  if (S > 0) k_export<<<(S * kSlots + 127) / 128, 128, 0, st>>>(f->ev, O);
+  MKFG_CUDA_TRY(cudaGetLastError());
+  auto dn = [&](void* h, const void* d, size_t bytes) -> int {
+    if (!h) return MKFG_OK;
+    MKFG_CUDA_TRY(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, st));
+    return MKFG_OK;
+  };
+  const size_t ns = n_seeds_in;
+  if ((rc = dn(out->n_cands, O.n_cands, 4 * ns))) return rc;
+  if ((rc = dn(out->region, O.region, 4 * ns))) return rc;
+  if ((rc = dn(out->par, O.par, 4 * 6 * ns * m))) return rc;
+  if ((rc = dn(out->err, O.err, 4 * 21 * ns * m))) return rc;
+  if ((rc = dn(out->chg, O.chg, 4 * ns * m))) return rc;
+  if ((rc = dn(out->chi2, O.chi2, 4 * ns * m))) return rc;
+  if ((rc = dn(out->score, O.score, 4 * ns * m))) return rc;
+  if ((rc = dn(out->nfound, O.nfound, 4 * ns * m))) return rc;
+  if ((rc = dn(out->ntot, O.ntot, 4 * ns * m))) return rc;
+  if ((rc = dn(out->noverlap, O.noverlap, 4 * ns * m))) return rc;
+  if ((rc = dn(out->ninside, O.ninside, 4 * ns * m))) return rc;
+  if ((rc = dn(out->ntail, O.ntail, 4 * ns * m))) return rc;
+  if ((rc = dn(out->hit_idx, O.hit_idx, 4 * ns * m * kExportHits))) return rc;
+  if ((rc = dn(out->hit_lyr, O.hit_lyr, 4 * ns * m * kExportHits))) return rc;
+  int flags = 0;
+  MKFG_CUDA_TRY(cudaMemcpyAsync(&flags, f->ev.err_flags, 4, cudaMemcpyDeviceToHost, st));
+  MKFG_CUDA_TRY(cudaStreamSynchronize(st));
+  if (flags & kErrArena)
+    return set_error(MKFG_ERR_OVERFLOW, "hit-on-track arena overflow (capacity %d per seed)",
+                     f->ev.hot_cap);
+  return MKFG_OK;
+}
+
+}  // namespace mkfg
+
+extern "C" int mkfg_find_upload(mkfg_context* ctx, const mkfg_event* ev) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  MKFG_REQUIRE(ev != nullptr, "null event");
+  Finder* f = finder_of(ctx);
+  MKFG_REQUIRE(f->configured, "mkfg_finder_setup was not called");
+  return upload_event(ctx, f, ev);
+}
+
+extern "C" int mkfg_find_run(mkfg_context* ctx) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  Finder* f = finder_of(ctx);
+  MKFG_REQUIRE(f->configured && f->events_loaded, "no event uploaded");
+  return run_plain(ctx, f);
+}
+
+extern "C" int mkfg_find_download(mkfg_context* ctx, int n_seeds, mkfg_find_out* out) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  Finder* f = finder_of(ctx);
+  MKFG_REQUIRE(out != nullptr, "null output");
+  MKFG_REQUIRE(f->events_loaded && n_seeds == f->n_seeds, "seed count mismatch");
+  return download(ctx, f, out, n_seeds);
+}
+
+extern "C" int mkfg_find_event(mkfg_context* ctx, const mkfg_event* ev, mkfg_find_out* out) {
+  int rc;
+  if ((rc = mkfg_find_upload(ctx, ev))) return rc;
+  if ((rc = mkfg_find_run(ctx))) return rc;
+  return mkfg_find_download(ctx, ev->n_seeds, out);
+}
+
+extern "C" int mkfg_prepare_event_host(const mkfg_find_config* cfg, const mkfg_event* ev,
+                                       uint32_t* bins, int32_t* n_bins, int32_t* srank,
+                                       int32_t* seed_order, int32_t* seed_region) {
+  MKFG_REQUIRE(cfg && ev && n_bins, "null argument");
+  MKFG_REQUIRE(cfg->n_layers > 0 && cfg->n_layers <= kMaxLayers && ev->n_layers == cfg->n_layers,
+               "layer count mismatch");
+  std::vector<LayerBinning> lb(cfg->n_layers);
+  int off = 0;
+  for (int l = 0; l < cfg->n_layers; ++l) {
+    lb[l] = setup_layer_binning(cfg->layer_desc + (size_t)l * LC_COUNT);
+    lb[l].bin_offset = off;
+    off += lb[l].nq * kPhiBins;
+  }
+  *n_bins = off;
+  if (!bins) return MKFG_OK;
+  const int nh = ev->layer_begin[cfg->n_layers];
+  EventHitsPrep prep;
+  prepare_event_hits(lb, ev->layer_begin, cfg->n_layers, ev->pos, nh, ev->detid, ev->cpcm, prep);
+  std::copy(prep.bins.begin(), prep.bins.end(), bins);
+  if (srank) std::copy(prep.srank.begin(), prep.srank.end(), srank);
+  if (seed_order || seed_region) {
+    SeedInput si{ev->n_seeds, ev->seed_par, ev->seed_chg, ev->seed_nhits, ev->seed_hit_layer,
+                 ev->seed_hit_index};
+    SeedOrder so;
+    partition_seeds_cms2017(cfg->layer_desc, cfg->n_layers, si, ev->layer_begin, ev->pos, nh, so);
+    if (seed_order) std::copy(so.order.begin(), so.order.end(), seed_order);
+    if (seed_region) std::copy(so.region.begin(), so.region.end(), seed_region);
+  }
+  return MKFG_OK;
+}

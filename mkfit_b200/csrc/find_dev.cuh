@@ -1,0 +1,161 @@
+// Device data structures and per-candidate building blocks of the
+// clone-engine combinatorial finder. Used by the plain (one launch per layer
+// step) and the batched persistent forms.
+#pragma once
+
+#include <cstdint>
+
+#include "kalman.cuh"
+
+namespace mkfg {
+
+constexpr int kSlots = 8;               // candidate slots per seed (maxCandsPerSeed <= 8)
+constexpr int kMaxXHits = 16;           // MkFinder::MPlexHitIdxMax
+constexpr int kRecPerCand = kMaxXHits + 1;
+constexpr int kRecPerSeed = kSlots * kRecPerCand;
+constexpr int kMaxLayers = 128;
+constexpr int kMaxPlan = 64;
+constexpr int kMaxRegions = 8;
+constexpr int kExportHits = 64;         // Config::nMaxTrkHits
+constexpr int kRecInvalid = -1000000;
+
+enum SeedState { kDormant = 0, kFinding = 1, kFinished = 2 };
+enum WsrCode { kWsrInside = 0, kWsrEdge = 1, kWsrOutside = 2 };
+enum ErrBits { kErrArena = 1, kErrLayerSize = 2 };
+
+struct LayerDev {
+  float rin, rout, zmin, zmax, propagate_to;
+  float hole_min, hole_max;
+  float min_dphi, max_dphi, min_dq, max_dq;
+  float c_dp_sf, c_dp_0, c_dp_1, c_dp_2;
+  float c_dq_sf, c_dq_0, c_dq_1, c_dq_2;
+  float c_c2_sf, c_c2_0, c_c2_1, c_c2_2;
+  float qmin, fq;
+  int nq, bin_offset;
+  int is_barrel, has_hole, is_pix, pad;
+};
+
+struct FindConfigDev {
+  LayerDev layer[kMaxLayers];
+  int plan[kMaxRegions][kMaxPlan];
+  int plan_len[kMaxRegions];
+  int pickup[kMaxRegions];
+  int n_layers, n_regions, max_steps;
+  int max_cands, max_holes, max_consec_holes;
+  float chi2_cut_min, chi2_cut_overlap, pt_cut_overlap;
+  unsigned inter_pflags, intra_pflags;
+  Material mat;
+};
+
+// Candidate state, structure of arrays over slots (seed * kSlots + c).
+struct CandSoA {
+  float* par;  // [6][cap]
+  float* err;  // [21][cap]
+  int* chg;
+  float* chi2;
+  float* score;
+  int* last;   // arena index of the last hit-on-track node
+  int* nfound;
+  int* nmiss;
+  int* nover;
+  int* ninside;  // TrackCand::nInsideMinusOneHits_
+  int* ntail;    // TrackCand::nTailMinusOneHits_
+  int cap;
+};
+
+// One event (or a batch of events laid out back to back) on the device.
+struct EventDev {
+  // Hits (original order within each layer; global index = layer_begin + i).
+  const float* hpos;
+  const float* herr;
+  int hstride;
+  const uint32_t* hinfo;  // detid (12 bit) | charge per cm << 12
+  const int* layer_begin; // [n_layers + 1] (per event: + event_layer_offset)
+  // Per-layer bins: (first | last << 16) over nq x 256 bins; sorted hits.
+  const uint32_t* bins;
+  const float* sphi;
+  const float* sq;
+  const int* srank;
+  // Seeds in sorted order (index = seed slot s).
+  int n_seeds;
+  int* seed_label;   // input index
+  int* seed_event;   // event of the seed (batched form)
+  int* region;
+  int* pickup_layer;
+  int* state;
+  int* n_cands;
+  int* cur;          // which candidate buffer holds the seed's current candidates
+  int* hot_size;
+  // Candidates: two buffers, kSlots per seed; best short candidate per seed.
+  CandSoA cand[2];
+  CandSoA bshort;
+  int* bshort_valid;
+  // Hit-on-track arena, hot_cap nodes per seed.
+  int* node_hot;   // index (24 bit, signed) | layer << 24 (HitOnTrack layout)
+  float* node_chi2;
+  int* node_prev;
+  int hot_cap;
+  // Step scratch per candidate slot.
+  float* ppar;     // [6][S*kSlots] state propagated to the layer
+  float* perr;     // [21][S*kSlots]
+  int* xsize;      // XHitSize (-1: outside)
+  int* xhit;       // [kMaxXHits][S*kSlots] hit index within layer
+  int* wsr;        // WSR code | extra kind << 8
+  int* extra_last; // arena node of the held-back copy (kind 2)
+  int* upd;        // needs UpdateWithLastHit (per slot of the new buffer)
+  // Records (IdxChi2List) per seed: kRecPerSeed slots.
+  float* rscore;
+  float* rchi2;
+  float* rchi2hit;
+  float* rpt;
+  int* rhit;       // kRecInvalid when the slot holds no record
+  int* rmodule;
+  int* rcounts;    // nhits | ntailholes << 8 | noverlaps << 16 | nholes << 24
+  // (cand slot, hit) pairs for the chi2 pass.
+  int* pairs;
+  int* pair_count; // [max_steps + 1]
+  int* err_flags;
+};
+
+__device__ __forceinline__ int hot_pack(int index, int layer) {
+  return (index & 0xffffff) | (layer << 24);
+}
+__device__ __forceinline__ int hot_index(int v) { return (v << 8) >> 8; }  // sign-extend 24 bit
+__device__ __forceinline__ int hot_layer(int v) { return v >> 24; }
+
+// getScoreCalc (Track.h:648-670).
+__device__ __forceinline__ float score_calc(int nfound, int ntail, int nover, int nmiss, float chi2,
+                                            float pt, bool in_find) {
+  const float maxBonus = 8.0f;
+  float bonus = 0.2f * nfound + 4.0f;
+  float penalty = 8.0f;
+  const float tailPenalty = 3.0f;
+  const float overlapBonus = 0.0f;
+  if (pt < 0.9f) {
+    penalty *= in_find ? 1.7f : 1.5f;
+    bonus = fminf(bonus * (in_find ? 0.9f : 1.0f), maxBonus);
+  }
+  return __fsub_rn(__fsub_rn(__fsub_rn(__fadd_rn(__fmul_rn(bonus, (float)nfound),
+                                                 __fmul_rn(overlapBonus, (float)nover)),
+                                        __fmul_rn(penalty, (float)nmiss)),
+                             __fmul_rn(tailPenalty, (float)ntail)),
+                   chi2);
+}
+
+// getScoreStruct (Track.h:685-697): inFindCandidates = true.
+__device__ __forceinline__ float score_struct(int nhits, int ntail, int nover, int nholes,
+                                              float chi2, float pt) {
+  if (chi2 < 0) chi2 = 0.f;
+  return score_calc(nhits, ntail, nover, nholes, chi2, pt, true);
+}
+
+// std::tan(float) as the host C library rounds it.
+__device__ __forceinline__ float f_tan(float x) {
+#if MKFG_LIBM_EXACT
+  return (float)tan((double)x);
+#else
+  return tanf(x);
+#endif
+}
+
+}  // namespace mkfg

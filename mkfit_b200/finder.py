@@ -1,0 +1,182 @@
+"""Host mirror of the reference's finding interface (MkBuilder /
+MkFinder clone engine) over the C ABI: configuration from the CMS-2017
+geometry, event upload, run and export."""
+import ctypes
+
+import numpy as np
+
+from . import capi
+from .geometry import LAYER_FIELDS, cms2017
+
+vp = ctypes.c_void_p
+
+
+class MkfgFindConfig(ctypes.Structure):
+    _fields_ = [("n_layers", ctypes.c_int32), ("layer_desc", vp), ("n_regions", ctypes.c_int32),
+                ("max_plan", ctypes.c_int32), ("plans", vp), ("plan_len", vp), ("pickup", vp),
+                ("max_cands_per_seed", ctypes.c_int32), ("max_holes_per_cand", ctypes.c_int32),
+                ("max_consec_holes", ctypes.c_int32), ("chi2_cut_min", ctypes.c_float),
+                ("chi2_cut_overlap", ctypes.c_float), ("pt_cut_overlap", ctypes.c_float),
+                ("inter_layer_pflags", ctypes.c_uint32), ("intra_layer_pflags", ctypes.c_uint32),
+                ("requires_prop_to_hit", ctypes.c_int32)]
+
+
+class MkfgEvent(ctypes.Structure):
+    _fields_ = [("n_layers", ctypes.c_int32), ("layer_begin", vp), ("pos", vp), ("err", vp),
+                ("detid", vp), ("cpcm", vp), ("n_seeds", ctypes.c_int32), ("seed_par", vp),
+                ("seed_err", vp), ("seed_chg", vp), ("seed_nhits", vp), ("seed_hit_layer", vp),
+                ("seed_hit_index", vp)]
+
+
+class MkfgFindOut(ctypes.Structure):
+    _fields_ = [(k, vp) for k in ("n_cands", "region", "par", "err", "chg", "chi2", "score",
+                                  "nfound", "ntot", "noverlap", "ninside", "ntail", "hit_idx",
+                                  "hit_lyr")]
+
+
+def _bind(lib):
+    if getattr(lib, "_finder_bound", False):
+        return
+    lib.mkfg_finder_setup.argtypes = [vp, ctypes.POINTER(MkfgFindConfig)]
+    lib.mkfg_find_upload.argtypes = [vp, ctypes.POINTER(MkfgEvent)]
+    lib.mkfg_find_run.argtypes = [vp]
+    lib.mkfg_find_download.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(MkfgFindOut)]
+    lib.mkfg_find_event.argtypes = [vp, ctypes.POINTER(MkfgEvent), ctypes.POINTER(MkfgFindOut)]
+    lib.mkfg_prepare_event_host.argtypes = [ctypes.POINTER(MkfgFindConfig),
+                                            ctypes.POINTER(MkfgEvent), vp,
+                                            ctypes.POINTER(ctypes.c_int32), vp, vp, vp]
+    lib._finder_bound = True
+
+
+class FindConfig:
+    """Iteration-0 CMS-2017 configuration with the workload's overrides:
+    maxCandsPerSeed, chi2Cut_min and (zero_c2) a flat chi2 cut."""
+
+    def __init__(self, geom=None, max_cands=6, chi2_cut=30.0, zero_c2=True):
+        g = geom or cms2017()
+        self.geom = g
+        desc = g.layer_desc.copy()
+        if zero_c2:
+            for k in ("c_c2_0", "c_c2_1", "c_c2_2"):
+                desc[:, LAYER_FIELDS.index(k)] = 0.0
+        self.layer_desc = np.ascontiguousarray(desc, np.float32)
+        self.plans = np.ascontiguousarray(g.plans, np.int32)
+        self.plan_len = np.ascontiguousarray(g.plan_len, np.int32)
+        self.pickup = np.ascontiguousarray(g.pickup, np.int32)
+        ip = g.iter_params
+        self.max_cands = int(max_cands)
+        c = MkfgFindConfig()
+        c.n_layers = g.n_layers
+        c.layer_desc = self.layer_desc.ctypes.data
+        c.n_regions = self.plans.shape[0]
+        c.max_plan = self.plans.shape[1]
+        c.plans = self.plans.ctypes.data
+        c.plan_len = self.plan_len.ctypes.data
+        c.pickup = self.pickup.ctypes.data
+        c.max_cands_per_seed = self.max_cands
+        c.max_holes_per_cand = int(ip[1])
+        c.max_consec_holes = int(ip[2])
+        c.chi2_cut_min = float(chi2_cut)
+        c.chi2_cut_overlap = float(ip[4])
+        c.pt_cut_overlap = float(ip[5])
+        c.inter_layer_pflags = int(g.flags[1])
+        c.intra_layer_pflags = int(g.flags[2])
+        c.requires_prop_to_hit = int(g.flags[0])
+        self.c = c
+
+
+def event_struct(ev):
+    """ctypes view of a synth.CmsEvent (keeps references to the arrays)."""
+    keep = {}
+
+    def p(name, arr, dt):
+        a = np.ascontiguousarray(arr, dt)
+        keep[name] = a
+        return a.ctypes.data
+
+    e = MkfgEvent()
+    e.n_layers = ev.n_layers
+    e.layer_begin = p("lb", ev.layer_begin, np.int32)
+    e.pos = p("pos", ev.hit_pos, np.float32)
+    e.err = p("err", ev.hit_err, np.float32)
+    e.detid = p("det", ev.hit_detid, np.int32)
+    e.cpcm = p("cpcm", ev.hit_cpcm, np.int32)
+    e.n_seeds = ev.n_seeds
+    e.seed_par = p("spar", ev.seed_par, np.float32)
+    e.seed_err = p("serr", ev.seed_err, np.float32)
+    e.seed_chg = p("schg", ev.seed_chg, np.int32)
+    e.seed_nhits = p("snh", ev.seed_nhits, np.int32)
+    e.seed_hit_layer = p("shl", ev.seed_hit_layer, np.int32)
+    e.seed_hit_index = p("shi", ev.seed_hit_index, np.int32)
+    e._keep = keep
+    return e
+
+
+def output_arrays(n_seeds, m):
+    no = n_seeds * m
+    return dict(n_cands=np.zeros(n_seeds, np.int32), region=np.zeros(n_seeds, np.int32),
+                par=np.zeros((no, 6), np.float32), err=np.zeros((no, 21), np.float32),
+                chg=np.zeros(no, np.int32), chi2=np.zeros(no, np.float32),
+                score=np.zeros(no, np.float32), nfound=np.zeros(no, np.int32),
+                ntot=np.zeros(no, np.int32), noverlap=np.zeros(no, np.int32),
+                ninside=np.zeros(no, np.int32), ntail=np.zeros(no, np.int32),
+                hit_idx=np.zeros((no, 64), np.int32), hit_lyr=np.zeros((no, 64), np.int32))
+
+
+def out_struct(o):
+    s = MkfgFindOut()
+    for k, _ in MkfgFindOut._fields_:
+        setattr(s, k, o[k].ctypes.data if o.get(k) is not None else None)
+    return s
+
+
+class Finder:
+    """Clone-engine finding on one context (plain form)."""
+
+    def __init__(self, ctx, cfg=None):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        _bind(self.lib)
+        self.cfg = cfg or FindConfig()
+        g = self.cfg.geom
+        ctx.set_material(g.rl, g.xi)
+        capi.check(self.lib.mkfg_finder_setup(ctx.handle, ctypes.byref(self.cfg.c)))
+
+    def upload(self, ev):
+        self._ev = event_struct(ev)
+        capi.check(self.lib.mkfg_find_upload(self.ctx.handle, ctypes.byref(self._ev)))
+
+    def run(self):
+        capi.check(self.lib.mkfg_find_run(self.ctx.handle))
+
+    def download(self, n_seeds):
+        o = output_arrays(n_seeds, self.cfg.max_cands)
+        capi.check(self.lib.mkfg_find_download(self.ctx.handle, n_seeds,
+                                               ctypes.byref(out_struct(o))))
+        return o
+
+    def find_event(self, ev):
+        e = event_struct(ev)
+        o = output_arrays(ev.n_seeds, self.cfg.max_cands)
+        capi.check(self.lib.mkfg_find_event(self.ctx.handle, ctypes.byref(e),
+                                            ctypes.byref(out_struct(o))))
+        return o
+
+
+def prepare_event_host(ev, cfg=None):
+    """Host-side hit index + seed order of the library (no GPU needed)."""
+    lib = capi.load()
+    _bind(lib)
+    cfg = cfg or FindConfig()
+    e = event_struct(ev)
+    nb = ctypes.c_int32(0)
+    capi.check(lib.mkfg_prepare_event_host(ctypes.byref(cfg.c), ctypes.byref(e), None,
+                                           ctypes.byref(nb), None, None, None))
+    bins = np.zeros(nb.value, np.uint32)
+    srank = np.zeros(ev.n_hits, np.int32)
+    order = np.zeros(ev.n_seeds, np.int32)
+    region = np.zeros(ev.n_seeds, np.int32)
+    capi.check(lib.mkfg_prepare_event_host(ctypes.byref(cfg.c), ctypes.byref(e),
+                                           bins.ctypes.data, ctypes.byref(nb), srank.ctypes.data,
+                                           order.ctypes.data, region.ctypes.data))
+    return dict(bins=bins, srank=srank, seed_order=order, seed_region=region)

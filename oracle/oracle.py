@@ -196,3 +196,31 @@ def ref_find(reflib, ev, max_cands=6, chi2_cut=30.0, zero_c2=True, repeat=1):
         raise RuntimeError(f"ref_find failed rc={rc}")
     o["seconds"] = secs.value
     return o
+
+
+def ref_event_prep(reflib, ev):
+    """The reference's hit index bins / sorted ranks and seed order for an
+    event (oracle/ref_driver.cc ref_event_prep)."""
+    lib = reflib.lib
+    lib.ref_event_prep.restype = ctypes.c_int
+    lib.ref_event_prep.argtypes = [ctypes.c_int, _i32p, _f32p, _f32p, _i32p, _i32p, ctypes.c_int,
+                                   _f32p, _f32p, _i32p, _i32p, _i32p, _i32p, ctypes.c_void_p,
+                                   ctypes.POINTER(ctypes.c_int), ctypes.c_void_p, ctypes.c_void_p,
+                                   ctypes.c_void_p]
+    c = lambda a, t: np.ascontiguousarray(a, t)
+    args = [ev.n_layers, c(ev.layer_begin, np.int32), c(ev.hit_pos, np.float32),
+            c(ev.hit_err, np.float32), c(ev.hit_detid, np.int32), c(ev.hit_cpcm, np.int32),
+            ev.n_seeds, c(ev.seed_par, np.float32), c(ev.seed_err, np.float32),
+            c(ev.seed_chg, np.int32), c(ev.seed_nhits, np.int32), c(ev.seed_hit_layer, np.int32),
+            c(ev.seed_hit_index, np.int32)]
+    nb = ctypes.c_int(0)
+    lib.ref_event_prep(*args, None, ctypes.byref(nb), None, None, None)
+    bins = np.zeros(nb.value, np.uint32)
+    srank = np.zeros(ev.n_hits, np.int32)
+    order = np.zeros(ev.n_seeds, np.int32)
+    region = np.zeros(ev.n_seeds, np.int32)
+    rc = lib.ref_event_prep(*args, bins.ctypes.data, ctypes.byref(nb), srank.ctypes.data,
+                            order.ctypes.data, region.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"ref_event_prep failed rc={rc}")
+    return dict(bins=bins, srank=srank, seed_order=order, seed_region=region)

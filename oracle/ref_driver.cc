@@ -385,3 +385,70 @@ int ref_find(int n_layers_in, const int* layer_begin, const float* hpos, const f
 }
 
 }  // extern "C"
+
+extern "C" {
+
+// The reference's own hit index (LayerOfHits::SuckInHits) and seed order
+// (MkBuilder::import_seeds) for one event, in the layout of
+// mkfg_prepare_event_host: bins per layer (first | last << 16) over
+// nq x 256, sorted-position -> index-within-layer, seed order and regions.
+int ref_event_prep(int n_layers_in, const int* layer_begin, const float* hpos, const float* herr,
+                   const int* detid, const int* cpcm, int ns, const float* spar,
+                   const float* serr, const int* schg, const int* seed_nhits,
+                   const int* seed_hit_layer, const int* seed_hit_index, unsigned* bins,
+                   int* n_bins, int* srank, int* seed_order, int* seed_region) {
+  ensure_cms2017();
+  const int n_layers = (int)Config::TrkInfo.m_layers.size();
+  if (n_layers_in != n_layers) return -1;
+  const int nh_tot = layer_begin[n_layers];
+  std::vector<HitVec> layer_hits(n_layers);
+  for (int l = 0; l < n_layers; ++l)
+    for (int h = layer_begin[l]; h < layer_begin[l + 1]; ++h) {
+      Hit hit = make_hit(h, nh_tot, hpos, herr);
+      if (cpcm[h] < 0) hit.setupAsPixel(detid[h], 1, 1);
+      else hit.setupAsStrip(detid[h], cpcm[h], 1);
+      layer_hits[l].push_back(hit);
+    }
+  EventOfHits eoh(Config::TrkInfo);
+  for (int l = 0; l < n_layers; ++l) eoh.SuckInHits(l, layer_hits[l]);
+  int off = 0;
+  for (int l = 0; l < n_layers; ++l) {
+    const LayerOfHits& L = eoh[l];
+    if (bins)
+      for (int q = 0; q < L.m_nq; ++q)
+        for (int p = 0; p < Config::m_nphi; ++p) {
+          auto b = L.m_phi_bin_infos[q][p];
+          bins[off + q * Config::m_nphi + p] = unsigned(b.first) | (unsigned(b.second) << 16);
+        }
+    off += L.m_nq * Config::m_nphi;
+    if (srank)
+      for (int i = 0; i < layer_begin[l + 1] - layer_begin[l]; ++i)
+        srank[layer_begin[l] + i] = L.GetOriginalHitIndex(i);
+  }
+  *n_bins = off;
+  if (!seed_order) return 0;
+
+  TrackVec seeds;
+  for (int s = 0; s < ns; ++s) {
+    Track t = make_track(s, ns, spar, serr, schg);
+    t.setLabel(s);
+    for (int k = 0; k < seed_nhits[s]; ++k)
+      t.addHitIdx(seed_hit_index[s * 4 + k], seed_hit_layer[s * 4 + k], 0.f);
+    seeds.push_back(t);
+  }
+  IterationConfig itconf = Config::ItrInfo[0];
+  MkJob job({Config::TrkInfo, itconf, eoh, nullptr});
+  RefBuilder builder;
+  builder.begin_event(&job, nullptr, "ref_event_prep");
+  builder.find_tracks_load_seeds(seeds);
+  EventOfCombCandidates& eocc = builder.eocc();
+  for (int i = 0; i < eocc.m_size; ++i) {
+    const TrackCand& tc = eocc[i].front();
+    seed_order[i] = tc.label();
+    seed_region[tc.label()] = tc.getEtaRegion();
+  }
+  builder.end_event();
+  return 0;
+}
+
+}  // extern "C"
