@@ -205,6 +205,12 @@ typedef struct {
  * partition as import_seeds), run (one launch sequence per layer step),
  * download (export of all candidates, as TrackCand::exportTrack). */
 int mkfg_find_upload(mkfg_context* ctx, const mkfg_event* ev);
+/* Batched form: n_events events uploaded together and found by the same
+ * launches (or graph replay); mkfg_find_download then returns the seeds of
+ * all events concatenated in event order (n_seeds = the total). No
+ * reference counterpart: the reference runs events in separate threads
+ * (mkFit/mkFit.cc:308-425). */
+int mkfg_find_upload_batch(mkfg_context* ctx, const mkfg_event* evs, int32_t n_events);
 int mkfg_find_run(mkfg_context* ctx);
 int mkfg_find_download(mkfg_context* ctx, int32_t n_seeds, mkfg_find_out* out);
 int mkfg_find_event(mkfg_context* ctx, const mkfg_event* ev, mkfg_find_out* out);

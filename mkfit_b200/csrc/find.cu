@@ -17,8 +17,10 @@
 #include "find_steps.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 namespace mkfg {
@@ -87,10 +89,11 @@ __global__ void __launch_bounds__(kBlock) k_prep(EventDev E, const FindConfigDev
       propagate_to_r(par, err, chg, L.propagate_to, C.inter_pflags, C.mat, false, ppar, perr);
     else
       propagate_to_z(par, err, chg, L.propagate_to, C.inter_pflags, C.mat, false, ppar, perr);
-    const int ev_base = 0;
-    const int hit_base = E.layer_begin[ev_base + layer];
+    const int ev = E.seed_event[s];
+    const int hit_base = E.layer_begin[ev * E.lb_stride + layer];
     const int stride = E.cand[0].cap;
-    xs = select_hits(E, L, layer, hit_base, ppar, perr, E.xhit + slot, stride, wsr);
+    xs = select_hits(E, L, E.bins + (size_t)ev * E.n_bins, hit_base, ppar, perr, E.xhit + slot,
+                     stride, wsr);
     // find_tracks_handle_missed_layers (mkFit/MkBuilder.cc:1568-1637).
     const float cand_r = hypot_f(ppar[0], ppar[1]);
     if (L.is_barrel && cand_r < L.rin) {
@@ -163,7 +166,7 @@ __global__ void __launch_bounds__(kBlock) k_chi2(EventDev E, const FindConfigDev
     const CandSoA& B = E.cand[E.cur[s]];
     const int chg = B.chg[slot];
     const int hidx = E.xhit[h * stride + slot];
-    const int g = E.layer_begin[layer] + hidx;
+    const int g = E.layer_begin[E.seed_event[s] * E.lb_stride + layer] + hidx;
     float mpos[3], merr[6];
 #pragma unroll
     for (int e = 0; e < 3; ++e) mpos[e] = __ldg(E.hpos + e * E.hstride + g);
@@ -530,7 +533,7 @@ __global__ void __launch_bounds__(kBlock) k_update(EventDev E, const FindConfigD
   // After an arena overflow (reported through err_flags) the last node may
   // not be a hit: skip rather than read outside the hit arrays.
   if (hot_index(hv) < 0 || hl < 0 || hl >= C.n_layers) return;
-  const int g = E.layer_begin[hl] + hot_index(hv);
+  const int g = E.layer_begin[E.seed_event[s] * E.lb_stride + hl] + hot_index(hv);
   float mpos[3], merr[6];
 #pragma unroll
   for (int e = 0; e < 3; ++e) mpos[e] = __ldg(E.hpos + e * E.hstride + g);
@@ -700,6 +703,7 @@ struct Finder {
   DevBuf hits, seeds, cands, scratch, recs, arena, outb;
   EventDev ev{};
   int n_seeds = 0;
+  int n_events = 0;
   int events_loaded = 0;
 };
 
@@ -822,71 +826,118 @@ extern "C" int mkfg_finder_setup(mkfg_context* ctx, const mkfg_find_config* cfg)
 
 namespace mkfg {
 
-// Host preparation + upload of one event into the finder's device buffers.
-static int upload_event(mkfg_context* ctx, Finder* f, const mkfg_event* ev) {
+// Host preparation + upload of a batch of events (one event for the plain
+// drop-in form) into the finder's device buffers. Hits and seeds of all
+// events are laid out back to back; every seed knows its event.
+static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int n_ev) {
   const int L = f->host_cfg.n_layers;
-  MKFG_REQUIRE(ev->n_layers == L, "event has %d layers, configuration %d", ev->n_layers, L);
-  const int nh = ev->layer_begin[L];
-  for (int l = 0; l < L; ++l)
-    MKFG_REQUIRE(ev->layer_begin[l + 1] - ev->layer_begin[l] <= 65535,
-                 "layer %d holds more than 65535 hits", l);
-  const int S = ev->n_seeds;
-  for (int s = 0; s < S; ++s)
-    MKFG_REQUIRE(ev->seed_nhits[s] >= 1 && ev->seed_nhits[s] <= 4, "seed %d hit count", s);
+  MKFG_REQUIRE(n_ev >= 1, "empty batch");
+  std::vector<int> hit_off(n_ev + 1, 0), seed_off(n_ev + 1, 0);
+  for (int e = 0; e < n_ev; ++e) {
+    const mkfg_event* ev = evs + e;
+    MKFG_REQUIRE(ev->n_layers == L, "event %d has %d layers, configuration %d", e, ev->n_layers, L);
+    for (int l = 0; l < L; ++l)
+      MKFG_REQUIRE(ev->layer_begin[l + 1] - ev->layer_begin[l] <= 65535,
+                   "event %d layer %d holds more than 65535 hits", e, l);
+    for (int s = 0; s < ev->n_seeds; ++s)
+      MKFG_REQUIRE(ev->seed_nhits[s] >= 1 && ev->seed_nhits[s] <= 4, "seed %d hit count", s);
+    hit_off[e + 1] = hit_off[e] + ev->layer_begin[L];
+    seed_off[e + 1] = seed_off[e] + ev->n_seeds;
+  }
+  const int NH = hit_off[n_ev], S = seed_off[n_ev];
+  const int nb = f->n_bins;
 
-  // Hits: bins and sorted arrays.
-  EventHitsPrep prep;
-  prepare_event_hits(f->binning, ev->layer_begin, L, ev->pos, nh, ev->detid, ev->cpcm, prep);
-  // Seed partition and order.
-  SeedInput si{S, ev->seed_par, ev->seed_chg, ev->seed_nhits, ev->seed_hit_layer, ev->seed_hit_index};
-  SeedOrder so;
-  partition_seeds_cms2017(f->layer_desc.data(), L, si, ev->layer_begin, ev->pos, nh, so);
+  // Per-event host preparation (hit index, seed order), in parallel.
+  std::vector<EventHitsPrep> preps(n_ev);
+  std::vector<SeedOrder> orders(n_ev);
+  {
+    auto work = [&](int e) {
+      const mkfg_event* ev = evs + e;
+      const int nh = ev->layer_begin[L];
+      prepare_event_hits(f->binning, ev->layer_begin, L, ev->pos, nh, ev->detid, ev->cpcm, preps[e]);
+      SeedInput si{ev->n_seeds, ev->seed_par, ev->seed_chg, ev->seed_nhits, ev->seed_hit_layer,
+                   ev->seed_hit_index};
+      partition_seeds_cms2017(f->layer_desc.data(), L, si, ev->layer_begin, ev->pos, nh, orders[e]);
+    };
+    const int nthr = std::max(1, std::min(n_ev, (int)std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    std::atomic<int> next(0);
+    for (int t = 0; t < nthr; ++t)
+      pool.emplace_back([&] {
+        for (int e = next++; e < n_ev; e = next++) work(e);
+      });
+    for (auto& th : pool) th.join();
+  }
+
+  // Host staging of the concatenated arrays.
+  const int NHs = std::max(NH, 1);
+  std::vector<float> h_pos(3 * (size_t)NHs), h_err(6 * (size_t)NHs), h_sphi(NHs), h_sq(NHs);
+  std::vector<uint32_t> h_info(NHs), h_bins((size_t)nb * n_ev);
+  std::vector<int> h_srank(NHs), h_lb((size_t)(L + 1) * n_ev);
+  for (int e = 0; e < n_ev; ++e) {
+    const mkfg_event* ev = evs + e;
+    const int nh = ev->layer_begin[L], o = hit_off[e];
+    for (int r = 0; r < 3; ++r)
+      std::memcpy(&h_pos[(size_t)r * NHs + o], ev->pos + (size_t)r * nh, 4 * (size_t)nh);
+    for (int r = 0; r < 6; ++r)
+      std::memcpy(&h_err[(size_t)r * NHs + o], ev->err + (size_t)r * nh, 4 * (size_t)nh);
+    std::copy(preps[e].sphi.begin(), preps[e].sphi.end(), h_sphi.begin() + o);
+    std::copy(preps[e].sq.begin(), preps[e].sq.end(), h_sq.begin() + o);
+    std::copy(preps[e].srank.begin(), preps[e].srank.end(), h_srank.begin() + o);
+    std::copy(preps[e].hinfo.begin(), preps[e].hinfo.end(), h_info.begin() + o);
+    std::copy(preps[e].bins.begin(), preps[e].bins.end(), h_bins.begin() + (size_t)e * nb);
+    for (int l = 0; l <= L; ++l) h_lb[(size_t)e * (L + 1) + l] = o + ev->layer_begin[l];
+  }
 
   cudaStream_t st = ctx->stream;
   int rc;
+  auto up = [&](void* d, const void* h, size_t bytes) -> int {
+    if (bytes == 0) return MKFG_OK;
+    MKFG_CUDA_TRY(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st));
+    return MKFG_OK;
+  };
   // ---- hits
   {
-    const size_t need = rounded(sizeof(float) * 9 * std::max(nh, 1)) + rounded(4 * std::max(nh, 1)) +
-                        rounded(4 * (L + 1)) + rounded(4 * std::max(f->n_bins, 1)) +
-                        3 * rounded(4 * std::max(nh, 1));
+    const size_t need = rounded(12 * (size_t)NHs) + rounded(24 * (size_t)NHs) + 4 * rounded(4 * (size_t)NHs) +
+                        rounded(4 * h_lb.size()) + rounded(4 * h_bins.size()) + 4096;
     if ((rc = f->hits.ensure(need))) return rc;
     char* p = f->hits.as<char>();
-    float* d_pos = carve<float>(p, 3 * (size_t)std::max(nh, 1));
-    float* d_err = carve<float>(p, 6 * (size_t)std::max(nh, 1));
-    uint32_t* d_info = carve<uint32_t>(p, std::max(nh, 1));
-    int* d_lb = carve<int>(p, L + 1);
-    uint32_t* d_bins = carve<uint32_t>(p, std::max(f->n_bins, 1));
-    float* d_sphi = carve<float>(p, std::max(nh, 1));
-    float* d_sq = carve<float>(p, std::max(nh, 1));
-    int* d_srank = carve<int>(p, std::max(nh, 1));
-    if (nh > 0) {
-      MKFG_CUDA_TRY(cudaMemcpyAsync(d_pos, ev->pos, 12 * (size_t)nh, cudaMemcpyHostToDevice, st));
-      MKFG_CUDA_TRY(cudaMemcpyAsync(d_err, ev->err, 24 * (size_t)nh, cudaMemcpyHostToDevice, st));
-      MKFG_CUDA_TRY(cudaMemcpyAsync(d_info, prep.hinfo.data(), 4 * (size_t)nh, cudaMemcpyHostToDevice, st));
-      MKFG_CUDA_TRY(cudaMemcpyAsync(d_sphi, prep.sphi.data(), 4 * (size_t)nh, cudaMemcpyHostToDevice, st));
-      MKFG_CUDA_TRY(cudaMemcpyAsync(d_sq, prep.sq.data(), 4 * (size_t)nh, cudaMemcpyHostToDevice, st));
-      MKFG_CUDA_TRY(cudaMemcpyAsync(d_srank, prep.srank.data(), 4 * (size_t)nh, cudaMemcpyHostToDevice, st));
-    }
-    MKFG_CUDA_TRY(cudaMemcpyAsync(d_lb, ev->layer_begin, 4 * (size_t)(L + 1), cudaMemcpyHostToDevice, st));
-    MKFG_CUDA_TRY(cudaMemcpyAsync(d_bins, prep.bins.data(), 4 * (size_t)f->n_bins, cudaMemcpyHostToDevice, st));
+    float* d_pos = carve<float>(p, 3 * (size_t)NHs);
+    float* d_err = carve<float>(p, 6 * (size_t)NHs);
+    uint32_t* d_info = carve<uint32_t>(p, NHs);
+    int* d_lb = carve<int>(p, h_lb.size());
+    uint32_t* d_bins = carve<uint32_t>(p, h_bins.size());
+    float* d_sphi = carve<float>(p, NHs);
+    float* d_sq = carve<float>(p, NHs);
+    int* d_srank = carve<int>(p, NHs);
+    if ((rc = up(d_pos, h_pos.data(), 4 * h_pos.size()))) return rc;
+    if ((rc = up(d_err, h_err.data(), 4 * h_err.size()))) return rc;
+    if ((rc = up(d_info, h_info.data(), 4 * h_info.size()))) return rc;
+    if ((rc = up(d_lb, h_lb.data(), 4 * h_lb.size()))) return rc;
+    if ((rc = up(d_bins, h_bins.data(), 4 * h_bins.size()))) return rc;
+    if ((rc = up(d_sphi, h_sphi.data(), 4 * h_sphi.size()))) return rc;
+    if ((rc = up(d_sq, h_sq.data(), 4 * h_sq.size()))) return rc;
+    if ((rc = up(d_srank, h_srank.data(), 4 * h_srank.size()))) return rc;
     f->ev.hpos = d_pos;
     f->ev.herr = d_err;
-    f->ev.hstride = std::max(nh, 1);
+    f->ev.hstride = NHs;
     f->ev.hinfo = d_info;
     f->ev.layer_begin = d_lb;
+    f->ev.lb_stride = L + 1;
+    f->ev.n_bins = nb;
     f->ev.bins = d_bins;
     f->ev.sphi = d_sphi;
     f->ev.sq = d_sq;
     f->ev.srank = d_srank;
   }
-  // ---- seeds and candidates
-  const int SC = std::max(S, 1) * kSlots;
+  // ---- seeds, candidates, scratch, records, arena
+  const int SS = std::max(S, 1);
+  const int SC = SS * kSlots;
   const int max_steps = f->host_cfg.max_steps;
   const int M = f->host_cfg.max_cands;
   const int hot_cap = ((8 + max_steps * (2 * M + 3)) + 31) / 32 * 32;
   {
-    const size_t per_buf = rounded(4 * (size_t)SC) * 37;
-    const size_t need = 2 * per_buf + rounded(4 * (size_t)std::max(S, 1)) * 37 + rounded(4 * (size_t)std::max(S, 1)) * 9;
+    const size_t need = 2 * rounded(4 * (size_t)SC) * 37 + rounded(4 * (size_t)SS) * 46 + 4096;
     if ((rc = f->cands.ensure(need))) return rc;
     char* p = f->cands.as<char>();
     auto mk = [&](int cap) {
@@ -907,8 +958,7 @@ static int upload_event(mkfg_context* ctx, Finder* f, const mkfg_event* ev) {
     };
     f->ev.cand[0] = mk(SC);
     f->ev.cand[1] = mk(SC);
-    f->ev.bshort = mk(std::max(S, 1));
-    const int SS = std::max(S, 1);
+    f->ev.bshort = mk(SS);
     f->ev.seed_label = carve<int>(p, SS);
     f->ev.seed_event = carve<int>(p, SS);
     f->ev.region = carve<int>(p, SS);
@@ -920,8 +970,8 @@ static int upload_event(mkfg_context* ctx, Finder* f, const mkfg_event* ev) {
     f->ev.bshort_valid = carve<int>(p, SS);
   }
   {
-    const size_t need = rounded(4 * (size_t)SC) * (27 + kMaxXHits + 4) + rounded(4 * (size_t)SC * kMaxXHits) +
-                        rounded(4 * (size_t)(max_steps + 2)) + rounded(64);
+    const size_t need = rounded(4 * (size_t)SC) * (27 + 5) + 2 * rounded(4 * (size_t)SC * kMaxXHits) +
+                        rounded(4 * (size_t)(max_steps + 2)) + rounded(64) + 4096;
     if ((rc = f->scratch.ensure(need))) return rc;
     char* p = f->scratch.as<char>();
     f->ev.ppar = carve<float>(p, 6 * (size_t)SC);
@@ -936,8 +986,8 @@ static int upload_event(mkfg_context* ctx, Finder* f, const mkfg_event* ev) {
     f->ev.err_flags = carve<int>(p, 16);
   }
   {
-    const size_t nrec = (size_t)std::max(S, 1) * kRecPerSeed;
-    if ((rc = f->recs.ensure(rounded(4 * nrec) * 7))) return rc;
+    const size_t nrec = (size_t)SS * kRecPerSeed;
+    if ((rc = f->recs.ensure(rounded(4 * nrec) * 7 + 4096))) return rc;
     char* p = f->recs.as<char>();
     f->ev.rscore = carve<float>(p, nrec);
     f->ev.rchi2 = carve<float>(p, nrec);
@@ -948,8 +998,8 @@ static int upload_event(mkfg_context* ctx, Finder* f, const mkfg_event* ev) {
     f->ev.rcounts = carve<int>(p, nrec);
   }
   {
-    const size_t nn = (size_t)std::max(S, 1) * hot_cap;
-    if ((rc = f->arena.ensure(rounded(4 * nn) * 3))) return rc;
+    const size_t nn = (size_t)SS * hot_cap;
+    if ((rc = f->arena.ensure(rounded(4 * nn) * 3 + 4096))) return rc;
     char* p = f->arena.as<char>();
     f->ev.node_hot = carve<int>(p, nn);
     f->ev.node_chi2 = carve<float>(p, nn);
@@ -958,78 +1008,73 @@ static int upload_event(mkfg_context* ctx, Finder* f, const mkfg_event* ev) {
   }
   f->ev.n_seeds = S;
 
-  // Initial candidates: the seeds in sorted order (CombCandidate::ImportSeed,
-  // mkFit/HitStructures.cc:483-509). Built on the host, uploaded once.
-  std::vector<float> par(6 * (size_t)SC, 0.f), err(21 * (size_t)SC, 0.f), fz(SC, 0.f);
-  std::vector<int> chg(SC, 0), last(SC, 0), nfound(SC, 0), nmiss(SC, 0), zi(SC, 0);
-  std::vector<float> chi2(SC, 0.f), score(SC, 0.f);
-  std::vector<int> label(std::max(S, 1)), region(std::max(S, 1)), pickup(std::max(S, 1)),
-      state(std::max(S, 1), kDormant), ncand(std::max(S, 1), 1), cur(std::max(S, 1), 0),
-      hot_size(std::max(S, 1)), zero(std::max(S, 1), 0);
-  std::vector<int> node_hot((size_t)std::max(S, 1) * hot_cap, 0), node_prev((size_t)std::max(S, 1) * hot_cap, -1);
-  std::vector<float> node_chi2((size_t)std::max(S, 1) * hot_cap, 0.f);
-  for (int s = 0; s < S; ++s) {
-    const int i = so.order[s];
-    label[s] = i;
-    region[s] = so.region[i];
-    const int nhs = ev->seed_nhits[i];
-    pickup[s] = ev->seed_hit_layer[i * 4 + nhs - 1];
-    const int slot = s * kSlots;
-    for (int e = 0; e < 6; ++e) par[e * SC + slot] = ev->seed_par[e * S + i];
-    for (int e = 0; e < 21; ++e) err[e * SC + slot] = ev->seed_err[e * S + i];
-    chg[slot] = ev->seed_chg[i];
-    int nf = 0, nm = 0, nin = 0, ntl = 0;
-    int prev = -1;
-    for (int k = 0; k < nhs; ++k) {
-      const int hi = ev->seed_hit_index[i * 4 + k], hl = ev->seed_hit_layer[i * 4 + k];
-      node_hot[(size_t)s * hot_cap + k] = (hi & 0xffffff) | (hl << 24);
-      node_prev[(size_t)s * hot_cap + k] = prev;
-      prev = k;
-      if (hi >= 0 || hi == -9) {
-        ++nf;
-        nin += ntl;
-        ntl = 0;
-      } else {
-        ++nm;
-        if (hi == -1) ++ntl;
+  // Initial candidates: each event's seeds in sorted order
+  // (CombCandidate::ImportSeed, mkFit/HitStructures.cc:483-509).
+  std::vector<float> par(6 * (size_t)SC, 0.f), err(21 * (size_t)SC, 0.f), score(SC, 0.f);
+  std::vector<int> chg(SC, 0), last(SC, 0), nfound(SC, 0), nmiss(SC, 0), ninside(SC, 0), ntail(SC, 0);
+  std::vector<int> label(SS, 0), sev(SS, 0), region(SS, 0), pickup(SS, 0), state(SS, kDormant),
+      ncand(SS, 1), cur(SS, 0), hot_size(SS, 0);
+  std::vector<int> node_hot((size_t)SS * hot_cap, 0), node_prev((size_t)SS * hot_cap, -1);
+  for (int e = 0; e < n_ev; ++e) {
+    const mkfg_event* ev = evs + e;
+    const int n = ev->n_seeds;
+    for (int k = 0; k < n; ++k) {
+      const int s = seed_off[e] + k;
+      const int i = orders[e].order[k];
+      label[s] = seed_off[e] + i;
+      sev[s] = e;
+      region[s] = orders[e].region[i];
+      const int nhs = ev->seed_nhits[i];
+      pickup[s] = ev->seed_hit_layer[i * 4 + nhs - 1];
+      const int slot = s * kSlots;
+      for (int c = 0; c < 6; ++c) par[c * (size_t)SC + slot] = ev->seed_par[c * n + i];
+      for (int c = 0; c < 21; ++c) err[c * (size_t)SC + slot] = ev->seed_err[c * n + i];
+      chg[slot] = ev->seed_chg[i];
+      int nf = 0, nm = 0, nin = 0, ntl = 0, prev = -1;
+      for (int h = 0; h < nhs; ++h) {
+        const int hi = ev->seed_hit_index[i * 4 + h], hl = ev->seed_hit_layer[i * 4 + h];
+        node_hot[(size_t)s * hot_cap + h] = (hi & 0xffffff) | (hl << 24);
+        node_prev[(size_t)s * hot_cap + h] = prev;
+        prev = h;
+        if (hi >= 0 || hi == -9) {
+          ++nf;
+          nin += ntl;
+          ntl = 0;
+        } else {
+          ++nm;
+          if (hi == -1) ++ntl;
+        }
       }
-    }
-    hot_size[s] = nhs;
-    last[slot] = nhs - 1;
-    nfound[slot] = nf;
-    nmiss[slot] = nm;
-    const float pt = std::abs(1.f / par[3 * SC + slot]);
-    // getScoreCand(cand) with default arguments (Track.h / HitStructures.h:519-531).
-    {
-      const float maxBonus = 8.0f;
-      float bonus = 0.2f * nf + 4.0f;
-      float penalty = 8.0f;
+      hot_size[s] = nhs;
+      last[slot] = nhs - 1;
+      nfound[slot] = nf;
+      nmiss[slot] = nm;
+      ninside[slot] = nin;
+      ntail[slot] = ntl;
+      // getScoreCand(cand) with default arguments (mkFit/HitStructures.h:519-531).
+      const float pt = std::abs(1.f / par[3 * (size_t)SC + slot]);
+      float bonus = 0.2f * nf + 4.0f, penalty = 8.0f;
       if (pt < 0.9f) {
         penalty *= 1.5f;
-        bonus = std::min(bonus * 1.0f, maxBonus);
+        bonus = std::min(bonus * 1.0f, 8.0f);
       }
       score[slot] = bonus * nf + 0.0f * 0 - penalty * nin - 3.0f * 0 - 0.0f;
     }
   }
-  auto up = [&](void* d, const void* h, size_t bytes) -> int {
-    MKFG_CUDA_TRY(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st));
-    return MKFG_OK;
-  };
   CandSoA& B0 = f->ev.cand[0];
-  const int SS = std::max(S, 1);
   if ((rc = up(B0.par, par.data(), 4 * par.size()))) return rc;
   if ((rc = up(B0.err, err.data(), 4 * err.size()))) return rc;
   if ((rc = up(B0.chg, chg.data(), 4 * (size_t)SC))) return rc;
-  if ((rc = up(B0.chi2, chi2.data(), 4 * (size_t)SC))) return rc;
+  MKFG_CUDA_TRY(cudaMemsetAsync(B0.chi2, 0, 4 * (size_t)SC, st));
   if ((rc = up(B0.score, score.data(), 4 * (size_t)SC))) return rc;
   if ((rc = up(B0.last, last.data(), 4 * (size_t)SC))) return rc;
   if ((rc = up(B0.nfound, nfound.data(), 4 * (size_t)SC))) return rc;
   if ((rc = up(B0.nmiss, nmiss.data(), 4 * (size_t)SC))) return rc;
   MKFG_CUDA_TRY(cudaMemsetAsync(B0.nover, 0, 4 * (size_t)SC, st));
-  MKFG_CUDA_TRY(cudaMemsetAsync(B0.ninside, 0, 4 * (size_t)SC, st));
-  MKFG_CUDA_TRY(cudaMemsetAsync(B0.ntail, 0, 4 * (size_t)SC, st));
+  if ((rc = up(B0.ninside, ninside.data(), 4 * (size_t)SC))) return rc;
+  if ((rc = up(B0.ntail, ntail.data(), 4 * (size_t)SC))) return rc;
   if ((rc = up(f->ev.seed_label, label.data(), 4 * (size_t)SS))) return rc;
-  MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.seed_event, 0, 4 * (size_t)SS, st));
+  if ((rc = up(f->ev.seed_event, sev.data(), 4 * (size_t)SS))) return rc;
   if ((rc = up(f->ev.region, region.data(), 4 * (size_t)SS))) return rc;
   if ((rc = up(f->ev.pickup_layer, pickup.data(), 4 * (size_t)SS))) return rc;
   if ((rc = up(f->ev.state, state.data(), 4 * (size_t)SS))) return rc;
@@ -1039,13 +1084,13 @@ static int upload_event(mkfg_context* ctx, Finder* f, const mkfg_event* ev) {
   MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.bshort_valid, 0, 4 * (size_t)SS, st));
   if ((rc = up(f->ev.node_hot, node_hot.data(), 4 * node_hot.size()))) return rc;
   if ((rc = up(f->ev.node_prev, node_prev.data(), 4 * node_prev.size()))) return rc;
-  if ((rc = up(f->ev.node_chi2, node_chi2.data(), 4 * node_chi2.size()))) return rc;
+  MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.node_chi2, 0, 4 * node_hot.size(), st));
   MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.upd, 0, 4 * (size_t)SC, st));
-  MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.pair_count, 0, 4 * (size_t)(max_steps + 2), st));
   MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.err_flags, 0, 64, st));
-  // Keep host staging alive until the copies have been consumed.
+  // The staging vectors die at return: wait for the copies.
   MKFG_CUDA_TRY(cudaStreamSynchronize(st));
   f->n_seeds = S;
+  f->n_events = n_ev;
   f->events_loaded = 1;
   return MKFG_OK;
 }
@@ -1136,7 +1181,16 @@ extern "C" int mkfg_find_upload(mkfg_context* ctx, const mkfg_event* ev) {
   MKFG_REQUIRE(ev != nullptr, "null event");
   Finder* f = finder_of(ctx);
   MKFG_REQUIRE(f->configured, "mkfg_finder_setup was not called");
-  return upload_event(ctx, f, ev);
+  return upload_batch(ctx, f, ev, 1);
+}
+
+extern "C" int mkfg_find_upload_batch(mkfg_context* ctx, const mkfg_event* evs, int32_t n_events) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  MKFG_REQUIRE(evs != nullptr && n_events >= 1, "empty batch");
+  Finder* f = finder_of(ctx);
+  MKFG_REQUIRE(f->configured, "mkfg_finder_setup was not called");
+  return upload_batch(ctx, f, evs, n_events);
 }
 
 extern "C" int mkfg_find_run(mkfg_context* ctx) {

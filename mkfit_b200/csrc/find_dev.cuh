@@ -70,7 +70,9 @@ struct EventDev {
   const float* herr;
   int hstride;
   const uint32_t* hinfo;  // detid (12 bit) | charge per cm << 12
-  const int* layer_begin; // [n_layers + 1] (per event: + event_layer_offset)
+  const int* layer_begin; // [n_events][lb_stride]: global index of each layer's first hit
+  int lb_stride;          // n_layers + 1
+  int n_bins;             // bins per event
   // Per-layer bins: (first | last << 16) over nq x 256 bins; sorted hits.
   const uint32_t* bins;
   const float* sphi;

@@ -96,8 +96,9 @@ __device__ __forceinline__ float cdist(float a) { return a > kPI ? kTwoPI - a : 
 // the sensitive-region test (TrackerInfo.h:118-138). Writes up to 16 hit
 // indices (index within layer) in bin-scan order; returns XHitSize (-1 when
 // outside the layer) and the WSR code.
-__device__ __forceinline__ int select_hits(const EventDev& E, const LayerDev& L, int layer,
-                                           int hit_base, const float (&par)[6],
+__device__ __forceinline__ int select_hits(const EventDev& E, const LayerDev& L,
+                                           const uint32_t* __restrict__ ev_bins, int hit_base,
+                                           const float (&par)[6],
                                            const float (&err)[21], int* xhit, int xstride,
                                            int& wsr) {
   float min_dq = L.min_dq, max_dq = L.max_dq, min_dphi = L.min_dphi, max_dphi = L.max_dphi;
@@ -154,7 +155,7 @@ __device__ __forceinline__ int select_hits(const EventDev& E, const LayerDev& L,
   const int pb2 = phi_bin(phi + dphi) + 1;
 
   int n = 0;
-  const uint32_t* bins = E.bins + L.bin_offset;
+  const uint32_t* bins = ev_bins + L.bin_offset;
   for (int qi = qb1; qi < qb2; ++qi) {
     for (int pi = pb1; pi < pb2; ++pi) {
       const int pb = pi & 0xff;

@@ -39,6 +39,7 @@ def _bind(lib):
         return
     lib.mkfg_finder_setup.argtypes = [vp, ctypes.POINTER(MkfgFindConfig)]
     lib.mkfg_find_upload.argtypes = [vp, ctypes.POINTER(MkfgEvent)]
+    lib.mkfg_find_upload_batch.argtypes = [vp, ctypes.POINTER(MkfgEvent), ctypes.c_int32]
     lib.mkfg_find_run.argtypes = [vp]
     lib.mkfg_find_download.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(MkfgFindOut)]
     lib.mkfg_find_event.argtypes = [vp, ctypes.POINTER(MkfgEvent), ctypes.POINTER(MkfgFindOut)]
@@ -145,6 +146,15 @@ class Finder:
     def upload(self, ev):
         self._ev = event_struct(ev)
         capi.check(self.lib.mkfg_find_upload(self.ctx.handle, ctypes.byref(self._ev)))
+
+    def upload_batch(self, events):
+        arr = (MkfgEvent * len(events))()
+        self._evs = [event_struct(ev) for ev in events]
+        for i, e in enumerate(self._evs):
+            arr[i] = e
+        self._arr = arr
+        capi.check(self.lib.mkfg_find_upload_batch(self.ctx.handle, arr, len(events)))
+        return sum(ev.n_seeds for ev in events)
 
     def run(self):
         capi.check(self.lib.mkfg_find_run(self.ctx.handle))
