@@ -1,20 +1,25 @@
 #!/usr/bin/env python3
-"""Benchmark of the B200 Kalman-filter hot path.
+"""Benchmark of the B200 Kalman-filter tracking hot path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-One JSON line on rank 0. A "step" is one pass of the hot path over one batch
-of seeded synthetic input resident in HBM (see DESIGN.md for the workload
-definition). For N > 1 the script runs under torchrun, one process per GPU,
-each rank processing its own batch (weak scaling, no data-path collective);
-the step time is the max over ranks of the device time.
+Prints one JSON line on rank 0. Headline: combinatorial track finding
+(clone engine, CMS-2017 geometry) in events built per second for the
+batched form -- a batch of 64 synthetic events of uneven size found by one
+graph-captured launch sequence -- beside the plain one-event form and the
+reference CPU build. A "step" is one pass over the batch with the inputs
+resident in HBM. Secondary: the Kalman fit in tracks fit per second.
 
---impl reference runs the reference's own CPU implementation (the
+Under torchrun (N > 1) each rank finds its own batch (weak scaling, no
+data-path collective); the step time is the max over ranks.
+
+--impl reference times the reference's own CPU implementation (the
 trackreco/mkFit sources compiled in oracle/_ref) on the host cores with all
-available threads, on the same workload and metric; rank 0 only.
+threads, several events in flight, on a bounded sample of the same events.
 """
 import argparse
 import json
+import multiprocessing as mp
 import os
 import statistics
 import subprocess
@@ -27,30 +32,74 @@ sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
+# Batched finding workload: 64 events, Poisson(3000) tracks clipped to
+# [500, 12000], CMS-2017 geometry, noise 1% x a per-layer ramp up to 20x.
+FIND_EVENTS = 64
+FIND_MEAN_TRACKS = 3000
+FIND_NOISE = 0.01
+FIND_DENSITY_RATIO = 20.0
+FIND_MAX_CANDS = 6
+FIND_CHI2_CUT = 30.0
+# Plain single-event workload: 800 tracks, 1% noise.
+PLAIN_TRACKS = 800
+# Algorithmic FLOPs per unit of work (counted in DESIGN.md from the
+# generated products and the restated arithmetic): propagation of a
+# candidate to a layer + hit selection; propagation to a hit + chi2; the
+# update step (propagation to the hit + Kalman update).
+FLOP_LAYER_PROP = 1000
+FLOP_HIT_CHI2 = 950
+FLOP_UPDATE = 1150
+# Fit (secondary metric): toy MC, 10 barrel layers.
 FIT_TRACKS_PER_EVENT = 20000
+FIT_EVENTS = 16
 FIT_LAYERS = 10
-FIT_EVENTS_PER_STEP = 64
-# Algorithmic work of one barrel fit step (track-layer): FLOPs from the
-# generated similarity/update products plus the hand-counted propagation,
-# material and update arithmetic, bytes moved from/to HBM.
-FLOP_PER_TRACK_LAYER = 1130
-BYTES_PER_TRACK_FIXED = 2 * (27 * 4 + 4)   # state in + state out
-BYTES_PER_TRACK_LAYER = 9 * 4 + 4          # hit (pos 3 + err 6) + hit index
+FLOP_FIT_TRACK_LAYER = 1130
 
 
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--events", type=int, default=FIND_EVENTS)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--events", type=int, default=FIT_EVENTS_PER_STEP,
-                   help="events of 20k tracks per step (profiling uses fewer)")
+    p.add_argument("--no-fit", action="store_true")
     return p.parse_args()
 
 
+# ----------------------------------------------------------------------------- inputs
+def find_event_args(n_events, rank):
+    from mkfit_b200 import synth
+    from mkfit_b200.geometry import cms2017
+    sizes = synth.batch_event_sizes(n_events, FIND_MEAN_TRACKS, 500, 12000, seed=0xB200 + rank)
+    ramp = synth.density_ramp(cms2017().n_layers, FIND_DENSITY_RATIO)
+    return [dict(n_tracks=int(n), seed=0xE000 + 1000 * rank + i, noise_frac=FIND_NOISE,
+                 noise_scale=ramp) for i, n in enumerate(sizes)]
+
+
+def generate(args_list):
+    """Generates events in a spawn process pool (started before CUDA)."""
+    from mkfit_b200 import synth
+    n = min(len(args_list), os.cpu_count() or 1)
+    if n <= 1:
+        return [synth.gen_cms_event(**a) for a in args_list]
+    with mp.get_context("spawn").Pool(n) as pool:
+        return pool.map(synth.gen_cms_event_args, args_list)
+
+
+def make_fit_batch(n_events, rank):
+    from mkfit_b200 import synth
+    evs = [synth.gen_fit_event(FIT_TRACKS_PER_EVENT, seed=0xC0FFEE + 1000 * rank + e)
+           for e in range(n_events)]
+    cat = lambda k, ax: np.ascontiguousarray(np.concatenate([getattr(e, k) for e in evs], axis=ax))
+    return synth.FitEvent(par=cat("par", 1), err=cat("err", 1), chg=cat("chg", 0),
+                          hit_pos=cat("hit_pos", 2), hit_err=cat("hit_err", 2),
+                          rl_grid=evs[0].rl_grid, xi_grid=evs[0].xi_grid, radii=evs[0].radii)
+
+
+# ----------------------------------------------------------------------------- utilities
 class ClockSampler:
     """nvidia-smi clock / throttle sampling during the timed region."""
 
@@ -101,8 +150,7 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-# --------------------------------------------------------------------------- helpers
-def dist_setup(args):
+def dist_setup():
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -132,105 +180,123 @@ def max_over_ranks(x, world):
     return float(t.item())
 
 
-def make_fit_batch(n_events, rank):
-    """One batch of n_events toy-MC events (20k tracks x 10 layers each),
-    concatenated: the batched form fits all of them in one launch."""
-    from mkfit_b200 import synth
-    evs = [synth.gen_fit_event(FIT_TRACKS_PER_EVENT, seed=0xC0FFEE + 1000 * rank + e)
-           for e in range(n_events)]
-    cat = lambda k, ax: np.ascontiguousarray(np.concatenate([getattr(e, k) for e in evs], axis=ax))
-    return synth.FitEvent(par=cat("par", 1), err=cat("err", 1), chg=cat("chg", 0),
-                          hit_pos=cat("hit_pos", 2), hit_err=cat("hit_err", 2),
-                          rl_grid=evs[0].rl_grid, xi_grid=evs[0].xi_grid, radii=evs[0].radii)
+def load_measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
 
 
-def cpu_reference_fit_rate(seconds_target=10.0, threads=None):
-    """Reference CPU MkFitter fit (oracle/_ref) on the host cores: tracks/s
-    on a bounded sample of the toy-MC workload."""
-    from oracle.oracle import RefLib
-    from mkfit_b200 import synth
-    ref = RefLib()
-    threads = threads or os.cpu_count()
-    ref.set_threads(threads)
-    ev = synth.gen_fit_event(FIT_TRACKS_PER_EVENT * 4, seed=0xBEEF)
-    _, _, _, t1 = ref.fit(ev.par, ev.err, ev.chg, ev.hit_pos, ev.hit_err, ev.rl_grid, ev.xi_grid,
-                          pflags=2, repeat=1)
-    reps = max(1, int(seconds_target / max(t1, 1e-4) / max(threads, 1)))
-    t0 = time.perf_counter()
-    _, _, _, best = ref.fit(ev.par, ev.err, ev.chg, ev.hit_pos, ev.hit_err, ev.rl_grid,
-                            ev.xi_grid, pflags=2, repeat=reps)
-    wall = time.perf_counter() - t0
-    return ev.n / best, threads, reps, ev.n, wall
+def fp32_peak(ctx):
+    import ctypes
+    v = ctypes.c_double(0)
+    rc = ctx.lib.mkfg_probe_fp32_peak(ctx.handle, 4000, ctypes.byref(v))
+    return v.value if rc == 0 else None
 
 
-# --------------------------------------------------------------------------- ours
-def run_ours(args):
+def timed_events(stream, fn, steps):
+    """Per-step CUDA-event timing on `stream`; returns per-step ms."""
     import torch
-    from mkfit_b200 import Context, FitBuffers
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    for s in range(steps):
+        starts[s].record(stream)
+        fn()
+        ends[s].record(stream)
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in zip(starts, ends)]
 
-    world, rank, local = dist_setup(args)
+
+# ----------------------------------------------------------------------------- ours
+def run_ours(args):
+    rank = int(os.environ.get("RANK", "0"))
+    # Inputs first (process pool before any CUDA call).
+    events = generate(find_event_args(args.events, rank))
+    from mkfit_b200 import synth
+    plain_ev = synth.gen_cms_event(PLAIN_TRACKS, seed=0xC0DE + rank, noise_frac=0.01)
+    fit_batch = None if args.no_fit else make_fit_batch(FIT_EVENTS, rank)
+
+    import torch
+    from mkfit_b200 import Context
+    from mkfit_b200.finder import FindConfig, Finder
+    world, rank, local = dist_setup()
     torch.cuda.set_device(local)
     ctx = Context(local)
     stream = ctx.torch_stream()
+    finder = Finder(ctx, FindConfig(max_cands=FIND_MAX_CANDS, chi2_cut=FIND_CHI2_CUT, zero_c2=True))
+    n_events = len(events)
+    n_seeds = sum(e.n_seeds for e in events)
+    n_hits = sum(e.n_hits for e in events)
 
-    n_events = args.events
-    batch = make_fit_batch(n_events, rank)
-    ctx.set_material(batch.rl_grid, batch.xi_grid)
-    dev = FitBuffers.upload(batch)
-    out = FitBuffers.outputs(batch.n)
-    n_tracks = batch.n
-
-    # Device-resident timing: one batched launch per step.
-    for _ in range(args.warmup):
-        ctx.fit_device(dev, out)
+    # Plain form: one event per upload, eager launch sequence per run.
+    finder.upload(plain_ev)
+    for _ in range(2):
+        finder.run()
     ctx.synchronize()
-    peak = ctypes_probe(ctx)
+    plain_cfg1_ms = statistics.median(timed_events(stream, finder.run, max(3, args.steps // 2)))
+    # Plain form on one event of the batch (same event size class).
+    finder.upload(events[0])
+    finder.run()
+    ctx.synchronize()
+    plain_b_ms = statistics.median(timed_events(stream, finder.run, max(3, args.steps // 2)))
+
+    # Batched form: all events resident, one graph replay per step.
+    finder.upload_batch(events)
+    for _ in range(args.warmup):
+        finder.run_graph()
+    ctx.synchronize()
+    work = finder.work()
+    peak = fp32_peak(ctx)
     sampler = ClockSampler(local)
     barrier(world)
     torch.cuda.synchronize()
     sampler.start()
-    # Untimed back-to-back launches for ~1.5 s so that the clock sampler
-    # (100 ms period) observes the clocks the timed steps run at.
-    t_load = time.perf_counter() + 1.5
+    t_load = time.perf_counter() + 1.5  # let the sampler see the clocks under load
     while time.perf_counter() < t_load:
-        for _ in range(10):
-            ctx.fit_device(dev, out)
+        for _ in range(4):
+            finder.run_graph()
         ctx.synchronize()
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    for s in range(args.steps):
-        starts[s].record(stream)
-        ctx.fit_device(dev, out)
-        ends[s].record(stream)
-    ctx.synchronize()
-    torch.cuda.synchronize()
+    step_ms = timed_events(stream, finder.run_graph, args.steps)
     clocks = sampler.stop()
     barrier(world)
-    step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
     total_ms = sum(step_ms)
     total_ms_max = max_over_ranks(total_ms, world)
-    value = world * n_tracks * args.steps / (total_ms_max * 1e-3)
+    value = world * n_events * args.steps / (total_ms_max * 1e-3)
+    ms_step = total_ms / args.steps
 
-    # Plain form: one launch per event (20k tracks), same data.
-    plain_ms = time_plain_fit(ctx, stream, dev, out, n_events, FIT_TRACKS_PER_EVENT,
-                              max(2, args.steps // 4))
+    flops = (work["active_cands"] * FLOP_LAYER_PROP + work["hit_pairs"] * FLOP_HIT_CHI2 +
+             work["updates"] * FLOP_UPDATE)
+    achieved_tf = flops / (ms_step * 1e-3) / 1e12
 
-    # End to end through the host-buffer C-ABI entry (pinned host memory,
-    # H2D + kernel + D2H inside the timed region).
-    e2e = None if args.no_e2e else time_e2e_fit(ctx, batch, max(2, args.steps // 4), args.warmup)
+    # End to end through the C ABI from host buffers: upload (host hit-index
+    # build + seed partition + H2D), run, download (export + D2H).
+    e2e = None
+    if not args.no_e2e:
+        e_steps = max(2, args.steps // 4)
+        ts = []
+        out = None
+        for _ in range(e_steps + 1):
+            t0 = time.perf_counter()
+            finder.upload_batch(events)
+            finder.run_graph()
+            out = finder.download(n_seeds)
+            ts.append(time.perf_counter() - t0)
+        h2d = sum(e.hit_pos.nbytes + e.hit_err.nbytes + e.hit_detid.nbytes + e.hit_cpcm.nbytes +
+                  e.seed_par.nbytes + e.seed_err.nbytes + e.seed_chg.nbytes for e in events)
+        d2h = sum(v.nbytes for v in out.values())
+        t = statistics.median(ts[1:])
+        e2e = {"value": n_events / t, "unit": "events/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": t * 1e3,
+               "entry": "mkfg_find_upload_batch + mkfg_find_run_graph + mkfg_find_download "
+                        "(host hit-index build, seed partition, copies, export)"}
 
-    kernel_ms = total_ms / args.steps
-    flops = n_tracks * FIT_LAYERS * FLOP_PER_TRACK_LAYER
-    bytes_alg = n_tracks * (BYTES_PER_TRACK_FIXED + FIT_LAYERS * BYTES_PER_TRACK_LAYER)
-    achieved_tf = flops / (kernel_ms * 1e-3) / 1e12
-    achieved_gbs = bytes_alg / (kernel_ms * 1e-3) / 1e9
+    fit = None if fit_batch is None else run_fit(ctx, stream, fit_batch, args)
+
     peaks = load_measured_peaks()
-    hbm_peak = peaks.get("hbm_gbs")
-
     line = {
-        "metric": "tracks fit/s",
+        "metric": "events built/s",
         "value": value,
-        "unit": "tracks/s",
+        "unit": "events/s",
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
@@ -239,46 +305,47 @@ def run_ours(args):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32",
-        "data": "synthetic (seeded toy MC, mkfit_b200.synth.gen_fit_event)",
+        "data": "synthetic (seeded, mkfit_b200.synth.gen_cms_event on the CMS-2017 layer table)",
         "config": {
-            "workload": (f"Kalman fit, toy MC: {n_events} events x "
-                         f"{FIT_TRACKS_PER_EVENT} tracks x {FIT_LAYERS} barrel layers per step, "
-                         "one batched launch (the reference's MkFitter fit)"),
-            "tracks_per_step": n_tracks,
-            "layers": FIT_LAYERS,
-            "pflags": "apply_material",
-            "l2": "inputs larger than L2 (%.0f MB per step)" % (bytes_alg / 1e6),
-            "parallelism": f"dp{world} (independent events per GPU)",
+            "workload": (f"batched clone-engine finding: {n_events} CMS-2017 events per step, "
+                         f"Poisson({FIND_MEAN_TRACKS}) tracks clipped to [500, 12000], "
+                         f"noise {FIND_NOISE:.0%} x per-layer ramp up to {FIND_DENSITY_RATIO:.0f}x, "
+                         f"maxCandsPerSeed {FIND_MAX_CANDS}, chi2 cut {FIND_CHI2_CUT:.0f}, "
+                         "one CUDA-graph replay per step"),
+            "events_per_step": n_events, "seeds_per_step": n_seeds, "hits_per_step": n_hits,
+            "l2": "inputs + candidate state ~%.0f MB per step (L2 126 MB); no flush" % (
+                (n_hits * 40 + n_seeds * 8 * 37 * 4 * 3) / 1e6),
+            "parallelism": f"dp{world} (independent event batches per GPU)",
         },
-        "plain_form": {"events_per_launch": 1, "tracks_per_launch": FIT_TRACKS_PER_EVENT,
-                       "value": n_tracks / (plain_ms * 1e-3), "unit": "tracks/s",
-                       "ms_per_step": plain_ms,
-                       "launches_per_step": n_events},
+        "plain_form": {
+            "cms_800_tracks": {"events_per_launch_sequence": 1, "value": 1e3 / plain_cfg1_ms,
+                               "unit": "events/s", "ms_per_event": plain_cfg1_ms,
+                               "seeds": plain_ev.n_seeds},
+            "batch_event0": {"value": 1e3 / plain_b_ms, "unit": "events/s",
+                             "ms_per_event": plain_b_ms, "seeds": events[0].n_seeds},
+            "batched_over_plain": (value / world) / (1e3 / plain_b_ms),
+        },
         "roofline": {
             "bound": "fp32",
-            "kernel": "fit_kernel<false>",
+            "scope": "whole finding step (all kernels of the graph)",
             "achieved": achieved_tf,
             "peak": peak,
             "unit": "TFLOP/s",
             "frac": achieved_tf / peak if peak else None,
             "peak_source": "measured FP32 FMA probe (mkfg_probe_fp32_peak), same run",
-            "flop_per_launch": flops,
+            "flop_per_step": flops,
+            "work_per_step": work,
             "traffic": None,
-            "hbm": {"achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
-                    "frac": achieved_gbs / hbm_peak if hbm_peak else None,
-                    "bytes_per_launch": bytes_alg, "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
+            "hbm_peak_gbs": peaks.get("hbm_gbs"),
         },
         "e2e": e2e,
         "gpu_launches": args.steps,
+        "gpu_launches_note": "one CUDA graph launch per step (reset + 4 kernels per layer step + merge)",
         "clocks": clocks,
+        "fit": fit,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, threads, reps, sample_n, wall = cpu_reference_fit_rate()
-        line["cpu_baseline"] = {
-            "value": rate, "unit": "tracks/s", "cores": threads, "kind": "reference",
-            "sample": (f"reference MkFitter fit (oracle/_ref, AVX2 Matriplex) of {sample_n} "
-                       f"toy-MC tracks x {FIT_LAYERS} layers, best of {reps} repeats, "
-                       f"{wall:.1f} s wall")}
+        line["cpu_baseline"] = cpu_baseline_find(events)
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -287,131 +354,80 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def ctypes_probe(ctx):
-    import ctypes
-    v = ctypes.c_double(0)
-    rc = ctx.lib.mkfg_probe_fp32_peak(ctx.handle, 20000, ctypes.byref(v))
-    return v.value if rc == 0 else None
+def run_fit(ctx, stream, batch, args):
+    from mkfit_b200 import FitBuffers
+    ctx.set_material(batch.rl_grid, batch.xi_grid)
+    dev = FitBuffers.upload(batch)
+    out = FitBuffers.outputs(batch.n)
+    for _ in range(args.warmup):
+        ctx.fit_device(dev, out)
+    ctx.synchronize()
+    ms = timed_events(stream, lambda: ctx.fit_device(dev, out), args.steps)
+    t = sum(ms) / len(ms)
+    flops = batch.n * FIT_LAYERS * FLOP_FIT_TRACK_LAYER
+    return {"metric": "tracks fit/s", "value": batch.n / (t * 1e-3), "unit": "tracks/s",
+            "ms_per_step": t, "tracks_per_step": batch.n,
+            "workload": f"toy-MC Kalman fit, {FIT_EVENTS} events x {FIT_TRACKS_PER_EVENT} tracks x "
+                        f"{FIT_LAYERS} barrel layers, material on, one launch",
+            "achieved_tflops": flops / (t * 1e-3) / 1e12}
 
 
-def time_plain_fit(ctx, stream, dev, out, n_events, per_event, steps):
-    """One launch per event: the plain drop-in form of the fit."""
-    import torch
-    from mkfit_b200 import capi
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
-    ms = []
-    for s in range(steps + 1):
-        t0.record(stream)
-        for e in range(n_events):
-            ctx_fit_slice(ctx, dev, out, e * per_event, per_event)
-        t1.record(stream)
-        ctx.synchronize()
-        if s > 0:
-            ms.append(t0.elapsed_time(t1))
-    return sum(ms) / len(ms)
+def cpu_baseline_find(events, n_sample=8):
+    from oracle.oracle import RefLib, ref_find_batch
+    ref = RefLib()
+    threads = os.cpu_count()
+    ref.set_threads(threads)
+    sample = events[:n_sample]
+    t0 = time.perf_counter()
+    o = ref_find_batch(ref, sample, max_cands=FIND_MAX_CANDS, chi2_cut=FIND_CHI2_CUT, repeat=3)
+    wall = time.perf_counter() - t0
+    return {"value": len(sample) / o["seconds"], "unit": "events/s", "cores": threads,
+            "kind": "reference",
+            "sample": (f"{len(sample)} of the step's events ({sum(e.n_seeds for e in sample)} seeds), "
+                       f"reference find_tracks_load_seeds + FindTracksCloneEngine, events in flight "
+                       f"on a {threads}-thread pool, AVX2 Matriplex (NN=8), best of 3, "
+                       f"{wall:.1f} s wall incl. hit-index build")}
 
 
-def ctx_fit_slice(ctx, dev, out, begin, count):
-    """Fit tracks [begin, begin+count) of the device batch (views with the
-    batch stride)."""
-    import ctypes
-    from mkfit_b200 import capi
-    n = dev["n"]
-    a = capi.MkfgFitArgs()
-    f4 = 4
-    a.in_ = capi.MkfgTracks(dev["par"].data_ptr() + begin * f4, dev["err"].data_ptr() + begin * f4,
-                            dev["chg"].data_ptr() + begin * f4, count, n)
-    a.out = capi.MkfgTracks(out["par"].data_ptr() + begin * f4, out["err"].data_ptr() + begin * f4,
-                            out["chg"].data_ptr() + begin * f4, count, n)
-    a.hits = capi.MkfgHits(dev["hit_pos"].data_ptr(), dev["hit_err"].data_ptr(),
-                           dev["layer_begin"].data_ptr(), dev["n_layers"], dev["n_hits"])
-    a.hot_index = dev["hot"].data_ptr() + begin * f4
-    a.hot_stride = n
-    a.n_steps = dev["n_layers"]
-    hl = np.arange(dev["n_layers"], dtype=np.int32)
-    a._hl = hl
-    a.hit_layer = hl.ctypes.data
-    a.endcap_mask = 0
-    a.pflags = capi.PF_MATERIAL
-    a.out_chi2 = None
-    capi.check(ctx.lib.mkfg_fit(ctx.handle, ctypes.byref(a)))
-
-
-def time_e2e_fit(ctx, batch, steps, warmup):
-    import torch
-    n = batch.n
-    nl = batch.hit_pos.shape[0]
-    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
-    par, err, chg = pin(batch.par), pin(batch.err), pin(batch.chg)
-    hp = pin(batch.hit_pos.transpose(1, 0, 2).reshape(3, nl * n))
-    he = pin(batch.hit_err.transpose(1, 0, 2).reshape(6, nl * n))
-    out = dict(par=pin(np.zeros((6, n), np.float32)), err=pin(np.zeros((21, n), np.float32)),
-               chg=pin(np.zeros(n, np.int32)), chi2=pin(np.zeros(n, np.float32)))
-    for _ in range(max(1, warmup // 2)):
-        ctx.fit_host(par, err, chg, hp, he, out=out)
-    ts = []
-    for _ in range(steps):
-        t0 = time.perf_counter()
-        ctx.fit_host(par, err, chg, hp, he, out=out)
-        ts.append(time.perf_counter() - t0)
-    t = sum(ts) / len(ts)
-    h2d = par.nbytes + err.nbytes + chg.nbytes + hp.nbytes + he.nbytes + 4 * (nl + 1) + 4 * nl * n
-    d2h = out["par"].nbytes + out["err"].nbytes + out["chg"].nbytes
-    return {"value": n / t, "unit": "tracks/s", "h2d_bytes_per_step": int(h2d),
-            "d2h_bytes_per_step": int(d2h), "ms_per_step": t * 1e3,
-            "entry": "mkfg_fit_host (pinned host buffers; H2D + fit + D2H + sync)"}
-
-
-def load_measured_peaks():
-    try:
-        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except Exception:
-        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
-
-
-# --------------------------------------------------------------------------- reference
+# ----------------------------------------------------------------------------- reference
 def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from oracle.oracle import RefLib, have_ref
-    from mkfit_b200 import synth
+    from oracle.oracle import RefLib, have_ref, ref_find_batch
     if not have_ref():
         print(json.dumps({"impl": "reference", "unavailable":
                           "reference CPU build oracle/_ref missing (built by __graft_entry__.build "
-                          "from /root/reference)"}))
+                          "from the reference sources)"}))
         return
+    events = generate(find_event_args(args.events, 0))
+    sample = events[:8]
     ref = RefLib()
     threads = os.cpu_count()
     ref.set_threads(threads)
-    # A step is a bounded sample of the same workload: 4 events of 20k tracks.
-    n_ev = 4
-    ev = make_fit_batch(n_ev, 0)
-    for _ in range(args.warmup):
-        ref.fit(ev.par, ev.err, ev.chg, ev.hit_pos, ev.hit_err, ev.rl_grid, ev.xi_grid, pflags=2)
-    times = []
+    for _ in range(max(1, min(args.warmup, 2))):
+        ref_find_batch(ref, sample, max_cands=FIND_MAX_CANDS, chi2_cut=FIND_CHI2_CUT)
+    secs = []
     for _ in range(args.steps):
-        _, _, _, t = ref.fit(ev.par, ev.err, ev.chg, ev.hit_pos, ev.hit_err, ev.rl_grid,
-                             ev.xi_grid, pflags=2)
-        times.append(t)
-    total = sum(times)
-    value = ev.n * args.steps / total
+        o = ref_find_batch(ref, sample, max_cands=FIND_MAX_CANDS, chi2_cut=FIND_CHI2_CUT)
+        secs.append(o["seconds"])
+    total = sum(secs)
+    value = len(sample) * args.steps / total
     line = {
         "impl": "reference",
-        "metric": "tracks fit/s", "value": value, "unit": "tracks/s", "n_gpus": world,
+        "metric": "events built/s", "value": value, "unit": "events/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded toy MC, mkfit_b200.synth.gen_fit_event)",
-        "config": {"workload": (f"Kalman fit, toy MC: {n_ev} events x {FIT_TRACKS_PER_EVENT} "
-                                f"tracks x {FIT_LAYERS} barrel layers per step (bounded sample "
-                                f"of the GPU arm's {FIT_EVENTS_PER_STEP}-event step)"),
-                   "tracks_per_step": ev.n, "layers": FIT_LAYERS, "pflags": "apply_material"},
-        "cpu_baseline": {"value": value, "unit": "tracks/s", "cores": threads, "kind": "reference",
-                         "sample": f"{ev.n} tracks per step, reference MkFitter fit, TBB-shim "
-                                   f"thread pool of {threads} threads, AVX2 Matriplex (NN=8)"},
-        "e2e": {"value": value, "unit": "tracks/s", "h2d_bytes_per_step": 0,
+        "data": "synthetic (seeded, mkfit_b200.synth.gen_cms_event on the CMS-2017 layer table)",
+        "config": {"workload": (f"clone-engine finding, CMS-2017: a bounded sample of {len(sample)} "
+                                f"of the GPU arm's {len(events)} events per step, events in flight"),
+                   "events_per_step": len(sample),
+                   "seeds_per_step": sum(e.n_seeds for e in sample)},
+        "cpu_baseline": {"value": value, "unit": "events/s", "cores": threads, "kind": "reference",
+                         "sample": f"{len(sample)} events per step on a {threads}-thread pool, "
+                                   "reference MkBuilder::FindTracksCloneEngine, AVX2 Matriplex"},
+        "e2e": {"value": value, "unit": "events/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
         "gpu_launches": 0,
     }

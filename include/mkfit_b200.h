@@ -212,6 +212,14 @@ int mkfg_find_upload(mkfg_context* ctx, const mkfg_event* ev);
  * (mkFit/mkFit.cc:308-425). */
 int mkfg_find_upload_batch(mkfg_context* ctx, const mkfg_event* evs, int32_t n_events);
 int mkfg_find_run(mkfg_context* ctx);
+/* The same sequence captured once per upload into a CUDA graph and
+ * replayed (one graph launch per call). No reference counterpart. */
+int mkfg_find_run_graph(mkfg_context* ctx);
+/* Work done by the last run (for FLOP accounting): candidate propagations
+ * to a layer, (candidate, hit) chi2 evaluations, Kalman updates, and the
+ * number of layer-plan steps. No reference counterpart. */
+int mkfg_find_work(mkfg_context* ctx, int64_t* active_cands, int64_t* hit_pairs,
+                   int64_t* updates, int32_t* steps);
 int mkfg_find_download(mkfg_context* ctx, int32_t n_seeds, mkfg_find_out* out);
 int mkfg_find_event(mkfg_context* ctx, const mkfg_event* ev, mkfg_find_out* out);
 

@@ -73,6 +73,10 @@ __global__ void __launch_bounds__(kBlock) k_prep(EventDev E, const FindConfigDev
     }
   }
   const unsigned act = __ballot_sync(0xffffffffu, active) & grp;
+  {
+    const unsigned all = __ballot_sync(0xffffffffu, active);
+    if (lane == 0 && all) atomicAdd(&E.work[step * 4 + 0], __popc(all));
+  }
   if (in_range && c == 0) {
     if (layer >= 0 && state == kFinding && act == 0) state = kFinished;
     E.state[s] = state;
@@ -524,6 +528,7 @@ __global__ void __launch_bounds__(kBlock) k_update(EventDev E, const FindConfigD
   const int slot = s * kSlots + c;
   if (!E.upd[slot]) return;
   E.upd[slot] = 0;
+  atomicAdd(&E.work[step * 4 + 1], 1);
   const CandSoA& B = E.cand[E.cur[s]];
   float par[6], err[21];
   load_state(B, slot, par, err);
@@ -554,6 +559,27 @@ __global__ void __launch_bounds__(kBlock) k_update(EventDev E, const FindConfigD
   }
   store_state(B, slot, par, err);
   B.chg[slot] = chg;
+}
+
+//------------------------------------------------------------------------------
+// Reset: restore the imported seeds as the only candidates (the state after
+// MkBuilder::find_tracks_load_seeds), so every run starts from the upload.
+//------------------------------------------------------------------------------
+__global__ void k_reset(EventDev E, int n_work) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n_work) E.work[t] = 0;
+  if (t == 0) E.err_flags[0] = 0;
+  const int s = t / kSlots, c = t % kSlots;
+  if (s >= E.n_seeds) return;
+  copy_slot(E.init, t, E.cand[0], t);
+  E.upd[t] = 0;
+  if (c == 0) {
+    E.n_cands[s] = 1;
+    E.state[s] = kDormant;
+    E.cur[s] = 0;
+    E.hot_size[s] = E.init_hot[s];
+    E.bshort_valid[s] = 0;
+  }
 }
 
 //------------------------------------------------------------------------------
@@ -705,6 +731,11 @@ struct Finder {
   int n_seeds = 0;
   int n_events = 0;
   int events_loaded = 0;
+  cudaGraphExec_t graph = nullptr;  // captured run sequence of the current upload
+  void drop_graph() {
+    if (graph) cudaGraphExecDestroy(graph);
+    graph = nullptr;
+  }
 };
 
 namespace {
@@ -728,6 +759,7 @@ void finder_release(mkfg_context* ctx) {
   if (!ctx || !ctx->finder) return;
   Finder* f = static_cast<Finder*>(ctx->finder);
   if (f->d_cfg) cudaFree(f->d_cfg);
+  f->drop_graph();
   f->hits.release();
   f->seeds.release();
   f->cands.release();
@@ -937,7 +969,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   const int M = f->host_cfg.max_cands;
   const int hot_cap = ((8 + max_steps * (2 * M + 3)) + 31) / 32 * 32;
   {
-    const size_t need = 2 * rounded(4 * (size_t)SC) * 37 + rounded(4 * (size_t)SS) * 46 + 4096;
+    const size_t need = 3 * rounded(4 * (size_t)SC) * 37 + rounded(4 * (size_t)SS) * 47 + 4096;
     if ((rc = f->cands.ensure(need))) return rc;
     char* p = f->cands.as<char>();
     auto mk = [&](int cap) {
@@ -958,7 +990,9 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     };
     f->ev.cand[0] = mk(SC);
     f->ev.cand[1] = mk(SC);
+    f->ev.init = mk(SC);
     f->ev.bshort = mk(SS);
+    f->ev.init_hot = carve<int>(p, SS);
     f->ev.seed_label = carve<int>(p, SS);
     f->ev.seed_event = carve<int>(p, SS);
     f->ev.region = carve<int>(p, SS);
@@ -971,7 +1005,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   }
   {
     const size_t need = rounded(4 * (size_t)SC) * (27 + 5) + 2 * rounded(4 * (size_t)SC * kMaxXHits) +
-                        rounded(4 * (size_t)(max_steps + 2)) + rounded(64) + 4096;
+                        rounded(4 * (size_t)(max_steps + 2)) * 5 + rounded(64) + 4096;
     if ((rc = f->scratch.ensure(need))) return rc;
     char* p = f->scratch.as<char>();
     f->ev.ppar = carve<float>(p, 6 * (size_t)SC);
@@ -984,6 +1018,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     f->ev.pairs = carve<int>(p, (size_t)SC * kMaxXHits);
     f->ev.pair_count = carve<int>(p, max_steps + 2);
     f->ev.err_flags = carve<int>(p, 16);
+    f->ev.work = carve<int>(p, 4 * (size_t)(max_steps + 2));
   }
   {
     const size_t nrec = (size_t)SS * kRecPerSeed;
@@ -1061,7 +1096,8 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
       score[slot] = bonus * nf + 0.0f * 0 - penalty * nin - 3.0f * 0 - 0.0f;
     }
   }
-  CandSoA& B0 = f->ev.cand[0];
+  f->drop_graph();
+  CandSoA& B0 = f->ev.init;
   if ((rc = up(B0.par, par.data(), 4 * par.size()))) return rc;
   if ((rc = up(B0.err, err.data(), 4 * err.size()))) return rc;
   if ((rc = up(B0.chg, chg.data(), 4 * (size_t)SC))) return rc;
@@ -1080,7 +1116,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   if ((rc = up(f->ev.state, state.data(), 4 * (size_t)SS))) return rc;
   if ((rc = up(f->ev.n_cands, ncand.data(), 4 * (size_t)SS))) return rc;
   if ((rc = up(f->ev.cur, cur.data(), 4 * (size_t)SS))) return rc;
-  if ((rc = up(f->ev.hot_size, hot_size.data(), 4 * (size_t)SS))) return rc;
+  if ((rc = up(f->ev.init_hot, hot_size.data(), 4 * (size_t)SS))) return rc;
   MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.bshort_valid, 0, 4 * (size_t)SS, st));
   if ((rc = up(f->ev.node_hot, node_hot.data(), 4 * node_hot.size()))) return rc;
   if ((rc = up(f->ev.node_prev, node_prev.data(), 4 * node_prev.size()))) return rc;
@@ -1095,14 +1131,17 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   return MKFG_OK;
 }
 
-static int run_plain(mkfg_context* ctx, Finder* f) {
+// Enqueues the whole finding sequence of the uploaded batch on `st`:
+// reset, then for every layer-plan step prep -> chi2 -> clone -> update,
+// then the final merge.
+static int enqueue_run(Finder* f, cudaStream_t st) {
   const int S = f->n_seeds;
-  if (S == 0) return MKFG_OK;
-  cudaStream_t st = ctx->stream;
+  const int n_work = 4 * (f->host_cfg.max_steps + 2);
   const int threads_c = S * kSlots;
   const int grid_c = (threads_c + kBlock - 1) / kBlock;
   const int grid_w = (S * 32 + kBlock - 1) / kBlock;
   const int grid_p = std::min((S * kSlots * 4 + kBlock - 1) / kBlock, 148 * 16);
+  k_reset<<<std::max(grid_c, (n_work + kBlock - 1) / kBlock), kBlock, 0, st>>>(f->ev, n_work);
   MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.pair_count, 0, 4 * (size_t)(f->host_cfg.max_steps + 2), st));
   for (int step = 1; step <= f->host_cfg.max_steps; ++step) {
     k_prep<<<grid_c, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
@@ -1112,6 +1151,37 @@ static int run_plain(mkfg_context* ctx, Finder* f) {
   }
   k_merge<<<(S + 127) / 128, 128, 0, st>>>(f->ev, f->d_cfg);
   MKFG_CUDA_TRY(cudaGetLastError());
+  return MKFG_OK;
+}
+
+static int run_plain(mkfg_context* ctx, Finder* f) {
+  if (f->n_seeds == 0) return MKFG_OK;
+  return enqueue_run(f, ctx->stream);
+}
+
+// Same sequence captured once into a CUDA graph and replayed: one launch
+// for the whole batch of events and all layer steps.
+static int run_graph(mkfg_context* ctx, Finder* f) {
+  if (f->n_seeds == 0) return MKFG_OK;
+  cudaStream_t st = ctx->stream;
+  if (!f->graph) {
+    cudaGraph_t g = nullptr;
+    MKFG_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    const int rc = enqueue_run(f, st);
+    const cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) return set_error(MKFG_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+    const cudaError_t ei = cudaGraphInstantiate(&f->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+      f->graph = nullptr;
+      return set_error(MKFG_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ei));
+    }
+  }
+  MKFG_CUDA_TRY(cudaGraphLaunch(f->graph, st));
   return MKFG_OK;
 }
 
@@ -1199,6 +1269,38 @@ extern "C" int mkfg_find_run(mkfg_context* ctx) {
   Finder* f = finder_of(ctx);
   MKFG_REQUIRE(f->configured && f->events_loaded, "no event uploaded");
   return run_plain(ctx, f);
+}
+
+extern "C" int mkfg_find_run_graph(mkfg_context* ctx) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  Finder* f = finder_of(ctx);
+  MKFG_REQUIRE(f->configured && f->events_loaded, "no event uploaded");
+  return run_graph(ctx, f);
+}
+
+extern "C" int mkfg_find_work(mkfg_context* ctx, int64_t* active_cands, int64_t* hit_pairs,
+                              int64_t* updates, int32_t* steps) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  Finder* f = finder_of(ctx);
+  MKFG_REQUIRE(f->events_loaded, "no event uploaded");
+  const int ns = f->host_cfg.max_steps + 2;
+  std::vector<int> work(4 * (size_t)ns), pairs(ns);
+  MKFG_CUDA_TRY(cudaMemcpyAsync(work.data(), f->ev.work, 4 * work.size(), cudaMemcpyDeviceToHost, ctx->stream));
+  MKFG_CUDA_TRY(cudaMemcpyAsync(pairs.data(), f->ev.pair_count, 4 * pairs.size(), cudaMemcpyDeviceToHost, ctx->stream));
+  MKFG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  int64_t a = 0, p = 0, u = 0;
+  for (int i = 0; i < ns; ++i) {
+    a += work[4 * i];
+    u += work[4 * i + 1];
+    p += pairs[i];
+  }
+  if (active_cands) *active_cands = a;
+  if (hit_pairs) *hit_pairs = p;
+  if (updates) *updates = u;
+  if (steps) *steps = f->host_cfg.max_steps;
+  return MKFG_OK;
 }
 
 extern "C" int mkfg_find_download(mkfg_context* ctx, int n_seeds, mkfg_find_out* out) {

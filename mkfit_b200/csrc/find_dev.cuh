@@ -117,6 +117,11 @@ struct EventDev {
   int* pairs;
   int* pair_count; // [max_steps + 1]
   int* err_flags;
+  // Pristine initial state (restored by the reset kernel before every run).
+  CandSoA init;
+  int* init_hot;   // number of seed nodes per seed
+  // Work counters per step: [step][0] active candidates, [1] updates.
+  int* work;
 };
 
 __device__ __forceinline__ int hot_pack(int index, int layer) {

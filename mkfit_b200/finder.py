@@ -41,6 +41,9 @@ def _bind(lib):
     lib.mkfg_find_upload.argtypes = [vp, ctypes.POINTER(MkfgEvent)]
     lib.mkfg_find_upload_batch.argtypes = [vp, ctypes.POINTER(MkfgEvent), ctypes.c_int32]
     lib.mkfg_find_run.argtypes = [vp]
+    lib.mkfg_find_run_graph.argtypes = [vp]
+    i64p = ctypes.POINTER(ctypes.c_int64)
+    lib.mkfg_find_work.argtypes = [vp, i64p, i64p, i64p, ctypes.POINTER(ctypes.c_int32)]
     lib.mkfg_find_download.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(MkfgFindOut)]
     lib.mkfg_find_event.argtypes = [vp, ctypes.POINTER(MkfgEvent), ctypes.POINTER(MkfgFindOut)]
     lib.mkfg_prepare_event_host.argtypes = [ctypes.POINTER(MkfgFindConfig),
@@ -158,6 +161,16 @@ class Finder:
 
     def run(self):
         capi.check(self.lib.mkfg_find_run(self.ctx.handle))
+
+    def run_graph(self):
+        capi.check(self.lib.mkfg_find_run_graph(self.ctx.handle))
+
+    def work(self):
+        a, p, u = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        st = ctypes.c_int32()
+        capi.check(self.lib.mkfg_find_work(self.ctx.handle, ctypes.byref(a), ctypes.byref(p),
+                                           ctypes.byref(u), ctypes.byref(st)))
+        return dict(active_cands=a.value, hit_pairs=p.value, updates=u.value, steps=st.value)
 
     def download(self, n_seeds):
         o = output_arrays(n_seeds, self.cfg.max_cands)

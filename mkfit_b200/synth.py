@@ -529,3 +529,20 @@ def gen_cms_event(n_tracks=800, seed=0xC0FFEE, geom=None, pt_range=(0.5, 50.0), 
         seed_chg=schg, seed_nhits=snh, seed_hit_layer=shl, seed_hit_index=shi,
         seed_mc=np.array(seed_tracks, np.int32), n_tracks=n, seed=seed,
         n_signal_hits=int((mc >= 0).sum()))
+
+
+def density_ramp(n_layers, ratio=20.0):
+    """Per-layer noise multipliers rising geometrically from 1 to `ratio`
+    over the layer index (hit density varying ~ratio x across layers)."""
+    return np.power(ratio, np.arange(n_layers) / max(n_layers - 1, 1))
+
+
+def batch_event_sizes(n_events, mean, lo, hi, seed):
+    """Poisson track counts per event, clipped to [lo, hi]."""
+    rng = np.random.default_rng(seed)
+    return np.clip(rng.poisson(mean, n_events), lo, hi).astype(int)
+
+
+def gen_cms_event_args(args):
+    """Picklable entry for process pools: gen_cms_event(**args)."""
+    return gen_cms_event(**args)

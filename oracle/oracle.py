@@ -224,3 +224,40 @@ def ref_event_prep(reflib, ev):
     if rc != 0:
         raise RuntimeError(f"ref_event_prep failed rc={rc}")
     return dict(bins=bins, srank=srank, seed_order=order, seed_region=region)
+
+
+def ref_find_batch(reflib, events, max_cands=6, chi2_cut=30.0, zero_c2=True, repeat=1):
+    """Reference clone-engine finding of several events in flight
+    (oracle/ref_driver.cc ref_find_batch). Returns best-candidate summaries
+    per concatenated seed and the best timed-region seconds."""
+    lib = reflib.lib
+    L = events[0].n_layers
+    hit_off = np.zeros(len(events) + 1, np.int32)
+    seed_off = np.zeros(len(events) + 1, np.int32)
+    for i, ev in enumerate(events):
+        hit_off[i + 1] = hit_off[i] + ev.n_hits
+        seed_off[i + 1] = seed_off[i] + ev.n_seeds
+    cat = lambda k, ax, t: np.ascontiguousarray(np.concatenate([getattr(e, k) for e in events], axis=ax), t)
+    lb = np.ascontiguousarray(np.stack([ev.layer_begin for ev in events]), np.int32)
+    NS = int(seed_off[-1])
+    lib.ref_find_batch.restype = ctypes.c_int
+    lib.ref_find_batch.argtypes = ([ctypes.c_int, _i32p, _i32p, _i32p, _f32p, _f32p, _i32p, _i32p,
+                                    _f32p, _f32p, _i32p, _i32p, _i32p, _i32p, ctypes.c_int,
+                                    ctypes.c_float, ctypes.c_int, ctypes.c_int] +
+                                   [_i32p] * 5 + [ctypes.POINTER(ctypes.c_double)])
+    o = dict(n_cands=np.zeros(NS, np.int32), nfound=np.zeros(NS, np.int32),
+             ntot=np.zeros(NS, np.int32), hit_idx=np.zeros((NS, 64), np.int32),
+             hit_lyr=np.zeros((NS, 64), np.int32))
+    secs = ctypes.c_double(0)
+    rc = lib.ref_find_batch(len(events), hit_off, seed_off, lb, cat("hit_pos", 1, np.float32),
+                            cat("hit_err", 1, np.float32), cat("hit_detid", 0, np.int32),
+                            cat("hit_cpcm", 0, np.int32), cat("seed_par", 1, np.float32),
+                            cat("seed_err", 1, np.float32), cat("seed_chg", 0, np.int32),
+                            cat("seed_nhits", 0, np.int32), cat("seed_hit_layer", 0, np.int32),
+                            cat("seed_hit_index", 0, np.int32), int(max_cands), float(chi2_cut),
+                            int(zero_c2), int(repeat), o["n_cands"], o["nfound"], o["ntot"],
+                            o["hit_idx"], o["hit_lyr"], ctypes.byref(secs))
+    if rc != 0:
+        raise RuntimeError(f"ref_find_batch failed rc={rc}")
+    o["seconds"] = secs.value
+    return o

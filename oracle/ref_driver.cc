@@ -452,3 +452,100 @@ int ref_event_prep(int n_layers_in, const int* layer_begin, const float* hpos, c
 }
 
 }  // extern "C"
+
+//------------------------------------------------------------------------------
+// Several events "in flight" (mkFit/mkFit.cc:308-425): events are found
+// concurrently on the shim thread pool, each with its own builder, while
+// every event's FindTracksCloneEngine also parallelises over its regions
+// and seed chunks. Inputs are the per-event arrays concatenated:
+//   hit_off[n_ev+1], seed_off[n_ev+1] (prefix sums), layer_begin[n_ev][L+1]
+//   (event-local), pos[3][NH], err[6][NH], detid[NH], cpcm[NH],
+//   spar[6][NS], serr[21][NS], schg[NS], seed_nhits[NS], hit layer/index
+//   [NS][4]. Outputs per concatenated seed as in ref_find. The timed region
+//   (best of `repeat`) covers seed import + FindTracksCloneEngine of all
+//   events; the hit-index build precedes it, as in the reference's own
+//   timing (mkFit/buildtestMPlex.cc:342-366).
+extern "C" int ref_find_batch(int n_ev, const int* hit_off, const int* seed_off,
+                              const int* layer_begin, const float* hpos, const float* herr,
+                              const int* detid, const int* cpcm, const float* spar,
+                              const float* serr, const int* schg, const int* seed_nhits,
+                              const int* seed_hit_layer, const int* seed_hit_index, int max_cands,
+                              float chi2_cut, int zero_c2, int repeat, int* n_cands,
+                              int* best_nfound, int* best_ntot, int* best_hit_idx,
+                              int* best_hit_lyr, double* best_seconds) {
+  ensure_cms2017();
+  fillZRgridME();
+  const int L = (int)Config::TrkInfo.m_layers.size();
+  IterationConfig itconf = Config::ItrInfo[0];
+  itconf.m_params.maxCandsPerSeed = max_cands;
+  itconf.m_backward_params.maxCandsPerSeed = max_cands;
+  itconf.m_params.chi2Cut_min = chi2_cut;
+  itconf.m_backward_params.chi2Cut_min = chi2_cut;
+  if (zero_c2)
+    for (auto& lc : itconf.m_layer_configs) lc.c_c2_0 = lc.c_c2_1 = lc.c_c2_2 = 0.f;
+  const int NH = hit_off[n_ev], NS = seed_off[n_ev];
+
+  std::vector<std::vector<HitVec>> hits(n_ev, std::vector<HitVec>(L));
+  std::vector<std::unique_ptr<EventOfHits>> eohs(n_ev);
+  std::vector<TrackVec> seeds(n_ev);
+  for (int e = 0; e < n_ev; ++e) {
+    const int* lb = layer_begin + (size_t)e * (L + 1);
+    for (int l = 0; l < L; ++l)
+      for (int h = lb[l]; h < lb[l + 1]; ++h) {
+        const int g = hit_off[e] + h;
+        Hit hit = make_hit(g, NH, hpos, herr);
+        if (cpcm[g] < 0) hit.setupAsPixel(detid[g], 1, 1);
+        else hit.setupAsStrip(detid[g], cpcm[g], 1);
+        hits[e][l].push_back(hit);
+      }
+    eohs[e].reset(new EventOfHits(Config::TrkInfo));
+    for (int l = 0; l < L; ++l) eohs[e]->SuckInHits(l, hits[e][l]);
+    for (int s = seed_off[e]; s < seed_off[e + 1]; ++s) {
+      Track t = make_track(s, NS, spar, serr, schg);
+      t.setLabel(s);
+      for (int k = 0; k < seed_nhits[s]; ++k)
+        t.addHitIdx(seed_hit_index[s * 4 + k], seed_hit_layer[s * 4 + k], 0.f);
+      seeds[e].push_back(t);
+    }
+  }
+  std::vector<std::unique_ptr<RefBuilder>> builders(n_ev);
+  std::vector<std::unique_ptr<MkJob>> jobs(n_ev);
+  for (int e = 0; e < n_ev; ++e) {
+    builders[e].reset(new RefBuilder);
+    jobs[e].reset(new MkJob({Config::TrkInfo, itconf, *eohs[e], nullptr}));
+  }
+  double best = 1e30;
+  for (int r = 0; r < std::max(1, repeat); ++r) {
+    const double t0 = now_s();
+    tbb::parallel_for(tbb::blocked_range<int>(0, n_ev, 1), [&](const tbb::blocked_range<int>& rg) {
+      for (int e = rg.begin(); e < rg.end(); ++e) {
+        builders[e]->begin_event(jobs[e].get(), nullptr, "ref_find_batch");
+        builders[e]->find_tracks_load_seeds(seeds[e]);
+        builders[e]->FindTracksCloneEngine();
+      }
+    });
+    best = std::min(best, now_s() - t0);
+  }
+  if (best_seconds) *best_seconds = best;
+  std::fill(n_cands, n_cands + NS, 0);
+  for (int e = 0; e < n_ev; ++e) {
+    EventOfCombCandidates& eocc = builders[e]->eocc();
+    for (int i = 0; i < eocc.m_size; ++i) {
+      CombCandidate& cc = eocc[i];
+      if (cc.empty()) continue;
+      const int s = cc.front().label();
+      n_cands[s] = std::min((int)cc.size(), max_cands);
+      const TrackCand& tc = cc.front();
+      best_nfound[s] = tc.nFoundHits();
+      best_ntot[s] = tc.nTotalHits();
+      Track t = tc.exportTrack(false);
+      const int nh = std::min(t.nTotalHits(), Config::nMaxTrkHits);
+      for (int k = 0; k < Config::nMaxTrkHits; ++k) {
+        best_hit_idx[s * Config::nMaxTrkHits + k] = k < nh ? t.getHitIdx(k) : -100;
+        best_hit_lyr[s * Config::nMaxTrkHits + k] = k < nh ? t.getHitLyr(k) : -100;
+      }
+    }
+    builders[e]->end_event();
+  }
+  return 0;
+}
