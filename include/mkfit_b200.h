@@ -220,6 +220,9 @@ int mkfg_find_run_graph(mkfg_context* ctx);
  * number of layer-plan steps. No reference counterpart. */
 int mkfg_find_work(mkfg_context* ctx, int64_t* active_cands, int64_t* hit_pairs,
                    int64_t* updates, int32_t* steps);
+/* Diagnostics of the last mkfg_find_work call: chi2 evaluations counted by
+ * the chi2 kernel, seed-steps handled by the clone kernel. */
+int mkfg_find_work_detail(mkfg_context* ctx, int64_t* chi2_evals, int64_t* seeds_cloned);
 int mkfg_find_download(mkfg_context* ctx, int32_t n_seeds, mkfg_find_out* out);
 int mkfg_find_event(mkfg_context* ctx, const mkfg_event* ev, mkfg_find_out* out);
 

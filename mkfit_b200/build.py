@@ -30,8 +30,11 @@ def _newer(dst, srcs):
     return any(os.path.getmtime(s) > t for s in srcs)
 
 
-def build(verbose=False, extra_flags=()):
-    os.makedirs(OBJ_DIR, exist_ok=True)
+def build(verbose=False, extra_flags=(), out_dir=None):
+    """Compiles csrc/ into OUT_DIR (or out_dir, for variant builds)."""
+    lib = LIB if out_dir is None else os.path.join(out_dir, "libmkfit_b200.so")
+    obj_dir = OBJ_DIR if out_dir is None else os.path.join(out_dir, "obj")
+    os.makedirs(obj_dir, exist_ok=True)
     gen = os.path.join(CSRC, "generated_ops.cuh")
     if _newer(gen, [os.path.join(CSRC, "gen_ops.py")]):
         subprocess.check_call([sys.executable, os.path.join(CSRC, "gen_ops.py")])
@@ -39,7 +42,7 @@ def build(verbose=False, extra_flags=()):
         glob.glob(os.path.join(HERE, "..", "include", "*.h"))
     objs = []
     for src in sorted(glob.glob(os.path.join(CSRC, "*.cc"))):
-        obj = os.path.join(OBJ_DIR, os.path.basename(src)[:-3] + "_host.o")
+        obj = os.path.join(obj_dir, os.path.basename(src)[:-3] + "_host.o")
         objs.append(obj)
         if _newer(obj, [src] + headers):
             cmd = [os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-fPIC", "-c", src, "-o", obj]
@@ -47,17 +50,17 @@ def build(verbose=False, extra_flags=()):
                 print(" ".join(cmd))
             subprocess.check_call(cmd)
     for src in sorted(glob.glob(os.path.join(CSRC, "*.cu"))):
-        obj = os.path.join(OBJ_DIR, os.path.basename(src)[:-3] + ".o")
+        obj = os.path.join(obj_dir, os.path.basename(src)[:-3] + ".o")
         objs.append(obj)
         if _newer(obj, [src] + headers):
             cmd = [NVCC] + ARCH + FLAGS + list(extra_flags) + ["-c", src, "-o", obj]
             if verbose:
                 print(" ".join(cmd))
             subprocess.check_call(cmd)
-    if _newer(LIB, objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+    if _newer(lib, objs):
+        cmd = [NVCC] + ARCH + ["-shared", "-o", lib] + objs + ["-lcudart"]
         subprocess.check_call(cmd)
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":

@@ -8,7 +8,7 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_lib", "libmkfit_b200.so")
+LIB_PATH = os.environ.get("MKFIT_B200_LIB", os.path.join(HERE, "_lib", "libmkfit_b200.so"))
 HEADER_PATH = os.path.join(HERE, "..", "include", "mkfit_b200.h")
 
 MKFG_OK = 0

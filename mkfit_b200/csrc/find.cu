@@ -154,6 +154,7 @@ __global__ void __launch_bounds__(kBlock) k_chi2(EventDev E, const FindConfigDev
                                                  int step) {
   const FindConfigDev& C = *Cp;
   const int n_pairs = E.pair_count[step];
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&E.work[step * 4 + 2], n_pairs);
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n_pairs; p += gridDim.x * blockDim.x) {
     const int code = E.pairs[p];
     const int slot = code / kMaxXHits, h = code % kMaxXHits;
@@ -336,6 +337,7 @@ __global__ void __launch_bounds__(kBlock) k_clone(EventDev E, const FindConfigDe
     }
   }
 
+  if (lane == 0) atomicAdd(&E.work[step * 4 + 3], 1);
   if (n_valid == 0) {
     // hitsForSeed empty (CandCloner.cc:163-172).
     if (state != kFinding) return;
@@ -684,10 +686,23 @@ __global__ void k_export(EventDev E, FindOutDev O) {
     O.n_cands[label] = min(n, O.m);
     O.region[label] = E.region[s];
   }
-  if (c >= n) return;
+  const int o = label * O.m + c;
+  if (c >= n) {
+    // Unused slot: defined contents (zeros, empty hit list).
+    for (int e = 0; e < 6; ++e) O.par[o * 6 + e] = 0.f;
+    for (int e = 0; e < 21; ++e) O.err[o * 21 + e] = 0.f;
+    O.chg[o] = 0;
+    O.chi2[o] = 0.f;
+    O.score[o] = 0.f;
+    O.nfound[o] = O.ntot[o] = O.noverlap[o] = O.ninside[o] = O.ntail[o] = 0;
+    for (int k = 0; k < kExportHits; ++k) {
+      O.hit_idx[o * kExportHits + k] = -100;
+      O.hit_lyr[o * kExportHits + k] = -100;
+    }
+    return;
+  }
   const CandSoA& B = E.cand[E.cur[s]];
   const int slot = s * kSlots + c;
-  const int o = label * O.m + c;
   for (int e = 0; e < 6; ++e) O.par[o * 6 + e] = B.par[e * B.cap + slot];
   for (int e = 0; e < 21; ++e) O.err[o * 21 + e] = B.err[e * B.cap + slot];
   O.chg[o] = B.chg[slot];
@@ -732,6 +747,7 @@ struct Finder {
   int n_events = 0;
   int events_loaded = 0;
   cudaGraphExec_t graph = nullptr;  // captured run sequence of the current upload
+  int64_t last_chi2_evals = 0, last_seeds_cloned = 0;
   void drop_graph() {
     if (graph) cudaGraphExecDestroy(graph);
     graph = nullptr;
@@ -1290,12 +1306,16 @@ extern "C" int mkfg_find_work(mkfg_context* ctx, int64_t* active_cands, int64_t*
   MKFG_CUDA_TRY(cudaMemcpyAsync(work.data(), f->ev.work, 4 * work.size(), cudaMemcpyDeviceToHost, ctx->stream));
   MKFG_CUDA_TRY(cudaMemcpyAsync(pairs.data(), f->ev.pair_count, 4 * pairs.size(), cudaMemcpyDeviceToHost, ctx->stream));
   MKFG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-  int64_t a = 0, p = 0, u = 0;
+  int64_t a = 0, p = 0, u = 0, p2 = 0, cs = 0;
   for (int i = 0; i < ns; ++i) {
     a += work[4 * i];
     u += work[4 * i + 1];
+    p2 += work[4 * i + 2];
+    cs += work[4 * i + 3];
     p += pairs[i];
   }
+  f->last_chi2_evals = p2;
+  f->last_seeds_cloned = cs;
   if (active_cands) *active_cands = a;
   if (hit_pairs) *hit_pairs = p;
   if (updates) *updates = u;
@@ -1347,5 +1367,16 @@ extern "C" int mkfg_prepare_event_host(const mkfg_find_config* cfg, const mkfg_e
     if (seed_order) std::copy(so.order.begin(), so.order.end(), seed_order);
     if (seed_region) std::copy(so.region.begin(), so.region.end(), seed_region);
   }
+  return MKFG_OK;
+}
+
+// Diagnostic counters of the last mkfg_find_work call: chi2 evaluations seen
+// by the chi2 kernel and seed-steps handled by the clone kernel.
+extern "C" int mkfg_find_work_detail(mkfg_context* ctx, int64_t* chi2_evals, int64_t* seeds_cloned) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  Finder* f = finder_of(ctx);
+  if (chi2_evals) *chi2_evals = f->last_chi2_evals;
+  if (seeds_cloned) *seeds_cloned = f->last_seeds_cloned;
   return MKFG_OK;
 }

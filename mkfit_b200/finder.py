@@ -44,6 +44,7 @@ def _bind(lib):
     lib.mkfg_find_run_graph.argtypes = [vp]
     i64p = ctypes.POINTER(ctypes.c_int64)
     lib.mkfg_find_work.argtypes = [vp, i64p, i64p, i64p, ctypes.POINTER(ctypes.c_int32)]
+    lib.mkfg_find_work_detail.argtypes = [vp, i64p, i64p]
     lib.mkfg_find_download.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(MkfgFindOut)]
     lib.mkfg_find_event.argtypes = [vp, ctypes.POINTER(MkfgEvent), ctypes.POINTER(MkfgFindOut)]
     lib.mkfg_prepare_event_host.argtypes = [ctypes.POINTER(MkfgFindConfig),
@@ -170,7 +171,10 @@ class Finder:
         st = ctypes.c_int32()
         capi.check(self.lib.mkfg_find_work(self.ctx.handle, ctypes.byref(a), ctypes.byref(p),
                                            ctypes.byref(u), ctypes.byref(st)))
-        return dict(active_cands=a.value, hit_pairs=p.value, updates=u.value, steps=st.value)
+        e, c = ctypes.c_int64(), ctypes.c_int64()
+        capi.check(self.lib.mkfg_find_work_detail(self.ctx.handle, ctypes.byref(e), ctypes.byref(c)))
+        return dict(active_cands=a.value, hit_pairs=p.value, updates=u.value, steps=st.value,
+                    chi2_evals=e.value, seed_steps=c.value)
 
     def download(self, n_seeds):
         o = output_arrays(n_seeds, self.cfg.max_cands)
