@@ -215,6 +215,19 @@ int mkfg_find_run(mkfg_context* ctx);
 /* The same sequence captured once per upload into a CUDA graph and
  * replayed (one graph launch per call). No reference counterpart. */
 int mkfg_find_run_graph(mkfg_context* ctx);
+/* Fused form of the same run: one launch in which every thread block carries
+ * seeds_per_block consecutive seeds (4, 8 or 16; 0 = the value chosen by
+ * mkfg_find_autotune, 16 before any tuning) through all layer steps and the
+ * final merge, with the step scratch in shared memory. Same candidates and
+ * hit lists as mkfg_find_run; candidate states agree to FP32 rounding (the
+ * shared step code may be contracted into FMAs differently). No reference
+ * counterpart. */
+int mkfg_find_run_fused(mkfg_context* ctx, int32_t seeds_per_block);
+/* Times mkfg_find_run_fused on the uploaded events for every supported
+ * seeds_per_block, keeps the fastest for later calls with 0, and returns it
+ * with its time per run in milliseconds (either pointer may be NULL).
+ * Leaves the outputs of a completed run. No reference counterpart. */
+int mkfg_find_autotune(mkfg_context* ctx, int32_t* seeds_per_block, float* ms_per_run);
 /* Work done by the last run (for FLOP accounting): candidate propagations
  * to a layer, (candidate, hit) chi2 evaluations, Kalman updates, and the
  * number of layer-plan steps. No reference counterpart. */

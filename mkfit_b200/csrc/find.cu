@@ -14,6 +14,7 @@
 // then one merge launch (MergeCandsAndBestShortOne) and one export launch.
 #include "internal.h"
 #include "find_host.h"
+#include "find_fused.cuh"
 #include "find_steps.cuh"
 
 #include <algorithm>
@@ -39,39 +40,20 @@ __global__ void __launch_bounds__(kBlock) k_prep(EventDev E, const FindConfigDev
   const int lane = threadIdx.x & 31;
   const unsigned grp = 0xffu << (lane & ~7);
 
-  int reg = 0, layer = -1, prev_layer = -1, state = kFinished, ncand = 0, buf = 0;
+  int reg = 0, layer = -1, state = kFinished, ncand = 0, buf = 0;
   if (in_range) {
     reg = E.region[s];
     layer = plan_layer(C, reg, step);
-    prev_layer = layer >= 0 ? C.plan[reg][C.pickup[reg] + step - 1] : -1;
-    state = E.state[s];
+    state = wake_seed(C, reg, layer, step, E.state[s], E.pickup_layer[s]);
     ncand = E.n_cands[s];
     buf = E.cur[s];
-    // find_tracks_unroll_candidates (mkFit/MkBuilder.cc:1503-1566).
-    if (layer >= 0 && state == kDormant && E.pickup_layer[s] == prev_layer) state = kFinding;
   }
   const int slot = s * kSlots + c;
   const CandSoA& B = E.cand[buf];
-  bool active = false;
   float par[6], err[21];
   int chg = 0;
-  if (in_range && layer >= 0 && state == kFinding && c < ncand) {
-    const int last = B.last[slot];
-    if (hot_index(node_hot_of(E, s, last)) != -2) {
-      load_state(B, slot, par, err);
-      chg = B.chg[slot];
-      active = true;
-      const float pt = fabsf(1.f / par[3]);
-      if (pt < 1.2f) {
-        const float dphi = fabsf(f_atan2(par[1], par[0]) - par[4]);
-        if (par[0] * par[0] + par[1] * par[1] > 625.f && dphi > 1.371f && dphi < 4.512f) {
-          B.last[slot] = arena_append(E, s, -2, layer, 0.f, last);
-          B.nmiss[slot] += 1;
-          active = false;
-        }
-      }
-    }
-  }
+  const bool active = in_range && layer >= 0 && state == kFinding && c < ncand &&
+                      activate_cand(E, B, s, slot, layer, par, err, chg);
   const unsigned act = __ballot_sync(0xffffffffu, active) & grp;
   {
     const unsigned all = __ballot_sync(0xffffffffu, active);
@@ -83,67 +65,36 @@ __global__ void __launch_bounds__(kBlock) k_prep(EventDev E, const FindConfigDev
   }
   if (!in_range) return;
 
-  // Default: no records for this slot.
   const size_t rbase = (size_t)s * kRecPerSeed + c * kRecPerCand;
-  int xs = 0, wsr = kWsrOutside, extra = 0;
+  PrepOut o;
   if (active) {
     const LayerDev& L = C.layer[layer];
-    float ppar[6], perr[21];
-    if (L.is_barrel)
-      propagate_to_r(par, err, chg, L.propagate_to, C.inter_pflags, C.mat, false, ppar, perr);
-    else
-      propagate_to_z(par, err, chg, L.propagate_to, C.inter_pflags, C.mat, false, ppar, perr);
     const int ev = E.seed_event[s];
-    const int hit_base = E.layer_begin[ev * E.lb_stride + layer];
     const int stride = E.cand[0].cap;
-    xs = select_hits(E, L, E.bins + (size_t)ev * E.n_bins, hit_base, ppar, perr, E.xhit + slot,
-                     stride, wsr);
-    // find_tracks_handle_missed_layers (mkFit/MkBuilder.cc:1568-1637).
-    const float cand_r = hypot_f(ppar[0], ppar[1]);
-    if (L.is_barrel && cand_r < L.rin) {
-      xs = 0;
-      wsr = kWsrOutside;
-      extra = (reg == 2) ? 2 : 1;
-      if (extra == 2)
-        E.extra_last[slot] = arena_append(E, s, -2, layer, 0.f, B.last[slot]);
-    } else if (wsr == kWsrOutside) {
-      extra = 1;
-    }
+    prep_cand(E, C, L, E.bins + (size_t)ev * E.n_bins + L.bin_offset,
+              E.layer_begin[ev * E.lb_stride + layer], reg, layer, s, B, slot, par, err, chg,
+              E.xhit + slot, stride, o);
+    if (o.extra == 2) E.extra_last[slot] = o.extra_last;
 #pragma unroll
-    for (int e = 0; e < 6; ++e) E.ppar[e * stride + slot] = ppar[e];
+    for (int e = 0; e < 6; ++e) E.ppar[e * stride + slot] = o.ppar[e];
 #pragma unroll
-    for (int e = 0; e < 21; ++e) E.perr[e * stride + slot] = perr[e];
-    // Hole record (MkFinder::FindCandidatesCloneEngine, :1245-1283).
-    if (wsr != kWsrOutside) {
-      const int nin = B.ninside[slot], ntl = B.ntail[slot];
-      int fake = ((nin + ntl) < C.max_holes && ntl < C.max_consec_holes) ? -1 : -2;
-      if (wsr == kWsrEdge) fake = -3;
-      const int nfound = B.nfound[slot], nover = B.nover[slot];
-      const int ntail_rec = fake == -1 ? ntl + 1 : ntl;
-      const float pt = fabsf(1.0f / ppar[3]);
-      const float chi2 = B.chi2[slot];
-      const size_t r = rbase + kMaxXHits;
-      E.rhit[r] = fake;
-      E.rmodule[r] = -1;
-      E.rcounts[r] = nfound | (ntail_rec << 8) | (nover << 16) | (nin << 24);
-      E.rpt[r] = pt;
-      E.rchi2[r] = chi2;
-      E.rchi2hit[r] = 0.f;
-      E.rscore[r] = score_struct(nfound, ntail_rec, nover, nin, chi2, pt);
-    } else {
-      E.rhit[rbase + kMaxXHits] = kRecInvalid;
+    for (int e = 0; e < 21; ++e) E.perr[e * stride + slot] = o.perr[e];
+    if (o.xs > 0) {
+      const int base = atomicAdd(&E.pair_count[step], o.xs);
+      for (int h = 0; h < o.xs; ++h) E.pairs[base + h] = slot * kMaxXHits + h;
     }
-    if (xs > 0) {
-      const int base = atomicAdd(&E.pair_count[step], xs);
-      for (int h = 0; h < xs; ++h) E.pairs[base + h] = slot * kMaxXHits + h;
-    }
-  } else {
-    E.rhit[rbase + kMaxXHits] = kRecInvalid;
   }
-  for (int h = 0; h < kMaxXHits; ++h)
-    if (h >= xs) E.rhit[rbase + h] = kRecInvalid;
-  E.xsize[slot] = active ? xs : 0;
-  E.wsr[slot] = wsr | (extra << 8);
+  const size_t r = rbase + kMaxXHits;
+  if (o.hole) {
+    E.rhit[r] = o.hole_hit;
+    E.rmodule[r] = -1;
+    E.rchi2hit[r] = 0.f;
+    E.rscore[r] = o.hole_score;
+  } else {
+    E.rhit[r] = kRecInvalid;
+  }
+  for (int h = o.xs; h < kMaxXHits; ++h) E.rhit[rbase + h] = kRecInvalid;
+  E.wsr[slot] = o.wsr | (o.extra << 8);
 }
 
 //------------------------------------------------------------------------------
@@ -159,8 +110,7 @@ __global__ void __launch_bounds__(kBlock) k_chi2(EventDev E, const FindConfigDev
     const int code = E.pairs[p];
     const int slot = code / kMaxXHits, h = code % kMaxXHits;
     const int s = slot / kSlots, c = slot % kSlots;
-    const int reg = E.region[s];
-    const int layer = plan_layer(C, reg, step);
+    const int layer = plan_layer(C, E.region[s], step);
     const LayerDev& L = C.layer[layer];
     const int stride = E.cand[0].cap;
     float ppar[6], perr[21];
@@ -169,54 +119,20 @@ __global__ void __launch_bounds__(kBlock) k_chi2(EventDev E, const FindConfigDev
 #pragma unroll
     for (int e = 0; e < 21; ++e) perr[e] = E.perr[e * stride + slot];
     const CandSoA& B = E.cand[E.cur[s]];
-    const int chg = B.chg[slot];
     const int hidx = E.xhit[h * stride + slot];
     const int g = E.layer_begin[E.seed_event[s] * E.lb_stride + layer] + hidx;
-    float mpos[3], merr[6];
-#pragma unroll
-    for (int e = 0; e < 3; ++e) mpos[e] = __ldg(E.hpos + e * E.hstride + g);
-#pragma unroll
-    for (int e = 0; e < 6; ++e) merr[e] = __ldg(E.herr + e * E.hstride + g);
-    const uint32_t info = __ldg(E.hinfo + g);
-
-    // kalmanPropagateAndComputeChi2[Endcap] (mkFit/KalmanUtilsMPlex.cc:518-544, 744-770).
-    float hpar[6], herr_[21];
-    float chi2;
-    if (L.is_barrel) {
-      propagate_to_r(ppar, perr, chg, hypot_f(mpos[0], mpos[1]), C.intra_pflags, C.mat, false,
-                     hpar, herr_);
-      chi2 = kalman_barrel<true, false>(hpar, herr_, mpos, merr, hpar, herr_);
-    } else {
-      propagate_to_z(ppar, perr, chg, mpos[2], C.intra_pflags, C.mat, false, hpar, herr_);
-      chi2 = kalman_endcap<true, false>(hpar, herr_, mpos, merr, hpar, herr_);
-    }
-    chi2 = fabsf(chi2);
+    float chi2, score;
+    int module;
     const size_t r = (size_t)s * kRecPerSeed + c * kRecPerCand + h;
-    bool ok = chi2 < dynamic_chi2_cut(L, C.chi2_cut_min, ppar);
-    if (ok && !L.is_pix) {
-      ok = strip_q_compatible(L.is_barrel, perr, hpar, mpos, merr);
-      ok &= strip_charge_ok(L.is_barrel, info >> 12, hpar, merr);
-    }
-    const int nfound = B.nfound[slot];
-    if (ok && L.is_pix) {
-      // Seed-hit layer check on the first (seed) nodes of the arena.
-      for (int i = 0; i <= nfound && i <= 2; ++i)
-        if (hot_layer(node_hot_of(E, s, i)) == layer) ok = false;
-    }
-    if (!ok) {
+    if (eval_pair(E, C, L, layer, s, g, ppar, perr, B.chg[slot], B.nfound[slot], B.nover[slot],
+                  B.ninside[slot] + B.ntail[slot], B.chi2[slot], chi2, score, module)) {
+      E.rhit[r] = hidx;
+      E.rmodule[r] = module;
+      E.rchi2hit[r] = chi2;
+      E.rscore[r] = score;
+    } else {
       E.rhit[r] = kRecInvalid;
-      continue;
     }
-    const int nover = B.nover[slot], nholes = B.ninside[slot] + B.ntail[slot];
-    const float pt = fabsf(1.0f / ppar[3]);
-    const float tchi2 = B.chi2[slot] + chi2;
-    E.rhit[r] = hidx;
-    E.rmodule[r] = info & 0xfff;
-    E.rcounts[r] = (nfound + 1) | (0 << 8) | (nover << 16) | (nholes << 24);
-    E.rpt[r] = pt;
-    E.rchi2[r] = tchi2;
-    E.rchi2hit[r] = chi2;
-    E.rscore[r] = score_struct(nfound + 1, 0, nover, nholes, tchi2, pt);
   }
 }
 
@@ -224,298 +140,32 @@ __global__ void __launch_bounds__(kBlock) k_chi2(EventDev E, const FindConfigDev
 // Kernel 3: per-seed candidate cloning (CandCloner::ProcessSeedRange,
 // mkFit/CandCloner.cc:36-189). One warp per seed.
 //------------------------------------------------------------------------------
-struct NewCand {
-  int parent;    // slot offset (0..7) in the current buffer, or 8 + extra slot
-  int hit;       // added hit index (or hole code)
-  float chi2hit;
-  int ov;        // overlap: match index 0/1 in the parent's pair, or -1
-  float score;
-  int is_extra;  // 1: held-back copy (extra), 2: extra with a stop (-2) node
-};
-
-__device__ __forceinline__ void copy_slot(const CandSoA& from, int fs, const CandSoA& to, int ts) {
-#pragma unroll
-  for (int e = 0; e < 6; ++e) to.par[e * to.cap + ts] = from.par[e * from.cap + fs];
-#pragma unroll
-  for (int e = 0; e < 21; ++e) to.err[e * to.cap + ts] = from.err[e * from.cap + fs];
-  to.chg[ts] = from.chg[fs];
-  to.chi2[ts] = from.chi2[fs];
-  to.score[ts] = from.score[fs];
-  to.last[ts] = from.last[fs];
-  to.nfound[ts] = from.nfound[fs];
-  to.nmiss[ts] = from.nmiss[fs];
-  to.nover[ts] = from.nover[fs];
-  to.ninside[ts] = from.ninside[fs];
-  to.ntail[ts] = from.ntail[fs];
-}
-
-// TrackCand::addHitIdx counters (mkFit/HitStructures.h:714-735).
-__device__ __forceinline__ void add_hit_counts(int hit, float chi2, int& nfound, int& nmiss,
-                                               int& ninside, int& ntail, float& tchi2) {
-  if (hit >= 0 || hit == -9) {
-    ++nfound;
-    tchi2 += chi2;
-    ninside += ntail;
-    ntail = 0;
-  } else {
-    ++nmiss;
-    if (hit == -1) ++ntail;
-  }
-}
-
 __global__ void __launch_bounds__(kBlock) k_clone(EventDev E, const FindConfigDev* __restrict__ Cp,
                                                   int step) {
   const FindConfigDev& C = *Cp;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  const int s = warp;
+  __shared__ HitMatchPair s_hm[kBlock / 32][kSlots];
   if (s >= E.n_seeds) return;
-  const int reg = E.region[s];
-  const int layer = plan_layer(C, reg, step);
+  const int layer = plan_layer(C, E.region[s], step);
   if (layer < 0) return;
   const int state = E.state[s];
   if (state == kDormant) return;
-  const int ncand = E.n_cands[s];
   const int cur = E.cur[s];
-  const CandSoA& B = E.cand[cur];
-  const CandSoA& N = E.cand[cur ^ 1];
-  const size_t rb = (size_t)s * kRecPerSeed;
-  const int M = C.max_cands;
-
-  // Overlap candidates per parent (CandCloner consults them in :120-124);
-  // filled in hit order as MkFinder does (:1212-1216).
-  __shared__ HitMatchPair s_hm[kBlock / 32][kSlots];
-  HitMatchPair* hm = s_hm[threadIdx.x >> 5];
-  if (lane < kSlots) {
-    HitMatchPair p;
-    p.reset();
-    if (lane < ncand) {
-      for (int h = 0; h < kMaxXHits; ++h) {
-        const size_t r = rb + lane * kRecPerCand + h;
-        const int hit = E.rhit[r];
-        if (hit == kRecInvalid) continue;
-        const float c2 = E.rchi2hit[r];
-        if (c2 < C.chi2_cut_overlap) p.consider(hit, E.rmodule[r], c2);
-      }
-    }
-    hm[lane] = p;
-  }
-  __syncwarp();
-
-  // Valid records: up to kRecPerSeed, held 5 per lane.
-  constexpr int kPer = (kRecPerSeed + 31) / 32;
-  float sc[kPer];
-  bool valid[kPer];
-  int n_valid = 0;
-#pragma unroll
-  for (int k = 0; k < kPer; ++k) {
-    const int idx = lane + 32 * k;
-    valid[k] = false;
-    sc[k] = 0.f;
-    if (idx < kRecPerSeed) {
-      const int c = idx / kRecPerCand;
-      if (c < ncand && E.rhit[rb + idx] != kRecInvalid) {
-        valid[k] = true;
-        sc[k] = E.rscore[rb + idx];
-      }
-    }
-    n_valid += __popc(__ballot_sync(0xffffffffu, valid[k]));
-  }
-
-  // Extras (held-back candidates) in candidate order (MkBuilder.cc:1600-1626).
-  int extras[kSlots];
-  int extra_kind[kSlots];
-  int n_extras = 0;
-  if (state == kFinding) {
-    for (int c = 0; c < ncand; ++c) {
-      const int k = E.wsr[s * kSlots + c] >> 8;
-      if (k) {
-        extras[n_extras] = c;
-        extra_kind[n_extras] = k;
-        ++n_extras;
-      }
-    }
-  }
-
   if (lane == 0) atomicAdd(&E.work[step * 4 + 3], 1);
-  if (n_valid == 0) {
-    // hitsForSeed empty (CandCloner.cc:163-172).
-    if (state != kFinding) return;
-    for (int i = 0; i < n_extras; ++i) {
-      const int c = extras[i];
-      const int src = s * kSlots + c, dst = s * kSlots + i;
-      for (int f = lane; f < 37; f += 32) {
-        if (f < 6) N.par[f * N.cap + dst] = B.par[f * B.cap + src];
-        else if (f < 27) N.err[(f - 6) * N.cap + dst] = B.err[(f - 6) * B.cap + src];
-      }
-      if (lane == 0) {
-        N.chg[dst] = B.chg[src];
-        N.chi2[dst] = B.chi2[src];
-        N.score[dst] = B.score[src];
-        N.nfound[dst] = B.nfound[src];
-        N.nover[dst] = B.nover[src];
-        N.ninside[dst] = B.ninside[src];
-        N.ntail[dst] = B.ntail[src];
-        if (extra_kind[i] == 2) {
-          N.last[dst] = E.extra_last[src];
-          N.nmiss[dst] = B.nmiss[src] + 1;
-        } else {
-          N.last[dst] = B.last[src];
-          N.nmiss[dst] = B.nmiss[src];
-        }
-        E.upd[dst] = 0;
-      }
-    }
-    if (lane == 0) {
-      E.n_cands[s] = n_extras;
-      E.cur[s] = cur ^ 1;
-    }
-    return;
-  }
-
-  // Top-num_hits records in (score desc, record index asc) order: the
-  // reference's std::sort by score; on exact score ties this order is the
-  // stable one.
-  const int num_hits = min(n_valid, M);
-  int top[kSlots];
-  for (int i = 0; i < num_hits; ++i) {
-    float best = -INFINITY;
-    int bidx = INT_MAX;
-#pragma unroll
-    for (int k = 0; k < kPer; ++k) {
-      const int idx = lane + 32 * k;
-      if (valid[k] && (sc[k] > best || (sc[k] == best && idx < bidx))) {
-        best = sc[k];
-        bidx = idx;
-      }
-    }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      const float ob = __shfl_xor_sync(0xffffffffu, best, off);
-      const int oi = __shfl_xor_sync(0xffffffffu, bidx, off);
-      if (ob > best || (ob == best && oi < bidx)) {
-        best = ob;
-        bidx = oi;
-      }
-    }
-    top[i] = bidx;
-#pragma unroll
-    for (int k = 0; k < kPer; ++k)
-      if (lane + 32 * k == bidx) valid[k] = false;
-  }
-
-  // Build the new candidate list (sequential logic of ProcessSeedRange).
-  NewCand nc[kSlots];
-  int n_pushed = 0;
-  int ei = 0;
-  float bs_score = E.bshort_valid[s] ? E.bshort.score[s] : -1e16f;  // getScoreWorstPossible
-  int bs_from = -1;
-  for (int ih = 0; ih < num_hits; ++ih) {
-    const int idx = top[ih];
-    const size_t r = rb + idx;
-    const int parent = idx / kRecPerCand;
-    const int hit = E.rhit[r];
-    const float score = E.rscore[r];
-    if (hit == -2) {
-      if (score > bs_score) {
-        bs_score = score;
-        bs_from = idx;
-      }
-      continue;
-    }
-    while (ei < n_extras && E.cand[cur].score[s * kSlots + extras[ei]] > score && n_pushed < M) {
-      nc[n_pushed++] = NewCand{extras[ei], 0, 0.f, -1, 0.f, extra_kind[ei]};
-      ++ei;
-    }
-    if (n_pushed >= M) break;
-    int ov = -1;
-    const float ppt = fabsf(1.f / B.par[3 * B.cap + s * kSlots + parent]);
-    if (ppt > C.pt_cut_overlap && hit >= 0) ov = hm[parent].find(hit, E.rmodule[r]);
-    nc[n_pushed++] = NewCand{parent, hit, E.rchi2hit[r], ov, score, 0};
-  }
-  while (ei < n_extras && n_pushed < M) {
-    nc[n_pushed++] = NewCand{extras[ei], 0, 0.f, -1, 0.f, extra_kind[ei]};
-    ++ei;
-  }
-
-  // Best short candidate (a -2 record scoring above the current best).
-  if (bs_from >= 0) {
-    const int parent = bs_from / kRecPerCand;
-    const int src = s * kSlots + parent;
-    for (int f = lane; f < 27; f += 32) {
-      if (f < 6) E.bshort.par[f * E.bshort.cap + s] = B.par[f * B.cap + src];
-      else E.bshort.err[(f - 6) * E.bshort.cap + s] = B.err[(f - 6) * B.cap + src];
-    }
-    if (lane == 0) {
-      int nfound = B.nfound[src], nmiss = B.nmiss[src], nin = B.ninside[src], ntl = B.ntail[src];
-      float chi2 = B.chi2[src];
-      add_hit_counts(-2, 0.f, nfound, nmiss, nin, ntl, chi2);
-      E.bshort.last[s] = arena_append(E, s, -2, layer, 0.f, B.last[src]);
-      E.bshort.chg[s] = B.chg[src];
-      E.bshort.chi2[s] = chi2;
-      E.bshort.score[s] = bs_score;
-      E.bshort.nfound[s] = nfound;
-      E.bshort.nmiss[s] = nmiss;
-      E.bshort.nover[s] = B.nover[src];
-      E.bshort.ninside[s] = nin;
-      E.bshort.ntail[s] = ntl;
-      E.bshort_valid[s] = 1;
-    }
-  }
-
-  // Materialize the new candidates into the other buffer.
-  for (int i = 0; i < n_pushed; ++i) {
-    const NewCand& n = nc[i];
-    const int src = s * kSlots + n.parent, dst = s * kSlots + i;
-    for (int f = lane; f < 27; f += 32) {
-      if (f < 6) N.par[f * N.cap + dst] = B.par[f * B.cap + src];
-      else N.err[(f - 6) * N.cap + dst] = B.err[(f - 6) * B.cap + src];
-    }
-    if (lane == 0) {
-      int nfound = B.nfound[src], nmiss = B.nmiss[src], nin = B.ninside[src], ntl = B.ntail[src];
-      int nover = B.nover[src];
-      float chi2 = B.chi2[src];
-      int last = B.last[src];
-      float score = B.score[src];
-      int upd = 0;
-      if (n.is_extra) {
-        if (n.is_extra == 2) {
-          last = E.extra_last[src];
-          ++nmiss;
-        }
-      } else {
-        add_hit_counts(n.hit, n.chi2hit, nfound, nmiss, nin, ntl, chi2);
-        last = arena_append(E, s, n.hit, layer, n.chi2hit, last);
-        score = n.score;
-        if (n.ov >= 0) {
-          const HitMatchPair& p = hm[n.parent];
-          add_hit_counts(p.hit[n.ov], p.chi2[n.ov], nfound, nmiss, nin, ntl, chi2);
-          last = arena_append(E, s, p.hit[n.ov], layer, p.chi2[n.ov], last);
-          ++nover;
-        }
-        upd = n.hit >= 0;
-      }
-      N.chg[dst] = B.chg[src];
-      N.chi2[dst] = chi2;
-      N.score[dst] = score;
-      N.last[dst] = last;
-      N.nfound[dst] = nfound;
-      N.nmiss[dst] = nmiss;
-      N.nover[dst] = nover;
-      N.ninside[dst] = nin;
-      N.ntail[dst] = ntl;
-      E.upd[dst] = upd;
-    }
-  }
-  if (lane == 0) {
-    E.n_cands[s] = n_pushed;
+  const size_t rb = (size_t)s * kRecPerSeed;
+  const SeedRecords R{E.rhit + rb,          E.rscore + rb,           E.rchi2hit + rb,
+                        E.rmodule + rb,       E.wsr + s * kSlots,      E.extra_last + s * kSlots,
+                        E.upd + s * kSlots};
+  const int n = clone_seed(E, C, s, layer, state, E.n_cands[s], cur, R, s_hm[threadIdx.x >> 5], lane);
+  if (n >= 0 && lane == 0) {
+    E.n_cands[s] = n;
     E.cur[s] = cur ^ 1;
   }
 }
 
 //------------------------------------------------------------------------------
-// Kernel 4: UpdateWithLastHit + CopyOutParErr (mkFit/MkFinder.cc:1291-1335,
-// kalmanPropagateAndUpdate[Endcap], mkFit/KalmanUtilsMPlex.cc:471-505, 697-731).
+// Kernel 4: UpdateWithLastHit + CopyOutParErr for candidates that took a hit.
 //------------------------------------------------------------------------------
 __global__ void __launch_bounds__(kBlock) k_update(EventDev E, const FindConfigDev* __restrict__ Cp,
                                                    int step) {
@@ -523,44 +173,13 @@ __global__ void __launch_bounds__(kBlock) k_update(EventDev E, const FindConfigD
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int s = t / kSlots, c = t % kSlots;
   if (s >= E.n_seeds) return;
-  const int reg = E.region[s];
-  const int layer = plan_layer(C, reg, step);
-  if (layer < 0) return;
+  if (plan_layer(C, E.region[s], step) < 0) return;
   if (c >= E.n_cands[s]) return;
   const int slot = s * kSlots + c;
   if (!E.upd[slot]) return;
   E.upd[slot] = 0;
   atomicAdd(&E.work[step * 4 + 1], 1);
-  const CandSoA& B = E.cand[E.cur[s]];
-  float par[6], err[21];
-  load_state(B, slot, par, err);
-  int chg = B.chg[slot];
-  const int hv = node_hot_of(E, s, B.last[slot]);
-  const int hl = hot_layer(hv);
-  // After an arena overflow (reported through err_flags) the last node may
-  // not be a hit: skip rather than read outside the hit arrays.
-  if (hot_index(hv) < 0 || hl < 0 || hl >= C.n_layers) return;
-  const int g = E.layer_begin[E.seed_event[s] * E.lb_stride + hl] + hot_index(hv);
-  float mpos[3], merr[6];
-#pragma unroll
-  for (int e = 0; e < 3; ++e) mpos[e] = __ldg(E.hpos + e * E.hstride + g);
-#pragma unroll
-  for (int e = 0; e < 6; ++e) merr[e] = __ldg(E.herr + e * E.hstride + g);
-  const LayerDev& L = C.layer[hl];
-  float ppar[6], perr[21];
-  if (L.is_barrel) {
-    propagate_to_r(par, err, chg, hypot_f(mpos[0], mpos[1]), C.inter_pflags, C.mat, false, ppar, perr);
-    kalman_barrel<false, true>(ppar, perr, mpos, merr, par, err);
-  } else {
-    propagate_to_z(par, err, chg, mpos[2], C.inter_pflags, C.mat, false, ppar, perr);
-    kalman_endcap<false, true>(ppar, perr, mpos, merr, par, err);
-  }
-  if (par[3] < 0) {
-    chg = -chg;
-    par[3] = -par[3];
-  }
-  store_state(B, slot, par, err);
-  B.chg[slot] = chg;
+  update_cand(E, C, s, E.layer_begin + E.seed_event[s] * E.lb_stride, E.cand[E.cur[s]], slot);
 }
 
 //------------------------------------------------------------------------------
@@ -585,74 +204,14 @@ __global__ void k_reset(EventDev E, int n_work) {
 }
 
 //------------------------------------------------------------------------------
-// Kernel 5: CombCandidate::MergeCandsAndBestShortOne (update_score, sort)
-// (mkFit/HitStructures.cc:511-552). One thread per seed.
+// Kernel 5: CombCandidate::MergeCandsAndBestShortOne (one thread per seed).
 //------------------------------------------------------------------------------
-__device__ __forceinline__ float cand_score(const CandSoA& B, int slot) {
-  const float pt = fabsf(1.f / B.par[3 * B.cap + slot]);
-  float chi2 = B.chi2[slot];
-  if (chi2 < 0) chi2 = 0.f;
-  return score_calc(B.nfound[slot], 0, B.nover[slot], B.ninside[slot], chi2, pt, false);
-}
-
 __global__ void k_merge(EventDev E, const FindConfigDev* __restrict__ Cp) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= E.n_seeds) return;
-  const FindConfigDev& C = *Cp;
   const int cur = E.cur[s];
-  const CandSoA& B = E.cand[cur];
-  const CandSoA& N = E.cand[cur ^ 1];
-  int n = E.n_cands[s];
-  float score[kSlots + 1];
-  int order[kSlots + 1];
-  for (int c = 0; c < n; ++c) {
-    score[c] = cand_score(B, s * kSlots + c);
-    order[c] = c;
-  }
-  // Insertion sort by score, descending (std::sort on <= 16 elements).
-  for (int i = 1; i < n; ++i) {
-    const int o = order[i];
-    const float v = score[o];
-    int j = i;
-    while (j > 0 && score[order[j - 1]] < v) {
-      order[j] = order[j - 1];
-      --j;
-    }
-    order[j] = o;
-  }
-  const bool has_bs = E.bshort_valid[s];
-  float bs = has_bs ? cand_score(E.bshort, s) : 0.f;
-  int ins = -1;  // position of the best short candidate in the final list
-  if (n > 0) {
-    if (has_bs && bs > score[order[n - 1]]) {
-      int ci = 0;
-      while (score[order[ci]] > bs) ++ci;
-      if (n >= C.max_cands) --n;
-      ins = ci;
-    }
-  } else if (has_bs) {
-    ins = 0;
-  }
-  // Write the final list into the other buffer: sorted cands with the
-  // best short one inserted.
-  int w = 0;
-  for (int i = 0; i <= n; ++i) {
-    if (i == ins) {
-      const int dst = s * kSlots + w;
-      copy_slot(E.bshort, s, N, dst);
-      N.score[dst] = bs;
-      ++w;
-    }
-    if (i == n) break;
-    const int src = s * kSlots + order[i];
-    const int dst = s * kSlots + w;
-    copy_slot(B, src, N, dst);
-    N.score[dst] = score[order[i]];
-    ++w;
-  }
-  E.n_cands[s] = w;
+  E.n_cands[s] = merge_seed(E, *Cp, s, E.n_cands[s], cur);
   E.cur[s] = cur ^ 1;
-  E.bshort_valid[s] = 0;
 }
 
 //------------------------------------------------------------------------------
@@ -747,6 +306,7 @@ struct Finder {
   int n_events = 0;
   int events_loaded = 0;
   cudaGraphExec_t graph = nullptr;  // captured run sequence of the current upload
+  int fused_w = 16;                 // seeds per block of the fused form
   int64_t last_chi2_evals = 0, last_seeds_cloned = 0;
   void drop_graph() {
     if (graph) cudaGraphExecDestroy(graph);
@@ -1026,7 +586,6 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     char* p = f->scratch.as<char>();
     f->ev.ppar = carve<float>(p, 6 * (size_t)SC);
     f->ev.perr = carve<float>(p, 21 * (size_t)SC);
-    f->ev.xsize = carve<int>(p, SC);
     f->ev.xhit = carve<int>(p, (size_t)kMaxXHits * SC);
     f->ev.wsr = carve<int>(p, SC);
     f->ev.extra_last = carve<int>(p, SC);
@@ -1038,15 +597,12 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   }
   {
     const size_t nrec = (size_t)SS * kRecPerSeed;
-    if ((rc = f->recs.ensure(rounded(4 * nrec) * 7 + 4096))) return rc;
+    if ((rc = f->recs.ensure(rounded(4 * nrec) * 4 + 4096))) return rc;
     char* p = f->recs.as<char>();
     f->ev.rscore = carve<float>(p, nrec);
-    f->ev.rchi2 = carve<float>(p, nrec);
     f->ev.rchi2hit = carve<float>(p, nrec);
-    f->ev.rpt = carve<float>(p, nrec);
     f->ev.rhit = carve<int>(p, nrec);
     f->ev.rmodule = carve<int>(p, nrec);
-    f->ev.rcounts = carve<int>(p, nrec);
   }
   {
     const size_t nn = (size_t)SS * hot_cap;
@@ -1168,6 +724,31 @@ static int enqueue_run(Finder* f, cudaStream_t st) {
   k_merge<<<(S + 127) / 128, 128, 0, st>>>(f->ev, f->d_cfg);
   MKFG_CUDA_TRY(cudaGetLastError());
   return MKFG_OK;
+}
+
+template <int W>
+static int launch_fused(Finder* f, cudaStream_t st) {
+  const int smem = (int)sizeof(FusedShared<W>);
+  MKFG_CUDA_TRY(cudaFuncSetAttribute(k_find_fused<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  const int grid = (f->n_seeds + W - 1) / W;
+  k_find_fused<W><<<grid, W * kSlots, smem, st>>>(f->ev, f->d_cfg);
+  MKFG_CUDA_TRY(cudaGetLastError());
+  return MKFG_OK;
+}
+
+// Reset + one fused launch (all layer steps and the merge).
+static int enqueue_fused(Finder* f, cudaStream_t st, int w) {
+  const int S = f->n_seeds;
+  const int n_work = 4 * (f->host_cfg.max_steps + 2);
+  const int grid_c = (S * kSlots + kBlock - 1) / kBlock;
+  k_reset<<<std::max(grid_c, (n_work + kBlock - 1) / kBlock), kBlock, 0, st>>>(f->ev, n_work);
+  MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.pair_count, 0, 4 * (size_t)(f->host_cfg.max_steps + 2), st));
+  switch (w) {
+    case 4: return launch_fused<4>(f, st);
+    case 8: return launch_fused<8>(f, st);
+    case 16: return launch_fused<16>(f, st);
+    default: return set_error(MKFG_ERR_BAD_INPUT, "seeds_per_block must be 4, 8 or 16 (got %d)", w);
+  }
 }
 
 static int run_plain(mkfg_context* ctx, Finder* f) {
@@ -1293,6 +874,58 @@ extern "C" int mkfg_find_run_graph(mkfg_context* ctx) {
   Finder* f = finder_of(ctx);
   MKFG_REQUIRE(f->configured && f->events_loaded, "no event uploaded");
   return run_graph(ctx, f);
+}
+
+extern "C" int mkfg_find_run_fused(mkfg_context* ctx, int32_t seeds_per_block) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  Finder* f = finder_of(ctx);
+  MKFG_REQUIRE(f->configured && f->events_loaded, "no event uploaded");
+  if (f->n_seeds == 0) return MKFG_OK;
+  return enqueue_fused(f, ctx->stream, seeds_per_block ? seeds_per_block : f->fused_w);
+}
+
+extern "C" int mkfg_find_autotune(mkfg_context* ctx, int32_t* seeds_per_block, float* ms_per_run) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  Finder* f = finder_of(ctx);
+  MKFG_REQUIRE(f->configured && f->events_loaded, "no event uploaded");
+  float best_ms = 0.f;
+  int best_w = f->fused_w;
+  if (f->n_seeds > 0) {
+    cudaStream_t st = ctx->stream;
+    cudaEvent_t e0, e1;
+    MKFG_CUDA_TRY(cudaEventCreate(&e0));
+    MKFG_CUDA_TRY(cudaEventCreate(&e1));
+    best_ms = -1.f;
+    for (int w : {4, 8, 16}) {
+      if ((rc = enqueue_fused(f, st, w))) break;  // warm-up
+      if (cudaEventRecord(e0, st) != cudaSuccess) { rc = set_error(MKFG_ERR_CUDA, "event record"); break; }
+      for (int i = 0; i < 2 && !rc; ++i) rc = enqueue_fused(f, st, w);
+      if (rc) break;
+      if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) {
+        rc = set_error(MKFG_ERR_CUDA, "event timing failed");
+        break;
+      }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      ms *= 0.5f;
+      if (best_ms < 0.f || ms < best_ms) {
+        best_ms = ms;
+        best_w = w;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    f->fused_w = best_w;
+    // Leave the outputs of a completed run of the chosen configuration.
+    if ((rc = enqueue_fused(f, st, best_w))) return rc;
+    MKFG_CUDA_TRY(cudaStreamSynchronize(st));
+  }
+  if (seeds_per_block) *seeds_per_block = best_w;
+  if (ms_per_run) *ms_per_run = best_ms;
+  return MKFG_OK;
 }
 
 extern "C" int mkfg_find_work(mkfg_context* ctx, int64_t* active_cands, int64_t* hit_pairs,

@@ -100,19 +100,15 @@ struct EventDev {
   // Step scratch per candidate slot.
   float* ppar;     // [6][S*kSlots] state propagated to the layer
   float* perr;     // [21][S*kSlots]
-  int* xsize;      // XHitSize (-1: outside)
   int* xhit;       // [kMaxXHits][S*kSlots] hit index within layer
   int* wsr;        // WSR code | extra kind << 8
   int* extra_last; // arena node of the held-back copy (kind 2)
   int* upd;        // needs UpdateWithLastHit (per slot of the new buffer)
   // Records (IdxChi2List) per seed: kRecPerSeed slots.
   float* rscore;
-  float* rchi2;
   float* rchi2hit;
-  float* rpt;
   int* rhit;       // kRecInvalid when the slot holds no record
   int* rmodule;
-  int* rcounts;    // nhits | ntailholes << 8 | noverlaps << 16 | nholes << 24
   // (cand slot, hit) pairs for the chi2 pass.
   int* pairs;
   int* pair_count; // [max_steps + 1]

@@ -93,11 +93,12 @@ __device__ __forceinline__ int phi_bin(float phi) {
 __device__ __forceinline__ float cdist(float a) { return a > kPI ? kTwoPI - a : a; }
 
 // SelectHitIndices for one candidate (mkFit/MkFinder.cc:227-684) including
-// the sensitive-region test (TrackerInfo.h:118-138). Writes up to 16 hit
+// the sensitive-region test (TrackerInfo.h:118-138). `bins` is the layer's
+// (q bin, phi bin) table of the candidate's event. Writes up to 16 hit
 // indices (index within layer) in bin-scan order; returns XHitSize (-1 when
 // outside the layer) and the WSR code.
 __device__ __forceinline__ int select_hits(const EventDev& E, const LayerDev& L,
-                                           const uint32_t* __restrict__ ev_bins, int hit_base,
+                                           const uint32_t* __restrict__ bins, int hit_base,
                                            const float (&par)[6],
                                            const float (&err)[21], int* xhit, int xstride,
                                            int& wsr) {
@@ -155,7 +156,6 @@ __device__ __forceinline__ int select_hits(const EventDev& E, const LayerDev& L,
   const int pb2 = phi_bin(phi + dphi) + 1;
 
   int n = 0;
-  const uint32_t* bins = ev_bins + L.bin_offset;
   for (int qi = qb1; qi < qb2; ++qi) {
     for (int pi = pb1; pi < pb2; ++pi) {
       const int pb = pi & 0xff;
@@ -251,5 +251,521 @@ struct HitMatchPair {
     return hit[1] >= 0 ? 1 : -1;
   }
 };
+
+}  // namespace mkfg
+
+namespace mkfg {
+
+//------------------------------------------------------------------------------
+// Shared step implementations (plain kernels and the fused persistent kernel)
+//------------------------------------------------------------------------------
+
+struct NewCand {
+  int parent;    // candidate slot (0..7) the new candidate copies
+  int hit;       // added hit index (or hole code)
+  float chi2hit;
+  int ov;        // overlap: match index 0/1 in the parent's pair, or -1
+  float score;
+  int is_extra;  // 1: held-back copy (extra), 2: extra with a stop (-2) node
+};
+
+__device__ __forceinline__ void copy_slot(const CandSoA& from, int fs, const CandSoA& to, int ts) {
+#pragma unroll
+  for (int e = 0; e < 6; ++e) to.par[e * to.cap + ts] = from.par[e * from.cap + fs];
+#pragma unroll
+  for (int e = 0; e < 21; ++e) to.err[e * to.cap + ts] = from.err[e * from.cap + fs];
+  to.chg[ts] = from.chg[fs];
+  to.chi2[ts] = from.chi2[fs];
+  to.score[ts] = from.score[fs];
+  to.last[ts] = from.last[fs];
+  to.nfound[ts] = from.nfound[fs];
+  to.nmiss[ts] = from.nmiss[fs];
+  to.nover[ts] = from.nover[fs];
+  to.ninside[ts] = from.ninside[fs];
+  to.ntail[ts] = from.ntail[fs];
+}
+
+// TrackCand::addHitIdx counters (mkFit/HitStructures.h:714-735).
+__device__ __forceinline__ void add_hit_counts(int hit, float chi2, int& nfound, int& nmiss,
+                                               int& ninside, int& ntail, float& tchi2) {
+  if (hit >= 0 || hit == -9) {
+    ++nfound;
+    tchi2 += chi2;
+    ninside += ntail;
+    ntail = 0;
+  } else {
+    ++nmiss;
+    if (hit == -1) ++ntail;
+  }
+}
+
+// Seed state at the start of layer-plan step `step`: a dormant seed starts
+// finding at the step after its pickup layer (find_tracks_unroll_candidates,
+// mkFit/MkBuilder.cc:1503-1566).
+__device__ __forceinline__ int wake_seed(const FindConfigDev& C, int reg, int layer, int step,
+                                         int state, int pickup_layer) {
+  if (layer >= 0 && state == kDormant && pickup_layer == C.plan[reg][C.pickup[reg] + step - 1])
+    return kFinding;
+  return state;
+}
+
+// Output of the candidate preparation of one layer step.
+struct PrepOut {
+  bool active = false;  // candidate takes part in this layer
+  int xs = 0;           // XHitSize
+  int wsr = kWsrOutside;
+  int extra = 0;        // held back: 1 plain copy, 2 copy with a stop node
+  int extra_last = -1;  // arena node of the stop node (extra == 2)
+  bool hole = false;    // a hole record was produced
+  int hole_hit = 0;
+  float hole_score = 0.f;
+  float ppar[6];
+  float perr[21];
+};
+
+// Unroll + looper stop (mkFit/MkBuilder.cc:1503-1566) for a candidate of a
+// seed already in Finding state; returns whether it is active.
+__device__ __forceinline__ bool activate_cand(const EventDev& E, const CandSoA& B, int s, int slot,
+                                              int layer, float (&par)[6], float (&err)[21],
+                                              int& chg) {
+  const int last = B.last[slot];
+  if (hot_index(node_hot_of(E, s, last)) == -2) return false;
+  load_state(B, slot, par, err);
+  chg = B.chg[slot];
+  const float pt = fabsf(1.f / par[3]);
+  if (pt < 1.2f) {
+    const float dphi = fabsf(f_atan2(par[1], par[0]) - par[4]);
+    if (par[0] * par[0] + par[1] * par[1] > 625.f && dphi > 1.371f && dphi < 4.512f) {
+      B.last[slot] = arena_append(E, s, -2, layer, 0.f, last);
+      B.nmiss[slot] += 1;
+      return false;
+    }
+  }
+  return true;
+}
+
+// Propagation to the layer, SelectHitIndices, missed-layer handling
+// (mkFit/MkBuilder.cc:1568-1637) and the hole record (MkFinder.cc:1245-1283)
+// for an active candidate. xhit receives up to 16 indices with stride xstride.
+__device__ __forceinline__ void prep_cand(const EventDev& E, const FindConfigDev& C,
+                                          const LayerDev& L, const uint32_t* layer_bins,
+                                          int hit_base, int reg, int layer, int s, const CandSoA& B,
+                                          int slot, const float (&par)[6], const float (&err)[21],
+                                          int chg, int* xhit, int xstride, PrepOut& o) {
+  if (L.is_barrel)
+    propagate_to_r(par, err, chg, L.propagate_to, C.inter_pflags, C.mat, false, o.ppar, o.perr);
+  else
+    propagate_to_z(par, err, chg, L.propagate_to, C.inter_pflags, C.mat, false, o.ppar, o.perr);
+  o.active = true;
+  o.xs = select_hits(E, L, layer_bins, hit_base, o.ppar, o.perr, xhit, xstride, o.wsr);
+  const float cand_r = hypot_f(o.ppar[0], o.ppar[1]);
+  if (L.is_barrel && cand_r < L.rin) {
+    o.xs = 0;
+    o.wsr = kWsrOutside;
+    o.extra = (reg == 2) ? 2 : 1;
+    if (o.extra == 2) o.extra_last = arena_append(E, s, -2, layer, 0.f, B.last[slot]);
+  } else if (o.wsr == kWsrOutside) {
+    o.extra = 1;
+  }
+  if (o.xs < 0) o.xs = 0;
+  if (o.wsr != kWsrOutside) {
+    const int nin = B.ninside[slot], ntl = B.ntail[slot];
+    int fake = ((nin + ntl) < C.max_holes && ntl < C.max_consec_holes) ? -1 : -2;
+    if (o.wsr == kWsrEdge) fake = -3;
+    const int ntail_rec = fake == -1 ? ntl + 1 : ntl;
+    const float pt = fabsf(1.0f / o.ppar[3]);
+    o.hole = true;
+    o.hole_hit = fake;
+    o.hole_score = score_struct(B.nfound[slot], ntail_rec, B.nover[slot], nin, B.chi2[slot], pt);
+  }
+}
+
+// One (candidate, hit) evaluation (MkFinder::FindCandidatesCloneEngine,
+// mkFit/MkFinder.cc:1142-1240, with kalmanPropagateAndComputeChi2[Endcap]).
+// Returns whether the hit is accepted; fills chi2, score, module.
+__device__ __forceinline__ bool eval_pair(const EventDev& E, const FindConfigDev& C,
+                                          const LayerDev& L, int layer, int s, int g,
+                                          const float (&ppar)[6], const float (&perr)[21], int chg,
+                                          int nfound, int nover, int nholes, float cand_chi2,
+                                          float& chi2_out, float& score_out, int& module_out) {
+  float mpos[3], merr[6];
+#pragma unroll
+  for (int e = 0; e < 3; ++e) mpos[e] = __ldg(E.hpos + e * E.hstride + g);
+#pragma unroll
+  for (int e = 0; e < 6; ++e) merr[e] = __ldg(E.herr + e * E.hstride + g);
+  const uint32_t info = __ldg(E.hinfo + g);
+  float hpar[6], herr_[21];
+  float chi2;
+  if (L.is_barrel) {
+    propagate_to_r(ppar, perr, chg, hypot_f(mpos[0], mpos[1]), C.intra_pflags, C.mat, false, hpar,
+                   herr_);
+    chi2 = kalman_barrel<true, false>(hpar, herr_, mpos, merr, hpar, herr_);
+  } else {
+    propagate_to_z(ppar, perr, chg, mpos[2], C.intra_pflags, C.mat, false, hpar, herr_);
+    chi2 = kalman_endcap<true, false>(hpar, herr_, mpos, merr, hpar, herr_);
+  }
+  chi2 = fabsf(chi2);
+  bool ok = chi2 < dynamic_chi2_cut(L, C.chi2_cut_min, ppar);
+  if (ok && !L.is_pix) {
+    ok = strip_q_compatible(L.is_barrel, perr, hpar, mpos, merr);
+    ok &= strip_charge_ok(L.is_barrel, info >> 12, hpar, merr);
+  }
+  if (ok && L.is_pix) {
+    // Seed-hit layer check on the first (seed) nodes of the arena.
+    for (int i = 0; i <= nfound && i <= 2; ++i)
+      if (hot_layer(node_hot_of(E, s, i)) == layer) ok = false;
+  }
+  if (!ok) return false;
+  const float pt = fabsf(1.0f / ppar[3]);
+  const float tchi2 = cand_chi2 + chi2;
+  chi2_out = chi2;
+  module_out = info & 0xfff;
+  score_out = score_struct(nfound + 1, 0, nover, nholes, tchi2, pt);
+  return true;
+}
+
+// UpdateWithLastHit + CopyOutParErr for one candidate (mkFit/MkFinder.cc:
+// 1291-1335; kalmanPropagateAndUpdate[Endcap], KalmanUtilsMPlex.cc:471-505,
+// 697-731). Returns false if the last node is not a hit.
+__device__ __forceinline__ bool update_cand(const EventDev& E, const FindConfigDev& C, int s,
+                                            const int* lb, const CandSoA& B, int slot) {
+  float par[6], err[21];
+  load_state(B, slot, par, err);
+  int chg = B.chg[slot];
+  const int hv = node_hot_of(E, s, B.last[slot]);
+  const int hl = hot_layer(hv);
+  // After an arena overflow (reported through err_flags) the last node may
+  // not be a hit: skip rather than read outside the hit arrays.
+  if (hot_index(hv) < 0 || hl < 0 || hl >= C.n_layers) return false;
+  const int g = lb[hl] + hot_index(hv);
+  float mpos[3], merr[6];
+#pragma unroll
+  for (int e = 0; e < 3; ++e) mpos[e] = __ldg(E.hpos + e * E.hstride + g);
+#pragma unroll
+  for (int e = 0; e < 6; ++e) merr[e] = __ldg(E.herr + e * E.hstride + g);
+  const LayerDev& L = C.layer[hl];
+  float ppar[6], perr[21];
+  if (L.is_barrel) {
+    propagate_to_r(par, err, chg, hypot_f(mpos[0], mpos[1]), C.inter_pflags, C.mat, false, ppar, perr);
+    kalman_barrel<false, true>(ppar, perr, mpos, merr, par, err);
+  } else {
+    propagate_to_z(par, err, chg, mpos[2], C.inter_pflags, C.mat, false, ppar, perr);
+    kalman_endcap<false, true>(ppar, perr, mpos, merr, par, err);
+  }
+  if (par[3] < 0) {
+    chg = -chg;
+    par[3] = -par[3];
+  }
+  store_state(B, slot, par, err);
+  B.chg[slot] = chg;
+  return true;
+}
+
+// Records and per-candidate step results of one seed, wherever they live
+// (global memory in the plain form, shared memory in the fused form).
+struct SeedRecords {
+  const int* hit_;
+  const float* score_;
+  const float* chi2hit_;
+  const int* module_;
+  const int* wsr_;         // WSR code | extra kind << 8, per candidate
+  const int* extra_last_;  // stop node of a kind-2 extra, per candidate
+  int* upd_;               // per new candidate: needs UpdateWithLastHit
+  __device__ bool valid(int idx, int ncand) const {
+    return idx / kRecPerCand < ncand && hit_[idx] != kRecInvalid;
+  }
+  __device__ int hit(int idx) const { return hit_[idx]; }
+  __device__ float score(int idx) const { return score_[idx]; }
+  __device__ float chi2hit(int idx) const { return chi2hit_[idx]; }
+  __device__ int module(int idx) const { return module_[idx]; }
+  __device__ int extra_kind(int c) const { return wsr_[c] >> 8; }
+  __device__ int extra_last(int c) const { return extra_last_[c]; }
+  __device__ void set_upd(int i, int v) const { upd_[i] = v; }
+};
+
+// CandCloner::ProcessSeedRange for one seed (mkFit/CandCloner.cc:36-189),
+// executed by one warp. Returns the new candidate count, or -1 when the
+// seed's candidates are unchanged.
+__device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev& C, int s,
+                                          int layer, int state, int ncand, int cur,
+                                          const SeedRecords& R, HitMatchPair* hm, int lane) {
+  const CandSoA& B = E.cand[cur];
+  const CandSoA& N = E.cand[cur ^ 1];
+  const int M = C.max_cands;
+
+  // Overlap candidates per parent (consulted at CandCloner.cc:120-124),
+  // filled in hit order as MkFinder does (:1212-1216).
+  if (lane < kSlots) {
+    HitMatchPair p;
+    p.reset();
+    if (lane < ncand) {
+      for (int h = 0; h < kMaxXHits; ++h) {
+        const int idx = lane * kRecPerCand + h;
+        if (!R.valid(idx, ncand)) continue;
+        const float c2 = R.chi2hit(idx);
+        if (c2 < C.chi2_cut_overlap) p.consider(R.hit(idx), R.module(idx), c2);
+      }
+    }
+    hm[lane] = p;
+  }
+  __syncwarp();
+
+  constexpr int kPer = (kRecPerSeed + 31) / 32;
+  float sc[kPer];
+  bool valid[kPer];
+  int n_valid = 0;
+#pragma unroll
+  for (int k = 0; k < kPer; ++k) {
+    const int idx = lane + 32 * k;
+    valid[k] = idx < kRecPerSeed && R.valid(idx, ncand);
+    sc[k] = valid[k] ? R.score(idx) : 0.f;
+    n_valid += __popc(__ballot_sync(0xffffffffu, valid[k]));
+  }
+
+  // Extras (held-back candidates) in candidate order (MkBuilder.cc:1600-1626).
+  int extras[kSlots];
+  int extra_kind[kSlots];
+  int n_extras = 0;
+  if (state == kFinding) {
+    for (int c = 0; c < ncand; ++c) {
+      const int k = R.extra_kind(c);
+      if (k) {
+        extras[n_extras] = c;
+        extra_kind[n_extras] = k;
+        ++n_extras;
+      }
+    }
+  }
+
+  if (n_valid == 0) {
+    // hitsForSeed empty (CandCloner.cc:163-172).
+    if (state != kFinding) return -1;
+    for (int i = 0; i < n_extras; ++i) {
+      const int src = s * kSlots + extras[i], dst = s * kSlots + i;
+      for (int f = lane; f < 27; f += 32) {
+        if (f < 6) N.par[f * N.cap + dst] = B.par[f * B.cap + src];
+        else N.err[(f - 6) * N.cap + dst] = B.err[(f - 6) * B.cap + src];
+      }
+      if (lane == 0) {
+        N.chg[dst] = B.chg[src];
+        N.chi2[dst] = B.chi2[src];
+        N.score[dst] = B.score[src];
+        N.nfound[dst] = B.nfound[src];
+        N.nover[dst] = B.nover[src];
+        N.ninside[dst] = B.ninside[src];
+        N.ntail[dst] = B.ntail[src];
+        if (extra_kind[i] == 2) {
+          N.last[dst] = R.extra_last(extras[i]);
+          N.nmiss[dst] = B.nmiss[src] + 1;
+        } else {
+          N.last[dst] = B.last[src];
+          N.nmiss[dst] = B.nmiss[src];
+        }
+        R.set_upd(i, 0);
+      }
+    }
+    return n_extras;
+  }
+
+  // Top-num_hits records in (score desc, record index asc) order: the
+  // reference's std::sort by score; on exact score ties this order is the
+  // stable one.
+  const int num_hits = min(n_valid, M);
+  int top[kSlots];
+  for (int i = 0; i < num_hits; ++i) {
+    float best = -INFINITY;
+    int bidx = INT_MAX;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      const int idx = lane + 32 * k;
+      if (valid[k] && (sc[k] > best || (sc[k] == best && idx < bidx))) {
+        best = sc[k];
+        bidx = idx;
+      }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const float ob = __shfl_xor_sync(0xffffffffu, best, off);
+      const int oi = __shfl_xor_sync(0xffffffffu, bidx, off);
+      if (ob > best || (ob == best && oi < bidx)) {
+        best = ob;
+        bidx = oi;
+      }
+    }
+    top[i] = bidx;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k)
+      if (lane + 32 * k == bidx) valid[k] = false;
+  }
+
+  // Build the new candidate list (sequential logic of ProcessSeedRange).
+  NewCand nc[kSlots];
+  int n_pushed = 0;
+  int ei = 0;
+  float bs_score = E.bshort_valid[s] ? E.bshort.score[s] : -1e16f;  // getScoreWorstPossible
+  int bs_from = -1;
+  for (int ih = 0; ih < num_hits; ++ih) {
+    const int idx = top[ih];
+    const int parent = idx / kRecPerCand;
+    const int hit = R.hit(idx);
+    const float score = R.score(idx);
+    if (hit == -2) {
+      if (score > bs_score) {
+        bs_score = score;
+        bs_from = idx;
+      }
+      continue;
+    }
+    while (ei < n_extras && B.score[s * kSlots + extras[ei]] > score && n_pushed < M) {
+      nc[n_pushed++] = NewCand{extras[ei], 0, 0.f, -1, 0.f, extra_kind[ei]};
+      ++ei;
+    }
+    if (n_pushed >= M) break;
+    int ov = -1;
+    const float ppt = fabsf(1.f / B.par[3 * B.cap + s * kSlots + parent]);
+    if (ppt > C.pt_cut_overlap && hit >= 0) ov = hm[parent].find(hit, R.module(idx));
+    nc[n_pushed++] = NewCand{parent, hit, R.chi2hit(idx), ov, score, 0};
+  }
+  while (ei < n_extras && n_pushed < M) {
+    nc[n_pushed++] = NewCand{extras[ei], 0, 0.f, -1, 0.f, extra_kind[ei]};
+    ++ei;
+  }
+
+  // Best short candidate (a -2 record scoring above the current best).
+  if (bs_from >= 0) {
+    const int parent = bs_from / kRecPerCand;
+    const int src = s * kSlots + parent;
+    for (int f = lane; f < 27; f += 32) {
+      if (f < 6) E.bshort.par[f * E.bshort.cap + s] = B.par[f * B.cap + src];
+      else E.bshort.err[(f - 6) * E.bshort.cap + s] = B.err[(f - 6) * B.cap + src];
+    }
+    if (lane == 0) {
+      int nfound = B.nfound[src], nmiss = B.nmiss[src], nin = B.ninside[src], ntl = B.ntail[src];
+      float chi2 = B.chi2[src];
+      add_hit_counts(-2, 0.f, nfound, nmiss, nin, ntl, chi2);
+      E.bshort.last[s] = arena_append(E, s, -2, layer, 0.f, B.last[src]);
+      E.bshort.chg[s] = B.chg[src];
+      E.bshort.chi2[s] = chi2;
+      E.bshort.score[s] = bs_score;
+      E.bshort.nfound[s] = nfound;
+      E.bshort.nmiss[s] = nmiss;
+      E.bshort.nover[s] = B.nover[src];
+      E.bshort.ninside[s] = nin;
+      E.bshort.ntail[s] = ntl;
+      E.bshort_valid[s] = 1;
+    }
+  }
+
+  // Materialize the new candidates into the other buffer.
+  for (int i = 0; i < n_pushed; ++i) {
+    const NewCand& n = nc[i];
+    const int src = s * kSlots + n.parent, dst = s * kSlots + i;
+    for (int f = lane; f < 27; f += 32) {
+      if (f < 6) N.par[f * N.cap + dst] = B.par[f * B.cap + src];
+      else N.err[(f - 6) * N.cap + dst] = B.err[(f - 6) * B.cap + src];
+    }
+    if (lane == 0) {
+      int nfound = B.nfound[src], nmiss = B.nmiss[src], nin = B.ninside[src], ntl = B.ntail[src];
+      int nover = B.nover[src];
+      float chi2 = B.chi2[src];
+      int last = B.last[src];
+      float score = B.score[src];
+      int upd = 0;
+      if (n.is_extra) {
+        if (n.is_extra == 2) {
+          last = R.extra_last(n.parent);
+          ++nmiss;
+        }
+      } else {
+        add_hit_counts(n.hit, n.chi2hit, nfound, nmiss, nin, ntl, chi2);
+        last = arena_append(E, s, n.hit, layer, n.chi2hit, last);
+        score = n.score;
+        if (n.ov >= 0) {
+          const HitMatchPair& p = hm[n.parent];
+          add_hit_counts(p.hit[n.ov], p.chi2[n.ov], nfound, nmiss, nin, ntl, chi2);
+          last = arena_append(E, s, p.hit[n.ov], layer, p.chi2[n.ov], last);
+          ++nover;
+        }
+        upd = n.hit >= 0;
+      }
+      N.chg[dst] = B.chg[src];
+      N.chi2[dst] = chi2;
+      N.score[dst] = score;
+      N.last[dst] = last;
+      N.nfound[dst] = nfound;
+      N.nmiss[dst] = nmiss;
+      N.nover[dst] = nover;
+      N.ninside[dst] = nin;
+      N.ntail[dst] = ntl;
+      R.set_upd(i, upd);
+    }
+  }
+  return n_pushed;
+}
+
+// Candidate score for the final merge: getScoreCand with default arguments
+// (mkFit/HitStructures.h:519-531).
+__device__ __forceinline__ float cand_score(const CandSoA& B, int slot) {
+  const float pt = fabsf(1.f / B.par[3 * B.cap + slot]);
+  float chi2 = B.chi2[slot];
+  if (chi2 < 0) chi2 = 0.f;
+  return score_calc(B.nfound[slot], 0, B.nover[slot], B.ninside[slot], chi2, pt, false);
+}
+
+// CombCandidate::MergeCandsAndBestShortOne(update_score, sort_cands)
+// (mkFit/HitStructures.cc:511-552) for one seed; writes the final list into
+// buffer cur ^ 1 and returns the final candidate count.
+__device__ __forceinline__ int merge_seed(const EventDev& E, const FindConfigDev& C, int s,
+                                          int n, int cur) {
+  const CandSoA& B = E.cand[cur];
+  const CandSoA& N = E.cand[cur ^ 1];
+  float score[kSlots + 1];
+  int order[kSlots + 1];
+  for (int c = 0; c < n; ++c) {
+    score[c] = cand_score(B, s * kSlots + c);
+    order[c] = c;
+  }
+  // Insertion sort by score, descending (std::sort on <= 16 elements).
+  for (int i = 1; i < n; ++i) {
+    const int o = order[i];
+    const float v = score[o];
+    int j = i;
+    while (j > 0 && score[order[j - 1]] < v) {
+      order[j] = order[j - 1];
+      --j;
+    }
+    order[j] = o;
+  }
+  const bool has_bs = E.bshort_valid[s];
+  const float bs = has_bs ? cand_score(E.bshort, s) : 0.f;
+  int ins = -1;
+  if (n > 0) {
+    if (has_bs && bs > score[order[n - 1]]) {
+      int ci = 0;
+      while (score[order[ci]] > bs) ++ci;
+      if (n >= C.max_cands) --n;
+      ins = ci;
+    }
+  } else if (has_bs) {
+    ins = 0;
+  }
+  int w = 0;
+  for (int i = 0; i <= n; ++i) {
+    if (i == ins) {
+      const int dst = s * kSlots + w;
+      copy_slot(E.bshort, s, N, dst);
+      N.score[dst] = bs;
+      ++w;
+    }
+    if (i == n) break;
+    const int src = s * kSlots + order[i];
+    const int dst = s * kSlots + w;
+    copy_slot(B, src, N, dst);
+    N.score[dst] = score[order[i]];
+    ++w;
+  }
+  E.bshort_valid[s] = 0;
+  return w;
+}
 
 }  // namespace mkfg

@@ -42,6 +42,9 @@ def _bind(lib):
     lib.mkfg_find_upload_batch.argtypes = [vp, ctypes.POINTER(MkfgEvent), ctypes.c_int32]
     lib.mkfg_find_run.argtypes = [vp]
     lib.mkfg_find_run_graph.argtypes = [vp]
+    lib.mkfg_find_run_fused.argtypes = [vp, ctypes.c_int32]
+    lib.mkfg_find_autotune.argtypes = [vp, ctypes.POINTER(ctypes.c_int32),
+                                       ctypes.POINTER(ctypes.c_float)]
     i64p = ctypes.POINTER(ctypes.c_int64)
     lib.mkfg_find_work.argtypes = [vp, i64p, i64p, i64p, ctypes.POINTER(ctypes.c_int32)]
     lib.mkfg_find_work_detail.argtypes = [vp, i64p, i64p]
@@ -165,6 +168,17 @@ class Finder:
 
     def run_graph(self):
         capi.check(self.lib.mkfg_find_run_graph(self.ctx.handle))
+
+    def run_fused(self, seeds_per_block=0):
+        """One launch for all layer steps; seeds_per_block 0 = tuned value."""
+        capi.check(self.lib.mkfg_find_run_fused(self.ctx.handle, seeds_per_block))
+
+    def autotune(self):
+        """Picks the fastest seeds_per_block on the uploaded events;
+        returns (seeds_per_block, ms per run)."""
+        w, ms = ctypes.c_int32(), ctypes.c_float()
+        capi.check(self.lib.mkfg_find_autotune(self.ctx.handle, ctypes.byref(w), ctypes.byref(ms)))
+        return w.value, ms.value
 
     def work(self):
         a, p, u = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
