@@ -122,6 +122,36 @@ int mkfg_fit(mkfg_context* ctx, const mkfg_fit_args* args);
 int mkfg_fit_host(mkfg_context* ctx, const mkfg_fit_args* args);
 
 
+/* ------------------------------------------------------ differentiable fit */
+/* Summed chi2 of a barrel fit as a function of per-step alignment and
+ * material parameters, and its gradient (hand-derived reverse mode through
+ * the Kalman update, the covariance transport, the material effects and the
+ * iterative helix propagation). No reference counterpart: the reference fit
+ * (mkFit/MkFitter.cc:505-522) is not differentiable.
+ *
+ *   fit: as for mkfg_fit (device pointers); barrel steps only
+ *     (endcap_mask 0), pflags 0 or material (2). out tracks may be NULL;
+ *     out_chi2 (optional) receives each track's chi2 sum.
+ *   theta [n_steps][3] (device): per step a = hit shift along the
+ *     transverse tangent (r-phi, cm), b = hit shift in z (cm), c = scale of
+ *     the layer's radiation length and xi (1 = nominal).
+ *   checkpoint [n_steps][27][n] (device): state entering each step, written
+ *     by the forward call and read by the backward call.
+ *   chi2_sum (device, one double): L = sum over tracks and steps of chi2. */
+typedef struct {
+  mkfg_fit_args fit;
+  const float* theta;
+  float* checkpoint;
+  double* chi2_sum;
+} mkfg_align_args;
+
+int mkfg_align_chi2_forward(mkfg_context* ctx, const mkfg_align_args* args);
+/* grad_theta [n_steps][3] (device, double) = grad_out * dL/dtheta, for the
+ * checkpoints of the last forward call with the same args; grad_out is a
+ * device scalar (the incoming adjoint of L). */
+int mkfg_align_chi2_backward(mkfg_context* ctx, const mkfg_align_args* args,
+                             const float* grad_out, double* grad_theta);
+
 /* ------------------------------------------------------------- finding */
 /* Detector geometry + finding iteration configuration. Replaces the
  * reference's TrackerInfo / IterationConfig as consumed by MkBuilder

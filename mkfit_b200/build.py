@@ -63,5 +63,43 @@ def build(verbose=False, extra_flags=(), out_dir=None):
     return lib
 
 
+EXT_SRC = os.path.join(CSRC, "torch_ext", "align_ext.cc")
+EXT_NAME = "_align_ext"
+
+
+def ext_path(out_dir=None):
+    import sysconfig
+    return os.path.join(out_dir or OUT_DIR, EXT_NAME + sysconfig.get_config_var("EXT_SUFFIX"))
+
+
+def build_torch_ext(verbose=False, out_dir=None):
+    """Compiles the PyTorch binding of the differentiable fit (an autograd
+    Function in C++ over the C ABI) next to the library."""
+    import sysconfig
+    import torch
+    lib = build(verbose=verbose, out_dir=out_dir)
+    out = ext_path(out_dir)
+    header = os.path.join(HERE, "..", "include", "mkfit_b200.h")
+    if not _newer(out, [EXT_SRC, header]):
+        return out
+    tdir = os.path.dirname(torch.__file__)
+    abi = int(torch._C._GLIBCXX_USE_CXX11_ABI)
+    cmd = [os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-fPIC", "-shared", "-Wno-interference-size",
+           "-DTORCH_EXTENSION_NAME=" + EXT_NAME, "-DTORCH_API_INCLUDE_EXTENSION_H",
+           "-D_GLIBCXX_USE_CXX11_ABI=%d" % abi,
+           "-I" + os.path.join(tdir, "include"),
+           "-I" + os.path.join(tdir, "include", "torch", "csrc", "api", "include"),
+           "-I/usr/local/cuda/include", "-I" + sysconfig.get_paths()["include"],
+           EXT_SRC, "-o", out,
+           "-L" + os.path.join(tdir, "lib"), "-lc10", "-lc10_cuda", "-ltorch", "-ltorch_cpu",
+           "-ltorch_python", "-L" + os.path.dirname(lib), "-lmkfit_b200",
+           "-Wl,-rpath," + os.path.join(tdir, "lib"), "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.check_call(cmd)
+    return out
+
+
 if __name__ == "__main__":
     print(build(verbose=True))
+    print(build_torch_ext(verbose=True))

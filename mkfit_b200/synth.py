@@ -128,13 +128,19 @@ class FitEvent:
 
 def gen_fit_event(n_tracks=20000, seed=0xC0FFEE, radii=None, pt_range=(0.5, 10.0),
                   eta_max=1.0, sig_rphi=0.01, sig_z=0.1, x_over_x0=0.01,
-                  vtx_sigma_xy=0.01, vtx_sigma_z=5.0, r_start=1.0):
+                  vtx_sigma_xy=0.01, vtx_sigma_z=5.0, r_start=1.0, align_rphi=None,
+                  align_z=None, mat_scale=None):
     """Plain Kalman-fit toy MC: pT uniform, eta uniform in [-eta_max, eta_max],
     phi uniform, charge +-1, Gaussian vertex, one hit per cylinder layer with
     Gaussian r-phi / z smearing and a Highland multiple-scattering kick of
     `x_over_x0` radiation lengths (corrected for the crossing angle) at each
     layer. The initial state is the true state at radius r_start (default
-    1 cm, outside the vertex spread); its covariance is a fixed diagonal."""
+    1 cm, outside the vertex spread); its covariance is a fixed diagonal.
+
+    Misaligned detector (differentiable-fit workload): layer l is displaced
+    by align_rphi[l] along the transverse tangent and align_z[l] in z, so the
+    recorded hit (nominal geometry) is the true one moved back by those
+    offsets; its material is mat_scale[l] times nominal (scattering kick)."""
     rng = np.random.default_rng(seed)
     if radii is None:
         radii = [4.0 * (i + 1) for i in range(10)]
@@ -180,11 +186,17 @@ def gen_fit_event(n_tracks=20000, seed=0xC0FFEE, radii=None, pt_range=(0.5, 10.0
         hpos[li, 0] = x - np.sin(pphi) * d
         hpos[li, 1] = y + np.cos(pphi) * d
         hpos[li, 2] = z + rng.normal(0.0, sig_z, n)
+        if align_rphi is not None:
+            hpos[li, 0] += np.sin(pphi) * align_rphi[li]
+            hpos[li, 1] -= np.cos(pphi) * align_rphi[li]
+        if align_z is not None:
+            hpos[li, 2] -= align_z[li]
         herr[li] = barrel_hit_errors(pphi, sig_rphi, sig_z)
         # Multiple scattering at the layer.
         p = hel.pt / np.sin(hel.theta)
         beta = p / np.sqrt(p * p + mpi * mpi)
-        t0 = highland(p, beta, x_over_x0 * p / hel.pt)
+        xl = x_over_x0 * (mat_scale[li] if mat_scale is not None else 1.0)
+        t0 = highland(p, beta, xl * p / hel.pt)
         th_new = hel.theta + rng.normal(0.0, 1.0, n) * t0
         ph_new = ph + rng.normal(0.0, 1.0, n) * t0 / np.sin(hel.theta)
         mask = np.ones(n, dtype=bool)

@@ -132,6 +132,59 @@ class Restate:
         return out_par, out_err, chi2
 
 
+def adjoint_f64_lib_path():
+    return os.path.join(REF_DIR, "libadjoint_f64.so")
+
+
+def adj_f64_grad(par, err, chg, hit_pos, hit_err, theta, rl_grid=None, xi_grid=None, material=True):
+    """FP64 host evaluation of the product's generated fit-step adjoint
+    (oracle/adjoint_f64.cc): returns (sum chi2, gradient [n_steps][3])."""
+    lib = ctypes.CDLL(adjoint_f64_lib_path())
+    f = lib.adj_f64_fit_grad
+    f.restype = None
+    n = chg.shape[0]
+    ns = hit_pos.shape[0]
+    th = np.ascontiguousarray(theta, np.float64).reshape(ns, 3)
+    rl = np.ascontiguousarray(rl_grid, np.float32) if rl_grid is not None else None
+    xi = np.ascontiguousarray(xi_grid, np.float32) if xi_grid is not None else None
+    total = ctypes.c_double()
+    grad = np.zeros((ns, 3), np.float64)
+    args = [np.ascontiguousarray(par, np.float32), np.ascontiguousarray(err, np.float32),
+            np.ascontiguousarray(chg, np.int32), np.ascontiguousarray(hit_pos, np.float32),
+            np.ascontiguousarray(hit_err, np.float32), th]
+    f(ctypes.c_int(n), ctypes.c_int(ns), *[a.ctypes.data_as(ctypes.c_void_p) for a in args],
+      rl.ctypes.data_as(ctypes.c_void_p) if rl is not None else None,
+      xi.ctypes.data_as(ctypes.c_void_p) if xi is not None else None,
+      ctypes.c_int(1 if material else 0), ctypes.byref(total),
+      grad.ctypes.data_as(ctypes.c_void_p))
+    return total.value, grad
+
+
+def restate_chi2_sum(rs, ev, theta, material=True):
+    """Sum over tracks of the FP64 restatement's fit chi2 at parameters
+    theta [n_steps][3] (r-phi shift, z shift, material scale)."""
+    th = np.asarray(theta, np.float64).reshape(-1, 3)
+    _, _, chi2 = rs.fit(ev.par, ev.err, ev.chg, ev.hit_pos, ev.hit_err, ev.rl_grid, ev.xi_grid,
+                        pflags=2 if material else 0, shift_rphi=th[:, 0].copy(),
+                        shift_z=th[:, 1].copy(), mat_scale=th[:, 2].copy())
+    return float(np.sum(chi2))
+
+
+def restate_fd_grad(rs, ev, theta, h_shift=1e-4, h_scale=1e-3, material=True):
+    """Central finite differences of restate_chi2_sum in every parameter."""
+    th = np.asarray(theta, np.float64).reshape(-1, 3)
+    g = np.zeros_like(th)
+    for s in range(th.shape[0]):
+        for j in range(3):
+            h = h_scale if j == 2 else h_shift
+            tp, tm = th.copy(), th.copy()
+            tp[s, j] += h
+            tm[s, j] -= h
+            g[s, j] = (restate_chi2_sum(rs, ev, tp, material) -
+                       restate_chi2_sum(rs, ev, tm, material)) / (2 * h)
+    return g
+
+
 def _load_find_api(lib):
     c_int_p = ctypes.POINTER(ctypes.c_int)
     lib.ref_cms2017_sizes.argtypes = [c_int_p, c_int_p, c_int_p]
