@@ -121,6 +121,20 @@ int mkfg_fit(mkfg_context* ctx, const mkfg_fit_args* args);
  * args (including hits.layer_begin) are host pointers here. */
 int mkfg_fit_host(mkfg_context* ctx, const mkfg_fit_args* args);
 
+/* Same fit from HOST buffers without allocating anything: inputs and
+ * outputs are staged through a fixed 16 MiB device array compiled into the
+ * library (a file-scope __device__ array) instead of the context's
+ * grow-only scratch; no cudaMalloc / cudaFree or allocating library call is
+ * made. Inputs whose staging exceeds 16 MiB (e.g. more than ~16k tracks x
+ * 10 layers) are rejected with MKFG_ERR_BAD_INPUT and a message giving the
+ * size; use mkfg_fit_host for them. Nothing in the array needs to start at
+ * zero. The array is shared by all callers on a device: calls on the same
+ * device must not overlap (other threads, other contexts), or they race on
+ * it. The first call on a device resolves the array's address there
+ * (cudaGetSymbolAddress, which may load the module); the call synchronizes
+ * its stream before returning. No reference counterpart. */
+int mkfg_fit_host_static(mkfg_context* ctx, const mkfg_fit_args* args);
+
 
 /* ------------------------------------------------------ differentiable fit */
 /* Summed chi2 of a barrel fit as a function of per-step alignment and

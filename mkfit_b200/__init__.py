@@ -116,6 +116,28 @@ class Context:
         return out
 
 
+    def fit_host_static(self, par, err, chg, hit_pos, hit_err, pflags=capi.PF_MATERIAL,
+                        endcap_mask=0, with_chi2=False, out=None):
+        """fit_host through mkfg_fit_host_static: staging in the library's
+        fixed device array, no allocation; same arguments and outputs."""
+        n = chg.shape[0]
+        nl = hit_pos.shape[0]
+        hp = np.ascontiguousarray(hit_pos.transpose(1, 0, 2).reshape(3, nl * n), np.float32) \
+            if hit_pos.ndim == 3 else hit_pos
+        he = np.ascontiguousarray(hit_err.transpose(1, 0, 2).reshape(6, nl * n), np.float32) \
+            if hit_err.ndim == 3 else hit_err
+        lb = np.arange(nl + 1, dtype=np.int32) * n
+        hot = np.ascontiguousarray(np.broadcast_to(np.arange(n, dtype=np.int32), (nl, n)))
+        if out is None:
+            out = dict(par=np.zeros((6, n), np.float32), err=np.zeros((21, n), np.float32),
+                       chg=np.zeros(n, np.int32), chi2=np.zeros(n, np.float32))
+        a = self._fit_args(par, err, chg, out["par"], out["err"], out["chg"], hp, he, lb, hot,
+                           np.arange(nl), n, n, nl * n, nl, endcap_mask, pflags,
+                           out["chi2"] if with_chi2 else None)
+        capi.check(self.lib.mkfg_fit_host_static(self.handle, ctypes.byref(a)))
+        return out
+
+
 class FitBuffers:
     """Device-resident fit inputs in the C-ABI layout, built from a
     synth.FitEvent (hits of all layers concatenated, track i's hit on layer

@@ -69,6 +69,7 @@ def load():
     lib.mkfg_probe_fp32_peak.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     lib.mkfg_fit.argtypes = [vp, ctypes.POINTER(MkfgFitArgs)]
     lib.mkfg_fit_host.argtypes = [vp, ctypes.POINTER(MkfgFitArgs)]
+    lib.mkfg_fit_host_static.argtypes = [vp, ctypes.POINTER(MkfgFitArgs)]
     _lib = lib
     return lib
 
