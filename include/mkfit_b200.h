@@ -272,6 +272,21 @@ int mkfg_find_run_fused(mkfg_context* ctx, int32_t seeds_per_block);
  * with its time per run in milliseconds (either pointer may be NULL).
  * Leaves the outputs of a completed run. No reference counterpart. */
 int mkfg_find_autotune(mkfg_context* ctx, int32_t* seeds_per_block, float* ms_per_run);
+/* Backward fit of every seed's best candidate after a run (plain, graph or
+ * fused): from the last layer of the seed's region plan down to plan
+ * position bkfit_last[region] (host array, NULL = 0), refit over the
+ * candidate's hits with the covariance scaled by 100, chi2 summed;
+ * parameters, covariance, chi2 and score of candidate 0 are replaced
+ * (mkfg_find_download returns them), its charge is kept. Replaces
+ * MkBuilder::BackwardFit / fit_cands (mkFit/MkBuilder.cc:2153-2253) and
+ * MkFinder::BkFitInputTracks / BkFitFitTracks / BkFitOutputTracks
+ * (mkFit/MkFinder.cc:1368-1452, 1573-1742). pflags: Config::
+ * backward_fit_pflags. group_width: the reference's Matriplex width NN
+ * (8 for its AVX2 build, 16 for AVX-512; 0 = 8) -- seeds are fitted in
+ * groups of that many, whose members share layer skips and stand-in
+ * measurements as in the reference. Synchronizes the context stream. */
+int mkfg_find_backward_fit(mkfg_context* ctx, const int32_t* bkfit_last, uint32_t pflags,
+                           int32_t group_width);
 /* Work done by the last run (for FLOP accounting): candidate propagations
  * to a layer, (candidate, hit) chi2 evaluations, Kalman updates, and the
  * number of layer-plan steps. No reference counterpart. */
@@ -281,6 +296,14 @@ int mkfg_find_work(mkfg_context* ctx, int64_t* active_cands, int64_t* hit_pairs,
  * the chi2 kernel, seed-steps handled by the clone kernel. */
 int mkfg_find_work_detail(mkfg_context* ctx, int64_t* chi2_evals, int64_t* seeds_cloned);
 int mkfg_find_download(mkfg_context* ctx, int32_t n_seeds, mkfg_find_out* out);
+/* The same export for the best candidate of every seed only (m = 1 slot
+ * per seed in every output array; n_cands[s] = 1 when the seed has a
+ * candidate): replaces MkBuilder::export_best_comb_cands
+ * (mkFit/MkBuilder.cc:348-362, called by run_OneIteration,
+ * mkFit/buildtestMPlex.cc:734). Hit lists keep the missing-hit entries
+ * (negative indices), as exportTrack(false); a caller that wants
+ * remove_missing_hits drops them. */
+int mkfg_find_download_best(mkfg_context* ctx, int32_t n_seeds, mkfg_find_out* out);
 int mkfg_find_event(mkfg_context* ctx, const mkfg_event* ev, mkfg_find_out* out);
 
 /* Host-only (no device needed): the hit-index build and seed ordering that

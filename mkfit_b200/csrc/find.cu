@@ -1,16 +1,19 @@
 // Clone-engine combinatorial track finding: device kernels and C ABI.
 //
 // Plain form (the drop-in for MkBuilder::FindTracksCloneEngine,
-// mkFit/MkBuilder.cc:1847-2058): for every layer-plan step, four launches
-//   1. prep   : seed activation, candidate unroll + low-pT looper stop,
-//               propagation to the layer, SelectHitIndices, missed-layer
-//               handling, hole records        (one thread per candidate)
-//   2. chi2   : propagate to each selected hit, chi2, strip checks,
-//               hit records                   (one thread per (cand, hit))
-//   3. clone  : per-seed ranking of the records (warp top-M selection),
-//               overlap hits, extras, best short candidate, new candidates
-//               (one warp per seed) -- CandCloner::ProcessSeedRange
-//   4. update : UpdateWithLastHit for candidates that took a hit
+// mkFit/MkBuilder.cc:1847-2058): for every layer-plan step, five launches
+//   1. activate : seed activation, candidate unroll + low-pT looper stop,
+//                 compact list of the active candidates (one thread per
+//                 candidate slot; barrel and endcap candidates listed apart)
+//   2. propagate: propagation to the layer, SelectHitIndices, missed-layer
+//                 handling, hole records (one thread per active candidate)
+//   3. chi2     : propagate to each selected hit, chi2, strip checks,
+//                 hit records (one thread per (cand, hit) pair)
+//   4. clone    : per-seed ranking of the records (warp top-M selection),
+//                 overlap hits, extras, best short candidate, new
+//                 candidates (one warp per seed) -- CandCloner::ProcessSeedRange
+//   5. update   : UpdateWithLastHit for the listed candidates that took a hit
+//                 (barrel and endcap candidates listed apart)
 // then one merge launch (MergeCandsAndBestShortOne) and one export launch.
 #include "internal.h"
 #include "find_host.h"
@@ -27,12 +30,37 @@
 namespace mkfg {
 
 constexpr int kBlock = 256;
+// Minimum resident blocks per SM requested for the heavy per-candidate
+// kernels (propagate, chi2, update): trades registers for occupancy.
+#ifndef MKFG_HEAVY_MIN_BLOCKS
+#define MKFG_HEAVY_MIN_BLOCKS 1
+#endif
+
+// Appends `value` for the lanes where `want` holds to a two-ended list:
+// barrel entries from the front (counter cnt[0]), endcap entries from the
+// back (counter cnt[1]). One atomic per warp and end; all lanes call it.
+__device__ __forceinline__ void append_two_ended(bool want, bool barrel, int value, int* list,
+                                                 int cap, int* cnt, int lane) {
+  const unsigned mb = __ballot_sync(0xffffffffu, want && barrel);
+  const unsigned me = __ballot_sync(0xffffffffu, want && !barrel);
+  int bb = 0, be = 0;
+  if (lane == 0) {
+    if (mb) bb = atomicAdd(cnt + 0, __popc(mb));
+    if (me) be = atomicAdd(cnt + 1, __popc(me));
+  }
+  bb = __shfl_sync(0xffffffffu, bb, 0);
+  be = __shfl_sync(0xffffffffu, be, 0);
+  const unsigned below = (1u << lane) - 1u;
+  if (want && barrel) list[bb + __popc(mb & below)] = value;
+  if (want && !barrel) list[cap - 1 - (be + __popc(me & below))] = value;
+}
 
 //------------------------------------------------------------------------------
-// Kernel 1: prep
+// Kernel 1a: activation (one thread per candidate slot, light): seed wake-up,
+// unroll + looper stop, seed state, compact list of the active candidates.
 //------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) k_prep(EventDev E, const FindConfigDev* __restrict__ Cp,
-                                                 int step) {
+__global__ void __launch_bounds__(kBlock) k_activate(EventDev E, const FindConfigDev* __restrict__ Cp,
+                                                     int step) {
   const FindConfigDev& C = *Cp;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int s = t / kSlots, c = t % kSlots;
@@ -49,11 +77,8 @@ __global__ void __launch_bounds__(kBlock) k_prep(EventDev E, const FindConfigDev
     buf = E.cur[s];
   }
   const int slot = s * kSlots + c;
-  const CandSoA& B = E.cand[buf];
-  float par[6], err[21];
-  int chg = 0;
   const bool active = in_range && layer >= 0 && state == kFinding && c < ncand &&
-                      activate_cand(E, B, s, slot, layer, par, err, chg);
+                      cand_is_active(E, E.cand[buf], s, slot, layer);
   const unsigned act = __ballot_sync(0xffffffffu, active) & grp;
   {
     const unsigned all = __ballot_sync(0xffffffffu, active);
@@ -63,14 +88,43 @@ __global__ void __launch_bounds__(kBlock) k_prep(EventDev E, const FindConfigDev
     if (layer >= 0 && state == kFinding && act == 0) state = kFinished;
     E.state[s] = state;
   }
-  if (!in_range) return;
+  const bool barrel = active && C.layer[layer].is_barrel;
+  append_two_ended(active, barrel, slot, E.act_list, E.list_cap,
+                   E.step_count + step * kCntN + kCntActBarrel, lane);
+  // The clone step reads the records and extra flags of candidates
+  // [0, ncand) of seeds still finding: an inactive one among them has
+  // neither.
+  const bool seed_finding = layer >= 0 && state == kFinding && act != 0;
+  if (seed_finding && !active && c < ncand) {
+    const size_t rbase = (size_t)s * kRecPerSeed + c * kRecPerCand;
+    for (int h = 0; h <= kMaxXHits; ++h) E.rhit[rbase + h] = kRecInvalid;
+    E.wsr[slot] = kWsrOutside;
+  }
+}
 
-  const size_t rbase = (size_t)s * kRecPerSeed + c * kRecPerCand;
-  PrepOut o;
-  if (active) {
+//------------------------------------------------------------------------------
+// Kernel 1b: propagation to the layer, hit selection, missed-layer handling
+// and hole record for the active candidates (compact list; barrel and
+// endcap candidates in separate runs of the list).
+//------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock, MKFG_HEAVY_MIN_BLOCKS) k_propagate(EventDev E, const FindConfigDev* __restrict__ Cp,
+                                                      int step) {
+  const FindConfigDev& C = *Cp;
+  const int* cnt = E.step_count + step * kCntN;
+  const int nb = cnt[kCntActBarrel], ne = cnt[kCntActEndcap];
+  const int stride = E.cand[0].cap;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nb + ne; j += gridDim.x * blockDim.x) {
+    const int slot = j < nb ? E.act_list[j] : E.act_list[E.list_cap - 1 - (j - nb)];
+    const int s = slot / kSlots, c = slot % kSlots;
+    const int reg = E.region[s];
+    const int layer = plan_layer(C, reg, step);
+    const CandSoA& B = E.cand[E.cur[s]];
+    float par[6], err[21];
+    load_state(B, slot, par, err);
+    const int chg = B.chg[slot];
     const LayerDev& L = C.layer[layer];
     const int ev = E.seed_event[s];
-    const int stride = E.cand[0].cap;
+    PrepOut o;
     prep_cand(E, C, L, E.bins + (size_t)ev * E.n_bins + L.bin_offset,
               E.layer_begin[ev * E.lb_stride + layer], reg, layer, s, B, slot, par, err, chg,
               E.xhit + slot, stride, o);
@@ -80,34 +134,45 @@ __global__ void __launch_bounds__(kBlock) k_prep(EventDev E, const FindConfigDev
 #pragma unroll
     for (int e = 0; e < 21; ++e) E.perr[e * stride + slot] = o.perr[e];
     if (o.xs > 0) {
-      const int base = atomicAdd(&E.pair_count[step], o.xs);
-      for (int h = 0; h < o.xs; ++h) E.pairs[base + h] = slot * kMaxXHits + h;
+      if (L.is_barrel) {
+        const int base = atomicAdd(E.step_count + step * kCntN + kCntPairBarrel, o.xs);
+        for (int h = 0; h < o.xs; ++h) E.pairs[base + h] = slot * kMaxXHits + h;
+      } else {
+        const int base = atomicAdd(E.step_count + step * kCntN + kCntPairEndcap, o.xs);
+        for (int h = 0; h < o.xs; ++h) E.pairs[E.pair_cap - 1 - (base + h)] = slot * kMaxXHits + h;
+      }
     }
+    const size_t rbase = (size_t)s * kRecPerSeed + c * kRecPerCand;
+    const size_t r = rbase + kMaxXHits;
+    if (o.hole) {
+      E.rhit[r] = o.hole_hit;
+      E.rmodule[r] = -1;
+      E.rchi2hit[r] = 0.f;
+      E.rscore[r] = o.hole_score;
+    } else {
+      E.rhit[r] = kRecInvalid;
+    }
+    for (int h = o.xs; h < kMaxXHits; ++h) E.rhit[rbase + h] = kRecInvalid;
+    E.wsr[slot] = o.wsr | (o.extra << 8);
   }
-  const size_t r = rbase + kMaxXHits;
-  if (o.hole) {
-    E.rhit[r] = o.hole_hit;
-    E.rmodule[r] = -1;
-    E.rchi2hit[r] = 0.f;
-    E.rscore[r] = o.hole_score;
-  } else {
-    E.rhit[r] = kRecInvalid;
-  }
-  for (int h = o.xs; h < kMaxXHits; ++h) E.rhit[rbase + h] = kRecInvalid;
-  E.wsr[slot] = o.wsr | (o.extra << 8);
 }
 
 //------------------------------------------------------------------------------
 // Kernel 2: chi2 of every (candidate, selected hit) pair
 // (MkFinder::FindCandidatesCloneEngine, mkFit/MkFinder.cc:1116-1240).
 //------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) k_chi2(EventDev E, const FindConfigDev* __restrict__ Cp,
+__global__ void __launch_bounds__(kBlock, MKFG_HEAVY_MIN_BLOCKS) k_chi2(EventDev E, const FindConfigDev* __restrict__ Cp,
                                                  int step) {
   const FindConfigDev& C = *Cp;
-  const int n_pairs = E.pair_count[step];
-  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&E.work[step * 4 + 2], n_pairs);
+  const int* cnt = E.step_count + step * kCntN;
+  const int nb = cnt[kCntPairBarrel], ne = cnt[kCntPairEndcap];
+  const int n_pairs = nb + ne;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    atomicAdd(&E.work[step * 4 + 2], n_pairs);
+    E.pair_count[step] = n_pairs;
+  }
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n_pairs; p += gridDim.x * blockDim.x) {
-    const int code = E.pairs[p];
+    const int code = p < nb ? E.pairs[p] : E.pairs[E.pair_cap - 1 - (p - nb)];
     const int slot = code / kMaxXHits, h = code % kMaxXHits;
     const int s = slot / kSlots, c = slot % kSlots;
     const int layer = plan_layer(C, E.region[s], step);
@@ -149,8 +214,9 @@ __global__ void __launch_bounds__(kBlock) k_clone(EventDev E, const FindConfigDe
   if (s >= E.n_seeds) return;
   const int layer = plan_layer(C, E.region[s], step);
   if (layer < 0) return;
+  // A seed that is not finding at this step has no records: nothing to do.
   const int state = E.state[s];
-  if (state == kDormant) return;
+  if (state != kFinding) return;
   const int cur = E.cur[s];
   if (lane == 0) atomicAdd(&E.work[step * 4 + 3], 1);
   const size_t rb = (size_t)s * kRecPerSeed;
@@ -162,24 +228,29 @@ __global__ void __launch_bounds__(kBlock) k_clone(EventDev E, const FindConfigDe
     E.n_cands[s] = n;
     E.cur[s] = cur ^ 1;
   }
+  // Compact list of the new candidates that take a Kalman update (their
+  // hit is on this step's layer).
+  __syncwarp();
+  const bool upd = lane < n && E.upd[s * kSlots + lane];
+  append_two_ended(upd, C.layer[layer].is_barrel, s * kSlots + lane, E.upd_list, E.list_cap,
+                   E.step_count + step * kCntN + kCntUpdBarrel, lane);
 }
 
 //------------------------------------------------------------------------------
 // Kernel 4: UpdateWithLastHit + CopyOutParErr for candidates that took a hit.
 //------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) k_update(EventDev E, const FindConfigDev* __restrict__ Cp,
+__global__ void __launch_bounds__(kBlock, MKFG_HEAVY_MIN_BLOCKS) k_update(EventDev E, const FindConfigDev* __restrict__ Cp,
                                                    int step) {
   const FindConfigDev& C = *Cp;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int s = t / kSlots, c = t % kSlots;
-  if (s >= E.n_seeds) return;
-  if (plan_layer(C, E.region[s], step) < 0) return;
-  if (c >= E.n_cands[s]) return;
-  const int slot = s * kSlots + c;
-  if (!E.upd[slot]) return;
-  E.upd[slot] = 0;
-  atomicAdd(&E.work[step * 4 + 1], 1);
-  update_cand(E, C, s, E.layer_begin + E.seed_event[s] * E.lb_stride, E.cand[E.cur[s]], slot);
+  const int* cnt = E.step_count + step * kCntN;
+  const int nb = cnt[kCntUpdBarrel], ne = cnt[kCntUpdEndcap];
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&E.work[step * 4 + 1], nb + ne);
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nb + ne; j += gridDim.x * blockDim.x) {
+    const int slot = j < nb ? E.upd_list[j] : E.upd_list[E.list_cap - 1 - (j - nb)];
+    const int s = slot / kSlots;
+    E.upd[slot] = 0;
+    update_cand(E, C, s, E.layer_begin + E.seed_event[s] * E.lb_stride, E.cand[E.cur[s]], slot);
+  }
 }
 
 //------------------------------------------------------------------------------
@@ -192,14 +263,28 @@ __global__ void k_reset(EventDev E, int n_work) {
   if (t == 0) E.err_flags[0] = 0;
   const int s = t / kSlots, c = t % kSlots;
   if (s >= E.n_seeds) return;
-  copy_slot(E.init, t, E.cand[0], t);
   E.upd[t] = 0;
   if (c == 0) {
+    copy_slot(E.init, s, E.cand[0], t);
     E.n_cands[s] = 1;
     E.state[s] = kDormant;
     E.cur[s] = 0;
     E.hot_size[s] = E.init_hot[s];
     E.bshort_valid[s] = 0;
+  }
+}
+
+// Writes every seed's own hits as the first nodes of its hit-on-track
+// arena (CombCandidate::ImportSeed); appends during a run start after them.
+__global__ void k_seed_nodes(EventDev E, const int* __restrict__ seed_hot) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= E.n_seeds) return;
+  const int nhs = E.init_hot[s];
+  for (int h = 0; h < nhs; ++h) {
+    const size_t k = (size_t)s * E.hot_cap + h;
+    E.node_hot[k] = seed_hot[4 * s + h];
+    E.node_chi2[k] = 0.f;
+    E.node_prev[k] = h - 1;
   }
 }
 
@@ -212,6 +297,117 @@ __global__ void k_merge(EventDev E, const FindConfigDev* __restrict__ Cp) {
   const int cur = E.cur[s];
   E.n_cands[s] = merge_seed(E, *Cp, s, E.n_cands[s], cur);
   E.cur[s] = cur ^ 1;
+}
+
+//------------------------------------------------------------------------------
+// Backward fit of every seed's best candidate (MkBuilder::BackwardFit +
+// fit_cands, mkFit/MkBuilder.cc:2153-2253; MkFinder::BkFitInputTracks /
+// BkFitFitTracks / BkFitOutputTracks, mkFit/MkFinder.cc:1368-1452,
+// 1573-1742). The reference fits seeds in groups of NN consecutive seeds
+// (its Matriplex width) and the group's members interact: a layer where no
+// member has a hit is skipped by all of them, and on a layer where some
+// member has one the others are updated with a stand-in measurement at
+// their own position (variance 666, no material). Here each group runs on
+// `nn` lanes of a warp, which make those decisions with group ballots.
+//------------------------------------------------------------------------------
+struct BkFitArgs {
+  const int2* groups;  // (first sorted seed, count)
+  int n_groups;
+  int nn;              // lanes per group (8 or 16)
+  unsigned pflags;
+  int bkfit_last[kMaxRegions];
+};
+
+__global__ void __launch_bounds__(kBlock) k_bkfit(EventDev E, const FindConfigDev* __restrict__ Cp,
+                                                  const BkFitArgs A) {
+  const FindConfigDev& C = *Cp;
+  const int lane = threadIdx.x & 31;
+  const int per_warp = 32 / A.nn;
+  const int g = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * per_warp + lane / A.nn;
+  if (g >= A.n_groups) return;  // whole groups leave together
+  const int k = lane % A.nn;
+  const int base = lane - k;
+  const unsigned gmask = (A.nn == 32 ? 0xffffffffu : ((1u << A.nn) - 1u)) << base;
+  const int2 grp = A.groups[g];
+  const unsigned tracks = (grp.y >= 32 ? 0xffffffffu : ((1u << grp.y) - 1u)) << base;
+  const int s = grp.x + (k < grp.y ? k : 0);
+  const bool member = k < grp.y;
+  const CandSoA& B = E.cand[E.cur[s]];
+  const int slot = s * kSlots;
+  const bool present = member && E.n_cands[s] > 0;
+  float par[6], err[21];
+  int chg = 1, node = -1;
+  if (present) {
+    load_state(B, slot, par, err);
+#pragma unroll
+    for (int e = 0; e < 21; ++e) err[e] *= 100.f;  // Err[iC].Scale(100)
+    chg = B.chg[slot];
+    node = B.last[slot];
+  } else {
+#pragma unroll
+    for (int e = 0; e < 6; ++e) par[e] = 1.f;
+#pragma unroll
+    for (int e = 0; e < 21; ++e) err[e] = 1.f;
+  }
+  float chi2 = 0.f;
+  const int reg = E.region[grp.x];
+  const int* lb = E.layer_begin + E.seed_event[grp.x] * E.lb_stride;
+  for (int li = C.plan_len[reg] - 1; li >= A.bkfit_last[reg]; --li) {
+    const int layer = C.plan[reg][li];
+    while (node >= 0 && hot_index(node_hot_of(E, s, node)) < 0)
+      node = E.node_prev[(size_t)s * E.hot_cap + node];
+    const bool done = node < 0;
+    const bool here = !done && hot_layer(node_hot_of(E, s, node)) == layer;
+    float mpos[3], merr[6];
+    if (here) {
+      // The first of the candidate's consecutive nodes on this layer (an
+      // overlap hit follows the hit it pairs with).
+      int prev = E.node_prev[(size_t)s * E.hot_cap + node];
+      while (prev >= 0 && hot_layer(node_hot_of(E, s, prev)) == layer) {
+        node = prev;
+        prev = E.node_prev[(size_t)s * E.hot_cap + node];
+      }
+      const int gi = lb[layer] + hot_index(node_hot_of(E, s, node));
+#pragma unroll
+      for (int e = 0; e < 3; ++e) mpos[e] = __ldg(E.hpos + e * E.hstride + gi);
+#pragma unroll
+      for (int e = 0; e < 6; ++e) merr[e] = __ldg(E.herr + e * E.hstride + gi);
+      node = prev;
+    } else {
+      mpos[0] = par[0];
+      mpos[1] = par[1];
+      mpos[2] = par[2];
+      merr[0] = 666.f; merr[1] = 0.f; merr[2] = 666.f;
+      merr[3] = 0.f; merr[4] = 0.f; merr[5] = 666.f;
+    }
+    const unsigned done_m = __ballot_sync(gmask, member && done) & tracks;
+    const unsigned here_m = __ballot_sync(gmask, member && here) & tracks;
+    if (done_m == tracks) break;
+    if (here_m == 0) continue;
+    if (member) {
+      const LayerDev& L = C.layer[layer];
+      float ppar[6], perr[21];
+      float c2;
+      if (L.is_barrel) {
+        propagate_to_r(par, err, chg, hypot_f(mpos[0], mpos[1]), A.pflags, C.mat, !here, ppar, perr);
+        c2 = kalman_barrel<true, true>(ppar, perr, mpos, merr, par, err);
+      } else {
+        propagate_to_z(par, err, chg, mpos[2], A.pflags, C.mat, !here, ppar, perr);
+        c2 = kalman_endcap<true, true>(ppar, perr, mpos, merr, par, err);
+      }
+      if (par[3] < 0) {
+        chg = -chg;
+        par[3] = -par[3];
+      }
+      chi2 += c2;
+    }
+  }
+  if (!present) return;
+  // Parameters, errors, chi2 and score go back to the candidate; the charge
+  // stays as found (BkFitOutputTracks copies no charge).
+  store_state(B, slot, par, err);
+  B.chi2[slot] = chi2;
+  if (!isnan(chi2)) B.score[slot] = cand_score(B, slot);
 }
 
 //------------------------------------------------------------------------------
@@ -308,6 +504,11 @@ struct Finder {
   cudaGraphExec_t graph = nullptr;  // captured run sequence of the current upload
   int fused_w = 16;                 // seeds per block of the fused form
   int64_t last_chi2_evals = 0, last_seeds_cloned = 0;
+  // Host copies for the backward fit's seed groups: region of every sorted
+  // seed and the first sorted seed of every event.
+  std::vector<int> h_region;
+  std::vector<int> h_seed_off;
+  DevBuf bk;  // backward-fit seed groups
   void drop_graph() {
     if (graph) cudaGraphExecDestroy(graph);
     graph = nullptr;
@@ -336,6 +537,7 @@ void finder_release(mkfg_context* ctx) {
   Finder* f = static_cast<Finder*>(ctx->finder);
   if (f->d_cfg) cudaFree(f->d_cfg);
   f->drop_graph();
+  f->bk.release();
   f->hits.release();
   f->seeds.release();
   f->cands.release();
@@ -566,7 +768,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     };
     f->ev.cand[0] = mk(SC);
     f->ev.cand[1] = mk(SC);
-    f->ev.init = mk(SC);
+    f->ev.init = mk(SS);
     f->ev.bshort = mk(SS);
     f->ev.init_hot = carve<int>(p, SS);
     f->ev.seed_label = carve<int>(p, SS);
@@ -580,8 +782,8 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     f->ev.bshort_valid = carve<int>(p, SS);
   }
   {
-    const size_t need = rounded(4 * (size_t)SC) * (27 + 5) + 2 * rounded(4 * (size_t)SC * kMaxXHits) +
-                        rounded(4 * (size_t)(max_steps + 2)) * 5 + rounded(64) + 4096;
+    const size_t need = rounded(4 * (size_t)SC) * (27 + 8) + 2 * rounded(4 * (size_t)SC * kMaxXHits) +
+                        rounded(4 * (size_t)(max_steps + 2)) * (1 + 4 + kCntN) + rounded(64) + 8192;
     if ((rc = f->scratch.ensure(need))) return rc;
     char* p = f->scratch.as<char>();
     f->ev.ppar = carve<float>(p, 6 * (size_t)SC);
@@ -591,7 +793,12 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     f->ev.extra_last = carve<int>(p, SC);
     f->ev.upd = carve<int>(p, SC);
     f->ev.pairs = carve<int>(p, (size_t)SC * kMaxXHits);
+    f->ev.pair_cap = SC * kMaxXHits;
     f->ev.pair_count = carve<int>(p, max_steps + 2);
+    f->ev.act_list = carve<int>(p, SC);
+    f->ev.upd_list = carve<int>(p, SC);
+    f->ev.list_cap = SC;
+    f->ev.step_count = carve<int>(p, (size_t)kCntN * (max_steps + 2));
     f->ev.err_flags = carve<int>(p, 16);
     f->ev.work = carve<int>(p, 4 * (size_t)(max_steps + 2));
   }
@@ -617,11 +824,13 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
 
   // Initial candidates: each event's seeds in sorted order
   // (CombCandidate::ImportSeed, mkFit/HitStructures.cc:483-509).
-  std::vector<float> par(6 * (size_t)SC, 0.f), err(21 * (size_t)SC, 0.f), score(SC, 0.f);
-  std::vector<int> chg(SC, 0), last(SC, 0), nfound(SC, 0), nmiss(SC, 0), ninside(SC, 0), ntail(SC, 0);
+  // One initial candidate per seed, and the seed's hits as its first
+  // hit-on-track nodes (at most 4 per seed).
+  std::vector<float> par(6 * (size_t)SS, 0.f), err(21 * (size_t)SS, 0.f), score(SS, 0.f);
+  std::vector<int> chg(SS, 0), last(SS, 0), nfound(SS, 0), nmiss(SS, 0), ninside(SS, 0), ntail(SS, 0);
   std::vector<int> label(SS, 0), sev(SS, 0), region(SS, 0), pickup(SS, 0), state(SS, kDormant),
       ncand(SS, 1), cur(SS, 0), hot_size(SS, 0);
-  std::vector<int> node_hot((size_t)SS * hot_cap, 0), node_prev((size_t)SS * hot_cap, -1);
+  std::vector<int> seed_hot(4 * (size_t)SS, 0);
   for (int e = 0; e < n_ev; ++e) {
     const mkfg_event* ev = evs + e;
     const int n = ev->n_seeds;
@@ -633,16 +842,14 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
       region[s] = orders[e].region[i];
       const int nhs = ev->seed_nhits[i];
       pickup[s] = ev->seed_hit_layer[i * 4 + nhs - 1];
-      const int slot = s * kSlots;
-      for (int c = 0; c < 6; ++c) par[c * (size_t)SC + slot] = ev->seed_par[c * n + i];
-      for (int c = 0; c < 21; ++c) err[c * (size_t)SC + slot] = ev->seed_err[c * n + i];
+      const int slot = s;
+      for (int c = 0; c < 6; ++c) par[c * (size_t)SS + slot] = ev->seed_par[c * n + i];
+      for (int c = 0; c < 21; ++c) err[c * (size_t)SS + slot] = ev->seed_err[c * n + i];
       chg[slot] = ev->seed_chg[i];
-      int nf = 0, nm = 0, nin = 0, ntl = 0, prev = -1;
+      int nf = 0, nm = 0, nin = 0, ntl = 0;
       for (int h = 0; h < nhs; ++h) {
         const int hi = ev->seed_hit_index[i * 4 + h], hl = ev->seed_hit_layer[i * 4 + h];
-        node_hot[(size_t)s * hot_cap + h] = (hi & 0xffffff) | (hl << 24);
-        node_prev[(size_t)s * hot_cap + h] = prev;
-        prev = h;
+        seed_hot[4 * (size_t)s + h] = (hi & 0xffffff) | (hl << 24);
         if (hi >= 0 || hi == -9) {
           ++nf;
           nin += ntl;
@@ -659,7 +866,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
       ninside[slot] = nin;
       ntail[slot] = ntl;
       // getScoreCand(cand) with default arguments (mkFit/HitStructures.h:519-531).
-      const float pt = std::abs(1.f / par[3 * (size_t)SC + slot]);
+      const float pt = std::abs(1.f / par[3 * (size_t)SS + slot]);
       float bonus = 0.2f * nf + 4.0f, penalty = 8.0f;
       if (pt < 0.9f) {
         penalty *= 1.5f;
@@ -672,15 +879,15 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   CandSoA& B0 = f->ev.init;
   if ((rc = up(B0.par, par.data(), 4 * par.size()))) return rc;
   if ((rc = up(B0.err, err.data(), 4 * err.size()))) return rc;
-  if ((rc = up(B0.chg, chg.data(), 4 * (size_t)SC))) return rc;
-  MKFG_CUDA_TRY(cudaMemsetAsync(B0.chi2, 0, 4 * (size_t)SC, st));
-  if ((rc = up(B0.score, score.data(), 4 * (size_t)SC))) return rc;
-  if ((rc = up(B0.last, last.data(), 4 * (size_t)SC))) return rc;
-  if ((rc = up(B0.nfound, nfound.data(), 4 * (size_t)SC))) return rc;
-  if ((rc = up(B0.nmiss, nmiss.data(), 4 * (size_t)SC))) return rc;
-  MKFG_CUDA_TRY(cudaMemsetAsync(B0.nover, 0, 4 * (size_t)SC, st));
-  if ((rc = up(B0.ninside, ninside.data(), 4 * (size_t)SC))) return rc;
-  if ((rc = up(B0.ntail, ntail.data(), 4 * (size_t)SC))) return rc;
+  if ((rc = up(B0.chg, chg.data(), 4 * (size_t)SS))) return rc;
+  MKFG_CUDA_TRY(cudaMemsetAsync(B0.chi2, 0, 4 * (size_t)SS, st));
+  if ((rc = up(B0.score, score.data(), 4 * (size_t)SS))) return rc;
+  if ((rc = up(B0.last, last.data(), 4 * (size_t)SS))) return rc;
+  if ((rc = up(B0.nfound, nfound.data(), 4 * (size_t)SS))) return rc;
+  if ((rc = up(B0.nmiss, nmiss.data(), 4 * (size_t)SS))) return rc;
+  MKFG_CUDA_TRY(cudaMemsetAsync(B0.nover, 0, 4 * (size_t)SS, st));
+  if ((rc = up(B0.ninside, ninside.data(), 4 * (size_t)SS))) return rc;
+  if ((rc = up(B0.ntail, ntail.data(), 4 * (size_t)SS))) return rc;
   if ((rc = up(f->ev.seed_label, label.data(), 4 * (size_t)SS))) return rc;
   if ((rc = up(f->ev.seed_event, sev.data(), 4 * (size_t)SS))) return rc;
   if ((rc = up(f->ev.region, region.data(), 4 * (size_t)SS))) return rc;
@@ -690,15 +897,18 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   if ((rc = up(f->ev.cur, cur.data(), 4 * (size_t)SS))) return rc;
   if ((rc = up(f->ev.init_hot, hot_size.data(), 4 * (size_t)SS))) return rc;
   MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.bshort_valid, 0, 4 * (size_t)SS, st));
-  if ((rc = up(f->ev.node_hot, node_hot.data(), 4 * node_hot.size()))) return rc;
-  if ((rc = up(f->ev.node_prev, node_prev.data(), 4 * node_prev.size()))) return rc;
-  MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.node_chi2, 0, 4 * node_hot.size(), st));
+  if ((rc = f->seeds.ensure(rounded(16 * (size_t)SS)))) return rc;
+  if ((rc = up(f->seeds.ptr, seed_hot.data(), 4 * seed_hot.size()))) return rc;
+  if (S > 0) k_seed_nodes<<<(S + 127) / 128, 128, 0, st>>>(f->ev, f->seeds.as<int>());
+  MKFG_CUDA_TRY(cudaGetLastError());
   MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.upd, 0, 4 * (size_t)SC, st));
   MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.err_flags, 0, 64, st));
   // The staging vectors die at return: wait for the copies.
   MKFG_CUDA_TRY(cudaStreamSynchronize(st));
   f->n_seeds = S;
   f->n_events = n_ev;
+  f->h_region.assign(region.begin(), region.begin() + S);
+  f->h_seed_off = seed_off;
   f->events_loaded = 1;
   return MKFG_OK;
 }
@@ -713,13 +923,17 @@ static int enqueue_run(Finder* f, cudaStream_t st) {
   const int grid_c = (threads_c + kBlock - 1) / kBlock;
   const int grid_w = (S * 32 + kBlock - 1) / kBlock;
   const int grid_p = std::min((S * kSlots * 4 + kBlock - 1) / kBlock, 148 * 16);
+  const int grid_l = std::min(grid_c, 148 * 8);
   k_reset<<<std::max(grid_c, (n_work + kBlock - 1) / kBlock), kBlock, 0, st>>>(f->ev, n_work);
   MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.pair_count, 0, 4 * (size_t)(f->host_cfg.max_steps + 2), st));
+  MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.step_count, 0,
+                                4 * (size_t)kCntN * (f->host_cfg.max_steps + 2), st));
   for (int step = 1; step <= f->host_cfg.max_steps; ++step) {
-    k_prep<<<grid_c, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+    k_activate<<<grid_c, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+    k_propagate<<<grid_l, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
     k_chi2<<<std::max(grid_p, 1), kBlock, 0, st>>>(f->ev, f->d_cfg, step);
     k_clone<<<grid_w, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
-    k_update<<<grid_c, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+    k_update<<<grid_l, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
   }
   k_merge<<<(S + 127) / 128, 128, 0, st>>>(f->ev, f->d_cfg);
   MKFG_CUDA_TRY(cudaGetLastError());
@@ -782,9 +996,10 @@ static int run_graph(mkfg_context* ctx, Finder* f) {
   return MKFG_OK;
 }
 
-static int download(mkfg_context* ctx, Finder* f, mkfg_find_out* out, int n_seeds_in) {
+// Exports m_out candidate slots per seed (max_cands: all; 1: the best).
+static int download(mkfg_context* ctx, Finder* f, mkfg_find_out* out, int n_seeds_in, int m_out) {
   const int S = f->n_seeds;
-  const int m = f->host_cfg.max_cands;
+  const int m = m_out;
   const size_t no = (size_t)std::max(n_seeds_in, 1) * m;
   const size_t need = rounded(4 * (size_t)std::max(n_seeds_in, 1)) * 2 +
                       rounded(4 * no) * (6 + 21 + 9) + rounded(4 * no * kExportHits) * 2;
@@ -928,6 +1143,63 @@ extern "C" int mkfg_find_autotune(mkfg_context* ctx, int32_t* seeds_per_block, f
   return MKFG_OK;
 }
 
+extern "C" int mkfg_find_backward_fit(mkfg_context* ctx, const int32_t* bkfit_last,
+                                      uint32_t pflags, int32_t group_width) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  Finder* f = finder_of(ctx);
+  MKFG_REQUIRE(f->configured && f->events_loaded, "no event uploaded");
+  const int nn = group_width ? group_width : 8;
+  MKFG_REQUIRE(nn == 8 || nn == 16, "group_width must be 8 or 16 (got %d)", group_width);
+  MKFG_REQUIRE((pflags & ~3u) == 0, "unknown propagation flags 0x%x", pflags);
+  BkFitArgs A{};
+  A.nn = nn;
+  A.pflags = pflags;
+  for (int r = 0; r < f->host_cfg.n_regions; ++r) {
+    A.bkfit_last[r] = bkfit_last ? bkfit_last[r] : 0;
+    MKFG_REQUIRE(A.bkfit_last[r] >= 0 && A.bkfit_last[r] <= f->host_cfg.plan_len[r],
+                 "bkfit_last[%d] out of range", r);
+  }
+  if (f->n_seeds == 0) return MKFG_OK;
+  // Seed groups as MkBuilder::BackwardFit forms them: per event and eta
+  // region, the region's seed range is cut into tasks with grain
+  // clamp(n_seeds + 1, 4, 32) (numThreadsEvents = numThreadsFinder = 1,
+  // numSeedsPerTask = 32: the reference defaults), and fit_cands fits each
+  // task in groups of NN from its start. The task cut is the one of the
+  // task pool the reference is built with here: ceil(n / grain) pieces of
+  // near-equal size, the first n % pieces one seed longer.
+  std::vector<int2> groups;
+  for (int e = 0; e + 1 < (int)f->h_seed_off.size(); ++e) {
+    const int b = f->h_seed_off[e], end = f->h_seed_off[e + 1];
+    const int grain = std::min(std::max(end - b + 1, 4), 32);
+    for (int r0 = b; r0 < end;) {
+      int r1 = r0;
+      while (r1 < end && f->h_region[r1] == f->h_region[r0]) ++r1;
+      const int n = r1 - r0;
+      const int pieces = (n + grain - 1) / grain;
+      const int base = n / pieces, extra = n % pieces;
+      int t0 = r0;
+      for (int i = 0; i < pieces; ++i) {
+        const int t1 = t0 + base + (i < extra ? 1 : 0);
+        for (int g0 = t0; g0 < t1; g0 += nn) groups.push_back(make_int2(g0, std::min(nn, t1 - g0)));
+        t0 = t1;
+      }
+      r0 = r1;
+    }
+  }
+  if ((rc = f->bk.ensure(groups.size() * sizeof(int2)))) return rc;
+  MKFG_CUDA_TRY(cudaMemcpyAsync(f->bk.ptr, groups.data(), groups.size() * sizeof(int2),
+                                cudaMemcpyHostToDevice, ctx->stream));
+  A.groups = f->bk.as<int2>();
+  A.n_groups = (int)groups.size();
+  const int per_block = (kBlock / 32) * (32 / nn);
+  k_bkfit<<<(A.n_groups + per_block - 1) / per_block, kBlock, 0, ctx->stream>>>(f->ev, f->d_cfg, A);
+  MKFG_CUDA_TRY(cudaGetLastError());
+  // The group list is host memory: finish the copy before it goes away.
+  MKFG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return MKFG_OK;
+}
+
 extern "C" int mkfg_find_work(mkfg_context* ctx, int64_t* active_cands, int64_t* hit_pairs,
                               int64_t* updates, int32_t* steps) {
   int rc = activate(ctx);
@@ -962,7 +1234,16 @@ extern "C" int mkfg_find_download(mkfg_context* ctx, int n_seeds, mkfg_find_out*
   Finder* f = finder_of(ctx);
   MKFG_REQUIRE(out != nullptr, "null output");
   MKFG_REQUIRE(f->events_loaded && n_seeds == f->n_seeds, "seed count mismatch");
-  return download(ctx, f, out, n_seeds);
+  return download(ctx, f, out, n_seeds, f->host_cfg.max_cands);
+}
+
+extern "C" int mkfg_find_download_best(mkfg_context* ctx, int n_seeds, mkfg_find_out* out) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  Finder* f = finder_of(ctx);
+  MKFG_REQUIRE(out != nullptr, "null output");
+  MKFG_REQUIRE(f->events_loaded && n_seeds == f->n_seeds, "seed count mismatch");
+  return download(ctx, f, out, n_seeds, 1);
 }
 
 extern "C" int mkfg_find_event(mkfg_context* ctx, const mkfg_event* ev, mkfg_find_out* out) {

@@ -22,6 +22,10 @@ constexpr int kRecInvalid = -1000000;
 enum SeedState { kDormant = 0, kFinding = 1, kFinished = 2 };
 enum WsrCode { kWsrInside = 0, kWsrEdge = 1, kWsrOutside = 2 };
 enum ErrBits { kErrArena = 1, kErrLayerSize = 2 };
+enum StepCount {
+  kCntActBarrel = 0, kCntActEndcap, kCntPairBarrel, kCntPairEndcap, kCntUpdBarrel, kCntUpdEndcap,
+  kCntN = 8
+};
 
 struct LayerDev {
   float rin, rout, zmin, zmax, propagate_to;
@@ -109,9 +113,18 @@ struct EventDev {
   float* rchi2hit;
   int* rhit;       // kRecInvalid when the slot holds no record
   int* rmodule;
-  // (cand slot, hit) pairs for the chi2 pass.
+  // (cand slot, hit) pairs for the chi2 pass; in the plain form barrel
+  // pairs fill the array from the front and endcap pairs from the back.
   int* pairs;
-  int* pair_count; // [max_steps + 1]
+  int* pair_count; // [max_steps + 2] pairs per step
+  int pair_cap;
+  // Plain form, per step: compact lists of the active candidate slots and
+  // of the slots that take a Kalman update (barrel from the front, endcap
+  // from the back); counts in step_count[step][kCnt*].
+  int* act_list;
+  int* upd_list;
+  int list_cap;
+  int* step_count; // [max_steps + 2][kCntN]
   int* err_flags;
   // Pristine initial state (restored by the reset kernel before every run).
   CandSoA init;

@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(W * kSlots) k_find_fused(EventDev E,
       const int wlayer = plan_layer(C, E.region[ws], step);
       if (wlayer < 0) continue;
       const int wstate = E.state[ws];
-      if (wstate == kDormant) continue;
+      if (wstate != kFinding) continue;
       const int cur = E.cur[ws];
       if (lane == 0) atomicAdd(&E.work[step * 4 + 3], 1);
       const int rb = wl * kRecPerSeed;

@@ -324,23 +324,34 @@ struct PrepOut {
 };
 
 // Unroll + looper stop (mkFit/MkBuilder.cc:1503-1566) for a candidate of a
-// seed already in Finding state; returns whether it is active.
-__device__ __forceinline__ bool activate_cand(const EventDev& E, const CandSoA& B, int s, int slot,
-                                              int layer, float (&par)[6], float (&err)[21],
-                                              int& chg) {
+// seed already in Finding state: a candidate whose last node is a stop (-2)
+// is inactive; a low-pT looper outside r = 25 cm turning back gets a stop
+// node and is inactive. Returns whether the candidate is active.
+__device__ __forceinline__ bool cand_is_active(const EventDev& E, const CandSoA& B, int s, int slot,
+                                               int layer) {
   const int last = B.last[slot];
   if (hot_index(node_hot_of(E, s, last)) == -2) return false;
-  load_state(B, slot, par, err);
-  chg = B.chg[slot];
-  const float pt = fabsf(1.f / par[3]);
+  const float x = B.par[0 * B.cap + slot], y = B.par[1 * B.cap + slot];
+  const float ipt = B.par[3 * B.cap + slot], phi = B.par[4 * B.cap + slot];
+  const float pt = fabsf(1.f / ipt);
   if (pt < 1.2f) {
-    const float dphi = fabsf(f_atan2(par[1], par[0]) - par[4]);
-    if (par[0] * par[0] + par[1] * par[1] > 625.f && dphi > 1.371f && dphi < 4.512f) {
+    const float dphi = fabsf(f_atan2(y, x) - phi);
+    if (x * x + y * y > 625.f && dphi > 1.371f && dphi < 4.512f) {
       B.last[slot] = arena_append(E, s, -2, layer, 0.f, last);
       B.nmiss[slot] += 1;
       return false;
     }
   }
+  return true;
+}
+
+// cand_is_active, loading the state of an active candidate.
+__device__ __forceinline__ bool activate_cand(const EventDev& E, const CandSoA& B, int s, int slot,
+                                              int layer, float (&par)[6], float (&err)[21],
+                                              int& chg) {
+  if (!cand_is_active(E, B, s, slot, layer)) return false;
+  load_state(B, slot, par, err);
+  chg = B.chg[slot];
   return true;
 }
 
@@ -489,25 +500,40 @@ struct SeedRecords {
 __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev& C, int s,
                                           int layer, int state, int ncand, int cur,
                                           const SeedRecords& R, HitMatchPair* hm, int lane) {
+  constexpr unsigned kFull = 0xffffffffu;
   const CandSoA& B = E.cand[cur];
   const CandSoA& N = E.cand[cur ^ 1];
   const int M = C.max_cands;
 
   // Overlap candidates per parent (consulted at CandCloner.cc:120-124),
-  // filled in hit order as MkFinder does (:1212-1216).
+  // filled in hit order as MkFinder does (:1212-1216); lane c scans
+  // candidate c's records.
   if (lane < kSlots) {
     HitMatchPair p;
     p.reset();
     if (lane < ncand) {
+      int hv[kMaxXHits], mv[kMaxXHits];
+      float cv[kMaxXHits];
+#pragma unroll
       for (int h = 0; h < kMaxXHits; ++h) {
         const int idx = lane * kRecPerCand + h;
-        if (!R.valid(idx, ncand)) continue;
-        const float c2 = R.chi2hit(idx);
-        if (c2 < C.chi2_cut_overlap) p.consider(R.hit(idx), R.module(idx), c2);
+        hv[h] = R.hit(idx);
+        cv[h] = R.chi2hit(idx);
+        mv[h] = R.module(idx);
       }
+#pragma unroll
+      for (int h = 0; h < kMaxXHits; ++h)
+        if (hv[h] != kRecInvalid && cv[h] < C.chi2_cut_overlap) p.consider(hv[h], mv[h], cv[h]);
     }
     hm[lane] = p;
   }
+
+  // Per-candidate values, lane c holding candidate c's.
+  const int cslot = s * kSlots + (lane < kSlots ? lane : 0);
+  const bool is_cand = lane < ncand;
+  const float c_score = is_cand ? B.score[cslot] : 0.f;
+  const float c_ipt = is_cand ? B.par[3 * B.cap + cslot] : 1.f;
+  const int c_kind = (is_cand && state == kFinding) ? R.extra_kind(lane) : 0;
   __syncwarp();
 
   constexpr int kPer = (kRecPerSeed + 31) / 32;
@@ -519,59 +545,56 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
     const int idx = lane + 32 * k;
     valid[k] = idx < kRecPerSeed && R.valid(idx, ncand);
     sc[k] = valid[k] ? R.score(idx) : 0.f;
-    n_valid += __popc(__ballot_sync(0xffffffffu, valid[k]));
+    n_valid += __popc(__ballot_sync(kFull, valid[k]));
   }
 
   // Extras (held-back candidates) in candidate order (MkBuilder.cc:1600-1626).
-  int extras[kSlots];
-  int extra_kind[kSlots];
-  int n_extras = 0;
-  if (state == kFinding) {
-    for (int c = 0; c < ncand; ++c) {
-      const int k = R.extra_kind(c);
-      if (k) {
-        extras[n_extras] = c;
-        extra_kind[n_extras] = k;
-        ++n_extras;
-      }
-    }
-  }
+  const unsigned extra_mask = __ballot_sync(kFull, c_kind != 0);
+  const int n_extras = __popc(extra_mask);
 
   if (n_valid == 0) {
-    // hitsForSeed empty (CandCloner.cc:163-172).
+    // hitsForSeed empty (CandCloner.cc:163-172): the extras survive.
     if (state != kFinding) return -1;
+    unsigned m = extra_mask;
     for (int i = 0; i < n_extras; ++i) {
-      const int src = s * kSlots + extras[i], dst = s * kSlots + i;
-      for (int f = lane; f < 27; f += 32) {
-        if (f < 6) N.par[f * N.cap + dst] = B.par[f * B.cap + src];
-        else N.err[(f - 6) * N.cap + dst] = B.err[(f - 6) * B.cap + src];
+      const int c = __ffs(m) - 1;
+      m &= m - 1;
+      const int src = s * kSlots + c, dst = s * kSlots + i;
+      if (lane < 27) {
+        if (lane < 6) N.par[lane * N.cap + dst] = B.par[lane * B.cap + src];
+        else N.err[(lane - 6) * N.cap + dst] = B.err[(lane - 6) * B.cap + src];
       }
-      if (lane == 0) {
-        N.chg[dst] = B.chg[src];
-        N.chi2[dst] = B.chi2[src];
-        N.score[dst] = B.score[src];
-        N.nfound[dst] = B.nfound[src];
-        N.nover[dst] = B.nover[src];
-        N.ninside[dst] = B.ninside[src];
-        N.ntail[dst] = B.ntail[src];
-        if (extra_kind[i] == 2) {
-          N.last[dst] = R.extra_last(extras[i]);
-          N.nmiss[dst] = B.nmiss[src] + 1;
-        } else {
-          N.last[dst] = B.last[src];
-          N.nmiss[dst] = B.nmiss[src];
-        }
-        R.set_upd(i, 0);
+    }
+    if (lane < n_extras) {
+      // Lane i: the i-th extra.
+      unsigned mm = extra_mask;
+      for (int k = 0; k < lane; ++k) mm &= mm - 1;
+      const int c = __ffs(mm) - 1;
+      const int src = s * kSlots + c, dst = s * kSlots + lane;
+      N.chg[dst] = B.chg[src];
+      N.chi2[dst] = B.chi2[src];
+      N.score[dst] = B.score[src];
+      N.nfound[dst] = B.nfound[src];
+      N.nover[dst] = B.nover[src];
+      N.ninside[dst] = B.ninside[src];
+      N.ntail[dst] = B.ntail[src];
+      if (R.extra_kind(c) == 2) {
+        N.last[dst] = R.extra_last(c);
+        N.nmiss[dst] = B.nmiss[src] + 1;
+      } else {
+        N.last[dst] = B.last[src];
+        N.nmiss[dst] = B.nmiss[src];
       }
+      R.set_upd(lane, 0);
     }
     return n_extras;
   }
 
   // Top-num_hits records in (score desc, record index asc) order: the
   // reference's std::sort by score; on exact score ties this order is the
-  // stable one.
+  // stable one. Lane i keeps the i-th record's index and values.
   const int num_hits = min(n_valid, M);
-  int top[kSlots];
+  int my_rec = 0;
   for (int i = 0; i < num_hits; ++i) {
     float best = -INFINITY;
     int bidx = INT_MAX;
@@ -585,30 +608,38 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
-      const float ob = __shfl_xor_sync(0xffffffffu, best, off);
-      const int oi = __shfl_xor_sync(0xffffffffu, bidx, off);
+      const float ob = __shfl_xor_sync(kFull, best, off);
+      const int oi = __shfl_xor_sync(kFull, bidx, off);
       if (ob > best || (ob == best && oi < bidx)) {
         best = ob;
         bidx = oi;
       }
     }
-    top[i] = bidx;
+    if (lane == i) my_rec = bidx;
 #pragma unroll
     for (int k = 0; k < kPer; ++k)
       if (lane + 32 * k == bidx) valid[k] = false;
   }
+  const bool has_rec = lane < num_hits;
+  const int r_hit = has_rec ? R.hit(my_rec) : 0;
+  const float r_score = has_rec ? R.score(my_rec) : 0.f;
+  const float r_chi2 = has_rec ? R.chi2hit(my_rec) : 0.f;
+  const int r_module = has_rec ? R.module(my_rec) : 0;
 
-  // Build the new candidate list (sequential logic of ProcessSeedRange).
+  // Build the new candidate list (sequential logic of ProcessSeedRange),
+  // identically in every lane from the broadcast values.
   NewCand nc[kSlots];
   int n_pushed = 0;
-  int ei = 0;
+  unsigned em = extra_mask;  // extras not yet taken, in candidate order
   float bs_score = E.bshort_valid[s] ? E.bshort.score[s] : -1e16f;  // getScoreWorstPossible
   int bs_from = -1;
   for (int ih = 0; ih < num_hits; ++ih) {
-    const int idx = top[ih];
+    const int idx = __shfl_sync(kFull, my_rec, ih);
+    const int hit = __shfl_sync(kFull, r_hit, ih);
+    const float score = __shfl_sync(kFull, r_score, ih);
+    const float chi2hit = __shfl_sync(kFull, r_chi2, ih);
+    const int module = __shfl_sync(kFull, r_module, ih);
     const int parent = idx / kRecPerCand;
-    const int hit = R.hit(idx);
-    const float score = R.score(idx);
     if (hit == -2) {
       if (score > bs_score) {
         bs_score = score;
@@ -616,28 +647,31 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
       }
       continue;
     }
-    while (ei < n_extras && B.score[s * kSlots + extras[ei]] > score && n_pushed < M) {
-      nc[n_pushed++] = NewCand{extras[ei], 0, 0.f, -1, 0.f, extra_kind[ei]};
-      ++ei;
+    while (em && n_pushed < M) {
+      const int c = __ffs(em) - 1;
+      if (!(__shfl_sync(kFull, c_score, c) > score)) break;
+      nc[n_pushed++] = NewCand{c, 0, 0.f, -1, 0.f, __shfl_sync(kFull, c_kind, c)};
+      em &= em - 1;
     }
     if (n_pushed >= M) break;
     int ov = -1;
-    const float ppt = fabsf(1.f / B.par[3 * B.cap + s * kSlots + parent]);
-    if (ppt > C.pt_cut_overlap && hit >= 0) ov = hm[parent].find(hit, R.module(idx));
-    nc[n_pushed++] = NewCand{parent, hit, R.chi2hit(idx), ov, score, 0};
+    const float ppt = fabsf(1.f / __shfl_sync(kFull, c_ipt, parent));
+    if (ppt > C.pt_cut_overlap && hit >= 0) ov = hm[parent].find(hit, module);
+    nc[n_pushed++] = NewCand{parent, hit, chi2hit, ov, score, 0};
   }
-  while (ei < n_extras && n_pushed < M) {
-    nc[n_pushed++] = NewCand{extras[ei], 0, 0.f, -1, 0.f, extra_kind[ei]};
-    ++ei;
+  while (em && n_pushed < M) {
+    const int c = __ffs(em) - 1;
+    nc[n_pushed++] = NewCand{c, 0, 0.f, -1, 0.f, __shfl_sync(kFull, c_kind, c)};
+    em &= em - 1;
   }
 
   // Best short candidate (a -2 record scoring above the current best).
   if (bs_from >= 0) {
     const int parent = bs_from / kRecPerCand;
     const int src = s * kSlots + parent;
-    for (int f = lane; f < 27; f += 32) {
-      if (f < 6) E.bshort.par[f * E.bshort.cap + s] = B.par[f * B.cap + src];
-      else E.bshort.err[(f - 6) * E.bshort.cap + s] = B.err[(f - 6) * B.cap + src];
+    if (lane < 27) {
+      if (lane < 6) E.bshort.par[lane * E.bshort.cap + s] = B.par[lane * B.cap + src];
+      else E.bshort.err[(lane - 6) * E.bshort.cap + s] = B.err[(lane - 6) * B.cap + src];
     }
     if (lane == 0) {
       int nfound = B.nfound[src], nmiss = B.nmiss[src], nin = B.ninside[src], ntl = B.ntail[src];
@@ -656,49 +690,52 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
     }
   }
 
-  // Materialize the new candidates into the other buffer.
+  // Materialize the new candidates into the other buffer: parameters and
+  // covariance by all lanes, counters and hit-on-track nodes of new
+  // candidate i by lane i.
   for (int i = 0; i < n_pushed; ++i) {
-    const NewCand& n = nc[i];
-    const int src = s * kSlots + n.parent, dst = s * kSlots + i;
-    for (int f = lane; f < 27; f += 32) {
-      if (f < 6) N.par[f * N.cap + dst] = B.par[f * B.cap + src];
-      else N.err[(f - 6) * N.cap + dst] = B.err[(f - 6) * B.cap + src];
+    const int src = s * kSlots + nc[i].parent, dst = s * kSlots + i;
+    if (lane < 27) {
+      if (lane < 6) N.par[lane * N.cap + dst] = B.par[lane * B.cap + src];
+      else N.err[(lane - 6) * N.cap + dst] = B.err[(lane - 6) * B.cap + src];
     }
-    if (lane == 0) {
-      int nfound = B.nfound[src], nmiss = B.nmiss[src], nin = B.ninside[src], ntl = B.ntail[src];
-      int nover = B.nover[src];
-      float chi2 = B.chi2[src];
-      int last = B.last[src];
-      float score = B.score[src];
-      int upd = 0;
-      if (n.is_extra) {
-        if (n.is_extra == 2) {
-          last = R.extra_last(n.parent);
-          ++nmiss;
-        }
-      } else {
-        add_hit_counts(n.hit, n.chi2hit, nfound, nmiss, nin, ntl, chi2);
-        last = arena_append(E, s, n.hit, layer, n.chi2hit, last);
-        score = n.score;
-        if (n.ov >= 0) {
-          const HitMatchPair& p = hm[n.parent];
-          add_hit_counts(p.hit[n.ov], p.chi2[n.ov], nfound, nmiss, nin, ntl, chi2);
-          last = arena_append(E, s, p.hit[n.ov], layer, p.chi2[n.ov], last);
-          ++nover;
-        }
-        upd = n.hit >= 0;
+  }
+  if (lane < n_pushed) {
+    const NewCand n = nc[lane];
+    const int src = s * kSlots + n.parent, dst = s * kSlots + lane;
+    int nfound = B.nfound[src], nmiss = B.nmiss[src], nin = B.ninside[src], ntl = B.ntail[src];
+    int nover = B.nover[src];
+    float chi2 = B.chi2[src];
+    int last = B.last[src];
+    float score = B.score[src];
+    int upd = 0;
+    if (n.is_extra) {
+      if (n.is_extra == 2) {
+        last = R.extra_last(n.parent);
+        ++nmiss;
       }
-      N.chg[dst] = B.chg[src];
-      N.chi2[dst] = chi2;
-      N.score[dst] = score;
-      N.last[dst] = last;
-      N.nfound[dst] = nfound;
-      N.nmiss[dst] = nmiss;
-      N.nover[dst] = nover;
-      N.ninside[dst] = nin;
-      N.ntail[dst] = ntl;
-      R.set_upd(i, upd);
+    } else {
+      add_hit_counts(n.hit, n.chi2hit, nfound, nmiss, nin, ntl, chi2);
+      last = arena_append(E, s, n.hit, layer, n.chi2hit, last);
+      score = n.score;
+      if (n.ov >= 0) {
+        const HitMatchPair& p = hm[n.parent];
+        add_hit_counts(p.hit[n.ov], p.chi2[n.ov], nfound, nmiss, nin, ntl, chi2);
+        last = arena_append(E, s, p.hit[n.ov], layer, p.chi2[n.ov], last);
+        ++nover;
+      }
+      upd = n.hit >= 0;
     }
+    N.chg[dst] = B.chg[src];
+    N.chi2[dst] = chi2;
+    N.score[dst] = score;
+    N.last[dst] = last;
+    N.nfound[dst] = nfound;
+    N.nmiss[dst] = nmiss;
+    N.nover[dst] = nover;
+    N.ninside[dst] = nin;
+    N.ntail[dst] = ntl;
+    R.set_upd(lane, upd);
   }
   return n_pushed;
 }

@@ -42,6 +42,7 @@ def _bind(lib):
     lib.mkfg_find_upload_batch.argtypes = [vp, ctypes.POINTER(MkfgEvent), ctypes.c_int32]
     lib.mkfg_find_run.argtypes = [vp]
     lib.mkfg_find_run_graph.argtypes = [vp]
+    lib.mkfg_find_backward_fit.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_int32]
     lib.mkfg_find_run_fused.argtypes = [vp, ctypes.c_int32]
     lib.mkfg_find_autotune.argtypes = [vp, ctypes.POINTER(ctypes.c_int32),
                                        ctypes.POINTER(ctypes.c_float)]
@@ -49,6 +50,7 @@ def _bind(lib):
     lib.mkfg_find_work.argtypes = [vp, i64p, i64p, i64p, ctypes.POINTER(ctypes.c_int32)]
     lib.mkfg_find_work_detail.argtypes = [vp, i64p, i64p]
     lib.mkfg_find_download.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(MkfgFindOut)]
+    lib.mkfg_find_download_best.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(MkfgFindOut)]
     lib.mkfg_find_event.argtypes = [vp, ctypes.POINTER(MkfgEvent), ctypes.POINTER(MkfgFindOut)]
     lib.mkfg_prepare_event_host.argtypes = [ctypes.POINTER(MkfgFindConfig),
                                             ctypes.POINTER(MkfgEvent), vp,
@@ -169,6 +171,14 @@ class Finder:
     def run_graph(self):
         capi.check(self.lib.mkfg_find_run_graph(self.ctx.handle))
 
+    def backward_fit(self, group_width=8):
+        """Backward fit of every seed's best candidate (MkBuilder::BackwardFit)
+        with the geometry's bkfit_last and backward-fit propagation flags."""
+        g = self.cfg.geom
+        self._bk_last = np.ascontiguousarray(g.bkfit_last, np.int32)
+        capi.check(self.lib.mkfg_find_backward_fit(self.ctx.handle, self._bk_last.ctypes.data,
+                                                   int(g.flags[3]), int(group_width)))
+
     def run_fused(self, seeds_per_block=0):
         """One launch for all layer steps; seeds_per_block 0 = tuned value."""
         capi.check(self.lib.mkfg_find_run_fused(self.ctx.handle, seeds_per_block))
@@ -189,6 +199,13 @@ class Finder:
         capi.check(self.lib.mkfg_find_work_detail(self.ctx.handle, ctypes.byref(e), ctypes.byref(c)))
         return dict(active_cands=a.value, hit_pairs=p.value, updates=u.value, steps=st.value,
                     chi2_evals=e.value, seed_steps=c.value)
+
+    def download_best(self, n_seeds):
+        """Best candidate per seed only (mkfg_find_download_best)."""
+        o = output_arrays(n_seeds, 1)
+        capi.check(self.lib.mkfg_find_download_best(self.ctx.handle, n_seeds,
+                                                    ctypes.byref(out_struct(o))))
+        return o
 
     def download(self, n_seeds):
         o = output_arrays(n_seeds, self.cfg.max_cands)

@@ -33,6 +33,7 @@ class Geometry:
         self.plans = self.arrays["plans"]
         self.plan_len = self.arrays["plan_len"]
         self.pickup = self.arrays["pickup"]
+        self.bkfit_last = self.arrays["bkfit_last"]
         self.region_order = self.arrays["region_order"]
         self.iter_params = self.arrays["iter_params"]
         self.flags = self.arrays["flags"]

@@ -185,6 +185,125 @@ def restate_fd_grad(rs, ev, theta, h_shift=1e-4, h_scale=1e-3, material=True):
     return g
 
 
+def backward_fit_groups(region_sorted, nn=8):
+    """Seed groups of MkBuilder::BackwardFit (mkFit/MkBuilder.cc:2153-2190)
+    for one event, as lists of sorted positions: per eta region, the seed
+    range is cut into tasks with grain clamp(n_seeds + 1, 4, 32) -- as the
+    oracle's task pool cuts a blocked_range: ceil(n / grain) near-equal
+    pieces -- and fit_cands takes groups of nn from each task's start."""
+    ns = len(region_sorted)
+    grain = min(max(ns + 1, 4), 32)
+    groups = []
+    b = 0
+    while b < ns:
+        e = b
+        while e < ns and region_sorted[e] == region_sorted[b]:
+            e += 1
+        n = e - b
+        pieces = (n + grain - 1) // grain
+        base, extra = divmod(n, pieces)
+        t0 = b
+        for i in range(pieces):
+            t1 = t0 + base + (1 if i < extra else 0)
+            for g0 in range(t0, t1, nn):
+                groups.append(list(range(g0, min(g0 + nn, t1))))
+            t0 = t1
+        b = e
+    return groups
+
+
+def restate_backward_fit(rs, ev, found, geom, m, nn=8):
+    """FP64 restatement of the backward fit of every seed's best candidate
+    (MkFinder::BkFitInputTracks / BkFitFitTracks / BkFitOutputTracks,
+    mkFit/MkFinder.cc:1368-1452, 1573-1742, driven as MkBuilder::BackwardFit)
+    from a finding result `found` (ref_find output before the backward fit):
+    covariance scaled by 100, reverse layer plan down to bkfit_last, hits
+    taken from the candidate's hit list backwards (first node of a layer,
+    holes skipped), NN-wide groups sharing layer skips, stand-in
+    measurements (own position, variance 666, no material) for members
+    without a hit. Returns par [ns][6], err [ns][21], chi2 [ns] (float64),
+    indexed by seed label."""
+    L = rs.lib
+    d6 = ctypes.c_double * 6
+    d21 = ctypes.c_double * 21
+    d3 = ctypes.c_double * 3
+    L.rs_propagate_to_r.restype = ctypes.c_int
+    L.rs_kalman_barrel.restype = ctypes.c_double
+    L.rs_kalman_endcap.restype = ctypes.c_double
+    rl = np.ascontiguousarray(geom.rl, np.float32)
+    xi = np.ascontiguousarray(geom.xi, np.float32)
+    mat = RsMaterial(rl.ctypes.data, xi.ctypes.data)
+    pflags = int(geom.flags[3])
+    barrel = geom.field("is_barrel") > 0.5
+    ns = ev.n_seeds
+    label_at = np.empty(ns, np.int64)
+    label_at[found["sorted_pos"]] = np.arange(ns)
+    hp = np.asarray(ev.hit_pos, np.float64)
+    he = np.asarray(ev.hit_err, np.float64)
+    lb = np.asarray(ev.layer_begin)
+    out_par = np.zeros((ns, 6))
+    out_err = np.zeros((ns, 21))
+    out_chi2 = np.zeros(ns)
+    for grp in backward_fit_groups(found["region"][label_at], nn):
+        labels = [int(label_at[p]) for p in grp]
+        reg = int(found["region"][labels[0]])
+        st = []
+        for s in labels:
+            slot = s * m
+            ntot = int(found["ntot"][slot])
+            st.append(dict(p=found["par"][slot].astype(np.float64).copy(),
+                           e=found["err"][slot].astype(np.float64) * 100.0,
+                           chg=int(found["chg"][slot]), k=ntot - 1,
+                           idx=found["hit_idx"][slot][:ntot], lyr=found["hit_lyr"][slot][:ntot],
+                           chi2=0.0))
+        for li in range(int(geom.plan_len[reg]) - 1, int(geom.bkfit_last[reg]) - 1, -1):
+            layer = int(geom.plans[reg][li])
+            meas = []
+            for t in st:
+                while t["k"] >= 0 and t["idx"][t["k"]] < 0:
+                    t["k"] -= 1
+                done = t["k"] < 0
+                here = (not done) and t["lyr"][t["k"]] == layer
+                if here:
+                    while t["k"] - 1 >= 0 and t["lyr"][t["k"] - 1] == layer:
+                        t["k"] -= 1
+                    g = lb[layer] + t["idx"][t["k"]]
+                    t["k"] -= 1
+                    meas.append((done, here, hp[:, g].copy(), he[:, g].copy()))
+                else:
+                    meas.append((done, here, t["p"][:3].copy(),
+                                 np.array([666.0, 0.0, 666.0, 0.0, 0.0, 666.0])))
+            if all(mm[0] for mm in meas):
+                break
+            if not any(mm[1] for mm in meas):
+                continue
+            for t, (done, here, mpos, merr) in zip(st, meas):
+                pin, ein = d6(*t["p"]), d21(*t["e"])
+                pp, pe = d6(), d21()
+                pf = pflags if here else (pflags & ~2)
+                if barrel[layer]:
+                    L.rs_propagate_to_r(pin, ein, t["chg"], ctypes.c_double(float(np.hypot(mpos[0], mpos[1]))),
+                                        pf, ctypes.byref(mat), pp, pe)
+                    op, oe = d6(), d21()
+                    c2 = L.rs_kalman_barrel(pp, pe, d3(*mpos), d6(*merr), op, oe)
+                else:
+                    L.rs_propagate_to_z(pin, ein, t["chg"], ctypes.c_double(float(mpos[2])), pf,
+                                        ctypes.byref(mat), pp, pe)
+                    op, oe = d6(), d21()
+                    c2 = L.rs_kalman_endcap(pp, pe, d3(*mpos), d6(*merr), op, oe)
+                t["p"] = np.array(op[:])
+                t["e"] = np.array(oe[:])
+                if t["p"][3] < 0:
+                    t["chg"] = -t["chg"]
+                    t["p"][3] = -t["p"][3]
+                t["chi2"] += c2
+        for s, t in zip(labels, st):
+            out_par[s] = t["p"]
+            out_err[s] = t["e"]
+            out_chi2[s] = t["chi2"]
+    return out_par, out_err, out_chi2
+
+
 def _load_find_api(lib):
     c_int_p = ctypes.POINTER(ctypes.c_int)
     lib.ref_cms2017_sizes.argtypes = [c_int_p, c_int_p, c_int_p]
@@ -218,12 +337,15 @@ def cms2017_export(reflib):
     return out
 
 
-def ref_find(reflib, ev, max_cands=6, chi2_cut=30.0, zero_c2=True, repeat=1):
+def ref_find(reflib, ev, max_cands=6, chi2_cut=30.0, zero_c2=True, repeat=1, backward_fit=False):
     """Reference clone-engine finding (find_tracks_load_seeds +
-    FindTracksCloneEngine) on a synth.CmsEvent. Returns a dict of per-seed
-    candidate arrays (see oracle/ref_driver.cc ref_find)."""
+    FindTracksCloneEngine, then MkBuilder::BackwardFit when backward_fit)
+    on a synth.CmsEvent. Returns a dict of per-seed candidate arrays (see
+    oracle/ref_driver.cc ref_find)."""
     lib = reflib.lib
     _load_find_api(lib)
+    lib.ref_set_backward_fit.argtypes = [ctypes.c_int]
+    lib.ref_set_backward_fit(1 if backward_fit else 0)
     ns = ev.n_seeds
     m = max_cands
     o = dict(n_cands=np.zeros(ns, np.int32), region=np.zeros(ns, np.int32),
@@ -245,6 +367,7 @@ def ref_find(reflib, ev, max_cands=6, chi2_cut=30.0, zero_c2=True, repeat=1):
                       int(repeat), o["n_cands"], o["region"], o["sorted_pos"], o["par"], o["err"],
                       o["chg"], o["chi2"], o["score"], o["nfound"], o["ntot"], o["noverlap"],
                       o["ninside"], o["ntail"], o["hit_idx"], o["hit_lyr"], ctypes.byref(secs))
+    lib.ref_set_backward_fit(0)
     if rc != 0:
         raise RuntimeError(f"ref_find failed rc={rc}")
     o["seconds"] = secs.value

@@ -52,6 +52,8 @@ double now_s() {
 }
 
 bool g_cms2017_loaded = false;
+// ref_find runs MkBuilder::BackwardFit after the clone engine when set.
+bool g_backward_fit = false;
 
 void set_material(const float* rl_grid, const float* xi_grid) {
   if (rl_grid && xi_grid) {
@@ -187,6 +189,11 @@ void ensure_cms2017() {
 }  // namespace
 
 extern "C" {
+
+// ref_find: also run the backward fit (MkBuilder::BackwardFit,
+// mkFit/MkBuilder.cc:2153-2253) on the best candidate of every seed, as
+// run_OneIteration does with do_backward_fit (mkFit/buildtestMPlex.cc).
+void ref_set_backward_fit(int on) { g_backward_fit = on != 0; }
 
 // Geometry export sizes: n_layers, n_regions, max plan length.
 int ref_cms2017_sizes(int* n_layers, int* n_regions, int* max_plan) {
@@ -344,6 +351,7 @@ int ref_find(int n_layers_in, const int* layer_begin, const float* hpos, const f
     builder.find_tracks_load_seeds(seeds);
     const double t0 = now_s();
     builder.FindTracksCloneEngine();
+    if (g_backward_fit) builder.BackwardFit();
     best = std::min(best, now_s() - t0);
     if (r + 1 < std::max(1, repeat)) builder.end_event();
   }

@@ -74,3 +74,28 @@ def test_reference_threads_deterministic(reflib):
     reflib.set_threads(1)
     for x, y in zip(a[:3], b[:3]):
         np.testing.assert_array_equal(x, y)
+
+
+def test_restated_backward_fit_matches_reference(reflib, restate):
+    """The FP64 restatement of the backward fit (oracle.restate_backward_fit,
+    with the reference's NN-wide seed groups) reproduces the reference's own
+    MkBuilder::BackwardFit from the same finding result, within the FP32
+    error of the reference's fit (median at rounding level)."""
+    import numpy as np
+    from mkfit_b200 import synth
+    from mkfit_b200.geometry import cms2017
+    from oracle.oracle import ref_find, restate_backward_fit
+    ev = synth.gen_cms_event(400, seed=7, noise_frac=0.01)
+    m = 6
+    ref0 = ref_find(reflib, ev, max_cands=m)
+    ref = ref_find(reflib, ev, max_cands=m, backward_fit=True)
+    par, err, chi2 = restate_backward_fit(restate, ev, ref0, cms2017(), m)
+    slots = np.arange(ev.n_seeds) * m
+    r = ref["chi2"][slots]
+    ok = np.isfinite(r) & np.isfinite(chi2) & (chi2 < 1e6)
+    assert ok.mean() > 0.99
+    rel = np.abs(r[ok] - chi2[ok]) / np.maximum(np.abs(chi2[ok]), 1e-3)
+    assert np.median(rel) < 1e-4, np.median(rel)
+    assert np.percentile(rel, 99) < 1e-2, np.percentile(rel, 99)
+    dpar = np.abs(ref["par"][slots][ok] - par[ok]) / np.sqrt(np.maximum(err[ok][:, [0, 2, 5, 9, 14, 20]], 1e-30))
+    assert np.median(dpar) < 1e-3
