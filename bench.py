@@ -49,11 +49,22 @@ PLAIN_TRACKS = 800
 FLOP_LAYER_PROP = 1000
 FLOP_HIT_CHI2 = 950
 FLOP_UPDATE = 1150
+# Kernels per layer-plan step in the graph form.
+KERNELS_PER_LAYER_STEP = 5
 # Fit (secondary metric): toy MC, 10 barrel layers.
 FIT_TRACKS_PER_EVENT = 20000
 FIT_EVENTS = 16
 FIT_LAYERS = 10
 FLOP_FIT_TRACK_LAYER = 1130
+# Differentiable fit: 50,000 toy tracks x 10 layers on a misaligned detector
+# (r-phi and z offsets N(0, 20 um), material scale 1 +- 0.1), gradient of
+# the summed chi2 w.r.t. 30 layer parameters at the nominal point.
+ADJ_TRACKS = 50000
+# High-pileup finding: 16 events x 10,000 helices, pT 0.3-50 GeV, |eta| < 2.5,
+# 5% noise plus pileup-like uniform noise bringing each event to ~600k hits.
+PU_EVENTS = 16
+PU_TRACKS = 10000
+PU_NOISE = 2.16
 
 
 def parse():
@@ -66,6 +77,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-fit", action="store_true")
+    p.add_argument("--no-pu", action="store_true")
     return p.parse_args()
 
 
@@ -215,6 +227,8 @@ def run_ours(args):
     from mkfit_b200 import synth
     plain_ev = synth.gen_cms_event(PLAIN_TRACKS, seed=0xC0DE + rank, noise_frac=0.01)
     fit_batch = None if args.no_fit else make_fit_batch(FIT_EVENTS, rank)
+    adj_ev = None if args.no_fit else adjoint_event(rank)
+    pu_events = None if args.no_pu else generate(pu_event_args(rank))
 
     import torch
     from mkfit_b200 import Context
@@ -279,7 +293,7 @@ def run_ours(args):
             t0 = time.perf_counter()
             finder.upload_batch(events)
             finder.run_graph()
-            out = finder.download(n_seeds)
+            out = finder.download_best(n_seeds)
             ts.append(time.perf_counter() - t0)
         h2d = sum(e.hit_pos.nbytes + e.hit_err.nbytes + e.hit_detid.nbytes + e.hit_cpcm.nbytes +
                   e.seed_par.nbytes + e.seed_err.nbytes + e.seed_chg.nbytes for e in events)
@@ -287,10 +301,13 @@ def run_ours(args):
         t = statistics.median(ts[1:])
         e2e = {"value": n_events / t, "unit": "events/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": t * 1e3,
-               "entry": "mkfg_find_upload_batch + mkfg_find_run_graph + mkfg_find_download "
-                        "(host hit-index build, seed partition, copies, export)"}
+               "entry": "mkfg_find_upload_batch + mkfg_find_run_graph + mkfg_find_download_best "
+                        "(host hit-index build, seed partition, copies, export of the best "
+                        "candidate per seed as MkBuilder::export_best_comb_cands)"}
 
     fit = None if fit_batch is None else run_fit(ctx, stream, fit_batch, args)
+    adjoint = None if adj_ev is None else run_adjoint(ctx, stream, adj_ev, args)
+    pu200 = None if pu_events is None else run_pu200(ctx, stream, finder, pu_events, args)
 
     peaks = load_measured_peaks()
     line = {
@@ -339,13 +356,18 @@ def run_ours(args):
             "hbm_peak_gbs": peaks.get("hbm_gbs"),
         },
         "e2e": e2e,
-        "gpu_launches": args.steps,
-        "gpu_launches_note": "one CUDA graph launch per step (reset + 4 kernels per layer step + merge)",
+        "gpu_launches": args.steps * (2 + KERNELS_PER_LAYER_STEP * work["steps"]),
+        "gpu_launches_note": (f"kernels in the timed region: one CUDA graph replay per step = reset + "
+                              f"{KERNELS_PER_LAYER_STEP} kernels x {work['steps']} layer steps + merge"),
         "clocks": clocks,
         "fit": fit,
+        "adjoint": adjoint,
+        "pu200": pu200,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_find(events)
+        if pu_events is not None:
+            line["cpu_baseline"]["pu200"] = cpu_baseline_find(pu_events, n_sample=2)
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -370,6 +392,82 @@ def run_fit(ctx, stream, batch, args):
             "workload": f"toy-MC Kalman fit, {FIT_EVENTS} events x {FIT_TRACKS_PER_EVENT} tracks x "
                         f"{FIT_LAYERS} barrel layers, material on, one launch",
             "achieved_tflops": flops / (t * 1e-3) / 1e12}
+
+
+def adjoint_event(rank):
+    from mkfit_b200 import synth
+    rng = np.random.default_rng(0xAD1 + rank)
+    return synth.gen_fit_event(ADJ_TRACKS, seed=0xAD10 + rank,
+                               align_rphi=rng.normal(0, 0.002, FIT_LAYERS),
+                               align_z=rng.normal(0, 0.002, FIT_LAYERS),
+                               mat_scale=1 + rng.uniform(-0.1, 0.1, FIT_LAYERS))
+
+
+def run_adjoint(ctx, stream, ev, args):
+    """Forward (summed chi2, checkpoints) + adjoint (30-parameter gradient)
+    through the C ABI, timed per step with CUDA events."""
+    import ctypes
+    import torch
+    from mkfit_b200 import capi
+    from mkfit_b200.align import AlignedFit, _bind
+    fit = AlignedFit(ctx, ev, material=True)
+    lib = ctx.lib
+    _bind(lib)
+    th = fit.nominal()
+    n = ev.n
+    dev = th.device
+    ckpt = torch.empty((fit.n_steps, 27, n), dtype=torch.float32, device=dev)
+    total = torch.empty((), dtype=torch.float64, device=dev)
+    grad = torch.empty((fit.n_steps, 3), dtype=torch.float64, device=dev)
+    gout = torch.ones((), dtype=torch.float32, device=dev)
+    a = fit._args(th, ckpt, total)
+    torch.cuda.synchronize()
+
+    def step():
+        capi.check(lib.mkfg_align_chi2_forward(ctx.handle, ctypes.byref(a)))
+        capi.check(lib.mkfg_align_chi2_backward(ctx.handle, ctypes.byref(a), gout.data_ptr(),
+                                                grad.data_ptr()))
+    for _ in range(args.warmup):
+        step()
+    ctx.synchronize()
+    ms = timed_events(stream, step, args.steps)
+    t = sum(ms) / len(ms)
+    g = grad.cpu().numpy()
+    return {"metric": "tracks/s (forward + adjoint)", "value": n / (t * 1e-3),
+            "unit": "tracks/s", "ms_per_step": t, "tracks_per_step": n,
+            "workload": (f"differentiable fit: {n} toy tracks x {FIT_LAYERS} barrel layers, "
+                         "misaligned detector (offsets N(0, 20 um), material scale 1 +- 0.1), "
+                         "summed chi2 and its gradient w.r.t. 30 layer parameters at nominal, "
+                         "FP32 forward with per-layer checkpoints + FP32 adjoint, 2 launches"),
+            "chi2_sum": float(total.item()),
+            "grad_norm": float(np.linalg.norm(g)),
+            "accuracy": "gradient vs FP64 central finite differences: tests/test_adjoint_gpu.py"}
+
+
+def pu_event_args(rank):
+    return [dict(n_tracks=PU_TRACKS, seed=0x9200 + 1000 * rank + i, pt_range=(0.3, 50.0),
+                 eta_max=2.5, noise_frac=PU_NOISE) for i in range(PU_EVENTS)]
+
+
+def run_pu200(ctx, stream, finder, events, args):
+    finder.upload_batch(events)
+    for _ in range(max(args.warmup, 1)):
+        finder.run_graph()
+    ctx.synchronize()
+    ms = timed_events(stream, finder.run_graph, max(3, args.steps // 2))
+    t = sum(ms) / len(ms)
+    work = finder.work()
+    flops = (work["active_cands"] * FLOP_LAYER_PROP + work["hit_pairs"] * FLOP_HIT_CHI2 +
+             work["updates"] * FLOP_UPDATE)
+    return {"metric": "events built/s", "value": len(events) / (t * 1e-3), "unit": "events/s",
+            "ms_per_step": t, "events_per_step": len(events),
+            "seeds_per_step": sum(e.n_seeds for e in events),
+            "hits_per_event": float(np.mean([e.n_hits for e in events])),
+            "workload": (f"PU200-like finding: {len(events)} events x {PU_TRACKS} helices "
+                         "(pT log-uniform 0.3-50 GeV, |eta| < 2.5, vertex sigma_z 5 cm), 5% noise "
+                         f"plus uniform pileup-like noise (noise fraction {PU_NOISE} in total) to "
+                         "reach ~600k hits per event, one CUDA-graph replay per step"),
+            "achieved_tflops": flops / (t * 1e-3) / 1e12, "work_per_step": work}
 
 
 def cpu_baseline_find(events, n_sample=8):
