@@ -33,14 +33,15 @@ constexpr int kBlock = 256;
 // Minimum resident blocks per SM requested for the heavy per-candidate
 // kernels (propagate, chi2, update): trades registers for occupancy.
 #ifndef MKFG_HEAVY_MIN_BLOCKS
-#define MKFG_HEAVY_MIN_BLOCKS 1
+#define MKFG_HEAVY_MIN_BLOCKS 2
 #endif
 
 // Appends `value` for the lanes where `want` holds to a two-ended list:
 // barrel entries from the front (counter cnt[0]), endcap entries from the
 // back (counter cnt[1]). One atomic per warp and end; all lanes call it.
 __device__ __forceinline__ void append_two_ended(bool want, bool barrel, int value, int* list,
-                                                 int cap, int* cnt, int lane) {
+                                                 int cap, int* cnt, int lane, int value2 = 0,
+                                                 int* list2 = nullptr) {
   const unsigned mb = __ballot_sync(0xffffffffu, want && barrel);
   const unsigned me = __ballot_sync(0xffffffffu, want && !barrel);
   int bb = 0, be = 0;
@@ -51,8 +52,21 @@ __device__ __forceinline__ void append_two_ended(bool want, bool barrel, int val
   bb = __shfl_sync(0xffffffffu, bb, 0);
   be = __shfl_sync(0xffffffffu, be, 0);
   const unsigned below = (1u << lane) - 1u;
-  if (want && barrel) list[bb + __popc(mb & below)] = value;
-  if (want && !barrel) list[cap - 1 - (be + __popc(me & below))] = value;
+  const int at = !want ? -1 : barrel ? bb + __popc(mb & below) : cap - 1 - (be + __popc(me & below));
+  if (want) {
+    list[at] = value;
+    if (list2) list2[at] = value2;
+  }
+}
+
+// Warp-aggregated append of `value` for the lanes where `want` holds.
+__device__ __forceinline__ void append_list(bool want, int value, int* list, int* cnt, int lane) {
+  const unsigned m = __ballot_sync(0xffffffffu, want);
+  if (!m) return;
+  int base = 0;
+  if (lane == 0) base = atomicAdd(cnt, __popc(m));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (want) list[base + __popc(m & ((1u << lane) - 1u))] = value;
 }
 
 //------------------------------------------------------------------------------
@@ -62,43 +76,47 @@ __device__ __forceinline__ void append_two_ended(bool want, bool barrel, int val
 __global__ void __launch_bounds__(kBlock) k_activate(EventDev E, const FindConfigDev* __restrict__ Cp,
                                                      int step) {
   const FindConfigDev& C = *Cp;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int s = t / kSlots, c = t % kSlots;
-  const bool in_range = s < E.n_seeds;
   const int lane = threadIdx.x & 31;
   const unsigned grp = 0xffu << (lane & ~7);
-
-  int reg = 0, layer = -1, state = kFinished, ncand = 0, buf = 0;
-  if (in_range) {
-    reg = E.region[s];
-    layer = plan_layer(C, reg, step);
-    state = wake_seed(C, reg, layer, step, E.state[s], E.pickup_layer[s]);
-    ncand = E.n_cands[s];
-    buf = E.cur[s];
-  }
-  const int slot = s * kSlots + c;
-  const bool active = in_range && layer >= 0 && state == kFinding && c < ncand &&
-                      cand_is_active(E, E.cand[buf], s, slot, layer);
-  const unsigned act = __ballot_sync(0xffffffffu, active) & grp;
+  int* cnt = E.step_count + step * kCntN;
+  // One thread per candidate slot, seeds in order (coalesced seed data).
   {
-    const unsigned all = __ballot_sync(0xffffffffu, active);
-    if (lane == 0 && all) atomicAdd(&E.work[step * 4 + 0], __popc(all));
-  }
-  if (in_range && c == 0) {
-    if (layer >= 0 && state == kFinding && act == 0) state = kFinished;
-    E.state[s] = state;
-  }
-  const bool barrel = active && C.layer[layer].is_barrel;
-  append_two_ended(active, barrel, slot, E.act_list, E.list_cap,
-                   E.step_count + step * kCntN + kCntActBarrel, lane);
-  // The clone step reads the records and extra flags of candidates
-  // [0, ncand) of seeds still finding: an inactive one among them has
-  // neither.
-  const bool seed_finding = layer >= 0 && state == kFinding && act != 0;
-  if (seed_finding && !active && c < ncand) {
-    const size_t rbase = (size_t)s * kRecPerSeed + c * kRecPerCand;
-    for (int h = 0; h <= kMaxXHits; ++h) E.rhit[rbase + h] = kRecInvalid;
-    E.wsr[slot] = kWsrOutside;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool in_range = t < E.n_seeds * kSlots;
+    const int s = in_range ? t / kSlots : 0, c = t % kSlots;
+    int reg = 0, layer = -1, state = kFinished, ncand = 0, buf = 0;
+    if (in_range) {
+      reg = E.region[s];
+      layer = plan_layer(C, reg, step);
+      state = wake_seed(C, reg, layer, step, E.state[s], E.pickup_layer[s]);
+      ncand = E.n_cands[s];
+      buf = E.cur[s];
+    }
+    const int slot = s * kSlots + c;
+    const bool active = in_range && layer >= 0 && state == kFinding && c < ncand &&
+                        cand_is_active(E, E.cand[buf], s, slot, layer);
+    const unsigned act = __ballot_sync(0xffffffffu, active) & grp;
+    {
+      const unsigned all = __ballot_sync(0xffffffffu, active);
+      if (lane == 0 && all) atomicAdd(&E.work[step * 4 + 0], __popc(all));
+    }
+    const bool seed_finding = layer >= 0 && state == kFinding && act != 0;
+    if (in_range && c == 0) {
+      if (layer >= 0 && state == kFinding && act == 0) state = kFinished;
+      E.state[s] = state;
+    }
+    const bool barrel = active && C.layer[layer].is_barrel;
+    append_two_ended(active, barrel, slot, E.act_list, E.list_cap, cnt + kCntActBarrel, lane);
+    // Seeds finding at this step go to the clone step.
+    append_list(in_range && c == 0 && seed_finding, s, E.find_list, cnt + kCntFind, lane);
+    // The clone step reads the records and extra flags of candidates
+    // [0, ncand) of seeds still finding: an inactive one among them has
+    // neither.
+    if (seed_finding && !active && c < ncand) {
+      const size_t rbase = (size_t)s * kRecPerSeed + c * kRecPerCand;
+      for (int h = 0; h <= kMaxXHits; ++h) E.rhit[rbase + h] = kRecInvalid;
+      E.wsr[slot] = kWsrOutside;
+    }
   }
 }
 
@@ -208,36 +226,40 @@ __global__ void __launch_bounds__(kBlock, MKFG_HEAVY_MIN_BLOCKS) k_chi2(EventDev
 __global__ void __launch_bounds__(kBlock) k_clone(EventDev E, const FindConfigDev* __restrict__ Cp,
                                                   int step) {
   const FindConfigDev& C = *Cp;
-  const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   __shared__ HitMatchPair s_hm[kBlock / 32][kSlots];
-  if (s >= E.n_seeds) return;
-  const int layer = plan_layer(C, E.region[s], step);
-  if (layer < 0) return;
-  // A seed that is not finding at this step has no records: nothing to do.
-  const int state = E.state[s];
-  if (state != kFinding) return;
-  const int cur = E.cur[s];
-  if (lane == 0) atomicAdd(&E.work[step * 4 + 3], 1);
-  const size_t rb = (size_t)s * kRecPerSeed;
-  const SeedRecords R{E.rhit + rb,          E.rscore + rb,           E.rchi2hit + rb,
+  HitMatchPair* hm = s_hm[threadIdx.x >> 5];
+  int* cnt = E.step_count + step * kCntN;
+  const int n_find = cnt[kCntFind];
+  const int n_warps = gridDim.x * (blockDim.x >> 5);
+  for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n_find; w += n_warps) {
+    // A seed finding at this step (listed by the activation kernel).
+    const int s = E.find_list[w];
+    const int layer = plan_layer(C, E.region[s], step);
+    const int cur = E.cur[s];
+    if (lane == 0) atomicAdd(&E.work[step * 4 + 3], 1);
+    const size_t rb = (size_t)s * kRecPerSeed;
+    const SeedRecords R{E.rhit + rb,          E.rscore + rb,           E.rchi2hit + rb,
                         E.rmodule + rb,       E.wsr + s * kSlots,      E.extra_last + s * kSlots,
                         E.upd + s * kSlots};
-  const int n = clone_seed(E, C, s, layer, state, E.n_cands[s], cur, R, s_hm[threadIdx.x >> 5], lane);
-  if (n >= 0 && lane == 0) {
-    E.n_cands[s] = n;
-    E.cur[s] = cur ^ 1;
+    const int n = clone_seed(E, C, s, layer, kFinding, E.n_cands[s], cur, R, hm, lane);
+    if (n >= 0 && lane == 0) {
+      E.n_cands[s] = n;
+      E.cur[s] = cur ^ 1;
+    }
+    // Compact list of the new candidates that take a Kalman update, with
+    // the global index of the hit to update with (on this step's layer).
+    __syncwarp();
+    const int u = lane < n ? E.upd[s * kSlots + lane] : 0;
+    const int g = u ? E.layer_begin[E.seed_event[s] * E.lb_stride + layer] + (u - 1) : 0;
+    append_two_ended(u != 0, C.layer[layer].is_barrel, s * kSlots + lane, E.upd_list, E.list_cap,
+                     cnt + kCntUpdBarrel, lane, g, E.upd_hit);
+    __syncwarp();  // hm is reused by the next seed of this warp
   }
-  // Compact list of the new candidates that take a Kalman update (their
-  // hit is on this step's layer).
-  __syncwarp();
-  const bool upd = lane < n && E.upd[s * kSlots + lane];
-  append_two_ended(upd, C.layer[layer].is_barrel, s * kSlots + lane, E.upd_list, E.list_cap,
-                   E.step_count + step * kCntN + kCntUpdBarrel, lane);
 }
 
 //------------------------------------------------------------------------------
-// Kernel 4: UpdateWithLastHit + CopyOutParErr for candidates that took a hit.
+// Kernel 4: UpdateWithLastHit + CopyOutParErr for the listed candidates.
 //------------------------------------------------------------------------------
 __global__ void __launch_bounds__(kBlock, MKFG_HEAVY_MIN_BLOCKS) k_update(EventDev E, const FindConfigDev* __restrict__ Cp,
                                                    int step) {
@@ -246,10 +268,12 @@ __global__ void __launch_bounds__(kBlock, MKFG_HEAVY_MIN_BLOCKS) k_update(EventD
   const int nb = cnt[kCntUpdBarrel], ne = cnt[kCntUpdEndcap];
   if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&E.work[step * 4 + 1], nb + ne);
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nb + ne; j += gridDim.x * blockDim.x) {
-    const int slot = j < nb ? E.upd_list[j] : E.upd_list[E.list_cap - 1 - (j - nb)];
+    const int at = j < nb ? j : E.list_cap - 1 - (j - nb);
+    const int slot = E.upd_list[at];
     const int s = slot / kSlots;
     E.upd[slot] = 0;
-    update_cand(E, C, s, E.layer_begin + E.seed_event[s] * E.lb_stride, E.cand[E.cur[s]], slot);
+    const LayerDev& L = C.layer[plan_layer(C, E.region[s], step)];
+    update_cand_at(E, C, L, E.upd_hit[at], E.cand[E.cur[s]], slot);
   }
 }
 
@@ -509,6 +533,8 @@ struct Finder {
   std::vector<int> h_region;
   std::vector<int> h_seed_off;
   DevBuf bk;  // backward-fit seed groups
+  HostBuf hits_h;  // pinned mirror of the hits buffer for the upload
+  HostBuf outb_h;  // pinned mirror of the export buffer for the download
   void drop_graph() {
     if (graph) cudaGraphExecDestroy(graph);
     graph = nullptr;
@@ -538,6 +564,8 @@ void finder_release(mkfg_context* ctx) {
   if (f->d_cfg) cudaFree(f->d_cfg);
   f->drop_graph();
   f->bk.release();
+  f->hits_h.release();
+  f->outb_h.release();
   f->hits.release();
   f->seeds.release();
   f->cands.release();
@@ -657,17 +685,59 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   const int NH = hit_off[n_ev], S = seed_off[n_ev];
   const int nb = f->n_bins;
 
+  // Hits go to the device in one copy from a pinned host mirror of the
+  // device layout; every event's worker writes its part of it.
+  const int NHs = std::max(NH, 1);
+  const size_t n_lb = (size_t)(L + 1) * n_ev, n_bins_all = (size_t)nb * n_ev;
+  const size_t hit_bytes = rounded(12 * (size_t)NHs) + rounded(24 * (size_t)NHs) +
+                           rounded(4 * (size_t)NHs) + rounded(4 * n_lb) + rounded(4 * n_bins_all) +
+                           rounded(8 * (size_t)NHs) + rounded(4 * (size_t)NHs);
+  int rc;
+  if ((rc = f->hits.ensure(hit_bytes))) return rc;
+  if ((rc = f->hits_h.ensure(hit_bytes))) return rc;
+  struct HitsLayout {
+    float* pos;
+    float* err;
+    uint32_t* info;
+    int* lb;
+    uint32_t* bins;
+    float2* qphi;
+    int* srank;
+  };
+  auto layout = [&](char* p) {
+    HitsLayout h;
+    h.pos = carve<float>(p, 3 * (size_t)NHs);
+    h.err = carve<float>(p, 6 * (size_t)NHs);
+    h.info = carve<uint32_t>(p, NHs);
+    h.lb = carve<int>(p, n_lb);
+    h.bins = carve<uint32_t>(p, n_bins_all);
+    h.qphi = carve<float2>(p, NHs);
+    h.srank = carve<int>(p, NHs);
+    return h;
+  };
+  const HitsLayout hh = layout(static_cast<char*>(f->hits_h.ptr));
+  const HitsLayout dh = layout(f->hits.as<char>());
+
   // Per-event host preparation (hit index, seed order), in parallel.
-  std::vector<EventHitsPrep> preps(n_ev);
   std::vector<SeedOrder> orders(n_ev);
   {
     auto work = [&](int e) {
       const mkfg_event* ev = evs + e;
-      const int nh = ev->layer_begin[L];
-      prepare_event_hits(f->binning, ev->layer_begin, L, ev->pos, nh, ev->detid, ev->cpcm, preps[e]);
+      const int nh = ev->layer_begin[L], o = hit_off[e];
+      EventHitsPrep prep;
+      prepare_event_hits(f->binning, ev->layer_begin, L, ev->pos, nh, ev->detid, ev->cpcm, prep);
       SeedInput si{ev->n_seeds, ev->seed_par, ev->seed_chg, ev->seed_nhits, ev->seed_hit_layer,
                    ev->seed_hit_index};
       partition_seeds_cms2017(f->layer_desc.data(), L, si, ev->layer_begin, ev->pos, nh, orders[e]);
+      for (int r = 0; r < 3; ++r)
+        std::memcpy(hh.pos + (size_t)r * NHs + o, ev->pos + (size_t)r * nh, 4 * (size_t)nh);
+      for (int r = 0; r < 6; ++r)
+        std::memcpy(hh.err + (size_t)r * NHs + o, ev->err + (size_t)r * nh, 4 * (size_t)nh);
+      for (int h = 0; h < nh; ++h) hh.qphi[o + h] = make_float2(prep.sq[h], prep.sphi[h]);
+      std::copy(prep.srank.begin(), prep.srank.end(), hh.srank + o);
+      std::copy(prep.hinfo.begin(), prep.hinfo.end(), hh.info + o);
+      std::copy(prep.bins.begin(), prep.bins.end(), hh.bins + (size_t)e * nb);
+      for (int l = 0; l <= L; ++l) hh.lb[(size_t)e * (L + 1) + l] = o + ev->layer_begin[l];
     };
     const int nthr = std::max(1, std::min(n_ev, (int)std::thread::hardware_concurrency()));
     std::vector<std::thread> pool;
@@ -679,67 +749,23 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     for (auto& th : pool) th.join();
   }
 
-  // Host staging of the concatenated arrays.
-  const int NHs = std::max(NH, 1);
-  std::vector<float> h_pos(3 * (size_t)NHs), h_err(6 * (size_t)NHs), h_sphi(NHs), h_sq(NHs);
-  std::vector<uint32_t> h_info(NHs), h_bins((size_t)nb * n_ev);
-  std::vector<int> h_srank(NHs), h_lb((size_t)(L + 1) * n_ev);
-  for (int e = 0; e < n_ev; ++e) {
-    const mkfg_event* ev = evs + e;
-    const int nh = ev->layer_begin[L], o = hit_off[e];
-    for (int r = 0; r < 3; ++r)
-      std::memcpy(&h_pos[(size_t)r * NHs + o], ev->pos + (size_t)r * nh, 4 * (size_t)nh);
-    for (int r = 0; r < 6; ++r)
-      std::memcpy(&h_err[(size_t)r * NHs + o], ev->err + (size_t)r * nh, 4 * (size_t)nh);
-    std::copy(preps[e].sphi.begin(), preps[e].sphi.end(), h_sphi.begin() + o);
-    std::copy(preps[e].sq.begin(), preps[e].sq.end(), h_sq.begin() + o);
-    std::copy(preps[e].srank.begin(), preps[e].srank.end(), h_srank.begin() + o);
-    std::copy(preps[e].hinfo.begin(), preps[e].hinfo.end(), h_info.begin() + o);
-    std::copy(preps[e].bins.begin(), preps[e].bins.end(), h_bins.begin() + (size_t)e * nb);
-    for (int l = 0; l <= L; ++l) h_lb[(size_t)e * (L + 1) + l] = o + ev->layer_begin[l];
-  }
-
   cudaStream_t st = ctx->stream;
-  int rc;
   auto up = [&](void* d, const void* h, size_t bytes) -> int {
     if (bytes == 0) return MKFG_OK;
     MKFG_CUDA_TRY(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st));
     return MKFG_OK;
   };
-  // ---- hits
-  {
-    const size_t need = rounded(12 * (size_t)NHs) + rounded(24 * (size_t)NHs) + 4 * rounded(4 * (size_t)NHs) +
-                        rounded(4 * h_lb.size()) + rounded(4 * h_bins.size()) + 4096;
-    if ((rc = f->hits.ensure(need))) return rc;
-    char* p = f->hits.as<char>();
-    float* d_pos = carve<float>(p, 3 * (size_t)NHs);
-    float* d_err = carve<float>(p, 6 * (size_t)NHs);
-    uint32_t* d_info = carve<uint32_t>(p, NHs);
-    int* d_lb = carve<int>(p, h_lb.size());
-    uint32_t* d_bins = carve<uint32_t>(p, h_bins.size());
-    float* d_sphi = carve<float>(p, NHs);
-    float* d_sq = carve<float>(p, NHs);
-    int* d_srank = carve<int>(p, NHs);
-    if ((rc = up(d_pos, h_pos.data(), 4 * h_pos.size()))) return rc;
-    if ((rc = up(d_err, h_err.data(), 4 * h_err.size()))) return rc;
-    if ((rc = up(d_info, h_info.data(), 4 * h_info.size()))) return rc;
-    if ((rc = up(d_lb, h_lb.data(), 4 * h_lb.size()))) return rc;
-    if ((rc = up(d_bins, h_bins.data(), 4 * h_bins.size()))) return rc;
-    if ((rc = up(d_sphi, h_sphi.data(), 4 * h_sphi.size()))) return rc;
-    if ((rc = up(d_sq, h_sq.data(), 4 * h_sq.size()))) return rc;
-    if ((rc = up(d_srank, h_srank.data(), 4 * h_srank.size()))) return rc;
-    f->ev.hpos = d_pos;
-    f->ev.herr = d_err;
-    f->ev.hstride = NHs;
-    f->ev.hinfo = d_info;
-    f->ev.layer_begin = d_lb;
-    f->ev.lb_stride = L + 1;
-    f->ev.n_bins = nb;
-    f->ev.bins = d_bins;
-    f->ev.sphi = d_sphi;
-    f->ev.sq = d_sq;
-    f->ev.srank = d_srank;
-  }
+  if ((rc = up(f->hits.ptr, f->hits_h.ptr, hit_bytes))) return rc;
+  f->ev.hpos = dh.pos;
+  f->ev.herr = dh.err;
+  f->ev.hstride = NHs;
+  f->ev.hinfo = dh.info;
+  f->ev.layer_begin = dh.lb;
+  f->ev.lb_stride = L + 1;
+  f->ev.n_bins = nb;
+  f->ev.bins = dh.bins;
+  f->ev.qphi = dh.qphi;
+  f->ev.srank = dh.srank;
   // ---- seeds, candidates, scratch, records, arena
   const int SS = std::max(S, 1);
   const int SC = SS * kSlots;
@@ -782,7 +808,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     f->ev.bshort_valid = carve<int>(p, SS);
   }
   {
-    const size_t need = rounded(4 * (size_t)SC) * (27 + 8) + 2 * rounded(4 * (size_t)SC * kMaxXHits) +
+    const size_t need = rounded(4 * (size_t)SC) * (27 + 10) + 2 * rounded(4 * (size_t)SC * kMaxXHits) +
                         rounded(4 * (size_t)(max_steps + 2)) * (1 + 4 + kCntN) + rounded(64) + 8192;
     if ((rc = f->scratch.ensure(need))) return rc;
     char* p = f->scratch.as<char>();
@@ -797,6 +823,8 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     f->ev.pair_count = carve<int>(p, max_steps + 2);
     f->ev.act_list = carve<int>(p, SC);
     f->ev.upd_list = carve<int>(p, SC);
+    f->ev.upd_hit = carve<int>(p, SC);
+    f->ev.find_list = carve<int>(p, SS);
     f->ev.list_cap = SC;
     f->ev.step_count = carve<int>(p, (size_t)kCntN * (max_steps + 2));
     f->ev.err_flags = carve<int>(p, 16);
@@ -924,15 +952,15 @@ static int enqueue_run(Finder* f, cudaStream_t st) {
   const int grid_w = (S * 32 + kBlock - 1) / kBlock;
   const int grid_p = std::min((S * kSlots * 4 + kBlock - 1) / kBlock, 148 * 16);
   const int grid_l = std::min(grid_c, 148 * 8);
-  k_reset<<<std::max(grid_c, (n_work + kBlock - 1) / kBlock), kBlock, 0, st>>>(f->ev, n_work);
   MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.pair_count, 0, 4 * (size_t)(f->host_cfg.max_steps + 2), st));
   MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.step_count, 0,
                                 4 * (size_t)kCntN * (f->host_cfg.max_steps + 2), st));
+  k_reset<<<std::max(grid_c, (n_work + kBlock - 1) / kBlock), kBlock, 0, st>>>(f->ev, n_work);
   for (int step = 1; step <= f->host_cfg.max_steps; ++step) {
     k_activate<<<grid_c, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
     k_propagate<<<grid_l, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
     k_chi2<<<std::max(grid_p, 1), kBlock, 0, st>>>(f->ev, f->d_cfg, step);
-    k_clone<<<grid_w, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+    k_clone<<<std::min(grid_w, 148 * 16), kBlock, 0, st>>>(f->ev, f->d_cfg, step);
     k_update<<<grid_l, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
   }
   k_merge<<<(S + 127) / 128, 128, 0, st>>>(f->ev, f->d_cfg);
@@ -1026,30 +1054,45 @@ static int download(mkfg_context* ctx, Finder* f, mkfg_find_out* out, int n_seed
   MKFG_CUDA_TRY(cudaMemsetAsync(O.n_cands, 0, 4 * (size_t)n_seeds_in, st));
   if (S > 0) k_export<<<(S * kSlots + 127) / 128, 128, 0, st>>>(f->ev, O);
   MKFG_CUDA_TRY(cudaGetLastError());
-  auto dn = [&](void* h, const void* d, size_t bytes) -> int {
-    if (!h) return MKFG_OK;
-    MKFG_CUDA_TRY(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, st));
-    return MKFG_OK;
-  };
-  const size_t ns = n_seeds_in;
-  if ((rc = dn(out->n_cands, O.n_cands, 4 * ns))) return rc;
-  if ((rc = dn(out->region, O.region, 4 * ns))) return rc;
-  if ((rc = dn(out->par, O.par, 4 * 6 * ns * m))) return rc;
-  if ((rc = dn(out->err, O.err, 4 * 21 * ns * m))) return rc;
-  if ((rc = dn(out->chg, O.chg, 4 * ns * m))) return rc;
-  if ((rc = dn(out->chi2, O.chi2, 4 * ns * m))) return rc;
-  if ((rc = dn(out->score, O.score, 4 * ns * m))) return rc;
-  if ((rc = dn(out->nfound, O.nfound, 4 * ns * m))) return rc;
-  if ((rc = dn(out->ntot, O.ntot, 4 * ns * m))) return rc;
-  if ((rc = dn(out->noverlap, O.noverlap, 4 * ns * m))) return rc;
-  if ((rc = dn(out->ninside, O.ninside, 4 * ns * m))) return rc;
-  if ((rc = dn(out->ntail, O.ntail, 4 * ns * m))) return rc;
-  if ((rc = dn(out->hit_idx, O.hit_idx, 4 * ns * m * kExportHits))) return rc;
-  if ((rc = dn(out->hit_lyr, O.hit_lyr, 4 * ns * m * kExportHits))) return rc;
-  int flags = 0;
-  MKFG_CUDA_TRY(cudaMemcpyAsync(&flags, f->ev.err_flags, 4, cudaMemcpyDeviceToHost, st));
+  // One device-to-host copy of the whole export into a pinned mirror, then
+  // the fields the caller asked for are copied out in parallel.
+  const size_t used = (size_t)(p - f->outb.as<char>());
+  if ((rc = f->outb_h.ensure(used + 64))) return rc;
+  char* hbase = static_cast<char*>(f->outb_h.ptr);
+  MKFG_CUDA_TRY(cudaMemcpyAsync(hbase, f->outb.ptr, used, cudaMemcpyDeviceToHost, st));
+  int* flags = reinterpret_cast<int*>(hbase + used);
+  MKFG_CUDA_TRY(cudaMemcpyAsync(flags, f->ev.err_flags, 4, cudaMemcpyDeviceToHost, st));
   MKFG_CUDA_TRY(cudaStreamSynchronize(st));
-  if (flags & kErrArena)
+  const size_t ns = n_seeds_in;
+  struct Field {
+    void* dst;
+    const void* dev;
+    size_t bytes;
+  };
+  const Field fields[] = {
+      {out->n_cands, O.n_cands, 4 * ns},         {out->region, O.region, 4 * ns},
+      {out->par, O.par, 4 * 6 * ns * m},         {out->err, O.err, 4 * 21 * ns * m},
+      {out->chg, O.chg, 4 * ns * m},             {out->chi2, O.chi2, 4 * ns * m},
+      {out->score, O.score, 4 * ns * m},         {out->nfound, O.nfound, 4 * ns * m},
+      {out->ntot, O.ntot, 4 * ns * m},           {out->noverlap, O.noverlap, 4 * ns * m},
+      {out->ninside, O.ninside, 4 * ns * m},     {out->ntail, O.ntail, 4 * ns * m},
+      {out->hit_idx, O.hit_idx, 4 * ns * m * kExportHits},
+      {out->hit_lyr, O.hit_lyr, 4 * ns * m * kExportHits}};
+  const int n_fields = (int)(sizeof(fields) / sizeof(fields[0]));
+  auto copy_field = [&](int i) {
+    const Field& fd = fields[i];
+    if (fd.dst && fd.bytes)
+      std::memcpy(fd.dst, hbase + (static_cast<const char*>(fd.dev) - f->outb.as<char>()), fd.bytes);
+  };
+  if (used > (size_t(8) << 20)) {
+    std::vector<std::thread> pool;
+    for (int i = 0; i < n_fields; ++i) pool.emplace_back(copy_field, i);
+    for (auto& th : pool) th.join();
+  } else {
+    for (int i = 0; i < n_fields; ++i) copy_field(i);
+  }
+  const int flag_bits = *flags;
+  if (flag_bits & kErrArena)
     return set_error(MKFG_ERR_OVERFLOW, "hit-on-track arena overflow (capacity %d per seed)",
                      f->ev.hot_cap);
   return MKFG_OK;

@@ -24,7 +24,7 @@ enum WsrCode { kWsrInside = 0, kWsrEdge = 1, kWsrOutside = 2 };
 enum ErrBits { kErrArena = 1, kErrLayerSize = 2 };
 enum StepCount {
   kCntActBarrel = 0, kCntActEndcap, kCntPairBarrel, kCntPairEndcap, kCntUpdBarrel, kCntUpdEndcap,
-  kCntN = 8
+  kCntFind, kCntN = 8
 };
 
 struct LayerDev {
@@ -79,8 +79,7 @@ struct EventDev {
   int n_bins;             // bins per event
   // Per-layer bins: (first | last << 16) over nq x 256 bins; sorted hits.
   const uint32_t* bins;
-  const float* sphi;
-  const float* sq;
+  const float2* qphi;  // (q, phi) of each sorted hit
   const int* srank;
   // Seeds in sorted order (index = seed slot s).
   int n_seeds;
@@ -123,7 +122,10 @@ struct EventDev {
   // from the back); counts in step_count[step][kCnt*].
   int* act_list;
   int* upd_list;
+  int* upd_hit;    // global index of the hit each listed update uses
   int list_cap;
+  // Plain form, per step: seeds finding at the step (for the clone kernel).
+  int* find_list;
   int* step_count; // [max_steps + 2][kCntN]
   int* err_flags;
   // Pristine initial state (restored by the reset kernel before every run).

@@ -164,8 +164,9 @@ __device__ __forceinline__ int select_hits(const EventDev& E, const LayerDev& L,
       for (int hi = first; hi < last; ++hi) {
         if (n >= kMaxXHits) break;
         const int g = hit_base + hi;
-        const float ddq = fabsf(q - __ldg(E.sq + g));
-        const float ddphi = cdist(fabsf(phi - __ldg(E.sphi + g)));
+        const float2 hq = __ldg(E.qphi + g);
+        const float ddq = fabsf(q - hq.x);
+        const float ddphi = cdist(fabsf(phi - hq.y));
         if (ddq >= dq) continue;
         if (ddphi >= dphi) continue;
         xhit[n * xstride] = __ldg(E.srank + g);
@@ -437,24 +438,18 @@ __device__ __forceinline__ bool eval_pair(const EventDev& E, const FindConfigDev
 
 // UpdateWithLastHit + CopyOutParErr for one candidate (mkFit/MkFinder.cc:
 // 1291-1335; kalmanPropagateAndUpdate[Endcap], KalmanUtilsMPlex.cc:471-505,
-// 697-731). Returns false if the last node is not a hit.
-__device__ __forceinline__ bool update_cand(const EventDev& E, const FindConfigDev& C, int s,
-                                            const int* lb, const CandSoA& B, int slot) {
+// 697-731), given the hit's global index g and its layer.
+__device__ __forceinline__ void update_cand_at(const EventDev& E, const FindConfigDev& C,
+                                               const LayerDev& L, int g, const CandSoA& B,
+                                               int slot) {
   float par[6], err[21];
   load_state(B, slot, par, err);
   int chg = B.chg[slot];
-  const int hv = node_hot_of(E, s, B.last[slot]);
-  const int hl = hot_layer(hv);
-  // After an arena overflow (reported through err_flags) the last node may
-  // not be a hit: skip rather than read outside the hit arrays.
-  if (hot_index(hv) < 0 || hl < 0 || hl >= C.n_layers) return false;
-  const int g = lb[hl] + hot_index(hv);
   float mpos[3], merr[6];
 #pragma unroll
   for (int e = 0; e < 3; ++e) mpos[e] = __ldg(E.hpos + e * E.hstride + g);
 #pragma unroll
   for (int e = 0; e < 6; ++e) merr[e] = __ldg(E.herr + e * E.hstride + g);
-  const LayerDev& L = C.layer[hl];
   float ppar[6], perr[21];
   if (L.is_barrel) {
     propagate_to_r(par, err, chg, hypot_f(mpos[0], mpos[1]), C.inter_pflags, C.mat, false, ppar, perr);
@@ -469,6 +464,18 @@ __device__ __forceinline__ bool update_cand(const EventDev& E, const FindConfigD
   }
   store_state(B, slot, par, err);
   B.chg[slot] = chg;
+}
+
+// UpdateWithLastHit with the hit found from the candidate's last node.
+// Returns false if the last node is not a hit.
+__device__ __forceinline__ bool update_cand(const EventDev& E, const FindConfigDev& C, int s,
+                                            const int* lb, const CandSoA& B, int slot) {
+  const int hv = node_hot_of(E, s, B.last[slot]);
+  const int hl = hot_layer(hv);
+  // After an arena overflow (reported through err_flags) the last node may
+  // not be a hit: skip rather than read outside the hit arrays.
+  if (hot_index(hv) < 0 || hl < 0 || hl >= C.n_layers) return false;
+  update_cand_at(E, C, C.layer[hl], lb[hl] + hot_index(hv), B, slot);
   return true;
 }
 
@@ -481,7 +488,8 @@ struct SeedRecords {
   const int* module_;
   const int* wsr_;         // WSR code | extra kind << 8, per candidate
   const int* extra_last_;  // stop node of a kind-2 extra, per candidate
-  int* upd_;               // per new candidate: needs UpdateWithLastHit
+  int* upd_;               // per new candidate: 1 + index in its layer of the hit
+                           // to update with (the last one added), 0 = none
   __device__ bool valid(int idx, int ncand) const {
     return idx / kRecPerCand < ncand && hit_[idx] != kRecInvalid;
   }
@@ -724,7 +732,8 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
         last = arena_append(E, s, p.hit[n.ov], layer, p.chi2[n.ov], last);
         ++nover;
       }
-      upd = n.hit >= 0;
+      // UpdateWithLastHit uses the last hit added: the overlap hit if any.
+      if (n.hit >= 0) upd = 1 + (n.ov >= 0 ? hm[n.parent].hit[n.ov] : n.hit);
     }
     N.chg[dst] = B.chg[src];
     N.chi2[dst] = chi2;

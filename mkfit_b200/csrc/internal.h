@@ -53,6 +53,27 @@ struct DevBuf {
   }
 };
 
+// Grow-only pinned host buffer (staging for large host-to-device copies).
+struct HostBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  int ensure(size_t need) {
+    if (need <= bytes) return MKFG_OK;
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    size_t want = need + need / 4 + 256;
+    MKFG_CUDA_TRY(cudaHostAlloc(&ptr, want, cudaHostAllocDefault));
+    bytes = want;
+    return MKFG_OK;
+  }
+  void release() {
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    bytes = 0;
+  }
+};
+
 }  // namespace mkfg
 
 struct mkfg_context {
