@@ -287,6 +287,12 @@ int mkfg_find_autotune(mkfg_context* ctx, int32_t* seeds_per_block, float* ms_pe
  * measurements as in the reference. Synchronizes the context stream. */
 int mkfg_find_backward_fit(mkfg_context* ctx, const int32_t* bkfit_last, uint32_t pflags,
                            int32_t group_width);
+/* The hit index the upload built on the device for uploaded event `event`
+ * (LayerOfHits after SuckInHits / EndRegistrationOfHits,
+ * mkFit/HitStructures.cc:77-338): bins in the layout of
+ * mkfg_prepare_event_host, and srank for the event's hits; either may be
+ * NULL. For checking the device build against the host one. */
+int mkfg_find_hit_index(mkfg_context* ctx, int32_t event, uint32_t* bins, int32_t* srank);
 /* Work done by the last run (for FLOP accounting): candidate propagations
  * to a layer, (candidate, hit) chi2 evaluations, Kalman updates, and the
  * number of layer-plan steps. No reference counterpart. */

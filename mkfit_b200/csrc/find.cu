@@ -18,6 +18,7 @@
 #include "internal.h"
 #include "find_host.h"
 #include "find_fused.cuh"
+#include "layer_hits.cuh"
 #include "find_steps.cuh"
 
 #include <algorithm>
@@ -527,11 +528,13 @@ struct Finder {
   int events_loaded = 0;
   cudaGraphExec_t graph = nullptr;  // captured run sequence of the current upload
   int fused_w = 16;                 // seeds per block of the fused form
+  int max_nq = 1;                   // largest number of q bins of a layer
   int64_t last_chi2_evals = 0, last_seeds_cloned = 0;
   // Host copies for the backward fit's seed groups: region of every sorted
   // seed and the first sorted seed of every event.
   std::vector<int> h_region;
   std::vector<int> h_seed_off;
+  std::vector<int> h_hit_off;
   DevBuf bk;  // backward-fit seed groups
   HostBuf hits_h;  // pinned mirror of the hits buffer for the upload
   HostBuf outb_h;  // pinned mirror of the export buffer for the download
@@ -629,6 +632,11 @@ extern "C" int mkfg_finder_setup(mkfg_context* ctx, const mkfg_find_config* cfg)
     L.is_pix = d[LC_IS_PIX] > 0.5f;
   }
   f->n_bins = off;
+  f->max_nq = 1;
+  for (const auto& b : f->binning) f->max_nq = std::max(f->max_nq, b.nq);
+  MKFG_REQUIRE(f->max_nq * kFineStride * 4 <= 200 * 1024,
+               "a layer has %d q bins; the device hit-index build supports up to %d",
+               f->max_nq, 200 * 1024 / (kFineStride * 4));
   H.n_layers = cfg->n_layers;
   H.n_regions = cfg->n_regions;
   int max_steps = 0;
@@ -685,47 +693,55 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   const int NH = hit_off[n_ev], S = seed_off[n_ev];
   const int nb = f->n_bins;
 
-  // Hits go to the device in one copy from a pinned host mirror of the
-  // device layout; every event's worker writes its part of it.
+  // Hits go to the device in one copy from a pinned host mirror: positions,
+  // errors, module ids, charges and layer offsets, which every event's
+  // worker writes; the hit index (module info, bin table, sorted (q, phi)
+  // and ranks) is then built on the device (layer_hits.cuh).
   const int NHs = std::max(NH, 1);
   const size_t n_lb = (size_t)(L + 1) * n_ev, n_bins_all = (size_t)nb * n_ev;
-  const size_t hit_bytes = rounded(12 * (size_t)NHs) + rounded(24 * (size_t)NHs) +
-                           rounded(4 * (size_t)NHs) + rounded(4 * n_lb) + rounded(4 * n_bins_all) +
+  const size_t up_bytes = rounded(12 * (size_t)NHs) + rounded(24 * (size_t)NHs) +
+                          2 * rounded(4 * (size_t)NHs) + rounded(4 * n_lb);
+  const size_t hit_bytes = up_bytes + rounded(4 * (size_t)NHs) + rounded(4 * n_bins_all) +
                            rounded(8 * (size_t)NHs) + rounded(4 * (size_t)NHs);
   int rc;
   if ((rc = f->hits.ensure(hit_bytes))) return rc;
-  if ((rc = f->hits_h.ensure(hit_bytes))) return rc;
+  if ((rc = f->hits_h.ensure(up_bytes))) return rc;
   struct HitsLayout {
     float* pos;
     float* err;
-    uint32_t* info;
+    int* detid;
+    int* cpcm;
     int* lb;
+    uint32_t* info;
     uint32_t* bins;
     float2* qphi;
     int* srank;
   };
-  auto layout = [&](char* p) {
-    HitsLayout h;
+  auto layout = [&](char* p, bool device) {
+    HitsLayout h{};
     h.pos = carve<float>(p, 3 * (size_t)NHs);
     h.err = carve<float>(p, 6 * (size_t)NHs);
-    h.info = carve<uint32_t>(p, NHs);
+    h.detid = carve<int>(p, NHs);
+    h.cpcm = carve<int>(p, NHs);
     h.lb = carve<int>(p, n_lb);
-    h.bins = carve<uint32_t>(p, n_bins_all);
-    h.qphi = carve<float2>(p, NHs);
-    h.srank = carve<int>(p, NHs);
+    if (device) {
+      h.info = carve<uint32_t>(p, NHs);
+      h.bins = carve<uint32_t>(p, n_bins_all);
+      h.qphi = carve<float2>(p, NHs);
+      h.srank = carve<int>(p, NHs);
+    }
     return h;
   };
-  const HitsLayout hh = layout(static_cast<char*>(f->hits_h.ptr));
-  const HitsLayout dh = layout(f->hits.as<char>());
+  const HitsLayout hh = layout(static_cast<char*>(f->hits_h.ptr), false);
+  const HitsLayout dh = layout(f->hits.as<char>(), true);
 
-  // Per-event host preparation (hit index, seed order), in parallel.
+  // Per-event host work (seed order; copies into the pinned mirror), in
+  // parallel.
   std::vector<SeedOrder> orders(n_ev);
   {
     auto work = [&](int e) {
       const mkfg_event* ev = evs + e;
       const int nh = ev->layer_begin[L], o = hit_off[e];
-      EventHitsPrep prep;
-      prepare_event_hits(f->binning, ev->layer_begin, L, ev->pos, nh, ev->detid, ev->cpcm, prep);
       SeedInput si{ev->n_seeds, ev->seed_par, ev->seed_chg, ev->seed_nhits, ev->seed_hit_layer,
                    ev->seed_hit_index};
       partition_seeds_cms2017(f->layer_desc.data(), L, si, ev->layer_begin, ev->pos, nh, orders[e]);
@@ -733,10 +749,8 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
         std::memcpy(hh.pos + (size_t)r * NHs + o, ev->pos + (size_t)r * nh, 4 * (size_t)nh);
       for (int r = 0; r < 6; ++r)
         std::memcpy(hh.err + (size_t)r * NHs + o, ev->err + (size_t)r * nh, 4 * (size_t)nh);
-      for (int h = 0; h < nh; ++h) hh.qphi[o + h] = make_float2(prep.sq[h], prep.sphi[h]);
-      std::copy(prep.srank.begin(), prep.srank.end(), hh.srank + o);
-      std::copy(prep.hinfo.begin(), prep.hinfo.end(), hh.info + o);
-      std::copy(prep.bins.begin(), prep.bins.end(), hh.bins + (size_t)e * nb);
+      std::memcpy(hh.detid + o, ev->detid, 4 * (size_t)nh);
+      std::memcpy(hh.cpcm + o, ev->cpcm, 4 * (size_t)nh);
       for (int l = 0; l <= L; ++l) hh.lb[(size_t)e * (L + 1) + l] = o + ev->layer_begin[l];
     };
     const int nthr = std::max(1, std::min(n_ev, (int)std::thread::hardware_concurrency()));
@@ -755,7 +769,26 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     MKFG_CUDA_TRY(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st));
     return MKFG_OK;
   };
-  if ((rc = up(f->hits.ptr, f->hits_h.ptr, hit_bytes))) return rc;
+  if ((rc = up(f->hits.ptr, f->hits_h.ptr, up_bytes))) return rc;
+  {
+    LayerHitsArgs A;
+    A.pos = dh.pos;
+    A.hstride = NHs;
+    A.detid = dh.detid;
+    A.cpcm = dh.cpcm;
+    A.layer_begin = dh.lb;
+    A.lb_stride = L + 1;
+    A.n_layers = L;
+    A.hinfo = dh.info;
+    A.bins = dh.bins;
+    A.n_bins = nb;
+    A.qphi = dh.qphi;
+    A.srank = dh.srank;
+    const int smem = f->max_nq * kFineStride * 4;
+    MKFG_CUDA_TRY(cudaFuncSetAttribute(k_layer_hits, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    k_layer_hits<<<n_ev * L, kHitsBlock, smem, st>>>(A, f->d_cfg);
+    MKFG_CUDA_TRY(cudaGetLastError());
+  }
   f->ev.hpos = dh.pos;
   f->ev.herr = dh.err;
   f->ev.hstride = NHs;
@@ -937,6 +970,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   f->n_events = n_ev;
   f->h_region.assign(region.begin(), region.begin() + S);
   f->h_seed_off = seed_off;
+  f->h_hit_off = hit_off;
   f->events_loaded = 1;
   return MKFG_OK;
 }
@@ -1239,6 +1273,24 @@ extern "C" int mkfg_find_backward_fit(mkfg_context* ctx, const int32_t* bkfit_la
   k_bkfit<<<(A.n_groups + per_block - 1) / per_block, kBlock, 0, ctx->stream>>>(f->ev, f->d_cfg, A);
   MKFG_CUDA_TRY(cudaGetLastError());
   // The group list is host memory: finish the copy before it goes away.
+  MKFG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return MKFG_OK;
+}
+
+extern "C" int mkfg_find_hit_index(mkfg_context* ctx, int32_t event, uint32_t* bins,
+                                   int32_t* srank) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  Finder* f = finder_of(ctx);
+  MKFG_REQUIRE(f->events_loaded, "no event uploaded");
+  MKFG_REQUIRE(event >= 0 && event < f->n_events, "event %d out of range", event);
+  const int nh = f->h_hit_off[event + 1] - f->h_hit_off[event];
+  if (bins)
+    MKFG_CUDA_TRY(cudaMemcpyAsync(bins, f->ev.bins + (size_t)event * f->ev.n_bins,
+                                  4 * (size_t)f->ev.n_bins, cudaMemcpyDeviceToHost, ctx->stream));
+  if (srank && nh > 0)
+    MKFG_CUDA_TRY(cudaMemcpyAsync(srank, f->ev.srank + f->h_hit_off[event], 4 * (size_t)nh,
+                                  cudaMemcpyDeviceToHost, ctx->stream));
   MKFG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   return MKFG_OK;
 }

@@ -43,6 +43,7 @@ def _bind(lib):
     lib.mkfg_find_run.argtypes = [vp]
     lib.mkfg_find_run_graph.argtypes = [vp]
     lib.mkfg_find_backward_fit.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_int32]
+    lib.mkfg_find_hit_index.argtypes = [vp, ctypes.c_int32, vp, vp]
     lib.mkfg_find_run_fused.argtypes = [vp, ctypes.c_int32]
     lib.mkfg_find_autotune.argtypes = [vp, ctypes.POINTER(ctypes.c_int32),
                                        ctypes.POINTER(ctypes.c_float)]
@@ -199,6 +200,15 @@ class Finder:
         capi.check(self.lib.mkfg_find_work_detail(self.ctx.handle, ctypes.byref(e), ctypes.byref(c)))
         return dict(active_cands=a.value, hit_pairs=p.value, updates=u.value, steps=st.value,
                     chi2_evals=e.value, seed_steps=c.value)
+
+    def hit_index(self, event, n_bins, n_hits):
+        """The device-built hit index of uploaded event `event`:
+        (bins[n_bins], srank[n_hits])."""
+        bins = np.zeros(n_bins, np.uint32)
+        srank = np.zeros(n_hits, np.int32)
+        capi.check(self.lib.mkfg_find_hit_index(self.ctx.handle, int(event), bins.ctypes.data,
+                                                srank.ctypes.data))
+        return bins, srank
 
     def download_best(self, n_seeds):
         """Best candidate per seed only (mkfg_find_download_best)."""

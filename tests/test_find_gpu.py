@@ -251,3 +251,27 @@ def test_download_best_is_slot_zero(gpu_ctx):
     np.testing.assert_array_equal(best["n_cands"], np.minimum(full["n_cands"], 1))
     for k in ("par", "err", "chg", "chi2", "score", "nfound", "ntot", "hit_idx", "hit_lyr"):
         np.testing.assert_array_equal(best[k], full[k][::M], err_msg=k)
+
+
+def test_device_hit_index_equals_host(gpu_ctx):
+    """The hit index built on the device at upload (bins, sorted ranks) is
+    bit-identical to the host build (itself checked against the reference's
+    LayerOfHits in test_find_prep.py), including hits whose phi rounds to
+    +pi (fine phi bin 1024) and a dense event."""
+    from mkfit_b200.finder import prepare_event_host
+    evs = [synth.gen_cms_event(n, seed=500 + n, noise_frac=nf) for n, nf in ((400, 0.02), (3000, 0.5))]
+    ev = evs[0]
+    # Put a few hits of some layers on the -x axis: phi = +pi exactly or by rounding.
+    for l in (3, 20, 50):
+        h = int(ev.layer_begin[l])
+        if ev.layer_begin[l + 1] - h >= 2:
+            r = float(np.hypot(ev.hit_pos[0, h], ev.hit_pos[1, h]))
+            ev.hit_pos[0, h], ev.hit_pos[1, h] = -r, 0.0
+            ev.hit_pos[0, h + 1], ev.hit_pos[1, h + 1] = -r, 1e-9
+    fnd = Finder(gpu_ctx, FindConfig(max_cands=M))
+    fnd.upload_batch(evs)
+    for e, ev in enumerate(evs):
+        host = prepare_event_host(ev)
+        bins, srank = fnd.hit_index(e, host["bins"].size, ev.n_hits)
+        np.testing.assert_array_equal(bins, host["bins"], err_msg=f"bins of event {e}")
+        np.testing.assert_array_equal(srank, host["srank"], err_msg=f"ranks of event {e}")
