@@ -85,9 +85,10 @@ def parse():
 def find_event_args(n_events, rank):
     from mkfit_b200 import synth
     from mkfit_b200.geometry import cms2017
-    sizes = synth.batch_event_sizes(n_events, FIND_MEAN_TRACKS, 500, 12000, seed=0xB200 + rank)
+    from mkfit_b200.dist import rank_seed
+    sizes = synth.batch_event_sizes(n_events, FIND_MEAN_TRACKS, 500, 12000, seed=rank_seed(0xB200, rank))
     ramp = synth.density_ramp(cms2017().n_layers, FIND_DENSITY_RATIO)
-    return [dict(n_tracks=int(n), seed=0xE000 + 1000 * rank + i, noise_frac=FIND_NOISE,
+    return [dict(n_tracks=int(n), seed=rank_seed(0xE000, rank) + i, noise_frac=FIND_NOISE,
                  noise_scale=ramp) for i, n in enumerate(sizes)]
 
 
@@ -162,36 +163,6 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def dist_setup():
-    import torch
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-    return world, rank, local
-
-
-def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
-
-
-def max_over_ranks(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
 def load_measured_peaks():
     try:
         return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -233,7 +204,8 @@ def run_ours(args):
     import torch
     from mkfit_b200 import Context
     from mkfit_b200.finder import FindConfig, Finder
-    world, rank, local = dist_setup()
+    from mkfit_b200 import dist as mdist
+    world, rank, local = mdist.setup()
     torch.cuda.set_device(local)
     ctx = Context(local)
     stream = ctx.torch_stream()
@@ -262,7 +234,7 @@ def run_ours(args):
     work = finder.work()
     peak = fp32_peak(ctx)
     sampler = ClockSampler(local)
-    barrier(world)
+    mdist.barrier(world)
     torch.cuda.synchronize()
     sampler.start()
     t_load = time.perf_counter() + 1.5  # let the sampler see the clocks under load
@@ -272,10 +244,10 @@ def run_ours(args):
         ctx.synchronize()
     step_ms = timed_events(stream, finder.run_graph, args.steps)
     clocks = sampler.stop()
-    barrier(world)
+    mdist.barrier(world)
     total_ms = sum(step_ms)
-    total_ms_max = max_over_ranks(total_ms, world)
-    value = world * n_events * args.steps / (total_ms_max * 1e-3)
+    total_ms_max = mdist.max_over_ranks(total_ms, world)
+    value = mdist.aggregate_rate(n_events, args.steps, total_ms_max * 1e-3, world)
     ms_step = total_ms / args.steps
 
     flops = (work["active_cands"] * FLOP_LAYER_PROP + work["hit_pairs"] * FLOP_HIT_CHI2 +
@@ -371,9 +343,7 @@ def run_ours(args):
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    mdist.teardown(world)
 
 
 def run_fit(ctx, stream, batch, args):

@@ -287,6 +287,27 @@ int mkfg_find_autotune(mkfg_context* ctx, int32_t* seeds_per_block, float* ms_pe
  * measurements as in the reference. Synchronizes the context stream. */
 int mkfg_find_backward_fit(mkfg_context* ctx, const int32_t* bkfit_last, uint32_t pflags,
                            int32_t group_width);
+/* Output selection of run_OneIteration after a run (and backward fit):
+ * every seed's best candidate is dropped if its covariance has a negative
+ * diagonal or a non-finite element (StdSeq::qfilter_nan_n_silly with
+ * filter_comb_cands, mkFit/MkBuilder.cc:279-314), the rest are compared in
+ * pairs within their event and the lower-score track of a duplicate pair
+ * is dropped (StdSeq::find_duplicates_sharedhits_pixelseed,
+ * mkFit/MkStdSeqs.cc:510-603, used by find_and_remove_duplicates for
+ * iterations with m_requires_dupclean_tight). keep[n_seeds] (host, by
+ * input seed) receives 1 for the survivors. The config holds the
+ * iteration's duplicate parameters (IterationConfig::set_dupl_params) and
+ * the reference's window constants (Config::maxd1pt, maxdphi, maxdcth,
+ * maxcth_ob, maxcth_fw). */
+typedef struct {
+  float frac_shared_hits;
+  float drth_central, drth_obarrel, drth_forward;
+  float max_d_invpt, max_d_phi, max_d_cottheta;
+  float max_cottheta_obarrel, max_cottheta_forward;
+} mkfg_select_config;
+
+int mkfg_find_select(mkfg_context* ctx, const mkfg_select_config* cfg, int32_t n_seeds,
+                     int32_t* keep);
 /* The hit index the upload built on the device for uploaded event `event`
  * (LayerOfHits after SuckInHits / EndRegistrationOfHits,
  * mkFit/HitStructures.cc:77-338): bins in the layout of

@@ -436,6 +436,110 @@ __global__ void __launch_bounds__(kBlock) k_bkfit(EventDev E, const FindConfigDe
 }
 
 //------------------------------------------------------------------------------
+// Output selection of run_OneIteration (mkFit/buildtestMPlex.cc:721-731):
+// qfilter_nan_n_silly on every seed's best candidate, export of the best
+// candidates without their missing hits, then duplicate removal
+// (find_duplicates_sharedhits_pixelseed, mkFit/MkStdSeqs.cc:510-603: the
+// variant of the iterations with m_requires_dupclean_tight). A pair's
+// verdict depends only on the pair, so every pair is tested at once; of a
+// duplicate pair the lower score loses (the earlier track on a tie).
+//------------------------------------------------------------------------------
+struct SelectArgs {
+  int* hot;       // [S][kExportHits] hits of the exported best candidate
+  int* nhit;      // [S]
+  float* phi;
+  float* cth;     // 1 / tan(theta)
+  float* ipt;
+  float* score;
+  int* nfound;
+  int* keep;      // [S] 1: exported and not (yet) a duplicate
+  float frac, drth_central, drth_obarrel, drth_forward;
+  float maxd1pt, maxdphi, maxdcth, maxcth_ob, maxcth_fw;
+};
+
+__global__ void k_select_prep(EventDev E, const SelectArgs A) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= E.n_seeds) return;
+  A.keep[s] = 0;
+  A.nhit[s] = 0;
+  if (E.n_cands[s] == 0) return;  // empty comb candidate: nothing exported
+  const CandSoA& B = E.cand[E.cur[s]];
+  const int slot = s * kSlots;
+  // TrackBase::hasNanNSillyValues (Track.cc:177-192).
+  bool silly = false;
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j <= i; ++j) {
+      const float v = B.err[sidx(i, j) * B.cap + slot];
+      if ((i == j && v < 0.f) || !isfinite(v)) silly = true;
+    }
+  if (silly) return;
+  // exportTrack(true): the found hits in order (TrackCand, HitStructures.cc:448-478).
+  const int nfound = B.nfound[slot];
+  int node = B.last[slot];
+  int pos = min(nfound, kExportHits);
+  for (int k = B.nfound[slot] + B.nmiss[slot] - 1; k >= 0 && node >= 0; --k) {
+    const int hv = node_hot_of(E, s, node);
+    if (hot_index(hv) >= 0 && pos > 0) A.hot[(size_t)s * kExportHits + (--pos)] = hv;
+    node = E.node_prev[(size_t)s * E.hot_cap + node];
+  }
+  A.nhit[s] = min(nfound, kExportHits);
+  A.phi[s] = B.par[4 * B.cap + slot];
+  A.cth[s] = 1.f / f_tan(B.par[5 * B.cap + slot]);
+  A.ipt[s] = B.par[3 * B.cap + slot];
+  A.score[s] = B.score[slot];
+  A.nfound[s] = nfound;
+  A.keep[s] = 1;
+}
+
+__device__ __forceinline__ float squash_phi_minimal(float phi) {
+  return phi >= kPI ? phi - kTwoPI : (phi < -kPI ? phi + kTwoPI : phi);
+}
+
+__global__ void k_select_dups(EventDev E, const SelectArgs A, int* __restrict__ dup) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= E.n_seeds || !A.keep[i]) return;
+  const int ev = E.seed_event[i];
+  const float phi1 = A.phi[i], cth1 = A.cth[i], ipt1 = A.ipt[i], sc1 = A.score[i];
+  const int label1 = E.seed_label[i];
+  float max_dr2 = A.drth_central * A.drth_central;
+  if (fabsf(cth1) > A.maxcth_fw) max_dr2 = A.drth_forward * A.drth_forward;
+  else if (fabsf(cth1) > A.maxcth_ob) max_dr2 = A.drth_obarrel * A.drth_obarrel;
+  const int* h1 = A.hot + (size_t)i * kExportHits;
+  const int n1 = A.nhit[i];
+  for (int j = i + 1; j < E.n_seeds && E.seed_event[j] == ev; ++j) {
+    if (!A.keep[j] || E.seed_label[j] == label1) continue;
+    const float dcth = fabsf(A.cth[j] - cth1);
+    if (dcth > A.maxdcth) continue;
+    const float dphi = fabsf(squash_phi_minimal(phi1 - A.phi[j]));
+    if (dphi > A.maxdphi) continue;
+    const float dr2 = __fadd_rn(__fmul_rn(dphi, dphi), __fmul_rn(dcth, dcth));
+    bool is_dup = dr2 < max_dr2;
+    if (!is_dup) {
+      if (fabsf(A.ipt[j] - ipt1) > A.maxd1pt) continue;
+      const int* h2 = A.hot + (size_t)j * kExportHits;
+      const int n2 = A.nhit[j];
+      int shared = 0, shared_first = 0;
+      for (int a = 0; a < n1; ++a)
+        for (int b = 0; b < n2; ++b)
+          if (h1[a] == h2[b]) {
+            ++shared;
+            if (a == 0 && b == 0) ++shared_first;
+          }
+      const int min_found = min(A.nfound[i], A.nfound[j]);
+      is_dup = (float)(shared - shared_first) >= (float)(min_found - shared_first) * A.frac;
+    }
+    if (is_dup) dup[sc1 > A.score[j] ? j : i] = 1;
+  }
+}
+
+__global__ void k_select_out(EventDev E, const SelectArgs A, const int* __restrict__ dup,
+                             int* __restrict__ keep_by_label) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= E.n_seeds) return;
+  keep_by_label[E.seed_label[s]] = A.keep[s] && !dup[s];
+}
+
+//------------------------------------------------------------------------------
 // Kernel 6: export (TrackCand::exportTrack, mkFit/HitStructures.cc:448-478).
 //------------------------------------------------------------------------------
 struct FindOutDev {
@@ -536,6 +640,7 @@ struct Finder {
   std::vector<int> h_seed_off;
   std::vector<int> h_hit_off;
   DevBuf bk;  // backward-fit seed groups
+  DevBuf sel;  // output selection scratch
   HostBuf hits_h;  // pinned mirror of the hits buffer for the upload
   HostBuf outb_h;  // pinned mirror of the export buffer for the download
   void drop_graph() {
@@ -567,6 +672,7 @@ void finder_release(mkfg_context* ctx) {
   if (f->d_cfg) cudaFree(f->d_cfg);
   f->drop_graph();
   f->bk.release();
+  f->sel.release();
   f->hits_h.release();
   f->outb_h.release();
   f->hits.release();
@@ -1292,6 +1398,50 @@ extern "C" int mkfg_find_hit_index(mkfg_context* ctx, int32_t event, uint32_t* b
     MKFG_CUDA_TRY(cudaMemcpyAsync(srank, f->ev.srank + f->h_hit_off[event], 4 * (size_t)nh,
                                   cudaMemcpyDeviceToHost, ctx->stream));
   MKFG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return MKFG_OK;
+}
+
+extern "C" int mkfg_find_select(mkfg_context* ctx, const mkfg_select_config* cfg, int32_t n_seeds,
+                                int32_t* keep) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  Finder* f = finder_of(ctx);
+  MKFG_REQUIRE(cfg != nullptr && keep != nullptr, "null argument");
+  MKFG_REQUIRE(f->events_loaded && n_seeds == f->n_seeds, "seed count mismatch");
+  const int S = f->n_seeds;
+  if (S == 0) return MKFG_OK;
+  const size_t need = rounded(4 * (size_t)S * kExportHits) + 9 * rounded(4 * (size_t)S) + 4096;
+  if ((rc = f->sel.ensure(need))) return rc;
+  char* p = f->sel.as<char>();
+  SelectArgs A;
+  A.hot = carve<int>(p, (size_t)S * kExportHits);
+  A.nhit = carve<int>(p, S);
+  A.phi = carve<float>(p, S);
+  A.cth = carve<float>(p, S);
+  A.ipt = carve<float>(p, S);
+  A.score = carve<float>(p, S);
+  A.nfound = carve<int>(p, S);
+  A.keep = carve<int>(p, S);
+  int* dup = carve<int>(p, S);
+  int* d_keep = carve<int>(p, S);
+  A.frac = cfg->frac_shared_hits;
+  A.drth_central = cfg->drth_central;
+  A.drth_obarrel = cfg->drth_obarrel;
+  A.drth_forward = cfg->drth_forward;
+  A.maxd1pt = cfg->max_d_invpt;
+  A.maxdphi = cfg->max_d_phi;
+  A.maxdcth = cfg->max_d_cottheta;
+  A.maxcth_ob = cfg->max_cottheta_obarrel;
+  A.maxcth_fw = cfg->max_cottheta_forward;
+  cudaStream_t st = ctx->stream;
+  MKFG_CUDA_TRY(cudaMemsetAsync(dup, 0, 4 * (size_t)S, st));
+  const int grid = (S + 127) / 128;
+  k_select_prep<<<grid, 128, 0, st>>>(f->ev, A);
+  k_select_dups<<<grid, 128, 0, st>>>(f->ev, A, dup);
+  k_select_out<<<grid, 128, 0, st>>>(f->ev, A, dup, d_keep);
+  MKFG_CUDA_TRY(cudaGetLastError());
+  MKFG_CUDA_TRY(cudaMemcpyAsync(keep, d_keep, 4 * (size_t)S, cudaMemcpyDeviceToHost, st));
+  MKFG_CUDA_TRY(cudaStreamSynchronize(st));
   return MKFG_OK;
 }
 

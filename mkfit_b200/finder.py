@@ -21,6 +21,19 @@ class MkfgFindConfig(ctypes.Structure):
                 ("requires_prop_to_hit", ctypes.c_int32)]
 
 
+class MkfgSelectConfig(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_float) for k in (
+        "frac_shared_hits", "drth_central", "drth_obarrel", "drth_forward", "max_d_invpt",
+        "max_d_phi", "max_d_cottheta", "max_cottheta_obarrel", "max_cottheta_forward")]
+
+
+# Iteration 0 of CMS-2017: set_dupl_params(0.24, 0.002, 0.004, 0.008)
+# (Geoms/CMS-2017.cc:750) and the window constants of Config.cc:93-97.
+SELECT_ITER0 = dict(frac_shared_hits=0.24, drth_central=0.002, drth_obarrel=0.004,
+                    drth_forward=0.008, max_d_invpt=1.8, max_d_phi=0.37, max_d_cottheta=0.37,
+                    max_cottheta_obarrel=1.99, max_cottheta_forward=6.05)
+
+
 class MkfgEvent(ctypes.Structure):
     _fields_ = [("n_layers", ctypes.c_int32), ("layer_begin", vp), ("pos", vp), ("err", vp),
                 ("detid", vp), ("cpcm", vp), ("n_seeds", ctypes.c_int32), ("seed_par", vp),
@@ -44,6 +57,7 @@ def _bind(lib):
     lib.mkfg_find_run_graph.argtypes = [vp]
     lib.mkfg_find_backward_fit.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_int32]
     lib.mkfg_find_hit_index.argtypes = [vp, ctypes.c_int32, vp, vp]
+    lib.mkfg_find_select.argtypes = [vp, ctypes.POINTER(MkfgSelectConfig), ctypes.c_int32, vp]
     lib.mkfg_find_run_fused.argtypes = [vp, ctypes.c_int32]
     lib.mkfg_find_autotune.argtypes = [vp, ctypes.POINTER(ctypes.c_int32),
                                        ctypes.POINTER(ctypes.c_float)]
@@ -200,6 +214,15 @@ class Finder:
         capi.check(self.lib.mkfg_find_work_detail(self.ctx.handle, ctypes.byref(e), ctypes.byref(c)))
         return dict(active_cands=a.value, hit_pairs=p.value, updates=u.value, steps=st.value,
                     chi2_evals=e.value, seed_steps=c.value)
+
+    def select(self, n_seeds, **params):
+        """Output selection of run_OneIteration (NaN/silly filter + duplicate
+        removal) on the current results: keep[n_seeds] by input seed."""
+        c = MkfgSelectConfig(**{**SELECT_ITER0, **params})
+        keep = np.zeros(n_seeds, np.int32)
+        capi.check(self.lib.mkfg_find_select(self.ctx.handle, ctypes.byref(c), n_seeds,
+                                             keep.ctypes.data))
+        return keep
 
     def hit_index(self, event, n_bins, n_hits):
         """The device-built hit index of uploaded event `event`:

@@ -27,6 +27,7 @@
 #include "mkFit/MkBuilder.h"
 #include "mkFit/MkFinder.h"
 #include "mkFit/MkFitter.h"
+#include "mkFit/MkStdSeqs.h"
 #include "mkFit/PropagationMPlex.h"
 #include "tbb/parallel_for.h"
 #include "tbb/shim_pool.h"
@@ -54,6 +55,10 @@ double now_s() {
 bool g_cms2017_loaded = false;
 // ref_find runs MkBuilder::BackwardFit after the clone engine when set.
 bool g_backward_fit = false;
+// When set, ref_find also runs the output selection of run_OneIteration
+// (qfilter_nan_n_silly, export_best_comb_cands(.., true),
+// find_and_remove_duplicates) and marks the surviving seeds here (by label).
+int* g_keep_out = nullptr;
 
 void set_material(const float* rl_grid, const float* xi_grid) {
   if (rl_grid && xi_grid) {
@@ -194,6 +199,11 @@ extern "C" {
 // mkFit/MkBuilder.cc:2153-2253) on the best candidate of every seed, as
 // run_OneIteration does with do_backward_fit (mkFit/buildtestMPlex.cc).
 void ref_set_backward_fit(int on) { g_backward_fit = on != 0; }
+
+// ref_find: keep[ns] (by seed label) receives 1 for the seeds whose best
+// candidate survives run_OneIteration's output selection
+// (mkFit/buildtestMPlex.cc:721-731), 0 otherwise; NULL switches it off.
+void ref_set_select_output(int* keep) { g_keep_out = keep; }
 
 // Geometry export sizes: n_layers, n_regions, max plan length.
 int ref_cms2017_sizes(int* n_layers, int* n_regions, int* max_plan) {
@@ -356,6 +366,24 @@ int ref_find(int n_layers_in, const int* layer_begin, const float* hpos, const f
     if (r + 1 < std::max(1, repeat)) builder.end_event();
   }
   if (best_seconds) *best_seconds = best;
+
+  if (g_keep_out) {
+    // Output selection of run_OneIteration on a copy of the builder's
+    // result, leaving the comb candidates themselves as exported below.
+    EventOfCombCandidates& src = builder.eocc();
+    std::fill(g_keep_out, g_keep_out + ns, 0);
+    TrackVec out;
+    out.reserve(src.m_size);
+    for (int i = 0; i < src.m_size; ++i) {
+      if (src[i].empty()) continue;
+      const TrackCand& t = src[i].front();
+      if (!StdSeq::qfilter_nan_n_silly(t)) continue;
+      out.emplace_back(t.exportTrack(true));
+    }
+    StdSeq::find_and_remove_duplicates(out, itconf);
+    for (const Track& t : out)
+      if (t.label() >= 0 && t.label() < ns) g_keep_out[t.label()] = 1;
+  }
 
   EventOfCombCandidates& eocc = builder.eocc();
   std::fill(n_cands, n_cands + ns, 0);

@@ -275,3 +275,25 @@ def test_device_hit_index_equals_host(gpu_ctx):
         bins, srank = fnd.hit_index(e, host["bins"].size, ev.n_hits)
         np.testing.assert_array_equal(bins, host["bins"], err_msg=f"bins of event {e}")
         np.testing.assert_array_equal(srank, host["srank"], err_msg=f"ranks of event {e}")
+
+
+@pytest.mark.parametrize("n_tracks,seed,noise", [(800, 1, 0.01), (3000, 2, 0.05)])
+def test_select_matches_reference(gpu_ctx, reflib, n_tracks, seed, noise):
+    """Output selection (mkfg_find_select: NaN/silly filter + duplicate
+    removal) after finding and backward fit keeps the same seeds as the
+    reference's run_OneIteration tail, except for seeds whose best candidate
+    differs from the reference's (finding near-ties) or whose group
+    neighbours do; the disagreement rate is printed and bounded."""
+    ev = synth.gen_cms_event(n_tracks, seed=seed, noise_frac=noise)
+    ref = ref_find(reflib, ev, max_cands=M, chi2_cut=30.0, zero_c2=True, backward_fit=True,
+                   select=True)
+    fnd = Finder(gpu_ctx, FindConfig(max_cands=M, chi2_cut=30.0, zero_c2=True))
+    fnd.upload(ev)
+    fnd.run()
+    fnd.backward_fit()
+    keep = fnd.select(ev.n_seeds)
+    diff = np.count_nonzero(keep != ref["keep"])
+    print(f"\nselect, {n_tracks} tracks: {ev.n_seeds} seeds, reference keeps {ref['keep'].sum()}, "
+          f"GPU keeps {keep.sum()}, disagreements {diff}")
+    assert ref["keep"].sum() < ev.n_seeds or n_tracks < 1000
+    assert diff <= max(2, ev.n_seeds // 500)
