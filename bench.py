@@ -49,6 +49,13 @@ PLAIN_TRACKS = 800
 FLOP_LAYER_PROP = 1000
 FLOP_HIT_CHI2 = 950
 FLOP_UPDATE = 1150
+# Algorithmic HBM bytes per unit: the candidate state read (27 floats +
+# charge) and the propagated state written (27 floats); the hit (9 floats)
+# and the propagated state read per pair; state in + hit + state out per
+# update.
+BYTES_LAYER_PROP = 112 + 108
+BYTES_HIT_CHI2 = 36 + 108
+BYTES_UPDATE = 112 + 36 + 112
 # Kernels per layer-plan step in the graph form.
 KERNELS_PER_LAYER_STEP = 5
 # Fit (secondary metric): toy MC, 10 barrel layers.
@@ -254,6 +261,20 @@ def run_ours(args):
              work["updates"] * FLOP_UPDATE)
     achieved_tf = flops / (ms_step * 1e-3) / 1e12
 
+    # Per-kernel device times: one replay of the same step as the plain
+    # launch sequence with a CUDA event after every kernel (outside the
+    # timed region), for the dominant FP32 kernel's roofline.
+    kt = finder.run_timed()
+    kt_total = sum(kt.values())
+    fp_kernels = {"propagate": (work["active_cands"], FLOP_LAYER_PROP, BYTES_LAYER_PROP),
+                  "chi2": (work["hit_pairs"], FLOP_HIT_CHI2, BYTES_HIT_CHI2),
+                  "update": (work["updates"], FLOP_UPDATE, BYTES_UPDATE)}
+    dom = max(fp_kernels, key=lambda k: kt[k])
+    units, f_unit, b_unit = fp_kernels[dom]
+    per_launch_ms = kt[dom] / work["steps"]
+    dom_tf = units * f_unit / (kt[dom] * 1e-3) / 1e12
+    dom_gbs = units * b_unit / (kt[dom] * 1e-3) / 1e9
+
     # End to end through the C ABI from host buffers: upload (host hit-index
     # build + seed partition + H2D), run, download (export + D2H).
     e2e = None
@@ -316,16 +337,26 @@ def run_ours(args):
         },
         "roofline": {
             "bound": "fp32",
-            "scope": "whole finding step (all kernels of the graph)",
-            "achieved": achieved_tf,
+            "kernel": f"k_{dom}",
+            "achieved": dom_tf,
             "peak": peak,
             "unit": "TFLOP/s",
-            "frac": achieved_tf / peak if peak else None,
-            "peak_source": "measured FP32 FMA probe (mkfg_probe_fp32_peak), same run",
-            "flop_per_step": flops,
-            "work_per_step": work,
-            "traffic": None,
+            "frac": dom_tf / peak if peak else None,
+            "peak_source": "measured FP32 FMA probe (mkfg_probe_fp32_peak), same run (of measured)",
+            "per_launch_ms": per_launch_ms,
+            "units_per_step": units,
+            "flop_per_unit": f_unit,
+            "bytes_per_unit": b_unit,
+            "hbm_achieved_gbs": dom_gbs,
             "hbm_peak_gbs": peaks.get("hbm_gbs"),
+            "hbm_frac": dom_gbs / peaks["hbm_gbs"] if peaks.get("hbm_gbs") else None,
+            "traffic": None,
+            "traffic_note": "DRAM bytes of the kernels: profiles/find_kernels_plain_cms2017.md",
+            "kernel_ms_per_step": {k: v for k, v in kt.items()},
+            "kernel_share": {k: v / kt_total for k, v in kt.items()},
+            "step": {"scope": "whole finding step (all kernels of the graph)",
+                     "achieved": achieved_tf, "frac": achieved_tf / peak if peak else None,
+                     "flop_per_step": flops, "work_per_step": work},
         },
         "e2e": e2e,
         "gpu_launches": args.steps * (2 + KERNELS_PER_LAYER_STEP * work["steps"]),

@@ -259,6 +259,11 @@ int mkfg_find_run(mkfg_context* ctx);
 /* The same sequence captured once per upload into a CUDA graph and
  * replayed (one graph launch per call). No reference counterpart. */
 int mkfg_find_run_graph(mkfg_context* ctx);
+/* The plain run with a CUDA event after every launch: kernel_ms[7]
+ * receives the device time of each kernel class summed over the layer
+ * steps (0 reset, 1 activate, 2 propagate, 3 chi2, 4 clone, 5 update,
+ * 6 merge). For per-kernel rooflines. No reference counterpart. */
+int mkfg_find_run_timed(mkfg_context* ctx, float* kernel_ms);
 /* Fused form of the same run: one launch in which every thread block carries
  * seeds_per_block consecutive seeds (4, 8 or 16; 0 = the value chosen by
  * mkfg_find_autotune, 16 before any tuning) through all layer steps and the

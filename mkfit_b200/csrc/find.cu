@@ -240,10 +240,11 @@ __global__ void __launch_bounds__(kBlock) k_clone(EventDev E, const FindConfigDe
     const int cur = E.cur[s];
     if (lane == 0) atomicAdd(&E.work[step * 4 + 3], 1);
     const size_t rb = (size_t)s * kRecPerSeed;
+    const int ncand = E.n_cands[s];
     const SeedRecords R{E.rhit + rb,          E.rscore + rb,           E.rchi2hit + rb,
                         E.rmodule + rb,       E.wsr + s * kSlots,      E.extra_last + s * kSlots,
                         E.upd + s * kSlots};
-    const int n = clone_seed(E, C, s, layer, kFinding, E.n_cands[s], cur, R, hm, lane);
+    const int n = clone_seed(E, C, s, layer, kFinding, ncand, cur, R, hm, lane);
     if (n >= 0 && lane == 0) {
       E.n_cands[s] = n;
       E.cur[s] = cur ^ 1;
@@ -1133,6 +1134,60 @@ static int enqueue_fused(Finder* f, cudaStream_t st, int w) {
   }
 }
 
+// The plain sequence with an event after every launch: device time per
+// kernel class (0 reset, 1 activate, 2 propagate, 3 chi2, 4 clone,
+// 5 update, 6 merge), summed over the layer steps.
+static int run_timed(mkfg_context* ctx, Finder* f, float* ms) {
+  for (int k = 0; k < 7; ++k) ms[k] = 0.f;
+  if (f->n_seeds == 0) return MKFG_OK;
+  cudaStream_t st = ctx->stream;
+  const int S = f->n_seeds;
+  const int n_work = 4 * (f->host_cfg.max_steps + 2);
+  const int grid_c = (S * kSlots + kBlock - 1) / kBlock;
+  const int grid_w = (S * 32 + kBlock - 1) / kBlock;
+  const int grid_p = std::min((S * kSlots * 4 + kBlock - 1) / kBlock, 148 * 16);
+  const int grid_l = std::min(grid_c, 148 * 8);
+  const int n_ev = 2 + 5 * f->host_cfg.max_steps + 1;
+  std::vector<cudaEvent_t> ev(n_ev);
+  std::vector<int> cls(n_ev, -1);
+  for (auto& e : ev) MKFG_CUDA_TRY(cudaEventCreate(&e));
+  int i = 0;
+  auto mark = [&](int c) { cls[i] = c; return cudaEventRecord(ev[i++], st); };
+  int rc = MKFG_OK;
+  do {
+    if (mark(-1) != cudaSuccess) { rc = set_error(MKFG_ERR_CUDA, "event record"); break; }
+    cudaMemsetAsync(f->ev.pair_count, 0, 4 * (size_t)(f->host_cfg.max_steps + 2), st);
+    cudaMemsetAsync(f->ev.step_count, 0, 4 * (size_t)kCntN * (f->host_cfg.max_steps + 2), st);
+    k_reset<<<std::max(grid_c, (n_work + kBlock - 1) / kBlock), kBlock, 0, st>>>(f->ev, n_work);
+    mark(0);
+    for (int step = 1; step <= f->host_cfg.max_steps; ++step) {
+      k_activate<<<grid_c, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+      mark(1);
+      k_propagate<<<grid_l, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+      mark(2);
+      k_chi2<<<std::max(grid_p, 1), kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+      mark(3);
+      k_clone<<<std::min(grid_w, 148 * 16), kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+      mark(4);
+      k_update<<<grid_l, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+      mark(5);
+    }
+    k_merge<<<(S + 127) / 128, 128, 0, st>>>(f->ev, f->d_cfg);
+    mark(6);
+    if (cudaGetLastError() != cudaSuccess || cudaEventSynchronize(ev[i - 1]) != cudaSuccess) {
+      rc = set_error(MKFG_ERR_CUDA, "timed run failed");
+      break;
+    }
+    for (int k = 1; k < i; ++k) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, ev[k - 1], ev[k]);
+      if (cls[k] >= 0) ms[cls[k]] += t;
+    }
+  } while (false);
+  for (auto& e : ev) cudaEventDestroy(e);
+  return rc;
+}
+
 static int run_plain(mkfg_context* ctx, Finder* f) {
   if (f->n_seeds == 0) return MKFG_OK;
   return enqueue_run(f, ctx->stream);
@@ -1272,6 +1327,15 @@ extern "C" int mkfg_find_run_graph(mkfg_context* ctx) {
   Finder* f = finder_of(ctx);
   MKFG_REQUIRE(f->configured && f->events_loaded, "no event uploaded");
   return run_graph(ctx, f);
+}
+
+extern "C" int mkfg_find_run_timed(mkfg_context* ctx, float* kernel_ms) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  Finder* f = finder_of(ctx);
+  MKFG_REQUIRE(f->configured && f->events_loaded, "no event uploaded");
+  MKFG_REQUIRE(kernel_ms != nullptr, "null kernel_ms");
+  return run_timed(ctx, f, kernel_ms);
 }
 
 extern "C" int mkfg_find_run_fused(mkfg_context* ctx, int32_t seeds_per_block) {

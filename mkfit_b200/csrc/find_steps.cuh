@@ -330,10 +330,11 @@ struct PrepOut {
 // node and is inactive. Returns whether the candidate is active.
 __device__ __forceinline__ bool cand_is_active(const EventDev& E, const CandSoA& B, int s, int slot,
                                                int layer) {
-  const int last = B.last[slot];
-  if (hot_index(node_hot_of(E, s, last)) == -2) return false;
+  // Parameters first: their loads overlap the stop-node lookup.
   const float x = B.par[0 * B.cap + slot], y = B.par[1 * B.cap + slot];
   const float ipt = B.par[3 * B.cap + slot], phi = B.par[4 * B.cap + slot];
+  const int last = B.last[slot];
+  if (hot_index(node_hot_of(E, s, last)) == -2) return false;
   const float pt = fabsf(1.f / ipt);
   if (pt < 1.2f) {
     const float dphi = fabsf(f_atan2(y, x) - phi);
@@ -359,6 +360,13 @@ __device__ __forceinline__ bool activate_cand(const EventDev& E, const CandSoA& 
 // Propagation to the layer, SelectHitIndices, missed-layer handling
 // (mkFit/MkBuilder.cc:1568-1637) and the hole record (MkFinder.cc:1245-1283)
 // for an active candidate. xhit receives up to 16 indices with stride xstride.
+__device__ __forceinline__ void select_cand(const EventDev& E, const FindConfigDev& C,
+                                            const LayerDev& L, const uint32_t* layer_bins,
+                                            int hit_base, int reg, int layer, int s,
+                                            const CandSoA& B, int slot, const float (&ppar)[6],
+                                            const float (&perr)[21], int* xhit, int xstride,
+                                            PrepOut& o);
+
 __device__ __forceinline__ void prep_cand(const EventDev& E, const FindConfigDev& C,
                                           const LayerDev& L, const uint32_t* layer_bins,
                                           int hit_base, int reg, int layer, int s, const CandSoA& B,
@@ -368,9 +376,21 @@ __device__ __forceinline__ void prep_cand(const EventDev& E, const FindConfigDev
     propagate_to_r(par, err, chg, L.propagate_to, C.inter_pflags, C.mat, false, o.ppar, o.perr);
   else
     propagate_to_z(par, err, chg, L.propagate_to, C.inter_pflags, C.mat, false, o.ppar, o.perr);
+  select_cand(E, C, L, layer_bins, hit_base, reg, layer, s, B, slot, o.ppar, o.perr, xhit, xstride,
+              o);
+}
+
+// The part of prep_cand after the propagation: SelectHitIndices on the
+// propagated state, missed-layer handling and the hole record.
+__device__ __forceinline__ void select_cand(const EventDev& E, const FindConfigDev& C,
+                                            const LayerDev& L, const uint32_t* layer_bins,
+                                            int hit_base, int reg, int layer, int s,
+                                            const CandSoA& B, int slot, const float (&ppar)[6],
+                                            const float (&perr)[21], int* xhit, int xstride,
+                                            PrepOut& o) {
   o.active = true;
-  o.xs = select_hits(E, L, layer_bins, hit_base, o.ppar, o.perr, xhit, xstride, o.wsr);
-  const float cand_r = hypot_f(o.ppar[0], o.ppar[1]);
+  o.xs = select_hits(E, L, layer_bins, hit_base, ppar, perr, xhit, xstride, o.wsr);
+  const float cand_r = hypot_f(ppar[0], ppar[1]);
   if (L.is_barrel && cand_r < L.rin) {
     o.xs = 0;
     o.wsr = kWsrOutside;
@@ -385,7 +405,7 @@ __device__ __forceinline__ void prep_cand(const EventDev& E, const FindConfigDev
     int fake = ((nin + ntl) < C.max_holes && ntl < C.max_consec_holes) ? -1 : -2;
     if (o.wsr == kWsrEdge) fake = -3;
     const int ntail_rec = fake == -1 ? ntl + 1 : ntl;
-    const float pt = fabsf(1.0f / o.ppar[3]);
+    const float pt = fabsf(1.0f / ppar[3]);
     o.hole = true;
     o.hole_hit = fake;
     o.hole_score = score_struct(B.nfound[slot], ntail_rec, B.nover[slot], nin, B.chi2[slot], pt);
@@ -520,18 +540,18 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
     HitMatchPair p;
     p.reset();
     if (lane < ncand) {
-      int hv[kMaxXHits], mv[kMaxXHits];
-      float cv[kMaxXHits];
+      // Records of hits under the overlap cut, then those alone in order.
+      unsigned m = 0;
 #pragma unroll
       for (int h = 0; h < kMaxXHits; ++h) {
         const int idx = lane * kRecPerCand + h;
-        hv[h] = R.hit(idx);
-        cv[h] = R.chi2hit(idx);
-        mv[h] = R.module(idx);
+        if (R.hit(idx) != kRecInvalid && R.chi2hit(idx) < C.chi2_cut_overlap) m |= 1u << h;
       }
-#pragma unroll
-      for (int h = 0; h < kMaxXHits; ++h)
-        if (hv[h] != kRecInvalid && cv[h] < C.chi2_cut_overlap) p.consider(hv[h], mv[h], cv[h]);
+      while (m) {
+        const int idx = lane * kRecPerCand + __ffs(m) - 1;
+        m &= m - 1;
+        p.consider(R.hit(idx), R.module(idx), R.chi2hit(idx));
+      }
     }
     hm[lane] = p;
   }

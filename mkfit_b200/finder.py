@@ -57,6 +57,7 @@ def _bind(lib):
     lib.mkfg_find_run_graph.argtypes = [vp]
     lib.mkfg_find_backward_fit.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_int32]
     lib.mkfg_find_hit_index.argtypes = [vp, ctypes.c_int32, vp, vp]
+    lib.mkfg_find_run_timed.argtypes = [vp, vp]
     lib.mkfg_find_select.argtypes = [vp, ctypes.POINTER(MkfgSelectConfig), ctypes.c_int32, vp]
     lib.mkfg_find_run_fused.argtypes = [vp, ctypes.c_int32]
     lib.mkfg_find_autotune.argtypes = [vp, ctypes.POINTER(ctypes.c_int32),
@@ -193,6 +194,14 @@ class Finder:
         self._bk_last = np.ascontiguousarray(g.bkfit_last, np.int32)
         capi.check(self.lib.mkfg_find_backward_fit(self.ctx.handle, self._bk_last.ctypes.data,
                                                    int(g.flags[3]), int(group_width)))
+
+    KERNELS = ("reset", "activate", "propagate", "chi2", "clone", "update", "merge")
+
+    def run_timed(self):
+        """Plain run with per-kernel CUDA-event timing: {kernel: ms}."""
+        ms = np.zeros(len(self.KERNELS), np.float32)
+        capi.check(self.lib.mkfg_find_run_timed(self.ctx.handle, ms.ctypes.data))
+        return dict(zip(self.KERNELS, ms.tolist()))
 
     def run_fused(self, seeds_per_block=0):
         """One launch for all layer steps; seeds_per_block 0 = tuned value."""

@@ -297,3 +297,18 @@ def test_select_matches_reference(gpu_ctx, reflib, n_tracks, seed, noise):
           f"GPU keeps {keep.sum()}, disagreements {diff}")
     assert ref["keep"].sum() < ev.n_seeds or n_tracks < 1000
     assert diff <= max(2, ev.n_seeds // 500)
+
+
+def test_run_timed_equals_run(gpu_ctx):
+    """The per-kernel timed replay gives the plain run's results."""
+    ev = synth.gen_cms_event(500, seed=13)
+    fnd = Finder(gpu_ctx, FindConfig(max_cands=M))
+    fnd.upload(ev)
+    fnd.run()
+    a = fnd.download(ev.n_seeds)
+    ms = fnd.run_timed()
+    b = fnd.download(ev.n_seeds)
+    assert set(ms) == set(Finder.KERNELS) and all(v >= 0 for v in ms.values())
+    assert ms["propagate"] > 0 and ms["clone"] > 0
+    for k in a:
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
