@@ -60,6 +60,53 @@ __device__ __forceinline__ void append_two_ended(bool want, bool barrel, int val
   }
 }
 
+// Block-aggregated forms of the appends: one atomic per block (and end)
+// instead of one per warp, for lists every warp of a busy grid appends to
+// (same-address atomics serialise in L2). Every thread of the block calls
+// them, the same number of times: they synchronise the block.
+struct BlockAppend {
+  int n[kBlock / 32][2];
+  int base[kBlock / 32][2];
+};
+
+__device__ __forceinline__ void append_two_ended_block(bool want, bool barrel, int value, int* list,
+                                                       int cap, int* cnt, BlockAppend& sh,
+                                                       int value2 = 0, int* list2 = nullptr) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned mb = __ballot_sync(0xffffffffu, want && barrel);
+  const unsigned me = __ballot_sync(0xffffffffu, want && !barrel);
+  if (lane == 0) {
+    sh.n[warp][0] = __popc(mb);
+    sh.n[warp][1] = __popc(me);
+  }
+  __syncthreads();
+  if (threadIdx.x < 2) {
+    const int end = threadIdx.x;
+    int tot = 0;
+    for (int w = 0; w < kBlock / 32; ++w) {
+      sh.base[w][end] = tot;
+      tot += sh.n[w][end];
+    }
+    const int b = tot ? atomicAdd(cnt + end, tot) : 0;
+    for (int w = 0; w < kBlock / 32; ++w) sh.base[w][end] += b;
+  }
+  __syncthreads();
+  const unsigned below = (1u << lane) - 1u;
+  if (want) {
+    const int at = barrel ? sh.base[warp][0] + __popc(mb & below)
+                          : cap - 1 - (sh.base[warp][1] + __popc(me & below));
+    list[at] = value;
+    if (list2) list2[at] = value2;
+  }
+}
+
+// One-ended block-aggregated append (counter cnt[0]); uses sh.n[.][0] and
+// sh.base[.][0] only after the block synchronises, like the two-ended form.
+__device__ __forceinline__ void append_list_block(bool want, int value, int* list, int* cnt,
+                                                  BlockAppend& sh) {
+  append_two_ended_block(want, true, value, list, 0, cnt, sh);
+}
+
 // Warp-aggregated append of `value` for the lanes where `want` holds.
 __device__ __forceinline__ void append_list(bool want, int value, int* list, int* cnt, int lane) {
   const unsigned m = __ballot_sync(0xffffffffu, want);
@@ -97,19 +144,16 @@ __global__ void __launch_bounds__(kBlock) k_activate(EventDev E, const FindConfi
     const bool active = in_range && layer >= 0 && state == kFinding && c < ncand &&
                         cand_is_active(E, E.cand[buf], s, slot, layer);
     const unsigned act = __ballot_sync(0xffffffffu, active) & grp;
-    {
-      const unsigned all = __ballot_sync(0xffffffffu, active);
-      if (lane == 0 && all) atomicAdd(&E.work[step * 4 + 0], __popc(all));
-    }
     const bool seed_finding = layer >= 0 && state == kFinding && act != 0;
     if (in_range && c == 0) {
       if (layer >= 0 && state == kFinding && act == 0) state = kFinished;
       E.state[s] = state;
     }
     const bool barrel = active && C.layer[layer].is_barrel;
-    append_two_ended(active, barrel, slot, E.act_list, E.list_cap, cnt + kCntActBarrel, lane);
+    __shared__ BlockAppend sh;
+    append_two_ended_block(active, barrel, slot, E.act_list, E.list_cap, cnt + kCntActBarrel, sh);
     // Seeds finding at this step go to the clone step.
-    append_list(in_range && c == 0 && seed_finding, s, E.find_list, cnt + kCntFind, lane);
+    append_list_block(in_range && c == 0 && seed_finding, s, E.find_list, cnt + kCntFind, sh);
     // The clone step reads the records and extra flags of candidates
     // [0, ncand) of seeds still finding: an inactive one among them has
     // neither.
@@ -132,6 +176,7 @@ __global__ void __launch_bounds__(kBlock, MKFG_HEAVY_MIN_BLOCKS) k_propagate(Eve
   const int* cnt = E.step_count + step * kCntN;
   const int nb = cnt[kCntActBarrel], ne = cnt[kCntActEndcap];
   const int stride = E.cand[0].cap;
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&E.work[step * 4 + 0], nb + ne);
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nb + ne; j += gridDim.x * blockDim.x) {
     const int slot = j < nb ? E.act_list[j] : E.act_list[E.list_cap - 1 - (j - nb)];
     const int s = slot / kSlots, c = slot % kSlots;
@@ -227,36 +272,45 @@ __global__ void __launch_bounds__(kBlock, MKFG_HEAVY_MIN_BLOCKS) k_chi2(EventDev
 __global__ void __launch_bounds__(kBlock) k_clone(EventDev E, const FindConfigDev* __restrict__ Cp,
                                                   int step) {
   const FindConfigDev& C = *Cp;
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   __shared__ HitMatchPair s_hm[kBlock / 32][kSlots];
-  HitMatchPair* hm = s_hm[threadIdx.x >> 5];
+  __shared__ int s_scratch[kBlock / 32][32];
+  __shared__ BlockAppend sh;
+  HitMatchPair* hm = s_hm[warp];
   int* cnt = E.step_count + step * kCntN;
   const int n_find = cnt[kCntFind];
-  const int n_warps = gridDim.x * (blockDim.x >> 5);
-  for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n_find; w += n_warps) {
-    // A seed finding at this step (listed by the activation kernel).
-    const int s = E.find_list[w];
-    const int layer = plan_layer(C, E.region[s], step);
-    const int cur = E.cur[s];
-    if (lane == 0) atomicAdd(&E.work[step * 4 + 3], 1);
-    const size_t rb = (size_t)s * kRecPerSeed;
-    const int ncand = E.n_cands[s];
-    const SeedRecords R{E.rhit + rb,          E.rscore + rb,           E.rchi2hit + rb,
-                        E.rmodule + rb,       E.wsr + s * kSlots,      E.extra_last + s * kSlots,
-                        E.upd + s * kSlots};
-    const int n = clone_seed(E, C, s, layer, kFinding, ncand, cur, R, hm, lane);
-    if (n >= 0 && lane == 0) {
-      E.n_cands[s] = n;
-      E.cur[s] = cur ^ 1;
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&E.work[step * 4 + 3], n_find);
+  // Block-uniform loop (the update-list append synchronises the block):
+  // warp `warp` of the block takes seed base + warp of each round.
+  for (int base = blockIdx.x * (kBlock / 32); base < n_find; base += gridDim.x * (kBlock / 32)) {
+    const int w = base + warp;
+    int u = 0, g = 0, slot = 0;
+    bool barrel = true;
+    if (w < n_find) {
+      // A seed finding at this step (listed by the activation kernel).
+      const int s = E.find_list[w];
+      const int layer = plan_layer(C, E.region[s], step);
+      const int cur = E.cur[s];
+      const size_t rb = (size_t)s * kRecPerSeed;
+      const int ncand = E.n_cands[s];
+      const SeedRecords R{E.rhit + rb,          E.rscore + rb,           E.rchi2hit + rb,
+                          E.rmodule + rb,       E.wsr + s * kSlots,      E.extra_last + s * kSlots,
+                          E.upd + s * kSlots};
+      const int n = clone_seed(E, C, s, layer, kFinding, ncand, cur, R, hm, s_scratch[warp], lane);
+      if (n >= 0 && lane == 0) {
+        E.n_cands[s] = n;
+        E.cur[s] = cur ^ 1;
+      }
+      // The new candidates that take a Kalman update, with the global index
+      // of the hit to update with (on this step's layer).
+      slot = s * kSlots + lane;
+      u = lane < n ? E.upd[slot] : 0;
+      g = u ? E.layer_begin[E.seed_event[s] * E.lb_stride + layer] + (u - 1) : 0;
+      barrel = C.layer[layer].is_barrel;
     }
-    // Compact list of the new candidates that take a Kalman update, with
-    // the global index of the hit to update with (on this step's layer).
-    __syncwarp();
-    const int u = lane < n ? E.upd[s * kSlots + lane] : 0;
-    const int g = u ? E.layer_begin[E.seed_event[s] * E.lb_stride + layer] + (u - 1) : 0;
-    append_two_ended(u != 0, C.layer[layer].is_barrel, s * kSlots + lane, E.upd_list, E.list_cap,
-                     cnt + kCntUpdBarrel, lane, g, E.upd_hit);
-    __syncwarp();  // hm is reused by the next seed of this warp
+    append_two_ended_block(u != 0, barrel, slot, E.upd_list, E.list_cap, cnt + kCntUpdBarrel, sh, g,
+                           E.upd_hit);
+    __syncwarp();  // hm and scratch are reused by the next seed of this warp
   }
 }
 

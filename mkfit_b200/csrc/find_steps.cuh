@@ -522,16 +522,63 @@ struct SeedRecords {
   __device__ void set_upd(int i, int v) const { upd_[i] = v; }
 };
 
+// Total order of record scores as integers: the float order, with -0 taken
+// as +0 and NaN below every number (NaN records go last, in record order).
+__device__ __forceinline__ int score_key(float score) {
+  const float z = __fadd_rn(score, 0.f);
+  const int k = __float_as_int(z);
+  return z != z ? INT_MIN : (k >= 0 ? k : k ^ 0x7fffffff);
+}
+
+// Copies the parameters and covariance of new candidates i < n (parent
+// slot parent_i, lane i of `parent`) from buffer B to buffer N. Lane t
+// moves element t / 8 + 4 k of candidate t % 8: each access of the warp
+// covers four whole 32-byte sectors (a seed's 8 slots are contiguous).
+__device__ __forceinline__ void copy_par_err(const CandSoA& B, const CandSoA& N, int s, int n,
+                                             int parent, int lane) {
+  static_assert(kSlots == 8, "copy_par_err maps 8 slots to lane groups");
+  const int c = lane & 7;
+  const int pc = __shfl_sync(0xffffffffu, parent, c);
+  if (c >= n) return;
+  const int src = s * kSlots + pc, dst = s * kSlots + c;
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {
+    const int e = (lane >> 3) + 4 * k;
+    if (e >= 27) break;
+    const float* from = e < 6 ? B.par + e * B.cap : B.err + (e - 6) * B.cap;
+    float* to = e < 6 ? N.par + e * N.cap : N.err + (e - 6) * N.cap;
+    to[dst] = from[src];
+  }
+}
+
+// Writes a hit-on-track node at arena position pos of seed s (allocated by
+// the caller); returns pos, or prev after an overflow (flagged).
+__device__ __forceinline__ int arena_put(const EventDev& E, int s, int pos, int index, int layer,
+                                         float chi2, int prev) {
+  if (pos >= E.hot_cap) {
+    atomicOr(E.err_flags, kErrArena);
+    return prev;
+  }
+  const size_t k = (size_t)s * E.hot_cap + pos;
+  E.node_hot[k] = hot_pack(index, layer);
+  E.node_chi2[k] = chi2;
+  E.node_prev[k] = prev;
+  return pos;
+}
+
 // CandCloner::ProcessSeedRange for one seed (mkFit/CandCloner.cc:36-189),
 // executed by one warp. Returns the new candidate count, or -1 when the
-// seed's candidates are unchanged.
+// seed's candidates are unchanged. scratch: 32 ints of the warp's shared
+// memory.
 __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev& C, int s,
                                           int layer, int state, int ncand, int cur,
-                                          const SeedRecords& R, HitMatchPair* hm, int lane) {
+                                          const SeedRecords& R, HitMatchPair* hm, int* scratch,
+                                          int lane) {
   constexpr unsigned kFull = 0xffffffffu;
   const CandSoA& B = E.cand[cur];
   const CandSoA& N = E.cand[cur ^ 1];
   const int M = C.max_cands;
+  const unsigned below = (1u << lane) - 1u;
 
   // Overlap candidates per parent (consulted at CandCloner.cc:120-124),
   // filled in hit order as MkFinder does (:1212-1216); lane c scans
@@ -562,42 +609,37 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
   const float c_score = is_cand ? B.score[cslot] : 0.f;
   const float c_ipt = is_cand ? B.par[3 * B.cap + cslot] : 1.f;
   const int c_kind = (is_cand && state == kFinding) ? R.extra_kind(lane) : 0;
-  __syncwarp();
 
+  // Valid records: those of candidates [0, ncand) not marked invalid.
   constexpr int kPer = (kRecPerSeed + 31) / 32;
-  float sc[kPer];
   bool valid[kPer];
+  unsigned vmask[kPer];
   int n_valid = 0;
 #pragma unroll
   for (int k = 0; k < kPer; ++k) {
     const int idx = lane + 32 * k;
-    valid[k] = idx < kRecPerSeed && R.valid(idx, ncand);
-    sc[k] = valid[k] ? R.score(idx) : 0.f;
-    n_valid += __popc(__ballot_sync(kFull, valid[k]));
+    valid[k] = idx < ncand * kRecPerCand && R.valid(idx, ncand);
+    vmask[k] = __ballot_sync(kFull, valid[k]);
+    n_valid += __popc(vmask[k]);
   }
 
   // Extras (held-back candidates) in candidate order (MkBuilder.cc:1600-1626).
   const unsigned extra_mask = __ballot_sync(kFull, c_kind != 0);
   const int n_extras = __popc(extra_mask);
+  __syncwarp();
 
   if (n_valid == 0) {
     // hitsForSeed empty (CandCloner.cc:163-172): the extras survive.
     if (state != kFinding) return -1;
-    unsigned m = extra_mask;
-    for (int i = 0; i < n_extras; ++i) {
-      const int c = __ffs(m) - 1;
-      m &= m - 1;
-      const int src = s * kSlots + c, dst = s * kSlots + i;
-      if (lane < 27) {
-        if (lane < 6) N.par[lane * N.cap + dst] = B.par[lane * B.cap + src];
-        else N.err[(lane - 6) * N.cap + dst] = B.err[(lane - 6) * B.cap + src];
-      }
-    }
+    // Lane i: the i-th extra.
+    int c = 0;
     if (lane < n_extras) {
-      // Lane i: the i-th extra.
       unsigned mm = extra_mask;
       for (int k = 0; k < lane; ++k) mm &= mm - 1;
-      const int c = __ffs(mm) - 1;
+      c = __ffs(mm) - 1;
+    }
+    copy_par_err(B, N, s, n_extras, c, lane);
+    if (lane < n_extras) {
       const int src = s * kSlots + c, dst = s * kSlots + lane;
       N.chg[dst] = B.chg[src];
       N.chi2[dst] = B.chi2[src];
@@ -620,33 +662,60 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
 
   // Top-num_hits records in (score desc, record index asc) order: the
   // reference's std::sort by score; on exact score ties this order is the
-  // stable one. Lane i keeps the i-th record's index and values.
+  // stable one. Lane i receives the i-th record's index.
   const int num_hits = min(n_valid, M);
   int my_rec = 0;
-  for (int i = 0; i < num_hits; ++i) {
-    float best = -INFINITY;
-    int bidx = INT_MAX;
+  if (n_valid <= 32) {
+    // Compact the valid records in record order (lane p takes the p-th),
+    // rank each against all others, place the first num_hits by rank.
+    int off = 0;
 #pragma unroll
     for (int k = 0; k < kPer; ++k) {
-      const int idx = lane + 32 * k;
-      if (valid[k] && (sc[k] > best || (sc[k] == best && idx < bidx))) {
-        best = sc[k];
-        bidx = idx;
-      }
+      if (valid[k]) scratch[off + __popc(vmask[k] & below)] = lane + 32 * k;
+      off += __popc(vmask[k]);
     }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      const float ob = __shfl_xor_sync(kFull, best, off);
-      const int oi = __shfl_xor_sync(kFull, bidx, off);
-      if (ob > best || (ob == best && oi < bidx)) {
-        best = ob;
-        bidx = oi;
-      }
+    __syncwarp();
+    const int ridx = lane < n_valid ? scratch[lane] : 0;
+    const int key = lane < n_valid ? score_key(R.score(ridx)) : INT_MIN;
+    int rank = 0;
+    for (int j = 0; j < n_valid; ++j) {
+      const int kj = __shfl_sync(kFull, key, j);
+      rank += (kj > key) || (kj == key && j < lane);
     }
-    if (lane == i) my_rec = bidx;
+    __syncwarp();
+    if (lane < n_valid && rank < num_hits) scratch[rank] = ridx;
+    __syncwarp();
+    if (lane < num_hits) my_rec = scratch[lane];
+    __syncwarp();
+  } else {
+    // More records than lanes: num_hits rounds of a warp arg-max.
+    int key[kPer];
 #pragma unroll
-    for (int k = 0; k < kPer; ++k)
-      if (lane + 32 * k == bidx) valid[k] = false;
+    for (int k = 0; k < kPer; ++k) key[k] = valid[k] ? score_key(R.score(lane + 32 * k)) : INT_MIN;
+    for (int i = 0; i < num_hits; ++i) {
+      int best = INT_MIN, bidx = INT_MAX;
+#pragma unroll
+      for (int k = 0; k < kPer; ++k) {
+        const int idx = lane + 32 * k;
+        if (valid[k] && (key[k] > best || (key[k] == best && idx < bidx))) {
+          best = key[k];
+          bidx = idx;
+        }
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const int ob = __shfl_xor_sync(kFull, best, off);
+        const int oi = __shfl_xor_sync(kFull, bidx, off);
+        if (ob > best || (ob == best && oi < bidx)) {
+          best = ob;
+          bidx = oi;
+        }
+      }
+      if (lane == i) my_rec = bidx;
+#pragma unroll
+      for (int k = 0; k < kPer; ++k)
+        if (lane + 32 * k == bidx) valid[k] = false;
+    }
   }
   const bool has_rec = lane < num_hits;
   const int r_hit = has_rec ? R.hit(my_rec) : 0;
@@ -655,9 +724,14 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
   const int r_module = has_rec ? R.module(my_rec) : 0;
 
   // Build the new candidate list (sequential logic of ProcessSeedRange),
-  // identically in every lane from the broadcast values.
-  NewCand nc[kSlots];
+  // identically in every lane from the broadcast values; lane i keeps new
+  // candidate i.
+  NewCand nc{0, 0, 0.f, -1, 0.f, 0};
   int n_pushed = 0;
+  auto push = [&](const NewCand& v) {
+    if (lane == n_pushed) nc = v;
+    ++n_pushed;
+  };
   unsigned em = extra_mask;  // extras not yet taken, in candidate order
   float bs_score = E.bshort_valid[s] ? E.bshort.score[s] : -1e16f;  // getScoreWorstPossible
   int bs_from = -1;
@@ -678,20 +752,37 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
     while (em && n_pushed < M) {
       const int c = __ffs(em) - 1;
       if (!(__shfl_sync(kFull, c_score, c) > score)) break;
-      nc[n_pushed++] = NewCand{c, 0, 0.f, -1, 0.f, __shfl_sync(kFull, c_kind, c)};
+      push(NewCand{c, 0, 0.f, -1, 0.f, __shfl_sync(kFull, c_kind, c)});
       em &= em - 1;
     }
     if (n_pushed >= M) break;
     int ov = -1;
     const float ppt = fabsf(1.f / __shfl_sync(kFull, c_ipt, parent));
     if (ppt > C.pt_cut_overlap && hit >= 0) ov = hm[parent].find(hit, module);
-    nc[n_pushed++] = NewCand{parent, hit, chi2hit, ov, score, 0};
+    push(NewCand{parent, hit, chi2hit, ov, score, 0});
   }
   while (em && n_pushed < M) {
     const int c = __ffs(em) - 1;
-    nc[n_pushed++] = NewCand{c, 0, 0.f, -1, 0.f, __shfl_sync(kFull, c_kind, c)};
+    push(NewCand{c, 0, 0.f, -1, 0.f, __shfl_sync(kFull, c_kind, c)});
     em &= em - 1;
   }
+
+  // Arena nodes of this step, one allocation for the seed: the best short
+  // candidate's hole node first, then one or two nodes per new candidate
+  // with a hit, in candidate order.
+  const bool own = lane < n_pushed && !nc.is_extra;
+  const int n_nodes = own ? 1 + (nc.ov >= 0) : 0;
+  int node_off = n_nodes;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const int v = __shfl_up_sync(kFull, node_off, off);
+    if (lane >= off) node_off += v;
+  }
+  const int nodes_total = __shfl_sync(kFull, node_off, 31) + (bs_from >= 0);
+  node_off -= n_nodes;
+  int node_base = 0;
+  if (lane == 0 && nodes_total) node_base = atomicAdd(&E.hot_size[s], nodes_total);
+  node_base = __shfl_sync(kFull, node_base, 0) + (bs_from >= 0);
 
   // Best short candidate (a -2 record scoring above the current best).
   if (bs_from >= 0) {
@@ -705,7 +796,7 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
       int nfound = B.nfound[src], nmiss = B.nmiss[src], nin = B.ninside[src], ntl = B.ntail[src];
       float chi2 = B.chi2[src];
       add_hit_counts(-2, 0.f, nfound, nmiss, nin, ntl, chi2);
-      E.bshort.last[s] = arena_append(E, s, -2, layer, 0.f, B.last[src]);
+      E.bshort.last[s] = arena_put(E, s, node_base - 1, -2, layer, 0.f, B.last[src]);
       E.bshort.chg[s] = B.chg[src];
       E.bshort.chi2[s] = chi2;
       E.bshort.score[s] = bs_score;
@@ -721,39 +812,33 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
   // Materialize the new candidates into the other buffer: parameters and
   // covariance by all lanes, counters and hit-on-track nodes of new
   // candidate i by lane i.
-  for (int i = 0; i < n_pushed; ++i) {
-    const int src = s * kSlots + nc[i].parent, dst = s * kSlots + i;
-    if (lane < 27) {
-      if (lane < 6) N.par[lane * N.cap + dst] = B.par[lane * B.cap + src];
-      else N.err[(lane - 6) * N.cap + dst] = B.err[(lane - 6) * B.cap + src];
-    }
-  }
+  copy_par_err(B, N, s, n_pushed, nc.parent, lane);
   if (lane < n_pushed) {
-    const NewCand n = nc[lane];
-    const int src = s * kSlots + n.parent, dst = s * kSlots + lane;
+    const int src = s * kSlots + nc.parent, dst = s * kSlots + lane;
     int nfound = B.nfound[src], nmiss = B.nmiss[src], nin = B.ninside[src], ntl = B.ntail[src];
     int nover = B.nover[src];
     float chi2 = B.chi2[src];
     int last = B.last[src];
     float score = B.score[src];
     int upd = 0;
-    if (n.is_extra) {
-      if (n.is_extra == 2) {
-        last = R.extra_last(n.parent);
+    if (nc.is_extra) {
+      if (nc.is_extra == 2) {
+        last = R.extra_last(nc.parent);
         ++nmiss;
       }
     } else {
-      add_hit_counts(n.hit, n.chi2hit, nfound, nmiss, nin, ntl, chi2);
-      last = arena_append(E, s, n.hit, layer, n.chi2hit, last);
-      score = n.score;
-      if (n.ov >= 0) {
-        const HitMatchPair& p = hm[n.parent];
-        add_hit_counts(p.hit[n.ov], p.chi2[n.ov], nfound, nmiss, nin, ntl, chi2);
-        last = arena_append(E, s, p.hit[n.ov], layer, p.chi2[n.ov], last);
+      const int pos = node_base + node_off;
+      add_hit_counts(nc.hit, nc.chi2hit, nfound, nmiss, nin, ntl, chi2);
+      last = arena_put(E, s, pos, nc.hit, layer, nc.chi2hit, last);
+      score = nc.score;
+      if (nc.ov >= 0) {
+        const HitMatchPair& p = hm[nc.parent];
+        add_hit_counts(p.hit[nc.ov], p.chi2[nc.ov], nfound, nmiss, nin, ntl, chi2);
+        last = arena_put(E, s, pos + 1, p.hit[nc.ov], layer, p.chi2[nc.ov], last);
         ++nover;
       }
       // UpdateWithLastHit uses the last hit added: the overlap hit if any.
-      if (n.hit >= 0) upd = 1 + (n.ov >= 0 ? hm[n.parent].hit[n.ov] : n.hit);
+      if (nc.hit >= 0) upd = 1 + (nc.ov >= 0 ? hm[nc.parent].hit[nc.ov] : nc.hit);
     }
     N.chg[dst] = B.chg[src];
     N.chi2[dst] = chi2;
