@@ -100,6 +100,42 @@ __device__ __forceinline__ void append_two_ended_block(bool want, bool barrel, i
   }
 }
 
+// Block-aggregated reservation of `count` consecutive entries of a
+// two-ended list per thread: returns the thread's first position counted
+// from its end (barrel: list[pos + i], endcap: list[cap - 1 - (pos + i)]).
+__device__ __forceinline__ int reserve_two_ended_block(int count, bool barrel, int* cnt,
+                                                       BlockAppend& sh) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int cb = barrel ? count : 0, ce = barrel ? 0 : count;
+  int ib = cb, ie = ce;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const int vb = __shfl_up_sync(0xffffffffu, ib, off);
+    const int ve = __shfl_up_sync(0xffffffffu, ie, off);
+    if (lane >= off) {
+      ib += vb;
+      ie += ve;
+    }
+  }
+  if (lane == 31) {
+    sh.n[warp][0] = ib;
+    sh.n[warp][1] = ie;
+  }
+  __syncthreads();
+  if (threadIdx.x < 2) {
+    const int end = threadIdx.x;
+    int tot = 0;
+    for (int w = 0; w < kBlock / 32; ++w) {
+      sh.base[w][end] = tot;
+      tot += sh.n[w][end];
+    }
+    const int b = tot ? atomicAdd(cnt + end, tot) : 0;
+    for (int w = 0; w < kBlock / 32; ++w) sh.base[w][end] += b;
+  }
+  __syncthreads();
+  return barrel ? sh.base[warp][0] + ib - cb : sh.base[warp][1] + ie - ce;
+}
+
 // One-ended block-aggregated append (counter cnt[0]); uses sh.n[.][0] and
 // sh.base[.][0] only after the block synchronises, like the two-ended form.
 __device__ __forceinline__ void append_list_block(bool want, int value, int* list, int* cnt,
@@ -173,51 +209,54 @@ __global__ void __launch_bounds__(kBlock) k_activate(EventDev E, const FindConfi
 __global__ void __launch_bounds__(kBlock, MKFG_HEAVY_MIN_BLOCKS) k_propagate(EventDev E, const FindConfigDev* __restrict__ Cp,
                                                       int step) {
   const FindConfigDev& C = *Cp;
-  const int* cnt = E.step_count + step * kCntN;
+  int* cnt = E.step_count + step * kCntN;
   const int nb = cnt[kCntActBarrel], ne = cnt[kCntActEndcap];
   const int stride = E.cand[0].cap;
   if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&E.work[step * 4 + 0], nb + ne);
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nb + ne; j += gridDim.x * blockDim.x) {
-    const int slot = j < nb ? E.act_list[j] : E.act_list[E.list_cap - 1 - (j - nb)];
-    const int s = slot / kSlots, c = slot % kSlots;
-    const int reg = E.region[s];
-    const int layer = plan_layer(C, reg, step);
-    const CandSoA& B = E.cand[E.cur[s]];
-    float par[6], err[21];
-    load_state(B, slot, par, err);
-    const int chg = B.chg[slot];
-    const LayerDev& L = C.layer[layer];
-    const int ev = E.seed_event[s];
-    PrepOut o;
-    prep_cand(E, C, L, E.bins + (size_t)ev * E.n_bins + L.bin_offset,
-              E.layer_begin[ev * E.lb_stride + layer], reg, layer, s, B, slot, par, err, chg,
-              E.xhit + slot, stride, o);
-    if (o.extra == 2) E.extra_last[slot] = o.extra_last;
+  __shared__ BlockAppend sh;
+  // Block-uniform loop: the pair-list reservation synchronises the block.
+  for (int j0 = blockIdx.x * kBlock; j0 < nb + ne; j0 += gridDim.x * kBlock) {
+    const int j = j0 + threadIdx.x;
+    int xs = 0, slot = 0;
+    bool barrel = true;
+    if (j < nb + ne) {
+      slot = j < nb ? E.act_list[j] : E.act_list[E.list_cap - 1 - (j - nb)];
+      const int s = slot / kSlots, c = slot % kSlots;
+      const int reg = E.region[s];
+      const int layer = plan_layer(C, reg, step);
+      const CandSoA& B = E.cand[E.cur[s]];
+      float par[6], err[21];
+      load_state(B, slot, par, err);
+      const int chg = B.chg[slot];
+      const LayerDev& L = C.layer[layer];
+      const int ev = E.seed_event[s];
+      PrepOut o;
+      prep_cand(E, C, L, E.bins + (size_t)ev * E.n_bins + L.bin_offset,
+                E.layer_begin[ev * E.lb_stride + layer], reg, layer, s, B, slot, par, err, chg,
+                E.xhit + slot, stride, o);
+      if (o.extra == 2) E.extra_last[slot] = o.extra_last;
 #pragma unroll
-    for (int e = 0; e < 6; ++e) E.ppar[e * stride + slot] = o.ppar[e];
+      for (int e = 0; e < 6; ++e) E.ppar[e * stride + slot] = o.ppar[e];
 #pragma unroll
-    for (int e = 0; e < 21; ++e) E.perr[e * stride + slot] = o.perr[e];
-    if (o.xs > 0) {
-      if (L.is_barrel) {
-        const int base = atomicAdd(E.step_count + step * kCntN + kCntPairBarrel, o.xs);
-        for (int h = 0; h < o.xs; ++h) E.pairs[base + h] = slot * kMaxXHits + h;
+      for (int e = 0; e < 21; ++e) E.perr[e * stride + slot] = o.perr[e];
+      const size_t rbase = (size_t)s * kRecPerSeed + c * kRecPerCand;
+      const size_t r = rbase + kMaxXHits;
+      if (o.hole) {
+        E.rhit[r] = o.hole_hit;
+        E.rmodule[r] = -1;
+        E.rchi2hit[r] = 0.f;
+        E.rscore[r] = o.hole_score;
       } else {
-        const int base = atomicAdd(E.step_count + step * kCntN + kCntPairEndcap, o.xs);
-        for (int h = 0; h < o.xs; ++h) E.pairs[E.pair_cap - 1 - (base + h)] = slot * kMaxXHits + h;
+        E.rhit[r] = kRecInvalid;
       }
+      for (int h = o.xs; h < kMaxXHits; ++h) E.rhit[rbase + h] = kRecInvalid;
+      E.wsr[slot] = o.wsr | (o.extra << 8);
+      xs = max(o.xs, 0);
+      barrel = L.is_barrel;
     }
-    const size_t rbase = (size_t)s * kRecPerSeed + c * kRecPerCand;
-    const size_t r = rbase + kMaxXHits;
-    if (o.hole) {
-      E.rhit[r] = o.hole_hit;
-      E.rmodule[r] = -1;
-      E.rchi2hit[r] = 0.f;
-      E.rscore[r] = o.hole_score;
-    } else {
-      E.rhit[r] = kRecInvalid;
-    }
-    for (int h = o.xs; h < kMaxXHits; ++h) E.rhit[rbase + h] = kRecInvalid;
-    E.wsr[slot] = o.wsr | (o.extra << 8);
+    const int base = reserve_two_ended_block(xs, barrel, cnt + kCntPairBarrel, sh);
+    for (int h = 0; h < xs; ++h)
+      E.pairs[barrel ? base + h : E.pair_cap - 1 - (base + h)] = slot * kMaxXHits + h;
   }
 }
 

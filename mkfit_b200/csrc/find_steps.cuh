@@ -155,22 +155,30 @@ __device__ __forceinline__ int select_hits(const EventDev& E, const LayerDev& L,
   const int pb1 = phi_bin(phi - dphi);
   const int pb2 = phi_bin(phi + dphi) + 1;
 
+  // Bins in scan order (q row, then phi bin mod 256), read eight at a time
+  // so the loads of a row are in flight together.
+  constexpr int kBinChunk = 8;
   int n = 0;
   for (int qi = qb1; qi < qb2; ++qi) {
-    for (int pi = pb1; pi < pb2; ++pi) {
-      const int pb = pi & 0xff;
-      const uint32_t bin = __ldg(bins + qi * 256 + pb);
-      const int first = bin & 0xffff, last = bin >> 16;
-      for (int hi = first; hi < last; ++hi) {
-        if (n >= kMaxXHits) break;
-        const int g = hit_base + hi;
-        const float2 hq = __ldg(E.qphi + g);
-        const float ddq = fabsf(q - hq.x);
-        const float ddphi = cdist(fabsf(phi - hq.y));
-        if (ddq >= dq) continue;
-        if (ddphi >= dphi) continue;
-        xhit[n * xstride] = __ldg(E.srank + g);
-        ++n;
+    const uint32_t* row = bins + qi * 256;
+    for (int p0 = pb1; p0 < pb2; p0 += kBinChunk) {
+      uint32_t bv[kBinChunk];
+#pragma unroll
+      for (int k = 0; k < kBinChunk; ++k) bv[k] = p0 + k < pb2 ? __ldg(row + ((p0 + k) & 0xff)) : 0u;
+#pragma unroll
+      for (int k = 0; k < kBinChunk; ++k) {
+        const int first = bv[k] & 0xffff, last = bv[k] >> 16;
+        for (int hi = first; hi < last; ++hi) {
+          if (n >= kMaxXHits) break;
+          const int g = hit_base + hi;
+          const float2 hq = __ldg(E.qphi + g);
+          const float ddq = fabsf(q - hq.x);
+          const float ddphi = cdist(fabsf(phi - hq.y));
+          if (ddq >= dq) continue;
+          if (ddphi >= dphi) continue;
+          xhit[n * xstride] = __ldg(E.srank + g);
+          ++n;
+        }
       }
     }
   }
