@@ -36,6 +36,12 @@ constexpr int kBlock = 256;
 #ifndef MKFG_HEAVY_MIN_BLOCKS
 #define MKFG_HEAVY_MIN_BLOCKS 2
 #endif
+// The same for the clone kernel (one warp per seed, latency bound: the
+// full 64 warps per SM pay for the few registers spilled to L1).
+#ifndef MKFG_CLONE_MIN_BLOCKS
+#define MKFG_CLONE_MIN_BLOCKS 8
+#endif
+
 
 // Appends `value` for the lanes where `want` holds to a two-ended list:
 // barrel entries from the front (counter cnt[0]), endcap entries from the
@@ -308,7 +314,7 @@ __global__ void __launch_bounds__(kBlock, MKFG_HEAVY_MIN_BLOCKS) k_chi2(EventDev
 // Kernel 3: per-seed candidate cloning (CandCloner::ProcessSeedRange,
 // mkFit/CandCloner.cc:36-189). One warp per seed.
 //------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) k_clone(EventDev E, const FindConfigDev* __restrict__ Cp,
+__global__ void __launch_bounds__(kBlock, MKFG_CLONE_MIN_BLOCKS) k_clone(EventDev E, const FindConfigDev* __restrict__ Cp,
                                                   int step) {
   const FindConfigDev& C = *Cp;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

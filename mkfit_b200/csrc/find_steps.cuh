@@ -588,22 +588,41 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
   const int M = C.max_cands;
   const unsigned below = (1u << lane) - 1u;
 
+  // Valid records: those of candidates [0, ncand) not marked invalid; of
+  // them, the hit records (not the hole record) under the overlap chi2 cut.
+  constexpr int kPer = (kRecPerSeed + 31) / 32;
+  static_assert(kPer == 5, "record masks are five words");
+  bool valid[kPer];
+  unsigned vmask[kPer], omask[kPer];
+  int n_valid = 0;
+#pragma unroll
+  for (int k = 0; k < kPer; ++k) {
+    const int idx = lane + 32 * k;
+    valid[k] = idx < ncand * kRecPerCand && R.valid(idx, ncand);
+    const bool ov_ok = valid[k] && idx % kRecPerCand != kMaxXHits &&
+                       R.chi2hit(idx) < C.chi2_cut_overlap;
+    vmask[k] = __ballot_sync(kFull, valid[k]);
+    omask[k] = __ballot_sync(kFull, ov_ok);
+    n_valid += __popc(vmask[k]);
+  }
+
   // Overlap candidates per parent (consulted at CandCloner.cc:120-124),
-  // filled in hit order as MkFinder does (:1212-1216); lane c scans
-  // candidate c's records.
+  // filled in hit order as MkFinder does (:1212-1216): lane c takes
+  // candidate c's 16 bits of the overlap mask and considers those hits.
   if (lane < kSlots) {
     HitMatchPair p;
     p.reset();
     if (lane < ncand) {
-      // Records of hits under the overlap cut, then those alone in order.
-      unsigned m = 0;
-#pragma unroll
-      for (int h = 0; h < kMaxXHits; ++h) {
-        const int idx = lane * kRecPerCand + h;
-        if (R.hit(idx) != kRecInvalid && R.chi2hit(idx) < C.chi2_cut_overlap) m |= 1u << h;
-      }
+      const int bit = lane * kRecPerCand, word = bit >> 5, sh = bit & 31;
+      const unsigned lo = word == 0 ? omask[0] : word == 1 ? omask[1] : word == 2 ? omask[2]
+                                                                      : word == 3 ? omask[3]
+                                                                                  : omask[4];
+      const unsigned hi = word == 0 ? omask[1] : word == 1 ? omask[2] : word == 2 ? omask[3]
+                                                                                  : omask[4];
+      unsigned m = (lo >> sh) | (sh ? hi << (32 - sh) : 0u);
+      m &= (1u << kMaxXHits) - 1u;
       while (m) {
-        const int idx = lane * kRecPerCand + __ffs(m) - 1;
+        const int idx = bit + __ffs(m) - 1;
         m &= m - 1;
         p.consider(R.hit(idx), R.module(idx), R.chi2hit(idx));
       }
@@ -617,19 +636,6 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
   const float c_score = is_cand ? B.score[cslot] : 0.f;
   const float c_ipt = is_cand ? B.par[3 * B.cap + cslot] : 1.f;
   const int c_kind = (is_cand && state == kFinding) ? R.extra_kind(lane) : 0;
-
-  // Valid records: those of candidates [0, ncand) not marked invalid.
-  constexpr int kPer = (kRecPerSeed + 31) / 32;
-  bool valid[kPer];
-  unsigned vmask[kPer];
-  int n_valid = 0;
-#pragma unroll
-  for (int k = 0; k < kPer; ++k) {
-    const int idx = lane + 32 * k;
-    valid[k] = idx < ncand * kRecPerCand && R.valid(idx, ncand);
-    vmask[k] = __ballot_sync(kFull, valid[k]);
-    n_valid += __popc(vmask[k]);
-  }
 
   // Extras (held-back candidates) in candidate order (MkBuilder.cc:1600-1626).
   const unsigned extra_mask = __ballot_sync(kFull, c_kind != 0);
@@ -731,19 +737,51 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
   const float r_chi2 = has_rec ? R.chi2hit(my_rec) : 0.f;
   const int r_module = has_rec ? R.module(my_rec) : 0;
 
-  // Build the new candidate list (sequential logic of ProcessSeedRange),
-  // identically in every lane from the broadcast values; lane i keeps new
-  // candidate i.
+  // Build the new candidate list (logic of ProcessSeedRange); lane i keeps
+  // new candidate i.
   NewCand nc{0, 0, 0.f, -1, 0.f, 0};
   int n_pushed = 0;
+  float bs_score = E.bshort_valid[s] ? E.bshort.score[s] : -1e16f;  // getScoreWorstPossible
+  int bs_from = -1;
+  if (extra_mask == 0) {
+    // No extras: the new candidates are the records in order, less the
+    // stop (-2) records, of which the first (best) may replace the best
+    // short candidate. All lanes at once.
+    const bool is_stop = has_rec && r_hit == -2;
+    const unsigned stop_mask = __ballot_sync(kFull, is_stop);
+    const unsigned push_mask = __ballot_sync(kFull, has_rec && !is_stop);
+    n_pushed = __popc(push_mask);
+    if (stop_mask) {
+      const int f = __ffs(stop_mask) - 1;
+      const float sc = __shfl_sync(kFull, r_score, f);
+      const int rec = __shfl_sync(kFull, my_rec, f);
+      if (sc > bs_score) {
+        bs_score = sc;
+        bs_from = rec;
+      }
+    }
+    const int src = stop_mask ? (int)__fns(push_mask, 0, lane + 1) & 31 : lane;
+    const int idx = __shfl_sync(kFull, my_rec, src);
+    const int hit = __shfl_sync(kFull, r_hit, src);
+    const float score = __shfl_sync(kFull, r_score, src);
+    const float chi2hit = __shfl_sync(kFull, r_chi2, src);
+    const int module = __shfl_sync(kFull, r_module, src);
+    const int parent = idx / kRecPerCand;
+    const float ppt = fabsf(1.f / __shfl_sync(kFull, c_ipt, parent & 31));
+    if (lane < n_pushed) {
+      int ov = -1;
+      if (ppt > C.pt_cut_overlap && hit >= 0) ov = hm[parent].find(hit, module);
+      nc = NewCand{parent, hit, chi2hit, ov, score, 0};
+    }
+  }
   auto push = [&](const NewCand& v) {
     if (lane == n_pushed) nc = v;
     ++n_pushed;
   };
   unsigned em = extra_mask;  // extras not yet taken, in candidate order
-  float bs_score = E.bshort_valid[s] ? E.bshort.score[s] : -1e16f;  // getScoreWorstPossible
-  int bs_from = -1;
-  for (int ih = 0; ih < num_hits; ++ih) {
+  // With extras: sequentially, identically in every lane from the
+  // broadcast values.
+  for (int ih = 0; ih < (extra_mask ? num_hits : 0); ++ih) {
     const int idx = __shfl_sync(kFull, my_rec, ih);
     const int hit = __shfl_sync(kFull, r_hit, ih);
     const float score = __shfl_sync(kFull, r_score, ih);
