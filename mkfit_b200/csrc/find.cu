@@ -319,7 +319,7 @@ __global__ void __launch_bounds__(kBlock, MKFG_CLONE_MIN_BLOCKS) k_clone(EventDe
   const FindConfigDev& C = *Cp;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   __shared__ HitMatchPair s_hm[kBlock / 32][kSlots];
-  __shared__ int s_scratch[kBlock / 32][32];
+  __shared__ CloneScratch s_scratch[kBlock / 32];
   __shared__ BlockAppend sh;
   HitMatchPair* hm = s_hm[warp];
   int* cnt = E.step_count + step * kCntN;
@@ -338,10 +338,13 @@ __global__ void __launch_bounds__(kBlock, MKFG_CLONE_MIN_BLOCKS) k_clone(EventDe
       const int cur = E.cur[s];
       const size_t rb = (size_t)s * kRecPerSeed;
       const int ncand = E.n_cands[s];
+      const int hit0 = E.layer_begin[E.seed_event[s] * E.lb_stride + layer];
       const SeedRecords R{E.rhit + rb,          E.rscore + rb,           E.rchi2hit + rb,
                           E.rmodule + rb,       E.wsr + s * kSlots,      E.extra_last + s * kSlots,
-                          E.upd + s * kSlots};
-      const int n = clone_seed(E, C, s, layer, kFinding, ncand, cur, R, hm, s_scratch[warp], lane);
+                          nullptr};
+      int upd = 0;
+      const int n = clone_seed(E, C, s, layer, kFinding, ncand, cur, R, hm, s_scratch[warp], upd,
+                               lane);
       if (n >= 0 && lane == 0) {
         E.n_cands[s] = n;
         E.cur[s] = cur ^ 1;
@@ -349,8 +352,8 @@ __global__ void __launch_bounds__(kBlock, MKFG_CLONE_MIN_BLOCKS) k_clone(EventDe
       // The new candidates that take a Kalman update, with the global index
       // of the hit to update with (on this step's layer).
       slot = s * kSlots + lane;
-      u = lane < n ? E.upd[slot] : 0;
-      g = u ? E.layer_begin[E.seed_event[s] * E.lb_stride + layer] + (u - 1) : 0;
+      u = lane < n ? upd : 0;
+      g = u ? hit0 + (u - 1) : 0;
       barrel = C.layer[layer].is_barrel;
     }
     append_two_ended_block(u != 0, barrel, slot, E.upd_list, E.list_cap, cnt + kCntUpdBarrel, sh, g,
@@ -372,7 +375,6 @@ __global__ void __launch_bounds__(kBlock, MKFG_HEAVY_MIN_BLOCKS) k_update(EventD
     const int at = j < nb ? j : E.list_cap - 1 - (j - nb);
     const int slot = E.upd_list[at];
     const int s = slot / kSlots;
-    E.upd[slot] = 0;
     const LayerDev& L = C.layer[plan_layer(C, E.region[s], step)];
     update_cand_at(E, C, L, E.upd_hit[at], E.cand[E.cur[s]], slot);
   }

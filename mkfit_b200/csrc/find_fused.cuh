@@ -33,7 +33,7 @@ struct FusedShared {
   int rmodule[W * kRecPerSeed];
   unsigned short pairs[T * kMaxXHits];
   HitMatchPair hm[T / 32][kSlots];
-  int scratch[T / 32][32];
+  CloneScratch scratch[T / 32];
   int n_pairs;
 };
 
@@ -164,8 +164,9 @@ __global__ void __launch_bounds__(W * kSlots) k_find_fused(EventDev E,
       const SeedRecords R{S.rhit + rb,          S.rscore + rb,           S.rchi2hit + rb,
                           S.rmodule + rb,       S.wsr + wl * kSlots,     S.extra_last + wl * kSlots,
                           S.upd + wl * kSlots};
+      int upd = 0;
       const int n = clone_seed(E, C, ws, wlayer, wstate, E.n_cands[ws], cur, R, S.hm[warp],
-                                 S.scratch[warp], lane);
+                               S.scratch[warp], upd, lane);
       if (n >= 0 && lane == 0) {
         E.n_cands[ws] = n;
         E.cur[ws] = cur ^ 1;

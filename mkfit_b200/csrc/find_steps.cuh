@@ -517,7 +517,8 @@ struct SeedRecords {
   const int* wsr_;         // WSR code | extra kind << 8, per candidate
   const int* extra_last_;  // stop node of a kind-2 extra, per candidate
   int* upd_;               // per new candidate: 1 + index in its layer of the hit
-                           // to update with (the last one added), 0 = none
+                           // to update with (the last one added), 0 = none;
+                           // null: returned only
   __device__ bool valid(int idx, int ncand) const {
     return idx / kRecPerCand < ncand && hit_[idx] != kRecInvalid;
   }
@@ -527,7 +528,9 @@ struct SeedRecords {
   __device__ int module(int idx) const { return module_[idx]; }
   __device__ int extra_kind(int c) const { return wsr_[c] >> 8; }
   __device__ int extra_last(int c) const { return extra_last_[c]; }
-  __device__ void set_upd(int i, int v) const { upd_[i] = v; }
+  __device__ void set_upd(int i, int v) const {
+    if (upd_) upd_[i] = v;
+  }
 };
 
 // Total order of record scores as integers: the float order, with -0 taken
@@ -574,36 +577,86 @@ __device__ __forceinline__ int arena_put(const EventDev& E, int s, int pos, int 
   return pos;
 }
 
+// Shared-memory scratch of one warp's clone step: the valid records
+// compacted (then ranked) with their fields, and the counters of the
+// seed's candidates.
+struct CloneScratch {
+  int rec[32];
+  int hit[32];
+  float score[32];
+  float chi2[32];
+  int module[32];
+  // Per candidate: chg, chi2 bits, last, nfound, nmiss, nover, ninside,
+  // ntail, score bits, 1/pT bits, extra kind.
+  int cand[11][kSlots];
+};
+
 // CandCloner::ProcessSeedRange for one seed (mkFit/CandCloner.cc:36-189),
 // executed by one warp. Returns the new candidate count, or -1 when the
-// seed's candidates are unchanged. scratch: 32 ints of the warp's shared
-// memory.
+// seed's candidates are unchanged; upd_out: lane i's new candidate's
+// update code (SeedRecords::upd_). The warp owns the seed's arena counter.
 __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev& C, int s,
                                           int layer, int state, int ncand, int cur,
-                                          const SeedRecords& R, HitMatchPair* hm, int* scratch,
-                                          int lane) {
+                                          const SeedRecords& R, HitMatchPair* hm,
+                                          CloneScratch& X, int& upd_out, int lane) {
   constexpr unsigned kFull = 0xffffffffu;
   const CandSoA& B = E.cand[cur];
   const CandSoA& N = E.cand[cur ^ 1];
   const int M = C.max_cands;
   const unsigned below = (1u << lane) - 1u;
+  upd_out = 0;
+  const int hot0 = E.hot_size[s];
+
+  // Per-candidate values, staged by lane c for candidate c.
+  const int cslot = s * kSlots + (lane < kSlots ? lane : 0);
+  const bool is_cand = lane < ncand;
+  const int c_kind = (is_cand && state == kFinding) ? R.extra_kind(lane) : 0;
+  if (is_cand) {
+    X.cand[8][lane] = __float_as_int(B.score[cslot]);
+    X.cand[9][lane] = __float_as_int(B.par[3 * B.cap + cslot]);
+    X.cand[10][lane] = c_kind;
+    X.cand[0][lane] = B.chg[cslot];
+    X.cand[1][lane] = __float_as_int(B.chi2[cslot]);
+    X.cand[2][lane] = B.last[cslot];
+    X.cand[3][lane] = B.nfound[cslot];
+    X.cand[4][lane] = B.nmiss[cslot];
+    X.cand[5][lane] = B.nover[cslot];
+    X.cand[6][lane] = B.ninside[cslot];
+    X.cand[7][lane] = B.ntail[cslot];
+  }
 
   // Valid records: those of candidates [0, ncand) not marked invalid; of
   // them, the hit records (not the hole record) under the overlap chi2 cut.
+  // The first 32 valid ones are compacted in record order into X.
   constexpr int kPer = (kRecPerSeed + 31) / 32;
   static_assert(kPer == 5, "record masks are five words");
-  bool valid[kPer];
-  unsigned vmask[kPer], omask[kPer];
+  unsigned omask[kPer];
   int n_valid = 0;
 #pragma unroll
   for (int k = 0; k < kPer; ++k) {
     const int idx = lane + 32 * k;
-    valid[k] = idx < ncand * kRecPerCand && R.valid(idx, ncand);
-    const bool ov_ok = valid[k] && idx % kRecPerCand != kMaxXHits &&
-                       R.chi2hit(idx) < C.chi2_cut_overlap;
-    vmask[k] = __ballot_sync(kFull, valid[k]);
+    const bool in = idx < ncand * kRecPerCand;
+    int h = kRecInvalid, mo = 0;
+    float c2 = 0.f, sc = 0.f;
+    if (in) {
+      h = R.hit(idx);
+      c2 = R.chi2hit(idx);
+      sc = R.score(idx);
+      mo = R.module(idx);
+    }
+    const bool valid = in && h != kRecInvalid;
+    const bool ov_ok = valid && idx % kRecPerCand != kMaxXHits && c2 < C.chi2_cut_overlap;
+    const unsigned vmask = __ballot_sync(kFull, valid);
     omask[k] = __ballot_sync(kFull, ov_ok);
-    n_valid += __popc(vmask[k]);
+    const int pos = n_valid + __popc(vmask & below);
+    if (valid && pos < 32) {
+      X.rec[pos] = idx;
+      X.hit[pos] = h;
+      X.score[pos] = sc;
+      X.chi2[pos] = c2;
+      X.module[pos] = mo;
+    }
+    n_valid += __popc(vmask);
   }
 
   // Overlap candidates per parent (consulted at CandCloner.cc:120-124),
@@ -629,13 +682,6 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
     }
     hm[lane] = p;
   }
-
-  // Per-candidate values, lane c holding candidate c's.
-  const int cslot = s * kSlots + (lane < kSlots ? lane : 0);
-  const bool is_cand = lane < ncand;
-  const float c_score = is_cand ? B.score[cslot] : 0.f;
-  const float c_ipt = is_cand ? B.par[3 * B.cap + cslot] : 1.f;
-  const int c_kind = (is_cand && state == kFinding) ? R.extra_kind(lane) : 0;
 
   // Extras (held-back candidates) in candidate order (MkBuilder.cc:1600-1626).
   const unsigned extra_mask = __ballot_sync(kFull, c_kind != 0);
@@ -676,36 +722,54 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
 
   // Top-num_hits records in (score desc, record index asc) order: the
   // reference's std::sort by score; on exact score ties this order is the
-  // stable one. Lane i receives the i-th record's index.
+  // stable one. Lane i receives the i-th record and its fields.
   const int num_hits = min(n_valid, M);
-  int my_rec = 0;
+  const bool has_rec = lane < num_hits;
+  int my_rec = 0, r_hit = 0, r_module = 0;
+  float r_score = 0.f, r_chi2 = 0.f;
   if (n_valid <= 32) {
-    // Compact the valid records in record order (lane p takes the p-th),
-    // rank each against all others, place the first num_hits by rank.
-    int off = 0;
-#pragma unroll
-    for (int k = 0; k < kPer; ++k) {
-      if (valid[k]) scratch[off + __popc(vmask[k] & below)] = lane + 32 * k;
-      off += __popc(vmask[k]);
+    // All valid records are compacted (lane p holds the p-th): rank each
+    // against all others, place the first num_hits by rank.
+    const bool mine = lane < n_valid;
+    if (mine) {
+      my_rec = X.rec[lane];
+      r_hit = X.hit[lane];
+      r_score = X.score[lane];
+      r_chi2 = X.chi2[lane];
+      r_module = X.module[lane];
     }
-    __syncwarp();
-    const int ridx = lane < n_valid ? scratch[lane] : 0;
-    const int key = lane < n_valid ? score_key(R.score(ridx)) : INT_MIN;
+    const int key = mine ? score_key(r_score) : INT_MIN;
     int rank = 0;
     for (int j = 0; j < n_valid; ++j) {
       const int kj = __shfl_sync(kFull, key, j);
       rank += (kj > key) || (kj == key && j < lane);
     }
     __syncwarp();
-    if (lane < n_valid && rank < num_hits) scratch[rank] = ridx;
+    if (mine && rank < num_hits) {
+      X.rec[rank] = my_rec;
+      X.hit[rank] = r_hit;
+      X.score[rank] = r_score;
+      X.chi2[rank] = r_chi2;
+      X.module[rank] = r_module;
+    }
     __syncwarp();
-    if (lane < num_hits) my_rec = scratch[lane];
-    __syncwarp();
+    if (has_rec) {
+      my_rec = X.rec[lane];
+      r_hit = X.hit[lane];
+      r_score = X.score[lane];
+      r_chi2 = X.chi2[lane];
+      r_module = X.module[lane];
+    }
   } else {
     // More records than lanes: num_hits rounds of a warp arg-max.
     int key[kPer];
+    bool valid[kPer];
 #pragma unroll
-    for (int k = 0; k < kPer; ++k) key[k] = valid[k] ? score_key(R.score(lane + 32 * k)) : INT_MIN;
+    for (int k = 0; k < kPer; ++k) {
+      const int idx = lane + 32 * k;
+      valid[k] = idx < ncand * kRecPerCand && R.hit(idx) != kRecInvalid;
+      key[k] = valid[k] ? score_key(R.score(idx)) : INT_MIN;
+    }
     for (int i = 0; i < num_hits; ++i) {
       int best = INT_MIN, bidx = INT_MAX;
 #pragma unroll
@@ -730,12 +794,13 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
       for (int k = 0; k < kPer; ++k)
         if (lane + 32 * k == bidx) valid[k] = false;
     }
+    if (has_rec) {
+      r_hit = R.hit(my_rec);
+      r_score = R.score(my_rec);
+      r_chi2 = R.chi2hit(my_rec);
+      r_module = R.module(my_rec);
+    }
   }
-  const bool has_rec = lane < num_hits;
-  const int r_hit = has_rec ? R.hit(my_rec) : 0;
-  const float r_score = has_rec ? R.score(my_rec) : 0.f;
-  const float r_chi2 = has_rec ? R.chi2hit(my_rec) : 0.f;
-  const int r_module = has_rec ? R.module(my_rec) : 0;
 
   // Build the new candidate list (logic of ProcessSeedRange); lane i keeps
   // new candidate i.
@@ -767,8 +832,8 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
     const float chi2hit = __shfl_sync(kFull, r_chi2, src);
     const int module = __shfl_sync(kFull, r_module, src);
     const int parent = idx / kRecPerCand;
-    const float ppt = fabsf(1.f / __shfl_sync(kFull, c_ipt, parent & 31));
     if (lane < n_pushed) {
+      const float ppt = fabsf(1.f / __int_as_float(X.cand[9][parent]));
       int ov = -1;
       if (ppt > C.pt_cut_overlap && hit >= 0) ov = hm[parent].find(hit, module);
       nc = NewCand{parent, hit, chi2hit, ov, score, 0};
@@ -797,19 +862,19 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
     }
     while (em && n_pushed < M) {
       const int c = __ffs(em) - 1;
-      if (!(__shfl_sync(kFull, c_score, c) > score)) break;
-      push(NewCand{c, 0, 0.f, -1, 0.f, __shfl_sync(kFull, c_kind, c)});
+      if (!(__int_as_float(X.cand[8][c]) > score)) break;
+      push(NewCand{c, 0, 0.f, -1, 0.f, X.cand[10][c]});
       em &= em - 1;
     }
     if (n_pushed >= M) break;
     int ov = -1;
-    const float ppt = fabsf(1.f / __shfl_sync(kFull, c_ipt, parent));
+    const float ppt = fabsf(1.f / __int_as_float(X.cand[9][parent]));
     if (ppt > C.pt_cut_overlap && hit >= 0) ov = hm[parent].find(hit, module);
     push(NewCand{parent, hit, chi2hit, ov, score, 0});
   }
   while (em && n_pushed < M) {
     const int c = __ffs(em) - 1;
-    push(NewCand{c, 0, 0.f, -1, 0.f, __shfl_sync(kFull, c_kind, c)});
+    push(NewCand{c, 0, 0.f, -1, 0.f, X.cand[10][c]});
     em &= em - 1;
   }
 
@@ -826,9 +891,8 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
   }
   const int nodes_total = __shfl_sync(kFull, node_off, 31) + (bs_from >= 0);
   node_off -= n_nodes;
-  int node_base = 0;
-  if (lane == 0 && nodes_total) node_base = atomicAdd(&E.hot_size[s], nodes_total);
-  node_base = __shfl_sync(kFull, node_base, 0) + (bs_from >= 0);
+  if (lane == 0 && nodes_total) E.hot_size[s] = hot0 + nodes_total;
+  const int node_base = hot0 + (bs_from >= 0);
 
   // Best short candidate (a -2 record scoring above the current best).
   if (bs_from >= 0) {
@@ -860,12 +924,12 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
   // candidate i by lane i.
   copy_par_err(B, N, s, n_pushed, nc.parent, lane);
   if (lane < n_pushed) {
-    const int src = s * kSlots + nc.parent, dst = s * kSlots + lane;
-    int nfound = B.nfound[src], nmiss = B.nmiss[src], nin = B.ninside[src], ntl = B.ntail[src];
-    int nover = B.nover[src];
-    float chi2 = B.chi2[src];
-    int last = B.last[src];
-    float score = B.score[src];
+    const int pc = nc.parent, dst = s * kSlots + lane;
+    int nfound = X.cand[3][pc], nmiss = X.cand[4][pc], nin = X.cand[6][pc], ntl = X.cand[7][pc];
+    int nover = X.cand[5][pc];
+    float chi2 = __int_as_float(X.cand[1][pc]);
+    int last = X.cand[2][pc];
+    float score = __int_as_float(X.cand[8][pc]);
     int upd = 0;
     if (nc.is_extra) {
       if (nc.is_extra == 2) {
@@ -886,7 +950,7 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
       // UpdateWithLastHit uses the last hit added: the overlap hit if any.
       if (nc.hit >= 0) upd = 1 + (nc.ov >= 0 ? hm[nc.parent].hit[nc.ov] : nc.hit);
     }
-    N.chg[dst] = B.chg[src];
+    N.chg[dst] = X.cand[0][pc];
     N.chi2[dst] = chi2;
     N.score[dst] = score;
     N.last[dst] = last;
@@ -896,6 +960,7 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
     N.ninside[dst] = nin;
     N.ntail[dst] = ntl;
     R.set_upd(lane, upd);
+    upd_out = upd;
   }
   return n_pushed;
 }
