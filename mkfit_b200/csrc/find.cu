@@ -200,8 +200,7 @@ __global__ void __launch_bounds__(kBlock) k_activate(EventDev E, const FindConfi
     // [0, ncand) of seeds still finding: an inactive one among them has
     // neither.
     if (seed_finding && !active && c < ncand) {
-      const size_t rbase = (size_t)s * kRecPerSeed + c * kRecPerCand;
-      for (int h = 0; h <= kMaxXHits; ++h) E.rhit[rbase + h] = kRecInvalid;
+      E.rmask[slot] = 0u;
       E.wsr[slot] = kWsrOutside;
     }
   }
@@ -245,17 +244,11 @@ __global__ void __launch_bounds__(kBlock, MKFG_HEAVY_MIN_BLOCKS) k_propagate(Eve
       for (int e = 0; e < 6; ++e) E.ppar[e * stride + slot] = o.ppar[e];
 #pragma unroll
       for (int e = 0; e < 21; ++e) E.perr[e * stride + slot] = o.perr[e];
-      const size_t rbase = (size_t)s * kRecPerSeed + c * kRecPerCand;
-      const size_t r = rbase + kMaxXHits;
-      if (o.hole) {
-        E.rhit[r] = o.hole_hit;
-        E.rmodule[r] = -1;
-        E.rchi2hit[r] = 0.f;
-        E.rscore[r] = o.hole_score;
-      } else {
-        E.rhit[r] = kRecInvalid;
-      }
-      for (int h = o.xs; h < kMaxXHits; ++h) E.rhit[rbase + h] = kRecInvalid;
+      // The chi2 pass adds the bits of the accepted hits.
+      if (o.hole)
+        E.rec[(size_t)s * kRecPerSeed + c * kRecPerCand + kMaxXHits] =
+            Record{o.hole_hit, -1, 0.f, o.hole_score};
+      E.rmask[slot] = o.hole ? 1u << kMaxXHits : 0u;
       E.wsr[slot] = o.wsr | (o.extra << 8);
       xs = max(o.xs, 0);
       barrel = L.is_barrel;
@@ -300,12 +293,8 @@ __global__ void __launch_bounds__(kBlock, MKFG_HEAVY_MIN_BLOCKS) k_chi2(EventDev
     const size_t r = (size_t)s * kRecPerSeed + c * kRecPerCand + h;
     if (eval_pair(E, C, L, layer, s, g, ppar, perr, B.chg[slot], B.nfound[slot], B.nover[slot],
                   B.ninside[slot] + B.ntail[slot], B.chi2[slot], chi2, score, module)) {
-      E.rhit[r] = hidx;
-      E.rmodule[r] = module;
-      E.rchi2hit[r] = chi2;
-      E.rscore[r] = score;
-    } else {
-      E.rhit[r] = kRecInvalid;
+      E.rec[r] = Record{hidx, module, chi2, score};
+      atomicOr(E.rmask + slot, 1u << h);
     }
   }
 }
@@ -339,9 +328,8 @@ __global__ void __launch_bounds__(kBlock, MKFG_CLONE_MIN_BLOCKS) k_clone(EventDe
       const size_t rb = (size_t)s * kRecPerSeed;
       const int ncand = E.n_cands[s];
       const int hit0 = E.layer_begin[E.seed_event[s] * E.lb_stride + layer];
-      const SeedRecords R{E.rhit + rb,          E.rscore + rb,           E.rchi2hit + rb,
-                          E.rmodule + rb,       E.wsr + s * kSlots,      E.extra_last + s * kSlots,
-                          nullptr};
+      const SeedRecords R{E.rec + rb, E.rmask + s * kSlots, E.wsr + s * kSlots,
+                          E.extra_last + s * kSlots, nullptr};
       int upd = 0;
       const int n = clone_seed(E, C, s, layer, kFinding, ncand, cur, R, hm, s_scratch[warp], upd,
                                lane);
@@ -1073,12 +1061,11 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   }
   {
     const size_t nrec = (size_t)SS * kRecPerSeed;
-    if ((rc = f->recs.ensure(rounded(4 * nrec) * 4 + 4096))) return rc;
+    if ((rc = f->recs.ensure(rounded(sizeof(Record) * nrec) + rounded(4 * (size_t)SC) + 4096)))
+      return rc;
     char* p = f->recs.as<char>();
-    f->ev.rscore = carve<float>(p, nrec);
-    f->ev.rchi2hit = carve<float>(p, nrec);
-    f->ev.rhit = carve<int>(p, nrec);
-    f->ev.rmodule = carve<int>(p, nrec);
+    f->ev.rec = carve<Record>(p, nrec);
+    f->ev.rmask = carve<uint32_t>(p, SC);
   }
   {
     const size_t nn = (size_t)SS * hot_cap;

@@ -19,6 +19,15 @@ constexpr int kMaxRegions = 8;
 constexpr int kExportHits = 64;         // Config::nMaxTrkHits
 constexpr int kRecInvalid = -1000000;
 
+// One IdxChi2List entry of a candidate: a hit (index within the layer) or
+// a hole code (-1, -2, -3), with its module, chi2 and candidate score.
+struct __align__(16) Record {
+  int hit;
+  int module;
+  float chi2;
+  float score;
+};
+
 enum SeedState { kDormant = 0, kFinding = 1, kFinished = 2 };
 enum WsrCode { kWsrInside = 0, kWsrEdge = 1, kWsrOutside = 2 };
 enum ErrBits { kErrArena = 1, kErrLayerSize = 2 };
@@ -107,11 +116,11 @@ struct EventDev {
   int* wsr;        // WSR code | extra kind << 8
   int* extra_last; // arena node of the held-back copy (kind 2)
   int* upd;        // needs UpdateWithLastHit (per slot of the new buffer)
-  // Records (IdxChi2List) per seed: kRecPerSeed slots.
-  float* rscore;
-  float* rchi2hit;
-  int* rhit;       // kRecInvalid when the slot holds no record
-  int* rmodule;
+  // Records (IdxChi2List) per seed: kRecPerSeed slots, kRecPerCand per
+  // candidate (its hits in bin-scan order, then the hole record); a slot
+  // holds a record when its bit of the candidate's mask is set.
+  Record* rec;
+  uint32_t* rmask;  // per candidate slot
   // (cand slot, hit) pairs for the chi2 pass; in the plain form barrel
   // pairs fill the array from the front and endcap pairs from the back.
   int* pairs;

@@ -27,10 +27,8 @@ struct FusedShared {
   int wsr[T];
   int extra_last[T];
   int upd[T];
-  float rscore[W * kRecPerSeed];
-  float rchi2hit[W * kRecPerSeed];
-  int rhit[W * kRecPerSeed];
-  int rmodule[W * kRecPerSeed];
+  Record rec[W * kRecPerSeed];
+  uint32_t rmask[T];
   unsigned short pairs[T * kMaxXHits];
   HitMatchPair hm[T / 32][kSlots];
   CloneScratch scratch[T / 32];
@@ -101,15 +99,8 @@ __global__ void __launch_bounds__(W * kSlots) k_find_fused(EventDev E,
         for (int h = 0; h < o.xs; ++h) S.pairs[base + h] = (unsigned short)(tid * kMaxXHits + h);
       }
     }
-    if (o.hole) {
-      S.rhit[rbase + kMaxXHits] = o.hole_hit;
-      S.rmodule[rbase + kMaxXHits] = -1;
-      S.rchi2hit[rbase + kMaxXHits] = 0.f;
-      S.rscore[rbase + kMaxXHits] = o.hole_score;
-    } else {
-      S.rhit[rbase + kMaxXHits] = kRecInvalid;
-    }
-    for (int h = o.xs; h < kMaxXHits; ++h) S.rhit[rbase + h] = kRecInvalid;
+    if (o.hole) S.rec[rbase + kMaxXHits] = Record{o.hole_hit, -1, 0.f, o.hole_score};
+    S.rmask[tid] = o.hole ? 1u << kMaxXHits : 0u;
     S.wsr[tid] = o.wsr | (o.extra << 8);
     __syncthreads();
 
@@ -140,12 +131,8 @@ __global__ void __launch_bounds__(W * kSlots) k_find_fused(EventDev E,
       if (eval_pair(E, C, L, player, ps, g, ppar, perr, PB.chg[pslot], PB.nfound[pslot],
                     PB.nover[pslot], PB.ninside[pslot] + PB.ntail[pslot], PB.chi2[pslot], chi2,
                     score, module)) {
-        S.rhit[r] = hidx;
-        S.rmodule[r] = module;
-        S.rchi2hit[r] = chi2;
-        S.rscore[r] = score;
-      } else {
-        S.rhit[r] = kRecInvalid;
+        S.rec[r] = Record{hidx, module, chi2, score};
+        atomicOr(S.rmask + lt, 1u << h);
       }
     }
     __syncthreads();
@@ -161,9 +148,8 @@ __global__ void __launch_bounds__(W * kSlots) k_find_fused(EventDev E,
       const int cur = E.cur[ws];
       if (lane == 0) atomicAdd(&E.work[step * 4 + 3], 1);
       const int rb = wl * kRecPerSeed;
-      const SeedRecords R{S.rhit + rb,          S.rscore + rb,           S.rchi2hit + rb,
-                          S.rmodule + rb,       S.wsr + wl * kSlots,     S.extra_last + wl * kSlots,
-                          S.upd + wl * kSlots};
+      const SeedRecords R{S.rec + rb, S.rmask + wl * kSlots, S.wsr + wl * kSlots,
+                          S.extra_last + wl * kSlots, S.upd + wl * kSlots};
       int upd = 0;
       const int n = clone_seed(E, C, ws, wlayer, wstate, E.n_cands[ws], cur, R, S.hm[warp],
                                S.scratch[warp], upd, lane);

@@ -510,22 +510,15 @@ __device__ __forceinline__ bool update_cand(const EventDev& E, const FindConfigD
 // Records and per-candidate step results of one seed, wherever they live
 // (global memory in the plain form, shared memory in the fused form).
 struct SeedRecords {
-  const int* hit_;
-  const float* score_;
-  const float* chi2hit_;
-  const int* module_;
+  const Record* rec_;      // kRecPerSeed records
+  const uint32_t* mask_;   // per candidate: bit h set = record h present
   const int* wsr_;         // WSR code | extra kind << 8, per candidate
   const int* extra_last_;  // stop node of a kind-2 extra, per candidate
   int* upd_;               // per new candidate: 1 + index in its layer of the hit
                            // to update with (the last one added), 0 = none;
                            // null: returned only
-  __device__ bool valid(int idx, int ncand) const {
-    return idx / kRecPerCand < ncand && hit_[idx] != kRecInvalid;
-  }
-  __device__ int hit(int idx) const { return hit_[idx]; }
-  __device__ float score(int idx) const { return score_[idx]; }
-  __device__ float chi2hit(int idx) const { return chi2hit_[idx]; }
-  __device__ int module(int idx) const { return module_[idx]; }
+  __device__ Record rec(int idx) const { return rec_[idx]; }
+  __device__ uint32_t mask(int c) const { return mask_[c]; }
   __device__ int extra_kind(int c) const { return wsr_[c] >> 8; }
   __device__ int extra_last(int c) const { return extra_last_[c]; }
   __device__ void set_upd(int i, int v) const {
@@ -577,9 +570,8 @@ __device__ __forceinline__ int arena_put(const EventDev& E, int s, int pos, int 
   return pos;
 }
 
-// Shared-memory scratch of one warp's clone step: the valid records
-// compacted (then ranked) with their fields, and the counters of the
-// seed's candidates.
+// Shared-memory scratch of one warp's clone step: the ranked records with
+// their fields, and the counters of the seed's candidates.
 struct CloneScratch {
   int rec[32];
   int hit[32];
@@ -603,7 +595,6 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
   const CandSoA& B = E.cand[cur];
   const CandSoA& N = E.cand[cur ^ 1];
   const int M = C.max_cands;
-  const unsigned below = (1u << lane) - 1u;
   upd_out = 0;
   const int hot0 = E.hot_size[s];
 
@@ -625,60 +616,45 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
     X.cand[7][lane] = B.ntail[cslot];
   }
 
-  // Valid records: those of candidates [0, ncand) not marked invalid; of
-  // them, the hit records (not the hole record) under the overlap chi2 cut.
-  // The first 32 valid ones are compacted in record order into X.
-  constexpr int kPer = (kRecPerSeed + 31) / 32;
-  static_assert(kPer == 5, "record masks are five words");
-  unsigned omask[kPer];
-  int n_valid = 0;
+  constexpr int kPer = (kRecPerSeed + 31) / 32;  // present records per lane, at most
+  // Records present: the mask bits of candidates [0, ncand) (lane c holds
+  // candidate c's mask). In record order they get compacted indices
+  // p = 0 .. n_valid - 1; cincl is the inclusive count up to candidate c.
+  const uint32_t cm = is_cand ? R.mask(lane) : 0u;
+  const int ccount = __popc(cm);
+  int cincl = ccount;
 #pragma unroll
-  for (int k = 0; k < kPer; ++k) {
-    const int idx = lane + 32 * k;
-    const bool in = idx < ncand * kRecPerCand;
-    int h = kRecInvalid, mo = 0;
-    float c2 = 0.f, sc = 0.f;
-    if (in) {
-      h = R.hit(idx);
-      c2 = R.chi2hit(idx);
-      sc = R.score(idx);
-      mo = R.module(idx);
-    }
-    const bool valid = in && h != kRecInvalid;
-    const bool ov_ok = valid && idx % kRecPerCand != kMaxXHits && c2 < C.chi2_cut_overlap;
-    const unsigned vmask = __ballot_sync(kFull, valid);
-    omask[k] = __ballot_sync(kFull, ov_ok);
-    const int pos = n_valid + __popc(vmask & below);
-    if (valid && pos < 32) {
-      X.rec[pos] = idx;
-      X.hit[pos] = h;
-      X.score[pos] = sc;
-      X.chi2[pos] = c2;
-      X.module[pos] = mo;
-    }
-    n_valid += __popc(vmask);
+  for (int off = 1; off < kSlots; off <<= 1) {
+    const int v = __shfl_up_sync(kFull, cincl, off);
+    if (lane >= off) cincl += v;
   }
+  const int n_valid = __shfl_sync(kFull, cincl, kSlots - 1);
+  // Record index of present record p < n_valid (warp-collective).
+  auto locate = [&](int p) {
+    int c = 0;
+#pragma unroll
+    for (int j = 0; j < kSlots - 1; ++j) c += p >= __shfl_sync(kFull, cincl, j) ? 1 : 0;
+    const uint32_t m = __shfl_sync(kFull, cm, c);
+    const int first = __shfl_sync(kFull, cincl - ccount, c);
+    return c * kRecPerCand + (int)(__fns(m, 0, p - first + 1) & 31u);
+  };
+  const bool mine = lane < n_valid;
+  const int my_idx = locate(lane);
+  Record my_r{0, 0, 0.f, 0.f};
+  if (mine) my_r = R.rec(my_idx);
 
   // Overlap candidates per parent (consulted at CandCloner.cc:120-124),
-  // filled in hit order as MkFinder does (:1212-1216): lane c takes
-  // candidate c's 16 bits of the overlap mask and considers those hits.
+  // filled in hit order as MkFinder does (:1212-1216): lane c considers
+  // candidate c's hit records under the overlap chi2 cut.
   if (lane < kSlots) {
     HitMatchPair p;
     p.reset();
-    if (lane < ncand) {
-      const int bit = lane * kRecPerCand, word = bit >> 5, sh = bit & 31;
-      const unsigned lo = word == 0 ? omask[0] : word == 1 ? omask[1] : word == 2 ? omask[2]
-                                                                      : word == 3 ? omask[3]
-                                                                                  : omask[4];
-      const unsigned hi = word == 0 ? omask[1] : word == 1 ? omask[2] : word == 2 ? omask[3]
-                                                                                  : omask[4];
-      unsigned m = (lo >> sh) | (sh ? hi << (32 - sh) : 0u);
-      m &= (1u << kMaxXHits) - 1u;
-      while (m) {
-        const int idx = bit + __ffs(m) - 1;
-        m &= m - 1;
-        p.consider(R.hit(idx), R.module(idx), R.chi2hit(idx));
-      }
+    uint32_t m = cm & ((1u << kMaxXHits) - 1u);
+    while (m) {
+      const int h = __ffs(m) - 1;
+      m &= m - 1;
+      const Record q = R.rec(lane * kRecPerCand + h);
+      if (q.chi2 < C.chi2_cut_overlap) p.consider(q.hit, q.module, q.chi2);
     }
     hm[lane] = p;
   }
@@ -728,29 +704,20 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
   int my_rec = 0, r_hit = 0, r_module = 0;
   float r_score = 0.f, r_chi2 = 0.f;
   if (n_valid <= 32) {
-    // All valid records are compacted (lane p holds the p-th): rank each
-    // against all others, place the first num_hits by rank.
-    const bool mine = lane < n_valid;
-    if (mine) {
-      my_rec = X.rec[lane];
-      r_hit = X.hit[lane];
-      r_score = X.score[lane];
-      r_chi2 = X.chi2[lane];
-      r_module = X.module[lane];
-    }
-    const int key = mine ? score_key(r_score) : INT_MIN;
+    // Lane p holds present record p: rank each against all others, place
+    // the first num_hits by rank.
+    const int key = mine ? score_key(my_r.score) : INT_MIN;
     int rank = 0;
     for (int j = 0; j < n_valid; ++j) {
       const int kj = __shfl_sync(kFull, key, j);
       rank += (kj > key) || (kj == key && j < lane);
     }
-    __syncwarp();
     if (mine && rank < num_hits) {
-      X.rec[rank] = my_rec;
-      X.hit[rank] = r_hit;
-      X.score[rank] = r_score;
-      X.chi2[rank] = r_chi2;
-      X.module[rank] = r_module;
+      X.rec[rank] = my_idx;
+      X.hit[rank] = my_r.hit;
+      X.score[rank] = my_r.score;
+      X.chi2[rank] = my_r.chi2;
+      X.module[rank] = my_r.module;
     }
     __syncwarp();
     if (has_rec) {
@@ -761,23 +728,27 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
       r_module = X.module[lane];
     }
   } else {
-    // More records than lanes: num_hits rounds of a warp arg-max.
+    // More records than lanes: num_hits rounds of a warp arg-max over the
+    // compacted indices (their order is the record order).
     int key[kPer];
-    bool valid[kPer];
 #pragma unroll
     for (int k = 0; k < kPer; ++k) {
-      const int idx = lane + 32 * k;
-      valid[k] = idx < ncand * kRecPerCand && R.hit(idx) != kRecInvalid;
-      key[k] = valid[k] ? score_key(R.score(idx)) : INT_MIN;
+      const int p = lane + 32 * k;
+      const int idx = locate(p);
+      key[k] = p < n_valid ? score_key(R.rec(idx).score) : INT_MIN;
     }
+    bool left[kPer];
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) left[k] = lane + 32 * k < n_valid;
+    int my_p = 0;
     for (int i = 0; i < num_hits; ++i) {
       int best = INT_MIN, bidx = INT_MAX;
 #pragma unroll
       for (int k = 0; k < kPer; ++k) {
-        const int idx = lane + 32 * k;
-        if (valid[k] && (key[k] > best || (key[k] == best && idx < bidx))) {
+        const int p = lane + 32 * k;
+        if (left[k] && (key[k] > best || (key[k] == best && p < bidx))) {
           best = key[k];
-          bidx = idx;
+          bidx = p;
         }
       }
 #pragma unroll
@@ -789,16 +760,18 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
           bidx = oi;
         }
       }
-      if (lane == i) my_rec = bidx;
+      if (lane == i) my_p = bidx;
 #pragma unroll
       for (int k = 0; k < kPer; ++k)
-        if (lane + 32 * k == bidx) valid[k] = false;
+        if (lane + 32 * k == bidx) left[k] = false;
     }
+    my_rec = locate(my_p);
     if (has_rec) {
-      r_hit = R.hit(my_rec);
-      r_score = R.score(my_rec);
-      r_chi2 = R.chi2hit(my_rec);
-      r_module = R.module(my_rec);
+      const Record q = R.rec(my_rec);
+      r_hit = q.hit;
+      r_score = q.score;
+      r_chi2 = q.chi2;
+      r_module = q.module;
     }
   }
 
