@@ -264,6 +264,14 @@ int mkfg_find_run_graph(mkfg_context* ctx);
  * steps (0 reset, 1 activate, 2 propagate, 3 chi2, 4 clone, 5 update,
  * 6 merge). For per-kernel rooflines. No reference counterpart. */
 int mkfg_find_run_timed(mkfg_context* ctx, float* kernel_ms);
+/* Per layer-plan step of the last run: launch_ms[max_steps][5] the device
+ * time of each step launch of the last mkfg_find_run_timed (activate,
+ * propagate, chi2, clone, update), counts[max_steps][7] the work of the
+ * last run of any form that fills them (plain, graph, timed): active
+ * candidates in barrel / endcap layers, (candidate, hit) pairs barrel /
+ * endcap, Kalman updates barrel / endcap, seeds finding. Either pointer may
+ * be null. No reference counterpart (diagnostics). */
+int mkfg_find_step_profile(mkfg_context* ctx, float* launch_ms, int32_t* counts);
 /* Fused form of the same run: one launch in which every thread block carries
  * seeds_per_block consecutive seeds (4, 8 or 16; 0 = the value chosen by
  * mkfg_find_autotune, 16 before any tuning) through all layer steps and the

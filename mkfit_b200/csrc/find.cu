@@ -724,6 +724,12 @@ struct Finder {
   int fused_w = 16;                 // seeds per block of the fused form
   int max_nq = 1;                   // largest number of q bins of a layer
   int64_t last_chi2_evals = 0, last_seeds_cloned = 0;
+  // Per-launch device times of the last timed run: [max_steps][5] for the
+  // layer-step kernels (activate, propagate, chi2, clone, update).
+  std::vector<float> last_step_ms;
+  // Resident blocks (all SMs) of propagate, chi2, clone, update; 0 = not
+  // yet queried.
+  int resident[4] = {0, 0, 0, 0};
   // Host copies for the backward fit's seed groups: region of every sorted
   // seed and the first sorted seed of every event.
   std::vector<int> h_region;
@@ -1170,27 +1176,56 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   return MKFG_OK;
 }
 
+// Launch grids of the plain sequence. The list-driven kernels loop over
+// their lists, so their grids stop at a few waves of resident blocks:
+// one for chi2 (uniform work per pair), more where the work per list entry
+// varies and later waves balance the load.
+struct StepGrids {
+  int activate, propagate, chi2, clone, update;
+};
+
+static StepGrids step_grids(Finder* f) {
+  if (!f->resident[0]) {
+    int dev = 0, n_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    const void* fn[4] = {(const void*)k_propagate, (const void*)k_chi2, (const void*)k_clone,
+                         (const void*)k_update};
+    for (int k = 0; k < 4; ++k) {
+      int per_sm = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn[k], kBlock, 0);
+      f->resident[k] = std::max(1, n_sm * std::max(per_sm, 1));
+    }
+  }
+  const int S = f->n_seeds;
+  const int grid_c = (S * kSlots + kBlock - 1) / kBlock;
+  StepGrids g;
+  g.activate = grid_c;
+  g.propagate = std::min(grid_c, 4 * f->resident[0]);
+  g.chi2 = std::min((S * kSlots * 4 + kBlock - 1) / kBlock, f->resident[1]);
+  g.clone = std::min((S * 32 + kBlock - 1) / kBlock, 2 * f->resident[2]);
+  g.update = std::min(grid_c, 4 * f->resident[3]);
+  return g;
+}
+
 // Enqueues the whole finding sequence of the uploaded batch on `st`:
 // reset, then for every layer-plan step prep -> chi2 -> clone -> update,
 // then the final merge.
 static int enqueue_run(Finder* f, cudaStream_t st) {
   const int S = f->n_seeds;
   const int n_work = 4 * (f->host_cfg.max_steps + 2);
-  const int threads_c = S * kSlots;
-  const int grid_c = (threads_c + kBlock - 1) / kBlock;
-  const int grid_w = (S * 32 + kBlock - 1) / kBlock;
-  const int grid_p = std::min((S * kSlots * 4 + kBlock - 1) / kBlock, 148 * 16);
-  const int grid_l = std::min(grid_c, 148 * 8);
+  const int grid_c = (S * kSlots + kBlock - 1) / kBlock;
+  const StepGrids g = step_grids(f);
   MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.pair_count, 0, 4 * (size_t)(f->host_cfg.max_steps + 2), st));
   MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.step_count, 0,
                                 4 * (size_t)kCntN * (f->host_cfg.max_steps + 2), st));
   k_reset<<<std::max(grid_c, (n_work + kBlock - 1) / kBlock), kBlock, 0, st>>>(f->ev, n_work);
   for (int step = 1; step <= f->host_cfg.max_steps; ++step) {
-    k_activate<<<grid_c, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
-    k_propagate<<<grid_l, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
-    k_chi2<<<std::max(grid_p, 1), kBlock, 0, st>>>(f->ev, f->d_cfg, step);
-    k_clone<<<std::min(grid_w, 148 * 16), kBlock, 0, st>>>(f->ev, f->d_cfg, step);
-    k_update<<<grid_l, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+    k_activate<<<g.activate, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+    k_propagate<<<g.propagate, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+    k_chi2<<<g.chi2, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+    k_clone<<<g.clone, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+    k_update<<<g.update, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
   }
   k_merge<<<(S + 127) / 128, 128, 0, st>>>(f->ev, f->d_cfg);
   MKFG_CUDA_TRY(cudaGetLastError());
@@ -1232,9 +1267,7 @@ static int run_timed(mkfg_context* ctx, Finder* f, float* ms) {
   const int S = f->n_seeds;
   const int n_work = 4 * (f->host_cfg.max_steps + 2);
   const int grid_c = (S * kSlots + kBlock - 1) / kBlock;
-  const int grid_w = (S * 32 + kBlock - 1) / kBlock;
-  const int grid_p = std::min((S * kSlots * 4 + kBlock - 1) / kBlock, 148 * 16);
-  const int grid_l = std::min(grid_c, 148 * 8);
+  const StepGrids g = step_grids(f);
   const int n_ev = 2 + 5 * f->host_cfg.max_steps + 1;
   std::vector<cudaEvent_t> ev(n_ev);
   std::vector<int> cls(n_ev, -1);
@@ -1249,15 +1282,15 @@ static int run_timed(mkfg_context* ctx, Finder* f, float* ms) {
     k_reset<<<std::max(grid_c, (n_work + kBlock - 1) / kBlock), kBlock, 0, st>>>(f->ev, n_work);
     mark(0);
     for (int step = 1; step <= f->host_cfg.max_steps; ++step) {
-      k_activate<<<grid_c, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+      k_activate<<<g.activate, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
       mark(1);
-      k_propagate<<<grid_l, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+      k_propagate<<<g.propagate, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
       mark(2);
-      k_chi2<<<std::max(grid_p, 1), kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+      k_chi2<<<g.chi2, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
       mark(3);
-      k_clone<<<std::min(grid_w, 148 * 16), kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+      k_clone<<<g.clone, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
       mark(4);
-      k_update<<<grid_l, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+      k_update<<<g.update, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
       mark(5);
     }
     k_merge<<<(S + 127) / 128, 128, 0, st>>>(f->ev, f->d_cfg);
@@ -1266,10 +1299,13 @@ static int run_timed(mkfg_context* ctx, Finder* f, float* ms) {
       rc = set_error(MKFG_ERR_CUDA, "timed run failed");
       break;
     }
+    f->last_step_ms.assign(5 * (size_t)f->host_cfg.max_steps, 0.f);
     for (int k = 1; k < i; ++k) {
       float t = 0.f;
       cudaEventElapsedTime(&t, ev[k - 1], ev[k]);
       if (cls[k] >= 0) ms[cls[k]] += t;
+      // Events 2 .. 1 + 5 max_steps close the layer-step launches.
+      if (cls[k] >= 1 && cls[k] <= 5) f->last_step_ms[k - 2] = t;
     }
   } while (false);
   for (auto& e : ev) cudaEventDestroy(e);
@@ -1288,6 +1324,7 @@ static int run_graph(mkfg_context* ctx, Finder* f) {
   cudaStream_t st = ctx->stream;
   if (!f->graph) {
     cudaGraph_t g = nullptr;
+    step_grids(f);  // occupancy queries before the capture
     MKFG_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     const int rc = enqueue_run(f, st);
     const cudaError_t e = cudaStreamEndCapture(st, &g);
@@ -1424,6 +1461,27 @@ extern "C" int mkfg_find_run_timed(mkfg_context* ctx, float* kernel_ms) {
   MKFG_REQUIRE(f->configured && f->events_loaded, "no event uploaded");
   MKFG_REQUIRE(kernel_ms != nullptr, "null kernel_ms");
   return run_timed(ctx, f, kernel_ms);
+}
+
+extern "C" int mkfg_find_step_profile(mkfg_context* ctx, float* launch_ms, int32_t* counts) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  Finder* f = finder_of(ctx);
+  MKFG_REQUIRE(f->configured && f->events_loaded, "no event uploaded");
+  const int ns = f->host_cfg.max_steps;
+  if (launch_ms) {
+    MKFG_REQUIRE(f->last_step_ms.size() == 5 * (size_t)ns, "no timed run");
+    std::memcpy(launch_ms, f->last_step_ms.data(), sizeof(float) * 5 * ns);
+  }
+  if (counts) {
+    std::vector<int> all((size_t)kCntN * (ns + 2));
+    MKFG_CUDA_TRY(cudaMemcpyAsync(all.data(), f->ev.step_count, 4 * all.size(),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    MKFG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    for (int st = 1; st <= ns; ++st)
+      for (int k = 0; k < 7; ++k) counts[(st - 1) * 7 + k] = all[(size_t)st * kCntN + k];
+  }
+  return MKFG_OK;
 }
 
 extern "C" int mkfg_find_run_fused(mkfg_context* ctx, int32_t seeds_per_block) {

@@ -667,6 +667,7 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
   if (n_valid == 0) {
     // hitsForSeed empty (CandCloner.cc:163-172): the extras survive.
     if (state != kFinding) return -1;
+
     // Lane i: the i-th extra.
     int c = 0;
     if (lane < n_extras) {

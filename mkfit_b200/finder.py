@@ -58,6 +58,7 @@ def _bind(lib):
     lib.mkfg_find_backward_fit.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_int32]
     lib.mkfg_find_hit_index.argtypes = [vp, ctypes.c_int32, vp, vp]
     lib.mkfg_find_run_timed.argtypes = [vp, vp]
+    lib.mkfg_find_step_profile.argtypes = [vp, vp, vp]
     lib.mkfg_find_select.argtypes = [vp, ctypes.POINTER(MkfgSelectConfig), ctypes.c_int32, vp]
     lib.mkfg_find_run_fused.argtypes = [vp, ctypes.c_int32]
     lib.mkfg_find_autotune.argtypes = [vp, ctypes.POINTER(ctypes.c_int32),
@@ -109,6 +110,11 @@ class FindConfig:
         c.intra_layer_pflags = int(g.flags[2])
         c.requires_prop_to_hit = int(g.flags[0])
         self.c = c
+
+    @property
+    def max_steps(self):
+        """Layer-plan steps of a run: the longest plan after its pickup layer."""
+        return int(np.max(self.plan_len - self.pickup - 1))
 
 
 def event_struct(ev):
@@ -202,6 +208,23 @@ class Finder:
         ms = np.zeros(len(self.KERNELS), np.float32)
         capi.check(self.lib.mkfg_find_run_timed(self.ctx.handle, ms.ctypes.data))
         return dict(zip(self.KERNELS, ms.tolist()))
+
+    STEP_COUNTS = ("act_barrel", "act_endcap", "pairs_barrel", "pairs_endcap", "upd_barrel",
+                   "upd_endcap", "finding_seeds")
+
+    def step_profile(self, timed=True):
+        """Per layer-plan step: {kernel: ms[max_steps]} of the last run_timed
+        (when timed) and {counter: int[max_steps]} of the last run."""
+        ns = self.cfg.max_steps
+        ms = np.zeros((ns, 5), np.float32)
+        cnt = np.zeros((ns, len(self.STEP_COUNTS)), np.int32)
+        capi.check(self.lib.mkfg_find_step_profile(self.ctx.handle,
+                                                   ms.ctypes.data if timed else None,
+                                                   cnt.ctypes.data))
+        out = {k: cnt[:, i] for i, k in enumerate(self.STEP_COUNTS)}
+        if timed:
+            out.update({k: ms[:, i] for i, k in enumerate(self.KERNELS[1:6])})
+        return out
 
     def run_fused(self, seeds_per_block=0):
         """One launch for all layer steps; seeds_per_block 0 = tuned value."""

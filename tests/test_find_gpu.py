@@ -312,3 +312,19 @@ def test_run_timed_equals_run(gpu_ctx):
     assert ms["propagate"] > 0 and ms["clone"] > 0
     for k in a:
         np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+
+
+def test_step_profile(gpu_ctx):
+    """Per-step counters sum to the work totals; timed launches are listed."""
+    ev = synth.gen_cms_event(500, seed=17)
+    fnd = Finder(gpu_ctx, FindConfig(max_cands=M))
+    fnd.upload(ev)
+    fnd.run_timed()
+    prof = fnd.step_profile()
+    w = fnd.work()
+    assert len(prof["finding_seeds"]) == fnd.cfg.max_steps
+    assert int(prof["act_barrel"].sum() + prof["act_endcap"].sum()) == w["active_cands"]
+    assert int(prof["pairs_barrel"].sum() + prof["pairs_endcap"].sum()) == w["hit_pairs"]
+    assert int(prof["upd_barrel"].sum() + prof["upd_endcap"].sum()) == w["updates"]
+    assert int(prof["finding_seeds"].sum()) == w["seed_steps"]
+    assert prof["clone"].shape == (fnd.cfg.max_steps,) and float(prof["propagate"].sum()) > 0
