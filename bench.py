@@ -85,6 +85,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-fit", action="store_true")
     p.add_argument("--no-pu", action="store_true")
+    p.add_argument("--step-profile", action="store_true",
+                   help="print per layer-plan step work and launch times to stderr")
     return p.parse_args()
 
 
@@ -184,6 +186,16 @@ def fp32_peak(ctx):
     return v.value if rc == 0 else None
 
 
+def print_step_profile(prof):
+    """Per layer-plan step: work counters and launch times (us), to stderr."""
+    keys = list(prof)
+    print("step " + " ".join(k[:12].rjust(12) for k in keys), file=sys.stderr)
+    for i in range(len(prof[keys[0]])):
+        cells = [(f"{int(prof[k][i]):12d}" if prof[k].dtype.kind == "i" else
+                  f"{1000 * float(prof[k][i]):12.1f}") for k in keys]
+        print(f"{i + 1:4d} " + " ".join(cells), file=sys.stderr)
+
+
 def timed_events(stream, fn, steps):
     """Per-step CUDA-event timing on `stream`; returns per-step ms."""
     import torch
@@ -274,6 +286,8 @@ def run_ours(args):
     per_launch_ms = kt[dom] / work["steps"]
     dom_tf = units * f_unit / (kt[dom] * 1e-3) / 1e12
     dom_gbs = units * b_unit / (kt[dom] * 1e-3) / 1e9
+    if args.step_profile and rank == 0:
+        print_step_profile(finder.step_profile())
 
     # End to end through the C ABI from host buffers: upload (host hit-index
     # build + seed partition + H2D), run, download (export + D2H).
