@@ -201,6 +201,36 @@ typedef struct {
 
 int mkfg_finder_setup(mkfg_context* ctx, const mkfg_find_config* cfg);
 
+/* Seed cleaning (StdSeq::clean_cms_seedtracks_iter, mkFit/MkStdSeqs.cc:115-311):
+ * the iteration's window parameters (IterationParams c_ptthr_hpt, c_dzmax_*,
+ * c_drmax_*, mkFit/IterationConfig.h:107-116; set_seed_cleaning_params order)
+ * and the beam spot (BeamSpot x, y, Hit.h:340). */
+typedef struct {
+  float pt_thr;
+  float dzmax_bh, drmax_bh;
+  float dzmax_bl, drmax_bl;
+  float dzmax_eh, drmax_eh;
+  float dzmax_el, drmax_el;
+  float beam_x, beam_y;
+} mkfg_seed_clean_params;
+
+/* Cleans the seeds of n_events events (event e's seeds at
+ * [event_seed_begin[e], event_seed_begin[e+1]), the reference's seed order
+ * within an event). Host pointers. seed_par [6][n] (CCS), seed_chg [n],
+ * seed_nhits [n] with hits [n][in_hits] (layer, index). keep[n]: 1 for the
+ * seeds the reference keeps; out_nhits / out_hit_layer / out_hit_index
+ * ([n][max_hits], max_hits >= 15): the kept seeds' hit lists after the merge
+ * of the dropped seeds' hits (sorted by layer where hits were added).
+ * MKFG_ERR_OVERFLOW if more than 4096 overlapping pairs fall in one event.
+ * Replaces the call in MkBuilder's run_OneIteration (mkFit/buildtestMPlex.cc:
+ * 660-665). */
+int mkfg_clean_seeds(mkfg_context* ctx, const mkfg_seed_clean_params* p, int32_t n_events,
+                     const int32_t* event_seed_begin, const float* seed_par,
+                     const int32_t* seed_chg, const int32_t* seed_nhits,
+                     const int32_t* seed_hit_layer, const int32_t* seed_hit_index,
+                     int32_t in_hits, int32_t max_hits, int32_t* keep, int32_t* out_nhits,
+                     int32_t* out_hit_layer, int32_t* out_hit_index);
+
 /* One event: hits (layer l at [layer_begin[l], layer_begin[l+1])) and seeds.
  * Host pointers. cpcm: strip charge per cm as given to Hit::setupAsStrip,
  * negative for pixel hits (Hit.h:285-300); detid: 12-bit module id in the

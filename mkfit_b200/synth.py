@@ -558,3 +558,63 @@ def batch_event_sizes(n_events, mean, lo, hi, seed):
 def gen_cms_event_args(args):
     """Picklable entry for process pools: gen_cms_event(**args)."""
     return gen_cms_event(**args)
+
+
+def with_duplicate_seeds(ev, frac=0.25, seed=7, chain_frac=0.3):
+    """Seeds of `ev` plus near-duplicates, as a seeding step with overlapping
+    seeds gives them: a copy of a seed with small shifts of its position and
+    direction (tens of microns, ~1e-3 rad), 1/pT within a few percent and a
+    different third hit (the next hit of the same layer); some duplicates are
+    duplicated again (chains), and all are inserted at random places in the
+    seed order. Returns the seed arrays (par, err, chg, nhits, hit_layer,
+    hit_index) and `src`, the original seed each entry derives from."""
+    rng = np.random.default_rng(seed)
+    ns = ev.n_seeds
+    par = [ev.seed_par[:, i].astype(np.float64) for i in range(ns)]
+    err = [ev.seed_err[:, i] for i in range(ns)]
+    chg = list(ev.seed_chg)
+    nh = list(ev.seed_nhits)
+    hl = [ev.seed_hit_layer[i].copy() for i in range(ns)]
+    hi = [ev.seed_hit_index[i].copy() for i in range(ns)]
+    src = list(range(ns))
+    lb = ev.layer_begin
+
+    def dup(i):
+        p = par[i].copy()
+        p[0:3] += rng.normal(0.0, 0.003, 3)
+        p[3] *= 1.0 + rng.normal(0.0, 0.02)
+        p[4] += rng.normal(0.0, 0.001)
+        p[5] += rng.normal(0.0, 0.001)
+        h_l, h_i = hl[i].copy(), hi[i].copy()
+        k = nh[i] - 1
+        if k >= 0 and rng.random() < 0.7:
+            n_lay = lb[h_l[k] + 1] - lb[h_l[k]]
+            h_i[k] = (h_i[k] + 1) % max(n_lay, 1)
+        par.append(p)
+        err.append(err[i])
+        chg.append(chg[i])
+        nh.append(nh[i])
+        hl.append(h_l)
+        hi.append(h_i)
+        src.append(src[i])
+        return len(par) - 1
+
+    picks = rng.choice(ns, size=int(frac * ns), replace=False) if ns else []
+    for i in picks:
+        j = dup(int(i))
+        if rng.random() < chain_frac:
+            dup(j)
+    order = rng.permutation(len(par))
+    sel = lambda a: [a[k] for k in order]  # noqa: E731
+    if not par:
+        w = ev.seed_hit_layer.shape[1] if ev.seed_hit_layer.ndim == 2 else 4
+        z = lambda *shape: np.zeros(shape, np.int32)  # noqa: E731
+        return dict(par=np.zeros((6, 0), np.float32), err=np.zeros((21, 0), np.float32),
+                    chg=z(0), nhits=z(0), hit_layer=z(0, w), hit_index=z(0, w), src=z(0))
+    return dict(
+        par=np.ascontiguousarray(np.array(sel(par)).T, np.float32),
+        err=np.ascontiguousarray(np.array(sel(err)).T, np.float32),
+        chg=np.array(sel(chg), np.int32), nhits=np.array(sel(nh), np.int32),
+        hit_layer=np.ascontiguousarray(np.array(sel(hl)), np.int32),
+        hit_index=np.ascontiguousarray(np.array(sel(hi)), np.int32),
+        src=np.array(sel(src), np.int32))

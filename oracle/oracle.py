@@ -446,3 +446,162 @@ def ref_find_batch(reflib, events, max_cands=6, chi2_cut=30.0, zero_c2=True, rep
         raise RuntimeError(f"ref_find_batch failed rc={rc}")
     o["seconds"] = secs.value
     return o
+
+
+def ref_clean_seeds(reflib, seeds, params, beam=(0.0, 0.0), max_hits=16):
+    """Seed cleaning of one event's seeds by the reference
+    (StdSeq::clean_cms_seedtracks_iter via oracle/ref_driver.cc
+    ref_clean_seeds). seeds: dict par [6][n], err [21][n], chg, nhits,
+    hit_layer / hit_index [n][k]; params in set_seed_cleaning_params order.
+    Returns (keep, nhits, hit_layer, hit_index); rows of dropped seeds 0."""
+    lib = reflib.lib
+    lib.ref_clean_seeds.restype = ctypes.c_int
+    lib.ref_clean_seeds.argtypes = [ctypes.c_int, _f32p, _f32p, _i32p, _i32p, _i32p, _i32p,
+                                    ctypes.c_int, _f32p, ctypes.c_float, ctypes.c_float,
+                                    ctypes.c_int, _i32p, _i32p, _i32p, _i32p]
+    n = int(seeds["chg"].shape[0])
+    c = np.ascontiguousarray
+    hl = c(seeds["hit_layer"], np.int32)
+    keep = np.zeros(n, np.int32)
+    onh = np.zeros(n, np.int32)
+    ohl = np.zeros((n, max_hits), np.int32)
+    ohx = np.zeros((n, max_hits), np.int32)
+    lib.ref_clean_seeds(n, c(seeds["par"], np.float32), c(seeds["err"], np.float32),
+                        c(seeds["chg"], np.int32), c(seeds["nhits"], np.int32), hl,
+                        c(seeds["hit_index"], np.int32), hl.shape[1],
+                        np.ascontiguousarray(params, np.float32), float(beam[0]), float(beam[1]),
+                        max_hits, keep, onh, ohl, ohx)
+    return keep, onh, ohl, ohx
+
+
+# dz2*dzi + dr2*dri < 1 (MkStdSeqs.cc:247-254) as GCC contracts it: the
+# first product fused with the second as addend.
+WINDOW_SUM = lambda dz2, dzi, dr2, dri: _fma32(dz2, dzi, np.float32(dr2 * dri))  # noqa: E731
+
+
+def _fma32(a, b, c):
+    """Single-rounding a*b + c of float32 values (the float64 product is
+    exact; the sum is rounded twice, which differs from one rounding only in
+    rare ties)."""
+    return np.float32(np.float64(a) * np.float64(b) + np.float64(c))
+
+
+_LIBM = None
+
+
+def _libm_f32(name, v):
+    """The host C library's float function `name` (sinf, cosf, tanf, logf)
+    applied elementwise: the functions the reference's float calls reach."""
+    global _LIBM
+    if _LIBM is None:
+        _LIBM = ctypes.CDLL("libm.so.6")
+        for fn in ("sinf", "cosf", "tanf", "logf"):
+            getattr(_LIBM, fn).restype = ctypes.c_float
+            getattr(_LIBM, fn).argtypes = [ctypes.c_float]
+    f = getattr(_LIBM, name)
+    return np.array([f(float(x)) for x in np.asarray(v, np.float32).ravel()], np.float32)
+
+
+def clean_seed_features(seeds, beam=(0.0, 0.0)):
+    """Per-seed quantities of the seed cleaning (MkStdSeqs.cc:166-180) in
+    float32 with the host C library's float functions: pt, eta, pos2,
+    ctheta, invptq, d0 (Track::d0BeamSpot, Track.cc:195-210, with x - k*py
+    and y + k*px contracted into FMAs as the reference build does) and the
+    helix radius |k pt| that d0 is a difference against."""
+    f = np.float32
+    par = np.asarray(seeds["par"], np.float32)
+    chg = np.asarray(seeds["chg"], np.int32)
+    n = chg.shape[0]
+    x, y = par[0], par[1]
+    ipt, phi, theta = par[3], par[4], par[5]
+    pt = np.abs(f(1.0) / ipt)
+    eta = f(-1.0) * _libm_f32("logf", _libm_f32("tanf", theta / f(2.0)))
+    pos2 = (x.astype(np.float64) ** 2 + y.astype(np.float64) ** 2).astype(np.float32)
+    ctheta = f(1.0) / _libm_f32("tanf", theta)
+    invptq = chg.astype(np.float32) * ipt
+    sb = f(0.299792458) * f(3.8112)
+    k = np.where(chg < 0, f(100.0) / sb, f(-100.0) / sb).astype(np.float32)
+    px, py = pt * _libm_f32("cosf", phi), pt * _libm_f32("sinf", phi)
+    xc = np.array([_fma32(-k[i], py[i], x[i]) for i in range(n)], np.float32)
+    yc = np.array([_fma32(k[i], px[i], y[i]) for i in range(n)], np.float32)
+    radius = np.abs(k * pt)
+    d0 = (np.hypot((xc - f(beam[0])).astype(np.float64), (yc - f(beam[1])).astype(np.float64))
+          .astype(np.float32) - radius)
+    return dict(pt=pt, eta=eta, pos2=pos2, ctheta=ctheta, invptq=invptq, d0=d0, radius=radius)
+
+
+def restate_clean_seeds(seeds, params, beam=(0.0, 0.0), max_hits=16):
+    """Pure-Python restatement of StdSeq::clean_cms_seedtracks_iter
+    (mkFit/MkStdSeqs.cc:115-311) in float32 arithmetic, for small n: the
+    per-seed quantities (:166-180, Track::d0BeamSpot Track.cc:195-210), the
+    ordered pair loop with its skip of already-dropped seeds (:182-186), the
+    window (:196-256), the drop of the larger-d0 seed (:258-270) and the hit
+    merge with its 15-hit cap and layer sort (:271-305)."""
+    f = np.float32
+    par = np.asarray(seeds["par"], np.float32)
+    chg = np.asarray(seeds["chg"], np.int32)
+    n = chg.shape[0]
+    ptthr, dz_bh, dr_bh, dz_bl, dr_bl, dz_eh, dr_eh, dz_el, dr_el = [f(v) for v in params]
+    inv2 = lambda v: f(1.0) / (v * v)  # noqa: E731
+    dzi = dict(bh=inv2(dz_bh), bl=inv2(dz_bl), eh=inv2(dz_eh), el=inv2(dz_el))
+    dri = dict(bh=inv2(dr_bh), bl=inv2(dr_bl), eh=inv2(dr_eh), el=inv2(dr_el))
+    F = clean_seed_features(seeds, beam)
+    x, y, z, phi = par[0], par[1], par[2], par[4]
+    pt, eta, pos2, ctheta, invptq, d0 = (F[k] for k in ("pt", "eta", "pos2", "ctheta", "invptq",
+                                                          "d0"))
+    hits = [[(int(seeds["hit_index"][i][j]), int(seeds["hit_layer"][i][j]))
+             for j in range(int(seeds["nhits"][i]))] for i in range(n)]
+    write = [True] * n
+    inv_r1 = f(1.0) / f(87.6)
+    for ts in range(n):
+        if not write[ts]:
+            continue
+        added = 0
+        for tss in range(ts + 1, n):
+            if chg[tss] != chg[ts]:
+                continue
+            if abs(pt[tss] - pt[ts]) > f(0.25) * pt[ts]:
+                continue
+            deta2 = f((eta[ts] - eta[tss]) ** 2)
+            sign = f(-0.5) if pos2[tss] > pos2[ts] else f(0.5)
+            dx, dy = f(x[ts] - x[tss]), f(y[ts] - y[tss])
+            dxy = f(float(sign) * np.sqrt(float(dx) ** 2 + float(dy) ** 2))
+            t = dxy * inv_r1
+            # Contracted as the reference build does: phi -/+ t*invptq,
+            # deta2 + dphi^2, (z1 - z2) - dxy*(ct1 + ct2), and the window sum.
+            nphi1 = _fma32(-t, invptq[ts], phi[ts])
+            nphi2 = _fma32(t, invptq[tss], phi[tss])
+            dphi = abs(f(nphi1 - nphi2))
+            if dphi > f(np.pi):
+                dphi = f(2 * np.pi) - dphi
+            dr2 = _fma32(dphi, dphi, deta2)
+            dz = _fma32(-dxy, f(ctheta[ts] + ctheta[tss]), f(z[ts] - z[tss]))
+            dz2 = dz * dz
+            key = ("b" if abs(eta[ts]) < f(0.9) else "e") + ("h" if pt[ts] > ptthr else "l")
+            if not WINDOW_SUM(dz2, dzi[key], dr2, dri[key]) < f(1.0):
+                continue
+            if d0[tss] > d0[ts]:
+                write[tss] = False
+                i1, i2 = ts, tss
+            else:
+                write[ts] = False
+                i1, i2 = tss, ts
+            if len(hits[i1]) < 15:
+                for h in hits[i2]:
+                    if h[0] >= 0 and h not in hits[i1]:
+                        hits[i1].append(h)
+                        added += 1
+                        if len(hits[i1]) >= 15:
+                            break
+            if added > 0:
+                hits[i1].sort(key=lambda h: h[1])  # stable, by layer
+    keep = np.array(write, np.int32)
+    onh = np.zeros(n, np.int32)
+    ohl = np.zeros((n, max_hits), np.int32)
+    ohx = np.zeros((n, max_hits), np.int32)
+    for i in range(n):
+        if keep[i]:
+            onh[i] = len(hits[i])
+            for j, (hx, hly) in enumerate(hits[i][:max_hits]):
+                ohl[i, j], ohx[i, j] = hly, hx
+    return keep, onh, ohl, ohx

@@ -585,3 +585,45 @@ extern "C" int ref_find_batch(int n_ev, const int* hit_off, const int* seed_off,
   }
   return 0;
 }
+
+// Seed cleaning by the reference (StdSeq::clean_cms_seedtracks_iter,
+// mkFit/MkStdSeqs.cc:115-311) of one event's seeds: params = {pt_thr,
+// dzmax_bh, drmax_bh, dzmax_bl, drmax_bl, dzmax_eh, drmax_eh, dzmax_el,
+// drmax_el} in IterationConfig::set_seed_cleaning_params order. keep[ns]
+// marks the surviving seeds; their hit lists go to out_* ([ns][max_hits]).
+// Returns the number kept.
+extern "C" int ref_clean_seeds(int ns, const float* spar, const float* serr, const int* schg,
+                               const int* seed_nhits, const int* seed_hit_layer,
+                               const int* seed_hit_index, int in_hits, const float* params,
+                               float beam_x, float beam_y, int max_hits, int* keep,
+                               int* out_nhits, int* out_hit_layer, int* out_hit_index) {
+  IterationConfig itconf;
+  itconf.set_seed_cleaning_params(params[0], params[1], params[2], params[3], params[4],
+                                  params[5], params[6], params[7], params[8]);
+  BeamSpot bs;
+  bs.x = beam_x;
+  bs.y = beam_y;
+  TrackVec seeds;
+  seeds.reserve(ns);
+  for (int s = 0; s < ns; ++s) {
+    Track t = make_track(s, ns, spar, serr, schg);
+    t.setLabel(s);
+    for (int k = 0; k < seed_nhits[s]; ++k)
+      t.addHitIdx(seed_hit_index[s * in_hits + k], seed_hit_layer[s * in_hits + k], 0.f);
+    seeds.push_back(t);
+  }
+  StdSeq::clean_cms_seedtracks_iter(&seeds, itconf, bs);
+  for (int s = 0; s < ns; ++s) keep[s] = 0;
+  for (const Track& t : seeds) {
+    const int s = t.label();
+    keep[s] = 1;
+    const int n = std::min(t.nTotalHits(), max_hits);
+    out_nhits[s] = n;
+    for (int k = 0; k < n; ++k) {
+      const HitOnTrack h = t.getHitOnTrack(k);
+      out_hit_layer[s * max_hits + k] = h.layer;
+      out_hit_index[s * max_hits + k] = h.index;
+    }
+  }
+  return (int)seeds.size();
+}
