@@ -201,6 +201,89 @@ typedef struct {
 
 int mkfg_finder_setup(mkfg_context* ctx, const mkfg_find_config* cfg);
 
+/* ---- memoryFile event files (DataFile / Event::write_out / read_in,
+ * Event.cc:123-444; header Event.h:74-127) ---------------------------------
+ * Host-only: no context or device needed. The reader indexes the event
+ * records at open and reads any event by number into this library's SoA
+ * layout; the writer produces files the reference reads (format version 6,
+ * x86-64 struct layout: Track 160 B, Hit 44 B, HitOnTrack 4 B). */
+#define MKFG_MF_SIM_TRACK_STATES 0x1 /* DataFile::ES_SimTrackStates */
+#define MKFG_MF_SEEDS 0x2            /* ES_Seeds */
+#define MKFG_MF_CMSSW_TRACKS 0x4     /* ES_CmsswTracks */
+#define MKFG_MF_HIT_ITER_MASKS 0x8   /* ES_HitIterMasks */
+#define MKFG_MF_BEAM_SPOT 0x10       /* ES_BeamSpot */
+
+typedef struct {
+  int32_t format_version;
+  int32_t n_layers;
+  int32_t n_events; /* complete event records found */
+  int32_t extra_sections;
+} mkfg_mf_header;
+
+/* A track vector (Track fields; hits of track i at [hits_begin[i],
+ * hits_begin[i+1]) of hit_index / hit_layer, HitOnTrack order). On write,
+ * null valid / chi2 / score / status / label / nfound take the defaults
+ * (1, 0, 0, 0, -1, counted from the hits as Track::addHitIdx does). */
+typedef struct {
+  int32_t n;
+  const float* par;        /* [6][n] */
+  const float* err;        /* [21][n] packed symmetric */
+  const int32_t* charge;
+  const uint8_t* valid;
+  const float* chi2;
+  const float* score;
+  const uint32_t* status;  /* Track::Status raw bits */
+  const int32_t* label;
+  const int32_t* nfound;
+  const int32_t* hits_begin; /* [n+1] */
+  const int32_t* hit_index;
+  const int32_t* hit_layer;
+} mkfg_mf_tracks;
+
+/* One event. Hits of layer l at [layer_begin[l], layer_begin[l+1]).
+ * hit_packed: Hit::PackedData raw bits (detid 12 | charge-per-cm code 8 |
+ * span rows 3 | span cols 3). mc_info: [n_mc][4] MCHitInfo (track, layer,
+ * ith layer hit, mcHitID). beam_spot: 8 floats (x, y, z, sigmaZ,
+ * beamWidthX, beamWidthY, dxdz, dydz); null on write = BeamSpot defaults. */
+typedef struct {
+  int32_t n_layers;
+  const int32_t* layer_begin;
+  const float* hit_pos;      /* [3][n_hits] */
+  const float* hit_err;      /* [6][n_hits] */
+  const int32_t* hit_mcid;   /* Hit::mcHitID */
+  const uint32_t* hit_packed;
+  const uint64_t* hit_masks; /* [n_hits] iteration masks, or null */
+  int32_t n_mc;
+  const int32_t* mc_info;
+  mkfg_mf_tracks sim;
+  mkfg_mf_tracks seeds;
+  mkfg_mf_tracks cmssw;
+  int32_t n_sim_states;
+  const float* sim_state_par;  /* [6][n_sim_states] */
+  const float* sim_state_err;  /* [21][n_sim_states] */
+  const int32_t* sim_state_charge;
+  const float* beam_spot;
+} mkfg_mf_event;
+
+typedef struct mkfg_mf_reader mkfg_mf_reader;
+/* DataFile::OpenRead: checks magic, version (4..6), struct sizes and layer
+ * count, then indexes the event records. On a truncated file the reader is
+ * still returned (with the complete events) together with an error. */
+int mkfg_mf_open(const char* path, mkfg_mf_reader** out, mkfg_mf_header* hdr);
+/* Event::read_in of event number `event`; out's arrays belong to the
+ * reader and stay valid until its next read or close. */
+int mkfg_mf_read_event(mkfg_mf_reader* r, int32_t event, mkfg_mf_event* out);
+void mkfg_mf_close(mkfg_mf_reader* r);
+/* DataFile::OpenWrite + Event::write_out of every event + CloseWrite. */
+int mkfg_mf_write(const char* path, int32_t n_layers, int32_t extra_sections, int32_t n_events,
+                  const mkfg_mf_event* events);
+/* The finder's per-hit detid / charge-per-cm and [n_seeds][max_seed_hits]
+ * seed hits (mkfg_event fields) from a read event; any output may be null.
+ * MKFG_ERR_OVERFLOW if a seed has more than max_seed_hits hits. */
+int mkfg_mf_finder_event(const mkfg_mf_event* ev, int32_t* detid, int32_t* cpcm,
+                         int32_t max_seed_hits, int32_t* seed_nhits, int32_t* seed_hit_layer,
+                         int32_t* seed_hit_index);
+
 /* Seed cleaning (StdSeq::clean_cms_seedtracks_iter, mkFit/MkStdSeqs.cc:115-311):
  * the iteration's window parameters (IterationParams c_ptthr_hpt, c_dzmax_*,
  * c_drmax_*, mkFit/IterationConfig.h:107-116; set_seed_cleaning_params order)

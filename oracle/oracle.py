@@ -605,3 +605,112 @@ def restate_clean_seeds(seeds, params, beam=(0.0, 0.0), max_hits=16):
             for j, (hx, hly) in enumerate(hits[i][:max_hits]):
                 ohl[i, j], ohx[i, j] = hly, hx
     return keep, onh, ohl, ohx
+
+
+def _mf_tracks_args(t):
+    t = t or {}
+    n = len(t.get("charge", ()))
+    c = np.ascontiguousarray
+    z = lambda dt, *s: np.zeros(s, dt)  # noqa: E731
+    return [n, c(t.get("par", z(np.float32, 6, n)), np.float32).ravel(),
+            c(t.get("err", z(np.float32, 21, n)), np.float32).ravel(),
+            c(t.get("charge", z(np.int32, n)), np.int32),
+            c(t.get("chi2", z(np.float32, n)), np.float32),
+            c(t.get("score", z(np.float32, n)), np.float32),
+            c(t.get("status", z(np.uint32, n)), np.uint32),
+            c(t.get("label", np.full(n, -1)), np.int32),
+            c(t.get("hits_begin", z(np.int32, n + 1)), np.int32),
+            c(t.get("hit_index", z(np.int32, 1)), np.int32),
+            c(t.get("hit_layer", z(np.int32, 1)), np.int32)]
+
+
+def ref_mf_write(reflib, path, events, sections):
+    """Writes events (memory_file event dicts, 72 layers) with the
+    reference's DataFile::OpenWrite + Event::write_out + CloseWrite."""
+    lib = reflib.lib
+    vp = ctypes.c_void_p
+    lib.ref_mf_write_begin.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
+    lib.ref_mf_write_event.argtypes = [ctypes.c_int] + [vp] * 6 + [ctypes.c_int, vp] + \
+        ([ctypes.c_int] + [vp] * 10) * 3 + [vp, ctypes.c_int, vp, vp, vp]
+    keep = []
+
+    def p(a):
+        if a is None:
+            return None
+        keep.append(a)
+        return a.ctypes.data
+
+    if lib.ref_mf_write_begin(str(path).encode(), len(events), sections) != 0:
+        raise RuntimeError("ref_mf_write_begin failed")
+    c = np.ascontiguousarray
+    for ev in events:
+        mc = c(ev.get("mc_info", np.zeros((0, 4))), np.int32)
+        args = [int(ev["n_layers"]), p(c(ev["layer_begin"], np.int32)),
+                p(c(ev["hit_pos"], np.float32)), p(c(ev["hit_err"], np.float32)),
+                p(c(ev["hit_mcid"], np.int32)), p(c(ev["hit_packed"], np.uint32)),
+                p(None if ev.get("hit_masks") is None else c(ev["hit_masks"], np.uint64)),
+                mc.shape[0], p(mc)]
+        for key in ("sim", "seeds", "cmssw"):
+            ta = _mf_tracks_args(ev.get(key))
+            args += [ta[0]] + [p(a) for a in ta[1:]]
+        st = ev.get("sim_states") or {}
+        ns = len(st.get("charge", ()))
+        bs = ev.get("beam_spot")
+        args += [p(None if bs is None else c(bs, np.float32)), ns,
+                 p(c(st["par"], np.float32)) if ns else None,
+                 p(c(st["err"], np.float32)) if ns else None,
+                 p(c(st["charge"], np.int32)) if ns else None]
+        lib.ref_mf_write_event(*args)
+    return lib.ref_mf_write_end()
+
+
+def ref_mf_read(reflib, path, which, hit_cap=1 << 20, trk_cap=1 << 15, hcap=1 << 18):
+    """Event `which` of a memoryFile as the reference's Event::read_in sees
+    it, as a memory_file-style event dict."""
+    lib = reflib.lib
+    vp = ctypes.c_void_p
+    lib.ref_mf_read.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                ctypes.c_int] + [vp] * 23
+    counts = np.zeros(8, np.int32)
+    lb = np.zeros(129, np.int32)
+    pos = np.zeros((3, hit_cap), np.float32)
+    herr = np.zeros((6, hit_cap), np.float32)
+    mcid = np.zeros(hit_cap, np.int32)
+    packed = np.zeros(hit_cap, np.uint32)
+    masks = np.zeros(hit_cap, np.uint64)
+    mc = np.zeros((hit_cap, 4), np.int32)
+    T = 3
+    tpar = np.zeros((T, 6, trk_cap), np.float32)
+    terr = np.zeros((T, 21, trk_cap), np.float32)
+    ti = {k: np.zeros((T, trk_cap), dt) for k, dt in (("charge", np.int32), ("chi2", np.float32),
+                                                       ("score", np.float32), ("status", np.uint32),
+                                                       ("label", np.int32), ("nfound", np.int32))}
+    thb = np.zeros((T, trk_cap + 1), np.int32)
+    thi = np.zeros((T, hcap), np.int32)
+    thl = np.zeros((T, hcap), np.int32)
+    beam = np.zeros(8, np.float32)
+    stp = np.zeros((6, trk_cap), np.float32)
+    ste = np.zeros((21, trk_cap), np.float32)
+    stc = np.zeros(trk_cap, np.int32)
+    d = lambda a: a.ctypes.data  # noqa: E731
+    rc = lib.ref_mf_read(str(path).encode(), which, hit_cap, trk_cap, hcap, d(counts), d(lb),
+                         d(pos), d(herr), d(mcid), d(packed), d(masks), d(mc), d(tpar), d(terr),
+                         d(ti["charge"]), d(ti["chi2"]), d(ti["score"]), d(ti["status"]),
+                         d(ti["label"]), d(ti["nfound"]), d(thb), d(thi), d(thl), d(beam),
+                         d(stp), d(ste), d(stc))
+    if rc != 0:
+        raise RuntimeError("ref_mf_read: capacity exceeded")
+    nl, nh, nm = counts[0], counts[1], counts[2]
+    out = dict(n_layers=int(nl), layer_begin=lb[:nl + 1].copy(), hit_pos=pos[:, :nh].copy(),
+               hit_err=herr[:, :nh].copy(), hit_mcid=mcid[:nh].copy(), hit_packed=packed[:nh].copy(),
+               hit_masks=masks[:nh].copy(), mc_info=mc[:nm].copy(), beam_spot=beam.copy())
+    for k, key in enumerate(("sim", "seeds", "cmssw")):
+        n = counts[3 + k]
+        nh_t = thb[k, n]
+        out[key] = dict(par=tpar[k, :, :n].copy(), err=terr[k, :, :n].copy(),
+                        hits_begin=thb[k, :n + 1].copy(), hit_index=thi[k, :nh_t].copy(),
+                        hit_layer=thl[k, :nh_t].copy(),
+                        **{f: ti[f][k, :n].copy() for f in ti})
+    ns = counts[6]
+    out["sim_states"] = dict(par=stp[:, :ns].copy(), err=ste[:, :ns].copy(), charge=stc[:ns].copy())
+    return out

@@ -16,6 +16,7 @@
 //              (export of the best / all comb candidates)
 //   geometry : Geoms/CMS-2017.cc:717-859 (plugin creator, called directly)
 #include "Config.h"
+#include "Event.h"
 #include "Hit.h"
 #include "MaterialEffects.h"
 #include "Track.h"
@@ -626,4 +627,199 @@ extern "C" int ref_clean_seeds(int ns, const float* spar, const float* serr, con
     }
   }
   return (int)seeds.size();
+}
+
+// ---- memoryFile round trips through the reference's own DataFile / Event
+// (Event.cc:123-444, 866-1000). Track vectors are passed as flat arrays:
+// par [6][n], err [21][n], charge, chi2, score, status, label, hits_begin
+// [n+1], hit_index, hit_layer.
+namespace {
+
+TrackVec tracks_from(int n, const float* par, const float* err, const int* chg, const float* chi2,
+                     const float* score, const unsigned* status, const int* label,
+                     const int* hits_begin, const int* hit_index, const int* hit_layer) {
+  TrackVec tv;
+  tv.reserve(n);
+  for (int i = 0; i < n; ++i) {
+    Track t = make_track(i, n, par, err, chg);
+    for (int h = hits_begin[i]; h < hits_begin[i + 1]; ++h) t.addHitIdx(hit_index[h], hit_layer[h], 0.f);
+    t.setChi2(chi2[i]);
+    t.setScore(score[i]);
+    t.setRawStatus(status[i]);
+    t.setLabel(label[i]);
+    tv.push_back(t);
+  }
+  return tv;
+}
+
+int tracks_to(const TrackVec& tv, int cap, int hcap, float* par, float* err, int* chg, float* chi2,
+              float* score, unsigned* status, int* label, int* nfound, int* hits_begin,
+              int* hit_index, int* hit_layer) {
+  const int n = (int)tv.size();
+  if (n > cap) return -1;
+  hits_begin[0] = 0;
+  for (int i = 0; i < n; ++i) {
+    const Track& t = tv[i];
+    for (int k = 0; k < 6; ++k) par[k * cap + i] = t.parameters()[k];
+    for (int k = 0; k < 21; ++k) err[k * cap + i] = t.errors().Array()[k];
+    chg[i] = t.charge();
+    chi2[i] = t.chi2();
+    score[i] = t.score();
+    status[i] = t.getRawStatus();
+    label[i] = t.label();
+    nfound[i] = t.nFoundHits();
+    const int nh = t.nTotalHits();
+    if (hits_begin[i] + nh > hcap) return -1;
+    for (int h = 0; h < nh; ++h) {
+      hit_index[hits_begin[i] + h] = t.getHitIdx(h);
+      hit_layer[hits_begin[i] + h] = t.getHitLyr(h);
+    }
+    hits_begin[i + 1] = hits_begin[i] + nh;
+  }
+  return n;
+}
+
+DataFile g_wfile;
+int g_written = 0;
+
+}  // namespace
+
+extern "C" int ref_mf_write_begin(const char* path, int n_events, int extra_sections) {
+  ensure_cms2017();
+  g_written = 0;
+  g_wfile.f_header = DataFileHeader();  // takes Config::nTotalLayers as set by the geometry
+  g_wfile.OpenWrite(path, n_events, extra_sections);
+  return g_wfile.f_fp ? 0 : -1;
+}
+
+// One event: hits [3][NH] / [6][NH] with layer_begin[n_layers+1], mcHitID,
+// packed bits; masks [NH] (ignored unless the section is on); mc [n_mc][4];
+// sim, seed and cmssw track vectors; beam spot[8]; sim track states.
+extern "C" int ref_mf_write_event(
+    int n_layers, const int* layer_begin, const float* pos, const float* herr, const int* mcid,
+    const unsigned* packed, const unsigned long long* masks, int n_mc, const int* mc,
+    int ns, const float* s_par, const float* s_err, const int* s_chg, const float* s_chi2,
+    const float* s_score, const unsigned* s_status, const int* s_label, const int* s_hb,
+    const int* s_hi, const int* s_hl, int nd, const float* d_par, const float* d_err,
+    const int* d_chg, const float* d_chi2, const float* d_score, const unsigned* d_status,
+    const int* d_label, const int* d_hb, const int* d_hi, const int* d_hl, int nc,
+    const float* c_par, const float* c_err, const int* c_chg, const float* c_chi2,
+    const float* c_score, const unsigned* c_status, const int* c_label, const int* c_hb,
+    const int* c_hi, const int* c_hl, const float* beam, int n_states, const float* st_par,
+    const float* st_err, const int* st_chg) {
+  Event ev(g_written);
+  const int NH = layer_begin[n_layers];
+  ev.layerHits_.assign(n_layers, HitVec());
+  ev.layerHitMasks_.assign(n_layers, std::vector<uint64_t>());
+  for (int l = 0; l < n_layers; ++l) {
+    for (int h = layer_begin[l]; h < layer_begin[l + 1]; ++h) {
+      // Hit is a plain 44-byte record: fill its bytes as the file holds them.
+      Hit hit;
+      float f[9];
+      for (int k = 0; k < 3; ++k) f[k] = pos[k * NH + h];
+      for (int k = 0; k < 6; ++k) f[3 + k] = herr[k * NH + h];
+      unsigned char* b = reinterpret_cast<unsigned char*>(&hit);
+      std::memcpy(b, f, 36);
+      std::memcpy(b + 36, &mcid[h], 4);
+      std::memcpy(b + 40, &packed[h], 4);
+      ev.layerHits_[l].push_back(hit);
+      ev.layerHitMasks_[l].push_back(masks ? masks[h] : 0ull);
+    }
+  }
+  ev.simHitsInfo_.clear();
+  for (int i = 0; i < n_mc; ++i)
+    ev.simHitsInfo_.push_back(MCHitInfo(mc[4 * i], mc[4 * i + 1], mc[4 * i + 2], mc[4 * i + 3]));
+  ev.simTracks_ = tracks_from(ns, s_par, s_err, s_chg, s_chi2, s_score, s_status, s_label, s_hb, s_hi, s_hl);
+  ev.seedTracks_ = tracks_from(nd, d_par, d_err, d_chg, d_chi2, d_score, d_status, d_label, d_hb, d_hi, d_hl);
+  ev.cmsswTracks_ = tracks_from(nc, c_par, c_err, c_chg, c_chi2, c_score, c_status, c_label, c_hb, c_hi, c_hl);
+  if (beam) std::memcpy(&ev.beamSpot_, beam, sizeof(BeamSpot));
+  ev.simTrackStates_.clear();
+  for (int i = 0; i < n_states; ++i) {
+    TrackState ts;
+    for (int k = 0; k < 6; ++k) ts.parameters[k] = st_par[k * n_states + i];
+    for (int k = 0; k < 21; ++k) ts.errors.Array()[k] = st_err[k * n_states + i];
+    ts.charge = st_chg[i];
+    ev.simTrackStates_.push_back(ts);
+  }
+  ev.write_out(g_wfile);
+  ++g_written;
+  return 0;
+}
+
+extern "C" int ref_mf_write_end() {
+  g_wfile.CloseWrite(g_written);
+  return g_written;
+}
+
+// Reads event `which` of a file with the reference. counts out: n_layers,
+// n_hits, n_mc, n_sim, n_seeds, n_cmssw, n_states. Hit arrays sized by
+// hit_cap, track arrays by trk_cap (hits hcap). Returns 0, or -1 when a
+// capacity is exceeded.
+extern "C" int ref_mf_read(const char* path, int which, int hit_cap, int trk_cap, int hcap,
+                           int* counts, int* layer_begin, float* pos, float* herr, int* mcid,
+                           unsigned* packed, unsigned long long* masks, int* mc, float* tpar,
+                           float* terr, int* tchg, float* tchi2, float* tscore, unsigned* tstatus,
+                           int* tlabel, int* tnfound, int* thb, int* thi, int* thl, float* beam,
+                           float* st_par, float* st_err, int* st_chg) {
+  ensure_cms2017();
+  DataFile df;
+  const auto saved_seed = Config::seedInput;
+  const bool saved_cmssw = Config::readCmsswTracks;
+  Config::seedInput = simSeeds;  // OpenRead exits if cmsswSeeds and no seed section
+  Config::readCmsswTracks = false;
+  df.OpenRead(path, false);
+  if (df.HasSeeds()) Config::seedInput = cmsswSeeds;  // read_in reads seeds only then
+  Config::readCmsswTracks = df.HasCmsswTracks();
+  Event ev(0);
+  df.SkipNEvents(which);
+  ev.read_in(df);
+  Config::seedInput = saved_seed;
+  Config::readCmsswTracks = saved_cmssw;
+  df.Close();
+  const int nl = (int)ev.layerHits_.size();
+  layer_begin[0] = 0;
+  for (int l = 0; l < nl; ++l) layer_begin[l + 1] = layer_begin[l] + (int)ev.layerHits_[l].size();
+  const int NH = layer_begin[nl];
+  if (NH > hit_cap) return -1;
+  for (int l = 0; l < nl; ++l)
+    for (int h = layer_begin[l]; h < layer_begin[l + 1]; ++h) {
+      const Hit& hit = ev.layerHits_[l][h - layer_begin[l]];
+      const unsigned char* b = reinterpret_cast<const unsigned char*>(&hit);
+      float f[9];
+      std::memcpy(f, b, 36);
+      for (int k = 0; k < 3; ++k) pos[k * hit_cap + h] = f[k];
+      for (int k = 0; k < 6; ++k) herr[k * hit_cap + h] = f[3 + k];
+      std::memcpy(&mcid[h], b + 36, 4);
+      std::memcpy(&packed[h], b + 40, 4);
+      masks[h] = ev.layerHitMasks_[l][h - layer_begin[l]];
+    }
+  const int nm = (int)ev.simHitsInfo_.size();
+  for (int i = 0; i < nm && i < hit_cap; ++i) {
+    mc[4 * i] = ev.simHitsInfo_[i].mcTrackID_;
+    mc[4 * i + 1] = ev.simHitsInfo_[i].layer_;
+    mc[4 * i + 2] = ev.simHitsInfo_[i].ithLayerHit_;
+    mc[4 * i + 3] = ev.simHitsInfo_[i].mcHitID_;
+  }
+  counts[0] = nl;
+  counts[1] = NH;
+  counts[2] = nm;
+  const TrackVec* tv[3] = {&ev.simTracks_, &ev.seedTracks_, &ev.cmsswTracks_};
+  for (int k = 0; k < 3; ++k) {
+    const size_t o = (size_t)k * trk_cap, oh = (size_t)k * hcap;
+    const int n = tracks_to(*tv[k], trk_cap, hcap, tpar + 6 * o, terr + 21 * o, tchg + o, tchi2 + o,
+                            tscore + o, tstatus + o, tlabel + o, tnfound + o,
+                            thb + (size_t)k * (trk_cap + 1), thi + oh, thl + oh);
+    if (n < 0) return -1;
+    counts[3 + k] = n;
+  }
+  std::memcpy(beam, &ev.beamSpot_, sizeof(BeamSpot));
+  const int nst = (int)ev.simTrackStates_.size();
+  if (nst > trk_cap) return -1;
+  for (int i = 0; i < nst; ++i) {
+    for (int k = 0; k < 6; ++k) st_par[k * trk_cap + i] = ev.simTrackStates_[i].parameters[k];
+    for (int k = 0; k < 21; ++k) st_err[k * trk_cap + i] = ev.simTrackStates_[i].errors.Array()[k];
+    st_chg[i] = ev.simTrackStates_[i].charge;
+  }
+  counts[6] = nst;
+  return 0;
 }
