@@ -289,8 +289,9 @@ def run_ours(args):
     if args.step_profile and rank == 0:
         print_step_profile(finder.step_profile())
 
-    # End to end through the C ABI from host buffers: upload (host hit-index
-    # build + seed partition + H2D), run, download (export + D2H).
+    # End to end through the C ABI from host buffers: upload (seed partition
+    # and initial candidates on the host, H2D, device hit-index build), run,
+    # download (export + D2H into the caller's arrays, reused across steps).
     e2e = None
     if not args.no_e2e:
         e_steps = max(2, args.steps // 4)
@@ -300,7 +301,7 @@ def run_ours(args):
             t0 = time.perf_counter()
             finder.upload_batch(events)
             finder.run_graph()
-            out = finder.download_best(n_seeds)
+            out = finder.download_best(n_seeds, out)
             ts.append(time.perf_counter() - t0)
         h2d = sum(e.hit_pos.nbytes + e.hit_err.nbytes + e.hit_detid.nbytes + e.hit_cpcm.nbytes +
                   e.seed_par.nbytes + e.seed_err.nbytes + e.seed_chg.nbytes for e in events)
@@ -309,8 +310,9 @@ def run_ours(args):
         e2e = {"value": n_events / t, "unit": "events/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": t * 1e3,
                "entry": "mkfg_find_upload_batch + mkfg_find_run_graph + mkfg_find_download_best "
-                        "(host hit-index build, seed partition, copies, export of the best "
-                        "candidate per seed as MkBuilder::export_best_comb_cands)"}
+                        "(seed partition and initial candidates on the host, copies, device "
+                        "hit-index build, export of the best candidate per seed as "
+                        "MkBuilder::export_best_comb_cands into reused host arrays)"}
 
     fit = None if fit_batch is None else run_fit(ctx, stream, fit_batch, args)
     adjoint = None if adj_ev is None else run_adjoint(ctx, stream, adj_ev, args)

@@ -738,6 +738,7 @@ struct Finder {
   DevBuf bk;  // backward-fit seed groups
   DevBuf sel;  // output selection scratch
   HostBuf hits_h;  // pinned mirror of the hits buffer for the upload
+  HostBuf seeds_h; // pinned staging of the initial candidates for the upload
   HostBuf outb_h;  // pinned mirror of the export buffer for the download
   void drop_graph() {
     if (graph) cudaGraphExecDestroy(graph);
@@ -771,6 +772,7 @@ void finder_release(mkfg_context* ctx) {
   f->sel.release();
   f->hits_h.release();
   f->outb_h.release();
+  f->seeds_h.release();
   f->hits.release();
   f->seeds.release();
   f->cands.release();
@@ -937,8 +939,51 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   const HitsLayout hh = layout(static_cast<char*>(f->hits_h.ptr), false);
   const HitsLayout dh = layout(f->hits.as<char>(), true);
 
-  // Per-event host work (seed order; copies into the pinned mirror), in
-  // parallel.
+  // Initial candidates (CombCandidate::ImportSeed, mkFit/HitStructures.cc:
+  // 483-509), staged in pinned memory by the per-event workers: each
+  // event's seeds in sorted order, one initial candidate per seed, and the
+  // seed's hits as its first hit-on-track nodes (at most 4 per seed).
+  const int SS = std::max(S, 1);
+  struct SeedStage {
+    float* par;    // [6][SS]
+    float* err;    // [21][SS]
+    float* score;
+    int* chg;
+    int* last;
+    int* nfound;
+    int* nmiss;
+    int* ninside;
+    int* ntail;
+    int* label;
+    int* sev;
+    int* region;
+    int* pickup;
+    int* hot_size;
+    int* seed_hot;  // [SS][4]
+  };
+  if ((rc = f->seeds_h.ensure(rounded(4 * (size_t)SS) * (27 + 14 + 4) + 4096))) return rc;
+  SeedStage ss;
+  {
+    char* p = static_cast<char*>(f->seeds_h.ptr);
+    ss.par = carve<float>(p, 6 * (size_t)SS);
+    ss.err = carve<float>(p, 21 * (size_t)SS);
+    ss.score = carve<float>(p, SS);
+    ss.chg = carve<int>(p, SS);
+    ss.last = carve<int>(p, SS);
+    ss.nfound = carve<int>(p, SS);
+    ss.nmiss = carve<int>(p, SS);
+    ss.ninside = carve<int>(p, SS);
+    ss.ntail = carve<int>(p, SS);
+    ss.label = carve<int>(p, SS);
+    ss.sev = carve<int>(p, SS);
+    ss.region = carve<int>(p, SS);
+    ss.pickup = carve<int>(p, SS);
+    ss.hot_size = carve<int>(p, SS);
+    ss.seed_hot = carve<int>(p, 4 * (size_t)SS);
+  }
+
+  // Per-event host work (seed order and initial candidates; hit copies into
+  // the pinned mirror), in parallel.
   std::vector<SeedOrder> orders(n_ev);
   {
     auto work = [&](int e) {
@@ -954,15 +999,86 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
       std::memcpy(hh.detid + o, ev->detid, 4 * (size_t)nh);
       std::memcpy(hh.cpcm + o, ev->cpcm, 4 * (size_t)nh);
       for (int l = 0; l <= L; ++l) hh.lb[(size_t)e * (L + 1) + l] = o + ev->layer_begin[l];
+      const int n = ev->n_seeds;
+      for (int k = 0; k < n; ++k) {
+        const int s = seed_off[e] + k;
+        const int i = orders[e].order[k];
+        ss.label[s] = seed_off[e] + i;
+        ss.sev[s] = e;
+        ss.region[s] = orders[e].region[i];
+        const int nhs = ev->seed_nhits[i];
+        ss.pickup[s] = ev->seed_hit_layer[i * 4 + nhs - 1];
+        for (int c = 0; c < 6; ++c) ss.par[c * (size_t)SS + s] = ev->seed_par[c * n + i];
+        for (int c = 0; c < 21; ++c) ss.err[c * (size_t)SS + s] = ev->seed_err[c * n + i];
+        ss.chg[s] = ev->seed_chg[i];
+        int nf = 0, nm = 0, nin = 0, ntl = 0;
+        for (int h = 0; h < 4; ++h) {
+          if (h >= nhs) {
+            ss.seed_hot[4 * (size_t)s + h] = 0;
+            continue;
+          }
+          const int hi = ev->seed_hit_index[i * 4 + h], hl = ev->seed_hit_layer[i * 4 + h];
+          ss.seed_hot[4 * (size_t)s + h] = (hi & 0xffffff) | (hl << 24);
+          if (hi >= 0 || hi == -9) {
+            ++nf;
+            nin += ntl;
+            ntl = 0;
+          } else {
+            ++nm;
+            if (hi == -1) ++ntl;
+          }
+        }
+        ss.hot_size[s] = nhs;
+        ss.last[s] = nhs - 1;
+        ss.nfound[s] = nf;
+        ss.nmiss[s] = nm;
+        ss.ninside[s] = nin;
+        ss.ntail[s] = ntl;
+        // getScoreCand(cand) with default arguments (mkFit/HitStructures.h:519-531).
+        const float pt = std::abs(1.f / ss.par[3 * (size_t)SS + s]);
+        float bonus = 0.2f * nf + 4.0f, penalty = 8.0f;
+        if (pt < 0.9f) {
+          penalty *= 1.5f;
+          bonus = std::min(bonus * 1.0f, 8.0f);
+        }
+        ss.score[s] = bonus * nf + 0.0f * 0 - penalty * nin - 3.0f * 0 - 0.0f;
+      }
     };
+    // The calling thread issues each event's hit copies as soon as the
+    // event's worker is done, so the transfers overlap the host copies.
+    cudaStream_t st = ctx->stream;
+    std::vector<std::atomic<int>> ready(n_ev);
+    for (auto& r : ready) r.store(0);
     const int nthr = std::max(1, std::min(n_ev, (int)std::thread::hardware_concurrency()));
     std::vector<std::thread> pool;
     std::atomic<int> next(0);
     for (int t = 0; t < nthr; ++t)
       pool.emplace_back([&] {
-        for (int e = next++; e < n_ev; e = next++) work(e);
+        for (int e = next++; e < n_ev; e = next++) {
+          work(e);
+          ready[e].store(1, std::memory_order_release);
+        }
       });
+    char* hbase = static_cast<char*>(f->hits_h.ptr);
+    char* dbase = f->hits.as<char>();
+    cudaError_t ce = cudaSuccess;
+    auto copy_rows = [&](const void* h0, size_t row_stride, int rows, size_t off, size_t bytes) {
+      for (int r = 0; r < rows && ce == cudaSuccess && bytes; ++r) {
+        const char* h = static_cast<const char*>(h0) + r * row_stride + off;
+        ce = cudaMemcpyAsync(dbase + (h - hbase), h, bytes, cudaMemcpyHostToDevice, st);
+      }
+    };
+    for (int e = 0; e < n_ev; ++e) {
+      while (!ready[e].load(std::memory_order_acquire)) std::this_thread::yield();
+      const size_t o = 4 * (size_t)hit_off[e], nb = 4 * (size_t)(hit_off[e + 1] - hit_off[e]);
+      copy_rows(hh.pos, 4 * (size_t)NHs, 3, o, nb);
+      copy_rows(hh.err, 4 * (size_t)NHs, 6, o, nb);
+      copy_rows(hh.detid, 0, 1, o, nb);
+      copy_rows(hh.cpcm, 0, 1, o, nb);
+    }
     for (auto& th : pool) th.join();
+    copy_rows(hh.lb, 0, 1, 0, 4 * n_lb);
+    if (ce != cudaSuccess) return set_error(MKFG_ERR_CUDA, "hit upload: %s", cudaGetErrorString(ce));
   }
 
   cudaStream_t st = ctx->stream;
@@ -971,7 +1087,6 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     MKFG_CUDA_TRY(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st));
     return MKFG_OK;
   };
-  if ((rc = up(f->hits.ptr, f->hits_h.ptr, up_bytes))) return rc;
   {
     LayerHitsArgs A;
     A.pos = dh.pos;
@@ -1002,7 +1117,6 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   f->ev.qphi = dh.qphi;
   f->ev.srank = dh.srank;
   // ---- seeds, candidates, scratch, records, arena
-  const int SS = std::max(S, 1);
   const int SC = SS * kSlots;
   const int max_steps = f->host_cfg.max_steps;
   const int M = f->host_cfg.max_cands;
@@ -1084,92 +1198,37 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   }
   f->ev.n_seeds = S;
 
-  // Initial candidates: each event's seeds in sorted order
-  // (CombCandidate::ImportSeed, mkFit/HitStructures.cc:483-509).
-  // One initial candidate per seed, and the seed's hits as its first
-  // hit-on-track nodes (at most 4 per seed).
-  std::vector<float> par(6 * (size_t)SS, 0.f), err(21 * (size_t)SS, 0.f), score(SS, 0.f);
-  std::vector<int> chg(SS, 0), last(SS, 0), nfound(SS, 0), nmiss(SS, 0), ninside(SS, 0), ntail(SS, 0);
-  std::vector<int> label(SS, 0), sev(SS, 0), region(SS, 0), pickup(SS, 0), state(SS, kDormant),
-      ncand(SS, 1), cur(SS, 0), hot_size(SS, 0);
-  std::vector<int> seed_hot(4 * (size_t)SS, 0);
-  for (int e = 0; e < n_ev; ++e) {
-    const mkfg_event* ev = evs + e;
-    const int n = ev->n_seeds;
-    for (int k = 0; k < n; ++k) {
-      const int s = seed_off[e] + k;
-      const int i = orders[e].order[k];
-      label[s] = seed_off[e] + i;
-      sev[s] = e;
-      region[s] = orders[e].region[i];
-      const int nhs = ev->seed_nhits[i];
-      pickup[s] = ev->seed_hit_layer[i * 4 + nhs - 1];
-      const int slot = s;
-      for (int c = 0; c < 6; ++c) par[c * (size_t)SS + slot] = ev->seed_par[c * n + i];
-      for (int c = 0; c < 21; ++c) err[c * (size_t)SS + slot] = ev->seed_err[c * n + i];
-      chg[slot] = ev->seed_chg[i];
-      int nf = 0, nm = 0, nin = 0, ntl = 0;
-      for (int h = 0; h < nhs; ++h) {
-        const int hi = ev->seed_hit_index[i * 4 + h], hl = ev->seed_hit_layer[i * 4 + h];
-        seed_hot[4 * (size_t)s + h] = (hi & 0xffffff) | (hl << 24);
-        if (hi >= 0 || hi == -9) {
-          ++nf;
-          nin += ntl;
-          ntl = 0;
-        } else {
-          ++nm;
-          if (hi == -1) ++ntl;
-        }
-      }
-      hot_size[s] = nhs;
-      last[slot] = nhs - 1;
-      nfound[slot] = nf;
-      nmiss[slot] = nm;
-      ninside[slot] = nin;
-      ntail[slot] = ntl;
-      // getScoreCand(cand) with default arguments (mkFit/HitStructures.h:519-531).
-      const float pt = std::abs(1.f / par[3 * (size_t)SS + slot]);
-      float bonus = 0.2f * nf + 4.0f, penalty = 8.0f;
-      if (pt < 0.9f) {
-        penalty *= 1.5f;
-        bonus = std::min(bonus * 1.0f, 8.0f);
-      }
-      score[slot] = bonus * nf + 0.0f * 0 - penalty * nin - 3.0f * 0 - 0.0f;
-    }
-  }
   f->drop_graph();
+  // The initial candidates from the pinned staging (the per-run reset sets
+  // the candidate counts, seed states and buffers from them).
   CandSoA& B0 = f->ev.init;
-  if ((rc = up(B0.par, par.data(), 4 * par.size()))) return rc;
-  if ((rc = up(B0.err, err.data(), 4 * err.size()))) return rc;
-  if ((rc = up(B0.chg, chg.data(), 4 * (size_t)SS))) return rc;
+  if ((rc = up(B0.par, ss.par, 4 * 6 * (size_t)SS))) return rc;
+  if ((rc = up(B0.err, ss.err, 4 * 21 * (size_t)SS))) return rc;
+  if ((rc = up(B0.chg, ss.chg, 4 * (size_t)SS))) return rc;
   MKFG_CUDA_TRY(cudaMemsetAsync(B0.chi2, 0, 4 * (size_t)SS, st));
-  if ((rc = up(B0.score, score.data(), 4 * (size_t)SS))) return rc;
-  if ((rc = up(B0.last, last.data(), 4 * (size_t)SS))) return rc;
-  if ((rc = up(B0.nfound, nfound.data(), 4 * (size_t)SS))) return rc;
-  if ((rc = up(B0.nmiss, nmiss.data(), 4 * (size_t)SS))) return rc;
+  if ((rc = up(B0.score, ss.score, 4 * (size_t)SS))) return rc;
+  if ((rc = up(B0.last, ss.last, 4 * (size_t)SS))) return rc;
+  if ((rc = up(B0.nfound, ss.nfound, 4 * (size_t)SS))) return rc;
+  if ((rc = up(B0.nmiss, ss.nmiss, 4 * (size_t)SS))) return rc;
   MKFG_CUDA_TRY(cudaMemsetAsync(B0.nover, 0, 4 * (size_t)SS, st));
-  if ((rc = up(B0.ninside, ninside.data(), 4 * (size_t)SS))) return rc;
-  if ((rc = up(B0.ntail, ntail.data(), 4 * (size_t)SS))) return rc;
-  if ((rc = up(f->ev.seed_label, label.data(), 4 * (size_t)SS))) return rc;
-  if ((rc = up(f->ev.seed_event, sev.data(), 4 * (size_t)SS))) return rc;
-  if ((rc = up(f->ev.region, region.data(), 4 * (size_t)SS))) return rc;
-  if ((rc = up(f->ev.pickup_layer, pickup.data(), 4 * (size_t)SS))) return rc;
-  if ((rc = up(f->ev.state, state.data(), 4 * (size_t)SS))) return rc;
-  if ((rc = up(f->ev.n_cands, ncand.data(), 4 * (size_t)SS))) return rc;
-  if ((rc = up(f->ev.cur, cur.data(), 4 * (size_t)SS))) return rc;
-  if ((rc = up(f->ev.init_hot, hot_size.data(), 4 * (size_t)SS))) return rc;
-  MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.bshort_valid, 0, 4 * (size_t)SS, st));
+  if ((rc = up(B0.ninside, ss.ninside, 4 * (size_t)SS))) return rc;
+  if ((rc = up(B0.ntail, ss.ntail, 4 * (size_t)SS))) return rc;
+  if ((rc = up(f->ev.seed_label, ss.label, 4 * (size_t)SS))) return rc;
+  if ((rc = up(f->ev.seed_event, ss.sev, 4 * (size_t)SS))) return rc;
+  if ((rc = up(f->ev.region, ss.region, 4 * (size_t)SS))) return rc;
+  if ((rc = up(f->ev.pickup_layer, ss.pickup, 4 * (size_t)SS))) return rc;
+  if ((rc = up(f->ev.init_hot, ss.hot_size, 4 * (size_t)SS))) return rc;
   if ((rc = f->seeds.ensure(rounded(16 * (size_t)SS)))) return rc;
-  if ((rc = up(f->seeds.ptr, seed_hot.data(), 4 * seed_hot.size()))) return rc;
+  if ((rc = up(f->seeds.ptr, ss.seed_hot, 16 * (size_t)SS))) return rc;
   if (S > 0) k_seed_nodes<<<(S + 127) / 128, 128, 0, st>>>(f->ev, f->seeds.as<int>());
   MKFG_CUDA_TRY(cudaGetLastError());
   MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.upd, 0, 4 * (size_t)SC, st));
   MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.err_flags, 0, 64, st));
-  // The staging vectors die at return: wait for the copies.
+  // The pinned staging is reused by the next upload: wait for the copies.
   MKFG_CUDA_TRY(cudaStreamSynchronize(st));
   f->n_seeds = S;
   f->n_events = n_ev;
-  f->h_region.assign(region.begin(), region.begin() + S);
+  f->h_region.assign(ss.region, ss.region + S);
   f->h_seed_off = seed_off;
   f->h_hit_off = hit_off;
   f->events_loaded = 1;
@@ -1398,18 +1457,32 @@ static int download(mkfg_context* ctx, Finder* f, mkfg_find_out* out, int n_seed
       {out->ninside, O.ninside, 4 * ns * m},     {out->ntail, O.ntail, 4 * ns * m},
       {out->hit_idx, O.hit_idx, 4 * ns * m * kExportHits},
       {out->hit_lyr, O.hit_lyr, 4 * ns * m * kExportHits}};
-  const int n_fields = (int)(sizeof(fields) / sizeof(fields[0]));
-  auto copy_field = [&](int i) {
-    const Field& fd = fields[i];
-    if (fd.dst && fd.bytes)
-      std::memcpy(fd.dst, hbase + (static_cast<const char*>(fd.dev) - f->outb.as<char>()), fd.bytes);
+  // The fields in chunks of at most 4 MB, spread over the host threads.
+  struct Chunk {
+    char* dst;
+    const char* src;
+    size_t bytes;
   };
-  if (used > (size_t(8) << 20)) {
+  std::vector<Chunk> chunks;
+  constexpr size_t kChunk = size_t(4) << 20;
+  for (const Field& fd : fields) {
+    if (!fd.dst || !fd.bytes) continue;
+    const char* src = hbase + (static_cast<const char*>(fd.dev) - f->outb.as<char>());
+    for (size_t o = 0; o < fd.bytes; o += kChunk)
+      chunks.push_back({static_cast<char*>(fd.dst) + o, src + o, std::min(kChunk, fd.bytes - o)});
+  }
+  const int nthr = std::max(1, std::min((int)chunks.size(), (int)std::thread::hardware_concurrency()));
+  if (used > (size_t(8) << 20) && nthr > 1) {
+    std::atomic<int> next(0);
     std::vector<std::thread> pool;
-    for (int i = 0; i < n_fields; ++i) pool.emplace_back(copy_field, i);
+    for (int t = 0; t < nthr; ++t)
+      pool.emplace_back([&] {
+        for (int i = next++; i < (int)chunks.size(); i = next++)
+          std::memcpy(chunks[i].dst, chunks[i].src, chunks[i].bytes);
+      });
     for (auto& th : pool) th.join();
   } else {
-    for (int i = 0; i < n_fields; ++i) copy_field(i);
+    for (const Chunk& c : chunks) std::memcpy(c.dst, c.src, c.bytes);
   }
   const int flag_bits = *flags;
   if (flag_bits & kErrArena)

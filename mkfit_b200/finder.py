@@ -265,9 +265,10 @@ class Finder:
                                                 srank.ctypes.data))
         return bins, srank
 
-    def download_best(self, n_seeds):
-        """Best candidate per seed only (mkfg_find_download_best)."""
-        o = output_arrays(n_seeds, 1)
+    def download_best(self, n_seeds, out=None):
+        """Best candidate per seed only (mkfg_find_download_best). `out`: the
+        arrays of an earlier call with the same seed count, reused."""
+        o = out if out is not None and len(out["n_cands"]) == n_seeds else output_arrays(n_seeds, 1)
         capi.check(self.lib.mkfg_find_download_best(self.ctx.handle, n_seeds,
                                                     ctypes.byref(out_struct(o))))
         return o
