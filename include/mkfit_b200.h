@@ -413,6 +413,17 @@ int mkfg_find_autotune(mkfg_context* ctx, int32_t* seeds_per_block, float* ms_pe
  * measurements as in the reference. Synchronizes the context stream. */
 int mkfg_find_backward_fit(mkfg_context* ctx, const int32_t* bkfit_last, uint32_t pflags,
                            int32_t group_width);
+/* Backward search after mkfg_find_backward_fit (run_OneIteration with
+ * m_backward_search, mkFit/buildtestMPlex.cc:700-714):
+ * CompactifyHitStorageForBestCand without dropping seed hits + BeginBkwSearch
+ * (mkFit/HitStructures.cc:554-674), FindTracksCloneEngine(IT_BkwSearch)
+ * over each region's plan positions bksearch_pickup[region] .. 0 in reverse
+ * (SteeringParams::set_iterator_limits third argument; -1 = no backward
+ * plan, seeds left alone), then EndBkwSearch (:676-702) on the best
+ * candidate, which mkfg_find_download / _download_best then return with the
+ * hits found inward first. The low-pT looper stop does not apply (it is a
+ * forward-search rule). Synchronizes the context stream. */
+int mkfg_find_backward_search(mkfg_context* ctx, const int32_t* bksearch_pickup);
 /* Output selection of run_OneIteration after a run (and backward fit):
  * every seed's best candidate is dropped if its covariance has a negative
  * diagonal or a non-finite element (StdSeq::qfilter_nan_n_silly with

@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(kBlock) k_activate(EventDev E, const FindConfi
     }
     const int slot = s * kSlots + c;
     const bool active = in_range && layer >= 0 && state == kFinding && c < ncand &&
-                        cand_is_active(E, E.cand[buf], s, slot, layer);
+                        cand_is_active(E, E.cand[buf], s, slot, layer, C.looper_stop != 0);
     const unsigned act = __ballot_sync(0xffffffffu, active) & grp;
     const bool seed_finding = layer >= 0 && state == kFinding && act != 0;
     if (in_range && c == 0) {
@@ -409,9 +409,75 @@ __global__ void k_seed_nodes(EventDev E, const int* __restrict__ seed_hot) {
 __global__ void k_merge(EventDev E, const FindConfigDev* __restrict__ Cp) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= E.n_seeds) return;
+  // A region without a plan (backward search) leaves its seeds as they are.
+  if (Cp->plan_len[E.region[s]] == 0) return;
   const int cur = E.cur[s];
   E.n_cands[s] = merge_seed(E, *Cp, s, E.n_cands[s], cur);
   E.cur[s] = cur ^ 1;
+}
+
+//------------------------------------------------------------------------------
+// Backward search (run_OneIteration with m_backward_search,
+// mkFit/buildtestMPlex.cc:700-714): after the backward fit, every seed's best
+// candidate is searched again through the plan's first layers in reverse.
+// Begin: CombCandidate::CompactifyHitStorageForBestCand (without dropping
+// seed hits) + BeginBkwSearch (mkFit/HitStructures.cc:554-674): one
+// candidate per seed, whose "last" hit-on-track node becomes the first one
+// (the seed's innermost hit, arena node 0), with its inside/tail hole counts
+// saved and reset; the seed turns dormant with that node's layer as pickup.
+// End: EndBkwSearch (:676-702) for the merged best candidate: the nodes added
+// by the search are re-linked to follow the first node, and the forward
+// chain's end and hole counts come back.
+//------------------------------------------------------------------------------
+struct BkSearchSave {
+  int* last;
+  int* ninside;
+  int* ntail;
+};
+
+__global__ void k_bks_begin(EventDev E, const FindConfigDev* __restrict__ Cp, BkSearchSave V) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= E.n_seeds) return;
+  if (Cp->plan_len[E.region[s]] == 0 || E.n_cands[s] == 0) {
+    E.state[s] = kFinished;
+    V.last[s] = -1;
+    return;
+  }
+  const CandSoA& B = E.cand[E.cur[s]];
+  const int slot = s * kSlots;
+  E.n_cands[s] = 1;
+  V.last[s] = B.last[slot];
+  V.ninside[s] = B.ninside[slot];
+  V.ntail[s] = B.ntail[slot];
+  B.last[slot] = 0;
+  B.ninside[slot] = 0;
+  B.ntail[slot] = 0;
+  E.state[s] = kDormant;
+  E.pickup_layer[s] = hot_layer(node_hot_of(E, s, 0));
+  E.bshort_valid[s] = 0;
+}
+
+__global__ void k_bks_end(EventDev E, BkSearchSave V) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= E.n_seeds || V.last[s] < 0) return;
+  const CandSoA& B = E.cand[E.cur[s]];
+  const int slot = s * kSlots;
+  int* prev = E.node_prev + (size_t)s * E.hot_cap;
+  int curr = B.last[slot];
+  if (curr != 0) {
+    int last = -1, p;
+    // Bounded by the arena size (the chain visits each node once).
+    for (int guard = 0; guard < E.hot_cap; ++guard) {
+      p = prev[curr];
+      prev[curr] = last;
+      last = curr;
+      curr = p;
+      if (p == -1) break;
+    }
+  }
+  B.last[slot] = V.last[s];
+  B.ninside[slot] += V.ninside[s];
+  B.ntail[slot] += V.ntail[s];
 }
 
 //------------------------------------------------------------------------------
@@ -736,6 +802,8 @@ struct Finder {
   std::vector<int> h_seed_off;
   std::vector<int> h_hit_off;
   DevBuf bk;  // backward-fit seed groups
+  DevBuf bks;  // backward-search saved counts
+  FindConfigDev* d_cfg_bks = nullptr;  // backward-search plans
   DevBuf sel;  // output selection scratch
   HostBuf hits_h;  // pinned mirror of the hits buffer for the upload
   HostBuf seeds_h; // pinned staging of the initial candidates for the upload
@@ -767,6 +835,8 @@ void finder_release(mkfg_context* ctx) {
   if (!ctx || !ctx->finder) return;
   Finder* f = static_cast<Finder*>(ctx->finder);
   if (f->d_cfg) cudaFree(f->d_cfg);
+  if (f->d_cfg_bks) cudaFree(f->d_cfg_bks);
+  f->bks.release();
   f->drop_graph();
   f->bk.release();
   f->sel.release();
@@ -867,6 +937,7 @@ extern "C" int mkfg_finder_setup(mkfg_context* ctx, const mkfg_find_config* cfg)
   H.inter_pflags = cfg->inter_layer_pflags;
   H.intra_pflags = cfg->intra_layer_pflags;
   H.mat = Material{ctx->d_rl, ctx->d_xi};
+  H.looper_stop = 1;
   if (!f->d_cfg) MKFG_CUDA_TRY(cudaMalloc(&f->d_cfg, sizeof(FindConfigDev)));
   MKFG_CUDA_TRY(cudaMemcpyAsync(f->d_cfg, &H, sizeof(H), cudaMemcpyHostToDevice, ctx->stream));
   MKFG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
@@ -1606,6 +1677,66 @@ extern "C" int mkfg_find_autotune(mkfg_context* ctx, int32_t* seeds_per_block, f
   }
   if (seeds_per_block) *seeds_per_block = best_w;
   if (ms_per_run) *ms_per_run = best_ms;
+  return MKFG_OK;
+}
+
+extern "C" int mkfg_find_backward_search(mkfg_context* ctx, const int32_t* bksearch_pickup) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  Finder* f = finder_of(ctx);
+  MKFG_REQUIRE(f->configured && f->events_loaded, "no event uploaded");
+  MKFG_REQUIRE(bksearch_pickup != nullptr, "null bksearch_pickup");
+  // The backward plans: for a region with a pickup index p, the forward
+  // plan's entries p, p-1, ..., 0 (SteeringParams::make_iterator with
+  // IT_BkwSearch, mkFit/SteeringParams.h:140-144), entry 0 being the pickup;
+  // p = -1 means no backward plan (the region's seeds are left alone).
+  FindConfigDev H = f->host_cfg;
+  int max_steps = 0;
+  for (int r = 0; r < H.n_regions; ++r) {
+    const int p = bksearch_pickup[r];
+    MKFG_REQUIRE(p >= -1 && p < f->host_cfg.plan_len[r], "bksearch_pickup[%d] = %d out of range", r, p);
+    H.pickup[r] = 0;
+    H.plan_len[r] = p + 1;
+    for (int i = 0; i <= p; ++i) H.plan[r][i] = f->host_cfg.plan[r][p - i];
+    max_steps = std::max(max_steps, p);
+  }
+  H.max_steps = max_steps;
+  H.looper_stop = 0;
+  if (!f->d_cfg_bks) MKFG_CUDA_TRY(cudaMalloc(&f->d_cfg_bks, sizeof(FindConfigDev)));
+  cudaStream_t st = ctx->stream;
+  MKFG_CUDA_TRY(cudaMemcpyAsync(f->d_cfg_bks, &H, sizeof(FindConfigDev), cudaMemcpyHostToDevice, st));
+  const int S = f->n_seeds;
+  if (S == 0) {
+    MKFG_CUDA_TRY(cudaStreamSynchronize(st));
+    return MKFG_OK;
+  }
+  if ((rc = f->bks.ensure(3 * rounded(4 * (size_t)S) + 1024))) return rc;
+  BkSearchSave V;
+  {
+    char* p = f->bks.as<char>();
+    V.last = carve<int>(p, S);
+    V.ninside = carve<int>(p, S);
+    V.ntail = carve<int>(p, S);
+  }
+  MKFG_REQUIRE(max_steps <= f->host_cfg.max_steps, "backward plan longer than the forward one");
+  const int n_work = 4 * (f->host_cfg.max_steps + 2);
+  MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.pair_count, 0, 4 * (size_t)(f->host_cfg.max_steps + 2), st));
+  MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.step_count, 0, 4 * (size_t)kCntN * (f->host_cfg.max_steps + 2), st));
+  MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.work, 0, 4 * (size_t)n_work, st));
+  const StepGrids g = step_grids(f);
+  k_bks_begin<<<(S + 127) / 128, 128, 0, st>>>(f->ev, f->d_cfg_bks, V);
+  for (int step = 1; step <= max_steps; ++step) {
+    k_activate<<<g.activate, kBlock, 0, st>>>(f->ev, f->d_cfg_bks, step);
+    k_propagate<<<g.propagate, kBlock, 0, st>>>(f->ev, f->d_cfg_bks, step);
+    k_chi2<<<g.chi2, kBlock, 0, st>>>(f->ev, f->d_cfg_bks, step);
+    k_clone<<<g.clone, kBlock, 0, st>>>(f->ev, f->d_cfg_bks, step);
+    k_update<<<g.update, kBlock, 0, st>>>(f->ev, f->d_cfg_bks, step);
+  }
+  k_merge<<<(S + 127) / 128, 128, 0, st>>>(f->ev, f->d_cfg_bks);
+  k_bks_end<<<(S + 127) / 128, 128, 0, st>>>(f->ev, V);
+  MKFG_CUDA_TRY(cudaGetLastError());
+  // H is a host stack object read by the configuration copy.
+  MKFG_CUDA_TRY(cudaStreamSynchronize(st));
   return MKFG_OK;
 }
 

@@ -58,6 +58,7 @@ struct FindConfigDev {
   float chi2_cut_min, chi2_cut_overlap, pt_cut_overlap;
   unsigned inter_pflags, intra_pflags;
   Material mat;
+  int looper_stop;  // forward search: stop low-pT loopers turning back
 };
 
 // Candidate state, structure of arrays over slots (seed * kSlots + c).

@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(W * kSlots) k_find_fused(EventDev E,
     float par[6], err[21];
     int chg = 0;
     const bool active = in_range && layer >= 0 && state == kFinding && c < ncand &&
-                        activate_cand(E, B, s, slot, layer, par, err, chg);
+                        activate_cand(E, B, s, slot, layer, C.looper_stop != 0, par, err, chg);
     const unsigned act = __ballot_sync(0xffffffffu, active) & grp;
     {
       const unsigned all = __ballot_sync(0xffffffffu, active);

@@ -337,14 +337,14 @@ struct PrepOut {
 // is inactive; a low-pT looper outside r = 25 cm turning back gets a stop
 // node and is inactive. Returns whether the candidate is active.
 __device__ __forceinline__ bool cand_is_active(const EventDev& E, const CandSoA& B, int s, int slot,
-                                               int layer) {
+                                               int layer, bool looper_stop) {
   // Parameters first: their loads overlap the stop-node lookup.
   const float x = B.par[0 * B.cap + slot], y = B.par[1 * B.cap + slot];
   const float ipt = B.par[3 * B.cap + slot], phi = B.par[4 * B.cap + slot];
   const int last = B.last[slot];
   if (hot_index(node_hot_of(E, s, last)) == -2) return false;
   const float pt = fabsf(1.f / ipt);
-  if (pt < 1.2f) {
+  if (looper_stop && pt < 1.2f) {  // IT_FwdSearch only
     const float dphi = fabsf(f_atan2(y, x) - phi);
     if (x * x + y * y > 625.f && dphi > 1.371f && dphi < 4.512f) {
       B.last[slot] = arena_append(E, s, -2, layer, 0.f, last);
@@ -357,9 +357,9 @@ __device__ __forceinline__ bool cand_is_active(const EventDev& E, const CandSoA&
 
 // cand_is_active, loading the state of an active candidate.
 __device__ __forceinline__ bool activate_cand(const EventDev& E, const CandSoA& B, int s, int slot,
-                                              int layer, float (&par)[6], float (&err)[21],
-                                              int& chg) {
-  if (!cand_is_active(E, B, s, slot, layer)) return false;
+                                              int layer, bool looper_stop, float (&par)[6],
+                                              float (&err)[21], int& chg) {
+  if (!cand_is_active(E, B, s, slot, layer, looper_stop)) return false;
   load_state(B, slot, par, err);
   chg = B.chg[slot];
   return true;

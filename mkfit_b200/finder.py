@@ -58,6 +58,7 @@ def _bind(lib):
     lib.mkfg_find_backward_fit.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_int32]
     lib.mkfg_find_hit_index.argtypes = [vp, ctypes.c_int32, vp, vp]
     lib.mkfg_find_run_timed.argtypes = [vp, vp]
+    lib.mkfg_find_backward_search.argtypes = [vp, vp]
     lib.mkfg_find_step_profile.argtypes = [vp, vp, vp]
     lib.mkfg_find_select.argtypes = [vp, ctypes.POINTER(MkfgSelectConfig), ctypes.c_int32, vp]
     lib.mkfg_find_run_fused.argtypes = [vp, ctypes.c_int32]
@@ -200,6 +201,13 @@ class Finder:
         self._bk_last = np.ascontiguousarray(g.bkfit_last, np.int32)
         capi.check(self.lib.mkfg_find_backward_fit(self.ctx.handle, self._bk_last.ctypes.data,
                                                    int(g.flags[3]), int(group_width)))
+
+    def backward_search(self):
+        """Backward search of every seed's backward-fitted best candidate
+        through the geometry's backward plans (mkfg_find_backward_search)."""
+        self._bks_pickup = np.ascontiguousarray(self.cfg.geom.bksearch_pickup, np.int32)
+        capi.check(self.lib.mkfg_find_backward_search(self.ctx.handle,
+                                                      self._bks_pickup.ctypes.data))
 
     KERNELS = ("reset", "activate", "propagate", "chi2", "clone", "update", "merge")
 

@@ -34,6 +34,7 @@ class Geometry:
         self.plan_len = self.arrays["plan_len"]
         self.pickup = self.arrays["pickup"]
         self.bkfit_last = self.arrays["bkfit_last"]
+        self.bksearch_pickup = self.arrays["bksearch_pickup"]
         self.region_order = self.arrays["region_order"]
         self.iter_params = self.arrays["iter_params"]
         self.flags = self.arrays["flags"]

@@ -338,10 +338,11 @@ def cms2017_export(reflib):
 
 
 def ref_find(reflib, ev, max_cands=6, chi2_cut=30.0, zero_c2=True, repeat=1, backward_fit=False,
-             select=False):
+             select=False, backward_search=False):
     """Reference clone-engine finding (find_tracks_load_seeds +
-    FindTracksCloneEngine, then MkBuilder::BackwardFit when backward_fit)
-    on a synth.CmsEvent. Returns a dict of per-seed candidate arrays (see
+    FindTracksCloneEngine, then MkBuilder::BackwardFit when backward_fit,
+    or CompactifyHitStorageForBestCand + BackwardFit + the backward search
+    when backward_search) on a synth.CmsEvent. Returns a dict of per-seed candidate arrays (see
     oracle/ref_driver.cc ref_find); with select, also keep[ns]: 1 for the
     seeds whose best candidate survives run_OneIteration's output selection
     (NaN/silly filter, best-candidate export, duplicate removal)."""
@@ -349,6 +350,8 @@ def ref_find(reflib, ev, max_cands=6, chi2_cut=30.0, zero_c2=True, repeat=1, bac
     _load_find_api(lib)
     lib.ref_set_backward_fit.argtypes = [ctypes.c_int]
     lib.ref_set_backward_fit(1 if backward_fit else 0)
+    lib.ref_set_backward_search.argtypes = [ctypes.c_int]
+    lib.ref_set_backward_search(1 if backward_search else 0)
     lib.ref_set_select_output.argtypes = [ctypes.c_void_p]
     keep = np.zeros(ev.n_seeds, np.int32) if select else None
     lib.ref_set_select_output(keep.ctypes.data if select else None)
@@ -374,6 +377,7 @@ def ref_find(reflib, ev, max_cands=6, chi2_cut=30.0, zero_c2=True, repeat=1, bac
                       o["chg"], o["chi2"], o["score"], o["nfound"], o["ntot"], o["noverlap"],
                       o["ninside"], o["ntail"], o["hit_idx"], o["hit_lyr"], ctypes.byref(secs))
     lib.ref_set_backward_fit(0)
+    lib.ref_set_backward_search(0)
     lib.ref_set_select_output(None)
     if rc != 0:
         raise RuntimeError(f"ref_find failed rc={rc}")

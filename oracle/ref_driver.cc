@@ -56,6 +56,7 @@ double now_s() {
 bool g_cms2017_loaded = false;
 // ref_find runs MkBuilder::BackwardFit after the clone engine when set.
 bool g_backward_fit = false;
+bool g_backward_search = false;
 // When set, ref_find also runs the output selection of run_OneIteration
 // (qfilter_nan_n_silly, export_best_comb_cands(.., true),
 // find_and_remove_duplicates) and marks the surviving seeds here (by label).
@@ -200,6 +201,11 @@ extern "C" {
 // mkFit/MkBuilder.cc:2153-2253) on the best candidate of every seed, as
 // run_OneIteration does with do_backward_fit (mkFit/buildtestMPlex.cc).
 void ref_set_backward_fit(int on) { g_backward_fit = on != 0; }
+
+// ref_find then runs the backward search as run_OneIteration does:
+// CompactifyHitStorageForBestCand, BackwardFit, BeginBkwSearch,
+// FindTracksCloneEngine(IT_BkwSearch), EndBkwSearch.
+void ref_set_backward_search(int on) { g_backward_search = on != 0; }
 
 // ref_find: keep[ns] (by seed label) receives 1 for the seeds whose best
 // candidate survives run_OneIteration's output selection
@@ -362,7 +368,17 @@ int ref_find(int n_layers_in, const int* layer_begin, const float* hpos, const f
     builder.find_tracks_load_seeds(seeds);
     const double t0 = now_s();
     builder.FindTracksCloneEngine();
-    if (g_backward_fit) builder.BackwardFit();
+    if (g_backward_search) {
+      // run_OneIteration with m_backward_search (mkFit/buildtestMPlex.cc:700-714).
+      builder.CompactifyHitStorageForBestCand(itconf.m_backward_drop_seed_hits,
+                                              itconf.m_backward_fit_min_hits);
+      builder.BackwardFit();
+      builder.BeginBkwSearch();
+      builder.FindTracksCloneEngine(SteeringParams::IT_BkwSearch);
+      builder.EndBkwSearch();
+    } else if (g_backward_fit) {
+      builder.BackwardFit();
+    }
     best = std::min(best, now_s() - t0);
     if (r + 1 < std::max(1, repeat)) builder.end_event();
   }

@@ -328,3 +328,64 @@ def test_step_profile(gpu_ctx):
     assert int(prof["upd_barrel"].sum() + prof["upd_endcap"].sum()) == w["updates"]
     assert int(prof["finding_seeds"].sum()) == w["seed_steps"]
     assert prof["clone"].shape == (fnd.cfg.max_steps,) and float(prof["propagate"].sum()) > 0
+
+
+@pytest.mark.parametrize("n_tracks,seed,noise", [(800, 61, 0.01), (2500, 62, 0.02)])
+def test_backward_search_matches_reference(gpu_ctx, reflib, n_tracks, seed, noise):
+    """Backward search (mkfg_find_backward_search) after finding and the
+    backward fit, against the reference's CompactifyHitStorageForBestCand +
+    BackwardFit + BeginBkwSearch + FindTracksCloneEngine(IT_BkwSearch) +
+    EndBkwSearch on the same event. Best-candidate hit lists (inward hits
+    first) equal the reference's for >= 97% of seeds (the rest: near-ties of
+    the forward finding and of the FP32 backward-fitted states); where they
+    agree, the states agree within the backward fit's tolerance."""
+    ev = synth.gen_cms_event(n_tracks, seed=seed, noise_frac=noise)
+    ref = ref_find(reflib, ev, max_cands=M, chi2_cut=30.0, zero_c2=True, backward_search=True)
+    ref_fit = ref_find(reflib, ev, max_cands=M, chi2_cut=30.0, zero_c2=True, backward_fit=True)
+    fnd = Finder(gpu_ctx, FindConfig(max_cands=M, chi2_cut=30.0, zero_c2=True))
+    fnd.upload(ev)
+    fnd.run()
+    fnd.backward_fit()
+    fnd.backward_search()
+    gpu = fnd.download(ev.n_seeds)
+    seeds = [s for s in range(ev.n_seeds) if gpu["n_cands"][s] > 0 and ref["n_cands"][s] > 0]
+    same = [s for s in seeds if hit_list(gpu, s * M) == hit_list(ref, s * M)]
+    grown = [s for s in same if len(hit_list(ref, s * M)) > len(hit_list(ref_fit, s * M))]
+    print(f"\nbackward search, {n_tracks} tracks: {len(same)}/{len(seeds)} best-candidate hit lists "
+          f"equal, {len(grown)} of them grew in the search")
+    assert len(same) >= 0.97 * len(seeds)
+    assert len(grown) > 0
+    slots = np.array(same) * M
+    finite = (np.isfinite(gpu["par"][slots]).all(1) & np.isfinite(ref["par"][slots]).all(1) &
+              np.isfinite(ref["err"][slots]).all(1))
+    assert finite.mean() > 0.99  # diverged backward fits (both sides) are left out
+    pe = par_scaled_err(gpu["par"][slots[finite]].T, ref["par"][slots[finite]].T,
+                        ref["err"][slots[finite]].T)
+    print(f"  par vs reference {summarize(pe)}, {int((~finite).sum())} non-finite left out")
+    assert np.percentile(pe, 99) < 5e-2
+    for k in ("nfound", "ntot", "ninside", "ntail", "chg"):
+        np.testing.assert_array_equal(gpu[k][slots], ref[k][slots], err_msg=k)
+
+
+def test_backward_search_batched_equals_plain(gpu_ctx):
+    events = [synth.gen_cms_event(n, seed=500 + n, noise_frac=0.02) for n in (300, 57)]
+    fnd = Finder(gpu_ctx, FindConfig(max_cands=M))
+    plain = []
+    for ev in events:
+        fnd.upload(ev)
+        fnd.run()
+        fnd.backward_fit()
+        fnd.backward_search()
+        plain.append(fnd.download(ev.n_seeds))
+    total = fnd.upload_batch(events)
+    fnd.run_graph()
+    fnd.backward_fit()
+    fnd.backward_search()
+    batch = fnd.download(total)
+    off = 0
+    for ev, p in zip(events, plain):
+        n = ev.n_seeds
+        np.testing.assert_array_equal(batch["n_cands"][off:off + n], p["n_cands"])
+        for k in ("par", "chi2", "hit_idx", "hit_lyr", "ntot", "nfound"):
+            np.testing.assert_array_equal(batch[k][off * M:(off + n) * M], p[k], err_msg=k)
+        off += n
