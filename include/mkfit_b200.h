@@ -317,8 +317,10 @@ int mkfg_clean_seeds(mkfg_context* ctx, const mkfg_seed_clean_params* p, int32_t
 /* One event: hits (layer l at [layer_begin[l], layer_begin[l+1])) and seeds.
  * Host pointers. cpcm: strip charge per cm as given to Hit::setupAsStrip,
  * negative for pixel hits (Hit.h:285-300); detid: 12-bit module id in the
- * layer. Seed hits: [n_seeds][4] (layer, index within layer), seed_nhits
- * of them valid. */
+ * layer. Seed hits: [n_seeds][seed_hit_stride] (layer, index within
+ * layer), seed_nhits of them valid; seed_hit_stride 0 means 4, at most
+ * MKFG_MAX_SEED_HITS (seeds merged by the seed cleaning carry up to 15). */
+#define MKFG_MAX_SEED_HITS 16
 typedef struct {
   int32_t n_layers;
   const int32_t* layer_begin;
@@ -333,6 +335,7 @@ typedef struct {
   const int32_t* seed_nhits;
   const int32_t* seed_hit_layer;
   const int32_t* seed_hit_index;
+  int32_t seed_hit_stride;
 } mkfg_event;
 
 /* Finding output, indexed by input seed; m = max_cands_per_seed slots per

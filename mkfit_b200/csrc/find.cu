@@ -397,7 +397,7 @@ __global__ void k_seed_nodes(EventDev E, const int* __restrict__ seed_hot) {
   const int nhs = E.init_hot[s];
   for (int h = 0; h < nhs; ++h) {
     const size_t k = (size_t)s * E.hot_cap + h;
-    E.node_hot[k] = seed_hot[4 * s + h];
+    E.node_hot[k] = seed_hot[MKFG_MAX_SEED_HITS * s + h];
     E.node_chi2[k] = 0.f;
     E.node_prev[k] = h - 1;
   }
@@ -950,6 +950,9 @@ namespace mkfg {
 // Host preparation + upload of a batch of events (one event for the plain
 // drop-in form) into the finder's device buffers. Hits and seeds of all
 // events are laid out back to back; every seed knows its event.
+// Row width of an event's seed-hit arrays (0 means 4).
+static int seed_hit_stride(const mkfg_event* ev) { return ev->seed_hit_stride ? ev->seed_hit_stride : 4; }
+
 static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int n_ev) {
   const int L = f->host_cfg.n_layers;
   MKFG_REQUIRE(n_ev >= 1, "empty batch");
@@ -960,8 +963,10 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     for (int l = 0; l < L; ++l)
       MKFG_REQUIRE(ev->layer_begin[l + 1] - ev->layer_begin[l] <= 65535,
                    "event %d layer %d holds more than 65535 hits", e, l);
+    const int sw = seed_hit_stride(ev);
+    MKFG_REQUIRE(sw >= 1 && sw <= MKFG_MAX_SEED_HITS, "event %d: seed_hit_stride %d", e, sw);
     for (int s = 0; s < ev->n_seeds; ++s)
-      MKFG_REQUIRE(ev->seed_nhits[s] >= 1 && ev->seed_nhits[s] <= 4, "seed %d hit count", s);
+      MKFG_REQUIRE(ev->seed_nhits[s] >= 1 && ev->seed_nhits[s] <= sw, "seed %d hit count", s);
     hit_off[e + 1] = hit_off[e] + ev->layer_begin[L];
     seed_off[e + 1] = seed_off[e] + ev->n_seeds;
   }
@@ -1013,7 +1018,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   // Initial candidates (CombCandidate::ImportSeed, mkFit/HitStructures.cc:
   // 483-509), staged in pinned memory by the per-event workers: each
   // event's seeds in sorted order, one initial candidate per seed, and the
-  // seed's hits as its first hit-on-track nodes (at most 4 per seed).
+  // seed's hits as its first hit-on-track nodes (at most MKFG_MAX_SEED_HITS).
   const int SS = std::max(S, 1);
   struct SeedStage {
     float* par;    // [6][SS]
@@ -1030,9 +1035,10 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     int* region;
     int* pickup;
     int* hot_size;
-    int* seed_hot;  // [SS][4]
+    int* seed_hot;  // [SS][MKFG_MAX_SEED_HITS]
   };
-  if ((rc = f->seeds_h.ensure(rounded(4 * (size_t)SS) * (27 + 14 + 4) + 4096))) return rc;
+  if ((rc = f->seeds_h.ensure(rounded(4 * (size_t)SS) * (27 + 14 + MKFG_MAX_SEED_HITS) + 4096)))
+    return rc;
   SeedStage ss;
   {
     char* p = static_cast<char*>(f->seeds_h.ptr);
@@ -1050,7 +1056,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     ss.region = carve<int>(p, SS);
     ss.pickup = carve<int>(p, SS);
     ss.hot_size = carve<int>(p, SS);
-    ss.seed_hot = carve<int>(p, 4 * (size_t)SS);
+    ss.seed_hot = carve<int>(p, MKFG_MAX_SEED_HITS * (size_t)SS);
   }
 
   // Per-event host work (seed order and initial candidates; hit copies into
@@ -1060,8 +1066,9 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     auto work = [&](int e) {
       const mkfg_event* ev = evs + e;
       const int nh = ev->layer_begin[L], o = hit_off[e];
+      const int sw = seed_hit_stride(ev);
       SeedInput si{ev->n_seeds, ev->seed_par, ev->seed_chg, ev->seed_nhits, ev->seed_hit_layer,
-                   ev->seed_hit_index};
+                   ev->seed_hit_index, sw};
       partition_seeds_cms2017(f->layer_desc.data(), L, si, ev->layer_begin, ev->pos, nh, orders[e]);
       for (int r = 0; r < 3; ++r)
         std::memcpy(hh.pos + (size_t)r * NHs + o, ev->pos + (size_t)r * nh, 4 * (size_t)nh);
@@ -1078,18 +1085,18 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
         ss.sev[s] = e;
         ss.region[s] = orders[e].region[i];
         const int nhs = ev->seed_nhits[i];
-        ss.pickup[s] = ev->seed_hit_layer[i * 4 + nhs - 1];
+        ss.pickup[s] = ev->seed_hit_layer[i * sw + nhs - 1];
         for (int c = 0; c < 6; ++c) ss.par[c * (size_t)SS + s] = ev->seed_par[c * n + i];
         for (int c = 0; c < 21; ++c) ss.err[c * (size_t)SS + s] = ev->seed_err[c * n + i];
         ss.chg[s] = ev->seed_chg[i];
         int nf = 0, nm = 0, nin = 0, ntl = 0;
-        for (int h = 0; h < 4; ++h) {
+        for (int h = 0; h < MKFG_MAX_SEED_HITS; ++h) {
           if (h >= nhs) {
-            ss.seed_hot[4 * (size_t)s + h] = 0;
+            ss.seed_hot[MKFG_MAX_SEED_HITS * (size_t)s + h] = 0;
             continue;
           }
-          const int hi = ev->seed_hit_index[i * 4 + h], hl = ev->seed_hit_layer[i * 4 + h];
-          ss.seed_hot[4 * (size_t)s + h] = (hi & 0xffffff) | (hl << 24);
+          const int hi = ev->seed_hit_index[i * sw + h], hl = ev->seed_hit_layer[i * sw + h];
+          ss.seed_hot[MKFG_MAX_SEED_HITS * (size_t)s + h] = (hi & 0xffffff) | (hl << 24);
           if (hi >= 0 || hi == -9) {
             ++nf;
             nin += ntl;
@@ -1191,7 +1198,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   const int SC = SS * kSlots;
   const int max_steps = f->host_cfg.max_steps;
   const int M = f->host_cfg.max_cands;
-  const int hot_cap = ((8 + max_steps * (2 * M + 3)) + 31) / 32 * 32;
+  const int hot_cap = ((MKFG_MAX_SEED_HITS + 4 + max_steps * (2 * M + 3)) + 31) / 32 * 32;
   {
     const size_t need = 3 * rounded(4 * (size_t)SC) * 37 + rounded(4 * (size_t)SS) * 47 + 4096;
     if ((rc = f->cands.ensure(need))) return rc;
@@ -1289,8 +1296,8 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   if ((rc = up(f->ev.region, ss.region, 4 * (size_t)SS))) return rc;
   if ((rc = up(f->ev.pickup_layer, ss.pickup, 4 * (size_t)SS))) return rc;
   if ((rc = up(f->ev.init_hot, ss.hot_size, 4 * (size_t)SS))) return rc;
-  if ((rc = f->seeds.ensure(rounded(16 * (size_t)SS)))) return rc;
-  if ((rc = up(f->seeds.ptr, ss.seed_hot, 16 * (size_t)SS))) return rc;
+  if ((rc = f->seeds.ensure(rounded(4 * MKFG_MAX_SEED_HITS * (size_t)SS)))) return rc;
+  if ((rc = up(f->seeds.ptr, ss.seed_hot, 4 * MKFG_MAX_SEED_HITS * (size_t)SS))) return rc;
   if (S > 0) k_seed_nodes<<<(S + 127) / 128, 128, 0, st>>>(f->ev, f->seeds.as<int>());
   MKFG_CUDA_TRY(cudaGetLastError());
   MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.upd, 0, 4 * (size_t)SC, st));
@@ -1934,7 +1941,7 @@ extern "C" int mkfg_prepare_event_host(const mkfg_find_config* cfg, const mkfg_e
   if (srank) std::copy(prep.srank.begin(), prep.srank.end(), srank);
   if (seed_order || seed_region) {
     SeedInput si{ev->n_seeds, ev->seed_par, ev->seed_chg, ev->seed_nhits, ev->seed_hit_layer,
-                 ev->seed_hit_index};
+                 ev->seed_hit_index, seed_hit_stride(ev)};
     SeedOrder so;
     partition_seeds_cms2017(cfg->layer_desc, cfg->n_layers, si, ev->layer_begin, ev->pos, nh, so);
     if (seed_order) std::copy(so.order.begin(), so.order.end(), seed_order);

@@ -193,7 +193,7 @@ void partition_seeds_cms2017(const float* L, int n_layers, const SeedInput& s,
                 s.par[3 * n + i], s.par[4 * n + i], s.par[5 * n + i], s.chg[i]};
     // Eta of the seed's last hit (Hit::eta, Hit.h:82-87).
     const int last = s.nhits[i] - 1;
-    const int hl = s.hit_layer[i * 4 + last], hi = s.hit_index[i * 4 + last];
+    const int hl = s.hit_layer[i * s.stride + last], hi = s.hit_index[i * s.stride + last];
     const int h = layer_begin[hl] + hi;
     const float hx = hit_pos[h], hy = hit_pos[hit_stride + h], hz = hit_pos[2 * (size_t)hit_stride + h];
     const float theta = std::atan2(std::sqrt(hx * hx + hy * hy), hz);

@@ -65,8 +65,9 @@ struct SeedInput {
   const float* par;  // [6][n]
   const int32_t* chg;
   const int32_t* nhits;
-  const int32_t* hit_layer;  // [n][4]
-  const int32_t* hit_index;  // [n][4]
+  const int32_t* hit_layer;  // [n][stride]
+  const int32_t* hit_index;  // [n][stride]
+  int stride;
 };
 
 void partition_seeds_cms2017(const float* layer_desc, int n_layers, const SeedInput& s,

@@ -38,7 +38,7 @@ class MkfgEvent(ctypes.Structure):
     _fields_ = [("n_layers", ctypes.c_int32), ("layer_begin", vp), ("pos", vp), ("err", vp),
                 ("detid", vp), ("cpcm", vp), ("n_seeds", ctypes.c_int32), ("seed_par", vp),
                 ("seed_err", vp), ("seed_chg", vp), ("seed_nhits", vp), ("seed_hit_layer", vp),
-                ("seed_hit_index", vp)]
+                ("seed_hit_index", vp), ("seed_hit_stride", ctypes.c_int32)]
 
 
 class MkfgFindOut(ctypes.Structure):
@@ -141,6 +141,8 @@ def event_struct(ev):
     e.seed_nhits = p("snh", ev.seed_nhits, np.int32)
     e.seed_hit_layer = p("shl", ev.seed_hit_layer, np.int32)
     e.seed_hit_index = p("shi", ev.seed_hit_index, np.int32)
+    shl = np.asarray(ev.seed_hit_layer)
+    e.seed_hit_stride = int(shl.shape[1]) if shl.ndim == 2 else 4
     e._keep = keep
     return e
 

@@ -249,7 +249,7 @@ def from_cms_event(ev, with_seeds=True):
     return out
 
 
-def to_cms_event(ev, max_seed_hits=4):
+def to_cms_event(ev, max_seed_hits=16):
     """The finder's input (a CmsEvent: hits with detid / cpcm and seeds with
     up to max_seed_hits hits) from a read event dict."""
     from .synth import CmsEvent

@@ -64,3 +64,24 @@ def clean_seeds(ctx, event_seed_begin, par, chg, nhits, hit_layer, hit_index, be
                                     d(chg), d(nh), d(hl), d(hx), hl.shape[1], MAX_HITS,
                                     d(keep), d(onh), d(ohl), d(ohx)))
     return keep, onh, ohl, ohx
+
+
+def cleaned_event(ev, seeds, result):
+    """The finder's input after cleaning: event `ev`'s hits with the kept
+    seeds of `seeds` (a dict par [6][n], err [21][n], chg, ...) in their
+    order, with the merged hit lists of `result` (clean_seeds' output for
+    this event) as [k][MAX_HITS] rows."""
+    from .synth import CmsEvent
+    keep, nh, hl, hx = result
+    k = np.nonzero(keep == 1)[0]
+    return CmsEvent(
+        n_layers=ev.n_layers, layer_begin=ev.layer_begin, hit_pos=ev.hit_pos, hit_err=ev.hit_err,
+        hit_detid=ev.hit_detid, hit_cpcm=ev.hit_cpcm, hit_mc=ev.hit_mc,
+        seed_par=np.ascontiguousarray(seeds["par"][:, k], np.float32),
+        seed_err=np.ascontiguousarray(seeds["err"][:, k], np.float32),
+        seed_chg=np.ascontiguousarray(seeds["chg"][k], np.int32),
+        seed_nhits=np.ascontiguousarray(nh[k], np.int32),
+        seed_hit_layer=np.ascontiguousarray(hl[k], np.int32),
+        seed_hit_index=np.ascontiguousarray(hx[k], np.int32),
+        seed_mc=np.asarray(seeds.get("src", k), np.int32)[k] if "src" in seeds else k.astype(np.int32),
+        n_tracks=ev.n_tracks, seed=ev.seed, n_signal_hits=ev.n_signal_hits)

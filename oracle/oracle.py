@@ -337,6 +337,12 @@ def cms2017_export(reflib):
     return out
 
 
+def _set_seed_stride(lib, seed_hit_layer):
+    lib.ref_set_seed_hit_stride.argtypes = [ctypes.c_int]
+    a = np.asarray(seed_hit_layer)
+    lib.ref_set_seed_hit_stride(int(a.shape[1]) if a.ndim == 2 else 4)
+
+
 def ref_find(reflib, ev, max_cands=6, chi2_cut=30.0, zero_c2=True, repeat=1, backward_fit=False,
              select=False, backward_search=False):
     """Reference clone-engine finding (find_tracks_load_seeds +
@@ -352,6 +358,7 @@ def ref_find(reflib, ev, max_cands=6, chi2_cut=30.0, zero_c2=True, repeat=1, bac
     lib.ref_set_backward_fit(1 if backward_fit else 0)
     lib.ref_set_backward_search.argtypes = [ctypes.c_int]
     lib.ref_set_backward_search(1 if backward_search else 0)
+    _set_seed_stride(lib, ev.seed_hit_layer)
     lib.ref_set_select_output.argtypes = [ctypes.c_void_p]
     keep = np.zeros(ev.n_seeds, np.int32) if select else None
     lib.ref_set_select_output(keep.ctypes.data if select else None)
@@ -396,6 +403,7 @@ def ref_event_prep(reflib, ev):
                                    _f32p, _f32p, _i32p, _i32p, _i32p, _i32p, ctypes.c_void_p,
                                    ctypes.POINTER(ctypes.c_int), ctypes.c_void_p, ctypes.c_void_p,
                                    ctypes.c_void_p]
+    _set_seed_stride(lib, ev.seed_hit_layer)
     c = lambda a, t: np.ascontiguousarray(a, t)
     args = [ev.n_layers, c(ev.layer_begin, np.int32), c(ev.hit_pos, np.float32),
             c(ev.hit_err, np.float32), c(ev.hit_detid, np.int32), c(ev.hit_cpcm, np.int32),
@@ -429,6 +437,7 @@ def ref_find_batch(reflib, events, max_cands=6, chi2_cut=30.0, zero_c2=True, rep
     cat = lambda k, ax, t: np.ascontiguousarray(np.concatenate([getattr(e, k) for e in events], axis=ax), t)
     lb = np.ascontiguousarray(np.stack([ev.layer_begin for ev in events]), np.int32)
     NS = int(seed_off[-1])
+    _set_seed_stride(lib, events[0].seed_hit_layer if events else np.zeros((0, 4)))
     lib.ref_find_batch.restype = ctypes.c_int
     lib.ref_find_batch.argtypes = ([ctypes.c_int, _i32p, _i32p, _i32p, _f32p, _f32p, _i32p, _i32p,
                                     _f32p, _f32p, _i32p, _i32p, _i32p, _i32p, ctypes.c_int,

@@ -57,6 +57,8 @@ bool g_cms2017_loaded = false;
 // ref_find runs MkBuilder::BackwardFit after the clone engine when set.
 bool g_backward_fit = false;
 bool g_backward_search = false;
+// Row width of the seed-hit arrays the finding drivers take.
+int g_seed_hit_stride = 4;
 // When set, ref_find also runs the output selection of run_OneIteration
 // (qfilter_nan_n_silly, export_best_comb_cands(.., true),
 // find_and_remove_duplicates) and marks the surviving seeds here (by label).
@@ -207,6 +209,10 @@ void ref_set_backward_fit(int on) { g_backward_fit = on != 0; }
 // FindTracksCloneEngine(IT_BkwSearch), EndBkwSearch.
 void ref_set_backward_search(int on) { g_backward_search = on != 0; }
 
+// Row width of seed_hit_layer / seed_hit_index in ref_find, ref_event_prep
+// and ref_find_batch (default 4).
+void ref_set_seed_hit_stride(int w) { g_seed_hit_stride = w > 0 ? w : 4; }
+
 // ref_find: keep[ns] (by seed label) receives 1 for the seeds whose best
 // candidate survives run_OneIteration's output selection
 // (mkFit/buildtestMPlex.cc:721-731), 0 otherwise; NULL switches it off.
@@ -308,8 +314,9 @@ int ref_cms2017_export(float* layer_desc, int* plans, int* plan_len, int* pickup
 // Hits: layer l occupies [layer_begin[l], layer_begin[l+1]) of pos[3][nh],
 //   err[6][nh]; detid[nh] (12-bit module id), cpcm[nh] (< 0: pixel hit,
 //   otherwise the strip charge per cm given to Hit::setupAsStrip).
-// Seeds: par[6][ns], err[21][ns], chg[ns]; seed_nhits[ns] (<= 4) hits given
-//   as seed_hit_layer[ns][4], seed_hit_index[ns][4] (index within layer).
+// Seeds: par[6][ns], err[21][ns], chg[ns]; seed_nhits[ns] (<= w) hits given
+//   as seed_hit_layer[ns][w], seed_hit_index[ns][w] (index within layer;
+//   w = 4 unless ref_set_seed_hit_stride says otherwise).
 // Outputs, indexed by input seed (label), m = max_cands:
 //   n_cands[ns], region[ns], sorted_pos[ns] (position after the seed sort),
 //   c_par[ns*m][6], c_err[ns*m][21], c_chg, c_chi2, c_score, c_nfound,
@@ -356,7 +363,7 @@ int ref_find(int n_layers_in, const int* layer_begin, const float* hpos, const f
     Track t = make_track(s, ns, spar, serr, schg);
     t.setLabel(s);
     for (int k = 0; k < seed_nhits[s]; ++k)
-      t.addHitIdx(seed_hit_index[s * 4 + k], seed_hit_layer[s * 4 + k], 0.f);
+      t.addHitIdx(seed_hit_index[s * g_seed_hit_stride + k], seed_hit_layer[s * g_seed_hit_stride + k], 0.f);
     seeds.push_back(t);
   }
 
@@ -486,7 +493,7 @@ int ref_event_prep(int n_layers_in, const int* layer_begin, const float* hpos, c
     Track t = make_track(s, ns, spar, serr, schg);
     t.setLabel(s);
     for (int k = 0; k < seed_nhits[s]; ++k)
-      t.addHitIdx(seed_hit_index[s * 4 + k], seed_hit_layer[s * 4 + k], 0.f);
+      t.addHitIdx(seed_hit_index[s * g_seed_hit_stride + k], seed_hit_layer[s * g_seed_hit_stride + k], 0.f);
     seeds.push_back(t);
   }
   IterationConfig itconf = Config::ItrInfo[0];
@@ -557,7 +564,7 @@ extern "C" int ref_find_batch(int n_ev, const int* hit_off, const int* seed_off,
       Track t = make_track(s, NS, spar, serr, schg);
       t.setLabel(s);
       for (int k = 0; k < seed_nhits[s]; ++k)
-        t.addHitIdx(seed_hit_index[s * 4 + k], seed_hit_layer[s * 4 + k], 0.f);
+        t.addHitIdx(seed_hit_index[s * g_seed_hit_stride + k], seed_hit_layer[s * g_seed_hit_stride + k], 0.f);
       seeds[e].push_back(t);
     }
   }

@@ -389,3 +389,39 @@ def test_backward_search_batched_equals_plain(gpu_ctx):
         for k in ("par", "chi2", "hit_idx", "hit_lyr", "ntot", "nfound"):
             np.testing.assert_array_equal(batch[k][off * M:(off + n) * M], p[k], err_msg=k)
         off += n
+
+
+def test_full_iteration_matches_reference(gpu_ctx, reflib):
+    """run_OneIteration of initialStep end to end on the device — seed
+    cleaning, finding, backward fit, backward search, output selection — on
+    an event whose seeds include near-duplicates (so cleaning drops seeds and
+    merges hits into the kept ones, up to 15 per seed), against the same
+    sequence run by the reference: the same seeds kept, best-candidate hit
+    lists equal for >= 97% of the kept seeds and the selection's verdicts
+    equal for >= 99%."""
+    from mkfit_b200.seed_clean import PARAM_ORDER, SEED_CLEAN_ITER0, clean_seeds, cleaned_event
+    from oracle.oracle import ref_clean_seeds
+    ev = synth.gen_cms_event(1500, seed=71, noise_frac=0.02)
+    sd = synth.with_duplicate_seeds(ev, frac=0.3, seed=71)
+    n = len(sd["chg"])
+    dev = clean_seeds(gpu_ctx, [0, n], sd["par"], sd["chg"], sd["nhits"], sd["hit_layer"],
+                      sd["hit_index"])
+    ref_c = ref_clean_seeds(reflib, sd, [SEED_CLEAN_ITER0[k] for k in PARAM_ORDER])
+    np.testing.assert_array_equal(dev[0], ref_c[0])
+    assert (dev[1][dev[0] == 1] > 4).any(), "no seed carries merged hits"
+    cev = cleaned_event(ev, sd, dev)
+    ref = ref_find(reflib, cev, max_cands=M, chi2_cut=30.0, zero_c2=True, backward_search=True,
+                   select=True)
+    fnd = Finder(gpu_ctx, FindConfig(max_cands=M, chi2_cut=30.0, zero_c2=True))
+    fnd.upload(cev)
+    fnd.run()
+    fnd.backward_fit()
+    fnd.backward_search()
+    keep = fnd.select(cev.n_seeds)
+    gpu = fnd.download(cev.n_seeds)
+    same = sum(hit_list(gpu, s * M) == hit_list(ref, s * M) for s in range(cev.n_seeds))
+    agree = float((keep == ref["keep"]).mean())
+    print(f"\nfull iteration: {n} seeds, {cev.n_seeds} after cleaning, best hit lists equal "
+          f"{same}/{cev.n_seeds}, selection verdicts equal {agree:.4f}")
+    assert same >= 0.97 * cev.n_seeds
+    assert agree >= 0.99

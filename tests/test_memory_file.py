@@ -155,17 +155,17 @@ def test_errors(tmp_path):
             r[2]
     with pytest.raises(capi.MkfgError, match="n_layers"):
         mf.write(tmp_path / "x.bin", [ev], n_layers=71)
-    # A seed with more hits than the finder's row width is refused.
-    ev5 = dict(ev)
+    # A seed with more hits than the finder takes (16) is refused.
+    ev17 = dict(ev)
     s = dict(ev["seeds"])
-    s["hits_begin"] = np.concatenate([[0], np.full(len(s["charge"]), 5).cumsum()]).astype(np.int32)
-    s["hit_index"] = np.zeros(5 * len(s["charge"]), np.int32)
-    s["hit_layer"] = np.zeros(5 * len(s["charge"]), np.int32)
-    ev5["seeds"] = s
-    p5 = tmp_path / "five.bin"
-    mf.write(p5, [ev5], n_layers=72, sections=mf.SEEDS)
-    with pytest.raises(capi.MkfgError, match="5 hits"):
-        mf.to_cms_event(mf.read(p5)[1][0])
+    s["hits_begin"] = np.concatenate([[0], np.full(len(s["charge"]), 17).cumsum()]).astype(np.int32)
+    s["hit_index"] = np.zeros(17 * len(s["charge"]), np.int32)
+    s["hit_layer"] = np.zeros(17 * len(s["charge"]), np.int32)
+    ev17["seeds"] = s
+    p17 = tmp_path / "seventeen.bin"
+    mf.write(p17, [ev17], n_layers=72, sections=mf.SEEDS)
+    with pytest.raises(capi.MkfgError, match="17 hits"):
+        mf.to_cms_event(mf.read(p17)[1][0])
     assert os.path.getsize(good) == len(raw)
 
 
