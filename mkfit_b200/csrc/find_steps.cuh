@@ -451,8 +451,13 @@ __device__ __forceinline__ bool eval_pair(const EventDev& E, const FindConfigDev
     ok &= strip_charge_ok(L.is_barrel, info >> 12, hpar, merr);
   }
   if (ok && L.is_pix) {
-    // Seed-hit layer check on the first (seed) nodes of the arena.
-    for (int i = 0; i <= nfound && i <= 2; ++i)
+    // No second hit on a pixel layer of the first three hit-on-track nodes
+    // (MkFinder.cc:1195-1210: ccand.m_hots[0 .. min(nFound, 2)]). Those are
+    // the seed's own nodes, the first ones of its arena; for a seed with
+    // fewer than three hits the reference reads past the nodes it holds, so
+    // only the seed's nodes are checked here.
+    const int n_seed = E.init_hot[s];
+    for (int i = 0; i <= nfound && i <= 2 && i < n_seed; ++i)
       if (hot_layer(node_hot_of(E, s, i)) == layer) ok = false;
   }
   if (!ok) return false;
