@@ -48,6 +48,10 @@ constexpr int kBlock = 256;
 #ifndef MKFG_UPD_MIN_BLOCKS
 #define MKFG_UPD_MIN_BLOCKS MKFG_HEAVY_MIN_BLOCKS
 #endif
+// The activation kernel at full occupancy (32 registers): 18.90 vs 19.07 ms.
+#ifndef MKFG_ACT_MIN_BLOCKS
+#define MKFG_ACT_MIN_BLOCKS 8
+#endif
 // The same for the clone kernel (one warp per seed, latency bound: the
 // full 64 warps per SM pay for the few registers spilled to L1).
 #ifndef MKFG_CLONE_MIN_BLOCKS
@@ -175,7 +179,7 @@ __device__ __forceinline__ void append_list(bool want, int value, int* list, int
 // Kernel 1a: activation (one thread per candidate slot, light): seed wake-up,
 // unroll + looper stop, seed state, compact list of the active candidates.
 //------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) k_activate(EventDev E, const FindConfigDev* __restrict__ Cp,
+__global__ void __launch_bounds__(kBlock, MKFG_ACT_MIN_BLOCKS) k_activate(EventDev E, const FindConfigDev* __restrict__ Cp,
                                                      int step) {
   const FindConfigDev& C = *Cp;
   const int lane = threadIdx.x & 31;
