@@ -347,6 +347,7 @@ def run_ours(args):
                         "MkBuilder::export_best_comb_cands into reused host arrays); two "
                         "contexts alternate batches"}
 
+    stages = None if args.no_e2e else run_iteration_stages(ctx, stream, finder, events, n_seeds)
     fit = None if fit_batch is None else run_fit(ctx, stream, fit_batch, args)
     adjoint = None if adj_ev is None else run_adjoint(ctx, stream, adj_ev, args)
     pu200 = None if pu_events is None else run_pu200(ctx, stream, finder, pu_events, args)
@@ -415,6 +416,7 @@ def run_ours(args):
         "fit": fit,
         "adjoint": adjoint,
         "pu200": pu200,
+        "iteration_stages": stages,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_find(events)
@@ -497,6 +499,56 @@ def run_adjoint(ctx, stream, ev, args):
 def pu_event_args(rank):
     return [dict(n_tracks=PU_TRACKS, seed=0x9200 + 1000 * rank + i, pt_range=(0.3, 50.0),
                  eta_max=2.5, noise_frac=PU_NOISE) for i in range(PU_EVENTS)]
+
+
+def run_iteration_stages(ctx, stream, finder, events, n_seeds):
+    """Time of the steps of run_OneIteration around the finding, on the
+    same batch (median of 5; CUDA events on the context stream around each
+    call, so host-side setup inside the call counts): the backward fit, the
+    backward search, the output selection, and the seed cleaning of the
+    batch's seeds with 20% near-duplicates added (host-buffer call, wall
+    clock)."""
+    import torch
+    from mkfit_b200 import synth
+    from mkfit_b200.seed_clean import clean_seeds
+
+    def dev_ms(fn, pre=None, reps=5):
+        out = []
+        for _ in range(reps):
+            finder.run_graph()
+            if pre is not None:
+                pre()
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            out.append(a.elapsed_time(b))
+        return statistics.median(out)
+
+    bk = dev_ms(finder.backward_fit)
+    bs = dev_ms(finder.backward_search, pre=finder.backward_fit)
+    sel = dev_ms(lambda: finder.select(n_seeds))
+    sds = [synth.with_duplicate_seeds(e, frac=0.2, seed=i) for i, e in enumerate(events)]
+    begin = np.cumsum([0] + [len(d["chg"]) for d in sds]).astype(np.int32)
+    cat = lambda k, ax: np.concatenate([d[k] for d in sds], axis=ax)  # noqa: E731
+    args = (begin, cat("par", 1), cat("chg", 0), cat("nhits", 0), cat("hit_layer", 0),
+            cat("hit_index", 0))
+    clean_seeds(ctx, *args)
+    ts = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        keep = clean_seeds(ctx, *args)[0]
+        ts.append(time.perf_counter() - t0)
+    return {"events": len(events), "seeds": int(n_seeds),
+            "backward_fit_ms": bk, "backward_search_ms": bs, "select_ms": sel,
+            "seed_cleaning": {"seeds_in": int(begin[-1]), "kept": int(keep.sum()),
+                              "ms_host_buffers": statistics.median(ts) * 1e3},
+            "note": "stream times of the calls around the finding of the bench batch; seed "
+                    "cleaning on the batch's seeds plus 20% near-duplicates, through "
+                    "mkfg_clean_seeds with host buffers (wall clock)"}
 
 
 def run_pu200(ctx, stream, finder, events, args):

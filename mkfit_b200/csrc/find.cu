@@ -428,8 +428,9 @@ __global__ void k_merge(EventDev E, const FindConfigDev* __restrict__ Cp) {
   // A region without a plan (backward search) leaves its seeds as they are.
   if (Cp->plan_len[E.region[s]] == 0) return;
   const int cur = E.cur[s];
-  E.n_cands[s] = merge_seed(E, *Cp, s, E.n_cands[s], cur);
-  E.cur[s] = cur ^ 1;
+  bool moved = true;
+  E.n_cands[s] = merge_seed(E, *Cp, s, E.n_cands[s], cur, moved);
+  if (moved) E.cur[s] = cur ^ 1;
 }
 
 //------------------------------------------------------------------------------

@@ -179,8 +179,9 @@ __global__ void __launch_bounds__(W * kSlots) k_find_fused(EventDev E,
   if (tid < n_local) {
     const int ms = s0 + tid;
     const int cur = E.cur[ms];
-    E.n_cands[ms] = merge_seed(E, C, ms, E.n_cands[ms], cur);
-    E.cur[ms] = cur ^ 1;
+    bool moved = true;
+    E.n_cands[ms] = merge_seed(E, C, ms, E.n_cands[ms], cur, moved);
+    if (moved) E.cur[ms] = cur ^ 1;
   }
 }
 

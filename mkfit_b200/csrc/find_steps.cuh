@@ -955,9 +955,11 @@ __device__ __forceinline__ float cand_score(const CandSoA& B, int slot) {
 
 // CombCandidate::MergeCandsAndBestShortOne(update_score, sort_cands)
 // (mkFit/HitStructures.cc:511-552) for one seed; writes the final list into
-// buffer cur ^ 1 and returns the final candidate count.
+// buffer cur ^ 1 and returns the final candidate count. When the list
+// stays as it is (already in score order, no best short candidate to
+// insert) only the scores are written, in place, and `moved` is false.
 __device__ __forceinline__ int merge_seed(const EventDev& E, const FindConfigDev& C, int s,
-                                          int n, int cur) {
+                                          int n, int cur, bool& moved) {
   const CandSoA& B = E.cand[cur];
   const CandSoA& N = E.cand[cur ^ 1];
   float score[kSlots + 1];
@@ -989,6 +991,14 @@ __device__ __forceinline__ int merge_seed(const EventDev& E, const FindConfigDev
     }
   } else if (has_bs) {
     ins = 0;
+  }
+  bool identity = ins < 0;
+  for (int i = 0; i < n && identity; ++i) identity = order[i] == i;
+  moved = !identity;
+  if (identity) {
+    for (int c = 0; c < n; ++c) B.score[s * kSlots + c] = score[c];
+    E.bshort_valid[s] = 0;
+    return n;
   }
   int w = 0;
   for (int i = 0; i <= n; ++i) {
