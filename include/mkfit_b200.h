@@ -444,10 +444,55 @@ typedef struct {
   float drth_central, drth_obarrel, drth_forward;
   float max_d_invpt, max_d_phi, max_d_cottheta;
   float max_cottheta_obarrel, max_cottheta_forward;
+  /* Which duplicate removal runs (the branch find_and_remove_duplicates
+   * takes, mkFit/MkStdSeqs.cc:605-630): MKFG_DUP_PIXELSEED (iterations with
+   * m_requires_dupclean_tight), MKFG_DUP_SHAREDHITS
+   * (find_duplicates_sharedhits, :456-508: quality-filtered iterations
+   * without it; frac_shared_hits only), MKFG_DUP_ETA_PHI (find_duplicates +
+   * remove_duplicates, :334-429: the other iterations) or MKFG_DUP_NONE
+   * (run_OneIteration's do_remove_duplicates off). */
+  int32_t mode;
+  /* TrackBase algorithm code of the seeds (find_duplicates leaves tracks of
+   * algorithms 9 and 10 alone). */
+  int32_t algorithm;
+  /* find_duplicates windows: Config::maxdPt (on 1/pT), maxdPhi, maxdEta,
+   * maxdR, minFracHitsShared, useHitsForDuplicates (Config.cc:86-91). */
+  float ep_max_d_pt, ep_max_d_phi, ep_max_d_eta, ep_max_dr, ep_min_frac_hits_shared;
+  int32_t ep_use_hits;
 } mkfg_select_config;
+
+#define MKFG_DUP_PIXELSEED 0
+#define MKFG_DUP_SHAREDHITS 1
+#define MKFG_DUP_ETA_PHI 2
+#define MKFG_DUP_NONE 3
 
 int mkfg_find_select(mkfg_context* ctx, const mkfg_select_config* cfg, int32_t n_seeds,
                      int32_t* keep);
+/* A quality filter of run_OneIteration on every seed's best candidate, as
+ * MkBuilder::filter_comb_cands (mkFit/MkBuilder.cc:279-318) applies it
+ * (mkFit/buildtestMPlex.cc:676-724): the StdSeq filter `kind`
+ * (mkFit/MkStdSeqs.h:39-148) with min_hits for the hit-count filters and
+ * the beam spot for the d0 cuts. pass[n_seeds] (host, by input seed; may be
+ * NULL): 1 pass, 0 fail, -1 the seed has no candidate. With `remove`, a
+ * failing seed loses its comb candidate: the backward fit (whose seed groups
+ * are then formed over the remaining seeds, as in the reference's compacted
+ * candidate vector), the backward search, the selection and the downloads
+ * see it as empty. A run restores every seed. Synchronizes the stream. */
+#define MKFG_QF_NAN_N_SILLY 0       /* qfilter_nan_n_silly */
+#define MKFG_QF_N_HITS 1            /* qfilter_n_hits(min_hits) */
+#define MKFG_QF_N_HITS_PIXSEED 2    /* qfilter_n_hits_pixseed(min_hits) */
+#define MKFG_QF_N_LAYERS 3          /* qfilter_n_layers */
+#define MKFG_QF_N_LAYERS_PIXELLESS 4 /* qfilter_n_layers_pixelLess */
+#define MKFG_QF_PIXELLESS_FWD 5     /* qfilter_pixelLessFwd */
+#define MKFG_QF_PIXELLESS_BKWD 6    /* qfilter_pixelLessBkwd */
+typedef struct {
+  int32_t kind;
+  int32_t min_hits;
+  float beam_spot_x, beam_spot_y;
+} mkfg_qfilter_config;
+
+int mkfg_find_filter(mkfg_context* ctx, const mkfg_qfilter_config* cfg, int32_t n_seeds,
+                     int32_t remove, int32_t* pass);
 /* The hit index the upload built on the device for uploaded event `event`
  * (LayerOfHits after SuckInHits / EndRegistrationOfHits,
  * mkFit/HitStructures.cc:77-338): bins in the layout of

@@ -20,6 +20,7 @@
 #include "find_fused.cuh"
 #include "layer_hits.cuh"
 #include "find_steps.cuh"
+#include "quality.cuh"
 
 #include <algorithm>
 #include <atomic>
@@ -402,6 +403,7 @@ __global__ void k_reset(EventDev E, int n_work) {
     E.cur[s] = 0;
     E.hot_size[s] = E.init_hot[s];
     E.bshort_valid[s] = 0;
+    E.removed[s] = 0;
   }
 }
 
@@ -509,7 +511,8 @@ __global__ void k_bks_end(EventDev E, BkSearchSave V) {
 // `nn` lanes of a warp, which make those decisions with group ballots.
 //------------------------------------------------------------------------------
 struct BkFitArgs {
-  const int2* groups;  // (first sorted seed, count)
+  const int2* groups;  // (first position, count) in the seed order below
+  const int* members;  // sorted seeds left by the quality filters; NULL: all
   int n_groups;
   int nn;              // lanes per group (8 or 16)
   unsigned pflags;
@@ -528,7 +531,9 @@ __global__ void __launch_bounds__(kBlock) k_bkfit(EventDev E, const FindConfigDe
   const unsigned gmask = (A.nn == 32 ? 0xffffffffu : ((1u << A.nn) - 1u)) << base;
   const int2 grp = A.groups[g];
   const unsigned tracks = (grp.y >= 32 ? 0xffffffffu : ((1u << grp.y) - 1u)) << base;
-  const int s = grp.x + (k < grp.y ? k : 0);
+  const int pos = grp.x + (k < grp.y ? k : 0);
+  const int s = A.members ? A.members[pos] : pos;
+  const int first = A.members ? A.members[grp.x] : grp.x;
   const bool member = k < grp.y;
   const CandSoA& B = E.cand[E.cur[s]];
   const int slot = s * kSlots;
@@ -548,8 +553,8 @@ __global__ void __launch_bounds__(kBlock) k_bkfit(EventDev E, const FindConfigDe
     for (int e = 0; e < 21; ++e) err[e] = 1.f;
   }
   float chi2 = 0.f;
-  const int reg = E.region[grp.x];
-  const int* lb = E.layer_begin + E.seed_event[grp.x] * E.lb_stride;
+  const int reg = E.region[first];
+  const int* lb = E.layer_begin + E.seed_event[first] * E.lb_stride;
   for (int li = C.plan_len[reg] - 1; li >= A.bkfit_last[reg]; --li) {
     const int layer = C.plan[reg][li];
     while (node >= 0 && hot_index(node_hot_of(E, s, node)) < 0)
@@ -617,17 +622,29 @@ __global__ void __launch_bounds__(kBlock) k_bkfit(EventDev E, const FindConfigDe
 // verdict depends only on the pair, so every pair is tested at once; of a
 // duplicate pair the lower score loses (the earlier track on a tie).
 //------------------------------------------------------------------------------
+// Duplicate removal modes (MKFG_DUP_*): the branches of
+// find_and_remove_duplicates (mkFit/MkStdSeqs.cc:605-630) and none.
+enum DupMode { kDupPixelSeed = 0, kDupSharedHits = 1, kDupEtaPhi = 2, kDupNone = 3 };
+
 struct SelectArgs {
   int* hot;       // [S][kExportHits] hits of the exported best candidate
   int* nhit;      // [S]
   float* phi;
   float* cth;     // 1 / tan(theta)
   float* ipt;
+  float* eta;     // Track::momEta
+  float* pt;      // Track::pT
   float* score;
   int* nfound;
   int* keep;      // [S] 1: exported and not (yet) a duplicate
+  int mode;
+  int algorithm;
   float frac, drth_central, drth_obarrel, drth_forward;
   float maxd1pt, maxdphi, maxdcth, maxcth_ob, maxcth_fw;
+  // find_duplicates (Config::maxdPt, maxdPhi, maxdEta, maxdR,
+  // minFracHitsShared, useHitsForDuplicates).
+  float ep_max_dpt, ep_max_dphi, ep_max_deta, ep_max_dr, ep_min_frac;
+  int ep_use_hits;
 };
 
 __global__ void k_select_prep(EventDev E, const SelectArgs A) {
@@ -638,14 +655,7 @@ __global__ void k_select_prep(EventDev E, const SelectArgs A) {
   if (E.n_cands[s] == 0) return;  // empty comb candidate: nothing exported
   const CandSoA& B = E.cand[E.cur[s]];
   const int slot = s * kSlots;
-  // TrackBase::hasNanNSillyValues (Track.cc:177-192).
-  bool silly = false;
-  for (int i = 0; i < 6; ++i)
-    for (int j = 0; j <= i; ++j) {
-      const float v = B.err[sidx(i, j) * B.cap + slot];
-      if ((i == j && v < 0.f) || !isfinite(v)) silly = true;
-    }
-  if (silly) return;
+  if (silly_errors(B, slot)) return;
   // exportTrack(true): the found hits in order (TrackCand, HitStructures.cc:448-478).
   const int nfound = B.nfound[slot];
   int node = B.last[slot];
@@ -659,6 +669,10 @@ __global__ void k_select_prep(EventDev E, const SelectArgs A) {
   A.phi[s] = B.par[4 * B.cap + slot];
   A.cth[s] = 1.f / f_tan(B.par[5 * B.cap + slot]);
   A.ipt[s] = B.par[3 * B.cap + slot];
+  if (A.mode == kDupEtaPhi) {
+    A.eta[s] = eta_of_theta(B.par[5 * B.cap + slot]);
+    A.pt[s] = fabsf(1.f / B.par[3 * B.cap + slot]);
+  }
   A.score[s] = B.score[slot];
   A.nfound[s] = nfound;
   A.keep[s] = 1;
@@ -668,27 +682,79 @@ __device__ __forceinline__ float squash_phi_minimal(float phi) {
   return phi >= kPI ? phi - kTwoPI : (phi < -kPI ? phi + kTwoPI : phi);
 }
 
-__global__ void k_select_dups(EventDev E, const SelectArgs A, int* __restrict__ dup) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= E.n_seeds || !A.keep[i]) return;
+// find_duplicates (mkFit/MkStdSeqs.cc:334-423) for track i: pairs close in
+// (dphi, deta), or close in 1/pT and sharing most hits, lose their
+// lower-score member. Tracks of the pixelLess and tobTec algorithms (9, 10)
+// mark nothing; all tracks here share one algorithm.
+__device__ void select_dups_eta_phi(const EventDev& E, const SelectArgs& A, int i, int* __restrict__ dup) {
+  if (A.algorithm == 9 || A.algorithm == 10) return;
   const int ev = E.seed_event[i];
-  const float phi1 = A.phi[i], cth1 = A.cth[i], ipt1 = A.ipt[i], sc1 = A.score[i];
+  const float eta1 = A.eta[i], phi1 = A.phi[i], pt1 = A.pt[i], sc1 = A.score[i];
   const int label1 = E.seed_label[i];
-  float max_dr2 = A.drth_central * A.drth_central;
-  if (fabsf(cth1) > A.maxcth_fw) max_dr2 = A.drth_forward * A.drth_forward;
-  else if (fabsf(cth1) > A.maxcth_ob) max_dr2 = A.drth_obarrel * A.drth_obarrel;
+  float max_dr2 = __fmul_rn(A.ep_max_dr, A.ep_max_dr);
+  if (fabsf(eta1) > 2.5f) max_dr2 = __fmul_rn(max_dr2, 16.0f);
+  else if (fabsf(eta1) > 1.44f) max_dr2 = __fmul_rn(max_dr2, 9.0f);
   const int* h1 = A.hot + (size_t)i * kExportHits;
   const int n1 = A.nhit[i];
   for (int j = i + 1; j < E.n_seeds && E.seed_event[j] == ev; ++j) {
     if (!A.keep[j] || E.seed_label[j] == label1) continue;
-    const float dcth = fabsf(A.cth[j] - cth1);
-    if (dcth > A.maxdcth) continue;
-    const float dphi = fabsf(squash_phi_minimal(phi1 - A.phi[j]));
-    if (dphi > A.maxdphi) continue;
-    const float dr2 = __fadd_rn(__fmul_rn(dphi, dphi), __fmul_rn(dcth, dcth));
-    bool is_dup = dr2 < max_dr2;
+    const float deta = fabsf(__fsub_rn(A.eta[j], eta1));
+    if (deta > A.ep_max_deta) continue;
+    const float dphi = fabsf(squash_phi_minimal(__fsub_rn(phi1, A.phi[j])));
+    if (dphi > A.ep_max_dphi) continue;
+    // dphi * dphi + deta * deta, the first product fused as the reference
+    // build contracts it.
+    if (fmaf(dphi, dphi, __fmul_rn(deta, deta)) < max_dr2) {
+      dup[sc1 > A.score[j] ? j : i] = 1;
+      continue;
+    }
+    const float pt2 = A.pt[j];
+    if (pt1 == 0.f || pt2 == 0.f) continue;
+    if (!(fabsf(__fsub_rn(__fdiv_rn(1.f, pt2), __fdiv_rn(1.f, pt1))) < A.ep_max_dpt)) continue;
+    if (A.ep_use_hits) {
+      // Hits of track j also on track i (each of j's hits counted once).
+      const int* h2 = A.hot + (size_t)j * kExportHits;
+      const int n2 = A.nhit[j];
+      int shared = 0;
+      for (int b = 0; b < n2; ++b) {
+        bool on = false;
+        for (int a = 0; a < n1 && !on; ++a) on = h1[a] == h2[b];
+        shared += on;
+      }
+      const float frac = __fdiv_rn((float)shared, (float)min(A.nfound[i], A.nfound[j]));
+      if (frac < A.ep_min_frac) continue;
+    }
+    dup[sc1 > A.score[j] ? j : i] = 1;
+  }
+}
+
+__global__ void k_select_dups(EventDev E, const SelectArgs A, int* __restrict__ dup) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= E.n_seeds || !A.keep[i] || A.mode == kDupNone) return;
+  if (A.mode == kDupEtaPhi) {
+    select_dups_eta_phi(E, A, i, dup);
+    return;
+  }
+  const bool pixelseed = A.mode == kDupPixelSeed;
+  const int ev = E.seed_event[i];
+  const float phi1 = A.phi[i], cth1 = A.cth[i], ipt1 = A.ipt[i], sc1 = A.score[i];
+  const int label1 = E.seed_label[i];
+  float max_dr2 = __fmul_rn(A.drth_central, A.drth_central);
+  if (fabsf(cth1) > A.maxcth_fw) max_dr2 = __fmul_rn(A.drth_forward, A.drth_forward);
+  else if (fabsf(cth1) > A.maxcth_ob) max_dr2 = __fmul_rn(A.drth_obarrel, A.drth_obarrel);
+  const int* h1 = A.hot + (size_t)i * kExportHits;
+  const int n1 = A.nhit[i];
+  for (int j = i + 1; j < E.n_seeds && E.seed_event[j] == ev; ++j) {
+    if (!A.keep[j] || (pixelseed && E.seed_label[j] == label1)) continue;
+    const float dcth = fabsf(__fsub_rn(A.cth[j], cth1));
+    if (dcth > (pixelseed ? A.maxdcth : 1.f)) continue;
+    const float dphi = fabsf(squash_phi_minimal(__fsub_rn(phi1, A.phi[j])));
+    if (dphi > (pixelseed ? A.maxdphi : 1.f)) continue;
+    // dphi * dphi + dcth * dcth, the first product fused as the reference
+    // build contracts it.
+    bool is_dup = pixelseed && fmaf(dphi, dphi, __fmul_rn(dcth, dcth)) < max_dr2;
     if (!is_dup) {
-      if (fabsf(A.ipt[j] - ipt1) > A.maxd1pt) continue;
+      if (pixelseed && fabsf(__fsub_rn(A.ipt[j], ipt1)) > A.maxd1pt) continue;
       const int* h2 = A.hot + (size_t)j * kExportHits;
       const int n2 = A.nhit[j];
       int shared = 0, shared_first = 0;
@@ -703,6 +769,28 @@ __global__ void k_select_dups(EventDev E, const SelectArgs A, int* __restrict__ 
     }
     if (is_dup) dup[sc1 > A.score[j] ? j : i] = 1;
   }
+}
+
+//------------------------------------------------------------------------------
+// Quality filter of every seed's best candidate (MkBuilder::filter_comb_cands,
+// mkFit/MkBuilder.cc:279-318, with one of the StdSeq filters): the verdict
+// by input seed (1 pass, 0 fail, -1 no candidate) and, with `remove`, the
+// failing seeds lose their comb candidate.
+//------------------------------------------------------------------------------
+__global__ void k_qfilter(EventDev E, const FindConfigDev* __restrict__ Cp, const QFilterParams P,
+                          int remove, int* __restrict__ pass_by_label) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= E.n_seeds) return;
+  int res = -1;
+  if (E.n_cands[s] > 0) {
+    const bool pass = qfilter_pass(E, *Cp, E.cand[E.cur[s]], s, s * kSlots, P);
+    res = pass ? 1 : 0;
+    if (!pass && remove) {
+      E.n_cands[s] = 0;
+      E.removed[s] = 1;
+    }
+  }
+  pass_by_label[E.seed_label[s]] = res;
 }
 
 __global__ void k_select_out(EventDev E, const SelectArgs A, const int* __restrict__ dup,
@@ -822,6 +910,9 @@ struct Finder {
   DevBuf bks;  // backward-search saved counts
   FindConfigDev* d_cfg_bks = nullptr;  // backward-search plans
   DevBuf sel;  // output selection scratch
+  // A quality filter removed comb candidates since the upload (the device
+  // flags in ev.removed, cleared by every run, say which).
+  bool filter_removed = false;
   HostBuf hits_h;  // pinned mirror of the hits buffer for the upload
   HostBuf seeds_h; // pinned staging of the initial candidates for the upload
   HostBuf outb_h;  // pinned mirror of the export buffer for the download
@@ -921,6 +1012,7 @@ extern "C" int mkfg_finder_setup(mkfg_context* ctx, const mkfg_find_config* cfg)
     L.is_barrel = b.barrel;
     L.has_hole = d[LC_HAS_HOLE] > 0.5f;
     L.is_pix = d[LC_IS_PIX] > 0.5f;
+    L.is_stereo = d[LC_IS_STEREO] > 0.5f;
   }
   f->n_bins = off;
   f->max_nq = 1;
@@ -1250,6 +1342,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     f->ev.cur = carve<int>(p, SS);
     f->ev.hot_size = carve<int>(p, SS);
     f->ev.bshort_valid = carve<int>(p, SS);
+    f->ev.removed = carve<int>(p, SS);
   }
   {
     const size_t need = rounded(4 * (size_t)SC) * (27 + 10) + 2 * rounded(4 * (size_t)SC * kMaxXHits) +
@@ -1327,6 +1420,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   f->h_seed_off = seed_off;
   f->h_hit_off = hit_off;
   f->events_loaded = 1;
+  f->filter_removed = false;
   return MKFG_OK;
 }
 
@@ -1789,13 +1883,33 @@ extern "C" int mkfg_find_backward_fit(mkfg_context* ctx, const int32_t* bkfit_la
   // task in groups of NN from its start. The task cut is the one of the
   // task pool the reference is built with here: ceil(n / grain) pieces of
   // near-equal size, the first n % pieces one seed longer.
+  // Seeds whose comb candidate a quality filter removed are gone from the
+  // reference's candidate vector (MkBuilder::filter_comb_cands keeps the
+  // others in order): the groups are formed over the survivors.
+  std::vector<int> members;
+  bool filtered = false;
+  if (f->filter_removed) {
+    std::vector<int> removed(f->n_seeds);
+    MKFG_CUDA_TRY(cudaMemcpyAsync(removed.data(), f->ev.removed, 4 * (size_t)f->n_seeds,
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    MKFG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    for (int i = 0; i < f->n_seeds; ++i)
+      if (!removed[i]) members.push_back(i);
+    filtered = (int)members.size() != f->n_seeds;
+  }
+  // Position p of the seed order: members[p] when seeds were removed.
+  std::vector<int> ev_off(f->h_seed_off);
+  if (filtered)
+    for (size_t e = 0; e < ev_off.size(); ++e)
+      ev_off[e] = (int)(std::lower_bound(members.begin(), members.end(), f->h_seed_off[e]) - members.begin());
+  auto seed_at = [&](int p) { return filtered ? members[p] : p; };
   std::vector<int2> groups;
-  for (int e = 0; e + 1 < (int)f->h_seed_off.size(); ++e) {
-    const int b = f->h_seed_off[e], end = f->h_seed_off[e + 1];
+  for (int e = 0; e + 1 < (int)ev_off.size(); ++e) {
+    const int b = ev_off[e], end = ev_off[e + 1];
     const int grain = std::min(std::max(end - b + 1, 4), 32);
     for (int r0 = b; r0 < end;) {
       int r1 = r0;
-      while (r1 < end && f->h_region[r1] == f->h_region[r0]) ++r1;
+      while (r1 < end && f->h_region[seed_at(r1)] == f->h_region[seed_at(r0)]) ++r1;
       const int n = r1 - r0;
       const int pieces = (n + grain - 1) / grain;
       const int base = n / pieces, extra = n % pieces;
@@ -1808,10 +1922,19 @@ extern "C" int mkfg_find_backward_fit(mkfg_context* ctx, const int32_t* bkfit_la
       r0 = r1;
     }
   }
-  if ((rc = f->bk.ensure(groups.size() * sizeof(int2)))) return rc;
+  if (groups.empty()) return MKFG_OK;
+  const size_t gbytes = rounded(groups.size() * sizeof(int2));
+  if ((rc = f->bk.ensure(gbytes + 4 * members.size()))) return rc;
   MKFG_CUDA_TRY(cudaMemcpyAsync(f->bk.ptr, groups.data(), groups.size() * sizeof(int2),
                                 cudaMemcpyHostToDevice, ctx->stream));
   A.groups = f->bk.as<int2>();
+  A.members = nullptr;
+  if (filtered) {
+    int* dm = reinterpret_cast<int*>(f->bk.as<char>() + gbytes);
+    MKFG_CUDA_TRY(cudaMemcpyAsync(dm, members.data(), 4 * members.size(), cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    A.members = dm;
+  }
   A.n_groups = (int)groups.size();
   const int per_block = (kBlock / 32) * (32 / nn);
   k_bkfit<<<(A.n_groups + per_block - 1) / per_block, kBlock, 0, ctx->stream>>>(f->ev, f->d_cfg, A);
@@ -1848,7 +1971,8 @@ extern "C" int mkfg_find_select(mkfg_context* ctx, const mkfg_select_config* cfg
   MKFG_REQUIRE(f->events_loaded && n_seeds == f->n_seeds, "seed count mismatch");
   const int S = f->n_seeds;
   if (S == 0) return MKFG_OK;
-  const size_t need = rounded(4 * (size_t)S * kExportHits) + 9 * rounded(4 * (size_t)S) + 4096;
+  MKFG_REQUIRE(cfg->mode >= 0 && cfg->mode <= MKFG_DUP_NONE, "unknown duplicate mode %d", cfg->mode);
+  const size_t need = rounded(4 * (size_t)S * kExportHits) + 11 * rounded(4 * (size_t)S) + 4096;
   if ((rc = f->sel.ensure(need))) return rc;
   char* p = f->sel.as<char>();
   SelectArgs A;
@@ -1857,6 +1981,8 @@ extern "C" int mkfg_find_select(mkfg_context* ctx, const mkfg_select_config* cfg
   A.phi = carve<float>(p, S);
   A.cth = carve<float>(p, S);
   A.ipt = carve<float>(p, S);
+  A.eta = carve<float>(p, S);
+  A.pt = carve<float>(p, S);
   A.score = carve<float>(p, S);
   A.nfound = carve<int>(p, S);
   A.keep = carve<int>(p, S);
@@ -1871,6 +1997,14 @@ extern "C" int mkfg_find_select(mkfg_context* ctx, const mkfg_select_config* cfg
   A.maxdcth = cfg->max_d_cottheta;
   A.maxcth_ob = cfg->max_cottheta_obarrel;
   A.maxcth_fw = cfg->max_cottheta_forward;
+  A.mode = cfg->mode;
+  A.algorithm = cfg->algorithm;
+  A.ep_max_dpt = cfg->ep_max_d_pt;
+  A.ep_max_dphi = cfg->ep_max_d_phi;
+  A.ep_max_deta = cfg->ep_max_d_eta;
+  A.ep_max_dr = cfg->ep_max_dr;
+  A.ep_min_frac = cfg->ep_min_frac_hits_shared;
+  A.ep_use_hits = cfg->ep_use_hits;
   cudaStream_t st = ctx->stream;
   MKFG_CUDA_TRY(cudaMemsetAsync(dup, 0, 4 * (size_t)S, st));
   const int grid = (S + 127) / 128;
@@ -1880,6 +2014,32 @@ extern "C" int mkfg_find_select(mkfg_context* ctx, const mkfg_select_config* cfg
   MKFG_CUDA_TRY(cudaGetLastError());
   MKFG_CUDA_TRY(cudaMemcpyAsync(keep, d_keep, 4 * (size_t)S, cudaMemcpyDeviceToHost, st));
   MKFG_CUDA_TRY(cudaStreamSynchronize(st));
+  return MKFG_OK;
+}
+
+extern "C" int mkfg_find_filter(mkfg_context* ctx, const mkfg_qfilter_config* cfg, int32_t n_seeds,
+                                int32_t remove, int32_t* pass) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  Finder* f = finder_of(ctx);
+  MKFG_REQUIRE(cfg != nullptr, "null config");
+  MKFG_REQUIRE(f->events_loaded && n_seeds == f->n_seeds, "seed count mismatch");
+  MKFG_REQUIRE(cfg->kind >= 0 && cfg->kind < kQfCount, "unknown quality filter %d", cfg->kind);
+  const int S = f->n_seeds;
+  if (S == 0) return MKFG_OK;
+  if ((rc = f->sel.ensure(rounded(4 * (size_t)S)))) return rc;
+  int* d_pass = f->sel.as<int>();
+  QFilterParams P;
+  P.kind = cfg->kind;
+  P.min_hits = cfg->min_hits;
+  P.beam_x = cfg->beam_spot_x;
+  P.beam_y = cfg->beam_spot_y;
+  cudaStream_t st = ctx->stream;
+  k_qfilter<<<(S + 127) / 128, 128, 0, st>>>(f->ev, f->d_cfg, P, remove ? 1 : 0, d_pass);
+  MKFG_CUDA_TRY(cudaGetLastError());
+  if (pass) MKFG_CUDA_TRY(cudaMemcpyAsync(pass, d_pass, 4 * (size_t)S, cudaMemcpyDeviceToHost, st));
+  MKFG_CUDA_TRY(cudaStreamSynchronize(st));
+  if (remove) f->filter_removed = true;
   return MKFG_OK;
 }
 

@@ -45,7 +45,7 @@ struct LayerDev {
   float c_c2_sf, c_c2_0, c_c2_1, c_c2_2;
   float qmin, fq;
   int nq, bin_offset;
-  int is_barrel, has_hole, is_pix, pad;
+  int is_barrel, has_hole, is_pix, is_stereo;
 };
 
 struct FindConfigDev {
@@ -105,6 +105,7 @@ struct EventDev {
   CandSoA cand[2];
   CandSoA bshort;
   int* bshort_valid;
+  int* removed;    // the seed's comb candidate was dropped by a quality filter
   // Hit-on-track arena, hot_cap nodes per seed.
   int* node_hot;   // index (24 bit, signed) | layer << 24 (HitOnTrack layout)
   float* node_chi2;
@@ -184,6 +185,35 @@ __device__ __forceinline__ float f_tan(float x) {
 #else
   return tanf(x);
 #endif
+}
+
+// Track::momEta / getEta(theta) (Hit.h:77-79) with the float libm calls.
+__device__ __forceinline__ float eta_of_theta(float theta) {
+  return -1.0f * f_log(f_tan(theta / 2.0f));
+}
+
+// Helix radius per GeV of pT in cm, signed as TrackBase::d0BeamSpot takes
+// it: ((charge < 0) ? 100 : -100) / (Config::sol * Config::Bfield), in
+// float as the reference's constants.
+constexpr float kSolBfield = 0.299792458f * 3.8112f;
+constexpr float kD0KNeg = 100.0f / kSolBfield;
+constexpr float kD0KPos = -100.0f / kSolBfield;
+
+// TrackBase::d0BeamSpot, not linearised (Track.cc:195-210): the distance of
+// the helix centre from the beam spot less the helix radius. The reference
+// build contracts x - k*py and y + k*px into FMAs; d0 is a difference of two
+// numbers near the helix radius, so the rounding decides near-ties.
+__device__ __forceinline__ float d0_beam_spot(float x, float y, float ipt, float phi, int q, float bx,
+                                              float by) {
+  const float k = q < 0 ? kD0KNeg : kD0KPos;
+  const float pt = fabsf(1.f / ipt);
+  const float abs_ooc_half = fabsf(__fmul_rn(k, pt));
+  float sp, cp;
+  f_sincos(phi, &sp, &cp);
+  const float px = __fmul_rn(pt, cp), py = __fmul_rn(pt, sp);
+  const float xc = fmaf(-k, py, x);
+  const float yc = fmaf(k, px, y);
+  return __fsub_rn(hypot_f(__fsub_rn(xc, bx), __fsub_rn(yc, by)), abs_ooc_half);
 }
 
 }  // namespace mkfg

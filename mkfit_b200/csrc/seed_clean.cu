@@ -39,7 +39,6 @@ struct CleanParams {
   float dz2inv_bh, dr2inv_bh, dz2inv_bl, dr2inv_bl;
   float dz2inv_eh, dr2inv_eh, dz2inv_el, dr2inv_el;
   float beam_x, beam_y;
-  float k_neg, k_pos;  // d0BeamSpot helix constant for charge < 0 / >= 0
   int reach;           // eta bins scanned on each side
 };
 
@@ -72,11 +71,6 @@ struct CleanDev {
   int* err;             // bit 0: pair pool overflow, bit 1: per-event pair overflow
 };
 
-// Track::momEta / getEta(theta) (Hit.h:77-79) with the float libm calls.
-__device__ __forceinline__ float eta_of_theta(float theta) {
-  return -1.0f * f_log(f_tan(theta / 2.0f));
-}
-
 __global__ void k_clean_features(CleanDev D, CleanParams P) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= D.n) return;
@@ -93,20 +87,7 @@ __global__ void k_clean_features(CleanDev D, CleanParams P) {
   D.pos2[i] = (float)((double)x * (double)x + (double)y * (double)y);
   D.ctheta[i] = 1.f / f_tan(theta);
   D.invptq[i] = __fmul_rn((float)q, ipt);
-  // TrackBase::d0BeamSpot, not linearised (Track.cc:195-210).
-  {
-    const float k = q < 0 ? P.k_neg : P.k_pos;
-    const float abs_ooc_half = fabsf(__fmul_rn(k, pt));
-    float sp, cp;
-    f_sincos(phi, &sp, &cp);
-    const float px = __fmul_rn(pt, cp), py = __fmul_rn(pt, sp);
-    // The reference build contracts x - k*py and y + k*px into FMAs; d0 is a
-    // difference of two numbers near the helix radius, so the rounding
-    // decides near-ties between duplicates.
-    const float xc = fmaf(-k, py, x);
-    const float yc = fmaf(k, px, y);
-    D.d0[i] = __fsub_rn(hypot_f(__fsub_rn(xc, P.beam_x), __fsub_rn(yc, P.beam_y)), abs_ooc_half);
-  }
+  D.d0[i] = d0_beam_spot(x, y, ipt, phi, q, P.beam_x, P.beam_y);
   // Eta bin (NaN and out-of-range values go to the edge bins: only the
   // window test decides, the bins only bound the scan).
   const float f = (eta - kEtaLo) * (kEtaBins / (kEtaHi - kEtaLo));
@@ -375,13 +356,6 @@ extern "C" int mkfg_clean_seeds(mkfg_context* ctx, const mkfg_seed_clean_params*
   P.dr2inv_el = inv2(p->drmax_el);
   P.beam_x = p->beam_x;
   P.beam_y = p->beam_y;
-  {
-    // Config::sol * Config::Bfield in float, as the reference's constants.
-    const float sol = 0.299792458f, bfield = 3.8112f;
-    const float sb = sol * bfield;
-    P.k_neg = 100.0f / sb;
-    P.k_pos = -100.0f / sb;
-  }
   const float drmax = std::max(std::max(p->drmax_bh, p->drmax_bl), std::max(p->drmax_eh, p->drmax_el));
   MKFG_REQUIRE(drmax > 0.f && drmax < 1.f, "drmax out of range");
   P.reach = (int)std::ceil(drmax * (kEtaBins / (kEtaHi - kEtaLo))) + 1;

@@ -24,14 +24,73 @@ class MkfgFindConfig(ctypes.Structure):
 class MkfgSelectConfig(ctypes.Structure):
     _fields_ = [(k, ctypes.c_float) for k in (
         "frac_shared_hits", "drth_central", "drth_obarrel", "drth_forward", "max_d_invpt",
-        "max_d_phi", "max_d_cottheta", "max_cottheta_obarrel", "max_cottheta_forward")]
+        "max_d_phi", "max_d_cottheta", "max_cottheta_obarrel", "max_cottheta_forward")] + [
+        ("mode", ctypes.c_int32), ("algorithm", ctypes.c_int32)] + [
+        (k, ctypes.c_float) for k in ("ep_max_d_pt", "ep_max_d_phi", "ep_max_d_eta", "ep_max_dr",
+                                      "ep_min_frac_hits_shared")] + [
+        ("ep_use_hits", ctypes.c_int32)]
 
+
+class MkfgQFilterConfig(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("min_hits", ctypes.c_int32),
+                ("beam_spot_x", ctypes.c_float), ("beam_spot_y", ctypes.c_float)]
+
+
+# Duplicate removal modes of mkfg_find_select (MKFG_DUP_*).
+DUP_PIXELSEED, DUP_SHAREDHITS, DUP_ETA_PHI, DUP_NONE = range(4)
+# Quality filters of mkfg_find_filter (MKFG_QF_*), StdSeq::qfilter_*.
+(QF_NAN_N_SILLY, QF_N_HITS, QF_N_HITS_PIXSEED, QF_N_LAYERS, QF_N_LAYERS_PIXELLESS,
+ QF_PIXELLESS_FWD, QF_PIXELLESS_BKWD) = range(7)
 
 # Iteration 0 of CMS-2017: set_dupl_params(0.24, 0.002, 0.004, 0.008)
-# (Geoms/CMS-2017.cc:750) and the window constants of Config.cc:93-97.
+# (Geoms/CMS-2017.cc:750), the window constants of Config.cc:93-97 and the
+# find_duplicates constants of Config.cc:86-91.
 SELECT_ITER0 = dict(frac_shared_hits=0.24, drth_central=0.002, drth_obarrel=0.004,
                     drth_forward=0.008, max_d_invpt=1.8, max_d_phi=0.37, max_d_cottheta=0.37,
-                    max_cottheta_obarrel=1.99, max_cottheta_forward=6.05)
+                    max_cottheta_obarrel=1.99, max_cottheta_forward=6.05, mode=DUP_PIXELSEED,
+                    algorithm=4, ep_max_d_pt=0.5, ep_max_d_phi=0.25, ep_max_d_eta=0.05,
+                    ep_max_dr=0.0025, ep_min_frac_hits_shared=0.75, ep_use_hits=1)
+
+
+def _iteration_selection():
+    """run_OneIteration's filters and duplicate removal for the ten CMS-2017
+    iterations (Geoms/CMS-2017.cc:740-845; mkFit/buildtestMPlex.cc:676-731):
+    (TrackBase algorithm, filter after finding, filter after the backward
+    fit, min hits, duplicate mode, frac_shared_hits, (drth central,
+    obarrel, forward)). None = no filter."""
+    rows = {
+        # index: (algorithm, requires_quality_filter, dupclean_tight, minHitsQF, frac, drth)
+        0: (4, False, True, 4, 0.24, (0.002, 0.004, 0.008)),
+        1: (22, False, True, 4, 0.24, (0.03, 0.05, 0.08)),
+        2: (23, False, True, 4, 0.5, (0.01, 0.03, 0.05)),
+        3: (5, False, True, 4, 0.33, (0.018, 0.05, 0.018)),
+        4: (24, False, True, 4, 0.24, (0.018, 0.05, 0.05)),
+        5: (7, True, True, 4, 0.24, (0.01, 0.01, 0.1)),
+        6: (8, False, True, 4, 0.2, (0.05, 0.05, 0.05)),
+        7: (9, True, False, 3, 0.14, (0.001, 0.001, 0.001)),
+        8: (10, True, False, 4, 0.25, (0.001, 0.001, 0.001)),
+        9: (6, True, True, 4, 0.5, (0.03, 0.05, 0.05)),
+    }
+    out = {}
+    for it, (algo, qf, tight, min_hits, frac, drth) in rows.items():
+        pre = post = None
+        if qf and algo != 7:
+            pre = {6: QF_N_HITS_PIXSEED, 9: QF_PIXELLESS_FWD}.get(algo, QF_N_HITS)
+        if qf and algo in (7, 9):
+            post = QF_N_LAYERS if algo == 7 else QF_PIXELLESS_BKWD
+        if qf and not tight:
+            mode = DUP_SHAREDHITS
+        elif tight:
+            mode = DUP_PIXELSEED
+        else:
+            mode = DUP_ETA_PHI
+        out[it] = dict(algorithm=algo, pre=pre, post=post,
+                       min_hits=3 if algo == 6 else min_hits, mode=mode, frac_shared_hits=frac,
+                       drth=drth)
+    return out
+
+
+ITERATION_SELECTION = _iteration_selection()
 
 
 class MkfgEvent(ctypes.Structure):
@@ -61,6 +120,8 @@ def _bind(lib):
     lib.mkfg_find_backward_search.argtypes = [vp, vp]
     lib.mkfg_find_step_profile.argtypes = [vp, vp, vp]
     lib.mkfg_find_select.argtypes = [vp, ctypes.POINTER(MkfgSelectConfig), ctypes.c_int32, vp]
+    lib.mkfg_find_filter.argtypes = [vp, ctypes.POINTER(MkfgQFilterConfig), ctypes.c_int32,
+                                     ctypes.c_int32, vp]
     lib.mkfg_find_run_fused.argtypes = [vp, ctypes.c_int32]
     lib.mkfg_find_autotune.argtypes = [vp, ctypes.POINTER(ctypes.c_int32),
                                        ctypes.POINTER(ctypes.c_float)]
@@ -259,12 +320,44 @@ class Finder:
 
     def select(self, n_seeds, **params):
         """Output selection of run_OneIteration (NaN/silly filter + duplicate
-        removal) on the current results: keep[n_seeds] by input seed."""
+        removal, `mode` one of DUP_*) on the current results: keep[n_seeds]
+        by input seed."""
         c = MkfgSelectConfig(**{**SELECT_ITER0, **params})
         keep = np.zeros(n_seeds, np.int32)
         capi.check(self.lib.mkfg_find_select(self.ctx.handle, ctypes.byref(c), n_seeds,
                                              keep.ctypes.data))
         return keep
+
+    def filter(self, n_seeds, kind, min_hits=4, beam_spot=(0.0, 0.0), remove=False):
+        """A quality filter (QF_*) on every seed's best candidate, as
+        MkBuilder::filter_comb_cands applies it: pass[n_seeds] by input seed
+        (1 pass, 0 fail, -1 no candidate); with remove, failing seeds lose
+        their comb candidate until the next run."""
+        c = MkfgQFilterConfig(kind, min_hits, beam_spot[0], beam_spot[1])
+        out = np.zeros(n_seeds, np.int32)
+        capi.check(self.lib.mkfg_find_filter(self.ctx.handle, ctypes.byref(c), n_seeds,
+                                             1 if remove else 0, out.ctypes.data))
+        return out
+
+    def run_iteration_selection(self, n_seeds, iteration=0, beam_spot=(0.0, 0.0), backward_fit=True,
+                                remove_duplicates=True):
+        """The steps of run_OneIteration after the clone engine for CMS-2017
+        iteration `iteration` (mkFit/buildtestMPlex.cc:676-731): its
+        quality filter with removal, the backward fit, the filter after it,
+        then the NaN/silly filter and duplicate removal. Returns keep by
+        input seed. The backward search is not part of it (backward_search
+        runs it on its own)."""
+        sel = ITERATION_SELECTION[iteration]
+        if sel["pre"] is not None:
+            self.filter(n_seeds, sel["pre"], sel["min_hits"], beam_spot, remove=True)
+        if backward_fit:
+            self.backward_fit()
+            if sel["post"] is not None:
+                self.filter(n_seeds, sel["post"], sel["min_hits"], beam_spot, remove=True)
+        d = sel["drth"]
+        return self.select(n_seeds, mode=sel["mode"] if remove_duplicates else DUP_NONE,
+                           algorithm=sel["algorithm"], frac_shared_hits=sel["frac_shared_hits"],
+                           drth_central=d[0], drth_obarrel=d[1], drth_forward=d[2])
 
     def hit_index(self, event, n_bins, n_hits):
         """The device-built hit index of uploaded event `event`:

@@ -344,16 +344,29 @@ def _set_seed_stride(lib, seed_hit_layer):
 
 
 def ref_find(reflib, ev, max_cands=6, chi2_cut=30.0, zero_c2=True, repeat=1, backward_fit=False,
-             select=False, backward_search=False):
+             select=False, backward_search=False, qf_pre=-1, qf_post=-1, qf_min_hits=0,
+             beam=(0.0, 0.0), dup_mode=0, dup_params=None):
     """Reference clone-engine finding (find_tracks_load_seeds +
     FindTracksCloneEngine, then MkBuilder::BackwardFit when backward_fit,
     or CompactifyHitStorageForBestCand + BackwardFit + the backward search
     when backward_search) on a synth.CmsEvent. Returns a dict of per-seed candidate arrays (see
     oracle/ref_driver.cc ref_find); with select, also keep[ns]: 1 for the
     seeds whose best candidate survives run_OneIteration's output selection
-    (NaN/silly filter, best-candidate export, duplicate removal)."""
+    (NaN/silly filter, best-candidate export, duplicate removal).
+    qf_pre / qf_post: quality filter (QF_KINDS index, -1 none) applied with
+    MkBuilder::filter_comb_cands after the clone engine / after the backward
+    fit or search, as run_OneIteration does; dup_mode: the duplicate removal
+    of the selection (DUP_MODES index) with dup_params (fracSharedHits,
+    drth central, obarrel, forward) replacing iteration 0's."""
     lib = reflib.lib
     _load_find_api(lib)
+    lib.ref_set_iteration_filters.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_float, ctypes.c_float, ctypes.c_int,
+                                              ctypes.c_void_p]
+    dp = None if dup_params is None else np.ascontiguousarray(dup_params, np.float32)
+    lib.ref_set_iteration_filters(int(qf_pre), int(qf_post), int(qf_min_hits), float(beam[0]),
+                                  float(beam[1]), int(dup_mode),
+                                  None if dp is None else dp.ctypes.data)
     lib.ref_set_backward_fit.argtypes = [ctypes.c_int]
     lib.ref_set_backward_fit(1 if backward_fit else 0)
     lib.ref_set_backward_search.argtypes = [ctypes.c_int]
@@ -386,6 +399,7 @@ def ref_find(reflib, ev, max_cands=6, chi2_cut=30.0, zero_c2=True, repeat=1, bac
     lib.ref_set_backward_fit(0)
     lib.ref_set_backward_search(0)
     lib.ref_set_select_output(None)
+    lib.ref_set_iteration_filters(-1, -1, 0, 0.0, 0.0, 0, None)
     if rc != 0:
         raise RuntimeError(f"ref_find failed rc={rc}")
     o["seconds"] = secs.value
@@ -532,6 +546,21 @@ def clean_seed_features(seeds, beam=(0.0, 0.0)):
     pos2 = (x.astype(np.float64) ** 2 + y.astype(np.float64) ** 2).astype(np.float32)
     ctheta = f(1.0) / _libm_f32("tanf", theta)
     invptq = chg.astype(np.float32) * ipt
+    d0, radius = d0_beam_spot(par, chg, beam)
+    return dict(pt=pt, eta=eta, pos2=pos2, ctheta=ctheta, invptq=invptq, d0=d0, radius=radius)
+
+
+def d0_beam_spot(par, chg, beam=(0.0, 0.0)):
+    """TrackBase::d0BeamSpot, not linearised (Track.cc:195-210), in float32
+    with the host C library's sinf / cosf and x - k*py, y + k*px contracted
+    into FMAs as the reference build does. par [6][n]. Returns (d0, |k pt|),
+    the second being the helix radius d0 is a difference against."""
+    f = np.float32
+    par = np.asarray(par, np.float32)
+    chg = np.asarray(chg, np.int32)
+    n = chg.shape[0]
+    x, y, ipt, phi = par[0], par[1], par[3], par[4]
+    pt = np.abs(f(1.0) / ipt)
     sb = f(0.299792458) * f(3.8112)
     k = np.where(chg < 0, f(100.0) / sb, f(-100.0) / sb).astype(np.float32)
     px, py = pt * _libm_f32("cosf", phi), pt * _libm_f32("sinf", phi)
@@ -540,7 +569,7 @@ def clean_seed_features(seeds, beam=(0.0, 0.0)):
     radius = np.abs(k * pt)
     d0 = (np.hypot((xc - f(beam[0])).astype(np.float64), (yc - f(beam[1])).astype(np.float64))
           .astype(np.float32) - radius)
-    return dict(pt=pt, eta=eta, pos2=pos2, ctheta=ctheta, invptq=invptq, d0=d0, radius=radius)
+    return d0, radius
 
 
 def restate_clean_seeds(seeds, params, beam=(0.0, 0.0), max_hits=16):
@@ -727,3 +756,318 @@ def ref_mf_read(reflib, path, which, hit_cap=1 << 20, trk_cap=1 << 15, hcap=1 <<
     ns = counts[6]
     out["sim_states"] = dict(par=stp[:, :ns].copy(), err=ste[:, :ns].copy(), charge=stc[:ns].copy())
     return out
+
+
+# ---------------------------------------------------------------------------
+# Quality filters and duplicate removal of run_OneIteration
+# ---------------------------------------------------------------------------
+
+# StdSeq quality filters (mkFit/MkStdSeqs.h:39-148) in the order of their
+# codes (the bits of ref_qfilters / restate_qfilters).
+QF_KINDS = ("nan_n_silly", "n_hits", "n_hits_pixseed", "n_layers", "n_layers_pixelless",
+            "pixelless_fwd", "pixelless_bkwd")
+# Duplicate removal by the branch of find_and_remove_duplicates
+# (mkFit/MkStdSeqs.cc:605-630), plus "none" (do_remove_duplicates off).
+DUP_MODES = ("pixelseed", "sharedhits", "eta_phi", "none")
+
+
+def ref_qfilters(reflib, cands, nseed, min_hits=4, beam=(0.0, 0.0)):
+    """Every quality filter on candidates given as exported hit lists (chain
+    order, missing-hit entries included), by the reference (oracle/ref_driver.cc
+    ref_qfilters: each candidate rebuilt as a TrackCand). cands: par [n][6],
+    err [n][21], chg, ntot [n], hit_idx / hit_lyr [n][w]; nseed [n]: hits of
+    the seed. Returns int32 [n], bit k = QF_KINDS[k] passes."""
+    lib = reflib.lib
+    lib.ref_qfilters.restype = ctypes.c_int
+    lib.ref_qfilters.argtypes = [ctypes.c_int, _f32p, _f32p, _i32p, _i32p, _i32p, _i32p, _i32p,
+                                 ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float, _i32p]
+    c = np.ascontiguousarray
+    n = int(len(cands["chg"]))
+    hi = c(cands["hit_idx"], np.int32)
+    out = np.zeros(n, np.int32)
+    rc = lib.ref_qfilters(n, c(cands["par"], np.float32).reshape(n, 6),
+                          c(cands["err"], np.float32).reshape(n, 21), c(cands["chg"], np.int32),
+                          c(nseed, np.int32), c(cands["ntot"], np.int32), hi,
+                          c(cands["hit_lyr"], np.int32), hi.shape[1], int(min_hits),
+                          float(beam[0]), float(beam[1]), out)
+    if rc != 0:
+        raise RuntimeError(f"ref_qfilters failed rc={rc}")
+    return out
+
+
+def ref_dups(reflib, mode, tracks, algo=0, frac=0.24, drth=(0.002, 0.004, 0.008)):
+    """Duplicate removal (DUP_MODES[mode]) by the reference on exported
+    tracks (oracle/ref_driver.cc ref_dups). tracks: par [n][6], chg, score,
+    label, nfound, nh [n], hit_idx / hit_lyr [n][w] (no missing-hit
+    entries). Returns keep [n]."""
+    lib = reflib.lib
+    lib.ref_dups.restype = ctypes.c_int
+    lib.ref_dups.argtypes = [ctypes.c_int, ctypes.c_int, _f32p, _i32p, _f32p, _i32p, ctypes.c_int,
+                             _i32p, _i32p, _i32p, _i32p, ctypes.c_int, ctypes.c_float,
+                             ctypes.c_float, ctypes.c_float, ctypes.c_float, _i32p]
+    c = np.ascontiguousarray
+    n = int(len(tracks["chg"]))
+    hi = c(tracks["hit_idx"], np.int32)
+    keep = np.zeros(n, np.int32)
+    rc = lib.ref_dups(int(mode), n, c(tracks["par"], np.float32).reshape(n, 6),
+                      c(tracks["chg"], np.int32), c(tracks["score"], np.float32),
+                      c(tracks["label"], np.int32), int(algo), c(tracks["nfound"], np.int32),
+                      c(tracks["nh"], np.int32), hi, c(tracks["hit_lyr"], np.int32), hi.shape[1],
+                      float(frac), float(drth[0]), float(drth[1]), float(drth[2]), keep)
+    if rc != 0:
+        raise RuntimeError(f"ref_dups failed rc={rc}")
+    return keep
+
+
+def _in_pix_ranges(lyr):
+    """The pixel layers TrackCand::getLastFoundPixelHitLyr names
+    (HitStructures.h:753-773): 0-3, 18-20, 45-47."""
+    return 0 <= lyr <= 3 or 18 <= lyr <= 20 or 45 <= lyr <= 47
+
+
+def restate_qfilters(cands, nseed, is_pix, is_stereo, min_hits=4, beam=(0.0, 0.0)):
+    """Pure-Python restatement of the quality filters on the same inputs as
+    ref_qfilters: the TrackCand hit walks (HitStructures.h:732-859, newest
+    hit first, with their quirks: the 'previous stereo' flag holds the
+    stereo count so far, a double stereo layer matches the mono layer
+    below it), TrackBase::d0BeamSpot and the cuts of MkStdSeqs.h:39-148 in
+    float32. is_pix / is_stereo: per-layer flags of the geometry."""
+    f = np.float32
+    n = len(cands["chg"])
+    par = np.asarray(cands["par"], np.float32).reshape(n, 6)
+    err = np.asarray(cands["err"], np.float32).reshape(n, 21)
+    chg = np.asarray(cands["chg"], np.int32)
+    d0, _ = d0_beam_spot(par.T, chg, beam)
+    pi_over_2 = f(f(3.14159265358979323846) / f(2.0))
+    out = np.zeros(n, np.int32)
+    for i in range(n):
+        nt = int(cands["ntot"][i])
+        hots = [(int(cands["hit_idx"][i][k]), int(cands["hit_lyr"][i][k])) for k in range(nt)]
+        found = lambda h: h[0] >= 0 or h[0] == -9  # noqa: E731
+        nfound = sum(1 for h in hots if found(h))
+        nseed4 = int(nseed[i]) & 15
+        back = hots[::-1]
+        # getLastFoundHitLyr / getLastFoundPixelHitLyr
+        llyr = next((h[1] for h in back if h[0] >= 0), -1)
+        lplyr = next((h[1] for h in back if h[0] >= 0 and _in_pix_ranges(h[1])), -1)
+        # nUniqueLayers
+        nul, prev = 0, -1
+        for idx, lyr in back:
+            if lyr >= 0 and (idx >= 0 or idx == -9) and lyr != prev:
+                nul += 1
+                prev = lyr
+        # nHitsByTypeEncoded
+        pix = stereo = mono = matched = 0
+        prev, prev_stereo, double_stereo = -1, 0, -1
+        for idx, lyr in back:
+            if lyr >= 0 and (idx >= 0 or idx == -9):
+                if is_pix[lyr]:
+                    pix += 1
+                elif is_stereo[lyr]:
+                    stereo += 1
+                    if lyr == prev:
+                        double_stereo = lyr
+                else:
+                    mono += 1
+                    if prev_stereo and lyr == prev - 1:
+                        matched += 1
+                    elif lyr == prev and lyr == double_stereo - 1:
+                        matched += 1
+                prev = lyr
+                prev_stereo = stereo
+        enhits = pix + 100 * stereo + 10000 * mono + 1000000 * matched
+        # nLayersByTypeEncoded
+        pix = stereo = mono = matched = 0
+        prev, prev_stereo = -1, 0
+        for idx, lyr in back:
+            if lyr >= 0 and (idx >= 0 or idx == -9) and lyr != prev:
+                if is_pix[lyr]:
+                    pix += 1
+                elif is_stereo[lyr]:
+                    stereo += 1
+                else:
+                    mono += 1
+                    if prev_stereo and lyr == prev - 1:
+                        matched += 1
+                prev = lyr
+                prev_stereo = stereo
+        enlyrs = pix + 100 * stereo + 10000 * mono + 1000000 * matched
+
+        def tot_match(e):
+            return e % 100 + (e // 100) % 100 + (e // 10000) % 100 - e // 1000000
+
+        invpt = par[i, 3]
+        ad0 = abs(d0[i])
+        theta = par[i, 5]
+        thetasym = abs(f(theta - pi_over_2))
+        red = 2 if nseed4 <= 5 else 3
+        m = 0
+        # qfilter_nan_n_silly: hasNanNSillyValues over the packed lower triangle.
+        silly = False
+        k = 0
+        for a in range(6):
+            for b in range(a + 1):
+                v = err[i, k]
+                if (a == b and v < 0) or not np.isfinite(v):
+                    silly = True
+                k += 1
+        m |= (not silly) << 0
+        m |= (nfound - red >= min_hits) << 1
+        m |= (nfound >= min_hits) << 2
+        npixhits, npixlyrs, nmatlyrs = enhits % 100, enlyrs % 100, tot_match(enlyrs)
+        ends_pix = llyr in (2, 18, 45)
+        last_pix = (0 <= lplyr < 3) or (18 <= lplyr < 20) or (45 <= lplyr < 47)
+        invptmin = f(1.43)
+        d0max = f(0.1)
+        fail = (((npixhits <= 3 or npixlyrs <= 3) and ends_pix
+                 and (invpt < invptmin or (invpt >= invptmin and ad0 > d0max)))
+                or ((npixlyrs <= 3 and nmatlyrs <= 6) and last_pix and llyr != lplyr
+                    and ad0 > d0max))
+        m |= (not fail) << 3
+        m |= (not ((nfound <= 6 or nul <= 6) and ad0 > d0max)) << 4
+        nlyrs, nhits = tot_match(enlyrs), tot_match(enhits)
+        iptm = f(1.11)
+        fwd = (((nfound - red >= 4 and invpt < iptm)
+                or (nfound - red >= 3 and invpt > iptm and thetasym <= f(1.11))
+                or (nfound - red >= 4 and invpt > iptm and thetasym > f(1.11)))
+               and not ((nlyrs <= 4 or nhits <= 4) and ad0 > f(0.05) and invpt < iptm))
+        m |= fwd << 5
+        bkwd = not ((nlyrs <= 3 or nhits <= 3)
+                    or ((nlyrs <= 4 or nhits <= 4)
+                        and (invpt < iptm or (thetasym > f(0.80) and ad0 > d0max)))
+                    or ((nlyrs <= 6 or nhits <= 6)
+                        and (invpt > iptm and thetasym > f(1.11) and ad0 > d0max)))
+        m |= bkwd << 6
+        out[i] = m
+    return out
+
+
+def _squash_phi_minimal(phi):
+    f = np.float32
+    two_pi, pi = f(2.0 * np.pi), f(np.pi)
+    return f(phi - two_pi) if phi >= pi else (f(phi + two_pi) if phi < -pi else phi)
+
+
+DR2_SUM = lambda a, b: _fma32(a, a, np.float32(b * b))  # noqa: E731
+
+
+def restate_dups(mode, tracks, algo=0, frac=0.24, drth=(0.002, 0.004, 0.008)):
+    """Pure-Python restatement of the duplicate removal on the same inputs as
+    ref_dups: find_duplicates_sharedhits_pixelseed (MkStdSeqs.cc:510-603),
+    find_duplicates_sharedhits (:456-508) or find_duplicates (:334-423), in
+    float32; every pair i < j is tested (a flag set earlier does not stop a
+    track from marking others) and of a duplicate pair the lower score loses
+    (the first track on a tie). dphi^2 + d^2 is formed as the reference
+    build contracts it: the first product fused, the second as addend."""
+    f = np.float32
+    n = len(tracks["chg"])
+    par = np.asarray(tracks["par"], np.float32).reshape(n, 6)
+    score = np.asarray(tracks["score"], np.float32)
+    label = np.asarray(tracks["label"], np.int32)
+    nfound = np.asarray(tracks["nfound"], np.int32)
+    hits = [[(int(tracks["hit_idx"][i][k]), int(tracks["hit_lyr"][i][k]))
+             for k in range(int(tracks["nh"][i]))] for i in range(n)]
+    tan = lambda v: _libm_f32("tanf", [v])[0]  # noqa: E731
+    log = lambda v: _libm_f32("logf", [v])[0]  # noqa: E731
+    cth = [f(f(1.0) / tan(par[i, 5])) for i in range(n)]
+    dup = np.zeros(n, bool)
+    if mode == 3:
+        return np.ones(n, np.int32)
+
+    def mark(i, j):
+        dup[j if score[i] > score[j] else i] = True
+
+    def shared(i, j):
+        cnt = first = 0
+        for a, (ia, la) in enumerate(hits[i]):
+            if ia < 0:
+                continue
+            for b, (ib, lb) in enumerate(hits[j]):
+                if ib < 0:
+                    continue
+                if la == lb and ia == ib:
+                    cnt += 1
+                    if a == 0 and b == 0:
+                        first += 1
+        return cnt, first
+
+    if mode in (0, 1):
+        dc, do, dfw = (f(v) for v in drth)
+        for i in range(n):
+            phi1, ipt1, c1 = par[i, 4], par[i, 3], cth[i]
+            for j in range(i + 1, n):
+                if mode == 0 and label[i] == label[j]:
+                    continue
+                dcth = abs(f(cth[j] - c1))
+                dphi = abs(_squash_phi_minimal(f(phi1 - par[j, 4])))
+                if mode == 1:
+                    if dcth > 1.0 or dphi > 1.0:
+                        continue
+                else:
+                    if dcth > f(0.37) or dphi > f(0.37):
+                        continue
+                    max_dr2 = f(dc * dc)
+                    if abs(c1) > f(6.05):
+                        max_dr2 = f(dfw * dfw)
+                    elif abs(c1) > f(1.99):
+                        max_dr2 = f(do * do)
+                    if DR2_SUM(dphi, dcth) < max_dr2:
+                        mark(i, j)
+                        continue
+                    if abs(f(par[j, 3] - ipt1)) > f(1.8):
+                        continue
+                cnt, first = shared(i, j)
+                mf = min(nfound[i], nfound[j])
+                if f(cnt - first) >= f(f(mf - first) * f(frac)):
+                    mark(i, j)
+    else:
+        eta = [f(f(-1.0) * log(tan(f(par[i, 5] / f(2.0))))) for i in range(n)]
+        pt = [abs(f(f(1.0) / par[i, 3])) for i in range(n)]
+        for i in range(n - 1):
+            if algo in (9, 10):
+                continue
+            for j in range(i + 1, n):
+                if label[i] == label[j]:
+                    continue
+                deta = abs(f(eta[j] - eta[i]))
+                if deta > f(0.05):
+                    continue
+                dphi = abs(_squash_phi_minimal(f(par[i, 4] - par[j, 4])))
+                if dphi > f(0.25):
+                    continue
+                max_dr2 = f(f(0.0025) * f(0.0025))
+                if abs(eta[i]) > f(2.5):
+                    max_dr2 = f(max_dr2 * f(16.0))
+                elif abs(eta[i]) > f(1.44):
+                    max_dr2 = f(max_dr2 * f(9.0))
+                if DR2_SUM(dphi, deta) < max_dr2:
+                    mark(i, j)
+                    continue
+                if pt[i] == 0 or pt[j] == 0:
+                    continue
+                if abs(f(f(f(1.0) / pt[j]) - f(f(1.0) / pt[i]))) < f(0.5):
+                    mine = set(hits[i])
+                    nsh = sum(1 for h in hits[j] if h[0] >= 0 and h in mine)
+                    mf = min(nfound[i], nfound[j])
+                    with np.errstate(divide="ignore", invalid="ignore"):
+                        fr = f(f(nsh) / f(mf))
+                    if fr < f(0.75):
+                        continue
+                    mark(i, j)
+    return (~dup).astype(np.int32)
+
+
+def ref_cms2017_iteration(reflib, it):
+    """The selection settings of CMS-2017 iteration `it` as the reference's
+    geometry plugin sets them: dict algorithm, quality_filter,
+    dupclean_tight, min_hits_qf, frac_shared_hits, drth (3)."""
+    lib = reflib.lib
+    lib.ref_cms2017_iteration.restype = ctypes.c_int
+    lib.ref_cms2017_iteration.argtypes = [ctypes.c_int, _i32p, _f32p]
+    iv = np.zeros(4, np.int32)
+    fv = np.zeros(4, np.float32)
+    if lib.ref_cms2017_iteration(int(it), iv, fv) != 0:
+        raise IndexError(it)
+    return dict(algorithm=int(iv[0]), quality_filter=bool(iv[1]), dupclean_tight=bool(iv[2]),
+                min_hits_qf=int(iv[3]), frac_shared_hits=float(fv[0]),
+                drth=tuple(float(x) for x in fv[1:]))

@@ -63,6 +63,20 @@ int g_seed_hit_stride = 4;
 // (qfilter_nan_n_silly, export_best_comb_cands(.., true),
 // find_and_remove_duplicates) and marks the surviving seeds here (by label).
 int* g_keep_out = nullptr;
+// Quality filters ref_find applies with MkBuilder::filter_comb_cands, as
+// run_OneIteration does (mkFit/buildtestMPlex.cc:676-719): after the clone
+// engine (g_qf_pre) and after the backward fit / search (g_qf_post); -1 =
+// none; kinds in the order of qfilter_by_kind.
+int g_qf_pre = -1, g_qf_post = -1, g_qf_min_hits = 0;
+float g_bs_x = 0.f, g_bs_y = 0.f;
+// Duplicate removal of the output selection (find_and_remove_duplicates,
+// mkFit/MkStdSeqs.cc:605-630, by the branch it takes): 0
+// find_duplicates_sharedhits_pixelseed, 1 find_duplicates_sharedhits,
+// 2 find_duplicates + remove_duplicates, 3 none (do_remove_duplicates off).
+int g_dup_mode = 0;
+// Duplicate parameters of the selection replacing iteration 0's when >= 0:
+// fracSharedHits, drth_central, drth_obarrel, drth_forward.
+float g_dup_params[4] = {-1.f, -1.f, -1.f, -1.f};
 
 void set_material(const float* rl_grid, const float* xi_grid) {
   if (rl_grid && xi_grid) {
@@ -195,6 +209,53 @@ void ensure_cms2017() {
   g_cms2017_loaded = true;
 }
 
+// The StdSeq quality filters (mkFit/MkStdSeqs.h:39-148) by code: 0
+// qfilter_nan_n_silly, 1 qfilter_n_hits, 2 qfilter_n_hits_pixseed,
+// 3 qfilter_n_layers, 4 qfilter_n_layers_pixelLess, 5 qfilter_pixelLessFwd,
+// 6 qfilter_pixelLessBkwd.
+bool qfilter_by_kind(const TrackCand& t, int kind, int min_hits, const BeamSpot& bs) {
+  const TrackerInfo& ti = Config::TrkInfo;
+  switch (kind) {
+    case 0: return StdSeq::qfilter_nan_n_silly(t);
+    case 1: return StdSeq::qfilter_n_hits(t, min_hits);
+    case 2: return StdSeq::qfilter_n_hits_pixseed(t, min_hits);
+    case 3: return StdSeq::qfilter_n_layers(t, bs, ti);
+    case 4: return StdSeq::qfilter_n_layers_pixelLess(t, bs);
+    case 5: return StdSeq::qfilter_pixelLessFwd(t, bs, ti);
+    case 6: return StdSeq::qfilter_pixelLessBkwd(t, bs, ti);
+  }
+  return true;
+}
+
+constexpr int kNumQFilters = 7;
+
+// MkBuilder::filter_comb_cands with one of the filters. The reference reads
+// front() of every comb candidate, so an empty one is refused (-3) rather
+// than read.
+int apply_qfilter(RefBuilder& b, int kind) {
+  EventOfCombCandidates& eocc = b.eocc();
+  for (int i = 0; i < eocc.m_size; ++i)
+    if (eocc[i].empty()) return -3;
+  BeamSpot bs;
+  bs.x = g_bs_x;
+  bs.y = g_bs_y;
+  b.filter_comb_cands([&](const TrackCand& t) { return qfilter_by_kind(t, kind, g_qf_min_hits, bs); });
+  return 0;
+}
+
+// find_and_remove_duplicates by branch (g_dup_mode codes).
+void remove_dups(TrackVec& out, int mode, const IterationParams& p) {
+  if (mode == 0)
+    StdSeq::find_duplicates_sharedhits_pixelseed(out, p.fracSharedHits, p.drth_central, p.drth_obarrel,
+                                                 p.drth_forward);
+  else if (mode == 1)
+    StdSeq::find_duplicates_sharedhits(out, p.fracSharedHits);
+  else if (mode == 2) {
+    StdSeq::find_duplicates(out);
+    StdSeq::remove_duplicates(out);
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -217,6 +278,113 @@ void ref_set_seed_hit_stride(int w) { g_seed_hit_stride = w > 0 ? w : 4; }
 // candidate survives run_OneIteration's output selection
 // (mkFit/buildtestMPlex.cc:721-731), 0 otherwise; NULL switches it off.
 void ref_set_select_output(int* keep) { g_keep_out = keep; }
+
+// ref_find: quality filters applied with filter_comb_cands after the clone
+// engine (pre) and after the backward fit / search (post), by
+// qfilter_by_kind code (-1 none); min_hits for qfilter_n_hits*, the beam
+// spot for the d0 cuts. dup_mode picks the duplicate removal of the output
+// selection (0 pixelseed, 1 sharedhits, 2 find_duplicates, 3 none).
+void ref_set_iteration_filters(int pre, int post, int min_hits, float bs_x, float bs_y, int dup_mode,
+                               const float* dup_params) {
+  for (int k = 0; k < 4; ++k) g_dup_params[k] = dup_params ? dup_params[k] : -1.f;
+  g_qf_pre = pre;
+  g_qf_post = post;
+  g_qf_min_hits = min_hits;
+  g_bs_x = bs_x;
+  g_bs_y = bs_y;
+  g_dup_mode = dup_mode;
+}
+
+// The quality filters on candidates given as exported hit lists (hits in
+// chain order, oldest first, missing-hit entries included). Each one is
+// rebuilt as the clone engine holds it: CombCandidate::ImportSeed of a seed
+// made of the first nseed[i] entries (which sets the 4-bit seed-hit count),
+// then TrackCand::addHitIdx for the rest. par[n][6], err[n][21], chg[n],
+// ntot[n], hit_idx / hit_lyr[n][w]. out[i] bit k: filter k (qfilter_by_kind
+// code) passes.
+int ref_qfilters(int n, const float* par, const float* err, const int* chg, const int* nseed,
+                 const int* ntot, const int* hit_idx, const int* hit_lyr, int w, int min_hits,
+                 float bs_x, float bs_y, int* out) {
+  ensure_cms2017();
+  if (n <= 0) return 0;
+  EventOfCombCandidates eocc;
+  eocc.Reset(n, 1, 2 * w);
+  BeamSpot bs;
+  bs.x = bs_x;
+  bs.y = bs_y;
+  for (int i = 0; i < n; ++i) {
+    if (nseed[i] > ntot[i] || ntot[i] > w) return -1;
+    TrackState ts;
+    for (int k = 0; k < 6; ++k) ts.parameters[k] = par[i * 6 + k];
+    for (int k = 0; k < 21; ++k) ts.errors.Array()[k] = err[i * 21 + k];
+    ts.charge = chg[i];
+    Track seed(ts, 0.f, i, 0, nullptr);
+    for (int k = 0; k < nseed[i]; ++k) seed.addHitIdx(hit_idx[i * w + k], hit_lyr[i * w + k], 0.f);
+    eocc.InsertSeed(seed, 0);
+    TrackCand& tc = eocc[i].front();
+    for (int k = nseed[i]; k < ntot[i]; ++k) tc.addHitIdx(hit_idx[i * w + k], hit_lyr[i * w + k], 0.f);
+    int m = 0;
+    for (int q = 0; q < kNumQFilters; ++q)
+      if (qfilter_by_kind(tc, q, min_hits, bs)) m |= 1 << q;
+    out[i] = m;
+  }
+  return 0;
+}
+
+// Duplicate removal of run_OneIteration's output on exported tracks (hits
+// without missing entries), by g_dup_mode code: par[n][6], chg, score,
+// label, nfound, nh[n], hit_idx / hit_lyr[n][w]; every track has algorithm
+// `algo`. The parameters are iteration 0's duplicate parameters with frac
+// and the three dR thresholds replaced. keep[i]: 1 when track i survives.
+int ref_dups(int mode, int n, const float* par, const int* chg, const float* score, const int* label,
+             int algo, const int* nfound, const int* nh, const int* hit_idx, const int* hit_lyr, int w,
+             float frac, float drth_c, float drth_ob, float drth_fw, int* keep) {
+  ensure_cms2017();
+  TrackVec tv;
+  tv.reserve(n);
+  for (int i = 0; i < n; ++i) {
+    if (nh[i] > w) return -1;
+    TrackState ts;
+    for (int k = 0; k < 6; ++k) ts.parameters[k] = par[i * 6 + k];
+    ts.charge = chg[i];
+    Track t(ts, 0.f, label[i], 0, nullptr);
+    t.resizeHits(nh[i], nfound[i]);
+    for (int k = 0; k < nh[i]; ++k) t.setHitIdxAtPos(k, HitOnTrack{hit_idx[i * w + k], hit_lyr[i * w + k]});
+    t.setScore(score[i]);
+    t.setAlgoint(algo);
+    // The position rides in chi2, which no duplicate test reads.
+    t.setChi2((float)i);
+    tv.push_back(t);
+  }
+  IterationParams p = Config::ItrInfo[0].m_params;
+  p.fracSharedHits = frac;
+  p.drth_central = drth_c;
+  p.drth_obarrel = drth_ob;
+  p.drth_forward = drth_fw;
+  remove_dups(tv, mode, p);
+  std::fill(keep, keep + n, 0);
+  for (const Track& t : tv) keep[(int)t.chi2()] = 1;
+  return 0;
+}
+
+// The selection settings of CMS-2017 iteration `it` (Geoms/CMS-2017.cc):
+// iv = {track algorithm, requires_quality_filter, requires_dupclean_tight,
+// minHitsQF}, fv = {fracSharedHits, drth_central, drth_obarrel,
+// drth_forward}.
+int ref_cms2017_iteration(int it, int* iv, float* fv) {
+  ensure_cms2017();
+  if (it < 0 || it >= (int)Config::ItrInfo.m_iterations.size()) return -1;
+  const IterationConfig& c = Config::ItrInfo[it];
+  iv[0] = c.m_track_algorithm;
+  iv[1] = c.m_requires_quality_filter;
+  iv[2] = c.m_requires_dupclean_tight;
+  iv[3] = c.m_params.minHitsQF;
+  fv[0] = c.m_params.fracSharedHits;
+  fv[1] = c.m_params.drth_central;
+  fv[2] = c.m_params.drth_obarrel;
+  fv[3] = c.m_params.drth_forward;
+  return 0;
+}
 
 // Geometry export sizes: n_layers, n_regions, max plan length.
 int ref_cms2017_sizes(int* n_layers, int* n_regions, int* max_plan) {
@@ -375,6 +543,7 @@ int ref_find(int n_layers_in, const int* layer_begin, const float* hpos, const f
     builder.find_tracks_load_seeds(seeds);
     const double t0 = now_s();
     builder.FindTracksCloneEngine();
+    if (g_qf_pre >= 0 && apply_qfilter(builder, g_qf_pre)) return -3;
     if (g_backward_search) {
       // run_OneIteration with m_backward_search (mkFit/buildtestMPlex.cc:700-714).
       builder.CompactifyHitStorageForBestCand(itconf.m_backward_drop_seed_hits,
@@ -386,6 +555,7 @@ int ref_find(int n_layers_in, const int* layer_begin, const float* hpos, const f
     } else if (g_backward_fit) {
       builder.BackwardFit();
     }
+    if (g_qf_post >= 0 && apply_qfilter(builder, g_qf_post)) return -3;
     best = std::min(best, now_s() - t0);
     if (r + 1 < std::max(1, repeat)) builder.end_event();
   }
@@ -404,7 +574,12 @@ int ref_find(int n_layers_in, const int* layer_begin, const float* hpos, const f
       if (!StdSeq::qfilter_nan_n_silly(t)) continue;
       out.emplace_back(t.exportTrack(true));
     }
-    StdSeq::find_and_remove_duplicates(out, itconf);
+    IterationParams dp = itconf.m_params;
+    if (g_dup_params[0] >= 0.f) dp.fracSharedHits = g_dup_params[0];
+    if (g_dup_params[1] >= 0.f) dp.drth_central = g_dup_params[1];
+    if (g_dup_params[2] >= 0.f) dp.drth_obarrel = g_dup_params[2];
+    if (g_dup_params[3] >= 0.f) dp.drth_forward = g_dup_params[3];
+    remove_dups(out, g_dup_mode, dp);
     for (const Track& t : out)
       if (t.label() >= 0 && t.label() < ns) g_keep_out[t.label()] = 1;
   }
