@@ -618,3 +618,37 @@ def with_duplicate_seeds(ev, frac=0.25, seed=7, chain_frac=0.3):
         hit_layer=np.ascontiguousarray(np.array(sel(hl)), np.int32),
         hit_index=np.ascontiguousarray(np.array(sel(hi)), np.int32),
         src=np.array(sel(src), np.int32))
+
+
+def without_first_seed_hit(ev):
+    """The event with every seed's innermost hit taken out of the seed
+    (three-hit seeds become hit pairs): the backward search then has that
+    layer to find again, and hit-count cuts meet seeds of two hits."""
+    d = dict(ev.__dict__)
+    hl, hi = ev.seed_hit_layer.copy(), ev.seed_hit_index.copy()
+    hl[:, :-1], hi[:, :-1] = ev.seed_hit_layer[:, 1:], ev.seed_hit_index[:, 1:]
+    hl[:, -1] = hi[:, -1] = -1
+    d.update(seed_hit_layer=hl, seed_hit_index=hi, seed_nhits=ev.seed_nhits - 1)
+    return CmsEvent(**d)
+
+
+def thinned(ev, frac, seed):
+    """The event with a fraction `frac` of its non-pixel hits removed (an
+    inefficient strip tracker): candidates come out short and with holes.
+    Seeds keep their pixel hits and indices."""
+    from .geometry import cms2017
+    rng = np.random.default_rng(seed)
+    is_pix = cms2017().field("is_pix") > 0.5
+    lb = np.asarray(ev.layer_begin)
+    keep = np.ones(ev.n_hits, bool)
+    for lyr in range(ev.n_layers):
+        if not is_pix[lyr]:
+            keep[lb[lyr]:lb[lyr + 1]] = rng.random(lb[lyr + 1] - lb[lyr]) >= frac
+    counts = [int(keep[lb[i]:lb[i + 1]].sum()) for i in range(ev.n_layers)]
+    d = dict(ev.__dict__)
+    d["layer_begin"] = np.concatenate([[0], np.cumsum(counts)]).astype(np.int32)
+    for k in ("hit_pos", "hit_err"):
+        d[k] = np.ascontiguousarray(getattr(ev, k)[:, keep])
+    for k in ("hit_detid", "hit_cpcm", "hit_mc"):
+        d[k] = np.ascontiguousarray(getattr(ev, k)[keep])
+    return CmsEvent(**d)

@@ -330,18 +330,6 @@ def test_step_profile(gpu_ctx):
     assert prof["clone"].shape == (fnd.cfg.max_steps,) and float(prof["propagate"].sum()) > 0
 
 
-def without_first_seed_hit(ev):
-    """The event with every seed's innermost hit taken out of the seed: the
-    backward search then has that layer to find again."""
-    from mkfit_b200.synth import CmsEvent
-    d = dict(ev.__dict__)
-    hl, hi = ev.seed_hit_layer.copy(), ev.seed_hit_index.copy()
-    hl[:, :-1], hi[:, :-1] = ev.seed_hit_layer[:, 1:], ev.seed_hit_index[:, 1:]
-    hl[:, -1] = hi[:, -1] = -1
-    d.update(seed_hit_layer=hl, seed_hit_index=hi, seed_nhits=ev.seed_nhits - 1)
-    return CmsEvent(**d)
-
-
 @pytest.mark.parametrize("n_tracks,seed,noise,drop_first", [(800, 61, 0.01, False),
                                                             (2500, 62, 0.02, False),
                                                             (1500, 63, 0.02, True)])
@@ -355,7 +343,7 @@ def test_backward_search_matches_reference(gpu_ctx, reflib, n_tracks, seed, nois
     agree, the states agree within the backward fit's tolerance."""
     ev = synth.gen_cms_event(n_tracks, seed=seed, noise_frac=noise)
     if drop_first:
-        ev = without_first_seed_hit(ev)
+        ev = synth.without_first_seed_hit(ev)
     ref = ref_find(reflib, ev, max_cands=M, chi2_cut=30.0, zero_c2=True, backward_search=True)
     ref_fit = ref_find(reflib, ev, max_cands=M, chi2_cut=30.0, zero_c2=True, backward_fit=True)
     fnd = Finder(gpu_ctx, FindConfig(max_cands=M, chi2_cut=30.0, zero_c2=True))
@@ -452,7 +440,7 @@ def test_repeat_runs_identical(gpu_ctx):
     """A run leaves nothing behind that the next one reads: the same event
     run twice, and uploaded again and run, gives the same candidates (seeds
     with two hits included, whose arena holds fewer than three seed nodes)."""
-    ev = without_first_seed_hit(synth.gen_cms_event(1200, seed=64, noise_frac=0.02))
+    ev = synth.without_first_seed_hit(synth.gen_cms_event(1200, seed=64, noise_frac=0.02))
     fnd = Finder(gpu_ctx, FindConfig(max_cands=M, chi2_cut=30.0, zero_c2=True))
     outs = []
     fnd.upload(ev)

@@ -302,7 +302,7 @@ def test_device_filters_match_reference(gpu_ctx, reflib, stage):
     cosf are off by one ulp for ~1% of angles)."""
     from mkfit_b200 import synth
     from oracle.oracle import d0_beam_spot
-    ev = synth.gen_cms_event(2500, seed=81, noise_frac=0.02)
+    ev = synth.thinned(synth.gen_cms_event(2500, seed=81, noise_frac=0.02), 0.6, 81)
     fnd = _finder(gpu_ctx)
     fnd.upload(ev)
     fnd.run()
@@ -315,7 +315,7 @@ def test_device_filters_match_reference(gpu_ctx, reflib, stage):
     cands = _take(c, has)
     nseed = ev.seed_nhits[has]
     fails = np.zeros(len(QF_KINDS), int)
-    for beam in ((0.0, 0.0), (0.08, -0.05)):
+    for beam in ((0.0, 0.0), (0.08, -0.05), (0.3, 0.2)):
         d0, radius = d0_beam_spot(cands["par"].T, cands["chg"], beam)
         gap = np.min([np.abs(np.abs(d0) - np.float32(cut)) for cut in QF_D0_CUTS], axis=0)
         near = gap < 2e-6 * radius + 1e-6
@@ -329,6 +329,7 @@ def test_device_filters_match_reference(gpu_ctx, reflib, stage):
                 assert near[bad].all(), f"{name} beam {beam} min_hits {min_hits}: {len(bad)} differ"
                 fails[k] += int((r == 0).sum())
     print(f"\nfilters ({stage}): failing candidates per filter {dict(zip(QF_KINDS, fails))}")
+    # Every filter but the NaN / silly one fails some candidates.
     assert fails[1:].min() > 0
 
 
@@ -401,7 +402,9 @@ def test_iteration_selection_matches_reference(gpu_ctx, reflib, it):
     """run_OneIteration's steps after the clone engine with the selection of
     CMS-2017 iteration `it` (its filter with removal after the finding, the
     backward fit over the remaining seeds, its filter after the backward
-    fit, duplicate removal) on the iteration-0 finding, against the same
+    fit, duplicate removal) on the iteration-0 finding of an event with half
+    its strip hits removed (short candidates, which the filters drop),
+    against the same
     sequence run by the reference: the same seeds removed and kept for
     >= 99% of the seeds (the rest are finding near-ties)."""
     from mkfit_b200 import synth
@@ -409,7 +412,11 @@ def test_iteration_selection_matches_reference(gpu_ctx, reflib, it):
     from oracle.oracle import ref_find
     sel = ITERATION_SELECTION[it]
     beam = (0.02, -0.01)
-    ev = synth.gen_cms_event(1500, seed=100 + it, noise_frac=0.02)
+    ev = synth.thinned(synth.gen_cms_event(1500, seed=100 + it, noise_frac=0.02), 0.5, 100 + it)
+    if it == 9:
+        # pixelPairStep seeds are hit pairs: qfilter_n_hits_pixseed(3) drops
+        # the ones that found nothing.
+        ev = synth.without_first_seed_hit(ev)
     ref = ref_find(reflib, ev, max_cands=M, chi2_cut=30.0, zero_c2=True, backward_fit=True,
                    select=True, qf_pre=-1 if sel["pre"] is None else sel["pre"],
                    qf_post=-1 if sel["post"] is None else sel["post"], qf_min_hits=sel["min_hits"],
