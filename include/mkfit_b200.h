@@ -427,6 +427,20 @@ int mkfg_find_backward_fit(mkfg_context* ctx, const int32_t* bkfit_last, uint32_
  * hits found inward first. The low-pT looper stop does not apply (it is a
  * forward-search rule). Synchronizes the context stream. */
 int mkfg_find_backward_search(mkfg_context* ctx, const int32_t* bksearch_pickup);
+/* IterationParams of a search (the fields of mkFit/IterationConfig.h:96-104
+ * the clone engine reads). */
+typedef struct {
+  int32_t max_cands_per_seed, max_holes_per_cand, max_consec_holes;
+  float chi2_cut_min, chi2_cut_overlap, pt_cut_overlap;
+} mkfg_search_params;
+/* mkfg_find_backward_search with the iteration's own backward-search
+ * parameters (IterationConfig::m_backward_params: pixelLessStep and
+ * tobTecStep allow holes there, mkFit/Geoms/CMS-2017.cc
+ * SetupBackwardSearch_Iter7/8); NULL = the forward parameters. Seed hits
+ * are kept (m_backward_drop_seed_hits off, as in every CMS-2017
+ * iteration). */
+int mkfg_find_backward_search_with(mkfg_context* ctx, const int32_t* bksearch_pickup,
+                                   const mkfg_search_params* params);
 /* Output selection of run_OneIteration after a run (and backward fit):
  * every seed's best candidate is dropped if its covariance has a negative
  * diagonal or a non-finite element (StdSeq::qfilter_nan_n_silly with

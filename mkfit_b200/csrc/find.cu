@@ -894,6 +894,10 @@ struct Finder {
   cudaGraphExec_t graph = nullptr;  // captured run sequence of the current upload
   int fused_w = 16;                 // seeds per block of the fused form
   int max_nq = 1;                   // largest number of q bins of a layer
+  // Layer steps a backward search can take (the longest plan less its
+  // first entry); per-step buffers and the hit-on-track arena hold a
+  // forward run plus a backward search of that length.
+  int bks_steps = 0;
   int64_t last_chi2_evals = 0, last_seeds_cloned = 0;
   // Per-launch device times of the last timed run: [max_steps][5] for the
   // layer-step kernels (activate, propagate, chi2, clone, update).
@@ -1023,6 +1027,7 @@ extern "C" int mkfg_finder_setup(mkfg_context* ctx, const mkfg_find_config* cfg)
   H.n_layers = cfg->n_layers;
   H.n_regions = cfg->n_regions;
   int max_steps = 0;
+  f->bks_steps = 0;
   for (int r = 0; r < cfg->n_regions; ++r) {
     H.plan_len[r] = cfg->plan_len[r];
     H.pickup[r] = cfg->pickup[r];
@@ -1035,6 +1040,7 @@ extern "C" int mkfg_finder_setup(mkfg_context* ctx, const mkfg_find_config* cfg)
       H.plan[r][i] = l;
     }
     max_steps = std::max(max_steps, cfg->plan_len[r] - cfg->pickup[r] - 1);
+    f->bks_steps = std::max(f->bks_steps, cfg->plan_len[r] - 1);
   }
   H.max_steps = max_steps;
   H.max_cands = cfg->max_cands_per_seed;
@@ -1305,9 +1311,12 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   f->ev.srank = dh.srank;
   // ---- seeds, candidates, scratch, records, arena
   const int SC = SS * kSlots;
-  const int max_steps = f->host_cfg.max_steps;
+  // Per-step buffers cover the forward run or a backward search, whichever
+  // is longer; the arena holds both (the search appends to the run's nodes).
+  const int max_steps = std::max(f->host_cfg.max_steps, f->bks_steps);
   const int M = f->host_cfg.max_cands;
-  const int hot_cap = ((MKFG_MAX_SEED_HITS + 4 + max_steps * (2 * M + 3)) + 31) / 32 * 32;
+  const int hot_cap =
+      ((MKFG_MAX_SEED_HITS + 4 + (f->host_cfg.max_steps + f->bks_steps) * (2 * M + 3)) + 31) / 32 * 32;
   {
     const size_t need = 3 * rounded(4 * (size_t)SC) * 37 + rounded(4 * (size_t)SS) * 47 + 4096;
     if ((rc = f->cands.ensure(need))) return rc;
@@ -1799,11 +1808,19 @@ extern "C" int mkfg_find_autotune(mkfg_context* ctx, int32_t* seeds_per_block, f
 }
 
 extern "C" int mkfg_find_backward_search(mkfg_context* ctx, const int32_t* bksearch_pickup) {
+  return mkfg_find_backward_search_with(ctx, bksearch_pickup, nullptr);
+}
+
+extern "C" int mkfg_find_backward_search_with(mkfg_context* ctx, const int32_t* bksearch_pickup,
+                                              const mkfg_search_params* params) {
   int rc = activate(ctx);
   if (rc) return rc;
   Finder* f = finder_of(ctx);
   MKFG_REQUIRE(f->configured && f->events_loaded, "no event uploaded");
   MKFG_REQUIRE(bksearch_pickup != nullptr, "null bksearch_pickup");
+  MKFG_REQUIRE(params == nullptr ||
+                   (params->max_cands_per_seed >= 1 && params->max_cands_per_seed <= kSlots),
+               "max_cands_per_seed must be in [1, %d]", kSlots);
   // The backward plans: for a region with a pickup index p, the forward
   // plan's entries p, p-1, ..., 0 (SteeringParams::make_iterator with
   // IT_BkwSearch, mkFit/SteeringParams.h:140-144), entry 0 being the pickup;
@@ -1820,6 +1837,16 @@ extern "C" int mkfg_find_backward_search(mkfg_context* ctx, const int32_t* bksea
   }
   H.max_steps = max_steps;
   H.looper_stop = 0;
+  if (params) {
+    // IterationConfig::m_backward_params (find_tracks_in_layers takes them
+    // for IT_BkwSearch, mkFit/MkBuilder.cc:1924-1926).
+    H.max_cands = params->max_cands_per_seed;
+    H.max_holes = params->max_holes_per_cand;
+    H.max_consec_holes = params->max_consec_holes;
+    H.chi2_cut_min = params->chi2_cut_min;
+    H.chi2_cut_overlap = params->chi2_cut_overlap;
+    H.pt_cut_overlap = params->pt_cut_overlap;
+  }
   if (!f->d_cfg_bks) MKFG_CUDA_TRY(cudaMalloc(&f->d_cfg_bks, sizeof(FindConfigDev)));
   cudaStream_t st = ctx->stream;
   MKFG_CUDA_TRY(cudaMemcpyAsync(f->d_cfg_bks, &H, sizeof(FindConfigDev), cudaMemcpyHostToDevice, st));
@@ -1836,10 +1863,12 @@ extern "C" int mkfg_find_backward_search(mkfg_context* ctx, const int32_t* bksea
     V.ninside = carve<int>(p, S);
     V.ntail = carve<int>(p, S);
   }
-  MKFG_REQUIRE(max_steps <= f->host_cfg.max_steps, "backward plan longer than the forward one");
-  const int n_work = 4 * (f->host_cfg.max_steps + 2);
-  MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.pair_count, 0, 4 * (size_t)(f->host_cfg.max_steps + 2), st));
-  MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.step_count, 0, 4 * (size_t)kCntN * (f->host_cfg.max_steps + 2), st));
+  // Per-step buffers were sized for the longest plan at upload.
+  MKFG_REQUIRE(max_steps <= std::max(f->host_cfg.max_steps, f->bks_steps),
+               "backward plan longer than the configured plans");
+  const int n_work = 4 * (max_steps + 2);
+  MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.pair_count, 0, 4 * (size_t)(max_steps + 2), st));
+  MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.step_count, 0, 4 * (size_t)kCntN * (max_steps + 2), st));
   MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.work, 0, 4 * (size_t)n_work, st));
   const StepGrids g = step_grids(f);
   k_bks_begin<<<(S + 127) / 128, 128, 0, st>>>(f->ev, f->d_cfg_bks, V);
@@ -1853,8 +1882,13 @@ extern "C" int mkfg_find_backward_search(mkfg_context* ctx, const int32_t* bksea
   k_merge<<<(S + 127) / 128, 128, 0, st>>>(f->ev, f->d_cfg_bks);
   k_bks_end<<<(S + 127) / 128, 128, 0, st>>>(f->ev, V);
   MKFG_CUDA_TRY(cudaGetLastError());
+  int flag_bits = 0;
+  MKFG_CUDA_TRY(cudaMemcpyAsync(&flag_bits, f->ev.err_flags, 4, cudaMemcpyDeviceToHost, st));
   // H is a host stack object read by the configuration copy.
   MKFG_CUDA_TRY(cudaStreamSynchronize(st));
+  if (flag_bits & kErrArena)
+    return set_error(MKFG_ERR_OVERFLOW, "hit-on-track arena overflow (capacity %d per seed)",
+                     f->ev.hot_cap);
   return MKFG_OK;
 }
 

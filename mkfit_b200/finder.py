@@ -31,6 +31,12 @@ class MkfgSelectConfig(ctypes.Structure):
         ("ep_use_hits", ctypes.c_int32)]
 
 
+class MkfgSearchParams(ctypes.Structure):
+    _fields_ = [("max_cands_per_seed", ctypes.c_int32), ("max_holes_per_cand", ctypes.c_int32),
+                ("max_consec_holes", ctypes.c_int32), ("chi2_cut_min", ctypes.c_float),
+                ("chi2_cut_overlap", ctypes.c_float), ("pt_cut_overlap", ctypes.c_float)]
+
+
 class MkfgQFilterConfig(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int32), ("min_hits", ctypes.c_int32),
                 ("beam_spot_x", ctypes.c_float), ("beam_spot_y", ctypes.c_float)]
@@ -118,6 +124,7 @@ def _bind(lib):
     lib.mkfg_find_hit_index.argtypes = [vp, ctypes.c_int32, vp, vp]
     lib.mkfg_find_run_timed.argtypes = [vp, vp]
     lib.mkfg_find_backward_search.argtypes = [vp, vp]
+    lib.mkfg_find_backward_search_with.argtypes = [vp, vp, ctypes.POINTER(MkfgSearchParams)]
     lib.mkfg_find_step_profile.argtypes = [vp, vp, vp]
     lib.mkfg_find_select.argtypes = [vp, ctypes.POINTER(MkfgSelectConfig), ctypes.c_int32, vp]
     lib.mkfg_find_filter.argtypes = [vp, ctypes.POINTER(MkfgQFilterConfig), ctypes.c_int32,
@@ -138,11 +145,13 @@ def _bind(lib):
 
 
 class FindConfig:
-    """Iteration-0 CMS-2017 configuration with the workload's overrides:
-    maxCandsPerSeed, chi2Cut_min and (zero_c2) a flat chi2 cut."""
+    """CMS-2017 finding configuration of one iteration (default
+    initialStep) with the workload's overrides: maxCandsPerSeed,
+    chi2Cut_min (None: the iteration's own) and (zero_c2) a flat chi2
+    cut."""
 
-    def __init__(self, geom=None, max_cands=6, chi2_cut=30.0, zero_c2=True):
-        g = geom or cms2017()
+    def __init__(self, geom=None, max_cands=6, chi2_cut=30.0, zero_c2=True, iteration=0):
+        g = geom or cms2017(iteration)
         self.geom = g
         desc = g.layer_desc.copy()
         if zero_c2:
@@ -153,6 +162,11 @@ class FindConfig:
         self.plan_len = np.ascontiguousarray(g.plan_len, np.int32)
         self.pickup = np.ascontiguousarray(g.pickup, np.int32)
         ip = g.iter_params
+        if max_cands is None:
+            max_cands = int(ip[0])
+        if chi2_cut is None:
+            chi2_cut = float(ip[3])
+        self.chi2_cut = float(chi2_cut)
         self.max_cands = int(max_cands)
         c = MkfgFindConfig()
         c.n_layers = g.n_layers
@@ -267,10 +281,19 @@ class Finder:
 
     def backward_search(self):
         """Backward search of every seed's backward-fitted best candidate
-        through the geometry's backward plans (mkfg_find_backward_search)."""
-        self._bks_pickup = np.ascontiguousarray(self.cfg.geom.bksearch_pickup, np.int32)
-        capi.check(self.lib.mkfg_find_backward_search(self.ctx.handle,
-                                                      self._bks_pickup.ctypes.data))
+        through the iteration's backward plans with its backward-search
+        parameters (m_backward_params; maxCandsPerSeed and the chi2 cut
+        follow this configuration's overrides, as the reference driver's
+        do) — mkfg_find_backward_search_with."""
+        g = self.cfg.geom
+        if int(g.bk_flags[0]):
+            raise NotImplementedError("backward search that drops the seed hits")
+        bk = g.bk_iter_params
+        self._bks_params = MkfgSearchParams(self.cfg.max_cands, int(bk[1]), int(bk[2]),
+                                            self.cfg.chi2_cut, float(bk[4]), float(bk[5]))
+        self._bks_pickup = np.ascontiguousarray(g.bksearch_pickup, np.int32)
+        capi.check(self.lib.mkfg_find_backward_search_with(
+            self.ctx.handle, self._bks_pickup.ctypes.data, ctypes.byref(self._bks_params)))
 
     KERNELS = ("reset", "activate", "propagate", "chi2", "clone", "update", "merge")
 

@@ -1,7 +1,9 @@
 """Writes mkfit_b200/geom/cms2017.npz: the CMS-2017 detector description and
-iteration-0 finding configuration, exported from the reference's own
-geometry plugin (Geoms/CMS-2017.cc, run in-process through the oracle
-build in oracle/_ref).
+the finding configuration of its ten iterations, exported from the
+reference's own geometry plugin (Geoms/CMS-2017.cc, run in-process through
+the oracle build in oracle/_ref). Iteration 0's arrays sit under their own
+names; every iteration's steering, search windows and parameters are also
+stacked under "it_<name>" (index = iteration).
 
     python mkfit_b200/geom/make_cms2017.py
 
@@ -20,7 +22,28 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from oracle.oracle import RefLib, cms2017_export  # noqa: E402
 
+# Arrays that depend on the iteration.
+ITER_KEYS = ("layer_desc", "plans", "plan_len", "pickup", "bkfit_last", "bksearch_pickup",
+             "region_order", "iter_params", "bk_iter_params", "bk_flags")
+N_ITERATIONS = 10
+
+
+def export_all(ref):
+    g = cms2017_export(ref, 0)
+    per = [cms2017_export(ref, it) for it in range(N_ITERATIONS)]
+    mp = max(e["plans"].shape[1] for e in per)
+    for k in ITER_KEYS:
+        rows = []
+        for e in per:
+            v = e[k]
+            if k == "plans" and v.shape[1] < mp:
+                v = np.pad(v, ((0, 0), (0, mp - v.shape[1])), constant_values=-1)
+            rows.append(v)
+        g["it_" + k] = np.stack(rows)
+    return g
+
+
 if __name__ == "__main__":
-    g = cms2017_export(RefLib())
+    g = export_all(RefLib())
     np.savez_compressed(os.path.join(HERE, "cms2017.npz"), **g)
     print("wrote", os.path.join(HERE, "cms2017.npz"))

@@ -280,7 +280,7 @@ def _next_crossing(st, rs, is_barrel, zmin, zmax, rin, rout, hole, hmin, hmax, p
 
 def gen_cms_event(n_tracks=800, seed=0xC0FFEE, geom=None, pt_range=(0.5, 50.0), eta_max=2.4,
                   noise_frac=0.01, noise_scale=None, vtx_sigma_xy=0.01, vtx_sigma_z=5.0,
-                  r_start=1.0, overlap_prob=0.05, strip_len=10.0):
+                  r_start=1.0, overlap_prob=0.05, strip_len=10.0, seed_layers=None, seed_hits=3):
     """Synthetic CMS-2017 event: helices with pT log-uniform in pt_range,
     |eta| < eta_max, transported through the layer table with a Highland
     multiple-scattering kick from the reference material grid at each
@@ -289,9 +289,10 @@ def gen_cms_event(n_tracks=800, seed=0xC0FFEE, geom=None, pt_range=(0.5, 50.0), 
     `strip_len` cm on the long axis) plus, with probability `overlap_prob`
     on strip layers, a second hit in the neighbouring module; noise hits at
     `noise_frac` of each layer's signal-hit count (times `noise_scale[l]`
-    when given) uniform in the layer's extent. Seeds: the first three pixel
-    hits of every track that has them, with the true state at the third hit
-    and a fixed diagonal covariance."""
+    when given) uniform in the layer's extent. Seeds: the first `seed_hits`
+    hits on seed layers (default the pixel layers; `seed_layers` a
+    per-layer boolean mask) of every track that has them, with the true
+    state at the last of them and a fixed diagonal covariance."""
     from .geometry import cms2017
     g = geom or cms2017()
     rng = np.random.default_rng(seed)
@@ -495,8 +496,9 @@ def gen_cms_event(n_tracks=800, seed=0xC0FFEE, geom=None, pt_range=(0.5, 50.0), 
     inv[perm] = np.arange(m)
     index_in_layer = inv - layer_begin[lay]
 
-    # Seeds: first three pixel hits (generation order) of each track.
-    sig_idx = np.nonzero((mc >= 0) & is_pix[lay] & (order < (1 << 40)))[0]
+    # Seeds: first seed_hits hits on seed layers (generation order) of each track.
+    seed_mask = is_pix if seed_layers is None else np.asarray(seed_layers, bool)
+    sig_idx = np.nonzero((mc >= 0) & seed_mask[lay] & (order < (1 << 40)))[0]
     sig_idx = sig_idx[np.lexsort((order[sig_idx], trk[sig_idx]))]
     seeds = []
     t_prev, cnt = -1, 0
@@ -505,21 +507,20 @@ def gen_cms_event(n_tracks=800, seed=0xC0FFEE, geom=None, pt_range=(0.5, 50.0), 
         t = int(trk[h])
         if t != t_prev:
             t_prev, cnt = t, 0
-        if cnt < 3:
+        if cnt < seed_hits:
             first3.setdefault(t, []).append(h)
         cnt += 1
-    seed_tracks = sorted(t for t, v in first3.items() if len(v) == 3)
+    seed_tracks = sorted(t for t, v in first3.items() if len(v) == seed_hits)
     ns = len(seed_tracks)
     spar = np.zeros((6, ns))
     serr = np.zeros((21, ns))
     schg = np.zeros(ns, np.int32)
-    snh = np.full(ns, 3, np.int32)
-    shl = np.full((ns, 4), -1, np.int32)
-    shi = np.full((ns, 4), -1, np.int32)
+    snh = np.full(ns, seed_hits, np.int32)
+    shl = np.full((ns, max(4, seed_hits)), -1, np.int32)
+    shi = np.full((ns, max(4, seed_hits)), -1, np.int32)
     for i, t in enumerate(seed_tracks):
         hs = first3[t]
-        h3 = hs[2]
-        Hh = H[h3]  # true crossing of the third seed hit (signal hits precede overlaps)
+        Hh = H[hs[-1]]  # true crossing of the last seed hit (signal hits precede overlaps)
         spar[:, i] = [Hh[2], Hh[3], Hh[4], 1.0 / Hh[7], Hh[5], Hh[6]]
         d = [0.01 ** 2, 0.01 ** 2, 0.01 ** 2, (0.05 / Hh[7]) ** 2, 0.005 ** 2, 0.005 ** 2]
         for k, (a, b) in enumerate(SYM6):

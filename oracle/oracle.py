@@ -317,11 +317,27 @@ def _load_find_api(lib):
                              [_i32p] * 5 + [_i32p, _i32p, ctypes.POINTER(ctypes.c_double)])
 
 
-def cms2017_export(reflib):
-    """CMS-2017 geometry + iteration-0 configuration from the reference's
-    own plugin (Geoms/CMS-2017.cc), as numpy arrays."""
+def _set_iteration(lib, it):
+    lib.ref_set_iteration.restype = ctypes.c_int
+    lib.ref_set_iteration.argtypes = [ctypes.c_int]
+    if lib.ref_set_iteration(int(it)) != 0:
+        raise IndexError(f"no iteration {it}")
+
+
+def cms2017_export(reflib, iteration=0):
+    """CMS-2017 geometry + the configuration of one iteration (layer plans,
+    search windows, iteration parameters) from the reference's own plugin
+    (Geoms/CMS-2017.cc), as numpy arrays."""
     lib = reflib.lib
     _load_find_api(lib)
+    _set_iteration(lib, iteration)
+    try:
+        return _cms2017_export(lib)
+    finally:
+        _set_iteration(lib, 0)
+
+
+def _cms2017_export(lib):
     nl, nr, mp = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
     lib.ref_cms2017_sizes(ctypes.byref(nl), ctypes.byref(nr), ctypes.byref(mp))
     nl, nr, mp = nl.value, nr.value, mp.value
@@ -334,6 +350,10 @@ def cms2017_export(reflib):
     lib.ref_cms2017_export(out["layer_desc"], out["plans"], out["plan_len"], out["pickup"],
                            out["bkfit_last"], out["bksearch_pickup"], out["region_order"],
                            out["iter_params"], out["flags"], out["eta"], out["rl"], out["xi"])
+    out["bk_iter_params"] = np.zeros(8, np.float32)
+    out["bk_flags"] = np.zeros(2, np.int32)
+    lib.ref_cms2017_backward_params.argtypes = [_f32p, _i32p]
+    lib.ref_cms2017_backward_params(out["bk_iter_params"], out["bk_flags"])
     return out
 
 
@@ -345,7 +365,7 @@ def _set_seed_stride(lib, seed_hit_layer):
 
 def ref_find(reflib, ev, max_cands=6, chi2_cut=30.0, zero_c2=True, repeat=1, backward_fit=False,
              select=False, backward_search=False, qf_pre=-1, qf_post=-1, qf_min_hits=0,
-             beam=(0.0, 0.0), dup_mode=0, dup_params=None):
+             beam=(0.0, 0.0), dup_mode=0, dup_params=None, iteration=0):
     """Reference clone-engine finding (find_tracks_load_seeds +
     FindTracksCloneEngine, then MkBuilder::BackwardFit when backward_fit,
     or CompactifyHitStorageForBestCand + BackwardFit + the backward search
@@ -357,9 +377,12 @@ def ref_find(reflib, ev, max_cands=6, chi2_cut=30.0, zero_c2=True, repeat=1, bac
     MkBuilder::filter_comb_cands after the clone engine / after the backward
     fit or search, as run_OneIteration does; dup_mode: the duplicate removal
     of the selection (DUP_MODES index) with dup_params (fracSharedHits,
-    drth central, obarrel, forward) replacing iteration 0's."""
+    drth central, obarrel, forward) replacing the iteration's. iteration:
+    the CMS-2017 iteration whose steering and parameters the finding uses
+    (max_cands, chi2_cut and zero_c2 still override)."""
     lib = reflib.lib
     _load_find_api(lib)
+    _set_iteration(lib, iteration)
     lib.ref_set_iteration_filters.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                               ctypes.c_float, ctypes.c_float, ctypes.c_int,
                                               ctypes.c_void_p]
@@ -400,6 +423,7 @@ def ref_find(reflib, ev, max_cands=6, chi2_cut=30.0, zero_c2=True, repeat=1, bac
     lib.ref_set_backward_search(0)
     lib.ref_set_select_output(None)
     lib.ref_set_iteration_filters(-1, -1, 0, 0.0, 0.0, 0, None)
+    _set_iteration(lib, 0)
     if rc != 0:
         raise RuntimeError(f"ref_find failed rc={rc}")
     o["seconds"] = secs.value

@@ -59,6 +59,9 @@ bool g_backward_fit = false;
 bool g_backward_search = false;
 // Row width of the seed-hit arrays the finding drivers take.
 int g_seed_hit_stride = 4;
+// CMS-2017 iteration whose configuration the geometry export and the
+// finding drivers use (Config::ItrInfo index).
+int g_iteration = 0;
 // When set, ref_find also runs the output selection of run_OneIteration
 // (qfilter_nan_n_silly, export_best_comb_cands(.., true),
 // find_and_remove_duplicates) and marks the surviving seeds here (by label).
@@ -270,6 +273,15 @@ void ref_set_backward_fit(int on) { g_backward_fit = on != 0; }
 // FindTracksCloneEngine(IT_BkwSearch), EndBkwSearch.
 void ref_set_backward_search(int on) { g_backward_search = on != 0; }
 
+// Iteration (0-9) whose configuration ref_cms2017_sizes / _export,
+// ref_find, ref_event_prep and ref_find_batch use; -1 if out of range.
+int ref_set_iteration(int it) {
+  ensure_cms2017();
+  if (it < 0 || it >= (int)Config::ItrInfo.m_iterations.size()) return -1;
+  g_iteration = it;
+  return 0;
+}
+
 // Row width of seed_hit_layer / seed_hit_index in ref_find, ref_event_prep
 // and ref_find_batch (default 4).
 void ref_set_seed_hit_stride(int w) { g_seed_hit_stride = w > 0 ? w : 4; }
@@ -389,7 +401,7 @@ int ref_cms2017_iteration(int it, int* iv, float* fv) {
 // Geometry export sizes: n_layers, n_regions, max plan length.
 int ref_cms2017_sizes(int* n_layers, int* n_regions, int* max_plan) {
   ensure_cms2017();
-  const IterationConfig& ic = Config::ItrInfo[0];
+  const IterationConfig& ic = Config::ItrInfo[g_iteration];
   *n_layers = (int)Config::TrkInfo.m_layers.size();
   *n_regions = ic.m_n_regions;
   int mp = 0;
@@ -413,7 +425,7 @@ int ref_cms2017_export(float* layer_desc, int* plans, int* plan_len, int* pickup
                        float* iter_params, int* flags, float* eta, float* rl, float* xi) {
   ensure_cms2017();
   const TrackerInfo& ti = Config::TrkInfo;
-  const IterationConfig& ic = Config::ItrInfo[0];
+  const IterationConfig& ic = Config::ItrInfo[g_iteration];
   int n_layers, n_regions, max_plan;
   ref_cms2017_sizes(&n_layers, &n_regions, &max_plan);
   for (int l = 0; l < n_layers; ++l) {
@@ -475,6 +487,27 @@ int ref_cms2017_export(float* layer_desc, int* plans, int* plan_len, int* pickup
   return 0;
 }
 
+// The backward search's IterationParams of the selected iteration
+// (IterationConfig::m_backward_params, set by SetupBackwardSearch_*):
+// bk[8] in the iter_params layout, and flags[2] = {m_backward_drop_seed_hits,
+// m_backward_fit_min_hits}.
+int ref_cms2017_backward_params(float* bk, int* flags) {
+  ensure_cms2017();
+  const IterationConfig& ic = Config::ItrInfo[g_iteration];
+  const IterationParams& ip = ic.m_backward_params;
+  bk[0] = ip.maxCandsPerSeed;
+  bk[1] = ip.maxHolesPerCand;
+  bk[2] = ip.maxConsecHoles;
+  bk[3] = ip.chi2Cut_min;
+  bk[4] = ip.chi2CutOverlap;
+  bk[5] = ip.pTCutOverlap;
+  bk[6] = ip.nlayers_per_seed;
+  bk[7] = 0;
+  flags[0] = ic.m_backward_drop_seed_hits;
+  flags[1] = ic.m_backward_fit_min_hits;
+  return 0;
+}
+
 // Clone-engine combinatorial finding on one event, CMS-2017 geometry,
 // iteration 0 with overrides (BASELINE config: max cands per seed, flat
 // chi2 cut: the dynamic c2 parameters are zeroed when zero_c2 != 0).
@@ -502,7 +535,7 @@ int ref_find(int n_layers_in, const int* layer_begin, const float* hpos, const f
   const int n_layers = (int)Config::TrkInfo.m_layers.size();
   if (n_layers_in != n_layers) return -1;
 
-  IterationConfig itconf = Config::ItrInfo[0];
+  IterationConfig itconf = Config::ItrInfo[g_iteration];
   itconf.m_params.maxCandsPerSeed = max_cands;
   itconf.m_backward_params.maxCandsPerSeed = max_cands;
   itconf.m_params.chi2Cut_min = chi2_cut;
@@ -671,7 +704,7 @@ int ref_event_prep(int n_layers_in, const int* layer_begin, const float* hpos, c
       t.addHitIdx(seed_hit_index[s * g_seed_hit_stride + k], seed_hit_layer[s * g_seed_hit_stride + k], 0.f);
     seeds.push_back(t);
   }
-  IterationConfig itconf = Config::ItrInfo[0];
+  IterationConfig itconf = Config::ItrInfo[g_iteration];
   MkJob job({Config::TrkInfo, itconf, eoh, nullptr});
   RefBuilder builder;
   builder.begin_event(&job, nullptr, "ref_event_prep");
@@ -711,7 +744,7 @@ extern "C" int ref_find_batch(int n_ev, const int* hit_off, const int* seed_off,
   ensure_cms2017();
   fillZRgridME();
   const int L = (int)Config::TrkInfo.m_layers.size();
-  IterationConfig itconf = Config::ItrInfo[0];
+  IterationConfig itconf = Config::ItrInfo[g_iteration];
   itconf.m_params.maxCandsPerSeed = max_cands;
   itconf.m_backward_params.maxCandsPerSeed = max_cands;
   itconf.m_params.chi2Cut_min = chi2_cut;

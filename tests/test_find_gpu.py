@@ -24,7 +24,7 @@ def hit_list(o, slot):
     return tuple(zip(o["hit_idx"][slot][:n].tolist(), o["hit_lyr"][slot][:n].tolist()))
 
 
-def compare(gpu, ref, n_seeds):
+def compare(gpu, ref, n_seeds, m=M):
     best_mismatch = 0
     all_mismatch = 0
     same_slots = []
@@ -35,12 +35,12 @@ def compare(gpu, ref, n_seeds):
         if nb == 0 or gpu["n_cands"][s] == 0:
             best_mismatch += int(nb != gpu["n_cands"][s])
             continue
-        if hit_list(gpu, s * M) != hit_list(ref, s * M):
+        if hit_list(gpu, s * m) != hit_list(ref, s * m):
             best_mismatch += 1
         eq = True
         for c in range(min(nb, gpu["n_cands"][s])):
-            if hit_list(gpu, s * M + c) == hit_list(ref, s * M + c):
-                same_slots.append(s * M + c)
+            if hit_list(gpu, s * m + c) == hit_list(ref, s * m + c):
+                same_slots.append(s * m + c)
             else:
                 eq = False
         if not eq and gpu["n_cands"][s] == nb:
@@ -68,6 +68,57 @@ def test_find_matches_reference(gpu_ctx, reflib, n_tracks, seed, noise):
         np.testing.assert_array_equal(gpu["nfound"][same], ref["nfound"][same])
     assert best_mm < 0.02
     assert all_mm < 0.05
+
+
+def iteration_event(it, n_tracks, seed):
+    """A CMS-2017 event with seeds where iteration `it` picks them up: pixel
+    triplets, except for pixelLessStep (7: the three layers before its plans'
+    pickup positions) and tobTecStep (8: hit pairs on the first two layers
+    of its forward search)."""
+    from mkfit_b200.geometry import cms2017
+    g = cms2017(it)
+    mask, nh = None, 3
+    if it in (7, 8):
+        nh = 3 if it == 7 else 2
+        mask = np.zeros(g.n_layers, bool)
+        for reg in range(g.n_regions):
+            p, k = g.plans[reg], int(g.pickup[reg])
+            lays = p[:k][-nh:] if it == 7 else p[k:k + nh]
+            mask[[lyr for lyr in lays if lyr >= 0]] = True
+    return synth.gen_cms_event(n_tracks, seed=seed, noise_frac=0.02, seed_layers=mask, seed_hits=nh)
+
+
+@pytest.mark.parametrize("it", range(1, 10))
+def test_iteration_finding_matches_reference(gpu_ctx, reflib, it):
+    """Finding with each CMS-2017 iteration's own configuration — its layer
+    plans and pickup positions, search windows, maxCandsPerSeed, hole
+    limits, chi2 cut with the dynamic per-layer terms — against the
+    reference run with the same iteration (Config::ItrInfo[it]), and the
+    backward search with the iteration's backward plans."""
+    ev = iteration_event(it, 1200, 110 + it)
+    cfg = FindConfig(iteration=it, max_cands=None, chi2_cut=None, zero_c2=False)
+    m = cfg.max_cands
+    ref = ref_find(reflib, ev, max_cands=m, chi2_cut=cfg.chi2_cut, zero_c2=False, iteration=it)
+    fnd = Finder(gpu_ctx, cfg)
+    gpu = fnd.find_event(ev)
+    np.testing.assert_array_equal(gpu["region"], ref["region"])
+    best_mm, all_mm, same = compare(gpu, ref, ev.n_seeds, m)
+    nfound = float(ref["nfound"][::m][ref["n_cands"] > 0].mean())
+    ref_b = ref_find(reflib, ev, max_cands=m, chi2_cut=cfg.chi2_cut, zero_c2=False, iteration=it,
+                     backward_search=True)
+    fnd.upload(ev)
+    fnd.run()
+    fnd.backward_fit()
+    fnd.backward_search()
+    gpu_b = fnd.download(ev.n_seeds)
+    best_b = np.mean([hit_list(gpu_b, s * m) != hit_list(ref_b, s * m) for s in range(ev.n_seeds)])
+    print(f"\niteration {it}: {ev.n_seeds} seeds, max cands {m}, chi2 cut {cfg.chi2_cut}, mean hits "
+          f"{nfound:.2f}; best-candidate mismatch {best_mm:.4f}, any-candidate {all_mm:.4f}; "
+          f"after the backward search {best_b:.4f}")
+    assert nfound > 4
+    assert best_mm < 0.02
+    assert all_mm < 0.05
+    assert best_b < 0.03
 
 
 def test_find_repeatable(gpu_ctx):

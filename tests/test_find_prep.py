@@ -28,11 +28,21 @@ def test_prep_empty_layers_and_no_seeds(reflib):
 
 
 def test_geometry_matches_reference_export(reflib):
-    """The committed geometry file equals what the reference plugin exports."""
-    from mkfit_b200.geometry import cms2017
+    """The committed geometry file equals what the reference plugin exports,
+    for every iteration's configuration."""
+    from mkfit_b200.geometry import ITER_KEYS, N_ITERATIONS, cms2017
     from oracle.oracle import cms2017_export
-    g = cms2017()
-    e = cms2017_export(reflib)
-    for k, v in e.items():
-        np.testing.assert_array_equal(g.arrays[k], v, err_msg=k)
-    assert FindConfig(g).c.n_layers == 72
+    for it in range(N_ITERATIONS):
+        g = cms2017(it)
+        e = cms2017_export(reflib, it)
+        for k, v in e.items():
+            got = g.arrays[k]
+            if k == "plans":
+                assert (got[:, v.shape[1]:] == -1).all()
+                got = got[:, :v.shape[1]]
+            np.testing.assert_array_equal(got, v, err_msg=f"iteration {it}: {k}")
+        assert FindConfig(g).c.n_layers == 72
+    # Iterations differ where the plugin makes them differ.
+    assert not np.array_equal(cms2017(7).plans, cms2017(0).plans)
+    assert cms2017(6).iter_params[0] != cms2017(0).iter_params[0]
+    assert all(k in cms2017().arrays for k in ["it_" + k for k in ITER_KEYS])
