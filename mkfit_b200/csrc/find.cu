@@ -398,12 +398,15 @@ __global__ void k_reset(EventDev E, int n_work) {
   E.upd[t] = 0;
   if (c == 0) {
     copy_slot(E.init, s, E.cand[0], t);
-    E.n_cands[s] = 1;
-    E.state[s] = kDormant;
+    // A seed the upload's post-cleaning dropped (nfound < 0) has no
+    // candidate and takes no part in the run.
+    const bool dropped = E.init.nfound[s] < 0;
+    E.n_cands[s] = dropped ? 0 : 1;
+    E.state[s] = dropped ? kFinished : kDormant;
     E.cur[s] = 0;
     E.hot_size[s] = E.init_hot[s];
     E.bshort_valid[s] = 0;
-    E.removed[s] = 0;
+    E.removed[s] = dropped ? 1 : 0;
   }
 }
 
@@ -1177,6 +1180,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   // Per-event host work (seed order and initial candidates; hit copies into
   // the pinned mirror), in parallel.
   std::vector<SeedOrder> orders(n_ev);
+  std::vector<int> n_silly(n_ev, 0);
   {
     auto work = [&](int e) {
       const mkfg_event* ev = evs + e;
@@ -1223,6 +1227,21 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
         }
         ss.hot_size[s] = nhs;
         ss.last[s] = nhs - 1;
+        // MkBuilder::seed_post_cleaning (mkFit/MkBuilder.cc:1151-1198, run
+        // by run_OneIteration before the seeds are loaded): a seed whose
+        // covariance has a negative diagonal or a non-finite element is
+        // dropped. nfound = -1 marks it; the per-run reset leaves it without
+        // a candidate.
+        bool silly = false;
+        for (int a = 0, c = 0; a < 6; ++a)
+          for (int b = 0; b <= a; ++b, ++c) {
+            const float v = ev->seed_err[c * n + i];
+            if ((a == b && v < 0.f) || !std::isfinite(v)) silly = true;
+          }
+        if (silly) {
+          nf = -1;
+          n_silly[e] += 1;
+        }
         ss.nfound[s] = nf;
         ss.nmiss[s] = nm;
         ss.ninside[s] = nin;
@@ -1429,7 +1448,10 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   f->h_seed_off = seed_off;
   f->h_hit_off = hit_off;
   f->events_loaded = 1;
+  // Seeds dropped by the post-cleaning are absent from the backward fit's
+  // seed groups, as filtered ones are.
   f->filter_removed = false;
+  for (int e = 0; e < n_ev; ++e) f->filter_removed |= n_silly[e] > 0;
   return MKFG_OK;
 }
 

@@ -567,6 +567,8 @@ int ref_find(int n_layers_in, const int* layer_begin, const float* hpos, const f
       t.addHitIdx(seed_hit_index[s * g_seed_hit_stride + k], seed_hit_layer[s * g_seed_hit_stride + k], 0.f);
     seeds.push_back(t);
   }
+  // run_OneIteration drops seeds with NaN / silly covariances first.
+  MkBuilder::seed_post_cleaning(seeds);
 
   MkJob job({Config::TrkInfo, itconf, eoh, nullptr});
   double best = 1e30;
@@ -704,6 +706,7 @@ int ref_event_prep(int n_layers_in, const int* layer_begin, const float* hpos, c
       t.addHitIdx(seed_hit_index[s * g_seed_hit_stride + k], seed_hit_layer[s * g_seed_hit_stride + k], 0.f);
     seeds.push_back(t);
   }
+  MkBuilder::seed_post_cleaning(seeds);
   IterationConfig itconf = Config::ItrInfo[g_iteration];
   MkJob job({Config::TrkInfo, itconf, eoh, nullptr});
   RefBuilder builder;
@@ -775,6 +778,7 @@ extern "C" int ref_find_batch(int n_ev, const int* hit_off, const int* seed_off,
         t.addHitIdx(seed_hit_index[s * g_seed_hit_stride + k], seed_hit_layer[s * g_seed_hit_stride + k], 0.f);
       seeds[e].push_back(t);
     }
+    MkBuilder::seed_post_cleaning(seeds[e]);
   }
   std::vector<std::unique_ptr<RefBuilder>> builders(n_ev);
   std::vector<std::unique_ptr<MkJob>> jobs(n_ev);

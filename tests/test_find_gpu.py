@@ -121,6 +121,38 @@ def test_iteration_finding_matches_reference(gpu_ctx, reflib, it):
     assert best_b < 0.03
 
 
+def test_silly_seeds_dropped_as_reference(gpu_ctx, reflib):
+    """Seeds whose covariance has a negative diagonal, a NaN or an infinity
+    are dropped before the finding (MkBuilder::seed_post_cleaning, which
+    run_OneIteration runs first): no candidates for them, the other seeds
+    found as the reference finds them, and the backward fit's seed groups
+    formed over the remaining seeds (states within the fit tolerance where
+    the hit lists agree)."""
+    ev = synth.gen_cms_event(1500, seed=131, noise_frac=0.02)
+    rng = np.random.default_rng(131)
+    bad = rng.choice(ev.n_seeds, 60, replace=False)
+    err = ev.seed_err.copy()
+    err[9, bad[:20]] = -1e-4
+    err[4, bad[20:40]] = np.nan
+    err[13, bad[40:]] = np.inf
+    ev.seed_err = err
+    ref = ref_find(reflib, ev, max_cands=M, chi2_cut=30.0, zero_c2=True, backward_fit=True)
+    fnd = Finder(gpu_ctx, FindConfig(max_cands=M, chi2_cut=30.0, zero_c2=True))
+    fnd.upload(ev)
+    fnd.run()
+    fnd.backward_fit()
+    gpu = fnd.download(ev.n_seeds)
+    assert (ref["n_cands"][bad] == 0).all()
+    assert (gpu["n_cands"][bad] == 0).all()
+    good = np.setdiff1d(np.arange(ev.n_seeds), bad)
+    same = [s for s in good if hit_list(gpu, s * M) == hit_list(ref, s * M)]
+    print(f"\n{len(bad)} silly seeds dropped; best hit lists equal {len(same)}/{len(good)}")
+    assert len(same) >= 0.98 * len(good)
+    slots = np.array(same) * M
+    ep = par_scaled_err(gpu["par"][slots].T, ref["par"][slots].T, ref["err"][slots].T)
+    assert np.percentile(ep, 99) < 1e-3
+
+
 def test_find_repeatable(gpu_ctx):
     """Two runs of the same event give identical outputs."""
     ev = synth.gen_cms_event(400, seed=9)
