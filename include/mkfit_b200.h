@@ -197,6 +197,10 @@ typedef struct {
   uint32_t inter_layer_pflags; /* Config::finding_inter_layer_pflags */
   uint32_t intra_layer_pflags; /* Config::finding_intra_layer_pflags */
   int32_t requires_prop_to_hit; /* Config::finding_requires_propagation_to_hit_pos; must be 1 */
+  /* IterationConfig::m_requires_seed_hit_sorting: the upload sorts every
+   * seed's hits by layer (Track::sortHitsByLayer, a stable sort) before it
+   * orders the seeds, as run_OneIteration does (pixelLessStep, tobTecStep). */
+  int32_t sort_seed_hits;
 } mkfg_find_config;
 
 int mkfg_finder_setup(mkfg_context* ctx, const mkfg_find_config* cfg);

@@ -901,6 +901,7 @@ struct Finder {
   // first entry); per-step buffers and the hit-on-track arena hold a
   // forward run plus a backward search of that length.
   int bks_steps = 0;
+  bool sort_seed_hits = false;  // IterationConfig::m_requires_seed_hit_sorting
   int64_t last_chi2_evals = 0, last_seeds_cloned = 0;
   // Per-launch device times of the last timed run: [max_steps][5] for the
   // layer-step kernels (activate, propagate, chi2, clone, update).
@@ -983,6 +984,7 @@ extern "C" int mkfg_finder_setup(mkfg_context* ctx, const mkfg_find_config* cfg)
   MKFG_REQUIRE(cfg->max_plan > 0 && cfg->max_plan <= kMaxPlan, "max_plan out of range");
   MKFG_REQUIRE(cfg->max_cands_per_seed >= 1 && cfg->max_cands_per_seed <= kSlots,
                "max_cands_per_seed must be in [1, %d]", kSlots);
+  MKFG_REQUIRE(cfg->sort_seed_hits == 0 || cfg->sort_seed_hits == 1, "sort_seed_hits must be 0 or 1");
   MKFG_REQUIRE(cfg->requires_prop_to_hit == 1,
                "only the propagate-to-hit finding mode (CMS geometries) is implemented");
   Finder* f = finder_of(ctx);
@@ -1031,6 +1033,7 @@ extern "C" int mkfg_finder_setup(mkfg_context* ctx, const mkfg_find_config* cfg)
   H.n_regions = cfg->n_regions;
   int max_steps = 0;
   f->bks_steps = 0;
+  f->sort_seed_hits = cfg->sort_seed_hits != 0;
   for (int r = 0; r < cfg->n_regions; ++r) {
     H.plan_len[r] = cfg->plan_len[r];
     H.pickup[r] = cfg->pickup[r];
@@ -1070,6 +1073,26 @@ namespace mkfg {
 // events are laid out back to back; every seed knows its event.
 // Row width of an event's seed-hit arrays (0 means 4).
 static int seed_hit_stride(const mkfg_event* ev) { return ev->seed_hit_stride ? ev->seed_hit_stride : 4; }
+
+
+// Track::sortHitsByLayer (Track.cc:241-245: a stable sort by layer) of every
+// seed of `ev` into hl / hi ([n_seeds][sw], like the event's own rows).
+static void sort_seed_hits_by_layer(const mkfg_event* ev, int sw, std::vector<int32_t>& hl,
+                                    std::vector<int32_t>& hi) {
+  hl.assign(ev->seed_hit_layer, ev->seed_hit_layer + (size_t)ev->n_seeds * sw);
+  hi.assign(ev->seed_hit_index, ev->seed_hit_index + (size_t)ev->n_seeds * sw);
+  std::vector<std::pair<int32_t, int32_t>> hs;
+  for (int i = 0; i < ev->n_seeds; ++i) {
+    const int nhs = ev->seed_nhits[i];
+    hs.clear();
+    for (int h = 0; h < nhs; ++h) hs.emplace_back(hl[(size_t)i * sw + h], hi[(size_t)i * sw + h]);
+    std::stable_sort(hs.begin(), hs.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    for (int h = 0; h < nhs; ++h) {
+      hl[(size_t)i * sw + h] = hs[h].first;
+      hi[(size_t)i * sw + h] = hs[h].second;
+    }
+  }
+}
 
 static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int n_ev) {
   const int L = f->host_cfg.n_layers;
@@ -1186,8 +1209,15 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
       const mkfg_event* ev = evs + e;
       const int nh = ev->layer_begin[L], o = hit_off[e];
       const int sw = seed_hit_stride(ev);
-      SeedInput si{ev->n_seeds, ev->seed_par, ev->seed_chg, ev->seed_nhits, ev->seed_hit_layer,
-                   ev->seed_hit_index, sw};
+      const int32_t* seed_hl = ev->seed_hit_layer;
+      const int32_t* seed_hi = ev->seed_hit_index;
+      std::vector<int32_t> sorted_hl, sorted_hi;
+      if (f->sort_seed_hits) {
+        sort_seed_hits_by_layer(ev, sw, sorted_hl, sorted_hi);
+        seed_hl = sorted_hl.data();
+        seed_hi = sorted_hi.data();
+      }
+      SeedInput si{ev->n_seeds, ev->seed_par, ev->seed_chg, ev->seed_nhits, seed_hl, seed_hi, sw};
       partition_seeds_cms2017(f->layer_desc.data(), L, si, ev->layer_begin, ev->pos, nh, orders[e]);
       for (int r = 0; r < 3; ++r)
         std::memcpy(hh.pos + (size_t)r * NHs + o, ev->pos + (size_t)r * nh, 4 * (size_t)nh);
@@ -1204,7 +1234,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
         ss.sev[s] = e;
         ss.region[s] = orders[e].region[i];
         const int nhs = ev->seed_nhits[i];
-        ss.pickup[s] = ev->seed_hit_layer[i * sw + nhs - 1];
+        ss.pickup[s] = seed_hl[i * sw + nhs - 1];
         for (int c = 0; c < 6; ++c) ss.par[c * (size_t)SS + s] = ev->seed_par[c * n + i];
         for (int c = 0; c < 21; ++c) ss.err[c * (size_t)SS + s] = ev->seed_err[c * n + i];
         ss.chg[s] = ev->seed_chg[i];
@@ -1214,7 +1244,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
             ss.seed_hot[MKFG_MAX_SEED_HITS * (size_t)s + h] = 0;
             continue;
           }
-          const int hi = ev->seed_hit_index[i * sw + h], hl = ev->seed_hit_layer[i * sw + h];
+          const int hi = seed_hi[i * sw + h], hl = seed_hl[i * sw + h];
           ss.seed_hot[MKFG_MAX_SEED_HITS * (size_t)s + h] = (hi & 0xffffff) | (hl << 24);
           if (hi >= 0 || hi == -9) {
             ++nf;
@@ -2173,8 +2203,12 @@ extern "C" int mkfg_prepare_event_host(const mkfg_find_config* cfg, const mkfg_e
   std::copy(prep.bins.begin(), prep.bins.end(), bins);
   if (srank) std::copy(prep.srank.begin(), prep.srank.end(), srank);
   if (seed_order || seed_region) {
-    SeedInput si{ev->n_seeds, ev->seed_par, ev->seed_chg, ev->seed_nhits, ev->seed_hit_layer,
-                 ev->seed_hit_index, seed_hit_stride(ev)};
+    const int sw = seed_hit_stride(ev);
+    std::vector<int32_t> hl, hi;
+    if (cfg->sort_seed_hits) sort_seed_hits_by_layer(ev, sw, hl, hi);
+    SeedInput si{ev->n_seeds, ev->seed_par, ev->seed_chg, ev->seed_nhits,
+                 cfg->sort_seed_hits ? hl.data() : ev->seed_hit_layer,
+                 cfg->sort_seed_hits ? hi.data() : ev->seed_hit_index, sw};
     SeedOrder so;
     partition_seeds_cms2017(cfg->layer_desc, cfg->n_layers, si, ev->layer_begin, ev->pos, nh, so);
     if (seed_order) std::copy(so.order.begin(), so.order.end(), seed_order);

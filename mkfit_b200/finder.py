@@ -18,7 +18,7 @@ class MkfgFindConfig(ctypes.Structure):
                 ("max_consec_holes", ctypes.c_int32), ("chi2_cut_min", ctypes.c_float),
                 ("chi2_cut_overlap", ctypes.c_float), ("pt_cut_overlap", ctypes.c_float),
                 ("inter_layer_pflags", ctypes.c_uint32), ("intra_layer_pflags", ctypes.c_uint32),
-                ("requires_prop_to_hit", ctypes.c_int32)]
+                ("requires_prop_to_hit", ctypes.c_int32), ("sort_seed_hits", ctypes.c_int32)]
 
 
 class MkfgSelectConfig(ctypes.Structure):
@@ -90,7 +90,7 @@ def _iteration_selection():
             mode = DUP_PIXELSEED
         else:
             mode = DUP_ETA_PHI
-        out[it] = dict(algorithm=algo, pre=pre, post=post,
+        out[it] = dict(algorithm=algo, pre=pre, post=post, sort_seed_hits=qf and not tight,
                        min_hits=3 if algo == 6 else min_hits, mode=mode, frac_shared_hits=frac,
                        drth=drth)
     return out
@@ -185,6 +185,8 @@ class FindConfig:
         c.inter_layer_pflags = int(g.flags[1])
         c.intra_layer_pflags = int(g.flags[2])
         c.requires_prop_to_hit = int(g.flags[0])
+        # m_requires_seed_hit_sorting (set_qf_flags: pixelLessStep, tobTecStep).
+        c.sort_seed_hits = int(ITERATION_SELECTION[g.iteration]["sort_seed_hits"])
         self.c = c
 
     @property

@@ -1088,10 +1088,10 @@ def ref_cms2017_iteration(reflib, it):
     lib = reflib.lib
     lib.ref_cms2017_iteration.restype = ctypes.c_int
     lib.ref_cms2017_iteration.argtypes = [ctypes.c_int, _i32p, _f32p]
-    iv = np.zeros(4, np.int32)
+    iv = np.zeros(5, np.int32)
     fv = np.zeros(4, np.float32)
     if lib.ref_cms2017_iteration(int(it), iv, fv) != 0:
         raise IndexError(it)
     return dict(algorithm=int(iv[0]), quality_filter=bool(iv[1]), dupclean_tight=bool(iv[2]),
-                min_hits_qf=int(iv[3]), frac_shared_hits=float(fv[0]),
+                min_hits_qf=int(iv[3]), sort_seed_hits=bool(iv[4]), frac_shared_hits=float(fv[0]),
                 drth=tuple(float(x) for x in fv[1:]))

@@ -381,7 +381,7 @@ int ref_dups(int mode, int n, const float* par, const int* chg, const float* sco
 
 // The selection settings of CMS-2017 iteration `it` (Geoms/CMS-2017.cc):
 // iv = {track algorithm, requires_quality_filter, requires_dupclean_tight,
-// minHitsQF}, fv = {fracSharedHits, drth_central, drth_obarrel,
+// minHitsQF, requires_seed_hit_sorting}, fv = {fracSharedHits, drth_central, drth_obarrel,
 // drth_forward}.
 int ref_cms2017_iteration(int it, int* iv, float* fv) {
   ensure_cms2017();
@@ -391,6 +391,7 @@ int ref_cms2017_iteration(int it, int* iv, float* fv) {
   iv[1] = c.m_requires_quality_filter;
   iv[2] = c.m_requires_dupclean_tight;
   iv[3] = c.m_params.minHitsQF;
+  iv[4] = c.m_requires_seed_hit_sorting;
   fv[0] = c.m_params.fracSharedHits;
   fv[1] = c.m_params.drth_central;
   fv[2] = c.m_params.drth_obarrel;
@@ -567,8 +568,11 @@ int ref_find(int n_layers_in, const int* layer_begin, const float* hpos, const f
       t.addHitIdx(seed_hit_index[s * g_seed_hit_stride + k], seed_hit_layer[s * g_seed_hit_stride + k], 0.f);
     seeds.push_back(t);
   }
-  // run_OneIteration drops seeds with NaN / silly covariances first.
+  // run_OneIteration drops seeds with NaN / silly covariances first, and
+  // sorts the seeds' hits by layer for the iterations that ask for it.
   MkBuilder::seed_post_cleaning(seeds);
+  if (itconf.m_requires_seed_hit_sorting)
+    for (auto& t : seeds) t.sortHitsByLayer();
 
   MkJob job({Config::TrkInfo, itconf, eoh, nullptr});
   double best = 1e30;

@@ -270,6 +270,7 @@ def test_iteration_table_matches_reference(reflib):
         assert (sel["pre"], sel["post"]) == (pre, post), it
         assert sel["min_hits"] == (3 if algo == 6 else r["min_hits_qf"]), it
         assert sel["mode"] == (DUP_SHAREDHITS if qf and not tight else DUP_PIXELSEED), it
+        assert sel["sort_seed_hits"] == r["sort_seed_hits"], it
         assert np.float32(sel["frac_shared_hits"]) == np.float32(r["frac_shared_hits"]), it
         assert tuple(np.float32(sel["drth"])) == tuple(np.float32(r["drth"])), it
 
