@@ -505,7 +505,8 @@ def run_iteration_stages(ctx, stream, finder, events, n_seeds):
     """Time of the steps of run_OneIteration around the finding, on the
     same batch (median of 5; CUDA events on the context stream around each
     call, so host-side setup inside the call counts): the backward fit, the
-    backward search, the output selection, and the seed cleaning of the
+    backward search, the output selection, a quality filter, and the seed
+    cleaning of the
     batch's seeds with 20% near-duplicates added (host-buffer call, wall
     clock)."""
     import torch
@@ -528,9 +529,13 @@ def run_iteration_stages(ctx, stream, finder, events, n_seeds):
             out.append(a.elapsed_time(b))
         return statistics.median(out)
 
+    from mkfit_b200.finder import QF_N_LAYERS
     bk = dev_ms(finder.backward_fit)
     bs = dev_ms(finder.backward_search, pre=finder.backward_fit)
     sel = dev_ms(lambda: finder.select(n_seeds))
+    # The costliest quality filter (a walk of every best candidate's hit
+    # chain), verdicts copied to the host.
+    qf = dev_ms(lambda: finder.filter(n_seeds, QF_N_LAYERS, beam_spot=(0.0, 0.0)))
     sds = [synth.with_duplicate_seeds(e, frac=0.2, seed=i) for i, e in enumerate(events)]
     begin = np.cumsum([0] + [len(d["chg"]) for d in sds]).astype(np.int32)
     cat = lambda k, ax: np.concatenate([d[k] for d in sds], axis=ax)  # noqa: E731
@@ -544,6 +549,7 @@ def run_iteration_stages(ctx, stream, finder, events, n_seeds):
         ts.append(time.perf_counter() - t0)
     return {"events": len(events), "seeds": int(n_seeds),
             "backward_fit_ms": bk, "backward_search_ms": bs, "select_ms": sel,
+            "quality_filter_ms": qf,
             "seed_cleaning": {"seeds_in": int(begin[-1]), "kept": int(keep.sum()),
                               "ms_host_buffers": statistics.median(ts) * 1e3},
             "note": "stream times of the calls around the finding of the bench batch; seed "
