@@ -340,6 +340,10 @@ typedef struct {
   const int32_t* seed_hit_layer;
   const int32_t* seed_hit_index;
   int32_t seed_hit_stride;
+  /* Hits that earlier iterations used, which the search skips
+   * (IterationMaskIfc: one flag per hit, layer by layer in the order of
+   * pos; 1 = masked), or NULL. */
+  const uint8_t* hit_mask;
 } mkfg_event;
 
 /* Finding output, indexed by input seed; m = max_cands_per_seed slots per

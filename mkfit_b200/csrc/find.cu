@@ -1120,8 +1120,10 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   // and ranks) is then built on the device (layer_hits.cuh).
   const int NHs = std::max(NH, 1);
   const size_t n_lb = (size_t)(L + 1) * n_ev, n_bins_all = (size_t)nb * n_ev;
+  bool any_mask = false;
+  for (int e = 0; e < n_ev; ++e) any_mask |= evs[e].hit_mask != nullptr;
   const size_t up_bytes = rounded(12 * (size_t)NHs) + rounded(24 * (size_t)NHs) +
-                          2 * rounded(4 * (size_t)NHs) + rounded(4 * n_lb);
+                          2 * rounded(4 * (size_t)NHs) + rounded(4 * n_lb) + rounded((size_t)NHs);
   const size_t hit_bytes = up_bytes + rounded(4 * (size_t)NHs) + rounded(4 * n_bins_all) +
                            rounded(8 * (size_t)NHs) + rounded(4 * (size_t)NHs);
   int rc;
@@ -1133,6 +1135,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     int* detid;
     int* cpcm;
     int* lb;
+    uint8_t* mask;  // hits masked by earlier iterations (1 = skip)
     uint32_t* info;
     uint32_t* bins;
     float2* qphi;
@@ -1145,6 +1148,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     h.detid = carve<int>(p, NHs);
     h.cpcm = carve<int>(p, NHs);
     h.lb = carve<int>(p, n_lb);
+    h.mask = carve<uint8_t>(p, NHs);
     if (device) {
       h.info = carve<uint32_t>(p, NHs);
       h.bins = carve<uint32_t>(p, n_bins_all);
@@ -1225,6 +1229,12 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
         std::memcpy(hh.err + (size_t)r * NHs + o, ev->err + (size_t)r * nh, 4 * (size_t)nh);
       std::memcpy(hh.detid + o, ev->detid, 4 * (size_t)nh);
       std::memcpy(hh.cpcm + o, ev->cpcm, 4 * (size_t)nh);
+      if (any_mask) {
+        if (ev->hit_mask)
+          std::memcpy(hh.mask + o, ev->hit_mask, (size_t)nh);
+        else
+          std::memset(hh.mask + o, 0, (size_t)nh);
+      }
       for (int l = 0; l <= L; ++l) hh.lb[(size_t)e * (L + 1) + l] = o + ev->layer_begin[l];
       const int n = ev->n_seeds;
       for (int k = 0; k < n; ++k) {
@@ -1317,6 +1327,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
       copy_rows(hh.err, 4 * (size_t)NHs, 6, o, nb);
       copy_rows(hh.detid, 0, 1, o, nb);
       copy_rows(hh.cpcm, 0, 1, o, nb);
+      if (any_mask) copy_rows(hh.mask, 0, 1, o / 4, nb / 4);
     }
     for (auto& th : pool) th.join();
     copy_rows(hh.lb, 0, 1, 0, 4 * n_lb);
@@ -1343,6 +1354,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     A.n_bins = nb;
     A.qphi = dh.qphi;
     A.srank = dh.srank;
+    A.mask = any_mask ? dh.mask : nullptr;
     const int smem = f->max_nq * kFineStride * 4;
     MKFG_CUDA_TRY(cudaFuncSetAttribute(k_layer_hits, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     k_layer_hits<<<n_ev * L, kHitsBlock, smem, st>>>(A, f->d_cfg);

@@ -49,6 +49,7 @@ struct LayerHitsArgs {
   int n_bins;
   float2* qphi;          // [NH] out, sorted order
   int* srank;            // [NH] out, sorted order
+  const uint8_t* mask;   // [NH] hits masked by earlier iterations, or NULL
 };
 
 // Dynamic shared memory: nq_max * kFineStride counters.
@@ -159,7 +160,11 @@ __global__ void __launch_bounds__(kHitsBlock) k_layer_hits(const LayerHitsArgs A
         }
         base = __shfl_sync(peers, base, leader);
         const uint32_t at = base + __popc(peers & ((1u << lane) - 1u));
-        A.qphi[h0 + at] = make_float2(q, phi);
+        // A masked hit (IterationMaskIfc, skipped by
+        // MkFinder::SelectHitIndices, mkFit/MkFinder.cc:476-482) keeps its
+        // bin but gets q = +inf, which no search window holds.
+        const bool masked = A.mask != nullptr && A.mask[h0 + i] != 0;
+        A.qphi[h0 + at] = make_float2(masked ? __int_as_float(0x7f800000) : q, phi);
         A.srank[h0 + at] = i;
       }
       __syncthreads();

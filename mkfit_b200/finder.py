@@ -103,7 +103,7 @@ class MkfgEvent(ctypes.Structure):
     _fields_ = [("n_layers", ctypes.c_int32), ("layer_begin", vp), ("pos", vp), ("err", vp),
                 ("detid", vp), ("cpcm", vp), ("n_seeds", ctypes.c_int32), ("seed_par", vp),
                 ("seed_err", vp), ("seed_chg", vp), ("seed_nhits", vp), ("seed_hit_layer", vp),
-                ("seed_hit_index", vp), ("seed_hit_stride", ctypes.c_int32)]
+                ("seed_hit_index", vp), ("seed_hit_stride", ctypes.c_int32), ("hit_mask", vp)]
 
 
 class MkfgFindOut(ctypes.Structure):
@@ -220,6 +220,8 @@ def event_struct(ev):
     e.seed_hit_index = p("shi", ev.seed_hit_index, np.int32)
     shl = np.asarray(ev.seed_hit_layer)
     e.seed_hit_stride = int(shl.shape[1]) if shl.ndim == 2 else 4
+    mask = getattr(ev, "hit_mask", None)
+    e.hit_mask = None if mask is None else p("mask", mask, np.uint8)
     e._keep = keep
     return e
 

@@ -365,7 +365,7 @@ def _set_seed_stride(lib, seed_hit_layer):
 
 def ref_find(reflib, ev, max_cands=6, chi2_cut=30.0, zero_c2=True, repeat=1, backward_fit=False,
              select=False, backward_search=False, qf_pre=-1, qf_post=-1, qf_min_hits=0,
-             beam=(0.0, 0.0), dup_mode=0, dup_params=None, iteration=0):
+             beam=(0.0, 0.0), dup_mode=0, dup_params=None, iteration=0, hit_mask=None):
     """Reference clone-engine finding (find_tracks_load_seeds +
     FindTracksCloneEngine, then MkBuilder::BackwardFit when backward_fit,
     or CompactifyHitStorageForBestCand + BackwardFit + the backward search
@@ -379,10 +379,15 @@ def ref_find(reflib, ev, max_cands=6, chi2_cut=30.0, zero_c2=True, repeat=1, bac
     of the selection (DUP_MODES index) with dup_params (fracSharedHits,
     drth central, obarrel, forward) replacing the iteration's. iteration:
     the CMS-2017 iteration whose steering and parameters the finding uses
-    (max_cands, chi2_cut and zero_c2 still override)."""
+    (max_cands, chi2_cut and zero_c2 still override). hit_mask: one flag per
+    hit in the event's layer order, hits used by earlier iterations
+    (IterationMaskIfc)."""
     lib = reflib.lib
     _load_find_api(lib)
     _set_iteration(lib, iteration)
+    lib.ref_set_hit_mask.argtypes = [ctypes.c_void_p]
+    hm = None if hit_mask is None else np.ascontiguousarray(hit_mask, np.uint8)
+    lib.ref_set_hit_mask(None if hm is None else hm.ctypes.data)
     lib.ref_set_iteration_filters.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                               ctypes.c_float, ctypes.c_float, ctypes.c_int,
                                               ctypes.c_void_p]
@@ -424,6 +429,7 @@ def ref_find(reflib, ev, max_cands=6, chi2_cut=30.0, zero_c2=True, repeat=1, bac
     lib.ref_set_select_output(None)
     lib.ref_set_iteration_filters(-1, -1, 0, 0.0, 0.0, 0, None)
     _set_iteration(lib, 0)
+    lib.ref_set_hit_mask(None)
     if rc != 0:
         raise RuntimeError(f"ref_find failed rc={rc}")
     o["seconds"] = secs.value

@@ -62,6 +62,10 @@ int g_seed_hit_stride = 4;
 // CMS-2017 iteration whose configuration the geometry export and the
 // finding drivers use (Config::ItrInfo index).
 int g_iteration = 0;
+// ref_find: hits masked by earlier iterations (one byte per hit in the
+// event's layer order, 1 = masked), given to the builder through the
+// reference's IterationMaskIfc; NULL = no mask.
+const unsigned char* g_hit_mask = nullptr;
 // When set, ref_find also runs the output selection of run_OneIteration
 // (qfilter_nan_n_silly, export_best_comb_cands(.., true),
 // find_and_remove_duplicates) and marks the surviving seeds here (by label).
@@ -281,6 +285,10 @@ int ref_set_iteration(int it) {
   g_iteration = it;
   return 0;
 }
+
+// ref_find: per-hit mask of hits used by earlier iterations (see
+// g_hit_mask); NULL switches it off.
+void ref_set_hit_mask(const unsigned char* mask) { g_hit_mask = mask; }
 
 // Row width of seed_hit_layer / seed_hit_index in ref_find, ref_event_prep
 // and ref_find_batch (default 4).
@@ -574,7 +582,14 @@ int ref_find(int n_layers_in, const int* layer_begin, const float* hpos, const f
   if (itconf.m_requires_seed_hit_sorting)
     for (auto& t : seeds) t.sortHitsByLayer();
 
-  MkJob job({Config::TrkInfo, itconf, eoh, nullptr});
+  IterationMaskIfc mask_ifc;
+  if (g_hit_mask) {
+    mask_ifc.m_mask_vector.resize(n_layers);
+    for (int l = 0; l < n_layers; ++l)
+      for (int h = layer_begin[l]; h < layer_begin[l + 1]; ++h)
+        mask_ifc.m_mask_vector[l].push_back(g_hit_mask[h] != 0);
+  }
+  MkJob job({Config::TrkInfo, itconf, eoh, g_hit_mask ? &mask_ifc : nullptr});
   double best = 1e30;
   RefBuilder builder;
   for (int r = 0; r < std::max(1, repeat); ++r) {

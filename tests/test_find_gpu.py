@@ -11,6 +11,7 @@ import pytest
 
 from mkfit_b200 import synth
 from mkfit_b200.finder import FindConfig, Finder
+from mkfit_b200.geometry import cms2017
 from oracle.oracle import ref_find
 from tests.tolerances import par_scaled_err, cov_scaled_err, summarize
 
@@ -75,7 +76,6 @@ def iteration_event(it, n_tracks, seed):
     triplets, except for pixelLessStep (7: the three layers before its plans'
     pickup positions) and tobTecStep (8: hit pairs on the first two layers
     of its forward search)."""
-    from mkfit_b200.geometry import cms2017
     g = cms2017(it)
     mask, nh = None, 3
     if it in (7, 8):
@@ -145,6 +145,45 @@ def test_seed_hits_sorted_by_layer(gpu_ctx, reflib):
     best_mm, _, _ = compare(got, ref, ev.n_seeds, m)
     print(f"\nreversed seed hits: best-candidate mismatch vs reference {best_mm:.4f}")
     assert best_mm < 0.02
+
+
+def test_hit_mask_matches_reference(gpu_ctx, reflib):
+    """Hits used by an earlier iteration (IterationMaskIfc: the hits of the
+    best candidates of half the seeds from a first pass, plus 20% of all
+    strip hits) are skipped by the search: the device with the mask equals
+    the reference with the same mask, no masked hit is picked up, and the
+    mask changes the result of many seeds."""
+    ev = synth.gen_cms_event(1500, seed=151, noise_frac=0.02)
+    first = ref_find(reflib, ev, max_cands=M, chi2_cut=30.0, zero_c2=True)
+    rng = np.random.default_rng(151)
+    lb = np.asarray(ev.layer_begin)
+    mask = np.zeros(ev.n_hits, np.uint8)
+    for s in range(0, ev.n_seeds, 2):
+        for idx, lyr in hit_list(first, s * M):
+            if idx >= 0:
+                mask[lb[lyr] + idx] = 1
+    strip = np.concatenate([np.arange(lb[l], lb[l + 1]) for l in range(ev.n_layers)
+                            if not cms2017().layer(l)["is_pix"] > 0.5])
+    mask[strip[rng.random(len(strip)) < 0.2]] = 1
+    mev = synth.CmsEvent(**dict(ev.__dict__))
+    mev.hit_mask = mask
+    ref = ref_find(reflib, mev, max_cands=M, chi2_cut=30.0, zero_c2=True, hit_mask=mask)
+    fnd = Finder(gpu_ctx, FindConfig(max_cands=M, chi2_cut=30.0, zero_c2=True))
+    gpu = fnd.find_event(mev)
+    plain = fnd.find_event(ev)
+    best_mm, all_mm, _ = compare(gpu, ref, ev.n_seeds)
+    seed_hits = {(int(ev.seed_hit_index[s, k]), int(ev.seed_hit_layer[s, k]))
+                 for s in range(ev.n_seeds) for k in range(ev.seed_nhits[s])}
+    picked = {h for s in range(ev.n_seeds) for c in range(gpu["n_cands"][s])
+              for h in hit_list(gpu, s * M + c) if h[0] >= 0}
+    masked_picked = [h for h in picked - seed_hits if mask[lb[h[1]] + h[0]]]
+    changed = sum(hit_list(gpu, s * M) != hit_list(plain, s * M) for s in range(ev.n_seeds))
+    print(f"\nmasked {int(mask.sum())} of {ev.n_hits} hits: best-candidate mismatch vs reference "
+          f"{best_mm:.4f}, any-candidate {all_mm:.4f}; {changed} seeds changed by the mask")
+    assert not masked_picked
+    assert best_mm < 0.02
+    assert all_mm < 0.05
+    assert changed > 0.2 * ev.n_seeds
 
 
 def test_silly_seeds_dropped_as_reference(gpu_ctx, reflib):
