@@ -515,6 +515,18 @@ typedef struct {
 
 int mkfg_find_filter(mkfg_context* ctx, const mkfg_qfilter_config* cfg, int32_t n_seeds,
                      int32_t remove, int32_t* pass);
+/* MkFinder::SelectHitIndices (mkFit/MkFinder.cc:227-684) as a plain worker
+ * call on the uploaded event `event`: for n states already propagated to
+ * layer `layer` (par[6][n], err[21][n], as MkFinder's Par[iP] / Err[iP]),
+ * the window from the position covariance and the layer's (dynamic)
+ * limits, the sensitive-region test and the bin scan. xhit_size[n]
+ * (XHitSize: hits found, at most 16; -1 when the state is outside the
+ * layer), xhit_idx[n][16] (XHitArr: hit indices within the layer in scan
+ * order, -1 after the last), wsr[n] (may be NULL: 0 inside, 1 edge,
+ * 2 outside). Synchronizes the stream. */
+int mkfg_find_select_hit_indices(mkfg_context* ctx, int32_t event, int32_t layer, int32_t n,
+                                 const float* par, const float* err, int32_t* xhit_size,
+                                 int32_t* xhit_idx, int32_t* wsr);
 /* The hit index the upload built on the device for uploaded event `event`
  * (LayerOfHits after SuckInHits / EndRegistrationOfHits,
  * mkFit/HitStructures.cc:77-338): bins in the layout of

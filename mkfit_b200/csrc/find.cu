@@ -796,6 +796,33 @@ __global__ void k_qfilter(EventDev E, const FindConfigDev* __restrict__ Cp, cons
   pass_by_label[E.seed_label[s]] = res;
 }
 
+//------------------------------------------------------------------------------
+// MkFinder::SelectHitIndices as a plain worker call (mkFit/MkFinder.cc:
+// 227-684): for caller-given states on layer `layer` of uploaded event
+// `event`, the hit window, the sensitive-region test and the first
+// kMaxXHits hits of the bin scan (indices within the layer; size -1 when
+// the state is outside the layer).
+//------------------------------------------------------------------------------
+__global__ void k_select_hit_indices(EventDev E, const FindConfigDev* __restrict__ Cp, int event,
+                                     int layer, int n, const float* __restrict__ par,
+                                     const float* __restrict__ err, int* __restrict__ xsize,
+                                     int* __restrict__ xhits, int* __restrict__ wsr_out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float p[6], e[21];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) p[k] = par[(size_t)k * n + i];
+#pragma unroll
+  for (int k = 0; k < 21; ++k) e[k] = err[(size_t)k * n + i];
+  const LayerDev& L = Cp->layer[layer];
+  const uint32_t* bins = E.bins + (size_t)event * E.n_bins + L.bin_offset;
+  const int hit_base = E.layer_begin[event * E.lb_stride + layer];
+  int wsr = kWsrInside;
+  const int x = select_hits(E, L, bins, hit_base, p, e, xhits + (size_t)i * kMaxXHits, 1, wsr);
+  xsize[i] = x;
+  if (wsr_out) wsr_out[i] = wsr;
+}
+
 __global__ void k_select_out(EventDev E, const SelectArgs A, const int* __restrict__ dup,
                              int* __restrict__ keep_by_label) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2111,6 +2138,40 @@ extern "C" int mkfg_find_select(mkfg_context* ctx, const mkfg_select_config* cfg
   k_select_out<<<grid, 128, 0, st>>>(f->ev, A, dup, d_keep);
   MKFG_CUDA_TRY(cudaGetLastError());
   MKFG_CUDA_TRY(cudaMemcpyAsync(keep, d_keep, 4 * (size_t)S, cudaMemcpyDeviceToHost, st));
+  MKFG_CUDA_TRY(cudaStreamSynchronize(st));
+  return MKFG_OK;
+}
+
+extern "C" int mkfg_find_select_hit_indices(mkfg_context* ctx, int32_t event, int32_t layer, int32_t n,
+                                            const float* par, const float* err, int32_t* xhit_size,
+                                            int32_t* xhit_idx, int32_t* wsr) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  Finder* f = finder_of(ctx);
+  MKFG_REQUIRE(f->events_loaded, "no event uploaded");
+  MKFG_REQUIRE(event >= 0 && event < f->n_events, "event %d out of range", event);
+  MKFG_REQUIRE(layer >= 0 && layer < f->host_cfg.n_layers, "layer %d out of range", layer);
+  MKFG_REQUIRE(n >= 0 && (n == 0 || (par && err && xhit_size && xhit_idx)), "null argument");
+  if (n == 0) return MKFG_OK;
+  const size_t in_bytes = rounded(4 * 27 * (size_t)n), out_bytes = rounded(4 * (size_t)n) * 2 +
+                                                                  rounded(4 * (size_t)n * kMaxXHits);
+  if ((rc = f->sel.ensure(in_bytes + out_bytes))) return rc;
+  char* p = f->sel.as<char>();
+  float* d_par = carve<float>(p, 6 * (size_t)n);
+  float* d_err = carve<float>(p, 21 * (size_t)n);
+  int* d_size = carve<int>(p, n);
+  int* d_wsr = carve<int>(p, n);
+  int* d_idx = carve<int>(p, (size_t)n * kMaxXHits);
+  cudaStream_t st = ctx->stream;
+  MKFG_CUDA_TRY(cudaMemcpyAsync(d_par, par, 4 * 6 * (size_t)n, cudaMemcpyHostToDevice, st));
+  MKFG_CUDA_TRY(cudaMemcpyAsync(d_err, err, 4 * 21 * (size_t)n, cudaMemcpyHostToDevice, st));
+  MKFG_CUDA_TRY(cudaMemsetAsync(d_idx, 0xff, 4 * (size_t)n * kMaxXHits, st));
+  k_select_hit_indices<<<(n + 127) / 128, 128, 0, st>>>(f->ev, f->d_cfg, event, layer, n, d_par, d_err,
+                                                        d_size, d_idx, d_wsr);
+  MKFG_CUDA_TRY(cudaGetLastError());
+  MKFG_CUDA_TRY(cudaMemcpyAsync(xhit_size, d_size, 4 * (size_t)n, cudaMemcpyDeviceToHost, st));
+  MKFG_CUDA_TRY(cudaMemcpyAsync(xhit_idx, d_idx, 4 * (size_t)n * kMaxXHits, cudaMemcpyDeviceToHost, st));
+  if (wsr) MKFG_CUDA_TRY(cudaMemcpyAsync(wsr, d_wsr, 4 * (size_t)n, cudaMemcpyDeviceToHost, st));
   MKFG_CUDA_TRY(cudaStreamSynchronize(st));
   return MKFG_OK;
 }

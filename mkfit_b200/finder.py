@@ -129,6 +129,8 @@ def _bind(lib):
     lib.mkfg_find_select.argtypes = [vp, ctypes.POINTER(MkfgSelectConfig), ctypes.c_int32, vp]
     lib.mkfg_find_filter.argtypes = [vp, ctypes.POINTER(MkfgQFilterConfig), ctypes.c_int32,
                                      ctypes.c_int32, vp]
+    lib.mkfg_find_select_hit_indices.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                                 vp, vp, vp, vp, vp]
     lib.mkfg_find_run_fused.argtypes = [vp, ctypes.c_int32]
     lib.mkfg_find_autotune.argtypes = [vp, ctypes.POINTER(ctypes.c_int32),
                                        ctypes.POINTER(ctypes.c_float)]
@@ -385,6 +387,21 @@ class Finder:
         return self.select(n_seeds, mode=sel["mode"] if remove_duplicates else DUP_NONE,
                            algorithm=sel["algorithm"], frac_shared_hits=sel["frac_shared_hits"],
                            drth_central=d[0], drth_obarrel=d[1], drth_forward=d[2])
+
+    def select_hit_indices(self, event, layer, par, err):
+        """MkFinder::SelectHitIndices on states par [6][n], err [21][n]
+        propagated to `layer` of uploaded event `event`: (xhit_size [n],
+        xhit_idx [n][16], wsr [n])."""
+        par = np.ascontiguousarray(par, np.float32)
+        err = np.ascontiguousarray(err, np.float32)
+        n = par.shape[1]
+        size = np.zeros(n, np.int32)
+        idx = np.zeros((n, 16), np.int32)
+        wsr = np.zeros(n, np.int32)
+        capi.check(self.lib.mkfg_find_select_hit_indices(
+            self.ctx.handle, int(event), int(layer), n, par.ctypes.data, err.ctypes.data,
+            size.ctypes.data, idx.ctypes.data, wsr.ctypes.data))
+        return size, idx, wsr
 
     def hit_index(self, event, n_bins, n_hits):
         """The device-built hit index of uploaded event `event`:

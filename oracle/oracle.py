@@ -1101,3 +1101,31 @@ def ref_cms2017_iteration(reflib, it):
     return dict(algorithm=int(iv[0]), quality_filter=bool(iv[1]), dupclean_tight=bool(iv[2]),
                 min_hits_qf=int(iv[3]), sort_seed_hits=bool(iv[4]), frac_shared_hits=float(fv[0]),
                 drth=tuple(float(x) for x in fv[1:]))
+
+
+def ref_select_hit_indices(reflib, ev, layer, par, err, chg, iteration=0):
+    """MkFinder::SelectHitIndices of the reference on states par [6][n],
+    err [21][n], chg [n] taken as propagated to `layer`, against the hits of
+    event `ev` (oracle/ref_driver.cc ref_select_hit_indices). Returns
+    (xsize [n], xidx [n][16])."""
+    lib = reflib.lib
+    lib.ref_select_hit_indices.restype = ctypes.c_int
+    lib.ref_select_hit_indices.argtypes = [ctypes.c_int, _i32p, _f32p, _f32p, _i32p, _i32p,
+                                           ctypes.c_int, ctypes.c_int, _f32p, _f32p, _i32p, _i32p,
+                                           _i32p]
+    _set_iteration(reflib.lib, iteration)
+    c = np.ascontiguousarray
+    n = int(len(chg))
+    xs = np.zeros(n, np.int32)
+    xi = np.zeros((n, 16), np.int32)
+    try:
+        rc = lib.ref_select_hit_indices(ev.n_layers, c(ev.layer_begin, np.int32),
+                                        c(ev.hit_pos, np.float32), c(ev.hit_err, np.float32),
+                                        c(ev.hit_detid, np.int32), c(ev.hit_cpcm, np.int32),
+                                        int(layer), n, c(par, np.float32), c(err, np.float32),
+                                        c(chg, np.int32), xs, xi)
+    finally:
+        _set_iteration(reflib.lib, 0)
+    if rc != 0:
+        raise RuntimeError(f"ref_select_hit_indices failed rc={rc}")
+    return xs, xi

@@ -496,6 +496,50 @@ int ref_cms2017_export(float* layer_desc, int* plans, int* plan_len, int* pickup
   return 0;
 }
 
+// MkFinder::SelectHitIndices on given states (taken as propagated to layer
+// `layer`: Par[iP] / Err[iP]) against one event's hits, built as in
+// ref_find; the selected iteration's windows. par[6][n], err[21][n]
+// (lane-fastest), chg[n]. Out: xsize[n] (XHitSize), xidx[n][16] (XHitArr,
+// -1 after the last hit).
+int ref_select_hit_indices(int n_layers_in, const int* layer_begin, const float* hpos,
+                           const float* herr, const int* detid, const int* cpcm, int layer, int n,
+                           const float* par, const float* err, const int* chg, int* xsize, int* xidx) {
+  ensure_cms2017();
+  const int n_layers = (int)Config::TrkInfo.m_layers.size();
+  if (n_layers_in != n_layers || layer < 0 || layer >= n_layers) return -1;
+  const int nh_tot = layer_begin[n_layers];
+  std::vector<HitVec> layer_hits(n_layers);
+  for (int l = 0; l < n_layers; ++l)
+    for (int h = layer_begin[l]; h < layer_begin[l + 1]; ++h) {
+      Hit hit = make_hit(h, nh_tot, hpos, herr);
+      if (cpcm[h] < 0)
+        hit.setupAsPixel(detid[h], 1, 1);
+      else
+        hit.setupAsStrip(detid[h], cpcm[h], 1);
+      layer_hits[l].push_back(hit);
+    }
+  EventOfHits eoh(Config::TrkInfo);
+  for (int l = 0; l < n_layers; ++l) eoh.SuckInHits(l, layer_hits[l]);
+  const IterationConfig& itconf = Config::ItrInfo[g_iteration];
+  TrackVec tracks;
+  tracks.reserve(n);
+  for (int i = 0; i < n; ++i) tracks.push_back(make_track(i, n, par, err, chg));
+  std::unique_ptr<MkFinder> mkf(new MkFinder);
+  mkf->Setup(itconf.m_params, itconf.m_layer_configs[layer], nullptr);
+  for (int beg = 0; beg < n; beg += NN) {
+    const int end = std::min(beg + NN, n);
+    mkf->InputTracksAndHitIdx(tracks, beg, end, true);
+    mkf->SelectHitIndices(eoh.m_layers_of_hits[layer], end - beg);
+    for (int i = beg; i < end; ++i) {
+      const int x = mkf->XHitSize.At(i - beg, 0, 0);
+      xsize[i] = x;
+      for (int k = 0; k < 16; ++k) xidx[i * 16 + k] = k < x ? mkf->XHitArr.At(i - beg, k, 0) : -1;
+    }
+  }
+  mkf->Release();
+  return 0;
+}
+
 // The backward search's IterationParams of the selected iteration
 // (IterationConfig::m_backward_params, set by SetupBackwardSearch_*):
 // bk[8] in the iter_params layout, and flags[2] = {m_backward_drop_seed_hits,

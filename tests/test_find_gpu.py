@@ -186,6 +186,47 @@ def test_hit_mask_matches_reference(gpu_ctx, reflib):
     assert changed > 0.2 * ev.n_seeds
 
 
+@pytest.mark.parametrize("layer", [3, 4, 10, 45, 48, 21])
+def test_select_hit_indices_matches_reference(gpu_ctx, reflib, layer):
+    """The plain SelectHitIndices call (mkfg_find_select_hit_indices) on the
+    seeds' states moved onto the layer with wider position errors, in an
+    event with three noise hits per signal hit (windows hold up to the
+    16-hit limit; states off the layer come back outside), against the
+    reference's MkFinder::SelectHitIndices on the same states and hits: the
+    hit lists equal, in scan order."""
+    ev = synth.gen_cms_event(3000, seed=161, noise_frac=3.0)
+    rng = np.random.default_rng(161 + layer)
+    n = ev.n_seeds
+    par = ev.seed_par.astype(np.float32).copy()
+    err = ev.seed_err.astype(np.float32).copy()
+    g = cms2017()
+    L = g.layer(layer)
+    # States on the layer's surface (barrel: radius, endcap: z) with wider
+    # position errors.
+    r = np.hypot(par[0], par[1])
+    if L["is_barrel"] > 0.5:
+        scale = np.float32(L["propagate_to"]) / np.maximum(r, 1e-3)
+        par[0] *= scale
+        par[1] *= scale
+        par[2] = par[2] * scale
+    else:
+        par[2] = np.float32(L["propagate_to"]) * np.sign(np.where(par[2] == 0, 1, par[2]))
+    for k, f in ((0, 0.1), (2, 0.1), (5, 10.0)):
+        err[k] = err[k] + np.float32(f) * rng.random(n).astype(np.float32)
+    fnd = Finder(gpu_ctx, FindConfig(max_cands=M, chi2_cut=30.0, zero_c2=True))
+    fnd.upload(ev)
+    size, idx, wsr = fnd.select_hit_indices(0, layer, par, err)
+    from oracle.oracle import ref_select_hit_indices
+    rsize, ridx = ref_select_hit_indices(reflib, ev, layer, par, err, ev.seed_chg)
+    bad = [i for i in range(n) if size[i] != rsize[i] or
+           (size[i] > 0 and (idx[i, :size[i]] != ridx[i, :size[i]]).any())]
+    print(f"\nlayer {layer}: {n} states, {int((size > 0).sum())} with hits, "
+          f"{int((size == 16).sum())} at the 16-hit limit, {int((size < 0).sum())} outside; "
+          f"{len(bad)} differ")
+    assert (size > 0).sum() > 0.05 * n
+    assert len(bad) <= max(1, n // 1000)
+
+
 def test_silly_seeds_dropped_as_reference(gpu_ctx, reflib):
     """Seeds whose covariance has a negative diagonal, a NaN or an infinity
     are dropped before the finding (MkBuilder::seed_post_cleaning, which
