@@ -216,6 +216,27 @@ void ensure_cms2017() {
   g_cms2017_loaded = true;
 }
 
+// MkFinder::FindCandidatesCloneEngine's pixel same-layer check reads the
+// first three hit-on-track nodes of the comb candidate
+// (mkFit/MkFinder.cc:1195-1210); for a seed of two hits the third is
+// storage the vector has reserved but not written, whose content depends on
+// what earlier calls left on the heap. Filling that storage with nodes on
+// no layer (-1) after the seeds are loaded makes the read see fresh storage
+// every time, so the reference's result no longer depends on call history.
+void fill_unused_nodes(RefBuilder& b) {
+  EventOfCombCandidates& eocc = b.eocc();
+  for (int i = 0; i < eocc.m_size; ++i) {
+    std::vector<HoTNode>& v = eocc[i].m_hots;
+    HoTNode* d = v.data();
+    for (size_t k = v.size(); k < v.capacity(); ++k) {
+      d[k].m_hot.index = -1;
+      d[k].m_hot.layer = -1;
+      d[k].m_chi2 = 0.f;
+      d[k].m_prev_idx = -1;
+    }
+  }
+}
+
 // The StdSeq quality filters (mkFit/MkStdSeqs.h:39-148) by code: 0
 // qfilter_nan_n_silly, 1 qfilter_n_hits, 2 qfilter_n_hits_pixseed,
 // 3 qfilter_n_layers, 4 qfilter_n_layers_pixelLess, 5 qfilter_pixelLessFwd,
@@ -639,6 +660,7 @@ int ref_find(int n_layers_in, const int* layer_begin, const float* hpos, const f
   for (int r = 0; r < std::max(1, repeat); ++r) {
     builder.begin_event(&job, nullptr, "ref_find");
     builder.find_tracks_load_seeds(seeds);
+    fill_unused_nodes(builder);
     const double t0 = now_s();
     builder.FindTracksCloneEngine();
     if (g_qf_pre >= 0 && apply_qfilter(builder, g_qf_pre)) return -3;
@@ -856,6 +878,7 @@ extern "C" int ref_find_batch(int n_ev, const int* hit_off, const int* seed_off,
       for (int e = rg.begin(); e < rg.end(); ++e) {
         builders[e]->begin_event(jobs[e].get(), nullptr, "ref_find_batch");
         builders[e]->find_tracks_load_seeds(seeds[e]);
+        fill_unused_nodes(*builders[e]);
         builders[e]->FindTracksCloneEngine();
       }
     });

@@ -210,7 +210,12 @@ def test_select_hit_indices_matches_reference(gpu_ctx, reflib, layer):
         par[1] *= scale
         par[2] = par[2] * scale
     else:
+        # On the disk, at a radius inside its [rin, rout].
         par[2] = np.float32(L["propagate_to"]) * np.sign(np.where(par[2] == 0, 1, par[2]))
+        rt = L["rin"] + (L["rout"] - L["rin"]) * rng.uniform(0.1, 0.9, n)
+        scale = (rt / np.maximum(r, 1e-3)).astype(np.float32)
+        par[0] *= scale
+        par[1] *= scale
     for k, f in ((0, 0.1), (2, 0.1), (5, 10.0)):
         err[k] = err[k] + np.float32(f) * rng.random(n).astype(np.float32)
     fnd = Finder(gpu_ctx, FindConfig(max_cands=M, chi2_cut=30.0, zero_c2=True))
