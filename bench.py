@@ -42,8 +42,8 @@ FIND_MAX_CANDS = 6
 FIND_CHI2_CUT = 30.0
 # Plain single-event workload: 800 tracks, 1% noise.
 PLAIN_TRACKS = 800
-# Algorithmic FLOPs per unit of work (counted in DESIGN.md from the
-# generated products and the restated arithmetic): propagation of a
+# Algorithmic FLOPs per unit of work (counted from the generated products
+# and the restated arithmetic): propagation of a
 # candidate to a layer + hit selection; propagation to a hit + chi2; the
 # update step (propagation to the hit + Kalman update).
 FLOP_LAYER_PROP = 1000
