@@ -40,6 +40,8 @@ FIND_NOISE = 0.01
 FIND_DENSITY_RATIO = 20.0
 FIND_MAX_CANDS = 6
 FIND_CHI2_CUT = 30.0
+# Batches in flight in the end-to-end measurement (one context each).
+E2E_IN_FLIGHT = 3
 # Plain single-event workload: 800 tracks, 1% noise.
 PLAIN_TRACKS = 800
 # Algorithmic FLOPs per unit of work (counted from the generated products
@@ -305,47 +307,53 @@ def run_ours(args):
             out = finder.download_best(n_seeds, out)
             ts.append(time.perf_counter() - t0)
         t_serial = statistics.median(ts[1:])
-        # Two batches in flight on two contexts (the reference keeps events in
-        # flight the same way): the host work of a batch's upload overlaps the
-        # device run of the previous one. Every step still copies its inputs
-        # from host memory and its results back to host memory.
-        ctx2 = Context(local)
-        finder2 = Finder(ctx2, FindConfig(max_cands=FIND_MAX_CANDS, chi2_cut=FIND_CHI2_CUT,
-                                          zero_c2=True))
-        pair, outs = (finder, finder2), [out, None]
+        # E2E_IN_FLIGHT batches in flight on as many contexts (the reference
+        # keeps events in flight the same way): the host work of a batch's
+        # upload overlaps the device runs of the earlier ones. Every step
+        # still copies its inputs from host memory and its results back to
+        # host memory; a context's results are read before it takes the
+        # next batch.
+        extra = [Context(local) for _ in range(E2E_IN_FLIGHT - 1)]
+        ring = [finder] + [Finder(c, FindConfig(max_cands=FIND_MAX_CANDS, chi2_cut=FIND_CHI2_CUT,
+                                                zero_c2=True)) for c in extra]
+        outs = [out] + [None] * (E2E_IN_FLIGHT - 1)
 
         def pipelined(steps):
-            pending = None
+            pending = []
             for i in range(steps):
-                k = i % 2
-                pair[k].upload_batch(events)
-                pair[k].run_graph()
-                if pending is not None:
-                    outs[pending] = pair[pending].download_best(n_seeds, outs[pending])
-                pending = k
-            outs[pending] = pair[pending].download_best(n_seeds, outs[pending])
+                k = i % E2E_IN_FLIGHT
+                if len(pending) == E2E_IN_FLIGHT:
+                    j = pending.pop(0)
+                    outs[j] = ring[j].download_best(n_seeds, outs[j])
+                ring[k].upload_batch(events)
+                ring[k].run_graph()
+                pending.append(k)
+            for j in pending:
+                outs[j] = ring[j].download_best(n_seeds, outs[j])
 
-        pipelined(2)
+        pipelined(E2E_IN_FLIGHT)
         t0 = time.perf_counter()
         pipelined(e_steps)
         t = (time.perf_counter() - t0) / e_steps
-        # Both contexts found the same candidates.
-        for k in ("n_cands", "hit_idx", "hit_lyr", "par"):
-            if not np.array_equal(outs[0][k], outs[1][k]):
-                raise RuntimeError(f"pipelined contexts disagree on {k}")
-        ctx2.close()
+        # Every context found the same candidates.
+        for o in outs[1:]:
+            for k in ("n_cands", "hit_idx", "hit_lyr", "par"):
+                if not np.array_equal(outs[0][k], o[k]):
+                    raise RuntimeError(f"pipelined contexts disagree on {k}")
+        for c in extra:
+            c.close()
         h2d = sum(e.hit_pos.nbytes + e.hit_err.nbytes + e.hit_detid.nbytes + e.hit_cpcm.nbytes +
                   e.seed_par.nbytes + e.seed_err.nbytes + e.seed_chg.nbytes for e in events)
         d2h = sum(v.nbytes for v in out.values())
         e2e = {"value": n_events / t, "unit": "events/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": t * 1e3,
-               "batches_in_flight": 2,
+               "batches_in_flight": E2E_IN_FLIGHT,
                "one_batch_at_a_time": {"value": n_events / t_serial, "ms_per_step": t_serial * 1e3},
                "entry": "mkfg_find_upload_batch + mkfg_find_run_graph + mkfg_find_download_best "
                         "(seed partition and initial candidates on the host, copies, device "
                         "hit-index build, export of the best candidate per seed as "
-                        "MkBuilder::export_best_comb_cands into reused host arrays); two "
-                        "contexts alternate batches"}
+                        "MkBuilder::export_best_comb_cands into reused host arrays); "
+                        f"{E2E_IN_FLIGHT} contexts take batches in turn"}
 
     stages = None if args.no_e2e else run_iteration_stages(ctx, stream, finder, events, n_seeds)
     fit = None if fit_batch is None else run_fit(ctx, stream, fit_batch, args)
