@@ -32,18 +32,21 @@ sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
-# Batched finding workload: 64 events, Poisson(3000) tracks clipped to
-# [500, 12000], CMS-2017 geometry, noise 1% x a per-layer ramp up to 20x.
-FIND_EVENTS = 64
-FIND_MEAN_TRACKS = 3000
-FIND_NOISE = 0.01
-FIND_DENSITY_RATIO = 20.0
-FIND_MAX_CANDS = 6
-FIND_CHI2_CUT = 30.0
+from mkfit_b200 import workloads as W  # noqa: E402
+
+# Workloads (mkfit_b200/workloads.py): batched finding, 64 CMS-2017 events,
+# Poisson(3000) tracks clipped to [500, 12000], noise 1% x a per-layer ramp
+# up to 20x; the plain one-event form on 800 tracks; the fit; the
+# differentiable fit; PU200-like finding.
+FIND_EVENTS = W.FIND_EVENTS
+FIND_MEAN_TRACKS = W.FIND_MEAN_TRACKS
+FIND_NOISE = W.FIND_NOISE
+FIND_DENSITY_RATIO = W.FIND_DENSITY_RATIO
+FIND_MAX_CANDS = W.FIND_MAX_CANDS
+FIND_CHI2_CUT = W.FIND_CHI2_CUT
 # Batches in flight in the end-to-end measurement (one context each).
 E2E_IN_FLIGHT = 3
-# Plain single-event workload: 800 tracks, 1% noise.
-PLAIN_TRACKS = 800
+PLAIN_TRACKS = W.PLAIN_TRACKS
 # Algorithmic FLOPs per unit of work (counted from the generated products
 # and the restated arithmetic): propagation of a
 # candidate to a layer + hit selection; propagation to a hit + chi2; the
@@ -60,20 +63,18 @@ BYTES_HIT_CHI2 = 36 + 108
 BYTES_UPDATE = 112 + 36 + 112
 # Kernels per layer-plan step in the graph form.
 KERNELS_PER_LAYER_STEP = 5
-# Fit (secondary metric): toy MC, 10 barrel layers.
-FIT_TRACKS_PER_EVENT = 20000
-FIT_EVENTS = 16
-FIT_LAYERS = 10
+FIT_TRACKS_PER_EVENT = W.FIT_TRACKS_PER_EVENT
+FIT_EVENTS = W.FIT_EVENTS
+FIT_LAYERS = W.FIT_LAYERS
 FLOP_FIT_TRACK_LAYER = 1130
-# Differentiable fit: 50,000 toy tracks x 10 layers on a misaligned detector
-# (r-phi and z offsets N(0, 20 um), material scale 1 +- 0.1), gradient of
-# the summed chi2 w.r.t. 30 layer parameters at the nominal point.
-ADJ_TRACKS = 50000
-# High-pileup finding: 16 events x 10,000 helices, pT 0.3-50 GeV, |eta| < 2.5,
-# 5% noise plus pileup-like uniform noise bringing each event to ~600k hits.
-PU_EVENTS = 16
-PU_TRACKS = 10000
-PU_NOISE = 2.16
+ADJ_TRACKS = W.ADJ_TRACKS
+PU_EVENTS = W.PU_EVENTS
+PU_TRACKS = W.PU_TRACKS
+PU_NOISE = W.PU_NOISE
+# Events of each workload the CPU baselines find (the whole batched-finding
+# step; half of the PU200-like step).
+CPU_FIND_EVENTS = FIND_EVENTS
+CPU_PU_EVENTS = 8
 
 
 def parse():
@@ -94,13 +95,7 @@ def parse():
 
 # ----------------------------------------------------------------------------- inputs
 def find_event_args(n_events, rank):
-    from mkfit_b200 import synth
-    from mkfit_b200.geometry import cms2017
-    from mkfit_b200.dist import rank_seed
-    sizes = synth.batch_event_sizes(n_events, FIND_MEAN_TRACKS, 500, 12000, seed=rank_seed(0xB200, rank))
-    ramp = synth.density_ramp(cms2017().n_layers, FIND_DENSITY_RATIO)
-    return [dict(n_tracks=int(n), seed=rank_seed(0xE000, rank) + i, noise_frac=FIND_NOISE,
-                 noise_scale=ramp) for i, n in enumerate(sizes)]
+    return W.find_event_args(n_events, rank)
 
 
 def generate(args_list):
@@ -114,13 +109,7 @@ def generate(args_list):
 
 
 def make_fit_batch(n_events, rank):
-    from mkfit_b200 import synth
-    evs = [synth.gen_fit_event(FIT_TRACKS_PER_EVENT, seed=0xC0FFEE + 1000 * rank + e)
-           for e in range(n_events)]
-    cat = lambda k, ax: np.ascontiguousarray(np.concatenate([getattr(e, k) for e in evs], axis=ax))
-    return synth.FitEvent(par=cat("par", 1), err=cat("err", 1), chg=cat("chg", 0),
-                          hit_pos=cat("hit_pos", 2), hit_err=cat("hit_err", 2),
-                          rl_grid=evs[0].rl_grid, xi_grid=evs[0].xi_grid, radii=evs[0].radii)
+    return W.fit_batch(n_events, rank)
 
 
 # ----------------------------------------------------------------------------- utilities
@@ -211,15 +200,101 @@ def timed_events(stream, fn, steps):
     return [a.elapsed_time(b) for a, b in zip(starts, ends)]
 
 
+# Algorithmic bytes of the clone step (k_clone): per candidate of a cloned
+# seed, its record-presence mask, hole/extra code, extra stop node and 11
+# counters read (56 B); per record present, the 16-byte record; per new
+# candidate, the parent's 27-float state read and written to the new slot
+# and 9 counters written (108 + 108 + 36 B); per Kalman update listed, its
+# hit-on-track node (12 B) and update-list entry (8 B).
+CLONE_BYTES_PER_CAND = 56
+CLONE_BYTES_PER_RECORD = 16
+CLONE_BYTES_PER_NEW_CAND = 252
+CLONE_BYTES_PER_UPDATE = 20
+
+
+# DRAM traffic of k_clone per new candidate written, from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum over the 42 clone launches
+# of one replay of an 8-event batch of the same workload, 1.866 GB for
+# 3,427,364 new candidates; profiles/clone_kernel_cms2017_batch.md).
+CLONE_DRAM_BYTES_PER_NEW_CAND = 544.4
+
+
+def clone_traffic_per_launch(work):
+    if CLONE_DRAM_BYTES_PER_NEW_CAND is None:
+        return None
+    return CLONE_DRAM_BYTES_PER_NEW_CAND * work["new_cands"] / work["steps"]
+
+
+def kernel_rooflines(work, kt, fp32_peak_tf, peaks):
+    """Rooflines of the finding kernels from one timed replay (kt: ms per
+    step per kernel) and the step's work counters: the dominant kernel by
+    time against its bound, and the dominant FP32 kernel against the FP32
+    peak."""
+    steps = work["steps"]
+    hbm = peaks.get("hbm_gbs")
+    fp = {"propagate": (work["active_cands"], FLOP_LAYER_PROP, BYTES_LAYER_PROP),
+          "chi2": (work["hit_pairs"], FLOP_HIT_CHI2, BYTES_HIT_CHI2),
+          "update": (work["updates"], FLOP_UPDATE, BYTES_UPDATE)}
+    clone_bytes = (CLONE_BYTES_PER_CAND * work["active_cands"] +
+                   CLONE_BYTES_PER_RECORD * work["records"] +
+                   CLONE_BYTES_PER_NEW_CAND * work["new_cands"] +
+                   CLONE_BYTES_PER_UPDATE * work["updates"])
+    f_dom = max(fp, key=lambda k: kt[k])
+    units, f_unit, b_unit = fp[f_dom]
+    f_tf = units * f_unit / (kt[f_dom] * 1e-3) / 1e12
+    fp32 = {"kernel": f"k_{f_dom}", "bound": "fp32", "achieved": f_tf, "peak": fp32_peak_tf,
+            "unit": "TFLOP/s", "frac": f_tf / fp32_peak_tf if fp32_peak_tf else None,
+            "peak_source": "measured FP32 FMA probe (mkfg_probe_fp32_peak), same run (of measured)",
+            "per_launch_ms": kt[f_dom] / steps, "units_per_step": units, "flop_per_unit": f_unit,
+            "bytes_per_unit": b_unit,
+            "hbm_achieved_gbs": units * b_unit / (kt[f_dom] * 1e-3) / 1e9}
+    by_time = max((k for k in kt if k not in ("reset", "merge")), key=lambda k: kt[k])
+    if by_time == "clone":
+        gbs = clone_bytes / (kt["clone"] * 1e-3) / 1e9
+        dom = {"kernel": "k_clone", "bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s",
+               "frac": gbs / hbm if hbm else None,
+               "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+               "per_launch_ms": kt["clone"] / steps,
+               "algorithmic_bytes_per_launch": clone_bytes / steps,
+               "bytes_model": {"per_candidate": CLONE_BYTES_PER_CAND,
+                               "per_record": CLONE_BYTES_PER_RECORD,
+                               "per_new_candidate": CLONE_BYTES_PER_NEW_CAND,
+                               "per_update": CLONE_BYTES_PER_UPDATE},
+               "traffic": clone_traffic_per_launch(work),
+               "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of k_clone "
+                                 "per new candidate, scaled to this launch "
+                                 "(profiles/clone_kernel_cms2017_batch.md)"}
+    else:
+        dom = dict(fp32)
+    return {"dominant": dom, "fp32": fp32, "fp32_peak": fp32_peak_tf}
+
+
+def find_config_line(events, world):
+    """The `config` of the batched-finding line, shared by both arms."""
+    n_seeds = sum(e.n_seeds for e in events)
+    n_hits = sum(e.n_hits for e in events)
+    return {
+        "workload": (f"batched clone-engine finding: {len(events)} CMS-2017 events per step, "
+                     f"Poisson({FIND_MEAN_TRACKS}) tracks clipped to [500, 12000], "
+                     f"noise {FIND_NOISE:.0%} x per-layer ramp up to {FIND_DENSITY_RATIO:.0f}x, "
+                     f"maxCandsPerSeed {FIND_MAX_CANDS}, chi2 cut {FIND_CHI2_CUT:.0f}"),
+        "events_per_step": len(events), "seeds_per_step": n_seeds, "hits_per_step": n_hits,
+        "l2": "inputs + candidate state ~%.0f MB per step (L2 126 MB); no flush" % (
+            (n_hits * 40 + n_seeds * 8 * 37 * 4 * 3) / 1e6),
+        "parallelism": f"dp{world} (independent event batches per GPU)",
+    }
+
+
 # ----------------------------------------------------------------------------- ours
 def run_ours(args):
     rank = int(os.environ.get("RANK", "0"))
     # Inputs first (process pool before any CUDA call).
     events = generate(find_event_args(args.events, rank))
     from mkfit_b200 import synth
-    plain_ev = synth.gen_cms_event(PLAIN_TRACKS, seed=0xC0DE + rank, noise_frac=0.01)
+    plain_ev = synth.gen_cms_event(**W.plain_event_args(rank))
     fit_batch = None if args.no_fit else make_fit_batch(FIT_EVENTS, rank)
-    adj_ev = None if args.no_fit else adjoint_event(rank)
+    # One sample for all ranks: the differentiable fit splits its tracks.
+    adj_ev = None if args.no_fit else adjoint_event(0)
     pu_events = None if args.no_pu else generate(pu_event_args(rank))
 
     import torch
@@ -252,6 +327,9 @@ def run_ours(args):
     for _ in range(args.warmup):
         finder.run_graph()
     ctx.synchronize()
+    # Work counters of the step: one eager run of the same sequence, which
+    # also counts the clone step's records and new candidates.
+    finder.run()
     work = finder.work()
     peak = fp32_peak(ctx)
     sampler = ClockSampler(local)
@@ -277,17 +355,13 @@ def run_ours(args):
 
     # Per-kernel device times: one replay of the same step as the plain
     # launch sequence with a CUDA event after every kernel (outside the
-    # timed region), for the dominant FP32 kernel's roofline.
+    # timed region), for the rooflines of the kernels.
     kt = finder.run_timed()
     kt_total = sum(kt.values())
-    fp_kernels = {"propagate": (work["active_cands"], FLOP_LAYER_PROP, BYTES_LAYER_PROP),
-                  "chi2": (work["hit_pairs"], FLOP_HIT_CHI2, BYTES_HIT_CHI2),
-                  "update": (work["updates"], FLOP_UPDATE, BYTES_UPDATE)}
-    dom = max(fp_kernels, key=lambda k: kt[k])
-    units, f_unit, b_unit = fp_kernels[dom]
-    per_launch_ms = kt[dom] / work["steps"]
-    dom_tf = units * f_unit / (kt[dom] * 1e-3) / 1e12
-    dom_gbs = units * b_unit / (kt[dom] * 1e-3) / 1e9
+    rl = kernel_rooflines(work, kt, peak, load_measured_peaks())
+    # The best candidate per seed of this step, for the comparison with the
+    # reference CPU run on the same events.
+    gpu_best = finder.download_best(n_seeds)
     if args.step_profile and rank == 0:
         print_step_profile(finder.step_profile())
 
@@ -357,8 +431,9 @@ def run_ours(args):
 
     stages = None if args.no_e2e else run_iteration_stages(ctx, stream, finder, events, n_seeds)
     fit = None if fit_batch is None else run_fit(ctx, stream, fit_batch, args)
-    adjoint = None if adj_ev is None else run_adjoint(ctx, stream, adj_ev, args)
-    pu200 = None if pu_events is None else run_pu200(ctx, stream, finder, pu_events, args)
+    adjoint = None if adj_ev is None else run_adjoint(ctx, stream, adj_ev, args, world, rank)
+    pu200, pu_best = (None, None) if pu_events is None else run_pu200(ctx, stream, finder,
+                                                                      pu_events, args)
 
     peaks = load_measured_peaks()
     line = {
@@ -374,17 +449,7 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded, mkfit_b200.synth.gen_cms_event on the CMS-2017 layer table)",
-        "config": {
-            "workload": (f"batched clone-engine finding: {n_events} CMS-2017 events per step, "
-                         f"Poisson({FIND_MEAN_TRACKS}) tracks clipped to [500, 12000], "
-                         f"noise {FIND_NOISE:.0%} x per-layer ramp up to {FIND_DENSITY_RATIO:.0f}x, "
-                         f"maxCandsPerSeed {FIND_MAX_CANDS}, chi2 cut {FIND_CHI2_CUT:.0f}, "
-                         "one CUDA-graph replay per step"),
-            "events_per_step": n_events, "seeds_per_step": n_seeds, "hits_per_step": n_hits,
-            "l2": "inputs + candidate state ~%.0f MB per step (L2 126 MB); no flush" % (
-                (n_hits * 40 + n_seeds * 8 * 37 * 4 * 3) / 1e6),
-            "parallelism": f"dp{world} (independent event batches per GPU)",
-        },
+        "config": find_config_line(events, world),
         "plain_form": {
             "cms_800_tracks": {"events_per_launch_sequence": 1, "value": 1e3 / plain_cfg1_ms,
                                "unit": "events/s", "ms_per_event": plain_cfg1_ms,
@@ -393,29 +458,13 @@ def run_ours(args):
                              "ms_per_event": plain_b_ms, "seeds": events[0].n_seeds},
             "batched_over_plain": (value / world) / (1e3 / plain_b_ms),
         },
-        "roofline": {
-            "bound": "fp32",
-            "kernel": f"k_{dom}",
-            "achieved": dom_tf,
-            "peak": peak,
-            "unit": "TFLOP/s",
-            "frac": dom_tf / peak if peak else None,
-            "peak_source": "measured FP32 FMA probe (mkfg_probe_fp32_peak), same run (of measured)",
-            "per_launch_ms": per_launch_ms,
-            "units_per_step": units,
-            "flop_per_unit": f_unit,
-            "bytes_per_unit": b_unit,
-            "hbm_achieved_gbs": dom_gbs,
-            "hbm_peak_gbs": peaks.get("hbm_gbs"),
-            "hbm_frac": dom_gbs / peaks["hbm_gbs"] if peaks.get("hbm_gbs") else None,
-            "traffic": None,
-            "traffic_note": "DRAM bytes of the kernels: profiles/find_kernels_plain_cms2017.md",
-            "kernel_ms_per_step": {k: v for k, v in kt.items()},
-            "kernel_share": {k: v / kt_total for k, v in kt.items()},
-            "step": {"scope": "whole finding step (all kernels of the graph)",
-                     "achieved": achieved_tf, "frac": achieved_tf / peak if peak else None,
-                     "flop_per_step": flops, "work_per_step": work},
-        },
+        "roofline": dict(rl["dominant"], kernel_ms_per_step=dict(kt),
+                         kernel_share={k: v / kt_total for k, v in kt.items()},
+                         fp32_kernel=rl["fp32"],
+                         step={"scope": "whole finding step (all kernels of the graph)",
+                               "achieved_tflops": achieved_tf,
+                               "fp32_frac": achieved_tf / rl["fp32_peak"] if rl["fp32_peak"] else None,
+                               "flop_per_step": flops, "work_per_step": work}),
         "e2e": e2e,
         "gpu_launches": args.steps * (2 + KERNELS_PER_LAYER_STEP * work["steps"]),
         "gpu_launches_note": (f"kernels in the timed region: one CUDA graph replay per step = reset + "
@@ -427,9 +476,10 @@ def run_ours(args):
         "iteration_stages": stages,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_find(events)
+        line["cpu_baseline"] = cpu_baseline_find(events, gpu_best)
         if pu_events is not None:
-            line["cpu_baseline"]["pu200"] = cpu_baseline_find(pu_events, n_sample=2)
+            line["cpu_baseline"]["pu200"] = cpu_baseline_find(pu_events, pu_best,
+                                                              n_sample=CPU_PU_EVENTS)
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -455,30 +505,29 @@ def run_fit(ctx, stream, batch, args):
 
 
 def adjoint_event(rank):
-    from mkfit_b200 import synth
-    rng = np.random.default_rng(0xAD1 + rank)
-    return synth.gen_fit_event(ADJ_TRACKS, seed=0xAD10 + rank,
-                               align_rphi=rng.normal(0, 0.002, FIT_LAYERS),
-                               align_z=rng.normal(0, 0.002, FIT_LAYERS),
-                               mat_scale=1 + rng.uniform(-0.1, 0.1, FIT_LAYERS))
+    return W.adjoint_event(rank)
 
 
-def run_adjoint(ctx, stream, ev, args):
+def run_adjoint(ctx, stream, ev, args, world=1, rank=0):
     """Forward (summed chi2, checkpoints) + adjoint (30-parameter gradient)
-    through the C ABI, timed per step with CUDA events."""
+    through the C ABI, timed per step with CUDA events. With N ranks the
+    tracks are split into one share per rank and each step ends with one
+    all-reduce of the 31 sums (strong scaling: the sample is the same)."""
     import ctypes
     import torch
     from mkfit_b200 import capi
+    from mkfit_b200 import dist as mdist
     from mkfit_b200.align import AlignedFit, _bind
-    fit = AlignedFit(ctx, ev, material=True)
+    begin, end = mdist.track_share(ev.n, world, rank)
+    fit = AlignedFit(ctx, ev.tracks(begin, end), material=True)
     lib = ctx.lib
     _bind(lib)
     th = fit.nominal()
-    n = ev.n
+    n = end - begin
     dev = th.device
     ckpt = torch.empty((fit.n_steps, 27, n), dtype=torch.float32, device=dev)
-    total = torch.empty((), dtype=torch.float64, device=dev)
-    grad = torch.empty((fit.n_steps, 3), dtype=torch.float64, device=dev)
+    sums = torch.empty(1 + 3 * fit.n_steps, dtype=torch.float64, device=dev)
+    total, grad = sums[:1], sums[1:]
     gout = torch.ones((), dtype=torch.float32, device=dev)
     a = fit._args(th, ckpt, total)
     torch.cuda.synchronize()
@@ -487,26 +536,33 @@ def run_adjoint(ctx, stream, ev, args):
         capi.check(lib.mkfg_align_chi2_forward(ctx.handle, ctypes.byref(a)))
         capi.check(lib.mkfg_align_chi2_backward(ctx.handle, ctypes.byref(a), gout.data_ptr(),
                                                 grad.data_ptr()))
+        if world > 1:
+            import torch.distributed as tdist
+            with torch.cuda.stream(stream):
+                tdist.all_reduce(sums)
     for _ in range(args.warmup):
         step()
     ctx.synchronize()
+    mdist.barrier(world)
     ms = timed_events(stream, step, args.steps)
-    t = sum(ms) / len(ms)
+    t = mdist.max_over_ranks(sum(ms) / len(ms), world)
     g = grad.cpu().numpy()
-    return {"metric": "tracks/s (forward + adjoint)", "value": n / (t * 1e-3),
-            "unit": "tracks/s", "ms_per_step": t, "tracks_per_step": n,
-            "workload": (f"differentiable fit: {n} toy tracks x {FIT_LAYERS} barrel layers, "
+    return {"metric": "tracks/s (forward + adjoint)", "value": ev.n / (t * 1e-3),
+            "unit": "tracks/s", "ms_per_step": t, "tracks_per_step": ev.n,
+            "scaling": "strong" if world > 1 else None,
+            "workload": (f"differentiable fit: {ev.n} toy tracks x {FIT_LAYERS} barrel layers, "
                          "misaligned detector (offsets N(0, 20 um), material scale 1 +- 0.1), "
                          "summed chi2 and its gradient w.r.t. 30 layer parameters at nominal, "
-                         "FP32 forward with per-layer checkpoints + FP32 adjoint, 2 launches"),
+                         "FP32 forward with per-layer checkpoints + FP32 adjoint, 2 launches"
+                         + (f", tracks split over {world} ranks + one all-reduce of the 31 "
+                            "sums per step" if world > 1 else "")),
             "chi2_sum": float(total.item()),
             "grad_norm": float(np.linalg.norm(g)),
             "accuracy": "gradient vs FP64 central finite differences: tests/test_adjoint_gpu.py"}
 
 
 def pu_event_args(rank):
-    return [dict(n_tracks=PU_TRACKS, seed=0x9200 + 1000 * rank + i, pt_range=(0.3, 50.0),
-                 eta_max=2.5, noise_frac=PU_NOISE) for i in range(PU_EVENTS)]
+    return W.pu_event_args(rank)
 
 
 def run_iteration_stages(ctx, stream, finder, events, n_seeds):
@@ -573,6 +629,7 @@ def run_pu200(ctx, stream, finder, events, args):
     ms = timed_events(stream, finder.run_graph, max(3, args.steps // 2))
     t = sum(ms) / len(ms)
     work = finder.work()
+    best = finder.download_best(sum(e.n_seeds for e in events))
     flops = (work["active_cands"] * FLOP_LAYER_PROP + work["hit_pairs"] * FLOP_HIT_CHI2 +
              work["updates"] * FLOP_UPDATE)
     return {"metric": "events built/s", "value": len(events) / (t * 1e-3), "unit": "events/s",
@@ -583,28 +640,65 @@ def run_pu200(ctx, stream, finder, events, args):
                          "(pT log-uniform 0.3-50 GeV, |eta| < 2.5, vertex sigma_z 5 cm), 5% noise "
                          f"plus uniform pileup-like noise (noise fraction {PU_NOISE} in total) to "
                          "reach ~600k hits per event, one CUDA-graph replay per step"),
-            "achieved_tflops": flops / (t * 1e-3) / 1e12, "work_per_step": work}
+            "achieved_tflops": flops / (t * 1e-3) / 1e12, "work_per_step": work}, best
 
 
-def cpu_baseline_find(events, n_sample=8):
+def best_mismatch(ref, gpu_best):
+    """Seeds whose best-candidate hit list (or candidate presence) differs
+    between the reference (ref_find_batch summaries) and the GPU
+    (download_best), over the seeds both hold."""
+    n = min(len(ref["n_cands"]), len(gpu_best["n_cands"]))
+    bad = 0
+    for s in range(n):
+        rc, gc = int(ref["n_cands"][s]) > 0, int(gpu_best["n_cands"][s]) > 0
+        if rc != gc:
+            bad += 1
+            continue
+        if not rc:
+            continue
+        k = int(ref["ntot"][s])
+        if (k != int(gpu_best["ntot"][s]) or
+                not np.array_equal(ref["hit_idx"][s, :k], gpu_best["hit_idx"][s, :k]) or
+                not np.array_equal(ref["hit_lyr"][s, :k], gpu_best["hit_lyr"][s, :k])):
+            bad += 1
+    return bad, n
+
+
+def cpu_baseline_find(events, gpu_best=None, n_sample=None):
+    """The reference CPU clone engine on the host cores (all threads, events
+    in flight), best of 3, on the first n_sample events (all by default);
+    with gpu_best (the GPU's best candidate per seed of the same events),
+    also the best-candidate hit-list mismatch rate against the GPU."""
     from oracle.oracle import RefLib, ref_find_batch
     ref = RefLib()
     threads = os.cpu_count()
     ref.set_threads(threads)
-    sample = events[:n_sample]
+    sample = events if n_sample is None else events[:n_sample]
     t0 = time.perf_counter()
     o = ref_find_batch(ref, sample, max_cands=FIND_MAX_CANDS, chi2_cut=FIND_CHI2_CUT, repeat=3)
     wall = time.perf_counter() - t0
-    return {"value": len(sample) / o["seconds"], "unit": "events/s", "cores": threads,
+    line = {"value": len(sample) / o["seconds"], "unit": "events/s", "cores": threads,
             "kind": "reference",
-            "sample": (f"{len(sample)} of the step's events ({sum(e.n_seeds for e in sample)} seeds), "
+            "sample": (f"{len(sample)} of the step's {len(events)} events "
+                       f"({sum(e.n_seeds for e in sample)} seeds), "
                        f"reference find_tracks_load_seeds + FindTracksCloneEngine, events in flight "
                        f"on a {threads}-thread pool, AVX2 Matriplex (NN=8), best of 3, "
                        f"{wall:.1f} s wall incl. hit-index build")}
+    if gpu_best is not None:
+        bad, n = best_mismatch(o, gpu_best)
+        line["mismatch"] = {"best_candidate_hit_list": bad / max(n, 1), "seeds_differing": bad,
+                            "seeds_compared": n,
+                            "note": "GPU batched form vs the reference on the same events; every "
+                                    "mismatch class is checked by tests/test_find_measured_gpu.py"}
+    return line
 
 
 # ----------------------------------------------------------------------------- reference
 def run_reference(args):
+    """The reference's own CPU clone engine (the unmodified sources compiled
+    in oracle/_ref) on the host cores with all threads and every event of
+    the batch in flight, on the same events and configuration as the GPU
+    arm; each step finds the whole batch."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -616,31 +710,29 @@ def run_reference(args):
                           "from the reference sources)"}))
         return
     events = generate(find_event_args(args.events, 0))
-    sample = events[:8]
     ref = RefLib()
     threads = os.cpu_count()
     ref.set_threads(threads)
     for _ in range(max(1, min(args.warmup, 2))):
-        ref_find_batch(ref, sample, max_cands=FIND_MAX_CANDS, chi2_cut=FIND_CHI2_CUT)
+        ref_find_batch(ref, events, max_cands=FIND_MAX_CANDS, chi2_cut=FIND_CHI2_CUT)
     secs = []
     for _ in range(args.steps):
-        o = ref_find_batch(ref, sample, max_cands=FIND_MAX_CANDS, chi2_cut=FIND_CHI2_CUT)
+        o = ref_find_batch(ref, events, max_cands=FIND_MAX_CANDS, chi2_cut=FIND_CHI2_CUT)
         secs.append(o["seconds"])
     total = sum(secs)
-    value = len(sample) * args.steps / total
+    value = len(events) * args.steps / total
     line = {
         "impl": "reference",
         "metric": "events built/s", "value": value, "unit": "events/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded, mkfit_b200.synth.gen_cms_event on the CMS-2017 layer table)",
-        "config": {"workload": (f"clone-engine finding, CMS-2017: a bounded sample of {len(sample)} "
-                                f"of the GPU arm's {len(events)} events per step, events in flight"),
-                   "events_per_step": len(sample),
-                   "seeds_per_step": sum(e.n_seeds for e in sample)},
+        "config": find_config_line(events, 1),
         "cpu_baseline": {"value": value, "unit": "events/s", "cores": threads, "kind": "reference",
-                         "sample": f"{len(sample)} events per step on a {threads}-thread pool, "
-                                   "reference MkBuilder::FindTracksCloneEngine, AVX2 Matriplex"},
+                         "sample": f"all {len(events)} events of the step, in flight on a "
+                                   f"{threads}-thread pool, reference find_tracks_load_seeds + "
+                                   "MkBuilder::FindTracksCloneEngine timed region, AVX2 "
+                                   "Matriplex (NN=8)"},
         "e2e": {"value": value, "unit": "events/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
         "gpu_launches": 0,
@@ -648,8 +740,24 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def spawn_ranks(args):
+    """`--gpus N` without a launcher: starts N ranks of this script (one per
+    GPU) with torch.distributed.run on 127.0.0.1 and returns their exit
+    status; rank 0 prints the line."""
+    import socket
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={args.gpus}", "--master-addr", "127.0.0.1",
+           f"--master-port={port}", os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(spawn_ranks(args))
     if args.impl == "reference":
         run_reference(args)
     else:

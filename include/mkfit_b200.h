@@ -203,6 +203,10 @@ typedef struct {
   int32_t sort_seed_hits;
 } mkfg_find_config;
 
+/* The finder takes a copy of the context's material map (mkfg_set_material)
+ * here: a later mkfg_set_material on the same context (e.g. for a fit on
+ * another detector) does not change what the finding propagates through;
+ * call mkfg_finder_setup again to take the new map. */
 int mkfg_finder_setup(mkfg_context* ctx, const mkfg_find_config* cfg);
 
 /* ---- memoryFile event files (DataFile / Event::write_out / read_in,
@@ -541,6 +545,13 @@ int mkfg_find_work(mkfg_context* ctx, int64_t* active_cands, int64_t* hit_pairs,
 /* Diagnostics of the last mkfg_find_work call: chi2 evaluations counted by
  * the chi2 kernel, seed-steps handled by the clone kernel. */
 int mkfg_find_work_detail(mkfg_context* ctx, int64_t* chi2_evals, int64_t* seeds_cloned);
+
+/* Clone-step counters of the last mkfg_find_work call: the records
+ * (IdxChi2List entries, hits and holes) present when the seeds were ranked
+ * and the new candidates written. Counted by the eager run (mkfg_find_run)
+ * only; zero after a graph replay. Diagnostic; no reference counterpart
+ * (the reference's CandCloner keeps no such totals). */
+int mkfg_find_work_clone(mkfg_context* ctx, int64_t* records, int64_t* new_cands);
 int mkfg_find_download(mkfg_context* ctx, int32_t n_seeds, mkfg_find_out* out);
 /* The same export for the best candidate of every seed only (m = 1 slot
  * per seed in every output array; n_cands[s] = 1 when the seed has a

@@ -9,6 +9,8 @@ adjoint (mkfg_align_chi2_forward / mkfg_align_chi2_backward).
 
 `chi2` goes through the compiled PyTorch extension (_lib/_align_ext*.so);
 `forward_backward` calls the C ABI directly (no autograd).
+`distributed_chi2_grad` splits the tracks over the ranks of a process
+group and sums the ranks' results with one all-reduce.
 """
 import ctypes
 import importlib.machinery
@@ -127,3 +129,24 @@ class AlignedFit:
         a.checkpoint = ckpt.data_ptr()
         a.chi2_sum = total.data_ptr()
         return a
+
+
+def distributed_chi2_grad(ctx, ev, theta, world, rank, material=True, grad_fn=None):
+    """Summed chi2 and its gradient over all tracks of `ev`, with the tracks
+    split into one contiguous share per rank (mkfit_b200.dist.track_share)
+    and the ranks' (chi2, gradient) summed by one all-reduce of
+    1 + 3 * n_layers float64 numbers. grad_fn(share_event, theta) ->
+    (chi2, grad [n_layers][3]) computes a share; by default the CUDA adjoint
+    (AlignedFit.forward_backward) on `ctx`. Returns (chi2, grad) as float64,
+    the same on every rank."""
+    from . import dist
+    begin, end = dist.track_share(ev.n, world, rank)
+    share = ev.tracks(begin, end)
+    if grad_fn is None:
+        def grad_fn(e, th):
+            c2, g = AlignedFit(ctx, e, material=material).forward_backward(th)
+            return c2, g.cpu().numpy()
+    c2, g = grad_fn(share, theta)
+    g = np.asarray(g, np.float64)
+    tot = dist.allreduce_sum(np.concatenate([[c2], g.ravel()]), world)
+    return float(tot[0]), tot[1:].reshape(g.shape)

@@ -234,7 +234,7 @@ __global__ void __launch_bounds__(kBlock, MKFG_PROP_MIN_BLOCKS) k_propagate(Even
   int* cnt = E.step_count + step * kCntN;
   const int nb = cnt[kCntActBarrel], ne = cnt[kCntActEndcap];
   const int stride = E.cand[0].cap;
-  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&E.work[step * 4 + 0], nb + ne);
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&E.work[step * kWorkN + 0], nb + ne);
   __shared__ BlockAppend sh;
   // Block-uniform loop: the pair-list reservation synchronises the block.
   for (int j0 = blockIdx.x * kBlock; j0 < nb + ne; j0 += gridDim.x * kBlock) {
@@ -287,7 +287,7 @@ __global__ void __launch_bounds__(kBlock, MKFG_CHI2_MIN_BLOCKS) k_chi2(EventDev 
   const int nb = cnt[kCntPairBarrel], ne = cnt[kCntPairEndcap];
   const int n_pairs = nb + ne;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    atomicAdd(&E.work[step * 4 + 2], n_pairs);
+    atomicAdd(&E.work[step * kWorkN + 2], n_pairs);
     E.pair_count[step] = n_pairs;
   }
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n_pairs; p += gridDim.x * blockDim.x) {
@@ -320,6 +320,10 @@ __global__ void __launch_bounds__(kBlock, MKFG_CHI2_MIN_BLOCKS) k_chi2(EventDev 
 // Kernel 3: per-seed candidate cloning (CandCloner::ProcessSeedRange,
 // mkFit/CandCloner.cc:36-189). One warp per seed.
 //------------------------------------------------------------------------------
+// kCount: also count the records present and the new candidates (work
+// counters 4 and 5). The eager launch sequence counts; the graph form, whose
+// kernel sits at its register cap, does not.
+template <bool kCount>
 __global__ void __launch_bounds__(kBlock, MKFG_CLONE_MIN_BLOCKS) k_clone(EventDev E, const FindConfigDev* __restrict__ Cp,
                                                   int step) {
   const FindConfigDev& C = *Cp;
@@ -327,10 +331,15 @@ __global__ void __launch_bounds__(kBlock, MKFG_CLONE_MIN_BLOCKS) k_clone(EventDe
   __shared__ HitMatchPair s_hm[kBlock / 32][kSlots];
   __shared__ CloneScratch s_scratch[kBlock / 32];
   __shared__ BlockAppend sh;
+  __shared__ int s_work[2];  // records present, new candidates (this block)
   HitMatchPair* hm = s_hm[warp];
   int* cnt = E.step_count + step * kCntN;
   const int n_find = cnt[kCntFind];
-  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&E.work[step * 4 + 3], n_find);
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&E.work[step * kWorkN + 3], n_find);
+  if (kCount) {
+    if (threadIdx.x < 2) s_work[threadIdx.x] = 0;
+    __syncthreads();
+  }
   // Block-uniform loop (the update-list append synchronises the block):
   // warp `warp` of the block takes seed base + warp of each round.
   for (int base = blockIdx.x * (kBlock / 32); base < n_find; base += gridDim.x * (kBlock / 32)) {
@@ -347,12 +356,16 @@ __global__ void __launch_bounds__(kBlock, MKFG_CLONE_MIN_BLOCKS) k_clone(EventDe
       const int hit0 = E.layer_begin[E.seed_event[s] * E.lb_stride + layer];
       const SeedRecords R{E.rec + rb, E.rmask + s * kSlots, E.wsr + s * kSlots,
                           E.extra_last + s * kSlots, nullptr};
-      int upd = 0;
+      int upd = 0, n_rec = 0;
       const int n = clone_seed(E, C, s, layer, kFinding, ncand, cur, R, hm, s_scratch[warp], upd,
-                               lane);
+                               lane, kCount ? &n_rec : nullptr);
       if (n >= 0 && lane == 0) {
         E.n_cands[s] = n;
         E.cur[s] = cur ^ 1;
+      }
+      if (kCount && lane == 0) {
+        atomicAdd(s_work, n_rec);
+        atomicAdd(s_work + 1, max(n, 0));
       }
       // The new candidates that take a Kalman update, with the global index
       // of the hit to update with (on this step's layer).
@@ -365,6 +378,11 @@ __global__ void __launch_bounds__(kBlock, MKFG_CLONE_MIN_BLOCKS) k_clone(EventDe
                            E.upd_hit);
     __syncwarp();  // hm and scratch are reused by the next seed of this warp
   }
+  if (kCount) {
+    __syncthreads();
+    if (threadIdx.x < 2 && s_work[threadIdx.x])
+      atomicAdd(&E.work[step * kWorkN + 4 + threadIdx.x], s_work[threadIdx.x]);
+  }
 }
 
 //------------------------------------------------------------------------------
@@ -375,7 +393,7 @@ __global__ void __launch_bounds__(kBlock, MKFG_UPD_MIN_BLOCKS) k_update(EventDev
   const FindConfigDev& C = *Cp;
   const int* cnt = E.step_count + step * kCntN;
   const int nb = cnt[kCntUpdBarrel], ne = cnt[kCntUpdEndcap];
-  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&E.work[step * 4 + 1], nb + ne);
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&E.work[step * kWorkN + 1], nb + ne);
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nb + ne; j += gridDim.x * blockDim.x) {
     const int at = j < nb ? j : E.list_cap - 1 - (j - nb);
     const int slot = E.upd_list[at];
@@ -929,7 +947,7 @@ struct Finder {
   // forward run plus a backward search of that length.
   int bks_steps = 0;
   bool sort_seed_hits = false;  // IterationConfig::m_requires_seed_hit_sorting
-  int64_t last_chi2_evals = 0, last_seeds_cloned = 0;
+  int64_t last_chi2_evals = 0, last_seeds_cloned = 0, last_records = 0, last_new_cands = 0;
   // Per-launch device times of the last timed run: [max_steps][5] for the
   // layer-step kernels (activate, propagate, chi2, clone, update).
   std::vector<float> last_step_ms;
@@ -944,6 +962,7 @@ struct Finder {
   DevBuf bk;  // backward-fit seed groups
   DevBuf bks;  // backward-search saved counts
   FindConfigDev* d_cfg_bks = nullptr;  // backward-search plans
+  float* d_mat = nullptr;  // material map (radiation lengths, then xi) taken at setup
   DevBuf sel;  // output selection scratch
   // A quality filter removed comb candidates since the upload (the device
   // flags in ev.removed, cleared by every run, say which).
@@ -979,6 +998,7 @@ void finder_release(mkfg_context* ctx) {
   Finder* f = static_cast<Finder*>(ctx->finder);
   if (f->d_cfg) cudaFree(f->d_cfg);
   if (f->d_cfg_bks) cudaFree(f->d_cfg_bks);
+  if (f->d_mat) cudaFree(f->d_mat);
   f->bks.release();
   f->drop_graph();
   f->bk.release();
@@ -1084,7 +1104,16 @@ extern "C" int mkfg_finder_setup(mkfg_context* ctx, const mkfg_find_config* cfg)
   H.pt_cut_overlap = cfg->pt_cut_overlap;
   H.inter_pflags = cfg->inter_layer_pflags;
   H.intra_pflags = cfg->intra_layer_pflags;
-  H.mat = Material{ctx->d_rl, ctx->d_xi};
+  // The finder keeps its own copy of the context's material map: a later
+  // mkfg_set_material (a fit on another detector through the same context)
+  // does not change what the finding propagates through.
+  const size_t mat_n = (size_t)kMatNZ * kMatNR;
+  if (!f->d_mat) MKFG_CUDA_TRY(cudaMalloc(&f->d_mat, 2 * mat_n * sizeof(float)));
+  MKFG_CUDA_TRY(cudaMemcpyAsync(f->d_mat, ctx->d_rl, mat_n * sizeof(float), cudaMemcpyDeviceToDevice,
+                                ctx->stream));
+  MKFG_CUDA_TRY(cudaMemcpyAsync(f->d_mat + mat_n, ctx->d_xi, mat_n * sizeof(float),
+                                cudaMemcpyDeviceToDevice, ctx->stream));
+  H.mat = Material{f->d_mat, f->d_mat + mat_n};
   H.looper_stop = 1;
   if (!f->d_cfg) MKFG_CUDA_TRY(cudaMalloc(&f->d_cfg, sizeof(FindConfigDev)));
   MKFG_CUDA_TRY(cudaMemcpyAsync(f->d_cfg, &H, sizeof(H), cudaMemcpyHostToDevice, ctx->stream));
@@ -1139,6 +1168,9 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     seed_off[e + 1] = seed_off[e] + ev->n_seeds;
   }
   const int NH = hit_off[n_ev], S = seed_off[n_ev];
+  // Work-list entries pack (candidate slot, hit) into 32-bit integers:
+  // seed count * 8 slots * 16 hits must stay below 2^31.
+  MKFG_REQUIRE(S <= (1 << 24), "%d seeds in the batch; at most %d", S, 1 << 24);
   const int nb = f->n_bins;
 
   // Hits go to the device in one copy from a pinned host mirror: positions,
@@ -1443,7 +1475,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   }
   {
     const size_t need = rounded(4 * (size_t)SC) * (27 + 10) + 2 * rounded(4 * (size_t)SC * kMaxXHits) +
-                        rounded(4 * (size_t)(max_steps + 2)) * (1 + 4 + kCntN) + rounded(64) + 8192;
+                        rounded(4 * (size_t)(max_steps + 2)) * (1 + kWorkN + kCntN) + rounded(64) + 8192;
     if ((rc = f->scratch.ensure(need))) return rc;
     char* p = f->scratch.as<char>();
     f->ev.ppar = carve<float>(p, 6 * (size_t)SC);
@@ -1462,7 +1494,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     f->ev.list_cap = SC;
     f->ev.step_count = carve<int>(p, (size_t)kCntN * (max_steps + 2));
     f->ev.err_flags = carve<int>(p, 16);
-    f->ev.work = carve<int>(p, 4 * (size_t)(max_steps + 2));
+    f->ev.work = carve<int>(p, kWorkN * (size_t)(max_steps + 2));
   }
   {
     const size_t nrec = (size_t)SS * kRecPerSeed;
@@ -1537,7 +1569,7 @@ static StepGrids step_grids(Finder* f) {
     int dev = 0, n_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-    const void* fn[4] = {(const void*)k_propagate, (const void*)k_chi2, (const void*)k_clone,
+    const void* fn[4] = {(const void*)k_propagate, (const void*)k_chi2, (const void*)k_clone<false>,
                          (const void*)k_update};
     for (int k = 0; k < 4; ++k) {
       int per_sm = 0;
@@ -1559,9 +1591,9 @@ static StepGrids step_grids(Finder* f) {
 // Enqueues the whole finding sequence of the uploaded batch on `st`:
 // reset, then for every layer-plan step prep -> chi2 -> clone -> update,
 // then the final merge.
-static int enqueue_run(Finder* f, cudaStream_t st) {
+static int enqueue_run(Finder* f, cudaStream_t st, bool count_clone = false) {
   const int S = f->n_seeds;
-  const int n_work = 4 * (f->host_cfg.max_steps + 2);
+  const int n_work = kWorkN * (f->host_cfg.max_steps + 2);
   const int grid_c = (S * kSlots + kBlock - 1) / kBlock;
   const StepGrids g = step_grids(f);
   MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.pair_count, 0, 4 * (size_t)(f->host_cfg.max_steps + 2), st));
@@ -1572,7 +1604,10 @@ static int enqueue_run(Finder* f, cudaStream_t st) {
     k_activate<<<g.activate, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
     k_propagate<<<g.propagate, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
     k_chi2<<<g.chi2, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
-    k_clone<<<g.clone, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+    if (count_clone)
+      k_clone<true><<<g.clone, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+    else
+      k_clone<false><<<g.clone, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
     k_update<<<g.update, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
   }
   k_merge<<<(S + 127) / 128, 128, 0, st>>>(f->ev, f->d_cfg);
@@ -1593,7 +1628,7 @@ static int launch_fused(Finder* f, cudaStream_t st) {
 // Reset + one fused launch (all layer steps and the merge).
 static int enqueue_fused(Finder* f, cudaStream_t st, int w) {
   const int S = f->n_seeds;
-  const int n_work = 4 * (f->host_cfg.max_steps + 2);
+  const int n_work = kWorkN * (f->host_cfg.max_steps + 2);
   const int grid_c = (S * kSlots + kBlock - 1) / kBlock;
   k_reset<<<std::max(grid_c, (n_work + kBlock - 1) / kBlock), kBlock, 0, st>>>(f->ev, n_work);
   MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.pair_count, 0, 4 * (size_t)(f->host_cfg.max_steps + 2), st));
@@ -1613,7 +1648,7 @@ static int run_timed(mkfg_context* ctx, Finder* f, float* ms) {
   if (f->n_seeds == 0) return MKFG_OK;
   cudaStream_t st = ctx->stream;
   const int S = f->n_seeds;
-  const int n_work = 4 * (f->host_cfg.max_steps + 2);
+  const int n_work = kWorkN * (f->host_cfg.max_steps + 2);
   const int grid_c = (S * kSlots + kBlock - 1) / kBlock;
   const StepGrids g = step_grids(f);
   const int n_ev = 2 + 5 * f->host_cfg.max_steps + 1;
@@ -1636,7 +1671,7 @@ static int run_timed(mkfg_context* ctx, Finder* f, float* ms) {
       mark(2);
       k_chi2<<<g.chi2, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
       mark(3);
-      k_clone<<<g.clone, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+      k_clone<false><<<g.clone, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
       mark(4);
       k_update<<<g.update, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
       mark(5);
@@ -1660,9 +1695,11 @@ static int run_timed(mkfg_context* ctx, Finder* f, float* ms) {
   return rc;
 }
 
+// The eager launch sequence also fills the clone-step counters
+// (mkfg_find_work_clone).
 static int run_plain(mkfg_context* ctx, Finder* f) {
   if (f->n_seeds == 0) return MKFG_OK;
-  return enqueue_run(f, ctx->stream);
+  return enqueue_run(f, ctx->stream, true);
 }
 
 // Same sequence captured once into a CUDA graph and replayed: one launch
@@ -1957,7 +1994,7 @@ extern "C" int mkfg_find_backward_search_with(mkfg_context* ctx, const int32_t* 
   // Per-step buffers were sized for the longest plan at upload.
   MKFG_REQUIRE(max_steps <= std::max(f->host_cfg.max_steps, f->bks_steps),
                "backward plan longer than the configured plans");
-  const int n_work = 4 * (max_steps + 2);
+  const int n_work = kWorkN * (max_steps + 2);
   MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.pair_count, 0, 4 * (size_t)(max_steps + 2), st));
   MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.step_count, 0, 4 * (size_t)kCntN * (max_steps + 2), st));
   MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.work, 0, 4 * (size_t)n_work, st));
@@ -1967,7 +2004,7 @@ extern "C" int mkfg_find_backward_search_with(mkfg_context* ctx, const int32_t* 
     k_activate<<<g.activate, kBlock, 0, st>>>(f->ev, f->d_cfg_bks, step);
     k_propagate<<<g.propagate, kBlock, 0, st>>>(f->ev, f->d_cfg_bks, step);
     k_chi2<<<g.chi2, kBlock, 0, st>>>(f->ev, f->d_cfg_bks, step);
-    k_clone<<<g.clone, kBlock, 0, st>>>(f->ev, f->d_cfg_bks, step);
+    k_clone<false><<<g.clone, kBlock, 0, st>>>(f->ev, f->d_cfg_bks, step);
     k_update<<<g.update, kBlock, 0, st>>>(f->ev, f->d_cfg_bks, step);
   }
   k_merge<<<(S + 127) / 128, 128, 0, st>>>(f->ev, f->d_cfg_bks);
@@ -2209,20 +2246,24 @@ extern "C" int mkfg_find_work(mkfg_context* ctx, int64_t* active_cands, int64_t*
   Finder* f = finder_of(ctx);
   MKFG_REQUIRE(f->events_loaded, "no event uploaded");
   const int ns = f->host_cfg.max_steps + 2;
-  std::vector<int> work(4 * (size_t)ns), pairs(ns);
+  std::vector<int> work(kWorkN * (size_t)ns), pairs(ns);
   MKFG_CUDA_TRY(cudaMemcpyAsync(work.data(), f->ev.work, 4 * work.size(), cudaMemcpyDeviceToHost, ctx->stream));
   MKFG_CUDA_TRY(cudaMemcpyAsync(pairs.data(), f->ev.pair_count, 4 * pairs.size(), cudaMemcpyDeviceToHost, ctx->stream));
   MKFG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-  int64_t a = 0, p = 0, u = 0, p2 = 0, cs = 0;
+  int64_t a = 0, p = 0, u = 0, p2 = 0, cs = 0, rec = 0, nc = 0;
   for (int i = 0; i < ns; ++i) {
-    a += work[4 * i];
-    u += work[4 * i + 1];
-    p2 += work[4 * i + 2];
-    cs += work[4 * i + 3];
+    a += work[kWorkN * i];
+    u += work[kWorkN * i + 1];
+    p2 += work[kWorkN * i + 2];
+    cs += work[kWorkN * i + 3];
+    rec += work[kWorkN * i + 4];
+    nc += work[kWorkN * i + 5];
     p += pairs[i];
   }
   f->last_chi2_evals = p2;
   f->last_seeds_cloned = cs;
+  f->last_records = rec;
+  f->last_new_cands = nc;
   if (active_cands) *active_cands = a;
   if (hit_pairs) *hit_pairs = p;
   if (updates) *updates = u;
@@ -2298,5 +2339,16 @@ extern "C" int mkfg_find_work_detail(mkfg_context* ctx, int64_t* chi2_evals, int
   Finder* f = finder_of(ctx);
   if (chi2_evals) *chi2_evals = f->last_chi2_evals;
   if (seeds_cloned) *seeds_cloned = f->last_seeds_cloned;
+  return MKFG_OK;
+}
+
+// Clone-step counters of the last mkfg_find_work call: records (IdxChi2List
+// entries) present when the seeds were ranked, and new candidates written.
+extern "C" int mkfg_find_work_clone(mkfg_context* ctx, int64_t* records, int64_t* new_cands) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  Finder* f = finder_of(ctx);
+  if (records) *records = f->last_records;
+  if (new_cands) *new_cands = f->last_new_cands;
   return MKFG_OK;
 }

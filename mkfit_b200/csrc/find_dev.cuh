@@ -13,6 +13,10 @@ constexpr int kSlots = 8;               // candidate slots per seed (maxCandsPer
 constexpr int kMaxXHits = 16;           // MkFinder::MPlexHitIdxMax
 constexpr int kRecPerCand = kMaxXHits + 1;
 constexpr int kRecPerSeed = kSlots * kRecPerCand;
+// Work counters per layer-plan step (EventDev::work): active candidates,
+// Kalman updates, (candidate, hit) pairs, seeds cloned, records present at
+// the clone step, new candidates written by it.
+constexpr int kWorkN = 6;
 constexpr int kMaxLayers = 128;
 constexpr int kMaxPlan = 64;
 constexpr int kMaxRegions = 8;

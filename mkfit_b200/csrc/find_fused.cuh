@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(W * kSlots) k_find_fused(EventDev E,
     const unsigned act = __ballot_sync(0xffffffffu, active) & grp;
     {
       const unsigned all = __ballot_sync(0xffffffffu, active);
-      if (lane == 0 && all) atomicAdd(&E.work[step * 4 + 0], __popc(all));
+      if (lane == 0 && all) atomicAdd(&E.work[step * kWorkN + 0], __popc(all));
     }
     if (in_range && c == 0) {
       if (layer >= 0 && state == kFinding && act == 0) state = kFinished;
@@ -108,7 +108,7 @@ __global__ void __launch_bounds__(W * kSlots) k_find_fused(EventDev E,
     const int np = S.n_pairs;
     if (tid == 0 && np) {
       atomicAdd(&E.pair_count[step], np);
-      atomicAdd(&E.work[step * 4 + 2], np);
+      atomicAdd(&E.work[step * kWorkN + 2], np);
     }
     for (int p = tid; p < np; p += T) {
       const int code = S.pairs[p];
@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(W * kSlots) k_find_fused(EventDev E,
       const int wstate = E.state[ws];
       if (wstate != kFinding) continue;
       const int cur = E.cur[ws];
-      if (lane == 0) atomicAdd(&E.work[step * 4 + 3], 1);
+      if (lane == 0) atomicAdd(&E.work[step * kWorkN + 3], 1);
       const int rb = wl * kRecPerSeed;
       const SeedRecords R{S.rec + rb, S.rmask + wl * kSlots, S.wsr + wl * kSlots,
                           S.extra_last + wl * kSlots, S.upd + wl * kSlots};
@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(W * kSlots) k_find_fused(EventDev E,
     //-------------------------------------------------------------- update
     if (in_range && layer >= 0 && c < E.n_cands[s] && S.upd[tid]) {
       S.upd[tid] = 0;
-      atomicAdd(&E.work[step * 4 + 1], 1);
+      atomicAdd(&E.work[step * kWorkN + 1], 1);
       update_cand(E, C, s, lb, E.cand[E.cur[s]], slot);
     }
     // A seed can still change if it is dormant (it may wake up) or finding

@@ -591,11 +591,13 @@ struct CloneScratch {
 // CandCloner::ProcessSeedRange for one seed (mkFit/CandCloner.cc:36-189),
 // executed by one warp. Returns the new candidate count, or -1 when the
 // seed's candidates are unchanged; upd_out: lane i's new candidate's
-// update code (SeedRecords::upd_). The warp owns the seed's arena counter.
+// update code (SeedRecords::upd_); n_records_out (optional): the records
+// present. The warp owns the seed's arena counter.
 __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev& C, int s,
                                           int layer, int state, int ncand, int cur,
                                           const SeedRecords& R, HitMatchPair* hm,
-                                          CloneScratch& X, int& upd_out, int lane) {
+                                          CloneScratch& X, int& upd_out, int lane,
+                                          int* n_records_out = nullptr) {
   constexpr unsigned kFull = 0xffffffffu;
   const CandSoA& B = E.cand[cur];
   const CandSoA& N = E.cand[cur ^ 1];
@@ -634,6 +636,7 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
     if (lane >= off) cincl += v;
   }
   const int n_valid = __shfl_sync(kFull, cincl, kSlots - 1);
+  if (n_records_out) *n_records_out = n_valid;
   // Record index of present record p < n_valid (warp-collective).
   auto locate = [&](int p) {
     int c = 0;
@@ -980,7 +983,11 @@ __device__ __forceinline__ int merge_seed(const EventDev& E, const FindConfigDev
     order[j] = o;
   }
   const bool has_bs = E.bshort_valid[s];
-  const float bs = has_bs ? cand_score(E.bshort, s) : 0.f;
+  // With candidates left the best short candidate's score is recomputed
+  // with theirs; with none it is appended as it is, keeping the score of
+  // the record that made it (getScoreStruct, in-finding weights, tail holes
+  // counted) -- HitStructures.cc:515-548.
+  const float bs = has_bs ? (n > 0 ? cand_score(E.bshort, s) : E.bshort.score[s]) : 0.f;
   int ins = -1;
   if (n > 0) {
     if (has_bs && bs > score[order[n - 1]]) {

@@ -53,7 +53,12 @@ __global__ void __launch_bounds__(kFitBlock) fit_kernel(const FitKernelArgs a) {
   for (int s = 0; s < a.n_steps; ++s) {
     int hidx = __ldg(a.hot + s * a.hot_stride + i);
     if (hidx < 0) hidx = 0;  // reference packer's null input (hit 0)
-    const int h = __ldg(a.layer_begin + a.hit_layer[s]) + hidx;
+    // An index past its layer is kept on the layer's last hit (and on hit 0
+    // of the buffer when the layer is empty), so every read stays inside the
+    // hit arrays; the host entry points reject such indexes before copying.
+    const int lb0 = __ldg(a.layer_begin + a.hit_layer[s]);
+    const int lb1 = __ldg(a.layer_begin + a.hit_layer[s] + 1);
+    const int h = max(min(lb0 + hidx, lb1 - 1), 0);
     float mpos[3], merr[6];
 #pragma unroll
     for (int e = 0; e < 3; ++e) mpos[e] = __ldg(a.hpos + e * a.hstride + h);
@@ -94,6 +99,46 @@ int check_fit_args(const mkfg_fit_args* a) {
                  "hit_layer[%d]=%d out of range", s, a->hit_layer[s]);
   return MKFG_OK;
 }
+
+}  // namespace
+
+// Checks of a host-buffer fit call, all made before anything is copied:
+// the device-pointer checks, non-null host arrays, a consistent layer
+// table, and every hit index inside its layer (a negative index means the
+// layer's hit 0, which must exist).
+int check_fit_host_args(const mkfg_fit_args* a) {
+  int rc = check_fit_args(a);
+  if (rc) return rc;
+  const int n = a->in.n, nl = a->hits.n_layers;
+  MKFG_REQUIRE(a->hits.layer_begin != nullptr, "null layer_begin");
+  MKFG_REQUIRE(a->hits.layer_begin[0] == 0, "layer_begin[0] must be 0");
+  for (int l = 0; l < nl; ++l)
+    MKFG_REQUIRE(a->hits.layer_begin[l + 1] >= a->hits.layer_begin[l],
+                 "layer_begin decreases at layer %d", l);
+  const int n_hits = a->hits.layer_begin[nl];
+  MKFG_REQUIRE(n_hits <= a->hits.stride, "hit count %d exceeds hit stride %d", n_hits,
+               a->hits.stride);
+  if (n == 0) return MKFG_OK;
+  MKFG_REQUIRE(a->in.par && a->in.err && a->in.chg && a->out.par && a->out.err && a->out.chg,
+               "null host track array");
+  MKFG_REQUIRE(n_hits == 0 || (a->hits.pos && a->hits.err), "null host hit array");
+  MKFG_REQUIRE(a->hot_index != nullptr || a->n_steps == 0, "null hot_index");
+  for (int s = 0; s < a->n_steps; ++s) {
+    const int l = a->hit_layer[s];
+    const int size = a->hits.layer_begin[l + 1] - a->hits.layer_begin[l];
+    const int32_t* row = a->hot_index + size_t(s) * a->hot_stride;
+    for (int i = 0; i < n; ++i) {
+      const int h = row[i] < 0 ? 0 : row[i];
+      if (h >= size)
+        return set_error(MKFG_ERR_BAD_INPUT,
+                         "hot_index[%d][%d] = %d outside layer %d, which holds %d hits", s, i,
+                         row[i], l, size);
+    }
+  }
+  return MKFG_OK;
+}
+
+namespace {
 
 int launch_fit(mkfg_context* ctx, const mkfg_fit_args* a) {
   if (a->in.n == 0) return MKFG_OK;
@@ -144,16 +189,13 @@ extern "C" int mkfg_fit(mkfg_context* ctx, const mkfg_fit_args* args) {
   return launch_fit(ctx, args);
 }
 
-extern "C" int mkfg_fit_host(mkfg_context* ctx, const mkfg_fit_args* args) {
-  int rc = activate(ctx);
-  if (rc) return rc;
-  if ((rc = check_fit_args(args))) return rc;
+namespace {
+
+int fit_host_staged(mkfg_context* ctx, const mkfg_fit_args* args) {
+  int rc;
   const int n = args->in.n;
   const int nl = args->hits.n_layers;
-  MKFG_REQUIRE(args->hits.layer_begin != nullptr, "null layer_begin");
   const int n_hits = args->hits.layer_begin[nl];
-  MKFG_REQUIRE(n_hits >= 0 && n_hits <= args->hits.stride, "bad hit count/stride");
-  if (n == 0) return MKFG_OK;
 
   // Device scratch: compact strides (n for tracks, n_hits for hits).
   const size_t trk_bytes = size_t(n) * (27 * sizeof(float) + sizeof(int));
@@ -215,4 +257,18 @@ extern "C" int mkfg_fit_host(mkfg_context* ctx, const mkfg_fit_args* args) {
     MKFG_CUDA_TRY(cudaMemcpyAsync(args->out_chi2, d_chi2, size_t(n) * 4, cudaMemcpyDeviceToHost, st));
   MKFG_CUDA_TRY(cudaStreamSynchronize(st));
   return MKFG_OK;
+}
+
+}  // namespace
+
+extern "C" int mkfg_fit_host(mkfg_context* ctx, const mkfg_fit_args* args) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  if ((rc = check_fit_host_args(args))) return rc;
+  if (args->in.n == 0) return MKFG_OK;
+  rc = fit_host_staged(ctx, args);
+  // On an error after copies were queued, let them finish before the caller
+  // reuses its host buffers.
+  if (rc) cudaStreamSynchronize(ctx->stream);
+  return rc;
 }

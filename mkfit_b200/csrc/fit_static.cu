@@ -43,21 +43,24 @@ static size_t stage_round(size_t bytes) { return (bytes + 255) / 256 * 256; }
 
 using namespace mkfg;
 
+namespace {
+
+int fit_static_staged(mkfg_context* ctx, const mkfg_fit_args* args, unsigned char* base);
+
+}  // namespace
+
 extern "C" int mkfg_fit_host_static(mkfg_context* ctx, const mkfg_fit_args* args) {
   int rc = activate(ctx);
   if (rc) return rc;
-  MKFG_REQUIRE(args != nullptr, "null fit args");
+  // Every check, the hit indexes against their layers included, comes
+  // before the first copy into the shared array.
+  if ((rc = check_fit_host_args(args))) return rc;
+  MKFG_REQUIRE(args->n_steps <= kFitStageMaxSteps, "n_steps must be in [0, %d]",
+               kFitStageMaxSteps);
   const int n = args->in.n;
   const int nl = args->hits.n_layers;
   const int n_steps = args->n_steps;
-  MKFG_REQUIRE(n >= 0 && n <= args->in.stride, "bad input track count/stride");
-  MKFG_REQUIRE(args->out.n == n && args->out.stride >= n, "bad output track count/stride");
-  MKFG_REQUIRE(nl > 0 && args->hits.layer_begin != nullptr, "no hit layers");
-  MKFG_REQUIRE(n_steps >= 0 && n_steps <= kFitStageMaxSteps, "n_steps must be in [0, %d]",
-               kFitStageMaxSteps);
-  MKFG_REQUIRE(args->hot_stride >= n, "hot_stride smaller than track count");
   const int n_hits = args->hits.layer_begin[nl];
-  MKFG_REQUIRE(n_hits >= 0 && n_hits <= args->hits.stride, "bad hit count/stride");
   if (n == 0) return MKFG_OK;
 
   // Staging layout (256-byte aligned pieces). Nothing in it has to start at
@@ -79,6 +82,27 @@ extern "C" int mkfg_fit_host_static(mkfg_context* ctx, const mkfg_fit_args* args
 
   unsigned char* base = nullptr;
   if ((rc = fit_stage_address(ctx->device, &base))) return rc;
+  rc = fit_static_staged(ctx, args, base);
+  // On an error after copies into the array were queued, let them finish:
+  // the caller may start the next call as soon as this one returns.
+  if (rc) cudaStreamSynchronize(ctx->stream);
+  return rc;
+}
+
+namespace {
+
+int fit_static_staged(mkfg_context* ctx, const mkfg_fit_args* args, unsigned char* base) {
+  int rc;
+  const int n = args->in.n;
+  const int nl = args->hits.n_layers;
+  const int n_steps = args->n_steps;
+  const int n_hits = args->hits.layer_begin[nl];
+  const size_t nn = size_t(n), nh = size_t(n_hits);
+  const size_t sz_in_par = stage_round(6 * nn * 4), sz_in_err = stage_round(21 * nn * 4);
+  const size_t sz_trk_int = stage_round(nn * 4);
+  const size_t sz_hpos = stage_round(3 * nh * 4), sz_herr = stage_round(6 * nh * 4);
+  const size_t sz_lb = stage_round(size_t(nl + 1) * 4);
+  const size_t sz_hot = stage_round(size_t(n_steps) * nn * 4);
   unsigned char* p = base;
   auto take = [&p](size_t bytes) {
     unsigned char* r = p;
@@ -140,3 +164,5 @@ extern "C" int mkfg_fit_host_static(mkfg_context* ctx, const mkfg_fit_args* args
   MKFG_CUDA_TRY(cudaStreamSynchronize(st));
   return MKFG_OK;
 }
+
+}  // namespace

@@ -92,4 +92,6 @@ namespace mkfg {
 int activate(mkfg_context* ctx);
 // Releases the finder state (find.cu).
 void finder_release(mkfg_context* ctx);
+// Validates a host-buffer fit call before anything is copied (fit.cu).
+int check_fit_host_args(const mkfg_fit_args* a);
 }  // namespace mkfg

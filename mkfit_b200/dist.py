@@ -1,8 +1,14 @@
-"""Multi-GPU plumbing of the batched finder: one process per GPU, each rank
-finds its own batch of events (events are independent, as the reference's
-events in flight are: mkFit/mkFit.cc:308-425), no data-path collective.
-Only the timing uses a collective: the step time is the maximum over
-ranks, and the throughput counts the events of all ranks.
+"""Multi-GPU plumbing: one process per GPU.
+
+Finding: each rank finds its own batch of events (events are independent,
+as the reference's events in flight are: mkFit/mkFit.cc:308-425), no
+data-path collective. Only the timing uses a collective: the step time is
+the maximum over ranks, and the throughput counts the events of all ranks.
+
+Differentiable fit: the tracks are split into contiguous shares, one per
+rank; each rank computes its share's summed chi2 and the gradient with
+respect to the per-layer parameters, and one all-reduce (sum) of those
+1 + 3 * n_layers numbers gives every rank the whole-sample result.
 
 Backend "nccl" on GPUs; "gloo" (CPU tensors) for the host-side tests.
 """
@@ -59,6 +65,28 @@ def sum_over_ranks(x, world):
     t = torch.tensor([float(x)], dtype=torch.float64, device=_device())
     dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
+
+
+def track_share(n, world, rank):
+    """The contiguous share [begin, end) of n tracks that `rank` takes:
+    shares differ by at most one track."""
+    base, extra = divmod(int(n), int(world))
+    begin = rank * base + min(rank, extra)
+    return begin, begin + base + (1 if rank < extra else 0)
+
+
+def allreduce_sum(values, world):
+    """Element-wise sum over ranks of a float64 vector (one all-reduce);
+    returns a numpy array."""
+    import numpy as np
+    v = np.asarray(values, np.float64).ravel()
+    if world == 1:
+        return v.copy()
+    import torch
+    import torch.distributed as dist
+    t = torch.from_numpy(v.copy()).to(_device())
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return t.cpu().numpy()
 
 
 def rank_seed(base, rank):

@@ -137,6 +137,7 @@ def _bind(lib):
     i64p = ctypes.POINTER(ctypes.c_int64)
     lib.mkfg_find_work.argtypes = [vp, i64p, i64p, i64p, ctypes.POINTER(ctypes.c_int32)]
     lib.mkfg_find_work_detail.argtypes = [vp, i64p, i64p]
+    lib.mkfg_find_work_clone.argtypes = [vp, i64p, i64p]
     lib.mkfg_find_download.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(MkfgFindOut)]
     lib.mkfg_find_download_best.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(MkfgFindOut)]
     lib.mkfg_find_event.argtypes = [vp, ctypes.POINTER(MkfgEvent), ctypes.POINTER(MkfgFindOut)]
@@ -344,8 +345,10 @@ class Finder:
                                            ctypes.byref(u), ctypes.byref(st)))
         e, c = ctypes.c_int64(), ctypes.c_int64()
         capi.check(self.lib.mkfg_find_work_detail(self.ctx.handle, ctypes.byref(e), ctypes.byref(c)))
+        r, n = ctypes.c_int64(), ctypes.c_int64()
+        capi.check(self.lib.mkfg_find_work_clone(self.ctx.handle, ctypes.byref(r), ctypes.byref(n)))
         return dict(active_cands=a.value, hit_pairs=p.value, updates=u.value, steps=st.value,
-                    chi2_evals=e.value, seed_steps=c.value)
+                    chi2_evals=e.value, seed_steps=c.value, records=r.value, new_cands=n.value)
 
     def select(self, n_seeds, **params):
         """Output selection of run_OneIteration (NaN/silly filter + duplicate

@@ -125,6 +125,16 @@ class FitEvent:
     def n(self):
         return self.chg.shape[0]
 
+    def tracks(self, begin, end):
+        """The tracks [begin, end) with their hits (same detector)."""
+        d = dict(self.__dict__)
+        d.update(par=np.ascontiguousarray(self.par[:, begin:end]),
+                 err=np.ascontiguousarray(self.err[:, begin:end]),
+                 chg=np.ascontiguousarray(self.chg[begin:end]),
+                 hit_pos=np.ascontiguousarray(self.hit_pos[:, :, begin:end]),
+                 hit_err=np.ascontiguousarray(self.hit_err[:, :, begin:end]))
+        return FitEvent(**d)
+
 
 def gen_fit_event(n_tracks=20000, seed=0xC0FFEE, radii=None, pt_range=(0.5, 10.0),
                   eta_max=1.0, sig_rphi=0.01, sig_z=0.1, x_over_x0=0.01,

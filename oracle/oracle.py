@@ -59,6 +59,18 @@ class RefLib:
     def set_threads(self, n):
         self.lib.ref_set_threads(int(n))
 
+    def set_task_split(self, mode, seed=1):
+        """How the TBB shim cuts parallel_for ranges into tasks: 0 near-equal
+        pieces of at most the grain size (default), 1 recursive halving as
+        TBB's simple_partitioner cuts them, 2 near-equal pieces of at most
+        twice the grain, 3 the whole range (cuts TBB's auto_partitioner
+        makes), 4 pieces of random sizes from half the grain to the grain
+        (seeded by `seed`; TBB's proportional splits)."""
+        self.lib.ref_set_task_split.argtypes = [ctypes.c_int]
+        self.lib.ref_set_task_split_seed.argtypes = [ctypes.c_uint]
+        self.lib.ref_set_task_split_seed(int(seed))
+        self.lib.ref_set_task_split(int(mode))
+
     def threads(self):
         return self.lib.ref_get_threads()
 
@@ -130,6 +142,44 @@ class Restate:
                         ms.ctypes.data if ms is not None else None,
                         out_par, out_err, chi2.ctypes.data if chi2 is not None else None)
         return out_par, out_err, chi2
+
+
+def restate_replay_cands(rs, ev, out, m, slots, geom=None):
+    """FP64 replay (oracle/restate.c rs_replay_cands) of the finding
+    candidates `slots` (indices seed * m + c into a finding result `out`,
+    by input seed) of event `ev` from their seeds along their hit lists.
+    Returns (par[n][6], err[n][21], chg[n], chi2[n]) in double."""
+    from mkfit_b200.geometry import cms2017
+    g = geom or cms2017()
+    slots = np.asarray(slots, np.int64)
+    n = len(slots)
+    seeds = slots // m
+    L = rs.lib
+    L.rs_replay_cands.restype = None
+    L.rs_replay_cands.argtypes = ([ctypes.c_int, _f32p, _f32p, _i32p, _i32p, _i32p, _i32p,
+                                   ctypes.c_int, _i32p, _f32p, _f32p, ctypes.c_int, _i32p, _i32p,
+                                   _f32p, ctypes.c_uint, ctypes.c_uint, ctypes.POINTER(RsMaterial),
+                                   _f64p, _f64p, _i32p, _f64p])
+    c = lambda a, t: np.ascontiguousarray(a, t)  # noqa: E731
+    sp = c(ev.seed_par.T[seeds], np.float32)
+    se = c(ev.seed_err.T[seeds], np.float32)
+    sc = c(ev.seed_chg[seeds], np.int32)
+    rl = c(g.rl, np.float32)
+    xi = c(g.xi, np.float32)
+    mat = RsMaterial(rl.ctypes.data, xi.ctypes.data)
+    par = np.zeros((n, 6), np.float64)
+    err = np.zeros((n, 21), np.float64)
+    chg = np.zeros(n, np.int32)
+    chi2 = np.zeros(n, np.float64)
+    hi = c(out["hit_idx"][slots], np.int32)
+    L.rs_replay_cands(n, sp, se, sc, c(out["ntot"][slots], np.int32), hi,
+                      c(out["hit_lyr"][slots], np.int32), hi.shape[1],
+                      c(ev.seed_nhits[seeds], np.int32), c(ev.hit_pos, np.float32),
+                      c(ev.hit_err, np.float32), ev.hit_pos.shape[1],
+                      c(ev.layer_begin, np.int32), c(g.field("is_barrel"), np.int32),
+                      c(g.field("propagate_to"), np.float32), int(g.flags[1]), int(g.flags[2]),
+                      ctypes.byref(mat), par, err, chg, chi2)
+    return par, err, chg, chi2
 
 
 def adjoint_f64_lib_path():

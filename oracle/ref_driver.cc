@@ -120,6 +120,13 @@ extern "C" {
 
 // Number of host threads the reference's TBB loops run on.
 void ref_set_threads(int n) { tbbshim::Pool::instance().resize(n); }
+// The shim's cut of parallel_for ranges (tbb/parallel_for.h): 0 near-equal
+// pieces of at most the grain, 1 recursive halving, 2 near-equal pieces of
+// at most twice the grain, 3 one piece, 4 random pieces of half the grain
+// to the grain.
+void ref_set_task_split(int mode) { tbbshim::split_mode() = mode; }
+// Seed of the random cut (mode 4).
+void ref_set_task_split_seed(unsigned seed) { tbbshim::split_seed() = seed; }
 int ref_get_threads() { return tbbshim::Pool::instance().concurrency(); }
 
 // Matriplex width this build was compiled with (8 for AVX2, 16 for AVX-512).

@@ -359,3 +359,86 @@ void rs_fit(int n, int n_steps, const float* par, const float* err, const int* c
     if (out_chi2) out_chi2[i] = chi2;
   }
 }
+
+/* Clone-engine candidates replayed in double precision from their seed
+ * state along their hit-on-track lists, with the arithmetic of the
+ * reference's finding steps:
+ *  - chi2 of a hit (MkFinder::FindCandidatesCloneEngine with
+ *    finding_requires_propagation_to_hit_pos, mkFit/MkFinder.cc:1116-1240,
+ *    KalmanUtilsMPlex.cc:518-544, 744-770): the candidate propagated to the
+ *    layer (inter-layer flags, r or z of the layer), then to the hit
+ *    (intra-layer flags), |chi2|;
+ *  - update (MkFinder::UpdateWithLastHit, mkFit/MkFinder.cc:1291-1308,
+ *    KalmanUtilsMPlex.cc:471-505, 697-731): the candidate propagated to the
+ *    last hit added on the layer (inter-layer flags) and updated with it;
+ *    a negative 1/pT flips the charge;
+ *  - a layer with no hit (a hole node) leaves the state as it is.
+ * The first skip[i] nodes (the seed's own hits) are not replayed. */
+void rs_replay_cands(int n, const float* seed_par, const float* seed_err, const int* seed_chg,
+                     const int* n_nodes, const int* node_hit, const int* node_layer,
+                     int node_stride, const int* skip, const float* hit_pos,
+                     const float* hit_err, int hit_stride, const int* layer_begin,
+                     const int* layer_is_barrel, const float* layer_prop_to,
+                     unsigned inter_pflags, unsigned intra_pflags, const rs_material* mat,
+                     double* out_par, double* out_err, int* out_chg, double* out_chi2) {
+  for (int i = 0; i < n; ++i) {
+    double p[6], e[21];
+    for (int k = 0; k < 6; ++k) p[k] = seed_par[i * 6 + k];
+    for (int k = 0; k < 21; ++k) e[k] = seed_err[i * 21 + k];
+    int chg = seed_chg[i];
+    double chi2 = 0;
+    const int* hits = node_hit + (size_t)i * node_stride;
+    const int* lays = node_layer + (size_t)i * node_stride;
+    int k = skip[i];
+    while (k < n_nodes[i]) {
+      const int lyr = lays[k];
+      int end = k;
+      while (end < n_nodes[i] && lays[end] == lyr) ++end;
+      int last = -1;
+      for (int j = k; j < end; ++j)
+        if (hits[j] >= 0) last = j;
+      if (last >= 0) {
+        const int barrel = layer_is_barrel[lyr];
+        double lp[6], le[21];
+        if (barrel)
+          propagate_r_scaled(p, e, chg, layer_prop_to[lyr], inter_pflags, mat, 1.0, lp, le);
+        else
+          propagate_z_scaled(p, e, chg, layer_prop_to[lyr], inter_pflags, mat, 1.0, lp, le);
+        for (int j = k; j < end; ++j) {
+          if (hits[j] < 0) continue;
+          const int g = layer_begin[lyr] + hits[j];
+          double m[3], me[6], hp[6], he[21];
+          for (int c = 0; c < 3; ++c) m[c] = hit_pos[(size_t)c * hit_stride + g];
+          for (int c = 0; c < 6; ++c) me[c] = hit_err[(size_t)c * hit_stride + g];
+          if (barrel) {
+            propagate_r_scaled(lp, le, chg, hipo(m[0], m[1]), intra_pflags, mat, 1.0, hp, he);
+            chi2 += fabs(rs_kalman_barrel(hp, he, m, me, NULL, NULL));
+          } else {
+            propagate_z_scaled(lp, le, chg, m[2], intra_pflags, mat, 1.0, hp, he);
+            chi2 += fabs(rs_kalman_endcap(hp, he, m, me, NULL, NULL));
+          }
+        }
+        const int g = layer_begin[lyr] + hits[last];
+        double m[3], me[6], hp[6], he[21];
+        for (int c = 0; c < 3; ++c) m[c] = hit_pos[(size_t)c * hit_stride + g];
+        for (int c = 0; c < 6; ++c) me[c] = hit_err[(size_t)c * hit_stride + g];
+        if (barrel) {
+          propagate_r_scaled(p, e, chg, hipo(m[0], m[1]), inter_pflags, mat, 1.0, hp, he);
+          rs_kalman_barrel(hp, he, m, me, p, e);
+        } else {
+          propagate_z_scaled(p, e, chg, m[2], inter_pflags, mat, 1.0, hp, he);
+          rs_kalman_endcap(hp, he, m, me, p, e);
+        }
+        if (p[3] < 0) {
+          chg = -chg;
+          p[3] = -p[3];
+        }
+      }
+      k = end;
+    }
+    for (int c = 0; c < 6; ++c) out_par[i * 6 + c] = p[c];
+    for (int c = 0; c < 21; ++c) out_err[i * 21 + c] = e[c];
+    out_chg[i] = chg;
+    out_chi2[i] = chi2;
+  }
+}

@@ -53,6 +53,24 @@ void rs_fit(int n, int n_steps, const float* par, const float* err, const int* c
             const double* shift_z, const double* mat_scale, double* out_par, double* out_err,
             double* out_chi2);
 
+/* Clone-engine candidates replayed from their seed state along their
+ * hit-on-track lists in double precision (the arithmetic of the reference's
+ * FindCandidatesCloneEngine chi2 and UpdateWithLastHit steps): n candidates
+ * with seed_par[n][6], seed_err[n][21], seed_chg[n]; nodes
+ * node_hit/node_layer[n][node_stride] (index within the layer, negative =
+ * hole), n_nodes[n], skip[n] seed nodes; hits hit_pos[3][hit_stride],
+ * hit_err[6][hit_stride] with layer l at [layer_begin[l], layer_begin[l+1]);
+ * per layer: barrel flag and the r or z the finding propagates to. Outputs
+ * the final state (out_par[n][6], out_err[n][21], out_chg[n]) and the sum
+ * of the hits' chi2 (out_chi2[n]). */
+void rs_replay_cands(int n, const float* seed_par, const float* seed_err, const int* seed_chg,
+                     const int* n_nodes, const int* node_hit, const int* node_layer,
+                     int node_stride, const int* skip, const float* hit_pos,
+                     const float* hit_err, int hit_stride, const int* layer_begin,
+                     const int* layer_is_barrel, const float* layer_prop_to,
+                     unsigned inter_pflags, unsigned intra_pflags, const rs_material* mat,
+                     double* out_par, double* out_err, int* out_chg, double* out_chi2);
+
 #ifdef __cplusplus
 }
 #endif

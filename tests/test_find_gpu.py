@@ -649,3 +649,17 @@ def test_repeat_runs_identical(gpu_ctx):
     for o in outs[1:]:
         for k in outs[0]:
             np.testing.assert_array_equal(o[k], outs[0][k], err_msg=k)
+
+
+def test_finder_keeps_its_material_map(gpu_ctx):
+    """The finder copies the context's material map at setup: a fit on
+    another detector through the same context (mkfg_set_material with the
+    toy map) leaves the finding results unchanged."""
+    ev = synth.gen_cms_event(600, seed=77, noise_frac=0.02)
+    fnd = Finder(gpu_ctx, FindConfig(max_cands=M))
+    a = fnd.find_event(ev)
+    fit_ev = synth.gen_fit_event(10, seed=1)
+    gpu_ctx.set_material(fit_ev.rl_grid, fit_ev.xi_grid)
+    b = fnd.find_event(ev)
+    for k in ("n_cands", "par", "err", "chi2", "hit_idx", "hit_lyr"):
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)

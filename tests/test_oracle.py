@@ -99,3 +99,24 @@ def test_restated_backward_fit_matches_reference(reflib, restate):
     assert np.percentile(rel, 99) < 1e-2, np.percentile(rel, 99)
     dpar = np.abs(ref["par"][slots][ok] - par[ok]) / np.sqrt(np.maximum(err[ok][:, [0, 2, 5, 9, 14, 20]], 1e-30))
     assert np.median(dpar) < 1e-3
+
+
+def test_restated_candidate_replay_matches_reference(reflib, restate):
+    """The FP64 replay of clone-engine candidates (restate_replay_cands)
+    reproduces the reference's own FP32 candidates: bulk at FP32 rounding,
+    the same charges; the tails are the reference's FP32 accumulation."""
+    from mkfit_b200 import synth
+    from oracle.oracle import ref_find, restate_replay_cands
+    from tests.tolerances import cov_scaled_err, par_scaled_err
+    m = 6
+    ev = synth.gen_cms_event(600, seed=21, noise_frac=0.05)
+    o = ref_find(reflib, ev, max_cands=m, chi2_cut=30.0, zero_c2=True)
+    slots = np.array([s * m + c for s in range(ev.n_seeds) for c in range(o["n_cands"][s])])
+    par, err, chg, chi2 = restate_replay_cands(restate, ev, o, m, slots)
+    ep = par_scaled_err(o["par"][slots].T, par.T, err.T)
+    ec = cov_scaled_err(o["err"][slots].T, err.T)
+    rc = np.abs(o["chi2"][slots] - chi2) / np.maximum(np.abs(chi2), 1e-3)
+    np.testing.assert_array_equal(chg, o["chg"][slots])
+    assert np.median(ep) < 1e-6 and np.percentile(ep, 99.9) < 1e-3
+    assert np.median(ec) < 1e-5 and np.percentile(ec, 99) < 1e-3
+    assert np.median(rc) < 1e-4 and np.percentile(rc, 99.9) < 1e-2
