@@ -546,6 +546,15 @@ int mkfg_find_work(mkfg_context* ctx, int64_t* active_cands, int64_t* hit_pairs,
  * the chi2 kernel, seed-steps handled by the clone kernel. */
 int mkfg_find_work_detail(mkfg_context* ctx, int64_t* chi2_evals, int64_t* seeds_cloned);
 
+/* Hit-on-track arena of the following uploads: nodes_per_seed nodes per
+ * seed (at least MKFG_MAX_SEED_HITS + 2), or 0 to size it for the
+ * configured plans (the default, which no run exceeds). A search that
+ * needs more nodes than the arena holds keeps the nodes it has, drops the
+ * rest and makes the next download return MKFG_ERR_OVERFLOW, with every
+ * output still written; the reference's CcPool throws std::bad_alloc
+ * instead (mkFit/HitStructures.h:428-435). */
+int mkfg_find_set_arena_capacity(mkfg_context* ctx, int32_t nodes_per_seed);
+
 /* Clone-step counters of the last mkfg_find_work call: the records
  * (IdxChi2List entries, hits and holes) present when the seeds were ranked
  * and the new candidates written. Counted by the eager run (mkfg_find_run)

@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("MKFIT_B200_LIB", os.path.join(HERE, "_lib", "libmkfit_b200.so"))
 HEADER_PATH = os.path.join(HERE, "..", "include", "mkfit_b200.h")
 
-MKFG_OK = 0
+MKFG_OK, MKFG_ERR_BAD_INPUT, MKFG_ERR_CUDA, MKFG_ERR_OVERFLOW, MKFG_ERR_TIMEOUT = 0, 1, 2, 3, 4
 STATUS_NAMES = {0: "OK", 1: "BAD_INPUT", 2: "CUDA", 3: "OVERFLOW", 4: "TIMEOUT", 5: "NO_DEVICE"}
 
 PF_NONE, PF_PARAM_BFIELD, PF_MATERIAL = 0, 1, 2

@@ -947,6 +947,7 @@ struct Finder {
   // forward run plus a backward search of that length.
   int bks_steps = 0;
   bool sort_seed_hits = false;  // IterationConfig::m_requires_seed_hit_sorting
+  int arena_cap = 0;            // hit-on-track nodes per seed; 0 = sized for the plans
   int64_t last_chi2_evals = 0, last_seeds_cloned = 0, last_records = 0, last_new_cands = 0;
   // Per-launch device times of the last timed run: [max_steps][5] for the
   // layer-step kernels (activate, propagate, chi2, clone, update).
@@ -1435,8 +1436,9 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   // is longer; the arena holds both (the search appends to the run's nodes).
   const int max_steps = std::max(f->host_cfg.max_steps, f->bks_steps);
   const int M = f->host_cfg.max_cands;
-  const int hot_cap =
+  const int hot_cap_auto =
       ((MKFG_MAX_SEED_HITS + 4 + (f->host_cfg.max_steps + f->bks_steps) * (2 * M + 3)) + 31) / 32 * 32;
+  const int hot_cap = f->arena_cap > 0 ? std::min(f->arena_cap, hot_cap_auto) : hot_cap_auto;
   {
     const size_t need = 3 * rounded(4 * (size_t)SC) * 37 + rounded(4 * (size_t)SS) * 47 + 4096;
     if ((rc = f->cands.ensure(need))) return rc;
@@ -2344,6 +2346,18 @@ extern "C" int mkfg_find_work_detail(mkfg_context* ctx, int64_t* chi2_evals, int
 
 // Clone-step counters of the last mkfg_find_work call: records (IdxChi2List
 // entries) present when the seeds were ranked, and new candidates written.
+extern "C" int mkfg_find_set_arena_capacity(mkfg_context* ctx, int32_t nodes_per_seed) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  // Seed nodes are written unconditionally at upload: the arena must hold
+  // them and at least one node found by the search.
+  MKFG_REQUIRE(nodes_per_seed == 0 || nodes_per_seed >= MKFG_MAX_SEED_HITS + 2,
+               "arena capacity %d: 0 (automatic) or at least %d nodes per seed", nodes_per_seed,
+               MKFG_MAX_SEED_HITS + 2);
+  finder_of(ctx)->arena_cap = nodes_per_seed;
+  return MKFG_OK;
+}
+
 extern "C" int mkfg_find_work_clone(mkfg_context* ctx, int64_t* records, int64_t* new_cands) {
   int rc = activate(ctx);
   if (rc) return rc;

@@ -138,6 +138,7 @@ def _bind(lib):
     lib.mkfg_find_work.argtypes = [vp, i64p, i64p, i64p, ctypes.POINTER(ctypes.c_int32)]
     lib.mkfg_find_work_detail.argtypes = [vp, i64p, i64p]
     lib.mkfg_find_work_clone.argtypes = [vp, i64p, i64p]
+    lib.mkfg_find_set_arena_capacity.argtypes = [vp, ctypes.c_int32]
     lib.mkfg_find_download.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(MkfgFindOut)]
     lib.mkfg_find_download_best.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(MkfgFindOut)]
     lib.mkfg_find_event.argtypes = [vp, ctypes.POINTER(MkfgEvent), ctypes.POINTER(MkfgFindOut)]

@@ -1,7 +1,7 @@
 """Detector description and finding configuration (CMS-2017).
 
 The numbers come from the reference's own geometry plugin, exported once
-into geom/cms2017.npz by geom/make_cms2017.py (layer table, per-region
+into geom/cms2017.npz by oracle/make_cms2017.py (layer table, per-region
 layer plans, search-window parameters, iteration parameters, propagation
 flags and the (z, r) material grid), for each of the ten CMS-2017
 iterations (initialStep, highPtTripletStep, lowPtQuadStep,

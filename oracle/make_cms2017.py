@@ -5,27 +5,27 @@ the oracle build in oracle/_ref). Iteration 0's arrays sit under their own
 names; every iteration's steering, search windows and parameters are also
 stacked under "it_<name>" (index = iteration).
 
-    python mkfit_b200/geom/make_cms2017.py
+    python oracle/make_cms2017.py
 
-The GPU path needs the same layer table, layer plans, search-window and
-material-map numbers as the reference to reproduce its results; exporting
-them from the running plugin (instead of transcribing its source tables)
-keeps them identical. tests/test_geometry.py re-exports and compares.
+A build-time exporter beside the oracle it runs: the product package only
+loads the committed file (mkfit_b200/geometry.py). The GPU path needs the
+same layer table, layer plans, search-window and material-map numbers as
+the reference to reproduce its results; exporting them from the running
+plugin (instead of transcribing its source tables) keeps them identical.
+tests/test_find_prep.py re-exports and compares.
 """
 import os
 import sys
 
 import numpy as np
 
-HERE = os.path.dirname(os.path.abspath(__file__))
-sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
 
+from mkfit_b200.geometry import ITER_KEYS, N_ITERATIONS  # noqa: E402
 from oracle.oracle import RefLib, cms2017_export  # noqa: E402
 
-# Arrays that depend on the iteration.
-ITER_KEYS = ("layer_desc", "plans", "plan_len", "pickup", "bkfit_last", "bksearch_pickup",
-             "region_order", "iter_params", "bk_iter_params", "bk_flags")
-N_ITERATIONS = 10
+OUT = os.path.join(ROOT, "mkfit_b200", "geom", "cms2017.npz")
 
 
 def export_all(ref):
@@ -45,5 +45,5 @@ def export_all(ref):
 
 if __name__ == "__main__":
     g = export_all(RefLib())
-    np.savez_compressed(os.path.join(HERE, "cms2017.npz"), **g)
-    print("wrote", os.path.join(HERE, "cms2017.npz"))
+    np.savez_compressed(OUT, **g)
+    print("wrote", OUT)

@@ -663,3 +663,39 @@ def test_finder_keeps_its_material_map(gpu_ctx):
     b = fnd.find_event(ev)
     for k in ("n_cands", "par", "err", "chi2", "hit_idx", "hit_lyr"):
         np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+
+
+def test_arena_overflow_reports_and_truncates_deterministically(gpu_ctx):
+    """An undersized hit-on-track arena (host-configured) makes the download
+    return MKFG_ERR_OVERFLOW with every output written, the same way on
+    every run; no candidate holds more nodes than the arena; back at the
+    automatic size the results are the normal ones again."""
+    import ctypes
+    from mkfit_b200 import capi
+    from mkfit_b200.finder import event_struct, out_struct, output_arrays
+    ev = synth.gen_cms_event(500, seed=31, noise_frac=0.05)
+    fnd = Finder(gpu_ctx, FindConfig(max_cands=M))
+    normal = fnd.find_event(ev)
+    lib = gpu_ctx.lib
+    assert lib.mkfg_find_set_arena_capacity(gpu_ctx.handle, 5) == capi.MKFG_ERR_BAD_INPUT
+    cap = 20
+    capi.check(lib.mkfg_find_set_arena_capacity(gpu_ctx.handle, cap))
+    try:
+        runs = []
+        for _ in range(2):
+            fnd.upload(ev)
+            fnd.run()
+            o = output_arrays(ev.n_seeds, M)
+            rc = lib.mkfg_find_download(gpu_ctx.handle, ev.n_seeds, ctypes.byref(out_struct(o)))
+            assert rc == capi.MKFG_ERR_OVERFLOW
+            assert "arena overflow" in capi.last_error()
+            runs.append(o)
+        for k in runs[0]:
+            np.testing.assert_array_equal(runs[0][k], runs[1][k], err_msg=k)
+        assert runs[0]["ntot"].max() <= cap
+        assert (runs[0]["ntot"] < normal["ntot"]).any()
+    finally:
+        capi.check(lib.mkfg_find_set_arena_capacity(gpu_ctx.handle, 0))
+    again = fnd.find_event(ev)
+    for k in ("n_cands", "ntot", "hit_idx", "par"):
+        np.testing.assert_array_equal(again[k], normal[k], err_msg=k)
