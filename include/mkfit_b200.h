@@ -531,6 +531,145 @@ int mkfg_find_filter(mkfg_context* ctx, const mkfg_qfilter_config* cfg, int32_t 
 int mkfg_find_select_hit_indices(mkfg_context* ctx, int32_t event, int32_t layer, int32_t n,
                                  const float* par, const float* err, int32_t* xhit_size,
                                  int32_t* xhit_idx, int32_t* wsr);
+
+/* Counters of the candidates a per-layer worker call takes: the TrackCand
+ * fields MkFinder::copy_in loads (mkFit/MkFinder.h:269-289). Host arrays
+ * of n entries. */
+typedef struct {
+  const int32_t* nfound;  /* nFoundHits */
+  const int32_t* nover;   /* nOverlapHits */
+  const int32_t* ninside; /* nInsideMinusOneHits */
+  const int32_t* ntail;   /* nTailMinusOneHits */
+  const float* chi2;      /* chi2 */
+} mkfg_cand_counts;
+
+/* Records a candidate can hand to the cloner on one layer: up to 16 hits
+ * and one hole. */
+#define MKFG_REC_PER_CAND 17
+
+/* IdxChi2List records (Track.h:28-42) of one worker call, [n][17] each,
+ * entries past n[i] zero. hit: index within the layer, or the hole code
+ * (-1 hole, -2 stop, -3 edge); module: the hit's detIDinLayer (-1 for the
+ * hole); chi2: chi2_hit; score: getScoreStruct of the record. */
+typedef struct {
+  int32_t* n;
+  int32_t* hit;
+  int32_t* module;
+  float* chi2;
+  float* score;
+} mkfg_ce_records;
+
+/* MkFinder::FindCandidatesCloneEngine (mkFit/MkFinder.cc:1116-1284) as a
+ * plain worker call on uploaded event `event`: for n candidates whose
+ * states are propagated to layer `layer` (par[6][n], err[21][n], chg[n], as
+ * Par[iP] / Err[iP]) with their counters, and the hit lists
+ * mkfg_find_select_hit_indices gave for them (xhit_size[n],
+ * xhit_idx[n][16], wsr[n]), the records each candidate hands to the
+ * cloner, in the order it hands them: its accepted hits in xhit_idx order
+ * (chi2 of kalmanPropagateAndComputeChi2 under the dynamic cut, strip
+ * compatibility and charge, the pixel same-layer check), then the hole
+ * record unless wsr says outside. seed_hot_layers[n][3] (may be NULL: no
+ * pixel check): layers of the comb candidate's first three hit-on-track
+ * nodes, -1 where it has none. The inactive-module code -7 is never
+ * produced (no module is inactive). Host arrays; a hit index outside the
+ * layer is refused with MKFG_ERR_BAD_INPUT. Synchronizes the stream. */
+int mkfg_find_candidates_clone_engine(mkfg_context* ctx, int32_t event, int32_t layer, int32_t n,
+                                      const float* par, const float* err, const int32_t* chg,
+                                      const mkfg_cand_counts* counts,
+                                      const int32_t* seed_hot_layers, const int32_t* xhit_size,
+                                      const int32_t* xhit_idx, const int32_t* wsr,
+                                      mkfg_ce_records* out);
+
+/* MkFinder::UpdateWithLastHit + CopyOutParErr (mkFit/MkFinder.cc:
+ * 1291-1335) as a plain worker call on uploaded event `event`: n states
+ * (par[6][n], err[21][n], chg[n], as Par[iP]) propagated to their hit on
+ * layer `layer` (hit_idx[n], index within the layer) with the finding's
+ * inter-layer flags and updated (kalmanPropagateAndUpdate[Endcap]), the
+ * charge flipped where 1/pT turns negative. Host arrays; in and out may
+ * alias. Synchronizes the stream. */
+int mkfg_find_update_with_last_hit(mkfg_context* ctx, int32_t event, int32_t layer, int32_t n,
+                                   const float* par, const float* err, const int32_t* chg,
+                                   const int32_t* hit_idx, float* out_par, float* out_err,
+                                   int32_t* out_chg);
+
+/* Hit index of a new candidate that added no hit of its own (a held-back
+ * copy). */
+#define MKFG_NO_HIT (-100000)
+
+/* Seeds in Finding state at one layer, as CandCloner::ProcessSeedRange
+ * takes them. Candidate slot k = 8 * seed + c, c < n_cands[seed] (at most
+ * the finder's maxCandsPerSeed); arrays of 8 * n_seeds entries
+ * ([6][8 n_seeds] and [21][8 n_seeds] for par / err), records
+ * [8 n_seeds][17] in the mkfg_ce_records layout, at most 16 hits and one
+ * hole per candidate. held_back: 0 searched on this layer, 1 held
+ * back as it is, 2 held back with a stop (-2) node added
+ * (MkBuilder::find_tracks_handle_missed_layers, mkFit/MkBuilder.cc:
+ * 1568-1637). A best short candidate exists where bshort_valid is set,
+ * with score bshort_score. Host arrays. */
+typedef struct {
+  int32_t n_seeds;
+  const int32_t* n_cands;
+  const float* par;
+  const float* err;
+  const int32_t* chg;
+  const float* chi2;
+  const float* score;
+  const int32_t* nfound;
+  const int32_t* nmiss;
+  const int32_t* nover;
+  const int32_t* ninside;
+  const int32_t* ntail;
+  const int32_t* held_back;
+  const int32_t* n_rec;
+  const int32_t* rec_hit;
+  const int32_t* rec_module;
+  const float* rec_chi2;
+  const float* rec_score;
+  const int32_t* bshort_valid;
+  const float* bshort_score;
+} mkfg_clone_in;
+
+/* The seeds after the clone step: n_cands, and per new candidate slot
+ * (same layout as the input) its state and counters, parent (input slot c
+ * it was made from), hit (the hit or hole code it added, MKFG_NO_HIT for
+ * a held-back copy), overlap_hit (the overlap hit it added, -1 none),
+ * update_hit (the hit UpdateWithLastHit must use, -1 when it takes no
+ * update); slots past n_cands hold parent -1. The best short candidate per
+ * seed: valid flag, score (-1e16, getScoreWorstPossible, when not valid),
+ * found hits and chi2. */
+typedef struct {
+  int32_t* n_cands;
+  float* par;
+  float* err;
+  int32_t* chg;
+  float* chi2;
+  float* score;
+  int32_t* nfound;
+  int32_t* nmiss;
+  int32_t* nover;
+  int32_t* ninside;
+  int32_t* ntail;
+  int32_t* parent;
+  int32_t* hit;
+  int32_t* overlap_hit;
+  int32_t* update_hit;
+  int32_t* bshort_valid; /* [n_seeds] */
+  float* bshort_score;   /* -1e16 (getScoreWorstPossible) when not valid */
+  int32_t* bshort_nfound;
+  float* bshort_chi2;
+} mkfg_clone_out;
+
+/* CandCloner::ProcessSeedRange (mkFit/CandCloner.cc:36-189) as a plain
+ * worker call for layer `layer`, with the configured finder's cuts
+ * (maxCandsPerSeed, chi2CutOverlap, pTCutOverlap): per seed the records
+ * ranked by score, the top maxCandsPerSeed taken, stop (-2) records
+ * offered to the best short candidate, held-back candidates merged in by
+ * score, the overlap hit of the parent's best pair appended (pT above the
+ * cut), the update list formed. Exact score ties are ranked by record
+ * position (candidate, then hand-over order), the order std::sort leaves
+ * when it keeps them. Needs mkfg_finder_setup, no event. Synchronizes. */
+int mkfg_find_clone_seeds(mkfg_context* ctx, int32_t layer, const mkfg_clone_in* in,
+                          mkfg_clone_out* out);
 /* The hit index the upload built on the device for uploaded event `event`
  * (LayerOfHits after SuckInHits / EndRegistrationOfHits,
  * mkFit/HitStructures.cc:77-338): bins in the layout of

@@ -38,13 +38,14 @@ constexpr int kBlock = 256;
 #define MKFG_HEAVY_MIN_BLOCKS 2
 #endif
 // The propagation kernel gains from 4 (64 registers, a few spilled to L1;
-// measured on the 64-event batch: 18.98 vs 20.06 ms per step); chi2 and
-// update do not.
+// measured on the 64-event batch: 18.98 vs 20.06 ms per step; 3 and 5 give
+// 5.74 and 5.55 ms against 5.25 ms for the kernel). The chi2 kernel gains
+// from 3 (2.45 vs 2.71 ms per step); update stays at 2.
 #ifndef MKFG_PROP_MIN_BLOCKS
 #define MKFG_PROP_MIN_BLOCKS 4
 #endif
 #ifndef MKFG_CHI2_MIN_BLOCKS
-#define MKFG_CHI2_MIN_BLOCKS MKFG_HEAVY_MIN_BLOCKS
+#define MKFG_CHI2_MIN_BLOCKS 3
 #endif
 #ifndef MKFG_UPD_MIN_BLOCKS
 #define MKFG_UPD_MIN_BLOCKS MKFG_HEAVY_MIN_BLOCKS
@@ -841,6 +842,122 @@ __global__ void k_select_hit_indices(EventDev E, const FindConfigDev* __restrict
   if (wsr_out) wsr_out[i] = wsr;
 }
 
+//------------------------------------------------------------------------------
+// MkFinder::FindCandidatesCloneEngine as a plain worker call (mkFit/
+// MkFinder.cc:1116-1284): for caller-given states on layer `layer` with the
+// hit lists of SelectHitIndices, the records (IdxChi2List) each candidate
+// hands to the cloner, in the order it hands them: the accepted hits in
+// XHitArr order, then the hole record. One thread per candidate.
+//------------------------------------------------------------------------------
+struct CeArgs {
+  int event, layer, n;
+  const float* par;      // [6][n]
+  const float* err;      // [21][n]
+  const int* chg;
+  const int* nfound;
+  const int* nover;
+  const int* ninside;
+  const int* ntail;
+  const float* chi2;
+  const int* hot_layers; // [n][3] or null
+  const int* xsize;
+  const int* xidx;       // [n][kMaxXHits]
+  const int* wsr;
+  int* n_rec;
+  Record* rec;           // [n][kRecPerCand]
+};
+
+__global__ void k_ce_records(EventDev E, const FindConfigDev* __restrict__ Cp, const CeArgs A) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.n) return;
+  const FindConfigDev& C = *Cp;
+  const LayerDev& L = C.layer[A.layer];
+  float p[6], e[21];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) p[k] = A.par[(size_t)k * A.n + i];
+#pragma unroll
+  for (int k = 0; k < 21; ++k) e[k] = A.err[(size_t)k * A.n + i];
+  const int chg = A.chg[i], nf = A.nfound[i], nov = A.nover[i], nin = A.ninside[i],
+            ntl = A.ntail[i];
+  const float c2 = A.chi2[i];
+  const int hit_base = E.layer_begin[A.event * E.lb_stride + A.layer];
+  Record* out = A.rec + (size_t)i * kRecPerCand;
+  int k = 0;
+  const int xs = min(A.xsize[i], kMaxXHits);
+  for (int h = 0; h < xs; ++h) {
+    const int hidx = A.xidx[(size_t)i * kMaxXHits + h];
+    float chi2;
+    int module;
+    bool ok = pair_accept(E, C, L, hit_base + hidx, p, e, chg, chi2, module);
+    // Pixel same-layer check on the comb candidate's first three nodes
+    // (MkFinder.cc:1195-1210), from the layers the caller gives.
+    if (ok && L.is_pix && A.hot_layers)
+      for (int j = 0; j <= nf && j <= 2; ++j)
+        if (A.hot_layers[(size_t)i * 3 + j] == A.layer) ok = false;
+    if (!ok) continue;
+    out[k++] = Record{hidx, module, chi2, hit_record_score(p, nf, nov, nin + ntl, c2, chi2)};
+  }
+  // The hole record (MkFinder.cc:1245-1283) unless the state is outside the
+  // layer; -7 (inactive module) is not produced: no module is inactive.
+  const int w = A.wsr[i];
+  if (w != kWsrOutside) {
+    int fake = ((nin + ntl) < C.max_holes && ntl < C.max_consec_holes) ? -1 : -2;
+    if (w == kWsrEdge) fake = -3;
+    const int ntail_rec = fake == -1 ? ntl + 1 : ntl;
+    out[k++] = Record{fake, -1, 0.f, score_struct(nf, ntail_rec, nov, nin, c2, fabsf(1.0f / p[3]))};
+  }
+  A.n_rec[i] = k;
+}
+
+//------------------------------------------------------------------------------
+// MkFinder::UpdateWithLastHit + CopyOutParErr as a plain worker call
+// (mkFit/MkFinder.cc:1291-1335): caller-given states updated with one hit
+// each of layer `layer` (index within the layer). One thread per state.
+//------------------------------------------------------------------------------
+__global__ void k_update_last_hit(EventDev E, const FindConfigDev* __restrict__ Cp, int event,
+                                  int layer, int n, const int* __restrict__ hit,
+                                  float* __restrict__ par, float* __restrict__ err,
+                                  int* __restrict__ chg) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const FindConfigDev& C = *Cp;
+  float p[6], e[21];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) p[k] = par[(size_t)k * n + i];
+#pragma unroll
+  for (int k = 0; k < 21; ++k) e[k] = err[(size_t)k * n + i];
+  int q = chg[i];
+  update_state(E, C, C.layer[layer], E.layer_begin[event * E.lb_stride + layer] + hit[i], p, e, q);
+#pragma unroll
+  for (int k = 0; k < 6; ++k) par[(size_t)k * n + i] = p[k];
+#pragma unroll
+  for (int k = 0; k < 21; ++k) err[(size_t)k * n + i] = e[k];
+  chg[i] = q;
+}
+
+//------------------------------------------------------------------------------
+// CandCloner::ProcessSeedRange as a plain worker call (mkFit/CandCloner.cc:
+// 36-189): the clone step of the graph form (clone_seed) run on
+// caller-given candidates and records held in a private EventDev. One warp
+// per seed.
+//------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_clone_worker(EventDev W, const FindConfigDev* __restrict__ Cp,
+                                                         int layer, int* __restrict__ n_new,
+                                                         int* __restrict__ parent) {
+  const FindConfigDev& C = *Cp;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __shared__ HitMatchPair s_hm[kBlock / 32][kSlots];
+  __shared__ CloneScratch s_scratch[kBlock / 32];
+  const int s = blockIdx.x * (kBlock / 32) + warp;
+  if (s >= W.n_seeds) return;
+  const SeedRecords R{W.rec + (size_t)s * kRecPerSeed, W.rmask + s * kSlots, W.wsr + s * kSlots,
+                      W.extra_last + s * kSlots, W.upd + s * kSlots};
+  int upd = 0;
+  const int n = clone_seed(W, C, s, layer, kFinding, W.n_cands[s], 0, R, s_hm[warp], s_scratch[warp],
+                           upd, lane, nullptr, parent + s * kSlots);
+  if (lane == 0) n_new[s] = n;
+}
+
 __global__ void k_select_out(EventDev E, const SelectArgs A, const int* __restrict__ dup,
                              int* __restrict__ keep_by_label) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -965,6 +1082,15 @@ struct Finder {
   FindConfigDev* d_cfg_bks = nullptr;  // backward-search plans
   float* d_mat = nullptr;  // material map (radiation lengths, then xi) taken at setup
   DevBuf sel;  // output selection scratch
+  DevBuf wrk;  // staging of the per-layer worker calls
+  // Global index of every uploaded event's layer starts ([n_events][L + 1]),
+  // for checking the hit indices the worker calls are given.
+  std::vector<int> h_lb;
+  // Hits of layer `layer` of uploaded event `event`.
+  int layer_size(int event, int layer) const {
+    const size_t o = (size_t)event * (host_cfg.n_layers + 1) + layer;
+    return h_lb[o + 1] - h_lb[o];
+  }
   // A quality filter removed comb candidates since the upload (the device
   // flags in ev.removed, cleared by every run, say which).
   bool filter_removed = false;
@@ -1004,6 +1130,7 @@ void finder_release(mkfg_context* ctx) {
   f->drop_graph();
   f->bk.release();
   f->sel.release();
+  f->wrk.release();
   f->hits_h.release();
   f->outb_h.release();
   f->seeds_h.release();
@@ -1550,6 +1677,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   f->h_region.assign(ss.region, ss.region + S);
   f->h_seed_off = seed_off;
   f->h_hit_off = hit_off;
+  f->h_lb.assign(hh.lb, hh.lb + n_lb);
   f->events_loaded = 1;
   // Seeds dropped by the post-cleaning are absent from the backward fit's
   // seed groups, as filtered ones are.
@@ -2212,6 +2340,381 @@ extern "C" int mkfg_find_select_hit_indices(mkfg_context* ctx, int32_t event, in
   MKFG_CUDA_TRY(cudaMemcpyAsync(xhit_idx, d_idx, 4 * (size_t)n * kMaxXHits, cudaMemcpyDeviceToHost, st));
   if (wsr) MKFG_CUDA_TRY(cudaMemcpyAsync(wsr, d_wsr, 4 * (size_t)n, cudaMemcpyDeviceToHost, st));
   MKFG_CUDA_TRY(cudaStreamSynchronize(st));
+  return MKFG_OK;
+}
+
+namespace {
+
+// Host -> device staging of a worker call's arrays in the finder's worker
+// buffer: reserve() every array first (sizes only), then ensure() once and
+// put() / get() them in the same order.
+struct Staging {
+  Finder* f;
+  cudaStream_t st;
+  size_t need = 0;
+  char* at = nullptr;
+  int rc = MKFG_OK;
+  void reserve(size_t bytes) { need += rounded(bytes); }
+  char* end = nullptr;
+  int ensure() {
+    const size_t bytes = need + 64 * 256;  // slack for the per-array rounding
+    if ((rc = f->wrk.ensure(bytes))) return rc;
+    at = f->wrk.as<char>();
+    end = at + bytes;
+    return MKFG_OK;
+  }
+  template <typename T>
+  T* take(size_t n) {
+    const size_t bytes = rounded(n * sizeof(T));
+    if (at + bytes > end) {
+      if (rc == MKFG_OK) rc = set_error(MKFG_ERR_CUDA, "worker staging sized short by %zu bytes",
+                                        (size_t)(at + bytes - end));
+      return reinterpret_cast<T*>(f->wrk.ptr);
+    }
+    T* d = reinterpret_cast<T*>(at);
+    at += bytes;
+    return d;
+  }
+  template <typename T>
+  T* put(const T* h, size_t n) {
+    T* d = take<T>(n);
+    if (rc == MKFG_OK && n) {
+      const cudaError_t ce = cudaMemcpyAsync(d, h, n * sizeof(T), cudaMemcpyHostToDevice, st);
+      if (ce != cudaSuccess) rc = set_error(MKFG_ERR_CUDA, "worker staging: %s", cudaGetErrorString(ce));
+    }
+    return d;
+  }
+  template <typename T>
+  void get(T* h, const T* d, size_t n) {
+    if (rc == MKFG_OK && n) {
+      const cudaError_t ce = cudaMemcpyAsync(h, d, n * sizeof(T), cudaMemcpyDeviceToHost, st);
+      if (ce != cudaSuccess) rc = set_error(MKFG_ERR_CUDA, "worker readback: %s", cudaGetErrorString(ce));
+    }
+  }
+};
+
+// Common checks of the event / layer worker calls.
+int check_worker(Finder* f, int event, int layer) {
+  MKFG_REQUIRE(f->configured, "mkfg_finder_setup was not called");
+  MKFG_REQUIRE(f->events_loaded, "no event uploaded");
+  MKFG_REQUIRE(event >= 0 && event < f->n_events, "event %d out of range", event);
+  MKFG_REQUIRE(layer >= 0 && layer < f->host_cfg.n_layers, "layer %d out of range", layer);
+  return MKFG_OK;
+}
+
+constexpr int kWorkerHotCap = 40;  // 16 setup nodes + a best short node + 2 per new candidate
+
+}  // namespace
+
+extern "C" int mkfg_find_candidates_clone_engine(mkfg_context* ctx, int32_t event, int32_t layer,
+                                                 int32_t n, const float* par, const float* err,
+                                                 const int32_t* chg, const mkfg_cand_counts* counts,
+                                                 const int32_t* seed_hot_layers,
+                                                 const int32_t* xhit_size, const int32_t* xhit_idx,
+                                                 const int32_t* wsr, mkfg_ce_records* out) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  Finder* f = finder_of(ctx);
+  if ((rc = check_worker(f, event, layer))) return rc;
+  MKFG_REQUIRE(n >= 0, "negative candidate count");
+  if (n == 0) return MKFG_OK;
+  MKFG_REQUIRE(par && err && chg && counts && xhit_size && xhit_idx && wsr && out, "null argument");
+  MKFG_REQUIRE(counts->nfound && counts->nover && counts->ninside && counts->ntail && counts->chi2,
+               "null candidate counter array");
+  MKFG_REQUIRE(out->n && out->hit && out->module && out->chi2 && out->score, "null record array");
+  const int lsize = f->layer_size(event, layer);
+  for (int i = 0; i < n; ++i) {
+    MKFG_REQUIRE(xhit_size[i] <= kMaxXHits, "xhit_size[%d] = %d above %d", i, xhit_size[i], kMaxXHits);
+    MKFG_REQUIRE(wsr[i] >= kWsrInside && wsr[i] <= kWsrOutside, "wsr[%d] = %d", i, wsr[i]);
+    for (int h = 0; h < xhit_size[i]; ++h) {
+      const int x = xhit_idx[(size_t)i * kMaxXHits + h];
+      MKFG_REQUIRE(x >= 0 && x < lsize, "xhit_idx[%d][%d] = %d outside layer %d, which holds %d hits",
+                   i, h, x, layer, lsize);
+    }
+  }
+  cudaStream_t st = ctx->stream;
+  Staging S{f, st};
+  const size_t N = (size_t)n;
+  S.reserve(4 * 27 * N);
+  S.reserve(4 * 6 * N);
+  if (seed_hot_layers) S.reserve(4 * 3 * N);
+  S.reserve(4 * (2 + kMaxXHits) * N);
+  S.reserve(4 * N + sizeof(Record) * kRecPerCand * N);
+  if ((rc = S.ensure())) return rc;
+  CeArgs A{};
+  A.event = event;
+  A.layer = layer;
+  A.n = n;
+  A.par = S.put(par, 6 * N);
+  A.err = S.put(err, 21 * N);
+  A.chg = S.put(chg, N);
+  A.nfound = S.put(counts->nfound, N);
+  A.nover = S.put(counts->nover, N);
+  A.ninside = S.put(counts->ninside, N);
+  A.ntail = S.put(counts->ntail, N);
+  A.chi2 = S.put(counts->chi2, N);
+  A.hot_layers = seed_hot_layers ? S.put(seed_hot_layers, 3 * N) : nullptr;
+  A.xsize = S.put(xhit_size, N);
+  A.xidx = S.put(xhit_idx, kMaxXHits * N);
+  A.wsr = S.put(wsr, N);
+  A.n_rec = S.take<int>(N);
+  A.rec = S.take<Record>(kRecPerCand * N);
+  if (S.rc) return S.rc;
+  k_ce_records<<<(n + 127) / 128, 128, 0, st>>>(f->ev, f->d_cfg, A);
+  MKFG_CUDA_TRY(cudaGetLastError());
+  std::vector<Record> rec(kRecPerCand * N);
+  S.get(out->n, A.n_rec, N);
+  S.get(rec.data(), A.rec, rec.size());
+  MKFG_CUDA_TRY(cudaStreamSynchronize(st));
+  if (S.rc) return S.rc;
+  for (size_t i = 0; i < N; ++i)
+    for (int k = 0; k < kRecPerCand; ++k) {
+      const size_t j = i * kRecPerCand + k;
+      const bool live = k < out->n[i];
+      out->hit[j] = live ? rec[j].hit : 0;
+      out->module[j] = live ? rec[j].module : 0;
+      out->chi2[j] = live ? rec[j].chi2 : 0.f;
+      out->score[j] = live ? rec[j].score : 0.f;
+    }
+  return MKFG_OK;
+}
+
+extern "C" int mkfg_find_update_with_last_hit(mkfg_context* ctx, int32_t event, int32_t layer,
+                                              int32_t n, const float* par, const float* err,
+                                              const int32_t* chg, const int32_t* hit_idx,
+                                              float* out_par, float* out_err, int32_t* out_chg) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  Finder* f = finder_of(ctx);
+  if ((rc = check_worker(f, event, layer))) return rc;
+  MKFG_REQUIRE(n >= 0, "negative candidate count");
+  if (n == 0) return MKFG_OK;
+  MKFG_REQUIRE(par && err && chg && hit_idx && out_par && out_err && out_chg, "null argument");
+  const int lsize = f->layer_size(event, layer);
+  for (int i = 0; i < n; ++i)
+    MKFG_REQUIRE(hit_idx[i] >= 0 && hit_idx[i] < lsize,
+                 "hit_idx[%d] = %d outside layer %d, which holds %d hits", i, hit_idx[i], layer, lsize);
+  cudaStream_t st = ctx->stream;
+  Staging S{f, st};
+  const size_t N = (size_t)n;
+  S.reserve(4 * 27 * N);
+  S.reserve(4 * 2 * N);
+  if ((rc = S.ensure())) return rc;
+  float* d_par = S.put(par, 6 * N);
+  float* d_err = S.put(err, 21 * N);
+  int* d_chg = S.put(chg, N);
+  const int* d_hit = S.put(hit_idx, N);
+  if (S.rc) return S.rc;
+  k_update_last_hit<<<(n + 127) / 128, 128, 0, st>>>(f->ev, f->d_cfg, event, layer, n, d_hit, d_par,
+                                                     d_err, d_chg);
+  MKFG_CUDA_TRY(cudaGetLastError());
+  S.get(out_par, d_par, 6 * N);
+  S.get(out_err, d_err, 21 * N);
+  S.get(out_chg, d_chg, N);
+  MKFG_CUDA_TRY(cudaStreamSynchronize(st));
+  return S.rc;
+}
+
+extern "C" int mkfg_find_clone_seeds(mkfg_context* ctx, int32_t layer, const mkfg_clone_in* in,
+                                     mkfg_clone_out* out) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  Finder* f = finder_of(ctx);
+  MKFG_REQUIRE(f->configured, "mkfg_finder_setup was not called");
+  MKFG_REQUIRE(in && out, "null argument");
+  MKFG_REQUIRE(layer >= 0 && layer < f->host_cfg.n_layers, "layer %d out of range", layer);
+  const int S = in->n_seeds;
+  MKFG_REQUIRE(S >= 0 && S <= (1 << 24), "seed count %d out of range", S);
+  if (S == 0) return MKFG_OK;
+  MKFG_REQUIRE(in->n_cands && in->par && in->err && in->chg && in->chi2 && in->score && in->nfound &&
+                   in->nmiss && in->nover && in->ninside && in->ntail && in->held_back && in->n_rec &&
+                   in->rec_hit && in->rec_module && in->rec_chi2 && in->rec_score &&
+                   in->bshort_valid && in->bshort_score,
+               "null input array");
+  MKFG_REQUIRE(out->n_cands && out->par && out->err && out->chg && out->chi2 && out->score &&
+                   out->nfound && out->nmiss && out->nover && out->ninside && out->ntail &&
+                   out->parent && out->hit && out->overlap_hit && out->update_hit &&
+                   out->bshort_valid && out->bshort_score && out->bshort_nfound && out->bshort_chi2,
+               "null output array");
+  const int M = f->host_cfg.max_cands;
+  const size_t SC = (size_t)S * kSlots;
+  // Records into the graph form's layout: a candidate's hit records at
+  // positions 0.. in the given order, its hole record at kMaxXHits.
+  std::vector<Record> rec((size_t)S * kRecPerSeed, Record{0, 0, 0.f, 0.f});
+  std::vector<uint32_t> rmask(SC, 0u);
+  std::vector<int> wsr(SC, 0), extra_last(SC, -1), last(SC, 0);
+  std::vector<int> node_hot((size_t)S * kWorkerHotCap, 0), node_prev((size_t)S * kWorkerHotCap, -1);
+  std::vector<int> hot_size(S, 2 * kSlots);
+  for (int s = 0; s < S; ++s) {
+    const int nc = in->n_cands[s];
+    MKFG_REQUIRE(nc >= 1 && nc <= M, "n_cands[%d] = %d outside [1, %d]", s, nc, M);
+    for (int c = 0; c < kSlots; ++c) {
+      const size_t k = (size_t)s * kSlots + c;
+      // Setup nodes: node c ends candidate c's list; node kSlots + c is the
+      // stop node of a candidate held back with one.
+      last[k] = c;
+      if (c >= nc) continue;
+      const int hb = in->held_back[k];
+      MKFG_REQUIRE(hb >= 0 && hb <= 2, "held_back[%d][%d] = %d", s, c, hb);
+      wsr[k] = hb << 8;
+      if (hb == 2) {
+        const size_t node = (size_t)s * kWorkerHotCap + kSlots + c;
+        node_hot[node] = (-2 & 0xffffff) | (layer << 24);
+        node_prev[node] = c;
+        extra_last[k] = kSlots + c;
+      }
+      const int nr = in->n_rec[k];
+      MKFG_REQUIRE(nr >= 0 && nr <= kRecPerCand, "n_rec[%d][%d] = %d", s, c, nr);
+      int nh = 0, nholes = 0;
+      for (int j = 0; j < nr; ++j) {
+        const size_t src = k * kRecPerCand + j;
+        const int hit = in->rec_hit[src];
+        int pos;
+        if (hit >= 0) {
+          MKFG_REQUIRE(nh < kMaxXHits, "seed %d candidate %d: more than %d hit records", s, c, kMaxXHits);
+          pos = nh++;
+        } else {
+          MKFG_REQUIRE(hit == -1 || hit == -2 || hit == -3,
+                       "seed %d candidate %d: record hit %d is neither a hit nor a hole code", s, c, hit);
+          MKFG_REQUIRE(nholes == 0, "seed %d candidate %d: more than one hole record", s, c);
+          ++nholes;
+          pos = kMaxXHits;
+        }
+        rec[(size_t)s * kRecPerSeed + c * kRecPerCand + pos] =
+            Record{hit, in->rec_module[src], in->rec_chi2[src], in->rec_score[src]};
+        rmask[k] |= 1u << pos;
+      }
+    }
+  }
+  cudaStream_t st = ctx->stream;
+  Staging St{f, st};
+  St.reserve(4 * 27 * SC * 2);           // par / err, both buffers
+  St.reserve(4 * 11 * SC);               // counters and scores, input buffer
+  St.reserve(4 * 11 * SC);               // output buffer
+  St.reserve(4 * 27 * (size_t)S + 4 * 12 * (size_t)S);  // best short candidate
+  St.reserve(4 * 3 * (size_t)S * kWorkerHotCap + 4 * (size_t)S * 4);
+  St.reserve(sizeof(Record) * rec.size() + 4 * 6 * SC + 64);
+  if ((rc = St.ensure())) return rc;
+  auto cand_view = [&](size_t cap) {
+    CandSoA c{};
+    c.par = St.take<float>(6 * cap);
+    c.err = St.take<float>(21 * cap);
+    c.chg = St.take<int>(cap);
+    c.chi2 = St.take<float>(cap);
+    c.score = St.take<float>(cap);
+    c.last = St.take<int>(cap);
+    c.nfound = St.take<int>(cap);
+    c.nmiss = St.take<int>(cap);
+    c.nover = St.take<int>(cap);
+    c.ninside = St.take<int>(cap);
+    c.ntail = St.take<int>(cap);
+    c.cap = (int)cap;
+    return c;
+  };
+  EventDev W{};
+  W.n_seeds = S;
+  W.cand[0] = cand_view(SC);
+  W.cand[1] = cand_view(SC);
+  W.bshort = cand_view((size_t)S);
+  auto up = [&](void* d, const void* h, size_t bytes) {
+    if (St.rc == MKFG_OK && bytes) {
+      const cudaError_t ce = cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st);
+      if (ce != cudaSuccess) St.rc = set_error(MKFG_ERR_CUDA, "worker staging: %s", cudaGetErrorString(ce));
+    }
+  };
+  const CandSoA& B = W.cand[0];
+  up(B.par, in->par, 4 * 6 * SC);
+  up(B.err, in->err, 4 * 21 * SC);
+  up(B.chg, in->chg, 4 * SC);
+  up(B.chi2, in->chi2, 4 * SC);
+  up(B.score, in->score, 4 * SC);
+  up(B.last, last.data(), 4 * SC);
+  up(B.nfound, in->nfound, 4 * SC);
+  up(B.nmiss, in->nmiss, 4 * SC);
+  up(B.nover, in->nover, 4 * SC);
+  up(B.ninside, in->ninside, 4 * SC);
+  up(B.ntail, in->ntail, 4 * SC);
+  up(W.bshort.score, in->bshort_score, 4 * (size_t)S);
+  W.bshort_valid = St.put(in->bshort_valid, (size_t)S);
+  W.n_cands = St.put(in->n_cands, (size_t)S);
+  W.hot_size = St.put(hot_size.data(), (size_t)S);
+  W.node_hot = St.put(node_hot.data(), node_hot.size());
+  W.node_prev = St.put(node_prev.data(), node_prev.size());
+  W.node_chi2 = St.take<float>((size_t)S * kWorkerHotCap);
+  W.hot_cap = kWorkerHotCap;
+  W.rec = St.put(rec.data(), rec.size());
+  W.rmask = St.put(rmask.data(), SC);
+  W.wsr = St.put(wsr.data(), SC);
+  W.extra_last = St.put(extra_last.data(), SC);
+  W.upd = St.take<int>(SC);
+  int* d_new = St.take<int>((size_t)S);
+  int* d_parent = St.take<int>(SC);
+  W.err_flags = St.take<int>(16);
+  if (St.rc) return St.rc;
+  MKFG_CUDA_TRY(cudaMemsetAsync(W.err_flags, 0, 4, st));
+  MKFG_CUDA_TRY(cudaMemsetAsync(W.upd, 0, 4 * SC, st));
+  MKFG_CUDA_TRY(cudaMemsetAsync(d_parent, 0xff, 4 * SC, st));
+  const int blocks = (S + kBlock / 32 - 1) / (kBlock / 32);
+  k_clone_worker<<<blocks, kBlock, 0, st>>>(W, f->d_cfg, layer, d_new, d_parent);
+  MKFG_CUDA_TRY(cudaGetLastError());
+  // Read back.
+  const CandSoA& N = W.cand[1];
+  std::vector<int> nnew(S), parent(SC), upd(SC), nlast(SC), flags(1);
+  std::vector<int> bvalid(S), bnfound(S);
+  std::vector<float> bscore(S), bchi2(S);
+  St.get(nnew.data(), d_new, (size_t)S);
+  St.get(parent.data(), d_parent, SC);
+  St.get(upd.data(), W.upd, SC);
+  St.get(out->par, N.par, 6 * SC);
+  St.get(out->err, N.err, 21 * SC);
+  St.get(out->chg, N.chg, SC);
+  St.get(out->chi2, N.chi2, SC);
+  St.get(out->score, N.score, SC);
+  St.get(nlast.data(), N.last, SC);
+  St.get(out->nfound, N.nfound, SC);
+  St.get(out->nmiss, N.nmiss, SC);
+  St.get(out->nover, N.nover, SC);
+  St.get(out->ninside, N.ninside, SC);
+  St.get(out->ntail, N.ntail, SC);
+  St.get(bvalid.data(), W.bshort_valid, (size_t)S);
+  St.get(bscore.data(), W.bshort.score, (size_t)S);
+  St.get(bchi2.data(), W.bshort.chi2, (size_t)S);
+  St.get(bnfound.data(), W.bshort.nfound, (size_t)S);
+  St.get(node_hot.data(), W.node_hot, node_hot.size());
+  St.get(node_prev.data(), W.node_prev, node_prev.size());
+  St.get(flags.data(), W.err_flags, 1);
+  MKFG_CUDA_TRY(cudaStreamSynchronize(st));
+  if (St.rc) return St.rc;
+  if (flags[0] & kErrArena) return set_error(MKFG_ERR_OVERFLOW, "clone worker arena overflow");
+  auto hot_idx = [&](int s, int node) { return (node_hot[(size_t)s * kWorkerHotCap + node] << 8) >> 8; };
+  for (int s = 0; s < S; ++s) {
+    out->n_cands[s] = nnew[s];
+    out->bshort_valid[s] = bvalid[s];
+    out->bshort_score[s] = bvalid[s] ? bscore[s] : -1e16f;  // getScoreWorstPossible
+    out->bshort_nfound[s] = bvalid[s] ? bnfound[s] : 0;
+    out->bshort_chi2[s] = bvalid[s] ? bchi2[s] : 0.f;
+    for (int c = 0; c < kSlots; ++c) {
+      const size_t k = (size_t)s * kSlots + c;
+      out->parent[k] = -1;
+      out->hit[k] = MKFG_NO_HIT;
+      out->overlap_hit[k] = -1;
+      out->update_hit[k] = -1;
+      if (c >= nnew[s]) continue;
+      out->parent[k] = parent[k];
+      out->update_hit[k] = upd[k] - 1;
+      // The nodes this step added (above the setup nodes): the hit or hole,
+      // then the overlap hit, if any.
+      const int l1 = nlast[k];
+      if (l1 < 2 * kSlots) continue;  // held back: no node of its own
+      const int l0 = node_prev[(size_t)s * kWorkerHotCap + l1];
+      if (l0 >= 2 * kSlots) {
+        out->hit[k] = hot_idx(s, l0);
+        out->overlap_hit[k] = hot_idx(s, l1);
+      } else {
+        out->hit[k] = hot_idx(s, l1);
+      }
+    }
+  }
   return MKFG_OK;
 }
 

@@ -420,14 +420,15 @@ __device__ __forceinline__ void select_cand(const EventDev& E, const FindConfigD
   }
 }
 
-// One (candidate, hit) evaluation (MkFinder::FindCandidatesCloneEngine,
-// mkFit/MkFinder.cc:1142-1240, with kalmanPropagateAndComputeChi2[Endcap]).
-// Returns whether the hit is accepted; fills chi2, score, module.
-__device__ __forceinline__ bool eval_pair(const EventDev& E, const FindConfigDev& C,
-                                          const LayerDev& L, int layer, int s, int g,
-                                          const float (&ppar)[6], const float (&perr)[21], int chg,
-                                          int nfound, int nover, int nholes, float cand_chi2,
-                                          float& chi2_out, float& score_out, int& module_out) {
+// The chi2 and the cuts of one (candidate, hit) evaluation
+// (MkFinder::FindCandidatesCloneEngine, mkFit/MkFinder.cc:1142-1193, with
+// kalmanPropagateAndComputeChi2[Endcap]): dynamic chi2 cut, strip
+// compatibility and strip charge. The pixel same-layer check is the
+// caller's. Returns whether the hit passes; fills chi2 and module.
+__device__ __forceinline__ bool pair_accept(const EventDev& E, const FindConfigDev& C,
+                                            const LayerDev& L, int g, const float (&ppar)[6],
+                                            const float (&perr)[21], int chg, float& chi2_out,
+                                            int& module_out) {
   float mpos[3], merr[6];
 #pragma unroll
   for (int e = 0; e < 3; ++e) mpos[e] = __ldg(E.hpos + e * E.hstride + g);
@@ -450,6 +451,29 @@ __device__ __forceinline__ bool eval_pair(const EventDev& E, const FindConfigDev
     ok = strip_q_compatible(L.is_barrel, perr, hpar, mpos, merr);
     ok &= strip_charge_ok(L.is_barrel, info >> 12, hpar, merr);
   }
+  chi2_out = chi2;
+  module_out = info & 0xfff;
+  return ok;
+}
+
+// Score of an accepted hit record (IdxChi2List with nhits + 1, no tail
+// holes, MkFinder.cc:1222-1233).
+__device__ __forceinline__ float hit_record_score(const float (&ppar)[6], int nfound, int nover,
+                                                  int nholes, float cand_chi2, float chi2) {
+  const float pt = fabsf(1.0f / ppar[3]);
+  return score_struct(nfound + 1, 0, nover, nholes, cand_chi2 + chi2, pt);
+}
+
+// One (candidate, hit) evaluation (MkFinder::FindCandidatesCloneEngine,
+// mkFit/MkFinder.cc:1142-1240). Returns whether the hit is accepted; fills
+// chi2, score, module.
+__device__ __forceinline__ bool eval_pair(const EventDev& E, const FindConfigDev& C,
+                                          const LayerDev& L, int layer, int s, int g,
+                                          const float (&ppar)[6], const float (&perr)[21], int chg,
+                                          int nfound, int nover, int nholes, float cand_chi2,
+                                          float& chi2_out, float& score_out, int& module_out) {
+  float chi2;
+  bool ok = pair_accept(E, C, L, g, ppar, perr, chg, chi2, module_out);
   if (ok && L.is_pix) {
     // No second hit on a pixel layer of the first three hit-on-track nodes
     // (MkFinder.cc:1195-1210: ccand.m_hots[0 .. min(nFound, 2)]). Those are
@@ -461,23 +485,18 @@ __device__ __forceinline__ bool eval_pair(const EventDev& E, const FindConfigDev
       if (hot_layer(node_hot_of(E, s, i)) == layer) ok = false;
   }
   if (!ok) return false;
-  const float pt = fabsf(1.0f / ppar[3]);
-  const float tchi2 = cand_chi2 + chi2;
   chi2_out = chi2;
-  module_out = info & 0xfff;
-  score_out = score_struct(nfound + 1, 0, nover, nholes, tchi2, pt);
+  score_out = hit_record_score(ppar, nfound, nover, nholes, cand_chi2, chi2);
   return true;
 }
 
-// UpdateWithLastHit + CopyOutParErr for one candidate (mkFit/MkFinder.cc:
-// 1291-1335; kalmanPropagateAndUpdate[Endcap], KalmanUtilsMPlex.cc:471-505,
-// 697-731), given the hit's global index g and its layer.
-__device__ __forceinline__ void update_cand_at(const EventDev& E, const FindConfigDev& C,
-                                               const LayerDev& L, int g, const CandSoA& B,
-                                               int slot) {
-  float par[6], err[21];
-  load_state(B, slot, par, err);
-  int chg = B.chg[slot];
+// UpdateWithLastHit on a state in registers (mkFit/MkFinder.cc:1291-1308;
+// kalmanPropagateAndUpdate[Endcap], KalmanUtilsMPlex.cc:471-505, 697-731):
+// propagation to the hit with the inter-layer flags, the update, and the
+// charge flip of a negative 1/pT; g is the hit's global index.
+__device__ __forceinline__ void update_state(const EventDev& E, const FindConfigDev& C,
+                                             const LayerDev& L, int g, float (&par)[6],
+                                             float (&err)[21], int& chg) {
   float mpos[3], merr[6];
 #pragma unroll
   for (int e = 0; e < 3; ++e) mpos[e] = __ldg(E.hpos + e * E.hstride + g);
@@ -495,6 +514,17 @@ __device__ __forceinline__ void update_cand_at(const EventDev& E, const FindConf
     chg = -chg;
     par[3] = -par[3];
   }
+}
+
+// UpdateWithLastHit + CopyOutParErr for one candidate slot of buffer B
+// (MkFinder.cc:1291-1335), given the hit's global index g and its layer.
+__device__ __forceinline__ void update_cand_at(const EventDev& E, const FindConfigDev& C,
+                                               const LayerDev& L, int g, const CandSoA& B,
+                                               int slot) {
+  float par[6], err[21];
+  load_state(B, slot, par, err);
+  int chg = B.chg[slot];
+  update_state(E, C, L, g, par, err, chg);
   store_state(B, slot, par, err);
   B.chg[slot] = chg;
 }
@@ -592,12 +622,14 @@ struct CloneScratch {
 // executed by one warp. Returns the new candidate count, or -1 when the
 // seed's candidates are unchanged; upd_out: lane i's new candidate's
 // update code (SeedRecords::upd_); n_records_out (optional): the records
-// present. The warp owns the seed's arena counter.
+// present; parent_out (optional, kSlots entries): each new candidate's
+// parent slot. The warp owns the seed's arena counter.
 __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev& C, int s,
                                           int layer, int state, int ncand, int cur,
                                           const SeedRecords& R, HitMatchPair* hm,
                                           CloneScratch& X, int& upd_out, int lane,
-                                          int* n_records_out = nullptr) {
+                                          int* n_records_out = nullptr,
+                                          int* parent_out = nullptr) {
   constexpr unsigned kFull = 0xffffffffu;
   const CandSoA& B = E.cand[cur];
   const CandSoA& N = E.cand[cur ^ 1];
@@ -685,6 +717,7 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
     }
     copy_par_err(B, N, s, n_extras, c, lane);
     if (lane < n_extras) {
+      if (parent_out) parent_out[lane] = c;
       const int src = s * kSlots + c, dst = s * kSlots + lane;
       N.chg[dst] = B.chg[src];
       N.chi2[dst] = B.chi2[src];
@@ -906,6 +939,7 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
   // candidate i by lane i.
   copy_par_err(B, N, s, n_pushed, nc.parent, lane);
   if (lane < n_pushed) {
+    if (parent_out) parent_out[lane] = nc.parent;
     const int pc = nc.parent, dst = s * kSlots + lane;
     int nfound = X.cand[3][pc], nmiss = X.cand[4][pc], nin = X.cand[6][pc], ntl = X.cand[7][pc];
     int nover = X.cand[5][pc];

@@ -42,6 +42,66 @@ class MkfgQFilterConfig(ctypes.Structure):
                 ("beam_spot_x", ctypes.c_float), ("beam_spot_y", ctypes.c_float)]
 
 
+class MkfgCandCounts(ctypes.Structure):
+    _fields_ = [(k, vp) for k in ("nfound", "nover", "ninside", "ntail", "chi2")]
+
+
+class MkfgCeRecords(ctypes.Structure):
+    _fields_ = [(k, vp) for k in ("n", "hit", "module", "chi2", "score")]
+
+
+# Input and output fields of mkfg_find_clone_seeds with their dtypes and
+# per-slot widths (0 = one per seed).
+CLONE_IN_FIELDS = [("n_cands", np.int32, 0), ("par", np.float32, 6), ("err", np.float32, 21),
+                   ("chg", np.int32, 1), ("chi2", np.float32, 1), ("score", np.float32, 1),
+                   ("nfound", np.int32, 1), ("nmiss", np.int32, 1), ("nover", np.int32, 1),
+                   ("ninside", np.int32, 1), ("ntail", np.int32, 1), ("held_back", np.int32, 1),
+                   ("n_rec", np.int32, 1), ("rec_hit", np.int32, 17), ("rec_module", np.int32, 17),
+                   ("rec_chi2", np.float32, 17), ("rec_score", np.float32, 17),
+                   ("bshort_valid", np.int32, 0), ("bshort_score", np.float32, 0)]
+CLONE_OUT_FIELDS = [("n_cands", np.int32, 0), ("par", np.float32, 6), ("err", np.float32, 21),
+                    ("chg", np.int32, 1), ("chi2", np.float32, 1), ("score", np.float32, 1),
+                    ("nfound", np.int32, 1), ("nmiss", np.int32, 1), ("nover", np.int32, 1),
+                    ("ninside", np.int32, 1), ("ntail", np.int32, 1), ("parent", np.int32, 1),
+                    ("hit", np.int32, 1), ("overlap_hit", np.int32, 1),
+                    ("update_hit", np.int32, 1), ("bshort_valid", np.int32, 0),
+                    ("bshort_score", np.float32, 0), ("bshort_nfound", np.int32, 0),
+                    ("bshort_chi2", np.float32, 0)]
+
+
+class MkfgCloneIn(ctypes.Structure):
+    _fields_ = [("n_seeds", ctypes.c_int32)] + [(k, vp) for k, _, _ in CLONE_IN_FIELDS]
+
+
+class MkfgCloneOut(ctypes.Structure):
+    _fields_ = [(k, vp) for k, _, _ in CLONE_OUT_FIELDS]
+
+
+# Records per candidate (MKFG_REC_PER_CAND) and the hit code of a
+# held-back copy (MKFG_NO_HIT).
+REC_PER_CAND = 17
+NO_HIT = -100000
+
+
+def clone_arrays(fields, n_seeds, given=None):
+    """Arrays of mkfg_clone_in / mkfg_clone_out for n_seeds seeds: the
+    given ones made contiguous with the field's dtype, the rest zero.
+    Per-slot arrays are [width][8 n_seeds] for par / err, [8 n_seeds][17]
+    for records, [8 n_seeds] otherwise."""
+    out = {}
+    for k, dt, w in fields:
+        shape = (n_seeds,) if w == 0 else ((w, 8 * n_seeds) if w in (6, 21) else
+                                           ((8 * n_seeds, w) if w == 17 else (8 * n_seeds,)))
+        if given is not None and k in given:
+            a = np.ascontiguousarray(given[k], dt)
+            if a.shape != shape:
+                raise ValueError(f"{k}: shape {a.shape}, expected {shape}")
+        else:
+            a = np.zeros(shape, dt)
+        out[k] = a
+    return out
+
+
 # Duplicate removal modes of mkfg_find_select (MKFG_DUP_*).
 DUP_PIXELSEED, DUP_SHAREDHITS, DUP_ETA_PHI, DUP_NONE = range(4)
 # Quality filters of mkfg_find_filter (MKFG_QF_*), StdSeq::qfilter_*.
@@ -131,6 +191,13 @@ def _bind(lib):
                                      ctypes.c_int32, vp]
     lib.mkfg_find_select_hit_indices.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                                  vp, vp, vp, vp, vp]
+    lib.mkfg_find_candidates_clone_engine.argtypes = [
+        vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, vp, vp, vp,
+        ctypes.POINTER(MkfgCandCounts), vp, vp, vp, vp, ctypes.POINTER(MkfgCeRecords)]
+    lib.mkfg_find_update_with_last_hit.argtypes = [vp, ctypes.c_int32, ctypes.c_int32,
+                                                   ctypes.c_int32, vp, vp, vp, vp, vp, vp, vp]
+    lib.mkfg_find_clone_seeds.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(MkfgCloneIn),
+                                          ctypes.POINTER(MkfgCloneOut)]
     lib.mkfg_find_run_fused.argtypes = [vp, ctypes.c_int32]
     lib.mkfg_find_autotune.argtypes = [vp, ctypes.POINTER(ctypes.c_int32),
                                        ctypes.POINTER(ctypes.c_float)]
@@ -406,6 +473,58 @@ class Finder:
             self.ctx.handle, int(event), int(layer), n, par.ctypes.data, err.ctypes.data,
             size.ctypes.data, idx.ctypes.data, wsr.ctypes.data))
         return size, idx, wsr
+
+    def candidates_clone_engine(self, event, layer, par, err, chg, counts, xhit_size, xhit_idx,
+                                wsr, seed_hot_layers=None):
+        """MkFinder::FindCandidatesCloneEngine on states par [6][n], err
+        [21][n], chg [n] propagated to `layer` of uploaded event `event`, with
+        counters `counts` (dict of nfound, nover, ninside, ntail, chi2 [n])
+        and the SelectHitIndices lists: dict of n [n] and hit, module, chi2,
+        score [n][17] (the records in hand-over order)."""
+        c = np.ascontiguousarray
+        par, err = c(par, np.float32), c(err, np.float32)
+        n = par.shape[1]
+        cnt = {k: c(counts[k], np.float32 if k == "chi2" else np.int32)
+               for k in ("nfound", "nover", "ninside", "ntail", "chi2")}
+        cc = MkfgCandCounts(**{k: v.ctypes.data for k, v in cnt.items()})
+        out = dict(n=np.zeros(n, np.int32), hit=np.zeros((n, 17), np.int32),
+                   module=np.zeros((n, 17), np.int32), chi2=np.zeros((n, 17), np.float32),
+                   score=np.zeros((n, 17), np.float32))
+        rec = MkfgCeRecords(**{k: v.ctypes.data for k, v in out.items()})
+        hl = None if seed_hot_layers is None else c(seed_hot_layers, np.int32)
+        xs, xi, w = c(xhit_size, np.int32), c(xhit_idx, np.int32), c(wsr, np.int32)
+        ch = c(chg, np.int32)
+        capi.check(self.lib.mkfg_find_candidates_clone_engine(
+            self.ctx.handle, int(event), int(layer), n, par.ctypes.data, err.ctypes.data,
+            ch.ctypes.data, ctypes.byref(cc), hl.ctypes.data if hl is not None else None,
+            xs.ctypes.data, xi.ctypes.data, w.ctypes.data, ctypes.byref(rec)))
+        return out
+
+    def update_with_last_hit(self, event, layer, par, err, chg, hit_idx):
+        """MkFinder::UpdateWithLastHit + CopyOutParErr: states par [6][n],
+        err [21][n], chg [n] updated with hit hit_idx[i] of `layer` of
+        uploaded event `event`. Returns (par, err, chg)."""
+        c = np.ascontiguousarray
+        par, err = c(par, np.float32).copy(), c(err, np.float32).copy()
+        chg, hit = c(chg, np.int32).copy(), c(hit_idx, np.int32)
+        n = par.shape[1]
+        capi.check(self.lib.mkfg_find_update_with_last_hit(
+            self.ctx.handle, int(event), int(layer), n, par.ctypes.data, err.ctypes.data,
+            chg.ctypes.data, hit.ctypes.data, par.ctypes.data, err.ctypes.data, chg.ctypes.data))
+        return par, err, chg
+
+    def clone_seeds(self, layer, inp):
+        """CandCloner::ProcessSeedRange for the seeds of `inp` (the
+        mkfg_clone_in fields, see clone_arrays) at `layer`. Returns the
+        mkfg_clone_out fields as a dict."""
+        n_seeds = len(inp["n_cands"])
+        a = clone_arrays(CLONE_IN_FIELDS, n_seeds, inp)
+        o = clone_arrays(CLONE_OUT_FIELDS, n_seeds)
+        ci = MkfgCloneIn(n_seeds=n_seeds, **{k: v.ctypes.data for k, v in a.items()})
+        co = MkfgCloneOut(**{k: v.ctypes.data for k, v in o.items()})
+        capi.check(self.lib.mkfg_find_clone_seeds(self.ctx.handle, int(layer), ctypes.byref(ci),
+                                                  ctypes.byref(co)))
+        return o
 
     def hit_index(self, event, n_bins, n_hits):
         """The device-built hit index of uploaded event `event`:

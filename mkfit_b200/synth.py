@@ -222,6 +222,117 @@ def gen_fit_event(n_tracks=20000, seed=0xC0FFEE, radii=None, pt_range=(0.5, 10.0
         radii=radii, rl_grid=rl, xi_grid=xi, seed=seed)
 
 
+def toy_material_grid_zr(radii, disks_z, x_over_x0=0.01, xi_per_x0=0.00217):
+    """toy_material_grid with, in addition, `x_over_x0` radiation lengths on
+    every disk at |z| in `disks_z` (the integer-cm z bins either side of it,
+    all radii); the reference looks the grid up at bin int(|z|)."""
+    rl, xi = toy_material_grid(radii, x_over_x0, xi_per_x0)
+    for z in disks_z:
+        for zb in (int(math.floor(abs(z))) - 1, int(math.floor(abs(z)))):
+            if 0 <= zb < 300:
+                rl[zb, :] = x_over_x0
+                xi[zb, :] = x_over_x0 * xi_per_x0
+    return rl, xi
+
+
+def disk_hit_errors(phi, sig_rphi, sig_r, sig_z=0.01):
+    """Hit covariance of a disk measurement smeared in r-phi and r at fixed
+    z: the (x, y) block is R diag(sig_r^2, sig_rphi^2) R^T with R the
+    rotation by phi."""
+    n = phi.shape[0]
+    e = np.zeros((6, n))
+    sp, cp = np.sin(phi), np.cos(phi)
+    a, b = sig_r ** 2, sig_rphi ** 2
+    e[0] = a * cp * cp + b * sp * sp
+    e[1] = (a - b) * sp * cp
+    e[2] = a * sp * sp + b * cp * cp
+    e[5] = np.full(n, sig_z ** 2)
+    return e
+
+
+def gen_fit_event_steered(n_tracks=20000, seed=0xF17E, radii=(4.0, 8.0),
+                          disks_z=(35.0, 45.0, 55.0, 65.0, 75.0, 85.0, 95.0, 105.0),
+                          pt_range=(1.0, 10.0), eta_range=(1.5, 2.0), sig_rphi=0.01,
+                          sig_z=0.1, sig_r=0.1, x_over_x0=0.01, vtx_sigma_xy=0.01,
+                          vtx_sigma_z=1.0, r_start=1.0):
+    """Steered-fit toy MC (MkFitter::FitTracksSteered): forward tracks,
+    |eta| uniform in eta_range with either sign, crossing the barrel
+    cylinders `radii` first and then the disks at z = sign(eta) * disks_z
+    (the defaults keep that order for every track). Step l is a barrel
+    step for l < len(radii) and an endcap (z) step after: endcap_mask has
+    the disk steps' bits. Smearing and multiple scattering as in
+    gen_fit_event; disk hits are smeared in r-phi and r."""
+    rng = np.random.default_rng(seed)
+    radii = np.asarray(radii, dtype=np.float64)
+    disks_z = np.asarray(disks_z, dtype=np.float64)
+    n = n_tracks
+    pt = rng.uniform(pt_range[0], pt_range[1], n)
+    side = np.where(rng.random(n) < 0.5, -1.0, 1.0)
+    eta = side * rng.uniform(eta_range[0], eta_range[1], n)
+    phi = rng.uniform(-math.pi, math.pi, n)
+    q = np.where(rng.random(n) < 0.5, -1, 1).astype(np.int32)
+    vx = rng.normal(0.0, vtx_sigma_xy, n)
+    vy = rng.normal(0.0, vtx_sigma_xy, n)
+    vz = rng.normal(0.0, vtx_sigma_z, n)
+    theta = 2.0 * np.arctan(np.exp(-eta))
+    hel = Helix(vx, vy, vz, pt, phi, theta, q)
+    s0 = hel.s_at_radius(np.full(n, r_start))
+    x0, y0, z0, ph0 = hel.at(s0)
+    hel.restart(np.ones(n, dtype=bool), x0, y0, z0, ph0, theta)
+    par0 = np.stack([x0, y0, z0, 1.0 / pt, ph0, theta])
+    cov = np.zeros((n, 6, 6))
+    diag = np.stack([np.full(n, 0.1 ** 2), np.full(n, 0.1 ** 2), np.full(n, 1.0 ** 2),
+                     (0.1 / pt) ** 2, np.full(n, 0.05 ** 2), np.full(n, 0.05 ** 2)], axis=1)
+    for k in range(6):
+        cov[:, k, k] = diag[:, k]
+
+    nb, nd = radii.shape[0], disks_z.shape[0]
+    hpos = np.zeros((nb + nd, 3, n))
+    herr = np.zeros((nb + nd, 6, n))
+    mpi = 0.140
+    last_z = z0.copy()
+    for li in range(nb + nd):
+        if li < nb:
+            s = hel.s_at_radius(np.full(n, radii[li]))
+        else:
+            s = hel.s_at_z(side * disks_z[li - nb])
+        x, y, z, ph = hel.at(s)
+        assert (np.abs(z) > np.abs(last_z)).all(), "crossings out of order"
+        last_z = z
+        pphi = np.arctan2(y, x)
+        d = rng.normal(0.0, sig_rphi, n)
+        if li < nb:
+            hpos[li, 0] = x - np.sin(pphi) * d
+            hpos[li, 1] = y + np.cos(pphi) * d
+            hpos[li, 2] = z + rng.normal(0.0, sig_z, n)
+            herr[li] = barrel_hit_errors(pphi, sig_rphi, sig_z)
+            path = 1.0 / np.sin(hel.theta)                       # p / pT
+        else:
+            dr = rng.normal(0.0, sig_r, n)
+            hpos[li, 0] = x - np.sin(pphi) * d + np.cos(pphi) * dr
+            hpos[li, 1] = y + np.cos(pphi) * d + np.sin(pphi) * dr
+            hpos[li, 2] = z
+            herr[li] = disk_hit_errors(pphi, sig_rphi, sig_r)
+            path = 1.0 / np.abs(np.cos(hel.theta))               # p / |pz|
+        p = hel.pt / np.sin(hel.theta)
+        beta = p / np.sqrt(p * p + mpi * mpi)
+        t0 = highland(p, beta, x_over_x0 * path)
+        th_new = hel.theta + rng.normal(0.0, 1.0, n) * t0
+        ph_new = ph + rng.normal(0.0, 1.0, n) * t0 / np.sin(hel.theta)
+        hel.restart(np.ones(n, dtype=bool), x, y, z, ph_new, th_new)
+
+    rl, xi = toy_material_grid_zr(radii, disks_z, x_over_x0)
+    endcap_mask = ((1 << (nb + nd)) - 1) & ~((1 << nb) - 1)
+    return FitEvent(
+        par=np.ascontiguousarray(par0, dtype=np.float32),
+        err=np.ascontiguousarray(pack_sym(cov), dtype=np.float32),
+        chg=q,
+        hit_pos=np.ascontiguousarray(hpos, dtype=np.float32),
+        hit_err=np.ascontiguousarray(herr, dtype=np.float32),
+        radii=radii, disks_z=disks_z, endcap_mask=endcap_mask, rl_grid=rl, xi_grid=xi,
+        seed=seed)
+
+
 # =============================================================================
 # CMS-2017 finding events
 # =============================================================================

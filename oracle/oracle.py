@@ -28,6 +28,14 @@ def restate_lib_path():
     return os.path.join(REF_DIR, "librestate.so")
 
 
+def shims_lib_path(flavour="avx2"):
+    return os.path.join(REF_DIR, f"libmkfit_shims_{flavour}.so")
+
+
+def have_shims(flavour="avx2"):
+    return os.path.exists(shims_lib_path(flavour))
+
+
 def have_ref(flavour="avx2"):
     return os.path.exists(ref_lib_path(flavour))
 
@@ -100,6 +108,36 @@ class RefLib:
         if rc != 0:
             raise RuntimeError(f"ref_fit failed rc={rc}")
         return out_par, out_err, out_chg, secs.value
+
+    def fit_steered(self, par, err, chg, hit_pos, hit_err, endcap_mask, rl_grid=None,
+                    xi_grid=None, pflags=2):
+        """MkFitter steered fit (InputTracksAndHits -> FitTracksSteered ->
+        OutputFittedTracks): step l is an endcap step when bit l of
+        endcap_mask is set. Returns (par, err, chg)."""
+        L = self.lib
+        L.ref_fit_steered.restype = ctypes.c_int
+        L.ref_fit_steered.argtypes = [ctypes.c_int, ctypes.c_int, _i32p, _f32p, _f32p, _i32p,
+                                      _f32p, _f32p, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_int, _f32p, _f32p, _i32p]
+        n = chg.shape[0]
+        nl = hit_pos.shape[0]
+        barrel = np.array([0 if (int(endcap_mask) >> l) & 1 else 1 for l in range(nl)], np.int32)
+        out_par = np.zeros((6, n), np.float32)
+        out_err = np.zeros((21, n), np.float32)
+        out_chg = np.zeros(n, np.int32)
+        rl = _opt(rl_grid, np.float32)
+        xi = _opt(xi_grid, np.float32)
+        rc = L.ref_fit_steered(n, nl, barrel, np.ascontiguousarray(par, np.float32),
+                               np.ascontiguousarray(err, np.float32),
+                               np.ascontiguousarray(chg, np.int32),
+                               np.ascontiguousarray(hit_pos, np.float32),
+                               np.ascontiguousarray(hit_err, np.float32),
+                               rl.ctypes.data if rl is not None else None,
+                               xi.ctypes.data if xi is not None else None, int(pflags),
+                               out_par, out_err, out_chg)
+        if rc != 0:
+            raise RuntimeError(f"ref_fit_steered failed rc={rc}")
+        return out_par, out_err, out_chg
 
 
 class RsMaterial(ctypes.Structure):
@@ -1179,3 +1217,133 @@ def ref_select_hit_indices(reflib, ev, layer, par, err, chg, iteration=0):
     if rc != 0:
         raise RuntimeError(f"ref_select_hit_indices failed rc={rc}")
     return xs, xi
+
+
+def _event_hit_args(ev):
+    c = np.ascontiguousarray
+    return (ev.n_layers, c(ev.layer_begin, np.int32), c(ev.hit_pos, np.float32),
+            c(ev.hit_err, np.float32), c(ev.hit_detid, np.int32), c(ev.hit_cpcm, np.int32))
+
+
+_EV_TYPES = [ctypes.c_int, _i32p, _f32p, _f32p, _i32p, _i32p]
+
+
+def ref_ce_records(reflib, ev, layer, par, err, chg, counts, hot_layers, chi2_cut=30.0,
+                   zero_c2=True):
+    """The reference's SelectHitIndices + FindCandidatesCloneEngine on
+    states par [6][n], err [21][n], chg [n] taken as propagated to `layer`
+    of event `ev`, with counters `counts` (dict of nfound, nover, ninside,
+    ntail, chi2 [n]) and each comb candidate's first three node layers
+    hot_layers [n][3], the chi2 cut set as ref_find sets it
+    (oracle/ref_driver.cc ref_ce_records). Returns
+    (xsize [n], records: dict of n [n] and hit, module, chi2, score
+    [n][17])."""
+    lib = reflib.lib
+    lib.ref_ce_records.restype = ctypes.c_int
+    lib.ref_ce_records.argtypes = _EV_TYPES + [ctypes.c_int, ctypes.c_int, _f32p, _f32p, _i32p,
+                                               _i32p, _i32p, _i32p, _i32p, _f32p, _i32p,
+                                               ctypes.c_float, ctypes.c_int, _i32p,
+                                               _i32p, _i32p, _i32p, _f32p, _f32p]
+    c = np.ascontiguousarray
+    n = int(len(chg))
+    xs = np.zeros(n, np.int32)
+    out = dict(n=np.zeros(n, np.int32), hit=np.zeros((n, 17), np.int32),
+               module=np.zeros((n, 17), np.int32), chi2=np.zeros((n, 17), np.float32),
+               score=np.zeros((n, 17), np.float32))
+    rc = lib.ref_ce_records(*_event_hit_args(ev), int(layer), n, c(par, np.float32),
+                            c(err, np.float32), c(chg, np.int32), c(counts["nfound"], np.int32),
+                            c(counts["nover"], np.int32), c(counts["ninside"], np.int32),
+                            c(counts["ntail"], np.int32), c(counts["chi2"], np.float32),
+                            c(hot_layers, np.int32), float(chi2_cut), int(bool(zero_c2)), xs,
+                            out["n"], out["hit"], out["module"],
+                            out["chi2"], out["score"])
+    if rc != 0:
+        raise RuntimeError(f"ref_ce_records failed rc={rc}")
+    return xs, out
+
+
+def ref_update_with_last_hit(reflib, ev, layer, par, err, chg, hit_idx):
+    """The reference's InputTracksAndHitIdx + UpdateWithLastHit +
+    CopyOutParErr (oracle/ref_driver.cc ref_update_with_last_hit): returns
+    (par, err, chg) updated."""
+    lib = reflib.lib
+    lib.ref_update_with_last_hit.restype = ctypes.c_int
+    lib.ref_update_with_last_hit.argtypes = _EV_TYPES + [ctypes.c_int, ctypes.c_int, _f32p, _f32p,
+                                                         _i32p, _i32p, _f32p, _f32p, _i32p]
+    n = int(len(chg))
+    c = np.ascontiguousarray
+    op = np.zeros((6, n), np.float32)
+    oe = np.zeros((21, n), np.float32)
+    oc = np.zeros(n, np.int32)
+    rc = lib.ref_update_with_last_hit(*_event_hit_args(ev), int(layer), n, c(par, np.float32),
+                                      c(err, np.float32), c(chg, np.int32),
+                                      c(hit_idx, np.int32), op, oe, oc)
+    if rc != 0:
+        raise RuntimeError(f"ref_update_with_last_hit failed rc={rc}")
+    return op, oe, oc
+
+
+def ref_clone_seeds(reflib, layer, inp, max_cands):
+    """CandCloner::ProcessSeedRange of the reference on the seeds of `inp`
+    (the fields of mkfg_clone_in, mkfit_b200.finder.clone_arrays layout) at
+    `layer` with maxCandsPerSeed = max_cands (oracle/ref_driver.cc
+    ref_clone_seeds). Returns the fields of mkfg_clone_out as a dict."""
+    from mkfit_b200.finder import CLONE_IN_FIELDS, CLONE_OUT_FIELDS, clone_arrays
+    n_seeds = len(inp["n_cands"])
+    a = clone_arrays(CLONE_IN_FIELDS, n_seeds, inp)
+    o = clone_arrays(CLONE_OUT_FIELDS, n_seeds)
+    lib = reflib.lib
+    lib.ref_clone_seeds.restype = ctypes.c_int
+    lib.ref_clone_seeds.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p] * (
+        len(CLONE_IN_FIELDS) + len(CLONE_OUT_FIELDS))
+    args = [a[k].ctypes.data for k, _, _ in CLONE_IN_FIELDS]
+    args += [o[k].ctypes.data for k, _, _ in CLONE_OUT_FIELDS]
+    rc = lib.ref_clone_seeds(int(layer), n_seeds, int(max_cands), *args)
+    if rc != 0:
+        raise RuntimeError(f"ref_clone_seeds failed rc={rc}")
+    return o
+
+
+_shims_lib = None
+
+
+def _shims():
+    global _shims_lib
+    if _shims_lib is None:
+        L = ctypes.CDLL(shims_lib_path())
+        common = [_f32p, _f32p, _i32p, _f32p, _f32p, ctypes.c_void_p, ctypes.c_void_p,
+                  ctypes.c_int, ctypes.c_int, _f32p, _f32p, _i32p]
+        L.shim_fit.restype = ctypes.c_int
+        L.shim_fit.argtypes = [ctypes.c_int, ctypes.c_int] + common
+        L.shim_fit_steered.restype = ctypes.c_int
+        L.shim_fit_steered.argtypes = [ctypes.c_int, ctypes.c_int, _i32p] + common
+        _shims_lib = L
+    return _shims_lib
+
+
+def _shim_call(fn, ev, pflags, chunk, *lead):
+    c = np.ascontiguousarray
+    n, nl = ev.n, ev.hit_pos.shape[0]
+    out = (np.zeros((6, n), np.float32), np.zeros((21, n), np.float32), np.zeros(n, np.int32))
+    rl, xi = c(ev.rl_grid, np.float32), c(ev.xi_grid, np.float32)
+    rc = fn(n, nl, *lead, c(ev.par, np.float32), c(ev.err, np.float32), c(ev.chg, np.int32),
+            c(ev.hit_pos, np.float32), c(ev.hit_err, np.float32), rl.ctypes.data, xi.ctypes.data,
+            int(pflags), int(chunk), *out)
+    if rc != 0:
+        raise RuntimeError(f"{fn.__name__} failed rc={rc}")
+    return out
+
+
+def shim_fit(ev, pflags=2, chunk=8):
+    """The reference's fitting loop (runFittingTestPlex) with the
+    MkFitterGpu adapter in place of MkFitter, `chunk` tracks per call
+    (oracle/shim_driver.cc). Returns (par, err, chg)."""
+    return _shim_call(_shims().shim_fit, ev, pflags, chunk)
+
+
+def shim_fit_steered(ev, pflags=2, chunk=8):
+    """InputTracksAndHits -> FitTracksSteered -> OutputFittedTracks with
+    MkFitterGpu, steps steered by ev.endcap_mask. Returns (par, err, chg)."""
+    nl = ev.hit_pos.shape[0]
+    barrel = np.array([0 if (int(ev.endcap_mask) >> l) & 1 else 1 for l in range(nl)], np.int32)
+    return _shim_call(_shims().shim_fit_steered, ev, pflags, chunk, barrel)

@@ -21,6 +21,7 @@
 #include "MaterialEffects.h"
 #include "Track.h"
 #include "TrackerInfo.h"
+#include "mkFit/CandCloner.h"
 #include "mkFit/FindingFoos.h"
 #include "mkFit/HitStructures.h"
 #include "mkFit/IterationConfig.h"
@@ -198,6 +199,57 @@ int ref_fit(int n_tracks, int n_layers, const float* par, const float* err, cons
   return 0;
 }
 
+// Steered fit (MkFitter::FitTracksSteered, mkFit/MkFitter.cc:473-503):
+// step l propagates to the hit's radius and runs the barrel update when
+// is_barrel[l], else to the hit's z and the endcap update. Tracks enter
+// through InputTracksAndHits (mkFit/MkFitter.cc:56-91), any number of
+// steps up to Config::nMaxTrkHits - 1. Arrays as in ref_fit.
+int ref_fit_steered(int n_tracks, int n_layers, const int* is_barrel, const float* par,
+                    const float* err, const int* chg, const float* hit_pos, const float* hit_err,
+                    const float* rl_grid, const float* xi_grid, int pflags, float* out_par,
+                    float* out_err, int* out_chg) {
+  if (n_layers <= 0 || n_layers > Config::nMaxTrkHits - 1 || n_tracks <= 0) return -1;
+  set_material(rl_grid, xi_grid);
+  std::vector<HitVec> layer_hits(n_layers);
+  for (int l = 0; l < n_layers; ++l) {
+    layer_hits[l].reserve(n_tracks);
+    for (int i = 0; i < n_tracks; ++i)
+      layer_hits[l].push_back(make_hit(i, n_tracks, hit_pos + size_t(l) * 3 * n_tracks,
+                                       hit_err + size_t(l) * 6 * n_tracks));
+  }
+  std::vector<Track> sim(n_tracks);
+  for (int i = 0; i < n_tracks; ++i) {
+    sim[i] = make_track(i, n_tracks, par, err, chg);
+    for (int l = 0; l < n_layers; ++l) sim[i].addHitIdx(i, l, 0.f);
+  }
+  std::vector<Track> rec(n_tracks);
+  std::unique_ptr<bool[]> barrel(new bool[n_layers]);
+  for (int l = 0; l < n_layers; ++l) barrel[l] = is_barrel[l] != 0;
+  const int count = (n_tracks + NN - 1) / NN;
+  tbb::parallel_for(
+      tbb::blocked_range<int>(0, count, std::max(1, Config::numSeedsPerTask / NN)),
+      [&](const tbb::blocked_range<int>& rng) {
+        std::unique_ptr<MkFitter> mkfp(new (_mm_malloc(sizeof(MkFitter), 64)) MkFitter);
+        mkfp->SetNhits(n_layers);
+        for (int it = rng.begin(); it < rng.end(); ++it) {
+          const int beg = it * NN;
+          const int end = std::min(beg + NN, n_tracks);
+          mkfp->InputTracksAndHits(sim, layer_hits, beg, end);
+          mkfp->FitTracksSteered(barrel.get(), end - beg, nullptr, PropagationFlags(pflags));
+          mkfp->OutputFittedTracks(rec, beg, end);
+        }
+        MkFitter* raw = mkfp.release();
+        raw->~MkFitter();
+        _mm_free(raw);
+      });
+  for (int i = 0; i < n_tracks; ++i) {
+    for (int k = 0; k < 6; ++k) out_par[k * n_tracks + i] = rec[i].parameters()[k];
+    for (int k = 0; k < 21; ++k) out_err[k * n_tracks + i] = rec[i].errors().Array()[k];
+    out_chg[i] = rec[i].charge();
+  }
+  return 0;
+}
+
 }  // extern "C"
 
 //==============================================================================
@@ -267,6 +319,26 @@ bool qfilter_by_kind(const TrackCand& t, int kind, int min_hits, const BeamSpot&
     case 6: return StdSeq::qfilter_pixelLessBkwd(t, bs, ti);
   }
   return true;
+}
+
+// One event's hits into the reference's containers, as ref_find builds
+// them (Hit::setupAsPixel / setupAsStrip, EventOfHits::SuckInHits).
+// layer_hits must outlive eoh: LayerOfHits points into it.
+void load_event_hits(int n_layers, const int* layer_begin, const float* hpos, const float* herr,
+                     const int* detid, const int* cpcm, std::vector<HitVec>& layer_hits,
+                     EventOfHits& eoh) {
+  const int nh_tot = layer_begin[n_layers];
+  layer_hits.assign(n_layers, HitVec());
+  for (int l = 0; l < n_layers; ++l)
+    for (int h = layer_begin[l]; h < layer_begin[l + 1]; ++h) {
+      Hit hit = make_hit(h, nh_tot, hpos, herr);
+      if (cpcm[h] < 0)
+        hit.setupAsPixel(detid[h], 1, 1);
+      else
+        hit.setupAsStrip(detid[h], cpcm[h], 1);
+      layer_hits[l].push_back(hit);
+    }
+  for (int l = 0; l < n_layers; ++l) eoh.SuckInHits(l, layer_hits[l]);
 }
 
 constexpr int kNumQFilters = 7;
@@ -542,19 +614,9 @@ int ref_select_hit_indices(int n_layers_in, const int* layer_begin, const float*
   ensure_cms2017();
   const int n_layers = (int)Config::TrkInfo.m_layers.size();
   if (n_layers_in != n_layers || layer < 0 || layer >= n_layers) return -1;
-  const int nh_tot = layer_begin[n_layers];
-  std::vector<HitVec> layer_hits(n_layers);
-  for (int l = 0; l < n_layers; ++l)
-    for (int h = layer_begin[l]; h < layer_begin[l + 1]; ++h) {
-      Hit hit = make_hit(h, nh_tot, hpos, herr);
-      if (cpcm[h] < 0)
-        hit.setupAsPixel(detid[h], 1, 1);
-      else
-        hit.setupAsStrip(detid[h], cpcm[h], 1);
-      layer_hits[l].push_back(hit);
-    }
+  std::vector<HitVec> layer_hits;
   EventOfHits eoh(Config::TrkInfo);
-  for (int l = 0; l < n_layers; ++l) eoh.SuckInHits(l, layer_hits[l]);
+  load_event_hits(n_layers, layer_begin, hpos, herr, detid, cpcm, layer_hits, eoh);
   const IterationConfig& itconf = Config::ItrInfo[g_iteration];
   TrackVec tracks;
   tracks.reserve(n);
@@ -572,6 +634,280 @@ int ref_select_hit_indices(int n_layers_in, const int* layer_begin, const float*
     }
   }
   mkf->Release();
+  return 0;
+}
+
+// Candidate i of a worker driver as comb candidate i of eocc, alone in it:
+// state, counters and the given hit-on-track nodes (index, layer pairs;
+// the candidate's last node is the last one given).
+static void worker_cand(EventOfCombCandidates& eocc, int i, int n, const float* par, const float* err,
+                 const int* chg, const HitOnTrack* nodes, int n_nodes) {
+  CombCandidate& cc = eocc[i];
+  int prev = -1;
+  for (int j = 0; j < n_nodes; ++j) prev = cc.AddHit(nodes[j], 0.f, prev);
+  cc.emplace_back(TrackCand(make_track(i, n, par, err, chg), &cc));
+  cc.back().setLastCcIndex(prev);
+  cc.m_state = CombCandidate::Finding;
+}
+
+// MkFinder::FindCandidatesCloneEngine (mkFit/MkFinder.cc:1116-1284) on
+// given states (Par[iP], taken as propagated to `layer`) with the given
+// counters, after the reference's own SelectHitIndices on them, as
+// find_tracks_in_layers calls the two (mkFit/MkBuilder.cc:1960-1990). Each
+// candidate is alone in a comb candidate whose first three nodes lie on
+// hot_layers[i][0..2] (the pixel same-layer check reads them); the chi2
+// cut set as ref_find sets it (chi2_cut, zero_c2). Out:
+// xsize[n] (XHitSize), and the records the cloner received per candidate,
+// in order: n_rec[n], r_hit / r_module / r_chi2 (chi2_hit) / r_score
+// [n][17].
+int ref_ce_records(int n_layers_in, const int* layer_begin, const float* hpos, const float* herr,
+                   const int* detid, const int* cpcm, int layer, int n, const float* par,
+                   const float* err, const int* chg, const int* nfound, const int* nover,
+                   const int* ninside, const int* ntail, const float* cchi2, const int* hot_layers,
+                   float chi2_cut, int zero_c2, int* xsize, int* n_rec, int* r_hit, int* r_module,
+                   float* r_chi2, float* r_score) {
+  ensure_cms2017();
+  fillZRgridME();  // the fit entry may have replaced the material grid
+  const int n_layers = (int)Config::TrkInfo.m_layers.size();
+  if (n_layers_in != n_layers || layer < 0 || layer >= n_layers || n <= 0) return -1;
+  std::vector<HitVec> layer_hits;
+  EventOfHits eoh(Config::TrkInfo);
+  load_event_hits(n_layers, layer_begin, hpos, herr, detid, cpcm, layer_hits, eoh);
+  // The chi2 cut as ref_find sets it (chi2Cut_min, dynamic terms zeroed
+  // when zero_c2).
+  IterationConfig itconf = Config::ItrInfo[g_iteration];
+  itconf.m_params.chi2Cut_min = chi2_cut;
+  if (zero_c2)
+    for (auto& lc : itconf.m_layer_configs) lc.c_c2_0 = lc.c_c2_1 = lc.c_c2_2 = 0.f;
+  EventOfCombCandidates eocc;
+  eocc.Reset(n, 1, 8);
+  eocc.m_size = n;
+  for (int i = 0; i < n; ++i) {
+    HitOnTrack nodes[3];
+    for (int j = 0; j < 3; ++j) nodes[j] = HitOnTrack{0, hot_layers[i * 3 + j]};
+    worker_cand(eocc, i, n, par, err, chg, nodes, 3);
+    TrackCand& t = eocc[i].back();
+    t.setNFoundHits(nfound[i]);
+    t.setNOverlapHits(nover[i]);
+    t.setNInsideMinusOneHits(ninside[i]);
+    t.setNTailMinusOneHits(ntail[i]);
+    t.setChi2(cchi2[i]);
+  }
+  std::vector<std::pair<int, int>> idxs(n), upd_list;
+  for (int i = 0; i < n; ++i) idxs[i] = {i, 0};
+  std::vector<std::vector<TrackCand>> extras(n);
+  CandCloner cloner;
+  cloner.Setup(itconf.m_params);
+  cloner.begin_eta_bin(&eocc, &upd_list, &extras, 0, n);
+  cloner.begin_layer(layer);
+  const LayerOfHits& loh = eoh.m_layers_of_hits[layer];
+  const FindingFoos& ff = FindingFoos::get_finding_foos(loh.is_barrel());
+  std::unique_ptr<MkFinder> mkf(new MkFinder);
+  mkf->Setup(itconf.m_params, itconf.m_layer_configs[layer], nullptr);
+  for (int beg = 0; beg < n; beg += NN) {
+    const int end = std::min(beg + NN, n);
+    mkf->InputTracksAndHitIdx(eocc.m_candidates, idxs, beg, end, true);
+    mkf->SelectHitIndices(loh, end - beg);
+    for (int i = beg; i < end; ++i) xsize[i] = mkf->XHitSize.At(i - beg, 0, 0);
+    mkf->FindCandidatesCloneEngine(loh, cloner, 0, end - beg, ff);
+  }
+  for (int i = 0; i < n; ++i) {
+    const std::vector<IdxChi2List>& v = cloner.m_hits_to_add[i];
+    n_rec[i] = (int)std::min<size_t>(v.size(), 17);
+    for (int k = 0; k < 17; ++k) {
+      const bool live = k < n_rec[i];
+      r_hit[i * 17 + k] = live ? v[k].hitIdx : 0;
+      r_module[i * 17 + k] = live ? (int)v[k].module : 0;
+      r_chi2[i * 17 + k] = live ? v[k].chi2_hit : 0.f;
+      r_score[i * 17 + k] = live ? v[k].score : 0.f;
+    }
+  }
+  mkf->Release();
+  cloner.Release();
+  return 0;
+}
+
+// MkFinder::UpdateWithLastHit + CopyOutParErr (mkFit/MkFinder.cc:
+// 1291-1335) as find_tracks_in_layers calls them (InputTracksAndHitIdx
+// with inputProp, mkFit/MkBuilder.cc:2020-2035): given states, each
+// updated with hit hit_idx[i] of `layer` (its comb candidate's last node).
+int ref_update_with_last_hit(int n_layers_in, const int* layer_begin, const float* hpos,
+                             const float* herr, const int* detid, const int* cpcm, int layer, int n,
+                             const float* par, const float* err, const int* chg,
+                             const int* hit_idx, float* out_par, float* out_err, int* out_chg) {
+  ensure_cms2017();
+  fillZRgridME();  // the fit entry may have replaced the material grid
+  const int n_layers = (int)Config::TrkInfo.m_layers.size();
+  if (n_layers_in != n_layers || layer < 0 || layer >= n_layers || n <= 0) return -1;
+  std::vector<HitVec> layer_hits;
+  EventOfHits eoh(Config::TrkInfo);
+  load_event_hits(n_layers, layer_begin, hpos, herr, detid, cpcm, layer_hits, eoh);
+  const IterationConfig& itconf = Config::ItrInfo[g_iteration];
+  EventOfCombCandidates eocc;
+  eocc.Reset(n, 1, 2);
+  eocc.m_size = n;
+  for (int i = 0; i < n; ++i) {
+    const HitOnTrack node{hit_idx[i], layer};
+    worker_cand(eocc, i, n, par, err, chg, &node, 1);
+  }
+  std::vector<std::pair<int, int>> idxs(n);
+  for (int i = 0; i < n; ++i) idxs[i] = {i, 0};
+  const LayerOfHits& loh = eoh.m_layers_of_hits[layer];
+  const FindingFoos& ff = FindingFoos::get_finding_foos(loh.is_barrel());
+  std::unique_ptr<MkFinder> mkf(new MkFinder);
+  mkf->Setup(itconf.m_params, itconf.m_layer_configs[layer], nullptr);
+  for (int beg = 0; beg < n; beg += NN) {
+    const int end = std::min(beg + NN, n);
+    mkf->InputTracksAndHitIdx(eocc.m_candidates, idxs, beg, end, true);
+    mkf->UpdateWithLastHit(loh, end - beg, ff);
+    mkf->CopyOutParErr(eocc.m_candidates, end - beg, false);
+  }
+  for (int i = 0; i < n; ++i) {
+    const TrackCand& t = eocc[i][0];
+    for (int k = 0; k < 6; ++k) out_par[k * n + i] = t.parameters()[k];
+    for (int k = 0; k < 21; ++k) out_err[k * n + i] = t.errors().Array()[k];
+    out_chg[i] = t.charge();
+  }
+  mkf->Release();
+  return 0;
+}
+
+// CandCloner::ProcessSeedRange (mkFit/CandCloner.cc:36-189) on given
+// seeds at `layer`, through the cloner as find_tracks_in_layers drives it
+// (begin_layer, add_cand, end_layer), with maxCandsPerSeed = max_cands
+// and the selected iteration's overlap cuts. Candidate slot k = 8 s + c;
+// par / err [6|21][8 n_seeds], records [8 n_seeds][17], held_back 0/1/2
+// (2: a stop node added, as find_tracks_handle_missed_layers does). Each
+// candidate starts from a node of its own (so its lineage can be traced);
+// its overlap memory is filled from its hit records under the overlap
+// chi2 cut, in record order, as FindCandidatesCloneEngine fills it. Out
+// per new slot: state, counters, parent slot, the hit and overlap hit it
+// added (-100000 / -1 for a held-back copy), the hit it takes the Kalman
+// update with (-1: not on the update list); per seed the best short
+// candidate.
+int ref_clone_seeds(int layer, int n_seeds, int max_cands, const int* n_cands, const float* par,
+                    const float* err, const int* chg, const float* chi2, const float* score,
+                    const int* nfound, const int* nmiss, const int* nover, const int* ninside,
+                    const int* ntail, const int* held_back, const int* n_rec, const int* rec_hit,
+                    const int* rec_module, const float* rec_chi2, const float* rec_score,
+                    const int* bshort_valid, const float* bshort_score, int* o_ncand,
+                    float* o_par, float* o_err, int* o_chg, float* o_chi2, float* o_score,
+                    int* o_nfound, int* o_nmiss, int* o_nover, int* o_ninside, int* o_ntail,
+                    int* o_parent, int* o_hit, int* o_ovl, int* o_upd, int* o_bvalid,
+                    float* o_bscore, int* o_bnfound, float* o_bchi2) {
+  ensure_cms2017();
+  if (n_seeds <= 0 || max_cands < 1 || max_cands > 8) return -1;
+  IterationParams params = Config::ItrInfo[g_iteration].m_params;
+  params.maxCandsPerSeed = max_cands;
+  const int S = n_seeds, SC = 8 * n_seeds;
+  EventOfCombCandidates eocc;
+  eocc.Reset(S, max_cands, 64);
+  eocc.m_size = S;
+  std::vector<std::vector<TrackCand>> extras(S);
+  std::vector<int> n_setup(S);
+  for (int s = 0; s < S; ++s) {
+    if (n_cands[s] < 1 || n_cands[s] > max_cands) return -2;
+    CombCandidate& cc = eocc[s];
+    cc.m_state = CombCandidate::Finding;
+    for (int c = 0; c < n_cands[s]; ++c) cc.AddHit(HitOnTrack{0, layer - 1}, 0.f, -1);
+    for (int c = 0; c < n_cands[s]; ++c) {
+      const int k = 8 * s + c;
+      cc.emplace_back(TrackCand(make_track(k, SC, par, err, chg), &cc));
+      TrackCand& t = cc.back();
+      t.setLastCcIndex(c);
+      t.setNFoundHits(nfound[k]);
+      t.setNMissingHits(nmiss[k]);
+      t.setNOverlapHits(nover[k]);
+      t.setNInsideMinusOneHits(ninside[k]);
+      t.setNTailMinusOneHits(ntail[k]);
+      t.setChi2(chi2[k]);
+      t.setScore(score[k]);
+      for (int j = 0; j < n_rec[k]; ++j) {
+        const int r = k * 17 + j;
+        if (rec_hit[r] >= 0 && rec_chi2[r] < params.chi2CutOverlap)
+          t.considerHitForOverlap(rec_hit[r], rec_module[r], rec_chi2[r]);
+      }
+    }
+    for (int c = 0; c < n_cands[s]; ++c) {
+      const int k = 8 * s + c;
+      if (held_back[k] == 0) continue;
+      extras[s].push_back(cc[c]);
+      if (held_back[k] == 2) extras[s].back().addHitIdx(-2, layer, 0.0f);
+    }
+    if (bshort_valid[s]) {
+      cc.m_best_short_cand = cc[0];
+      cc.m_best_short_cand.setScore(bshort_score[s]);
+    } else {
+      cc.m_best_short_cand.resetShortTrack();
+    }
+    n_setup[s] = (int)cc.m_hots.size();
+  }
+  std::vector<std::pair<int, int>> upd_list;
+  CandCloner cloner;
+  cloner.Setup(params);
+  cloner.begin_eta_bin(&eocc, &upd_list, &extras, 0, S);
+  cloner.begin_layer(layer);
+  for (int s = 0; s < S; ++s)
+    for (int c = 0; c < n_cands[s]; ++c) {
+      const int k = 8 * s + c;
+      for (int j = 0; j < n_rec[k]; ++j) {
+        const int r = k * 17 + j;
+        IdxChi2List h{};
+        h.trkIdx = c;
+        h.hitIdx = rec_hit[r];
+        h.module = (unsigned)rec_module[r];
+        h.chi2_hit = rec_chi2[r];
+        h.score = rec_score[r];
+        cloner.add_cand(s, h);
+      }
+    }
+  cloner.end_layer();
+  std::vector<int> upd_of(SC, -1);
+  for (const auto& u : upd_list) upd_of[8 * u.first + u.second] = 1;
+  for (int s = 0; s < S; ++s) {
+    const CombCandidate& cc = eocc[s];
+    o_ncand[s] = (int)cc.size();
+    for (int c = 0; c < 8; ++c) {
+      const int k = 8 * s + c;
+      o_parent[k] = -1;
+      o_hit[k] = -100000;
+      o_ovl[k] = -1;
+      o_upd[k] = -1;
+      if (c >= (int)cc.size()) continue;
+      const TrackCand& t = cc[c];
+      for (int e = 0; e < 6; ++e) o_par[e * SC + k] = t.parameters()[e];
+      for (int e = 0; e < 21; ++e) o_err[e * SC + k] = t.errors().Array()[e];
+      o_chg[k] = t.charge();
+      o_chi2[k] = t.chi2();
+      o_score[k] = t.score();
+      o_nfound[k] = t.nFoundHits();
+      o_nmiss[k] = t.nMissingHits();
+      o_nover[k] = t.nOverlapHits();
+      o_ninside[k] = t.nInsideMinusOneHits();
+      o_ntail[k] = t.nTailMinusOneHits();
+      // Nodes added by the clone step (above the setup nodes), last first.
+      int node = t.lastCcIndex(), added[2], n_added = 0;
+      while (node >= n_setup[s] && n_added < 2) {
+        added[n_added++] = node;
+        node = cc.m_hots[node].m_prev_idx;
+      }
+      if (node >= n_cands[s]) node = cc.m_hots[node].m_prev_idx;  // a setup stop node
+      o_parent[k] = node;
+      if (n_added == 2) {
+        o_hit[k] = cc.m_hots[added[1]].m_hot.index;
+        o_ovl[k] = cc.m_hots[added[0]].m_hot.index;
+      } else if (n_added == 1) {
+        o_hit[k] = cc.m_hots[added[0]].m_hot.index;
+      }
+      if (upd_of[k] > 0) o_upd[k] = cc.m_hots[t.lastCcIndex()].m_hot.index;
+    }
+    const TrackCand& b = cc.m_best_short_cand;
+    o_bvalid[s] = b.combCandidate() != nullptr;
+    o_bscore[s] = b.score();
+    o_bnfound[s] = b.nFoundHits();
+    o_bchi2[s] = b.chi2();
+  }
+  cloner.Release();
   return 0;
 }
 

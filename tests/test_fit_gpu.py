@@ -22,7 +22,8 @@ def gpu_fit(ctx, ev, pflags=2, with_chi2=False, grids=None):
     ctx.set_material(rl, xi)
     dev = FitBuffers.upload(ev)
     out = FitBuffers.outputs(ev.n)
-    ctx.fit_device(dev, out, pflags=pflags, with_chi2=with_chi2)
+    ctx.fit_device(dev, out, pflags=pflags, endcap_mask=getattr(ev, "endcap_mask", 0),
+                   with_chi2=with_chi2)
     ctx.synchronize()
     return {k: v.cpu().numpy() for k, v in out.items()}
 
@@ -60,6 +61,30 @@ def test_fit_matches_reference_20k(gpu_ctx, reflib, pflags):
                                   ev.xi_grid, pflags=pflags)
     assert_parity(out["par"], out["err"], par, err, f"20k pflags={pflags}")
     np.testing.assert_array_equal(out["chg"], chg)
+
+
+@pytest.mark.parametrize("pflags", [0, 2, 3])
+def test_steered_fit_matches_reference(gpu_ctx, reflib, restate, pflags):
+    """Steered fit (MkFitter::FitTracksSteered): two barrel steps, then
+    eight endcap steps (propagation to the hit's z and the endcap update)
+    selected by endcap_mask, against the reference's own steered fit on the
+    same tracks, and both against the FP64 restatement."""
+    ev = synth.gen_fit_event_steered(20000, seed=0x57EE)
+    out = gpu_fit(gpu_ctx, ev, pflags=pflags)
+    par, err, chg = reflib.fit_steered(ev.par, ev.err, ev.chg, ev.hit_pos, ev.hit_err,
+                                       ev.endcap_mask, ev.rl_grid, ev.xi_grid, pflags=pflags)
+    assert_parity(out["par"], out["err"], par, err, f"steered 20k pflags={pflags}")
+    np.testing.assert_array_equal(out["chg"], chg)
+    dpar, derr, _ = restate.fit(ev.par, ev.err, ev.chg, ev.hit_pos, ev.hit_err, ev.rl_grid,
+                                ev.xi_grid, pflags=pflags, endcap_mask=ev.endcap_mask)
+    g = cov_scaled_err(out["err"], derr)
+    r = cov_scaled_err(err, derr)
+    gp = par_scaled_err(out["par"], dpar, derr)
+    rp = par_scaled_err(par, dpar, derr)
+    print(f"  vs FP64: GPU par {summarize(gp)} cov {summarize(g)}; reference par "
+          f"{summarize(rp)} cov {summarize(r)}")
+    assert np.percentile(gp, 99.9) <= 1.5 * np.percentile(rp, 99.9) + 1e-7
+    assert np.percentile(g, 99.9) <= 1.5 * np.percentile(r, 99.9) + 1e-7
 
 
 def test_fit_error_vs_fp64(gpu_ctx, restate):

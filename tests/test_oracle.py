@@ -101,6 +101,27 @@ def test_restated_backward_fit_matches_reference(reflib, restate):
     assert np.median(dpar) < 1e-3
 
 
+def test_reference_steered_fit_matches_restatement(reflib, restate):
+    """The reference's steered fit (MkFitter::FitTracksSteered: barrel steps,
+    then endcap steps) agrees with the FP64 restatement given the same
+    endcap mask, within the reference's FP32 error."""
+    import numpy as np
+    from mkfit_b200 import synth
+    from tests.tolerances import PAR_RTOL, par_scaled_err
+    ev = synth.gen_fit_event_steered(2000, seed=21)
+    par, err, chg = reflib.fit_steered(ev.par, ev.err, ev.chg, ev.hit_pos, ev.hit_err,
+                                       ev.endcap_mask, ev.rl_grid, ev.xi_grid, pflags=2)
+    dpar, derr, _ = restate.fit(ev.par, ev.err, ev.chg, ev.hit_pos, ev.hit_err, ev.rl_grid,
+                                ev.xi_grid, pflags=2, endcap_mask=ev.endcap_mask)
+    ep = par_scaled_err(par, dpar, derr)
+    assert np.median(ep) < 1e-6
+    assert np.percentile(ep, 99.9) < PAR_RTOL
+    # Fitting the disks as barrel layers is far off: the mask matters.
+    bpar, _, _ = reflib.fit_steered(ev.par, ev.err, ev.chg, ev.hit_pos, ev.hit_err, 0,
+                                    ev.rl_grid, ev.xi_grid, pflags=2)
+    assert np.median(par_scaled_err(bpar, dpar, derr)) > 1e-3
+
+
 def test_restated_candidate_replay_matches_reference(reflib, restate):
     """The FP64 replay of clone-engine candidates (restate_replay_cands)
     reproduces the reference's own FP32 candidates: bulk at FP32 rounding,
