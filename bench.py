@@ -75,6 +75,8 @@ PU_NOISE = W.PU_NOISE
 # step; half of the PU200-like step).
 CPU_FIND_EVENTS = FIND_EVENTS
 CPU_PU_EVENTS = 8
+CPU_FIT_TRACKS = 320_000   # the whole fit step (16 x 20000)
+CPU_ADJ_TRACKS = 5_000
 
 
 def parse():
@@ -476,6 +478,10 @@ def run_ours(args):
         "iteration_stages": stages,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        if fit is not None:
+            fit["cpu_baseline"] = cpu_baseline_fit(fit_batch, min(CPU_FIT_TRACKS, fit_batch.n))
+        if adjoint is not None:
+            adjoint["cpu_baseline"] = cpu_baseline_adjoint(adj_ev, CPU_ADJ_TRACKS)
         line["cpu_baseline"] = cpu_baseline_find(events, gpu_best)
         if pu_events is not None:
             line["cpu_baseline"]["pu200"] = cpu_baseline_find(pu_events, pu_best,
@@ -502,6 +508,41 @@ def run_fit(ctx, stream, batch, args):
             "workload": f"toy-MC Kalman fit, {FIT_EVENTS} events x {FIT_TRACKS_PER_EVENT} tracks x "
                         f"{FIT_LAYERS} barrel layers, material on, one launch",
             "achieved_tflops": flops / (t * 1e-3) / 1e12}
+
+
+def cpu_baseline_fit(batch, n_sample):
+    """The reference's MkFitter fitting loop (runFittingTestPlex:
+    InputTracksForFit + FitTracksWithInterSlurp + OutputFittedTracks over
+    NN-track chunks, mkFit/fittestMPlex.cc:65-100) on all host threads,
+    best of 3, on the first n_sample tracks of the step."""
+    from oracle.oracle import RefLib
+    ref = RefLib()
+    threads = os.cpu_count()
+    ref.set_threads(threads)
+    sub = batch.tracks(0, n_sample)
+    _, _, _, secs = ref.fit(sub.par, sub.err, sub.chg, sub.hit_pos, sub.hit_err, sub.rl_grid,
+                            sub.xi_grid, pflags=2, repeat=3)
+    return {"value": n_sample / secs, "unit": "tracks/s", "cores": threads, "kind": "reference",
+            "sample": (f"{n_sample} of the step's {batch.n} tracks, reference MkFitter loop over "
+                       f"NN-track chunks on a {threads}-thread pool, AVX2 Matriplex (NN=8), "
+                       f"material on, best of 3")}
+
+
+def cpu_baseline_adjoint(ev, n_sample):
+    """The FP64 restatement of the forward fit + adjoint (the oracle's port:
+    the reference has no gradient) on one host thread, on the first
+    n_sample tracks."""
+    from oracle.oracle import adj_f64_grad
+    sub = ev.tracks(0, n_sample)
+    theta = np.zeros((sub.hit_pos.shape[0], 3))
+    theta[:, 2] = 1.0
+    t0 = time.perf_counter()
+    adj_f64_grad(sub.par, sub.err, sub.chg, sub.hit_pos, sub.hit_err, theta, sub.rl_grid,
+                 sub.xi_grid, material=True)
+    secs = time.perf_counter() - t0
+    return {"value": n_sample / secs, "unit": "tracks/s", "cores": 1, "kind": "port",
+            "sample": (f"{n_sample} of the step's {ev.n} tracks, FP64 forward fit + adjoint of "
+                       "the 30 layer parameters (oracle/adjoint_f64.cc), one thread, wall clock")}
 
 
 def adjoint_event(rank):
