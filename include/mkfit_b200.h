@@ -206,7 +206,8 @@ typedef struct {
 /* The finder takes a copy of the context's material map (mkfg_set_material)
  * here: a later mkfg_set_material on the same context (e.g. for a fit on
  * another detector) does not change what the finding propagates through;
- * call mkfg_finder_setup again to take the new map. */
+ * call mkfg_finder_setup again to take the new map. Events uploaded
+ * before a setup are dropped: upload again before the next run. */
 int mkfg_finder_setup(mkfg_context* ctx, const mkfg_find_config* cfg);
 
 /* ---- memoryFile event files (DataFile / Event::write_out / read_in,
@@ -693,6 +694,17 @@ int mkfg_find_work_detail(mkfg_context* ctx, int64_t* chi2_evals, int64_t* seeds
  * output still written; the reference's CcPool throws std::bad_alloc
  * instead (mkFit/HitStructures.h:428-435). */
 int mkfg_find_set_arena_capacity(mkfg_context* ctx, int32_t nodes_per_seed);
+
+/* Where the following uploads import the seeds (MkBuilder::import_seeds
+ * with the CMS-2017 partition, mkFit/MkBuilder.cc:214-275, and
+ * CombCandidate::ImportSeed): on_host = 0 (the default) on the device --
+ * region, eta order and initial candidates computed there, so the host
+ * only copies the seeds as given -- or 1 on the host's worker threads.
+ * Both give the same candidates. The upload uses the host whatever the
+ * setting for iterations that sort seed hits first (pixelLessStep), for an
+ * event of more than 16384 seeds, and for a seed whose last hit is not
+ * one of its event's hits. */
+int mkfg_find_set_seed_import(mkfg_context* ctx, int32_t on_host);
 
 /* Clone-step counters of the last mkfg_find_work call: the records
  * (IdxChi2List entries, hits and holes) present when the seeds were ranked

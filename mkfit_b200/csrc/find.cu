@@ -20,6 +20,7 @@
 #include "find_fused.cuh"
 #include "layer_hits.cuh"
 #include "find_steps.cuh"
+#include "seed_import.cuh"
 #include "quality.cuh"
 
 #include <algorithm>
@@ -1056,7 +1057,10 @@ struct Finder {
   int n_seeds = 0;
   int n_events = 0;
   int events_loaded = 0;
-  cudaGraphExec_t graph = nullptr;  // captured run sequence of the current upload
+  cudaGraphExec_t graph = nullptr;  // captured run sequence
+  // The device view the graph was captured with: an upload that leaves it
+  // unchanged (same seed count, same buffers) replays the same graph.
+  EventDev graph_ev{};
   int fused_w = 16;                 // seeds per block of the fused form
   int max_nq = 1;                   // largest number of q bins of a layer
   // Layer steps a backward search can take (the longest plan less its
@@ -1083,6 +1087,10 @@ struct Finder {
   float* d_mat = nullptr;  // material map (radiation lengths, then xi) taken at setup
   DevBuf sel;  // output selection scratch
   DevBuf wrk;  // staging of the per-layer worker calls
+  DevBuf seed_raw;  // the batch's seeds as given, for the device seed import
+  // Seed import on the host (partition, sort and initial candidates by the
+  // upload's worker threads) instead of on the device.
+  bool seed_import_host = false;
   // Global index of every uploaded event's layer starts ([n_events][L + 1]),
   // for checking the hit indices the worker calls are given.
   std::vector<int> h_lb;
@@ -1131,6 +1139,7 @@ void finder_release(mkfg_context* ctx) {
   f->bk.release();
   f->sel.release();
   f->wrk.release();
+  f->seed_raw.release();
   f->hits_h.release();
   f->outb_h.release();
   f->seeds_h.release();
@@ -1247,6 +1256,10 @@ extern "C" int mkfg_finder_setup(mkfg_context* ctx, const mkfg_find_config* cfg)
   MKFG_CUDA_TRY(cudaMemcpyAsync(f->d_cfg, &H, sizeof(H), cudaMemcpyHostToDevice, ctx->stream));
   MKFG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   f->configured = true;
+  // Buffers, launch sequence and graph follow the configuration: the next
+  // run needs a new upload.
+  f->drop_graph();
+  f->events_loaded = 0;
   return MKFG_OK;
 }
 
@@ -1369,10 +1382,51 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     int* hot_size;
     int* seed_hot;  // [SS][MKFG_MAX_SEED_HITS]
   };
-  if ((rc = f->seeds_h.ensure(rounded(4 * (size_t)SS) * (27 + 14 + MKFG_MAX_SEED_HITS) + 4096)))
+  // The device imports the seeds (seed_import.cuh) unless the iteration
+  // sorts seed hits on the host first, an event holds more seeds than the
+  // device sort takes, or the host path was asked for.
+  // The device reads each seed's last hit (its eta sets the order): a seed
+  // whose last hit is not one of the event's hits keeps the upload on the
+  // host path, which handles it as before.
+  bool dev_import = !f->seed_import_host && !f->sort_seed_hits && S > 0;
+  for (int e = 0; e < n_ev && dev_import; ++e) {
+    const mkfg_event* ev = evs + e;
+    dev_import &= ev->n_seeds <= kSeedSortMax;
+    const int sw = seed_hit_stride(ev);
+    for (int k = 0; k < ev->n_seeds && dev_import; ++k) {
+      const int last = ev->seed_nhits[k] - 1;
+      const int hl = ev->seed_hit_layer[(size_t)k * sw + last], hi = ev->seed_hit_index[(size_t)k * sw + last];
+      dev_import &= hl >= 0 && hl < L && hi >= 0 && hi < ev->layer_begin[hl + 1] - ev->layer_begin[hl];
+    }
+  }
+  if ((rc = f->seeds_h.ensure(rounded(4 * (size_t)SS) * (27 + 14 + 2 * MKFG_MAX_SEED_HITS) +
+                              rounded(4 * (size_t)(n_ev + 1)) + 4096)))
     return rc;
+  // Raw seeds for the device import, in the same pinned buffer.
+  struct RawStage {
+    float* par;   // [6][SS]
+    float* err;   // [21][SS]
+    int* chg;
+    int* nhits;
+    int* hl;      // [SS][MKFG_MAX_SEED_HITS]
+    int* hi;
+    int* seed_off;
+  } rs{};
+  size_t raw_bytes = 0;
+  if (dev_import) {
+    char* p = static_cast<char*>(f->seeds_h.ptr);
+    rs.par = carve<float>(p, 6 * (size_t)SS);
+    rs.err = carve<float>(p, 21 * (size_t)SS);
+    rs.chg = carve<int>(p, SS);
+    rs.nhits = carve<int>(p, SS);
+    rs.hl = carve<int>(p, MKFG_MAX_SEED_HITS * (size_t)SS);
+    rs.hi = carve<int>(p, MKFG_MAX_SEED_HITS * (size_t)SS);
+    rs.seed_off = carve<int>(p, n_ev + 1);
+    raw_bytes = (size_t)(p - static_cast<char*>(f->seeds_h.ptr));
+    for (int e = 0; e <= n_ev; ++e) rs.seed_off[e] = seed_off[e];
+  }
   SeedStage ss;
-  {
+  if (!dev_import) {
     char* p = static_cast<char*>(f->seeds_h.ptr);
     ss.par = carve<float>(p, 6 * (size_t)SS);
     ss.err = carve<float>(p, 21 * (size_t)SS);
@@ -1408,8 +1462,11 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
         seed_hl = sorted_hl.data();
         seed_hi = sorted_hi.data();
       }
-      SeedInput si{ev->n_seeds, ev->seed_par, ev->seed_chg, ev->seed_nhits, seed_hl, seed_hi, sw};
-      partition_seeds_cms2017(f->layer_desc.data(), L, si, ev->layer_begin, ev->pos, nh, orders[e]);
+      if (!dev_import) {
+        SeedInput si{ev->n_seeds, ev->seed_par, ev->seed_chg, ev->seed_nhits, seed_hl, seed_hi, sw};
+        partition_seeds_cms2017(f->layer_desc.data(), L, si, ev->layer_begin, ev->pos, nh,
+                                orders[e]);
+      }
       for (int r = 0; r < 3; ++r)
         std::memcpy(hh.pos + (size_t)r * NHs + o, ev->pos + (size_t)r * nh, 4 * (size_t)nh);
       for (int r = 0; r < 6; ++r)
@@ -1424,6 +1481,24 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
       }
       for (int l = 0; l <= L; ++l) hh.lb[(size_t)e * (L + 1) + l] = o + ev->layer_begin[l];
       const int n = ev->n_seeds;
+      if (dev_import) {
+        // The seeds as given; partition, order and initial candidates are
+        // made on the device.
+        const size_t so = seed_off[e];
+        for (int c = 0; c < 6; ++c)
+          std::memcpy(rs.par + c * (size_t)SS + so, ev->seed_par + (size_t)c * n, 4 * (size_t)n);
+        for (int c = 0; c < 21; ++c)
+          std::memcpy(rs.err + c * (size_t)SS + so, ev->seed_err + (size_t)c * n, 4 * (size_t)n);
+        std::memcpy(rs.chg + so, ev->seed_chg, 4 * (size_t)n);
+        std::memcpy(rs.nhits + so, ev->seed_nhits, 4 * (size_t)n);
+        for (int k = 0; k < n; ++k)
+          for (int h = 0; h < MKFG_MAX_SEED_HITS; ++h) {
+            const bool in = h < sw;
+            rs.hl[(so + k) * MKFG_MAX_SEED_HITS + h] = in ? seed_hl[(size_t)k * sw + h] : 0;
+            rs.hi[(so + k) * MKFG_MAX_SEED_HITS + h] = in ? seed_hi[(size_t)k * sw + h] : 0;
+          }
+        return;
+      }
       for (int k = 0; k < n; ++k) {
         const int s = seed_off[e] + k;
         const int i = orders[e].order[k];
@@ -1483,8 +1558,8 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
         ss.score[s] = bonus * nf + 0.0f * 0 - penalty * nin - 3.0f * 0 - 0.0f;
       }
     };
-    // The calling thread issues each event's hit copies as soon as the
-    // event's worker is done, so the transfers overlap the host copies.
+    // The calling thread issues the hit copies as the events' workers
+    // finish, so the transfers overlap the host copies.
     cudaStream_t st = ctx->stream;
     std::vector<std::atomic<int>> ready(n_ev);
     for (auto& r : ready) r.store(0);
@@ -1507,14 +1582,24 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
         ce = cudaMemcpyAsync(dbase + (h - hbase), h, bytes, cudaMemcpyHostToDevice, st);
       }
     };
-    for (int e = 0; e < n_ev; ++e) {
-      while (!ready[e].load(std::memory_order_acquire)) std::this_thread::yield();
-      const size_t o = 4 * (size_t)hit_off[e], nb = 4 * (size_t)(hit_off[e + 1] - hit_off[e]);
+    // Events' hits are consecutive in every row of the mirror: each run of
+    // events that became ready goes in one copy per row (at least
+    // kCopyEvents events a time but the last), so few large transfers
+    // follow the workers.
+    constexpr int kCopyEvents = 8;
+    for (int e0 = 0; e0 < n_ev;) {
+      int e1 = e0;
+      while (e1 < n_ev && (e1 - e0 < kCopyEvents || ready[e1].load(std::memory_order_acquire))) {
+        while (!ready[e1].load(std::memory_order_acquire)) std::this_thread::yield();
+        ++e1;
+      }
+      const size_t o = 4 * (size_t)hit_off[e0], nb = 4 * (size_t)(hit_off[e1] - hit_off[e0]);
       copy_rows(hh.pos, 4 * (size_t)NHs, 3, o, nb);
       copy_rows(hh.err, 4 * (size_t)NHs, 6, o, nb);
       copy_rows(hh.detid, 0, 1, o, nb);
       copy_rows(hh.cpcm, 0, 1, o, nb);
       if (any_mask) copy_rows(hh.mask, 0, 1, o / 4, nb / 4);
+      e0 = e1;
     }
     for (auto& th : pool) th.join();
     copy_rows(hh.lb, 0, 1, 0, 4 * n_lb);
@@ -1644,10 +1729,52 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   }
   f->ev.n_seeds = S;
 
-  f->drop_graph();
   // The initial candidates from the pinned staging (the per-run reset sets
   // the candidate counts, seed states and buffers from them).
   CandSoA& B0 = f->ev.init;
+  std::vector<int> h_nfound;
+  if ((rc = f->seeds.ensure(rounded(4 * MKFG_MAX_SEED_HITS * (size_t)SS)))) return rc;
+  if (dev_import) {
+    if ((rc = f->seed_raw.ensure(raw_bytes + 4 * rounded(4 * (size_t)SS) + 4096))) return rc;
+    char* draw = f->seed_raw.as<char>();
+    MKFG_CUDA_TRY(cudaMemcpyAsync(draw, f->seeds_h.ptr, raw_bytes, cudaMemcpyHostToDevice, st));
+    auto dev = [&](const void* h) {
+      return draw + (static_cast<const char*>(h) - static_cast<const char*>(f->seeds_h.ptr));
+    };
+    RawSeeds R;
+    R.par = reinterpret_cast<const float*>(dev(rs.par));
+    R.err = reinterpret_cast<const float*>(dev(rs.err));
+    R.chg = reinterpret_cast<const int*>(dev(rs.chg));
+    R.nhits = reinterpret_cast<const int*>(dev(rs.nhits));
+    R.hit_layer = reinterpret_cast<const int*>(dev(rs.hl));
+    R.hit_index = reinterpret_cast<const int*>(dev(rs.hi));
+    R.seed_off = reinterpret_cast<const int*>(dev(rs.seed_off));
+    R.n_events = n_ev;
+    R.n = S;
+    char* q = draw + raw_bytes;
+    int* d_region = carve<int>(q, SS);
+    float* d_key = carve<float>(q, SS);
+    int* d_event = carve<int>(q, SS);
+    int* d_order = carve<int>(q, SS);
+    const RegionCuts cuts = region_cuts_cms2017(f->layer_desc.data());
+    k_seed_keys<<<(S + 127) / 128, 128, 0, st>>>(R, f->ev, cuts, d_region, d_key, d_event);
+    MKFG_CUDA_TRY(cudaGetLastError());
+    const int smem = 8 * kSeedSortMax;
+    MKFG_CUDA_TRY(cudaFuncSetAttribute(k_seed_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    k_seed_sort<<<n_ev, kSeedSortBlock, smem, st>>>(R, d_key, d_order);
+    MKFG_CUDA_TRY(cudaGetLastError());
+    k_seed_import<<<(S + 127) / 128, 128, 0, st>>>(R, d_order, d_region, d_event, f->ev,
+                                                   f->seeds.as<int>());
+    MKFG_CUDA_TRY(cudaGetLastError());
+    // The host keeps the regions (backward-fit seed groups) and the seeds
+    // the post-cleaning dropped.
+    f->h_region.resize(S);
+    h_nfound.resize(S);
+    MKFG_CUDA_TRY(cudaMemcpyAsync(f->h_region.data(), f->ev.region, 4 * (size_t)S,
+                                  cudaMemcpyDeviceToHost, st));
+    MKFG_CUDA_TRY(cudaMemcpyAsync(h_nfound.data(), B0.nfound, 4 * (size_t)S, cudaMemcpyDeviceToHost,
+                                  st));
+  } else {
   if ((rc = up(B0.par, ss.par, 4 * 6 * (size_t)SS))) return rc;
   if ((rc = up(B0.err, ss.err, 4 * 21 * (size_t)SS))) return rc;
   if ((rc = up(B0.chg, ss.chg, 4 * (size_t)SS))) return rc;
@@ -1664,8 +1791,8 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   if ((rc = up(f->ev.region, ss.region, 4 * (size_t)SS))) return rc;
   if ((rc = up(f->ev.pickup_layer, ss.pickup, 4 * (size_t)SS))) return rc;
   if ((rc = up(f->ev.init_hot, ss.hot_size, 4 * (size_t)SS))) return rc;
-  if ((rc = f->seeds.ensure(rounded(4 * MKFG_MAX_SEED_HITS * (size_t)SS)))) return rc;
   if ((rc = up(f->seeds.ptr, ss.seed_hot, 4 * MKFG_MAX_SEED_HITS * (size_t)SS))) return rc;
+  }
   if (S > 0) k_seed_nodes<<<(S + 127) / 128, 128, 0, st>>>(f->ev, f->seeds.as<int>());
   MKFG_CUDA_TRY(cudaGetLastError());
   MKFG_CUDA_TRY(cudaMemsetAsync(f->ev.upd, 0, 4 * (size_t)SC, st));
@@ -1674,7 +1801,12 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   MKFG_CUDA_TRY(cudaStreamSynchronize(st));
   f->n_seeds = S;
   f->n_events = n_ev;
-  f->h_region.assign(ss.region, ss.region + S);
+  if (dev_import) {
+    for (int e = 0; e < n_ev; ++e)
+      for (int k = seed_off[e]; k < seed_off[e + 1]; ++k) n_silly[e] += h_nfound[k] < 0;
+  } else {
+    f->h_region.assign(ss.region, ss.region + S);
+  }
   f->h_seed_off = seed_off;
   f->h_hit_off = hit_off;
   f->h_lb.assign(hh.lb, hh.lb + n_lb);
@@ -1837,7 +1969,11 @@ static int run_plain(mkfg_context* ctx, Finder* f) {
 static int run_graph(mkfg_context* ctx, Finder* f) {
   if (f->n_seeds == 0) return MKFG_OK;
   cudaStream_t st = ctx->stream;
+  // The launches take the device view by value: a graph captured with
+  // another one is stale.
+  if (f->graph && std::memcmp(&f->graph_ev, &f->ev, sizeof(EventDev)) != 0) f->drop_graph();
   if (!f->graph) {
+    f->graph_ev = f->ev;
     cudaGraph_t g = nullptr;
     step_grids(f);  // occupancy queries before the capture
     MKFG_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
@@ -2858,6 +2994,14 @@ extern "C" int mkfg_find_set_arena_capacity(mkfg_context* ctx, int32_t nodes_per
                "arena capacity %d: 0 (automatic) or at least %d nodes per seed", nodes_per_seed,
                MKFG_MAX_SEED_HITS + 2);
   finder_of(ctx)->arena_cap = nodes_per_seed;
+  return MKFG_OK;
+}
+
+extern "C" int mkfg_find_set_seed_import(mkfg_context* ctx, int32_t on_host) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  MKFG_REQUIRE(on_host == 0 || on_host == 1, "on_host must be 0 or 1, got %d", on_host);
+  finder_of(ctx)->seed_import_host = on_host != 0;
   return MKFG_OK;
 }
 

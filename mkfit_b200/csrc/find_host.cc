@@ -114,10 +114,20 @@ namespace {
 struct SeedTrack {
   float x, y, z, ipt, phi, theta;
   int chg;
-  float pT() const { return std::abs(1.f / ipt); }
-  float px() const { return pT() * std::cos(phi); }
-  float py() const { return pT() * std::sin(phi); }
-  float pz() const { return pT() / std::tan(theta); }
+  // The momentum, as TrackBase computes it on every call (Track.h), taken
+  // once per seed: the same float operations on the same inputs.
+  float pt_, px_, py_, pz_;
+  SeedTrack(float x_, float y_, float z_, float ipt_, float phi_, float theta_, int chg_)
+      : x(x_), y(y_), z(z_), ipt(ipt_), phi(phi_), theta(theta_), chg(chg_) {
+    pt_ = std::abs(1.f / ipt);
+    px_ = pt_ * std::cos(phi);
+    py_ = pt_ * std::sin(phi);
+    pz_ = pt_ / std::tan(theta);
+  }
+  float pT() const { return pt_; }
+  float px() const { return px_; }
+  float py() const { return py_; }
+  float pz() const { return pz_; }
 
   float maxReachRadius() const {
     const float k = ((chg < 0) ? 100.0f : -100.0f) / (kSolf * kBfieldf);
@@ -154,22 +164,42 @@ struct SeedTrack {
 
 }  // namespace
 
+RegionCuts region_cuts_cms2017(const float* L) {
+  auto col = [&](int l, int c) { return L[l * LC_COUNT + c]; };
+  RegionCuts r;
+  r.tib1_rin = col(4, LC_RIN);
+  r.tib1_zmax = col(4, LC_ZMAX);
+  r.tib1_zmin = col(4, LC_ZMIN);
+  r.tob1_rin = col(10, LC_RIN);
+  r.tob1_zmax = col(10, LC_ZMAX);
+  r.tob1_zmin = col(10, LC_ZMIN);
+  r.tidp1_zmin = col(21, LC_ZMIN);
+  r.tidn1_zmax = col(48, LC_ZMAX);
+  r.tecp1_zmin = col(27, LC_ZMIN);
+  r.tecn1_zmax = col(54, LC_ZMAX);
+  r.tidp_rin = std::min(col(21, LC_RIN), col(22, LC_RIN));
+  r.tidp_rout = std::max(col(21, LC_ROUT), col(22, LC_ROUT));
+  r.tecp_rin = std::min(col(27, LC_RIN), col(28, LC_RIN));
+  r.tecp_rout = std::max(col(27, LC_ROUT), col(28, LC_ROUT));
+  r.tidn_rin = std::min(col(48, LC_RIN), col(49, LC_RIN));
+  r.tidn_rout = std::max(col(48, LC_ROUT), col(49, LC_ROUT));
+  r.tecn_rin = std::min(col(54, LC_RIN), col(55, LC_RIN));
+  r.tecn_rout = std::max(col(54, LC_ROUT), col(55, LC_ROUT));
+  return r;
+}
+
 void partition_seeds_cms2017(const float* L, int n_layers, const SeedInput& s,
                              const int32_t* layer_begin, const float* hit_pos, int hit_stride,
                              SeedOrder& out) {
-  auto col = [&](int l, int c) { return L[l * LC_COUNT + c]; };
-  const float tib1_rin = col(4, LC_RIN), tib1_zmax = col(4, LC_ZMAX), tib1_zmin = col(4, LC_ZMIN);
-  const float tob1_rin = col(10, LC_RIN), tob1_zmax = col(10, LC_ZMAX), tob1_zmin = col(10, LC_ZMIN);
-  const float tidp1_zmin = col(21, LC_ZMIN), tidn1_zmax = col(48, LC_ZMAX);
-  const float tecp1_zmin = col(27, LC_ZMIN), tecn1_zmax = col(54, LC_ZMAX);
-  const float tidp_rin = std::min(col(21, LC_RIN), col(22, LC_RIN));
-  const float tidp_rout = std::max(col(21, LC_ROUT), col(22, LC_ROUT));
-  const float tecp_rin = std::min(col(27, LC_RIN), col(28, LC_RIN));
-  const float tecp_rout = std::max(col(27, LC_ROUT), col(28, LC_ROUT));
-  const float tidn_rin = std::min(col(48, LC_RIN), col(49, LC_RIN));
-  const float tidn_rout = std::max(col(48, LC_ROUT), col(49, LC_ROUT));
-  const float tecn_rin = std::min(col(54, LC_RIN), col(55, LC_RIN));
-  const float tecn_rout = std::max(col(54, LC_ROUT), col(55, LC_ROUT));
+  const RegionCuts r = region_cuts_cms2017(L);
+  const float tib1_rin = r.tib1_rin, tib1_zmax = r.tib1_zmax, tib1_zmin = r.tib1_zmin;
+  const float tob1_rin = r.tob1_rin, tob1_zmax = r.tob1_zmax, tob1_zmin = r.tob1_zmin;
+  const float tidp1_zmin = r.tidp1_zmin, tidn1_zmax = r.tidn1_zmax;
+  const float tecp1_zmin = r.tecp1_zmin, tecn1_zmax = r.tecn1_zmax;
+  const float tidp_rin = r.tidp_rin, tidp_rout = r.tidp_rout;
+  const float tecp_rin = r.tecp_rin, tecp_rout = r.tecp_rout;
+  const float tidn_rin = r.tidn_rin, tidn_rout = r.tidn_rout;
+  const float tecn_rin = r.tecn_rin, tecn_rout = r.tecn_rout;
   (void)n_layers;
 
   auto barrel_pos = [](const SeedTrack& S, float maxR, float rin, float zmax) {
@@ -189,8 +219,8 @@ void partition_seeds_cms2017(const float* L, int n_layers, const SeedInput& s,
   std::vector<float> score(n);
   out.region.assign(n, 2);
   for (int i = 0; i < n; ++i) {
-    SeedTrack S{s.par[0 * n + i], s.par[1 * n + i], s.par[2 * n + i],
-                s.par[3 * n + i], s.par[4 * n + i], s.par[5 * n + i], s.chg[i]};
+    const SeedTrack S(s.par[0 * n + i], s.par[1 * n + i], s.par[2 * n + i], s.par[3 * n + i],
+                      s.par[4 * n + i], s.par[5 * n + i], s.chg[i]);
     // Eta of the seed's last hit (Hit::eta, Hit.h:82-87).
     const int last = s.nhits[i] - 1;
     const int hl = s.hit_layer[i * s.stride + last], hi = s.hit_index[i * s.stride + last];
@@ -202,25 +232,28 @@ void partition_seeds_cms2017(const float* L, int n_layers, const SeedInput& s,
     int reg;
     const bool z_dir_pos = S.pz() > 0;
     const float maxR = S.maxReachRadius();
+    // The tests are pure, so each pair is evaluated with a short circuit:
+    // the second only when the first fails (same regions, fewer helix
+    // steps).
     if (z_dir_pos) {
-      const bool in_tib = barrel_pos(S, maxR, tib1_rin, tib1_zmax);
-      const bool in_tob = barrel_pos(S, maxR, tob1_rin, tob1_zmax);
-      if (!in_tib && !in_tob) {
+      const bool in_barrel = barrel_pos(S, maxR, tib1_rin, tib1_zmax) ||
+                             barrel_pos(S, maxR, tob1_rin, tob1_zmax);
+      if (!in_barrel) {
         reg = 4;  // Reg_Endcap_Pos
       } else {
-        const bool in_tid = endcap_pos(S, maxR, tidp_rout, tidp_rin, tidp1_zmin);
-        const bool in_tec = endcap_pos(S, maxR, tecp_rout, tecp_rin, tecp1_zmin);
-        reg = (!in_tid && !in_tec) ? 2 : 3;  // Barrel : Transition_Pos
+        const bool in_endcap = endcap_pos(S, maxR, tidp_rout, tidp_rin, tidp1_zmin) ||
+                               endcap_pos(S, maxR, tecp_rout, tecp_rin, tecp1_zmin);
+        reg = in_endcap ? 3 : 2;  // Transition_Pos : Barrel
       }
     } else {
-      const bool in_tib = barrel_neg(S, maxR, tib1_rin, tib1_zmin);
-      const bool in_tob = barrel_neg(S, maxR, tob1_rin, tob1_zmin);
-      if (!in_tib && !in_tob) {
+      const bool in_barrel = barrel_neg(S, maxR, tib1_rin, tib1_zmin) ||
+                             barrel_neg(S, maxR, tob1_rin, tob1_zmin);
+      if (!in_barrel) {
         reg = 0;  // Reg_Endcap_Neg
       } else {
-        const bool in_tid = endcap_neg(S, maxR, tidn_rout, tidn_rin, tidn1_zmax);
-        const bool in_tec = endcap_neg(S, maxR, tecn_rout, tecn_rin, tecn1_zmax);
-        reg = (!in_tid && !in_tec) ? 2 : 1;  // Barrel : Transition_Neg
+        const bool in_endcap = endcap_neg(S, maxR, tidn_rout, tidn_rin, tidn1_zmax) ||
+                               endcap_neg(S, maxR, tecn_rout, tecn_rin, tecn1_zmax);
+        reg = in_endcap ? 1 : 2;  // Transition_Neg : Barrel
       }
     }
     out.region[i] = reg;

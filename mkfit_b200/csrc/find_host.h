@@ -70,6 +70,16 @@ struct SeedInput {
   int stride;
 };
 
+// The layer limits partitionSeeds1 tests seeds against (Geoms/CMS-2017.cc:
+// 440-470): first TIB and TOB layers, first TID and TEC disks each side,
+// and the radial extent of the first two disks of each.
+struct RegionCuts {
+  float tib1_rin, tib1_zmax, tib1_zmin, tob1_rin, tob1_zmax, tob1_zmin;
+  float tidp1_zmin, tidn1_zmax, tecp1_zmin, tecn1_zmax;
+  float tidp_rin, tidp_rout, tecp_rin, tecp_rout, tidn_rin, tidn_rout, tecn_rin, tecn_rout;
+};
+RegionCuts region_cuts_cms2017(const float* layer_desc);
+
 void partition_seeds_cms2017(const float* layer_desc, int n_layers, const SeedInput& s,
                              const int32_t* layer_begin, const float* hit_pos, int hit_stride,
                              SeedOrder& out);

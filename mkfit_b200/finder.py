@@ -206,6 +206,7 @@ def _bind(lib):
     lib.mkfg_find_work_detail.argtypes = [vp, i64p, i64p]
     lib.mkfg_find_work_clone.argtypes = [vp, i64p, i64p]
     lib.mkfg_find_set_arena_capacity.argtypes = [vp, ctypes.c_int32]
+    lib.mkfg_find_set_seed_import.argtypes = [vp, ctypes.c_int32]
     lib.mkfg_find_download.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(MkfgFindOut)]
     lib.mkfg_find_download_best.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(MkfgFindOut)]
     lib.mkfg_find_event.argtypes = [vp, ctypes.POINTER(MkfgEvent), ctypes.POINTER(MkfgFindOut)]
@@ -525,6 +526,11 @@ class Finder:
         capi.check(self.lib.mkfg_find_clone_seeds(self.ctx.handle, int(layer), ctypes.byref(ci),
                                                   ctypes.byref(co)))
         return o
+
+    def set_seed_import(self, on_host):
+        """Seed import of the following uploads on the host (True) or on the
+        device (False, the default); see mkfg_find_set_seed_import."""
+        capi.check(self.lib.mkfg_find_set_seed_import(self.ctx.handle, int(bool(on_host))))
 
     def hit_index(self, event, n_bins, n_hits):
         """The device-built hit index of uploaded event `event`:

@@ -923,3 +923,39 @@ def test_clone_worker_matches_reference(gpu_ctx, reflib):
     print(f"\n{len(inp['n_cands'])} seeds -> {len(live)} candidates: {n_ovl} with an overlap hit, "
           f"{n_held} held-back copies, {int(moved.sum())} new best short candidates")
     assert n_ovl > 50 and n_held > 50 and moved.sum() > 50
+
+
+def test_device_seed_import_equals_host(gpu_ctx):
+    """The device seed import (region, eta order and initial candidates made
+    on the device) and the host one (the upload's worker threads) give the
+    same candidates, bit for bit: eight events of the batched-finding
+    workload, a 5000-track event, events of iterations 1-6 and a batch with
+    a seedless event."""
+    from mkfit_b200 import workloads
+    batches = [[synth.gen_cms_event(**a) for a in workloads.find_event_args(8, 0)],
+               [synth.gen_cms_event(5000, seed=191, noise_frac=0.1)],
+               [synth.gen_cms_event(300, seed=192, noise_frac=0.02),
+                synth.CmsEvent(**dict(synth.gen_cms_event(50, seed=193, noise_frac=0.0).__dict__,
+                                      seed_par=np.zeros((6, 0), np.float32),
+                                      seed_err=np.zeros((21, 0), np.float32),
+                                      seed_chg=np.zeros(0, np.int32),
+                                      seed_nhits=np.zeros(0, np.int32),
+                                      seed_hit_layer=np.zeros((0, 4), np.int32),
+                                      seed_hit_index=np.zeros((0, 4), np.int32),
+                                      seed_mc=np.zeros(0, np.int32)))]]
+    cfgs = [FindConfig(max_cands=M, chi2_cut=30.0, zero_c2=True)] * 3
+    for it in range(1, 7):
+        batches.append([iteration_event(it, 600, 200 + it)])
+        cfgs.append(FindConfig(iteration=it, max_cands=None, chi2_cut=None, zero_c2=False))
+    for events, cfg in zip(batches, cfgs):
+        fnd = Finder(gpu_ctx, cfg)
+        got = {}
+        for on_host in (True, False):
+            fnd.set_seed_import(on_host)
+            total = fnd.upload_batch(events)
+            fnd.run_graph()
+            got[on_host] = fnd.download(total)
+        fnd.set_seed_import(False)
+        for k in got[True]:
+            np.testing.assert_array_equal(got[False][k], got[True][k], err_msg=k)
+        assert total == sum(e.n_seeds for e in events)
