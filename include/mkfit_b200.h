@@ -706,6 +706,16 @@ int mkfg_find_set_arena_capacity(mkfg_context* ctx, int32_t nodes_per_seed);
  * one of its event's hits. */
 int mkfg_find_set_seed_import(mkfg_context* ctx, int32_t on_host);
 
+/* on = 1: the propagation kernel of the following runs copies, per chunk
+ * of 256 active candidates, the (q bin, phi bin) table of the chunk's
+ * first (event, layer) into shared memory with one bulk copy (TMA,
+ * cp.async.bulk + mbarrier) and scans it there; 0 (the default): every
+ * candidate reads the table from global memory. Same results either way
+ * (LayerOfHits::m_phi_bin_infos, mkFit/HitStructures.h:152-159; the bin
+ * loop of MkFinder::SelectHitIndices, mkFit/MkFinder.cc:464-466). No
+ * reference counterpart. */
+int mkfg_find_set_bin_staging(mkfg_context* ctx, int32_t on);
+
 /* Clone-step counters of the last mkfg_find_work call: the records
  * (IdxChi2List entries, hits and holes) present when the seeds were ranked
  * and the new candidates written. Counted by the eager run (mkfg_find_run)

@@ -230,17 +230,107 @@ __global__ void __launch_bounds__(kBlock, MKFG_ACT_MIN_BLOCKS) k_activate(EventD
 // and hole record for the active candidates (compact list; barrel and
 // endcap candidates in separate runs of the list).
 //------------------------------------------------------------------------------
+// Bulk copy global -> shared memory completing on an mbarrier (TMA,
+// cp.async.bulk; no cluster multicast).
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_to_shared(void* dst, const void* src, unsigned bytes,
+                                               uint64_t* bar) {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+// Waits for the barrier's phase `parity` to complete, at most kMaxPolls
+// polls; false when it did not.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+  constexpr int kMaxPolls = 1 << 22;
+  for (int i = 0; i < kMaxPolls; ++i) {
+    unsigned done;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// kStageBins: each chunk of the active list first copies the bin table of
+// its first candidate's (event, layer) into shared memory (one bulk copy
+// of nq x 256 words, at most `stage_words`); the chunk's candidates on
+// that (event, layer) scan the copy, the others the global table. The
+// active list holds a seed's candidates together and the seeds of an
+// event and region consecutively, so a chunk seldom spans two tables.
+template <bool kStageBins>
 __global__ void __launch_bounds__(kBlock, MKFG_PROP_MIN_BLOCKS) k_propagate(EventDev E, const FindConfigDev* __restrict__ Cp,
-                                                      int step) {
+                                                      int step, int stage_words) {
   const FindConfigDev& C = *Cp;
   int* cnt = E.step_count + step * kCntN;
   const int nb = cnt[kCntActBarrel], ne = cnt[kCntActEndcap];
   const int stride = E.cand[0].cap;
   if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&E.work[step * kWorkN + 0], nb + ne);
   __shared__ BlockAppend sh;
+  extern __shared__ __align__(128) uint32_t s_bins[];
+  __shared__ __align__(8) uint64_t s_bar;
+  __shared__ int s_key;       // (event, layer) staged for this chunk, -1 none
+  __shared__ int s_pending;   // a copy may still be in flight (a wait gave up)
+  unsigned parity = 0;
+  if (kStageBins) {
+    if (threadIdx.x == 0) {
+      mbar_init(&s_bar);
+      s_pending = 0;
+    }
+    __syncthreads();
+  }
   // Block-uniform loop: the pair-list reservation synchronises the block.
   for (int j0 = blockIdx.x * kBlock; j0 < nb + ne; j0 += gridDim.x * kBlock) {
     const int j = j0 + threadIdx.x;
+    if (kStageBins) {
+      __syncthreads();  // the previous chunk's scans are done with the copy
+      if (threadIdx.x == 0) {
+        int key = -1;
+        if (!s_pending) {
+          const int sl = j0 < nb ? E.act_list[j0] : E.act_list[E.list_cap - 1 - (j0 - nb)];
+          const int ss = sl / kSlots;
+          const int lay = plan_layer(C, E.region[ss], step);
+          const LayerDev& SL = C.layer[lay];
+          const int ev0 = E.seed_event[ss];
+          if (SL.nq * 256 <= stage_words) {
+            key = ev0 * kMaxLayers + lay;
+            bulk_to_shared(s_bins, E.bins + (size_t)ev0 * E.n_bins + SL.bin_offset,
+                           (unsigned)(SL.nq * 256 * 4), &s_bar);
+          }
+        }
+        s_key = key;
+      }
+      __syncthreads();
+      if (s_key >= 0) {
+        const bool ok = mbar_wait(&s_bar, parity);
+        parity ^= 1u;
+        if (!__syncthreads_and(ok)) {
+          // The copy did not complete in time: no more staging in this
+          // block, the chunk reads the global table.
+          if (threadIdx.x == 0) {
+            atomicOr(E.err_flags, kErrStage);
+            s_pending = 1;
+            s_key = -1;
+          }
+          __syncthreads();
+        }
+      }
+    }
     int xs = 0, slot = 0;
     bool barrel = true;
     if (j < nb + ne) {
@@ -255,9 +345,14 @@ __global__ void __launch_bounds__(kBlock, MKFG_PROP_MIN_BLOCKS) k_propagate(Even
       const LayerDev& L = C.layer[layer];
       const int ev = E.seed_event[s];
       PrepOut o;
-      prep_cand(E, C, L, E.bins + (size_t)ev * E.n_bins + L.bin_offset,
-                E.layer_begin[ev * E.lb_stride + layer], reg, layer, s, B, slot, par, err, chg,
-                E.xhit + slot, stride, o);
+      const uint32_t* gbins = E.bins + (size_t)ev * E.n_bins + L.bin_offset;
+      if (kStageBins)
+        prep_cand<true>(E, C, L, s_key == ev * kMaxLayers + layer ? s_bins : gbins,
+                        E.layer_begin[ev * E.lb_stride + layer], reg, layer, s, B, slot, par, err,
+                        chg, E.xhit + slot, stride, o);
+      else
+        prep_cand(E, C, L, gbins, E.layer_begin[ev * E.lb_stride + layer], reg, layer, s, B, slot,
+                  par, err, chg, E.xhit + slot, stride, o);
       if (o.extra == 2) E.extra_last[slot] = o.extra_last;
 #pragma unroll
       for (int e = 0; e < 6; ++e) E.ppar[e * stride + slot] = o.ppar[e];
@@ -276,6 +371,9 @@ __global__ void __launch_bounds__(kBlock, MKFG_PROP_MIN_BLOCKS) k_propagate(Even
     for (int h = 0; h < xs; ++h)
       E.pairs[barrel ? base + h : E.pair_cap - 1 - (base + h)] = slot * kMaxXHits + h;
   }
+  // A copy whose wait gave up may still be writing shared memory: wait for
+  // it once more (bounded) before the block exits.
+  if (kStageBins && s_pending && threadIdx.x == 0) mbar_wait(&s_bar, parity ^ 1u);
 }
 
 //------------------------------------------------------------------------------
@@ -1091,6 +1189,8 @@ struct Finder {
   // Seed import on the host (partition, sort and initial candidates by the
   // upload's worker threads) instead of on the device.
   bool seed_import_host = false;
+  // Bin tables staged in shared memory by the propagation kernel.
+  bool stage_bins = false;
   // Global index of every uploaded event's layer starts ([n_events][L + 1]),
   // for checking the hit indices the worker calls are given.
   std::vector<int> h_lb;
@@ -1826,12 +1926,31 @@ struct StepGrids {
   int activate, propagate, chi2, clone, update;
 };
 
+// The propagation launch of one layer step, with the bin tables staged in
+// shared memory when the finder asks for it (mkfg_find_set_bin_staging).
+static cudaError_t launch_propagate(const Finder* f, int grid, cudaStream_t st,
+                                    const FindConfigDev* cfg, int step) {
+  if (!f->stage_bins) {
+    k_propagate<false><<<grid, kBlock, 0, st>>>(f->ev, cfg, step, 0);
+    return cudaGetLastError();
+  }
+  const int words = f->max_nq * 256;
+  const size_t smem = 4 * (size_t)words;
+  if (smem > 48 * 1024) {
+    const cudaError_t e = cudaFuncSetAttribute(k_propagate<true>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  k_propagate<true><<<grid, kBlock, smem, st>>>(f->ev, cfg, step, words);
+  return cudaGetLastError();
+}
+
 static StepGrids step_grids(Finder* f) {
   if (!f->resident[0]) {
     int dev = 0, n_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-    const void* fn[4] = {(const void*)k_propagate, (const void*)k_chi2, (const void*)k_clone<false>,
+    const void* fn[4] = {(const void*)k_propagate<false>, (const void*)k_chi2, (const void*)k_clone<false>,
                          (const void*)k_update};
     for (int k = 0; k < 4; ++k) {
       int per_sm = 0;
@@ -1864,7 +1983,7 @@ static int enqueue_run(Finder* f, cudaStream_t st, bool count_clone = false) {
   k_reset<<<std::max(grid_c, (n_work + kBlock - 1) / kBlock), kBlock, 0, st>>>(f->ev, n_work);
   for (int step = 1; step <= f->host_cfg.max_steps; ++step) {
     k_activate<<<g.activate, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
-    k_propagate<<<g.propagate, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+    MKFG_CUDA_TRY(launch_propagate(f, g.propagate, st, f->d_cfg, step));
     k_chi2<<<g.chi2, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
     if (count_clone)
       k_clone<true><<<g.clone, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
@@ -1929,7 +2048,7 @@ static int run_timed(mkfg_context* ctx, Finder* f, float* ms) {
     for (int step = 1; step <= f->host_cfg.max_steps; ++step) {
       k_activate<<<g.activate, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
       mark(1);
-      k_propagate<<<g.propagate, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
+      MKFG_CUDA_TRY(launch_propagate(f, g.propagate, st, f->d_cfg, step));
       mark(2);
       k_chi2<<<g.chi2, kBlock, 0, st>>>(f->ev, f->d_cfg, step);
       mark(3);
@@ -2268,7 +2387,7 @@ extern "C" int mkfg_find_backward_search_with(mkfg_context* ctx, const int32_t* 
   k_bks_begin<<<(S + 127) / 128, 128, 0, st>>>(f->ev, f->d_cfg_bks, V);
   for (int step = 1; step <= max_steps; ++step) {
     k_activate<<<g.activate, kBlock, 0, st>>>(f->ev, f->d_cfg_bks, step);
-    k_propagate<<<g.propagate, kBlock, 0, st>>>(f->ev, f->d_cfg_bks, step);
+    MKFG_CUDA_TRY(launch_propagate(f, g.propagate, st, f->d_cfg_bks, step));
     k_chi2<<<g.chi2, kBlock, 0, st>>>(f->ev, f->d_cfg_bks, step);
     k_clone<false><<<g.clone, kBlock, 0, st>>>(f->ev, f->d_cfg_bks, step);
     k_update<<<g.update, kBlock, 0, st>>>(f->ev, f->d_cfg_bks, step);
@@ -2994,6 +3113,16 @@ extern "C" int mkfg_find_set_arena_capacity(mkfg_context* ctx, int32_t nodes_per
                "arena capacity %d: 0 (automatic) or at least %d nodes per seed", nodes_per_seed,
                MKFG_MAX_SEED_HITS + 2);
   finder_of(ctx)->arena_cap = nodes_per_seed;
+  return MKFG_OK;
+}
+
+extern "C" int mkfg_find_set_bin_staging(mkfg_context* ctx, int32_t on) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  MKFG_REQUIRE(on == 0 || on == 1, "on must be 0 or 1, got %d", on);
+  Finder* f = finder_of(ctx);
+  if (f->stage_bins != (on != 0)) f->drop_graph();
+  f->stage_bins = on != 0;
   return MKFG_OK;
 }
 

@@ -34,7 +34,7 @@ struct __align__(16) Record {
 
 enum SeedState { kDormant = 0, kFinding = 1, kFinished = 2 };
 enum WsrCode { kWsrInside = 0, kWsrEdge = 1, kWsrOutside = 2 };
-enum ErrBits { kErrArena = 1, kErrLayerSize = 2 };
+enum ErrBits { kErrArena = 1, kErrLayerSize = 2, kErrStage = 4 };
 enum StepCount {
   kCntActBarrel = 0, kCntActEndcap, kCntPairBarrel, kCntPairEndcap, kCntUpdBarrel, kCntUpdEndcap,
   kCntFind, kCntN = 8

@@ -96,7 +96,10 @@ __device__ __forceinline__ float cdist(float a) { return a > kPI ? kTwoPI - a : 
 // the sensitive-region test (TrackerInfo.h:118-138). `bins` is the layer's
 // (q bin, phi bin) table of the candidate's event. Writes up to 16 hit
 // indices (index within layer) in bin-scan order; returns XHitSize (-1 when
-// outside the layer) and the WSR code.
+// outside the layer) and the WSR code. kGenericBins: `bins` may point to
+// shared memory (a staged copy of the table), so it is read with generic
+// loads rather than through the read-only data path.
+template <bool kGenericBins = false>
 __device__ __forceinline__ int select_hits(const EventDev& E, const LayerDev& L,
                                            const uint32_t* __restrict__ bins, int hit_base,
                                            const float (&par)[6],
@@ -164,7 +167,9 @@ __device__ __forceinline__ int select_hits(const EventDev& E, const LayerDev& L,
     for (int p0 = pb1; p0 < pb2; p0 += kBinChunk) {
       uint32_t bv[kBinChunk];
 #pragma unroll
-      for (int k = 0; k < kBinChunk; ++k) bv[k] = p0 + k < pb2 ? __ldg(row + ((p0 + k) & 0xff)) : 0u;
+      for (int k = 0; k < kBinChunk; ++k)
+        bv[k] = p0 + k < pb2 ? (kGenericBins ? row[(p0 + k) & 0xff] : __ldg(row + ((p0 + k) & 0xff)))
+                             : 0u;
 #pragma unroll
       for (int k = 0; k < kBinChunk; ++k) {
         const int first = bv[k] & 0xffff, last = bv[k] >> 16;
@@ -368,6 +373,7 @@ __device__ __forceinline__ bool activate_cand(const EventDev& E, const CandSoA& 
 // Propagation to the layer, SelectHitIndices, missed-layer handling
 // (mkFit/MkBuilder.cc:1568-1637) and the hole record (MkFinder.cc:1245-1283)
 // for an active candidate. xhit receives up to 16 indices with stride xstride.
+template <bool kGenericBins = false>
 __device__ __forceinline__ void select_cand(const EventDev& E, const FindConfigDev& C,
                                             const LayerDev& L, const uint32_t* layer_bins,
                                             int hit_base, int reg, int layer, int s,
@@ -375,6 +381,7 @@ __device__ __forceinline__ void select_cand(const EventDev& E, const FindConfigD
                                             const float (&perr)[21], int* xhit, int xstride,
                                             PrepOut& o);
 
+template <bool kGenericBins = false>
 __device__ __forceinline__ void prep_cand(const EventDev& E, const FindConfigDev& C,
                                           const LayerDev& L, const uint32_t* layer_bins,
                                           int hit_base, int reg, int layer, int s, const CandSoA& B,
@@ -384,12 +391,13 @@ __device__ __forceinline__ void prep_cand(const EventDev& E, const FindConfigDev
     propagate_to_r(par, err, chg, L.propagate_to, C.inter_pflags, C.mat, false, o.ppar, o.perr);
   else
     propagate_to_z(par, err, chg, L.propagate_to, C.inter_pflags, C.mat, false, o.ppar, o.perr);
-  select_cand(E, C, L, layer_bins, hit_base, reg, layer, s, B, slot, o.ppar, o.perr, xhit, xstride,
-              o);
+  select_cand<kGenericBins>(E, C, L, layer_bins, hit_base, reg, layer, s, B, slot, o.ppar, o.perr,
+                            xhit, xstride, o);
 }
 
 // The part of prep_cand after the propagation: SelectHitIndices on the
 // propagated state, missed-layer handling and the hole record.
+template <bool kGenericBins>
 __device__ __forceinline__ void select_cand(const EventDev& E, const FindConfigDev& C,
                                             const LayerDev& L, const uint32_t* layer_bins,
                                             int hit_base, int reg, int layer, int s,
@@ -397,7 +405,7 @@ __device__ __forceinline__ void select_cand(const EventDev& E, const FindConfigD
                                             const float (&perr)[21], int* xhit, int xstride,
                                             PrepOut& o) {
   o.active = true;
-  o.xs = select_hits(E, L, layer_bins, hit_base, ppar, perr, xhit, xstride, o.wsr);
+  o.xs = select_hits<kGenericBins>(E, L, layer_bins, hit_base, ppar, perr, xhit, xstride, o.wsr);
   const float cand_r = hypot_f(ppar[0], ppar[1]);
   if (L.is_barrel && cand_r < L.rin) {
     o.xs = 0;

@@ -207,6 +207,7 @@ def _bind(lib):
     lib.mkfg_find_work_clone.argtypes = [vp, i64p, i64p]
     lib.mkfg_find_set_arena_capacity.argtypes = [vp, ctypes.c_int32]
     lib.mkfg_find_set_seed_import.argtypes = [vp, ctypes.c_int32]
+    lib.mkfg_find_set_bin_staging.argtypes = [vp, ctypes.c_int32]
     lib.mkfg_find_download.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(MkfgFindOut)]
     lib.mkfg_find_download_best.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(MkfgFindOut)]
     lib.mkfg_find_event.argtypes = [vp, ctypes.POINTER(MkfgEvent), ctypes.POINTER(MkfgFindOut)]
@@ -526,6 +527,11 @@ class Finder:
         capi.check(self.lib.mkfg_find_clone_seeds(self.ctx.handle, int(layer), ctypes.byref(ci),
                                                   ctypes.byref(co)))
         return o
+
+    def set_bin_staging(self, on):
+        """Bin tables staged in shared memory by the propagation kernel of
+        the following runs (mkfg_find_set_bin_staging)."""
+        capi.check(self.lib.mkfg_find_set_bin_staging(self.ctx.handle, int(bool(on))))
 
     def set_seed_import(self, on_host):
         """Seed import of the following uploads on the host (True) or on the

@@ -959,3 +959,28 @@ def test_device_seed_import_equals_host(gpu_ctx):
         for k in got[True]:
             np.testing.assert_array_equal(got[False][k], got[True][k], err_msg=k)
         assert total == sum(e.n_seeds for e in events)
+
+
+def test_bin_staging_equals_global_reads(gpu_ctx):
+    """The propagation kernel with the bin tables staged in shared memory
+    by bulk copies (mkfg_find_set_bin_staging) finds the same candidates,
+    bit for bit, as with global reads, on eight batched-finding events
+    through the graph and on one event through the eager launches; no
+    staging wait gives up (the download reports no error)."""
+    from mkfit_b200 import workloads
+    events = [synth.gen_cms_event(**a) for a in workloads.find_event_args(8, 0)]
+    fnd = Finder(gpu_ctx, FindConfig(**workloads.find_config_kwargs()))
+    got = {}
+    for on in (False, True):
+        fnd.set_bin_staging(on)
+        total = fnd.upload_batch(events)
+        fnd.run_graph()
+        got[on] = fnd.download(total)
+        fnd.upload(events[0])
+        fnd.run()
+        got[on, "plain"] = fnd.download(events[0].n_seeds)
+    fnd.set_bin_staging(False)
+    for key in (True, (True, "plain")):
+        base = got[False] if key is True else got[False, "plain"]
+        for k in base:
+            np.testing.assert_array_equal(got[key][k], base[k], err_msg=str(k))
