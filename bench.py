@@ -324,8 +324,10 @@ def run_ours(args):
     ctx.synchronize()
     plain_b_ms = statistics.median(timed_events(stream, finder.run, max(3, args.steps // 2)))
 
-    # Batched form: all events resident, one graph replay per step.
+    # Batched form: all events resident, one graph replay per step, in the
+    # launch configuration the autotuner picks on this batch (untimed).
     finder.upload_batch(events)
+    tuning = finder.autotune_graph(reps=2)
     for _ in range(args.warmup):
         finder.run_graph()
     ctx.synchronize()
@@ -476,6 +478,10 @@ def run_ours(args):
         "adjoint": adjoint,
         "pu200": pu200,
         "iteration_stages": stages,
+        "autotune": dict(tuning, knobs="grid of the propagate, chi2, clone and update kernels as a "
+                                       "multiple of their resident blocks; bin staging",
+                         note="mkfg_find_autotune_graph on the step's batch before timing; "
+                              "ms_before / ms_after: summed per-launch device times of one run"),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         if fit is not None:

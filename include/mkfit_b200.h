@@ -716,6 +716,31 @@ int mkfg_find_set_seed_import(mkfg_context* ctx, int32_t on_host);
  * reference counterpart. */
 int mkfg_find_set_bin_staging(mkfg_context* ctx, int32_t on);
 
+/* Launch configuration of the graph form's list-driven kernels: grid of
+ * the propagation, chi2, clone and update kernels as a multiple of the
+ * blocks the device keeps resident for each (grid_mult[4]), and the bin
+ * staging of mkfg_find_set_bin_staging. ms_before / ms_after: the step
+ * time (sum of the per-launch device times of one run) before and after
+ * a tuning. No reference counterpart. */
+typedef struct {
+  int32_t grid_mult[4];
+  int32_t stage_bins;
+  float ms_before;
+  float ms_after;
+} mkfg_graph_tuning;
+
+/* Tunes the launch configuration on the uploaded batch: each kernel's
+ * grid multiple in turn over 1 .. 16 by its own device time (each setting
+ * timed `reps` times, the minimum kept), then the bin staging by the
+ * propagation kernel's time; the choice stays with the context for its
+ * following runs and is returned in *out (may be NULL). The results of a
+ * run do not depend on these settings. */
+int mkfg_find_autotune_graph(mkfg_context* ctx, int32_t reps, mkfg_graph_tuning* out);
+/* Sets or reads the launch configuration (e.g. one a caller kept from an
+ * earlier tuning). */
+int mkfg_find_set_graph_tuning(mkfg_context* ctx, const mkfg_graph_tuning* t);
+int mkfg_find_get_graph_tuning(mkfg_context* ctx, mkfg_graph_tuning* t);
+
 /* Clone-step counters of the last mkfg_find_work call: the records
  * (IdxChi2List entries, hits and holes) present when the seeds were ranked
  * and the new candidates written. Counted by the eager run (mkfg_find_run)

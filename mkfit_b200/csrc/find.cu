@@ -1191,6 +1191,10 @@ struct Finder {
   bool seed_import_host = false;
   // Bin tables staged in shared memory by the propagation kernel.
   bool stage_bins = false;
+  // Grids of the list-driven kernels (propagate, chi2, clone, update) as
+  // multiples of their resident blocks on the device; tuned by
+  // mkfg_find_autotune_graph.
+  int grid_mult[4] = {4, 1, 2, 4};
   // Global index of every uploaded event's layer starts ([n_events][L + 1]),
   // for checking the hit indices the worker calls are given.
   std::vector<int> h_lb;
@@ -1962,10 +1966,10 @@ static StepGrids step_grids(Finder* f) {
   const int grid_c = (S * kSlots + kBlock - 1) / kBlock;
   StepGrids g;
   g.activate = grid_c;
-  g.propagate = std::min(grid_c, 4 * f->resident[0]);
-  g.chi2 = std::min((S * kSlots * 4 + kBlock - 1) / kBlock, f->resident[1]);
-  g.clone = std::min((S * 32 + kBlock - 1) / kBlock, 2 * f->resident[2]);
-  g.update = std::min(grid_c, 4 * f->resident[3]);
+  g.propagate = std::min(grid_c, f->grid_mult[0] * f->resident[0]);
+  g.chi2 = std::min((S * kSlots * 4 + kBlock - 1) / kBlock, f->grid_mult[1] * f->resident[1]);
+  g.clone = std::min((S * 32 + kBlock - 1) / kBlock, f->grid_mult[2] * f->resident[2]);
+  g.update = std::min(grid_c, f->grid_mult[3] * f->resident[3]);
   return g;
 }
 
@@ -2317,6 +2321,97 @@ extern "C" int mkfg_find_autotune(mkfg_context* ctx, int32_t* seeds_per_block, f
   }
   if (seeds_per_block) *seeds_per_block = best_w;
   if (ms_per_run) *ms_per_run = best_ms;
+  return MKFG_OK;
+}
+
+extern "C" int mkfg_find_set_graph_tuning(mkfg_context* ctx, const mkfg_graph_tuning* t) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  MKFG_REQUIRE(t != nullptr, "null tuning");
+  for (int k = 0; k < 4; ++k)
+    MKFG_REQUIRE(t->grid_mult[k] >= 1 && t->grid_mult[k] <= 64, "grid_mult[%d] = %d outside [1, 64]",
+                 k, t->grid_mult[k]);
+  MKFG_REQUIRE(t->stage_bins == 0 || t->stage_bins == 1, "stage_bins must be 0 or 1");
+  Finder* f = finder_of(ctx);
+  for (int k = 0; k < 4; ++k) f->grid_mult[k] = t->grid_mult[k];
+  f->stage_bins = t->stage_bins != 0;
+  f->drop_graph();
+  return MKFG_OK;
+}
+
+extern "C" int mkfg_find_get_graph_tuning(mkfg_context* ctx, mkfg_graph_tuning* t) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  MKFG_REQUIRE(t != nullptr, "null tuning");
+  const Finder* f = finder_of(ctx);
+  for (int k = 0; k < 4; ++k) t->grid_mult[k] = f->grid_mult[k];
+  t->stage_bins = f->stage_bins;
+  t->ms_before = t->ms_after = 0.f;
+  return MKFG_OK;
+}
+
+extern "C" int mkfg_find_autotune_graph(mkfg_context* ctx, int32_t reps, mkfg_graph_tuning* out) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  Finder* f = finder_of(ctx);
+  MKFG_REQUIRE(f->configured && f->events_loaded, "no event uploaded");
+  MKFG_REQUIRE(reps >= 1 && reps <= 16, "reps %d outside [1, 16]", reps);
+  float ms[7];
+  // Kernel times of a run (min over reps per kernel, their sum the step).
+  auto measure = [&](float* best) -> int {
+    for (int k = 0; k < 7; ++k) best[k] = 1e30f;
+    for (int r = 0; r < reps; ++r) {
+      const int e = run_timed(ctx, f, ms);
+      if (e) return e;
+      for (int k = 0; k < 7; ++k) best[k] = std::min(best[k], ms[k]);
+    }
+    return MKFG_OK;
+  };
+  auto total = [](const float* t) {
+    float x = 0.f;
+    for (int k = 0; k < 7; ++k) x += t[k];
+    return x;
+  };
+  float cur[7];
+  if ((rc = measure(cur))) return rc;  // also the warm-up
+  if ((rc = measure(cur))) return rc;
+  const float before = total(cur);
+  // One kernel at a time: its grid multiple (its own time decides), then
+  // the bin staging (the propagation kernel's time decides). Kernel
+  // times index: 2 propagate, 3 chi2, 4 clone, 5 update.
+  static const int kMults[] = {1, 2, 3, 4, 6, 8, 12, 16};
+  for (int k = 0; k < 4; ++k) {
+    const int keep = f->grid_mult[k];
+    int best_m = keep;
+    float best_t = cur[2 + k];
+    for (int m : kMults) {
+      if (m == keep) continue;
+      f->grid_mult[k] = m;
+      float t[7];
+      if ((rc = measure(t))) return rc;
+      if (t[2 + k] < best_t) {
+        best_t = t[2 + k];
+        best_m = m;
+      }
+    }
+    f->grid_mult[k] = best_m;
+    if ((rc = measure(cur))) return rc;
+  }
+  {
+    const bool keep = f->stage_bins;
+    f->stage_bins = !keep;
+    float t[7];
+    if ((rc = measure(t))) return rc;
+    if (!(t[2] < cur[2])) f->stage_bins = keep;
+  }
+  f->drop_graph();
+  if ((rc = measure(cur))) return rc;
+  if (out) {
+    for (int k = 0; k < 4; ++k) out->grid_mult[k] = f->grid_mult[k];
+    out->stage_bins = f->stage_bins;
+    out->ms_before = before;
+    out->ms_after = total(cur);
+  }
   return MKFG_OK;
 }
 

@@ -42,6 +42,11 @@ class MkfgQFilterConfig(ctypes.Structure):
                 ("beam_spot_x", ctypes.c_float), ("beam_spot_y", ctypes.c_float)]
 
 
+class MkfgGraphTuning(ctypes.Structure):
+    _fields_ = [("grid_mult", ctypes.c_int32 * 4), ("stage_bins", ctypes.c_int32),
+                ("ms_before", ctypes.c_float), ("ms_after", ctypes.c_float)]
+
+
 class MkfgCandCounts(ctypes.Structure):
     _fields_ = [(k, vp) for k in ("nfound", "nover", "ninside", "ntail", "chi2")]
 
@@ -208,6 +213,9 @@ def _bind(lib):
     lib.mkfg_find_set_arena_capacity.argtypes = [vp, ctypes.c_int32]
     lib.mkfg_find_set_seed_import.argtypes = [vp, ctypes.c_int32]
     lib.mkfg_find_set_bin_staging.argtypes = [vp, ctypes.c_int32]
+    lib.mkfg_find_autotune_graph.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(MkfgGraphTuning)]
+    lib.mkfg_find_set_graph_tuning.argtypes = [vp, ctypes.POINTER(MkfgGraphTuning)]
+    lib.mkfg_find_get_graph_tuning.argtypes = [vp, ctypes.POINTER(MkfgGraphTuning)]
     lib.mkfg_find_download.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(MkfgFindOut)]
     lib.mkfg_find_download_best.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(MkfgFindOut)]
     lib.mkfg_find_event.argtypes = [vp, ctypes.POINTER(MkfgEvent), ctypes.POINTER(MkfgFindOut)]
@@ -527,6 +535,26 @@ class Finder:
         capi.check(self.lib.mkfg_find_clone_seeds(self.ctx.handle, int(layer), ctypes.byref(ci),
                                                   ctypes.byref(co)))
         return o
+
+    def autotune_graph(self, reps=2):
+        """Tunes the graph form's launch configuration on the uploaded
+        batch (mkfg_find_autotune_graph); returns it as a dict with the
+        step time before and after."""
+        t = MkfgGraphTuning()
+        capi.check(self.lib.mkfg_find_autotune_graph(self.ctx.handle, int(reps), ctypes.byref(t)))
+        return dict(grid_mult=list(t.grid_mult), stage_bins=int(t.stage_bins),
+                    ms_before=float(t.ms_before), ms_after=float(t.ms_after))
+
+    def graph_tuning(self):
+        t = MkfgGraphTuning()
+        capi.check(self.lib.mkfg_find_get_graph_tuning(self.ctx.handle, ctypes.byref(t)))
+        return dict(grid_mult=list(t.grid_mult), stage_bins=int(t.stage_bins))
+
+    def set_graph_tuning(self, tuning):
+        t = MkfgGraphTuning()
+        t.grid_mult[:] = [int(x) for x in tuning["grid_mult"]]
+        t.stage_bins = int(tuning["stage_bins"])
+        capi.check(self.lib.mkfg_find_set_graph_tuning(self.ctx.handle, ctypes.byref(t)))
 
     def set_bin_staging(self, on):
         """Bin tables staged in shared memory by the propagation kernel of

@@ -984,3 +984,28 @@ def test_bin_staging_equals_global_reads(gpu_ctx):
         base = got[False] if key is True else got[False, "plain"]
         for k in base:
             np.testing.assert_array_equal(got[key][k], base[k], err_msg=str(k))
+
+
+def test_graph_autotune_keeps_results(gpu_ctx):
+    """The graph form's autotuner (grid multiples of the list kernels and
+    the bin staging, mkfg_find_autotune_graph) on eight batched-finding
+    events: the candidates found with the tuned configuration equal those
+    of the default one bit for bit, the step is not slower, and the chosen
+    configuration can be read back and set again."""
+    from mkfit_b200 import workloads
+    events = [synth.gen_cms_event(**a) for a in workloads.find_event_args(8, 0)]
+    fnd = Finder(gpu_ctx, FindConfig(**workloads.find_config_kwargs()))
+    default = fnd.graph_tuning()
+    total = fnd.upload_batch(events)
+    fnd.run_graph()
+    base = fnd.download(total)
+    t = fnd.autotune_graph(reps=2)
+    print(f"\ntuned {t}")
+    assert t["ms_after"] <= 1.05 * t["ms_before"]
+    assert fnd.graph_tuning() == {k: t[k] for k in ("grid_mult", "stage_bins")}
+    fnd.run_graph()
+    tuned = fnd.download(total)
+    for k in base:
+        np.testing.assert_array_equal(tuned[k], base[k], err_msg=k)
+    fnd.set_graph_tuning(default)
+    assert fnd.graph_tuning() == default
