@@ -90,6 +90,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-fit", action="store_true")
     p.add_argument("--no-pu", action="store_true")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="keep the default launch configuration (fixed launch counts for profiling)")
     p.add_argument("--step-profile", action="store_true",
                    help="print per layer-plan step work and launch times to stderr")
     return p.parse_args()
@@ -327,7 +329,7 @@ def run_ours(args):
     # Batched form: all events resident, one graph replay per step, in the
     # launch configuration the autotuner picks on this batch (untimed).
     finder.upload_batch(events)
-    tuning = finder.autotune_graph(reps=2)
+    tuning = finder.graph_tuning() if args.no_autotune else finder.autotune_graph(reps=2)
     for _ in range(args.warmup):
         finder.run_graph()
     ctx.synchronize()
