@@ -1009,3 +1009,27 @@ def test_graph_autotune_keeps_results(gpu_ctx):
         np.testing.assert_array_equal(tuned[k], base[k], err_msg=k)
     fnd.set_graph_tuning(default)
     assert fnd.graph_tuning() == default
+
+
+def test_device_hit_index_on_bench_events(gpu_ctx):
+    """The device hit index on eight events of the batched-finding workload
+    (487k hits) against the host build: identical except for hits whose
+    phi the device's double-evaluated atan2 rounds to the other side of a
+    fine phi boundary than the host's float atan2 -- a handful of bin
+    entries and ranks, printed and bounded at 1e-5 of them."""
+    from mkfit_b200 import workloads
+    from mkfit_b200.finder import prepare_event_host
+    evs = [synth.gen_cms_event(**a) for a in workloads.find_event_args(8, 0)]
+    fnd = Finder(gpu_ctx, FindConfig(max_cands=M))
+    fnd.upload_batch(evs)
+    n_bins = n_ranks = d_bins = d_ranks = 0
+    for e, ev in enumerate(evs):
+        host = prepare_event_host(ev)
+        bins, srank = fnd.hit_index(e, host["bins"].size, ev.n_hits)
+        n_bins += bins.size
+        n_ranks += srank.size
+        d_bins += int((bins != host["bins"]).sum())
+        d_ranks += int((srank != host["srank"]).sum())
+    print(f"\n{len(evs)} events: bin entries differing {d_bins} of {n_bins}, ranks {d_ranks} of "
+          f"{n_ranks}")
+    assert d_bins <= 1e-5 * n_bins and d_ranks <= 1e-5 * n_ranks
