@@ -1407,8 +1407,18 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
                    "event %d layer %d holds more than 65535 hits", e, l);
     const int sw = seed_hit_stride(ev);
     MKFG_REQUIRE(sw >= 1 && sw <= MKFG_MAX_SEED_HITS, "event %d: seed_hit_stride %d", e, sw);
-    for (int s = 0; s < ev->n_seeds; ++s)
+    for (int s = 0; s < ev->n_seeds; ++s) {
       MKFG_REQUIRE(ev->seed_nhits[s] >= 1 && ev->seed_nhits[s] <= sw, "seed %d hit count", s);
+      // A seed's hits become hit-on-track nodes that the backward fit
+      // reads: a hit index (>= 0) must name a hit of its layer.
+      for (int h = 0; h < ev->seed_nhits[s]; ++h) {
+        const int hl = ev->seed_hit_layer[(size_t)s * sw + h], hi = ev->seed_hit_index[(size_t)s * sw + h];
+        if (hi < 0) continue;
+        MKFG_REQUIRE(hl >= 0 && hl < L && hi < ev->layer_begin[hl + 1] - ev->layer_begin[hl],
+                     "event %d seed %d hit %d: index %d on layer %d is not a hit of the layer", e, s,
+                     h, hi, hl);
+      }
+    }
     hit_off[e + 1] = hit_off[e] + ev->layer_begin[L];
     seed_off[e + 1] = seed_off[e] + ev->n_seeds;
   }

@@ -1033,3 +1033,20 @@ def test_device_hit_index_on_bench_events(gpu_ctx):
     print(f"\n{len(evs)} events: bin entries differing {d_bins} of {n_bins}, ranks {d_ranks} of "
           f"{n_ranks}")
     assert d_bins <= 1e-5 * n_bins and d_ranks <= 1e-5 * n_ranks
+
+
+def test_upload_rejects_seed_hit_outside_layer(gpu_ctx):
+    """A seed hit index past its layer's hits is refused by the upload
+    (MKFG_ERR_BAD_INPUT) before anything is copied: the backward fit would
+    read the hit through the seed's hit-on-track node."""
+    ev = synth.gen_cms_event(100, seed=5)
+    bad = synth.CmsEvent(**dict(ev.__dict__))
+    hi = ev.seed_hit_index.copy()
+    hl = int(ev.seed_hit_layer[3, 1])
+    hi[3, 1] = int(ev.layer_begin[hl + 1] - ev.layer_begin[hl])
+    bad.seed_hit_index = hi
+    fnd = Finder(gpu_ctx, FindConfig(max_cands=M))
+    with pytest.raises(Exception, match="not a hit of the layer"):
+        fnd.upload(bad)
+    out = fnd.find_event(ev)
+    assert out["n_cands"].shape == (ev.n_seeds,)
