@@ -116,6 +116,36 @@ typedef struct {
 
 int mkfg_fit(mkfg_context* ctx, const mkfg_fit_args* args);
 
+/* ----------------------------------------------------------- operators */
+/* The finding's operator table (FindingFoos, mkFit/FindingFoos.h:10-38,
+ * FindingFoos.cc:7-8) as plain calls on n states, endcap = 0 for the
+ * barrel member of the table and 1 for the endcap one. Arrays are
+ * lane-fastest with element stride `stride` >= n (element e of state i at
+ * e * stride + i: a Matriplex's storage with stride NN); only lanes
+ * [0, n) are read and written. Host pointers; the context's material map;
+ * pflags: PropagationFlags bits (1 B field, 2 material). Synchronize.
+ *
+ * mkfg_op_propagate <- MkBase::PropagateTracksToR / PropagateTracksToZ
+ *   (mkFit/MkBase.h:35-75): propagation to target[i] (r or z).
+ * mkfg_op_propagate_chi2 <- kalmanPropagateAndComputeChi2[Endcap]
+ *   (mkFit/KalmanUtilsMPlex.cc:524-544, 751-770): propagation to the hit's
+ *   radius / z, chi2 of the hit (not its absolute value), the propagated
+ *   parameters.
+ * mkfg_op_propagate_update <- kalmanPropagateAndUpdate[Endcap]
+ *   (:471-505, 697-731): propagation to the hit, update, charge flip of a
+ *   negative 1/pT; out_chg may alias chg. */
+int mkfg_op_propagate(mkfg_context* ctx, int32_t endcap, int32_t n, int32_t stride,
+                      const float* par, const float* err, const int32_t* chg, const float* target,
+                      uint32_t pflags, float* out_par, float* out_err);
+int mkfg_op_propagate_chi2(mkfg_context* ctx, int32_t endcap, int32_t n, int32_t stride,
+                           const float* par, const float* err, const int32_t* chg,
+                           const float* hit_pos, const float* hit_err, uint32_t pflags,
+                           float* out_chi2, float* out_prop_par);
+int mkfg_op_propagate_update(mkfg_context* ctx, int32_t endcap, int32_t n, int32_t stride,
+                             const float* par, const float* err, const int32_t* chg,
+                             const float* hit_pos, const float* hit_err, uint32_t pflags,
+                             float* out_par, float* out_err, int32_t* out_chg);
+
 /* Same fit from HOST buffers: copies inputs to device scratch owned by the
  * context, fits, copies outputs back, synchronizes. The pointers inside
  * args (including hits.layer_begin) are host pointers here. */

@@ -1347,3 +1347,31 @@ def shim_fit_steered(ev, pflags=2, chunk=8):
     nl = ev.hit_pos.shape[0]
     barrel = np.array([0 if (int(ev.endcap_mask) >> l) & 1 else 1 for l in range(nl)], np.int32)
     return _shim_call(_shims().shim_fit_steered, ev, pflags, chunk, barrel)
+
+
+def shim_ops(par, err, chg, hit_pos, hit_err, target, endcap, rl_grid, xi_grid, pflags=2):
+    """The finding operator table on n states through the reference's
+    FindingFoos and through FindingFoosGpu (oracle/shim_driver.cc
+    shim_ops): propagation to `target`, propagation to the hits with the
+    chi2 and with the update. Returns a dict of [2][...] arrays (0 the
+    reference, 1 the GPU): prop_par, prop_err, chi2, chi2_par, upd_par,
+    upd_err, upd_chg."""
+    L = ctypes.CDLL(shims_lib_path())
+    L.shim_ops.restype = ctypes.c_int
+    L.shim_ops.argtypes = [ctypes.c_int, ctypes.c_int, _f32p, _f32p, _i32p, _f32p, _f32p,
+                           ctypes.c_float, _f32p, _f32p, ctypes.c_int, _f32p, _f32p, _f32p,
+                           _f32p, _f32p, _f32p, _i32p]
+    c = np.ascontiguousarray
+    n = int(len(chg))
+    o = dict(prop_par=np.zeros((2, 6, n), np.float32), prop_err=np.zeros((2, 21, n), np.float32),
+             chi2=np.zeros((2, n), np.float32), chi2_par=np.zeros((2, 6, n), np.float32),
+             upd_par=np.zeros((2, 6, n), np.float32), upd_err=np.zeros((2, 21, n), np.float32),
+             upd_chg=np.zeros((2, n), np.int32))
+    rc = L.shim_ops(n, int(endcap), c(par, np.float32), c(err, np.float32), c(chg, np.int32),
+                    c(hit_pos, np.float32), c(hit_err, np.float32), float(target),
+                    c(rl_grid, np.float32), c(xi_grid, np.float32), int(pflags), o["prop_par"],
+                    o["prop_err"], o["chi2"], o["chi2_par"], o["upd_par"], o["upd_err"],
+                    o["upd_chg"])
+    if rc != 0:
+        raise RuntimeError(f"shim_ops failed rc={rc}")
+    return o
