@@ -54,6 +54,12 @@ int mkfg_context_create(int device, mkfg_context** out);
 int mkfg_context_destroy(mkfg_context* ctx);
 /* The cudaStream_t used by the context, as an opaque pointer. */
 void* mkfg_context_stream(mkfg_context* ctx);
+/* Makes the context enqueue its work on the caller's stream (a
+ * cudaStream_t of the context's device, as an opaque pointer; NULL: back
+ * to the stream the context created). Waits for the work already enqueued
+ * on the current stream first. The caller keeps the stream alive while the
+ * context uses it. */
+int mkfg_context_set_stream(mkfg_context* ctx, void* stream);
 int mkfg_context_synchronize(mkfg_context* ctx);
 
 /* Upload the (z, r) material grid, 300 x 120 floats each, row = z bin

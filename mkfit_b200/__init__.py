@@ -51,6 +51,15 @@ class Context:
     def stream_ptr(self):
         return self.lib.mkfg_context_stream(self.handle)
 
+    def set_stream(self, stream):
+        """Enqueue the context's work on `stream` (a torch.cuda.Stream, a
+        raw cudaStream_t as an int, or None for the context's own stream):
+        mkfg_context_set_stream."""
+        import ctypes
+        ptr = getattr(stream, "cuda_stream", stream)
+        self.lib.mkfg_context_set_stream.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        capi.check(self.lib.mkfg_context_set_stream(self.handle, ptr))
+
     def torch_stream(self):
         import torch
         return torch.cuda.ExternalStream(self.stream_ptr, device=torch.device("cuda", self.device))

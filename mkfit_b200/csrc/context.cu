@@ -55,7 +55,8 @@ int mkfg_context_create(int device, mkfg_context** out) {
   MKFG_CUDA_TRY(cudaSetDevice(device));
   mkfg_context* ctx = new mkfg_context;
   ctx->device = device;
-  cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  cudaError_t e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
+  ctx->stream = ctx->own_stream;
   if (e == cudaSuccess) e = cudaMalloc(&ctx->d_rl, sizeof(float) * kMatNZ * kMatNR);
   if (e == cudaSuccess) e = cudaMalloc(&ctx->d_xi, sizeof(float) * kMatNZ * kMatNR);
   if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_rl, 0, sizeof(float) * kMatNZ * kMatNR, ctx->stream);
@@ -80,12 +81,21 @@ int mkfg_context_destroy(mkfg_context* ctx) {
   ctx->scratch_hits.release();
   ctx->scratch_out.release();
   ctx->scratch_misc.release();
-  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
   return MKFG_OK;
 }
 
 void* mkfg_context_stream(mkfg_context* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int mkfg_context_set_stream(mkfg_context* ctx, void* stream) {
+  int rc = activate(ctx);
+  if (rc) return rc;
+  // Work already enqueued finishes on the stream it was enqueued on.
+  MKFG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+  return MKFG_OK;
+}
 
 int mkfg_context_synchronize(mkfg_context* ctx) {
   int rc = activate(ctx);

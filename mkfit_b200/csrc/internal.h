@@ -78,7 +78,8 @@ struct HostBuf {
 
 struct mkfg_context {
   int device = -1;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;      // where the context enqueues its work
+  cudaStream_t own_stream = nullptr;  // the stream the context created
   float* d_rl = nullptr;  // material grid, 300 x 120
   float* d_xi = nullptr;
   // Scratch for the host-buffer entry points.

@@ -170,3 +170,22 @@ def test_fit_host_rejects_hit_index_outside_layer(gpu_ctx, entry):
         else:
             assert rc == 1
             assert "outside layer" in capi.last_error()
+
+
+def test_fit_on_caller_stream(gpu_ctx):
+    """mkfg_context_set_stream: the fit enqueued on the caller's stream gives
+    the same result as on the context's own stream, and the context goes
+    back to its own stream on NULL."""
+    own = gpu_ctx.stream_ptr
+    ev = synth.gen_fit_event(2001, seed=31)
+    base = gpu_fit(gpu_ctx, ev, with_chi2=True)
+    s = torch.cuda.Stream()
+    gpu_ctx.set_stream(s)
+    try:
+        assert gpu_ctx.stream_ptr == s.cuda_stream
+        got = gpu_fit(gpu_ctx, ev, with_chi2=True)
+    finally:
+        gpu_ctx.set_stream(None)
+    assert gpu_ctx.stream_ptr == own
+    for k in base:
+        np.testing.assert_array_equal(got[k], base[k], err_msg=k)
