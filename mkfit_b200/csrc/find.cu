@@ -530,6 +530,21 @@ __global__ void k_reset(EventDev E, int n_work) {
 
 // Writes every seed's own hits as the first nodes of its hit-on-track
 // arena (CombCandidate::ImportSeed); appends during a run start after them.
+// The packed copy of the hits (EventDev::hit4), one thread per hit.
+__global__ void k_pack_hits(const float* __restrict__ pos, const float* __restrict__ err,
+                            int stride, int n, float4* __restrict__ out) {
+  const int h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= n) return;
+  float v[9];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) v[k] = pos[(size_t)k * stride + h];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) v[3 + k] = err[(size_t)k * stride + h];
+  out[3 * (size_t)h] = make_float4(v[0], v[1], v[2], v[3]);
+  out[3 * (size_t)h + 1] = make_float4(v[4], v[5], v[6], v[7]);
+  out[3 * (size_t)h + 2] = make_float4(v[8], 0.f, 0.f, 0.f);
+}
+
 __global__ void k_seed_nodes(EventDev E, const int* __restrict__ seed_hot) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= E.n_seeds) return;
@@ -692,10 +707,7 @@ __global__ void __launch_bounds__(kBlock) k_bkfit(EventDev E, const FindConfigDe
         prev = E.node_prev[(size_t)s * E.hot_cap + node];
       }
       const int gi = lb[layer] + hot_index(node_hot_of(E, s, node));
-#pragma unroll
-      for (int e = 0; e < 3; ++e) mpos[e] = __ldg(E.hpos + e * E.hstride + gi);
-#pragma unroll
-      for (int e = 0; e < 6; ++e) merr[e] = __ldg(E.herr + e * E.hstride + gi);
+      load_hit(E, gi, mpos, merr);
       node = prev;
     } else {
       mpos[0] = par[0];
@@ -1439,7 +1451,8 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   const size_t up_bytes = rounded(12 * (size_t)NHs) + rounded(24 * (size_t)NHs) +
                           2 * rounded(4 * (size_t)NHs) + rounded(4 * n_lb) + rounded((size_t)NHs);
   const size_t hit_bytes = up_bytes + rounded(4 * (size_t)NHs) + rounded(4 * n_bins_all) +
-                           rounded(8 * (size_t)NHs) + rounded(4 * (size_t)NHs);
+                           rounded(8 * (size_t)NHs) + rounded(4 * (size_t)NHs) +
+                           rounded(48 * (size_t)NHs);
   int rc;
   if ((rc = f->hits.ensure(hit_bytes))) return rc;
   if ((rc = f->hits_h.ensure(up_bytes))) return rc;
@@ -1454,6 +1467,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     uint32_t* bins;
     float2* qphi;
     int* srank;
+    float4* hit4;
   };
   auto layout = [&](char* p, bool device) {
     HitsLayout h{};
@@ -1468,6 +1482,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
       h.bins = carve<uint32_t>(p, n_bins_all);
       h.qphi = carve<float2>(p, NHs);
       h.srank = carve<int>(p, NHs);
+      h.hit4 = carve<float4>(p, 3 * (size_t)NHs);
     }
     return h;
   };
@@ -1746,8 +1761,11 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     k_layer_hits<<<n_ev * L, kHitsBlock, smem, st>>>(A, f->d_cfg);
     MKFG_CUDA_TRY(cudaGetLastError());
   }
+  if (NH > 0) k_pack_hits<<<(NH + 255) / 256, 256, 0, st>>>(dh.pos, dh.err, NHs, NH, dh.hit4);
+  MKFG_CUDA_TRY(cudaGetLastError());
   f->ev.hpos = dh.pos;
   f->ev.herr = dh.err;
+  f->ev.hit4 = dh.hit4;
   f->ev.hstride = NHs;
   f->ev.hinfo = dh.info;
   f->ev.layer_begin = dh.lb;

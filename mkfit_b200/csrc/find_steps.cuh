@@ -438,10 +438,7 @@ __device__ __forceinline__ bool pair_accept(const EventDev& E, const FindConfigD
                                             const float (&perr)[21], int chg, float& chi2_out,
                                             int& module_out) {
   float mpos[3], merr[6];
-#pragma unroll
-  for (int e = 0; e < 3; ++e) mpos[e] = __ldg(E.hpos + e * E.hstride + g);
-#pragma unroll
-  for (int e = 0; e < 6; ++e) merr[e] = __ldg(E.herr + e * E.hstride + g);
+  load_hit(E, g, mpos, merr);
   const uint32_t info = __ldg(E.hinfo + g);
   float hpar[6], herr_[21];
   float chi2;
@@ -506,10 +503,7 @@ __device__ __forceinline__ void update_state(const EventDev& E, const FindConfig
                                              const LayerDev& L, int g, float (&par)[6],
                                              float (&err)[21], int& chg) {
   float mpos[3], merr[6];
-#pragma unroll
-  for (int e = 0; e < 3; ++e) mpos[e] = __ldg(E.hpos + e * E.hstride + g);
-#pragma unroll
-  for (int e = 0; e < 6; ++e) merr[e] = __ldg(E.herr + e * E.hstride + g);
+  load_hit(E, g, mpos, merr);
   float ppar[6], perr[21];
   if (L.is_barrel) {
     propagate_to_r(par, err, chg, hypot_f(mpos[0], mpos[1]), C.inter_pflags, C.mat, false, ppar, perr);
