@@ -933,8 +933,9 @@ int ref_cms2017_backward_params(float* bk, int* flags) {
 }
 
 // Clone-engine combinatorial finding on one event, CMS-2017 geometry,
-// iteration 0 with overrides (BASELINE config: max cands per seed, flat
-// chi2 cut: the dynamic c2 parameters are zeroed when zero_c2 != 0).
+// iteration 0 with overrides (the benchmark workloads' settings: max cands
+// per seed, flat chi2 cut: the dynamic c2 parameters are zeroed when
+// zero_c2 != 0).
 //
 // Hits: layer l occupies [layer_begin[l], layer_begin[l+1]) of pos[3][nh],
 //   err[6][nh]; detid[nh] (12-bit module id), cpcm[nh] (< 0: pixel hit,
