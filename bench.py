@@ -456,6 +456,11 @@ def run_ours(args):
         "dtype": "f32",
         "data": "synthetic (seeded, mkfit_b200.synth.gen_cms_event on the CMS-2017 layer table)",
         "config": find_config_line(events, world),
+        "rates": {"seeds_per_s": n_seeds * world / (total_ms_max / args.steps * 1e-3),
+                  "candidate_hit_evals_per_s": work["hit_pairs"] * world /
+                                               (total_ms_max / args.steps * 1e-3),
+                  "note": "the batched-finding workload in two more units: seeds found and "
+                          "(candidate, hit) chi2 evaluations per second, whole job"},
         "plain_form": {
             "cms_800_tracks": {"events_per_launch_sequence": 1, "value": 1e3 / plain_cfg1_ms,
                                "unit": "events/s", "ms_per_event": plain_cfg1_ms,
