@@ -1050,3 +1050,19 @@ def test_upload_rejects_seed_hit_outside_layer(gpu_ctx):
         fnd.upload(bad)
     out = fnd.find_event(ev)
     assert out["n_cands"].shape == (ev.n_seeds,)
+
+
+def test_large_event_imports_seeds_on_host(gpu_ctx):
+    """An event with more seeds than the device sort takes (16384) is
+    imported on the host whatever the setting; the candidates equal those of
+    an upload forced onto the host path."""
+    ev = synth.gen_cms_event(17000, seed=211, noise_frac=0.01)
+    assert ev.n_seeds > 16384
+    fnd = Finder(gpu_ctx, FindConfig(max_cands=M))
+    got = {}
+    for on_host in (False, True):
+        fnd.set_seed_import(on_host)
+        got[on_host] = fnd.find_event(ev)
+    fnd.set_seed_import(False)
+    for k in got[True]:
+        np.testing.assert_array_equal(got[False][k], got[True][k], err_msg=k)
