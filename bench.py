@@ -500,7 +500,7 @@ def run_ours(args):
             line["cpu_baseline"]["pu200"] = cpu_baseline_find(pu_events, pu_best,
                                                               n_sample=CPU_PU_EVENTS)
     if rank == 0:
-        print(json.dumps(line), flush=True)
+        emit(line)
     ctx.close()
     mdist.teardown(world)
 
@@ -759,9 +759,9 @@ def run_reference(args):
         return
     from oracle.oracle import RefLib, have_ref, ref_find_batch
     if not have_ref():
-        print(json.dumps({"impl": "reference", "unavailable":
-                          "reference CPU build oracle/_ref missing (built by __graft_entry__.build "
-                          "from the reference sources)"}))
+        emit({"impl": "reference", "unavailable":
+              "reference CPU build oracle/_ref missing (built by __graft_entry__.build "
+              "from the reference sources)"})
         return
     events = generate(find_event_args(args.events, 0))
     ref = RefLib()
@@ -791,7 +791,7 @@ def run_reference(args):
                 "d2h_bytes_per_step": 0},
         "gpu_launches": 0,
     }
-    print(json.dumps(line), flush=True)
+    emit(line)
 
 
 def spawn_ranks(args):
@@ -808,10 +808,34 @@ def spawn_ranks(args):
     return subprocess.call(cmd)
 
 
+_RESULT_FD = None
+
+
+def emit(line):
+    """Prints the result line on the process's real standard output."""
+    data = (json.dumps(line) + "\n").encode()
+    if _RESULT_FD is None:
+        sys.stdout.write(data.decode())
+        sys.stdout.flush()
+    else:
+        os.write(_RESULT_FD, data)
+
+
+def keep_stdout_for_result():
+    """Sends everything else written to file descriptor 1 (the reference
+    library's own printf lines among it) to standard error, so that
+    standard output carries the one JSON line alone."""
+    global _RESULT_FD
+    sys.stdout.flush()
+    _RESULT_FD = os.dup(1)
+    os.dup2(2, 1)
+
+
 def main():
     args = parse()
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
         sys.exit(spawn_ranks(args))
+    keep_stdout_for_result()
     if args.impl == "reference":
         run_reference(args)
     else:
