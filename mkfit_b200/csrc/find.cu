@@ -214,7 +214,8 @@ __global__ void __launch_bounds__(kBlock, MKFG_ACT_MIN_BLOCKS) k_activate(EventD
     __shared__ BlockAppend sh;
     append_two_ended_block(active, barrel, slot, E.act_list, E.list_cap, cnt + kCntActBarrel, sh);
     // Seeds finding at this step go to the clone step.
-    append_list_block(in_range && c == 0 && seed_finding, s, E.find_list, cnt + kCntFind, sh);
+    append_two_ended_block(in_range && c == 0 && seed_finding, true, s, E.find_list, 0,
+                           cnt + kCntFind, sh, find_info_pack(buf, ncand, layer), E.find_info);
     // The clone step reads the records and extra flags of candidates
     // [0, ncand) of seeds still finding: an inactive one among them has
     // neither.
@@ -449,10 +450,9 @@ __global__ void __launch_bounds__(kBlock, MKFG_CLONE_MIN_BLOCKS) k_clone(EventDe
     if (w < n_find) {
       // A seed finding at this step (listed by the activation kernel).
       const int s = E.find_list[w];
-      const int layer = plan_layer(C, E.region[s], step);
-      const int cur = E.cur[s];
+      const int info = E.find_info[w];
+      const int cur = info & 1, ncand = (info >> 1) & 15, layer = info >> 5;
       const size_t rb = (size_t)s * kRecPerSeed;
-      const int ncand = E.n_cands[s];
       const int hit0 = E.layer_begin[E.seed_event[s] * E.lb_stride + layer];
       const SeedRecords R{E.rec + rb, E.rmask + s * kSlots, E.wsr + s * kSlots,
                           E.extra_last + s * kSlots, nullptr};
@@ -1326,9 +1326,9 @@ extern "C" int mkfg_finder_setup(mkfg_context* ctx, const mkfg_find_config* cfg)
   f->n_bins = off;
   f->max_nq = 1;
   for (const auto& b : f->binning) f->max_nq = std::max(f->max_nq, b.nq);
-  MKFG_REQUIRE(f->max_nq * kFineStride * 4 <= 200 * 1024,
+  MKFG_REQUIRE(hits_smem_bytes(f->max_nq) <= 200 * 1024,
                "a layer has %d q bins; the device hit-index build supports up to %d",
-               f->max_nq, 200 * 1024 / (kFineStride * 4));
+               f->max_nq, 200 * 1024 / (2 * kFineStride));
   H.n_layers = cfg->n_layers;
   H.n_regions = cfg->n_regions;
   int max_steps = 0;
@@ -1756,7 +1756,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     A.qphi = dh.qphi;
     A.srank = dh.srank;
     A.mask = any_mask ? dh.mask : nullptr;
-    const int smem = f->max_nq * kFineStride * 4;
+    const int smem = hits_smem_bytes(f->max_nq);
     MKFG_CUDA_TRY(cudaFuncSetAttribute(k_layer_hits, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     k_layer_hits<<<n_ev * L, kHitsBlock, smem, st>>>(A, f->d_cfg);
     MKFG_CUDA_TRY(cudaGetLastError());
@@ -1837,6 +1837,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     f->ev.upd_list = carve<int>(p, SC);
     f->ev.upd_hit = carve<int>(p, SC);
     f->ev.find_list = carve<int>(p, SS);
+    f->ev.find_info = carve<int>(p, SS);
     f->ev.list_cap = SC;
     f->ev.step_count = carve<int>(p, (size_t)kCntN * (max_steps + 2));
     f->ev.err_flags = carve<int>(p, 16);

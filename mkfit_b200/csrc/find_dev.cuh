@@ -18,6 +18,12 @@ constexpr int kRecPerSeed = kSlots * kRecPerCand;
 // the clone step, new candidates written by it.
 constexpr int kWorkN = 6;
 constexpr int kMaxLayers = 128;
+// find_list entry info: current buffer (bit 0), candidate count (bits
+// 1-4), layer (bits 5-12).
+__host__ __device__ constexpr int find_info_pack(int cur, int ncand, int layer) {
+  return cur | (ncand << 1) | (layer << 5);
+}
+static_assert(kSlots <= 15 && kMaxLayers <= 256, "find_info_pack field widths");
 constexpr int kMaxPlan = 64;
 constexpr int kMaxRegions = 8;
 constexpr int kExportHits = 64;         // Config::nMaxTrkHits
@@ -142,8 +148,11 @@ struct EventDev {
   int* upd_list;
   int* upd_hit;    // global index of the hit each listed update uses
   int list_cap;
-  // Plain form, per step: seeds finding at the step (for the clone kernel).
+  // Plain form, per step: seeds finding at the step (for the clone kernel),
+  // and per entry the seed's buffer, candidate count and layer at the step
+  // (find_info_pack), so the clone kernel starts its loads from one read.
   int* find_list;
+  int* find_info;
   int* step_count; // [max_steps + 2][kCntN]
   int* err_flags;
   // Pristine initial state (restored by the reset kernel before every run).

@@ -5,10 +5,14 @@
 // ranges, the sorted (q, phi) and the original index of every sorted hit.
 //
 // One thread block per (event, layer). The sort is a counting sort over the
-// layer's nq x 1024 fine keys in shared memory: a histogram, an exclusive
+// layer's nq x 1025 fine keys in shared memory: a histogram, an exclusive
 // scan (which also gives the bin table), then a scatter in hit order in
 // which equal keys take consecutive positions in order of their hit index
 // -- the stable order of the reference's sort, whatever the warp schedule.
+// The counters are 16 bits, two to a 32-bit word (a layer holds at most
+// 65535 hits, which the upload checks, so no count, start or end of a key
+// reaches the upper half): 55 KB for the 27 q bins of the largest layer,
+// four blocks of 512 threads per SM.
 #pragma once
 
 #include "find_dev.cuh"
@@ -52,10 +56,25 @@ struct LayerHitsArgs {
   const uint8_t* mask;   // [NH] hits masked by earlier iterations, or NULL
 };
 
-// Dynamic shared memory: nq_max * kFineStride counters.
-__global__ void __launch_bounds__(kHitsBlock) k_layer_hits(const LayerHitsArgs A,
+// Dynamic shared memory: nq_max * kFineStride 16-bit counters, rounded up
+// to whole words (hits_smem_bytes).
+__host__ __device__ constexpr int hits_smem_words(int nq) { return (nq * kFineStride + 1) / 2; }
+__host__ __device__ constexpr int hits_smem_bytes(int nq) { return 4 * hits_smem_words(nq); }
+
+// 16-bit counter k of the packed table.
+__device__ __forceinline__ uint32_t cnt16_get(const uint32_t* w, int k) {
+  return (w[k >> 1] >> ((k & 1) * 16)) & 0xffffu;
+}
+// Four blocks per SM (32 registers, a few spilled): the build is latency
+// bound (its scatter steps the block's warps in turn), and the 64-event
+// batch's 4608 blocks take 326 us against 496 us at two blocks per SM (62
+// registers) and 379 us at three.
+#ifndef MKFG_HITS_MIN_BLOCKS
+#define MKFG_HITS_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(kHitsBlock, MKFG_HITS_MIN_BLOCKS) k_layer_hits(const LayerHitsArgs A,
                                                            const FindConfigDev* __restrict__ Cp) {
-  extern __shared__ uint32_t cnt[];
+  extern __shared__ uint32_t cntw[];
   __shared__ uint32_t warp_tot[kHitsBlock / 32];
   __shared__ uint32_t warp_base[kHitsBlock / 32];
   const FindConfigDev& C = *Cp;
@@ -81,21 +100,27 @@ __global__ void __launch_bounds__(kHitsBlock) k_layer_hits(const LayerHitsArgs A
     return qb * kFineStride + fine;
   };
 
-  for (int k = tid; k < nkeys; k += kHitsBlock) cnt[k] = 0;
+  const int nwords = (nkeys + 1) / 2;
+  for (int k = tid; k < nwords; k += kHitsBlock) cntw[k] = 0;
   __syncthreads();
   for (int i = tid; i < n; i += kHitsBlock) {
     float q, phi;
-    atomicAdd(&cnt[hit_key(h0 + i, q, phi)], 1u);
+    const int key = hit_key(h0 + i, q, phi);
+    atomicAdd(&cntw[key >> 1], 1u << ((key & 1) * 16));
     A.hinfo[h0 + i] = (uint32_t(A.detid[h0 + i]) & 0xfffu) |
                       (decoded_charge_pcm_dev(A.cpcm[h0 + i]) << 12);
   }
   __syncthreads();
 
-  // Exclusive scan of the counters: thread t owns a contiguous segment.
-  const int seg = (nkeys + kHitsBlock - 1) / kHitsBlock;
+  // Exclusive scan of the counters: thread t owns a contiguous segment of
+  // whole words (both halves of a word are its own).
+  const int seg = 2 * ((nwords + kHitsBlock - 1) / kHitsBlock);
   const int k0 = min(tid * seg, nkeys), k1 = min(k0 + seg, nkeys);
   uint32_t local = 0;
-  for (int k = k0; k < k1; ++k) local += cnt[k];
+  for (int k = k0; k < k1; k += 2) {
+    const uint32_t v = cntw[k >> 1];
+    local += (v & 0xffffu) + (v >> 16);
+  }
   uint32_t incl = local;
 #pragma unroll
   for (int off = 1; off < 32; off <<= 1) {
@@ -116,25 +141,27 @@ __global__ void __launch_bounds__(kHitsBlock) k_layer_hits(const LayerHitsArgs A
   }
   __syncthreads();
   uint32_t run = warp_base[warp] + incl - local;
-  for (int k = k0; k < k1; ++k) {
-    const uint32_t c = cnt[k];
-    cnt[k] = run;
-    run += c;
+  for (int k = k0; k < k1; k += 2) {
+    // A key past the end (odd nkeys) shares the last word and counts 0.
+    const uint32_t v = cntw[k >> 1];
+    const uint32_t lo = run, hi = run + (v & 0xffffu);
+    cntw[k >> 1] = lo | (hi << 16);
+    run = hi + (v >> 16);
   }
   __syncthreads();
 
   // Bin table: (q bin, phi bin) covers fine keys q * kFineStride + 4 * phi
   // bin + 0..3; fine key 1024, when present, takes over phi bin 0.
   uint32_t* bins = A.bins + (size_t)ev * A.n_bins + L.bin_offset;
-  auto key_end = [&](int k) { return k < nkeys ? cnt[k] : (uint32_t)n; };
+  auto key_end = [&](int k) { return k < nkeys ? cnt16_get(cntw, k) : (uint32_t)n; };
   for (int b = tid; b < L.nq * kLayerPhiBins; b += kHitsBlock) {
     const int qb = b / kLayerPhiBins, pb = b % kLayerPhiBins;
     int k = qb * kFineStride + 4 * pb;
-    uint32_t first = cnt[k], last = key_end(k + 4);
+    uint32_t first = cnt16_get(cntw, k), last = key_end(k + 4);
     if (pb == 0) {
       const int k1024 = qb * kFineStride + kPhiFine;
-      if (key_end(k1024 + 1) != cnt[k1024]) {
-        first = cnt[k1024];
+      if (key_end(k1024 + 1) != cnt16_get(cntw, k1024)) {
+        first = cnt16_get(cntw, k1024);
         last = key_end(k1024 + 1);
       }
     }
@@ -155,8 +182,9 @@ __global__ void __launch_bounds__(kHitsBlock) k_layer_hits(const LayerHitsArgs A
         const int leader = __ffs(peers) - 1;
         uint32_t base = 0;
         if (lane == leader) {
-          base = cnt[key];
-          cnt[key] = base + __popc(peers);
+          // Leaders of the two keys of a word may meet here: add, not store.
+          const int sh = (key & 1) * 16;
+          base = (atomicAdd(&cntw[key >> 1], (uint32_t)__popc(peers) << sh) >> sh) & 0xffffu;
         }
         base = __shfl_sync(peers, base, leader);
         const uint32_t at = base + __popc(peers & ((1u << lane) - 1u));
