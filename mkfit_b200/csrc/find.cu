@@ -96,7 +96,8 @@ struct BlockAppend {
 
 __device__ __forceinline__ void append_two_ended_block(bool want, bool barrel, int value, int* list,
                                                        int cap, int* cnt, BlockAppend& sh,
-                                                       int value2 = 0, int* list2 = nullptr) {
+                                                       int value2 = 0, int* list2 = nullptr,
+                                                       int value3 = 0, int* list3 = nullptr) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned mb = __ballot_sync(0xffffffffu, want && barrel);
   const unsigned me = __ballot_sync(0xffffffffu, want && !barrel);
@@ -122,6 +123,7 @@ __device__ __forceinline__ void append_two_ended_block(bool want, bool barrel, i
                           : cap - 1 - (sh.base[warp][1] + __popc(me & below));
     list[at] = value;
     if (list2) list2[at] = value2;
+    if (list3) list3[at] = value3;
   }
 }
 
@@ -345,15 +347,15 @@ __global__ void __launch_bounds__(kBlock, MKFG_PROP_MIN_BLOCKS) k_propagate(Even
       const int chg = B.chg[slot];
       const LayerDev& L = C.layer[layer];
       const int ev = E.seed_event[s];
+      const int hit0 = E.layer_begin[ev * E.lb_stride + layer];
       PrepOut o;
       const uint32_t* gbins = E.bins + (size_t)ev * E.n_bins + L.bin_offset;
       if (kStageBins)
         prep_cand<true>(E, C, L, s_key == ev * kMaxLayers + layer ? s_bins : gbins,
-                        E.layer_begin[ev * E.lb_stride + layer], reg, layer, s, B, slot, par, err,
-                        chg, E.xhit + slot, stride, o);
+                        hit0, reg, layer, s, B, slot, par, err, chg, E.xhit + slot, stride, o);
       else
-        prep_cand(E, C, L, gbins, E.layer_begin[ev * E.lb_stride + layer], reg, layer, s, B, slot,
-                  par, err, chg, E.xhit + slot, stride, o);
+        prep_cand(E, C, L, gbins, hit0, reg, layer, s, B, slot, par, err, chg, E.xhit + slot,
+                  stride, o);
       if (o.extra == 2) E.extra_last[slot] = o.extra_last;
 #pragma unroll
       for (int e = 0; e < 6; ++e) E.ppar[e * stride + slot] = o.ppar[e];
@@ -445,7 +447,7 @@ __global__ void __launch_bounds__(kBlock, MKFG_CLONE_MIN_BLOCKS) k_clone(EventDe
   // warp `warp` of the block takes seed base + warp of each round.
   for (int base = blockIdx.x * (kBlock / 32); base < n_find; base += gridDim.x * (kBlock / 32)) {
     const int w = base + warp;
-    int u = 0, g = 0, slot = 0;
+    int u = 0, g = 0, slot = 0, upd_info = 0;
     bool barrel = true;
     if (w < n_find) {
       // A seed finding at this step (listed by the activation kernel).
@@ -473,9 +475,11 @@ __global__ void __launch_bounds__(kBlock, MKFG_CLONE_MIN_BLOCKS) k_clone(EventDe
       u = lane < n ? upd : 0;
       g = u ? hit0 + (u - 1) : 0;
       barrel = C.layer[layer].is_barrel;
+      // The new candidates sit in the other buffer.
+      upd_info = find_info_pack(cur ^ 1, 0, layer);
     }
     append_two_ended_block(u != 0, barrel, slot, E.upd_list, E.list_cap, cnt + kCntUpdBarrel, sh, g,
-                           E.upd_hit);
+                           E.upd_hit, upd_info, E.upd_info);
     __syncwarp();  // hm and scratch are reused by the next seed of this warp
   }
   if (kCount) {
@@ -497,9 +501,9 @@ __global__ void __launch_bounds__(kBlock, MKFG_UPD_MIN_BLOCKS) k_update(EventDev
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nb + ne; j += gridDim.x * blockDim.x) {
     const int at = j < nb ? j : E.list_cap - 1 - (j - nb);
     const int slot = E.upd_list[at];
-    const int s = slot / kSlots;
-    const LayerDev& L = C.layer[plan_layer(C, E.region[s], step)];
-    update_cand_at(E, C, L, E.upd_hit[at], E.cand[E.cur[s]], slot);
+    const int info = E.upd_info[at];
+    const LayerDev& L = C.layer[info >> 5];
+    update_cand_at(E, C, L, E.upd_hit[at], E.cand[info & 1], slot);
   }
 }
 
@@ -1836,6 +1840,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     f->ev.act_list = carve<int>(p, SC);
     f->ev.upd_list = carve<int>(p, SC);
     f->ev.upd_hit = carve<int>(p, SC);
+    f->ev.upd_info = carve<int>(p, SC);
     f->ev.find_list = carve<int>(p, SS);
     f->ev.find_info = carve<int>(p, SS);
     f->ev.list_cap = SC;

@@ -24,6 +24,7 @@ __host__ __device__ constexpr int find_info_pack(int cur, int ncand, int layer) 
   return cur | (ncand << 1) | (layer << 5);
 }
 static_assert(kSlots <= 15 && kMaxLayers <= 256, "find_info_pack field widths");
+
 constexpr int kMaxPlan = 64;
 constexpr int kMaxRegions = 8;
 constexpr int kExportHits = 64;         // Config::nMaxTrkHits
@@ -153,6 +154,10 @@ struct EventDev {
   // (find_info_pack), so the clone kernel starts its loads from one read.
   int* find_list;
   int* find_info;
+  // Beside the update list: the candidate's buffer and layer
+  // (find_info_pack without the count), so the update starts its loads
+  // from its list entry.
+  int* upd_info;
   int* step_count; // [max_steps + 2][kCntN]
   int* err_flags;
   // Pristine initial state (restored by the reset kernel before every run).
