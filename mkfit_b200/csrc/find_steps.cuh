@@ -283,20 +283,32 @@ struct NewCand {
   int is_extra;  // 1: held-back copy (extra), 2: extra with a stop (-2) node
 };
 
+// Every value is loaded before the first store: the compiler cannot tell
+// the two buffers apart, and interleaved loads and stores would wait for
+// one another (37 memory round trips instead of one).
 __device__ __forceinline__ void copy_slot(const CandSoA& from, int fs, const CandSoA& to, int ts) {
+  float par[6], err[21];
 #pragma unroll
-  for (int e = 0; e < 6; ++e) to.par[e * to.cap + ts] = from.par[e * from.cap + fs];
+  for (int e = 0; e < 6; ++e) par[e] = from.par[e * from.cap + fs];
 #pragma unroll
-  for (int e = 0; e < 21; ++e) to.err[e * to.cap + ts] = from.err[e * from.cap + fs];
-  to.chg[ts] = from.chg[fs];
-  to.chi2[ts] = from.chi2[fs];
-  to.score[ts] = from.score[fs];
-  to.last[ts] = from.last[fs];
-  to.nfound[ts] = from.nfound[fs];
-  to.nmiss[ts] = from.nmiss[fs];
-  to.nover[ts] = from.nover[fs];
-  to.ninside[ts] = from.ninside[fs];
-  to.ntail[ts] = from.ntail[fs];
+  for (int e = 0; e < 21; ++e) err[e] = from.err[e * from.cap + fs];
+  const int chg = from.chg[fs], last = from.last[fs], nfound = from.nfound[fs];
+  const int nmiss = from.nmiss[fs], nover = from.nover[fs], ninside = from.ninside[fs];
+  const int ntail = from.ntail[fs];
+  const float chi2 = from.chi2[fs], score = from.score[fs];
+#pragma unroll
+  for (int e = 0; e < 6; ++e) to.par[e * to.cap + ts] = par[e];
+#pragma unroll
+  for (int e = 0; e < 21; ++e) to.err[e * to.cap + ts] = err[e];
+  to.chg[ts] = chg;
+  to.chi2[ts] = chi2;
+  to.score[ts] = score;
+  to.last[ts] = last;
+  to.nfound[ts] = nfound;
+  to.nmiss[ts] = nmiss;
+  to.nover[ts] = nover;
+  to.ninside[ts] = ninside;
+  to.ntail[ts] = ntail;
 }
 
 // TrackCand::addHitIdx counters (mkFit/HitStructures.h:714-735).
@@ -582,13 +594,20 @@ __device__ __forceinline__ void copy_par_err(const CandSoA& B, const CandSoA& N,
   const int pc = __shfl_sync(0xffffffffu, parent, c);
   if (c >= n) return;
   const int src = s * kSlots + pc, dst = s * kSlots + c;
+  // All loads before the first store (the buffers may alias as far as the
+  // compiler knows: interleaved, each store would wait for its load).
+  float v[7];
 #pragma unroll
   for (int k = 0; k < 7; ++k) {
     const int e = (lane >> 3) + 4 * k;
-    if (e >= 27) break;
-    const float* from = e < 6 ? B.par + e * B.cap : B.err + (e - 6) * B.cap;
+    v[k] = 0.f;
+    if (e < 27) v[k] = (e < 6 ? B.par + e * B.cap : B.err + (e - 6) * B.cap)[src];
+  }
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {
+    const int e = (lane >> 3) + 4 * k;
     float* to = e < 6 ? N.par + e * N.cap : N.err + (e - 6) * N.cap;
-    to[dst] = from[src];
+    if (e < 27) to[dst] = v[k];
   }
 }
 
@@ -721,20 +740,21 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
     if (lane < n_extras) {
       if (parent_out) parent_out[lane] = c;
       const int src = s * kSlots + c, dst = s * kSlots + lane;
-      N.chg[dst] = B.chg[src];
-      N.chi2[dst] = B.chi2[src];
-      N.score[dst] = B.score[src];
-      N.nfound[dst] = B.nfound[src];
-      N.nover[dst] = B.nover[src];
-      N.ninside[dst] = B.ninside[src];
-      N.ntail[dst] = B.ntail[src];
-      if (R.extra_kind(c) == 2) {
-        N.last[dst] = R.extra_last(c);
-        N.nmiss[dst] = B.nmiss[src] + 1;
-      } else {
-        N.last[dst] = B.last[src];
-        N.nmiss[dst] = B.nmiss[src];
-      }
+      // Loads first (see copy_slot).
+      const int chg = B.chg[src], nfound = B.nfound[src], nover = B.nover[src];
+      const int ninside = B.ninside[src], ntail = B.ntail[src], nmiss = B.nmiss[src];
+      const float chi2 = B.chi2[src], score = B.score[src];
+      const bool stop = R.extra_kind(c) == 2;
+      const int last = stop ? R.extra_last(c) : B.last[src];
+      N.chg[dst] = chg;
+      N.chi2[dst] = chi2;
+      N.score[dst] = score;
+      N.nfound[dst] = nfound;
+      N.nover[dst] = nover;
+      N.ninside[dst] = ninside;
+      N.ntail[dst] = ntail;
+      N.last[dst] = last;
+      N.nmiss[dst] = nmiss + (stop ? 1 : 0);
       R.set_upd(lane, 0);
     }
     return n_extras;
@@ -922,14 +942,15 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
     if (lane == 0) {
       int nfound = B.nfound[src], nmiss = B.nmiss[src], nin = B.ninside[src], ntl = B.ntail[src];
       float chi2 = B.chi2[src];
+      const int chg = B.chg[src], nover = B.nover[src], last = B.last[src];
       add_hit_counts(-2, 0.f, nfound, nmiss, nin, ntl, chi2);
-      E.bshort.last[s] = arena_put(E, s, node_base - 1, -2, layer, 0.f, B.last[src]);
-      E.bshort.chg[s] = B.chg[src];
+      E.bshort.last[s] = arena_put(E, s, node_base - 1, -2, layer, 0.f, last);
+      E.bshort.chg[s] = chg;
       E.bshort.chi2[s] = chi2;
       E.bshort.score[s] = bs_score;
       E.bshort.nfound[s] = nfound;
       E.bshort.nmiss[s] = nmiss;
-      E.bshort.nover[s] = B.nover[src];
+      E.bshort.nover[s] = nover;
       E.bshort.ninside[s] = nin;
       E.bshort.ntail[s] = ntl;
       E.bshort_valid[s] = 1;
