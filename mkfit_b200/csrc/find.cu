@@ -1128,18 +1128,28 @@ __global__ void k_export(EventDev E, FindOutDev O) {
   }
   const CandSoA& B = E.cand[E.cur[s]];
   const int slot = s * kSlots + c;
-  for (int e = 0; e < 6; ++e) O.par[o * 6 + e] = B.par[e * B.cap + slot];
-  for (int e = 0; e < 21; ++e) O.err[o * 21 + e] = B.err[e * B.cap + slot];
-  O.chg[o] = B.chg[slot];
-  O.chi2[o] = B.chi2[slot];
-  O.score[o] = B.score[slot];
-  O.nfound[o] = B.nfound[slot];
-  const int ntot = B.nfound[slot] + B.nmiss[slot];
-  O.ntot[o] = ntot;
-  O.noverlap[o] = B.nover[slot];
-  O.ninside[o] = B.ninside[slot];
-  O.ntail[o] = B.ntail[slot];
+  // Every value is loaded before the first store, so the loads are in
+  // flight together (the output arrays may alias them as far as the
+  // compiler knows).
+  float par[6], err[21];
+  load_state(B, slot, par, err);
+  const int chg = B.chg[slot], nfound = B.nfound[slot], nmiss = B.nmiss[slot];
+  const int nover = B.nover[slot], ninside = B.ninside[slot], ntail = B.ntail[slot];
+  const float chi2 = B.chi2[slot], score = B.score[slot];
   int node = B.last[slot];
+#pragma unroll
+  for (int e = 0; e < 6; ++e) O.par[o * 6 + e] = par[e];
+#pragma unroll
+  for (int e = 0; e < 21; ++e) O.err[o * 21 + e] = err[e];
+  O.chg[o] = chg;
+  O.chi2[o] = chi2;
+  O.score[o] = score;
+  O.nfound[o] = nfound;
+  const int ntot = nfound + nmiss;
+  O.ntot[o] = ntot;
+  O.noverlap[o] = nover;
+  O.ninside[o] = ninside;
+  O.ntail[o] = ntail;
   for (int k = kExportHits - 1; k >= 0; --k) {
     O.hit_idx[o * kExportHits + k] = -100;
     O.hit_lyr[o * kExportHits + k] = -100;

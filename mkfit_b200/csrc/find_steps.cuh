@@ -583,32 +583,42 @@ __device__ __forceinline__ int score_key(float score) {
   return z != z ? INT_MIN : (k >= 0 ? k : k ^ 0x7fffffff);
 }
 
-// Copies the parameters and covariance of new candidates i < n (parent
-// slot parent_i, lane i of `parent`) from buffer B to buffer N. Lane t
-// moves element t / 8 + 4 k of candidate t % 8: each access of the warp
-// covers four whole 32-byte sectors (a seed's 8 slots are contiguous).
-__device__ __forceinline__ void copy_par_err(const CandSoA& B, const CandSoA& N, int s, int n,
-                                             int parent, int lane) {
-  static_assert(kSlots == 8, "copy_par_err maps 8 slots to lane groups");
+// Copy of the parameters and covariance of new candidates i < n (parent
+// slot parent_i, lane i of `parent`) from buffer B to buffer N, in two
+// halves so a caller can issue the loads early: load_par_err into seven
+// registers per lane, store_par_err from them. Lane t moves element
+// t / 8 + 4 k of candidate t % 8: each access of the warp covers four whole
+// 32-byte sectors (a seed's 8 slots are contiguous).
+__device__ __forceinline__ void load_par_err(const CandSoA& B, int s, int n, int parent, int lane,
+                                             float (&v)[7]) {
   const int c = lane & 7;
   const int pc = __shfl_sync(0xffffffffu, parent, c);
-  if (c >= n) return;
-  const int src = s * kSlots + pc, dst = s * kSlots + c;
-  // All loads before the first store (the buffers may alias as far as the
-  // compiler knows: interleaved, each store would wait for its load).
-  float v[7];
+  const int src = s * kSlots + pc;
 #pragma unroll
   for (int k = 0; k < 7; ++k) {
     const int e = (lane >> 3) + 4 * k;
     v[k] = 0.f;
-    if (e < 27) v[k] = (e < 6 ? B.par + e * B.cap : B.err + (e - 6) * B.cap)[src];
+    if (c < n && e < 27) v[k] = (e < 6 ? B.par + e * B.cap : B.err + (e - 6) * B.cap)[src];
   }
+}
+__device__ __forceinline__ void store_par_err(const CandSoA& N, int s, int n, int lane,
+                                              const float (&v)[7]) {
+  const int c = lane & 7;
+  if (c >= n) return;
+  const int dst = s * kSlots + c;
 #pragma unroll
   for (int k = 0; k < 7; ++k) {
     const int e = (lane >> 3) + 4 * k;
     float* to = e < 6 ? N.par + e * N.cap : N.err + (e - 6) * N.cap;
     if (e < 27) to[dst] = v[k];
   }
+}
+// Both halves at once (all loads before the first store).
+__device__ __forceinline__ void copy_par_err(const CandSoA& B, const CandSoA& N, int s, int n,
+                                             int parent, int lane) {
+  float v[7];
+  load_par_err(B, s, n, parent, lane, v);
+  store_par_err(N, s, n, lane, v);
 }
 
 // Writes a hit-on-track node at arena position pos of seed s (allocated by
@@ -915,6 +925,10 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
     em &= em - 1;
   }
 
+  // The parents' parameters and covariances are loaded now, so the loads
+  // overlap the node and best-short bookkeeping (stored at the end).
+  float pe[7];
+  load_par_err(B, s, n_pushed, nc.parent, lane, pe);
   // Arena nodes of this step, one allocation for the seed: the best short
   // candidate's hole node first, then one or two nodes per new candidate
   // with a hit, in candidate order.
@@ -960,7 +974,7 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
   // Materialize the new candidates into the other buffer: parameters and
   // covariance by all lanes, counters and hit-on-track nodes of new
   // candidate i by lane i.
-  copy_par_err(B, N, s, n_pushed, nc.parent, lane);
+  store_par_err(N, s, n_pushed, lane, pe);
   if (lane < n_pushed) {
     if (parent_out) parent_out[lane] = nc.parent;
     const int pc = nc.parent, dst = s * kSlots + lane;
