@@ -257,7 +257,9 @@ def kernel_rooflines(work, kt, fp32_peak_tf, peaks):
         gbs = clone_bytes / (kt["clone"] * 1e-3) / 1e9
         dom = {"kernel": "k_clone", "bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s",
                "frac": gbs / hbm if hbm else None,
-               "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+               "peak_source": ("fallback HBM copy bandwidth, no MEASURED_PEAKS.json on this "
+                               "machine (of fallback)" if peaks.get("source") == "fallback"
+                               else "MEASURED_PEAKS.json hbm_gbs (of measured)"),
                "per_launch_ms": kt["clone"] / steps,
                "algorithmic_bytes_per_launch": clone_bytes / steps,
                "bytes_model": {"per_candidate": CLONE_BYTES_PER_CAND,
