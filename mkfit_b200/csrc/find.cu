@@ -1465,8 +1465,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   const size_t up_bytes = rounded(12 * (size_t)NHs) + rounded(24 * (size_t)NHs) +
                           2 * rounded(4 * (size_t)NHs) + rounded(4 * n_lb) + rounded((size_t)NHs);
   const size_t hit_bytes = up_bytes + rounded(4 * (size_t)NHs) + rounded(4 * n_bins_all) +
-                           rounded(8 * (size_t)NHs) + rounded(4 * (size_t)NHs) +
-                           rounded(48 * (size_t)NHs);
+                           rounded(16 * (size_t)NHs) + rounded(48 * (size_t)NHs);
   int rc;
   if ((rc = f->hits.ensure(hit_bytes))) return rc;
   if ((rc = f->hits_h.ensure(up_bytes))) return rc;
@@ -1479,8 +1478,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     uint8_t* mask;  // hits masked by earlier iterations (1 = skip)
     uint32_t* info;
     uint32_t* bins;
-    float2* qphi;
-    int* srank;
+    SortedHit* sorted;
     float4* hit4;
   };
   auto layout = [&](char* p, bool device) {
@@ -1494,8 +1492,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     if (device) {
       h.info = carve<uint32_t>(p, NHs);
       h.bins = carve<uint32_t>(p, n_bins_all);
-      h.qphi = carve<float2>(p, NHs);
-      h.srank = carve<int>(p, NHs);
+      h.sorted = carve<SortedHit>(p, NHs);
       h.hit4 = carve<float4>(p, 3 * (size_t)NHs);
     }
     return h;
@@ -1767,8 +1764,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
     A.hinfo = dh.info;
     A.bins = dh.bins;
     A.n_bins = nb;
-    A.qphi = dh.qphi;
-    A.srank = dh.srank;
+    A.sorted = dh.sorted;
     A.mask = any_mask ? dh.mask : nullptr;
     const int smem = hits_smem_bytes(f->max_nq);
     MKFG_CUDA_TRY(cudaFuncSetAttribute(k_layer_hits, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
@@ -1786,8 +1782,7 @@ static int upload_batch(mkfg_context* ctx, Finder* f, const mkfg_event* evs, int
   f->ev.lb_stride = L + 1;
   f->ev.n_bins = nb;
   f->ev.bins = dh.bins;
-  f->ev.qphi = dh.qphi;
-  f->ev.srank = dh.srank;
+  f->ev.sorted_hits = dh.sorted;
   // ---- seeds, candidates, scratch, records, arena
   const int SC = SS * kSlots;
   // Per-step buffers cover the forward run or a backward search, whichever
@@ -2641,9 +2636,10 @@ extern "C" int mkfg_find_hit_index(mkfg_context* ctx, int32_t event, uint32_t* b
   if (bins)
     MKFG_CUDA_TRY(cudaMemcpyAsync(bins, f->ev.bins + (size_t)event * f->ev.n_bins,
                                   4 * (size_t)f->ev.n_bins, cudaMemcpyDeviceToHost, ctx->stream));
-  if (srank && nh > 0)
-    MKFG_CUDA_TRY(cudaMemcpyAsync(srank, f->ev.srank + f->h_hit_off[event], 4 * (size_t)nh,
-                                  cudaMemcpyDeviceToHost, ctx->stream));
+  if (srank && nh > 0)  // the rank column of the sorted hits
+    MKFG_CUDA_TRY(cudaMemcpy2DAsync(srank, 4, &f->ev.sorted_hits[f->h_hit_off[event]].rank,
+                                    sizeof(SortedHit), 4, nh, cudaMemcpyDeviceToHost,
+                                    ctx->stream));
   MKFG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   return MKFG_OK;
 }

@@ -30,6 +30,15 @@ constexpr int kMaxRegions = 8;
 constexpr int kExportHits = 64;         // Config::nMaxTrkHits
 constexpr int kRecInvalid = -1000000;
 
+// A hit of the layer index in sorted order, in one 16-byte word so the
+// hit selection reads the window test's inputs and the hit's index in the
+// layer's input order together: q (z in the barrel, r in the endcaps; +inf
+// for a hit masked by an earlier iteration), phi, and that index.
+struct __align__(16) SortedHit {
+  float q, phi;
+  int rank, unused;
+};
+
 // One IdxChi2List entry of a candidate: a hit (index within the layer) or
 // a hole code (-1, -2, -3), with its module, chi2 and candidate score.
 struct __align__(16) Record {
@@ -103,8 +112,7 @@ struct EventDev {
   int n_bins;             // bins per event
   // Per-layer bins: (first | last << 16) over nq x 256 bins; sorted hits.
   const uint32_t* bins;
-  const float2* qphi;  // (q, phi) of each sorted hit
-  const int* srank;
+  const SortedHit* sorted_hits;
   // Seeds in sorted order (index = seed slot s).
   int n_seeds;
   int* seed_label;   // input index

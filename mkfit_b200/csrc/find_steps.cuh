@@ -175,13 +175,12 @@ __device__ __forceinline__ int select_hits(const EventDev& E, const LayerDev& L,
         const int first = bv[k] & 0xffff, last = bv[k] >> 16;
         for (int hi = first; hi < last; ++hi) {
           if (n >= kMaxXHits) break;
-          const int g = hit_base + hi;
-          const float2 hq = __ldg(E.qphi + g);
-          const float ddq = fabsf(q - hq.x);
-          const float ddphi = cdist(fabsf(phi - hq.y));
+          const float4 hs = __ldg(reinterpret_cast<const float4*>(E.sorted_hits + hit_base + hi));
+          const float ddq = fabsf(q - hs.x);
+          const float ddphi = cdist(fabsf(phi - hs.y));
           if (ddq >= dq) continue;
           if (ddphi >= dphi) continue;
-          xhit[n * xstride] = __ldg(E.srank + g);
+          xhit[n * xstride] = __float_as_int(hs.z);
           ++n;
         }
       }

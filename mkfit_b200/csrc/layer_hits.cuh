@@ -51,8 +51,7 @@ struct LayerHitsArgs {
   uint32_t* hinfo;       // [NH] out, original order
   uint32_t* bins;        // [n_events][n_bins] out
   int n_bins;
-  float2* qphi;          // [NH] out, sorted order
-  int* srank;            // [NH] out, sorted order
+  SortedHit* sorted;     // [NH] out, sorted order
   const uint8_t* mask;   // [NH] hits masked by earlier iterations, or NULL
 };
 
@@ -192,8 +191,7 @@ __global__ void __launch_bounds__(kHitsBlock, MKFG_HITS_MIN_BLOCKS) k_layer_hits
         // MkFinder::SelectHitIndices, mkFit/MkFinder.cc:476-482) keeps its
         // bin but gets q = +inf, which no search window holds.
         const bool masked = A.mask != nullptr && A.mask[h0 + i] != 0;
-        A.qphi[h0 + at] = make_float2(masked ? __int_as_float(0x7f800000) : q, phi);
-        A.srank[h0 + at] = i;
+        A.sorted[h0 + at] = SortedHit{masked ? __int_as_float(0x7f800000) : q, phi, i, 0};
       }
       __syncthreads();
     }
