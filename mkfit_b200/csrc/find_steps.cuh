@@ -666,6 +666,10 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
   const int M = C.max_cands;
   upd_out = 0;
   const int hot0 = E.hot_size[s];
+  // The best short candidate's flag and score, loaded with the seed's
+  // other data rather than one after the other where they are used.
+  const int bs_valid = E.bshort_valid[s];
+  const float bs_score_in = E.bshort.score[s];
 
   // Per-candidate values, staged by lane c for candidate c.
   const int cslot = s * kSlots + (lane < kSlots ? lane : 0);
@@ -852,7 +856,7 @@ __device__ __forceinline__ int clone_seed(const EventDev& E, const FindConfigDev
   // new candidate i.
   NewCand nc{0, 0, 0.f, -1, 0.f, 0};
   int n_pushed = 0;
-  float bs_score = E.bshort_valid[s] ? E.bshort.score[s] : -1e16f;  // getScoreWorstPossible
+  float bs_score = bs_valid ? bs_score_in : -1e16f;  // getScoreWorstPossible
   int bs_from = -1;
   if (extra_mask == 0) {
     // No extras: the new candidates are the records in order, less the
