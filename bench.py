@@ -783,7 +783,10 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded, mkfit_b200.synth.gen_cms_event on the CMS-2017 layer table)",
-        "config": find_config_line(events, 1),
+        # The same config object as this workload's line from the GPU arm at
+        # this world size (rank 0's batch); the reference runs it on rank 0's
+        # host cores alone.
+        "config": find_config_line(events, world),
         "cpu_baseline": {"value": value, "unit": "events/s", "cores": threads, "kind": "reference",
                          "sample": f"all {len(events)} events of the step, in flight on a "
                                    f"{threads}-thread pool, reference find_tracks_load_seeds + "
